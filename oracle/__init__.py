@@ -1,0 +1,384 @@
+"""CPU oracle of the fh-fem iterative solve path (TEST INFRASTRUCTURE ONLY).
+
+A C++17 restatement of femahoy's crates/fem (sparse.rs, heat.rs tet kernels, tet10.rs,
+hex.rs, multigrid.rs, pmultigrid.rs, order.rs, symbolic.rs, cholesky.rs, solve.rs), built
+into ``liboracle.so`` by ``oracle/Makefile`` and loaded here with ctypes. Only the tests, the
+smoke check and the CPU-baseline leg of ``bench.py`` use it, as the checker; the product
+(``femahoy_b200`` / ``libfemgpu.so``) never imports it.
+
+Parity is pinned by the reference's own unit-test known answers (sparse.rs:299-325,
+cholesky.rs:527-560, order.rs:336-348, tet10.rs:302-338) ported in ``tests/test_oracle.py``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_SO = os.path.join(_HERE, "liboracle.so")
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (g++ only)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _SO
+
+
+def _load():
+    if not os.path.exists(_SO):
+        build()
+    lib = C.CDLL(_SO)
+    P, S, D, I = C.c_void_p, C.c_size_t, C.c_double, C.c_int
+    sig = {
+        "orc_pattern": (P, [S, P, S, I]),
+        "orc_csr_import": (P, [S, P, P, P]),
+        "orc_csr_info": (None, [P, P, P]),
+        "orc_csr_export": (None, [P, P, P, P]),
+        "orc_csr_free": (None, [P]),
+        "orc_add_element": (I, [P, P, I, P, P, S]),
+        "orc_mul": (None, [P, P, P]),
+        "orc_submatrix": (P, [P, P, S]),
+        "orc_reduced_rhs": (None, [P, P, P, P, S, P]),
+        "orc_tet_gradients": (None, [P, P, P]),
+        "orc_isotropic": (I, [D, D, P, P, P, S]),
+        "orc_element_matrix": (I, [I, P, P, P]),
+        "orc_assemble": (I, [P, I, P, P, S, P, P, S]),
+        "orc_quadratic": (S, [P, S, P, S, P, P]),
+        "orc_colour": (I, [S, P, S, I, P]),
+        "orc_colour_priority": (C.c_uint32, [C.c_uint32]),
+        "orc_rect_import": (P, [S, S, P, P, P]),
+        "orc_rect_info": (None, [P, P, P, P]),
+        "orc_rect_export": (None, [P, P, P, P]),
+        "orc_rect_free": (None, [P]),
+        "orc_rect_mul": (None, [P, P, P]),
+        "orc_rect_mul_transpose": (None, [P, P, P]),
+        "orc_galerkin": (P, [P, P]),
+        "orc_coarsen": (P, [P, P, S, P, S, P, S, P, P, S, P, P, P]),
+        "orc_prolongation": (P, [P, S, S, P, S, P, S, P, P]),
+        "orc_nested_dissection": (None, [P, P, P]),
+        "orc_direct_solve": (I, [P, P, P, P, P, S]),
+        "orc_solver_new": (P, [P, I, P, S, P, S, P, S, P, P, P, P, P, S, I, I, S, D,
+                               C.c_uint64, I, P, S]),
+        "orc_solver_free": (None, [P]),
+        "orc_solver_method": (I, [P]),
+        "orc_solver_levels": (S, [P]),
+        "orc_solver_level_size": (S, [P, S]),
+        "orc_solver_solve": (I, [P, P, P, D, S, P, P, P, P, S]),
+        "orc_solver_precondition": (None, [P, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+_lib = _load()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class OracleError(RuntimeError):
+    """The reference's error text (its ``Err(String)``)."""
+
+
+class Csr:
+    """sparse.rs:12-17, held by the oracle library."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _lib.orc_csr_free(self.h)
+            self.h = None
+
+    @classmethod
+    def from_arrays(cls, n, ptr, idx, val):
+        ptr = np.ascontiguousarray(ptr, dtype=np.int64)
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        return cls(_lib.orc_csr_import(n, _p(ptr), _p(idx), _p(val)))
+
+    @property
+    def shape(self):
+        n, nnz = C.c_size_t(), C.c_size_t()
+        _lib.orc_csr_info(self.h, C.byref(n), C.byref(nnz))
+        return n.value, nnz.value
+
+    @property
+    def n(self):
+        return self.shape[0]
+
+    def arrays(self):
+        n, nnz = self.shape
+        ptr = np.empty(n + 1, np.int64)
+        idx = np.empty(nnz, np.uint32)
+        val = np.empty(nnz, np.float64)
+        _lib.orc_csr_export(self.h, _p(ptr), _p(idx), _p(val))
+        return ptr, idx, val
+
+    def add_element(self, nodes, ke):
+        nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+        ke = np.ascontiguousarray(ke, dtype=np.float64)
+        err = C.create_string_buffer(512)
+        if _lib.orc_add_element(self.h, _p(nodes), len(nodes), _p(ke), err, 512):
+            raise OracleError(err.value.decode())
+
+    def mul(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.n)
+        _lib.orc_mul(self.h, _p(x), _p(y))
+        return y
+
+    def submatrix(self, keep):
+        keep = np.ascontiguousarray(keep, dtype=np.int64)
+        return Csr(_lib.orc_submatrix(self.h, _p(keep), len(keep)))
+
+    def reduced_rhs(self, load, t, free):
+        load = np.ascontiguousarray(load, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        free = np.ascontiguousarray(free, dtype=np.int64)
+        out = np.empty(len(free))
+        _lib.orc_reduced_rhs(self.h, _p(load), _p(t), _p(free), len(free), _p(out))
+        return out
+
+    def assemble(self, kind, xyz, nodes, coef):
+        """Add every element, in increasing element order (heat.rs:920-927,
+        elastic_tet.rs:183-193). kind 0 = P1 heat, 1 = P1 elasticity, 2 = P2 elasticity."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
+        coef = np.ascontiguousarray(coef, dtype=np.float64)
+        err = C.create_string_buffer(512)
+        if _lib.orc_assemble(self.h, kind, _p(xyz), _p(nodes), nodes.shape[0], _p(coef), err,
+                             512):
+            raise OracleError(err.value.decode())
+
+
+def pattern(n, elements):
+    """sparse.rs:22-65 for elements of equal size (rows of ``elements``)."""
+    e = np.ascontiguousarray(elements, dtype=np.uint32)
+    return Csr(_lib.orc_pattern(n, _p(e), e.shape[0], e.shape[1]))
+
+
+def dof_elements(nodes):
+    """The unknowns 3 node + component of each element (elastic_tet.rs:178-182)."""
+    nodes = np.asarray(nodes, dtype=np.uint32)
+    m = nodes.shape[1]
+    return (3 * np.repeat(nodes, 3, axis=1) + np.tile(np.arange(3, dtype=np.uint32), m)).astype(
+        np.uint32)
+
+
+def tet_gradients(p):
+    p = np.ascontiguousarray(p, dtype=np.float64).reshape(12)
+    g = np.empty(12)
+    v = C.c_double()
+    _lib.orc_tet_gradients(_p(p), _p(g), C.byref(v))
+    return g.reshape(4, 3), v.value
+
+
+def element_matrix(kind, p, coef):
+    p = np.ascontiguousarray(p, dtype=np.float64).reshape(12)
+    coef = np.ascontiguousarray(coef, dtype=np.float64)
+    m = {0: 4, 1: 12, 2: 30}[kind]
+    ke = np.empty(m * m)
+    _lib.orc_element_matrix(kind, _p(p), _p(coef), _p(ke))
+    return ke.reshape(m, m)
+
+
+def isotropic(e, nu):
+    normal = np.empty(9)
+    shear = np.empty(3)
+    err = C.create_string_buffer(512)
+    if _lib.orc_isotropic(e, nu, _p(normal), _p(shear), err, 512):
+        raise OracleError(err.value.decode())
+    return normal.reshape(3, 3), shear
+
+
+def quadratic(xyz, tets):
+    """tet10.rs:244-272: (edges (E, 2), tets10 (T, 10))."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    tets = np.ascontiguousarray(tets, dtype=np.uint32)
+    edges = np.empty((6 * len(tets), 2), np.uint32)
+    t10 = np.empty((len(tets), 10), np.uint32)
+    ne = _lib.orc_quadratic(_p(xyz), len(xyz), _p(tets), len(tets), _p(edges), _p(t10))
+    return edges[:ne].copy(), t10
+
+
+def colour(n, elements):
+    e = np.ascontiguousarray(elements, dtype=np.uint32)
+    out = np.empty(e.shape[0], np.uint32)
+    nc = _lib.orc_colour(n, _p(e), e.shape[0], e.shape[1], _p(out))
+    return out, nc
+
+
+class Rect:
+    """sparse.rs:202-293, held by the oracle library."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _lib.orc_rect_free(self.h)
+            self.h = None
+
+    @classmethod
+    def from_arrays(cls, rows, cols, ptr, idx, val):
+        ptr = np.ascontiguousarray(ptr, dtype=np.int64)
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        return cls(_lib.orc_rect_import(rows, cols, _p(ptr), _p(idx), _p(val)))
+
+    @property
+    def shape(self):
+        r, c, nnz = C.c_size_t(), C.c_size_t(), C.c_size_t()
+        _lib.orc_rect_info(self.h, C.byref(r), C.byref(c), C.byref(nnz))
+        return r.value, c.value, nnz.value
+
+    def arrays(self):
+        r, _, nnz = self.shape
+        ptr = np.empty(r + 1, np.int64)
+        idx = np.empty(nnz, np.uint32)
+        val = np.empty(nnz, np.float64)
+        _lib.orc_rect_export(self.h, _p(ptr), _p(idx), _p(val))
+        return ptr, idx, val
+
+    def mul(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.shape[0])
+        _lib.orc_rect_mul(self.h, _p(x), _p(y))
+        return y
+
+    def mul_transpose(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty(self.shape[1])
+        _lib.orc_rect_mul_transpose(self.h, _p(x), _p(y))
+        return y
+
+    def galerkin(self, a: Csr) -> Csr:
+        return Csr(_lib.orc_galerkin(self.h, a.h))
+
+
+def _level_args(planes, points, comp):
+    px, py, pz = (np.ascontiguousarray(p, dtype=np.float64) for p in planes)
+    pts = np.ascontiguousarray(points, dtype=np.uint32)
+    cmp_ = np.ascontiguousarray(comp, dtype=np.uint8)
+    return (px, py, pz, pts, cmp_)
+
+
+def coarsen(a: Csr, planes, points, comp):
+    """multigrid.rs:329-452: (P, coarse points, coarse comp) or None."""
+    px, py, pz, pts, cmp_ = _level_args(planes, points, comp)
+    n = len(pts)
+    cp = np.empty((n, 3), np.uint32)
+    cc = np.empty(n, np.uint8)
+    cn = C.c_size_t()
+    h = _lib.orc_coarsen(a.h, _p(px), len(px), _p(py), len(py), _p(pz), len(pz), _p(pts),
+                         _p(cmp_), n, _p(cp), _p(cc), C.byref(cn))
+    if not h:
+        return None
+    return Rect(h), cp[:cn.value].copy(), cc[:cn.value].copy()
+
+
+def prolongation(points, corners, edges, free):
+    """pmultigrid.rs:104-151: (P, coarse xyz)."""
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    e = np.ascontiguousarray(edges, dtype=np.uint32)
+    f = np.ascontiguousarray(free, dtype=np.int64)
+    cxyz = np.empty((len(f), 3))
+    nc = C.c_size_t()
+    h = _lib.orc_prolongation(_p(pts), len(pts), corners, _p(e), len(e), _p(f), len(f),
+                              _p(cxyz), C.byref(nc))
+    return Rect(h), cxyz[:nc.value].copy()
+
+
+def nested_dissection(a: Csr, xyz):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    out = np.empty(a.n, np.int64)
+    _lib.orc_nested_dissection(a.h, _p(xyz), _p(out))
+    return out
+
+
+def direct_solve(a: Csr, xyz, b):
+    """The FP64 direct oracle: nested dissection, symbolic analysis and the multifrontal
+    Cholesky factor (order.rs, symbolic.rs, cholesky.rs). Returns (x, factor entries)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    x = np.array(b, dtype=np.float64, copy=True)
+    entries = C.c_uint64()
+    err = C.create_string_buffer(512)
+    if _lib.orc_direct_solve(a.h, _p(xyz), _p(x), C.byref(entries), err, 512):
+        raise OracleError(err.value.decode())
+    return x, entries.value
+
+
+class Solver:
+    """solve.rs:58-250. ``kind``: 'grid' (planes, points, comp), 'points' (xyz) or
+    'quadratic' (xyz, p: Rect, coarse xyz). ``method``: None, 'direct' or 'multigrid'."""
+
+    def __init__(self, a: Csr, kind, *, planes=None, points=None, comp=None, xyz=None, p=None,
+                 coarse=None, method=None, crossover=("unknowns", 3000)):
+        err = C.create_string_buffer(512)
+        k = {"grid": 0, "points": 1, "quadratic": 2}[kind]
+        m = {None: -1, "direct": 0, "multigrid": 1}[method]
+        px = py = pz = pts = cmp_ = xyz_ = cx = None
+        nx = ny = nz = 0
+        if k == 0:
+            px, py, pz, pts, cmp_ = _level_args(planes, points, comp)
+            nx, ny, nz = len(px), len(py), len(pz)
+        if k >= 1:
+            xyz_ = np.ascontiguousarray(xyz, dtype=np.float64)
+        nc = 0
+        if k == 2:
+            cx = np.ascontiguousarray(coarse, dtype=np.float64)
+            nc = len(cx)
+        if crossover[0] == "unknowns":
+            fr, un, fl, en, flat = 0, crossover[1], 0.0, 0, 0
+        else:
+            fr, un = 1, 0
+            fl, en, flat = crossover[1], crossover[2], int(crossover[3])
+        self.h = _lib.orc_solver_new(a.h, k, _p(px), nx, _p(py), ny, _p(pz), nz, _p(pts),
+                                     _p(cmp_), _p(xyz_), p.h if p is not None else None, _p(cx),
+                                     nc, m, fr, un, fl, en, flat, err, 512)
+        if not self.h:
+            raise OracleError(err.value.decode())
+        self.n = a.n
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            _lib.orc_solver_free(self.h)
+            self.h = None
+
+    def method(self):
+        return ["direct", "multigrid"][_lib.orc_solver_method(self.h)]
+
+    def levels(self):
+        return [_lib.orc_solver_level_size(self.h, i)
+                for i in range(_lib.orc_solver_levels(self.h))]
+
+    def solve(self, b, x=None, tol=0.0, max_iter=0, cancel=None):
+        """Returns (x, iterations, residual); raises OracleError with the reference text."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x is None else np.array(x, dtype=np.float64, copy=True)
+        it, res = C.c_size_t(), C.c_double()
+        err = C.create_string_buffer(512)
+        flag = None
+        if cancel is not None:
+            flag = C.c_int(int(cancel))
+        st = _lib.orc_solver_solve(self.h, _p(b), _p(x), tol, max_iter,
+                                   C.byref(flag) if flag is not None else None, C.byref(it),
+                                   C.byref(res), err, 512)
+        if st:
+            raise OracleError(err.value.decode())
+        return x, it.value, res.value
+
+    def precondition(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros(self.n)
+        _lib.orc_solver_precondition(self.h, _p(r), _p(z))
+        return z

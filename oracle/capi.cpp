@@ -1,0 +1,364 @@
+// Oracle (test infrastructure): a C interface over the restatement, loaded with ctypes by the
+// tests, the smoke check and the CPU-baseline leg of the benchmark. Handles own C++ objects;
+// a function that fails returns a negative status and writes the reference's error text to
+// the caller's buffer.
+#include <atomic>
+#include <cstring>
+#include <memory>
+#include <thread>
+
+#include "oracle.hpp"
+
+using namespace orc;
+
+namespace {
+void put_error(char* buf, size_t len, const char* what) {
+    if (buf && len) {
+        std::strncpy(buf, what, len - 1);
+        buf[len - 1] = 0;
+    }
+}
+Csr* C(void* h) { return static_cast<Csr*>(h); }
+Rect* R(void* h) { return static_cast<Rect*>(h); }
+
+Level make_level(const double* px, size_t nx, const double* py, size_t ny, const double* pz,
+                 size_t nz, const uint32_t* points, const uint8_t* comp, size_t n) {
+    Level l;
+    l.planes[0].assign(px, px + nx);
+    l.planes[1].assign(py, py + ny);
+    l.planes[2].assign(pz, pz + nz);
+    l.points.resize(n);
+    for (size_t k = 0; k < n; ++k)
+        for (int d = 0; d < 3; ++d) l.points[k][d] = points[3 * k + d];
+    l.comp.assign(comp, comp + n);
+    return l;
+}
+vector<Vec3> make_points(const double* xyz, size_t n) {
+    vector<Vec3> v(n);
+    for (size_t k = 0; k < n; ++k) v[k] = {xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2]};
+    return v;
+}
+
+// Element loops share the work among threads by element range only when the caller asks for
+// it (the values are independent per element; the assembly itself is sequential).
+void tet_points(const double* xyz, const uint32_t* t, Vec3 p[4]) {
+    for (int c = 0; c < 4; ++c)
+        for (int d = 0; d < 3; ++d) p[c][d] = xyz[3 * (size_t)t[c] + d];
+}
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------- Csr
+void* orc_pattern(size_t n, const uint32_t* elements, size_t nel, int m) {
+    return new Csr(pattern(n, elements, nel, m));
+}
+void* orc_csr_import(size_t n, const int64_t* ptr, const uint32_t* idx, const double* val) {
+    Csr* a = new Csr;
+    a->n = n;
+    a->ptr.assign(ptr, ptr + n + 1);
+    size_t nnz = (size_t)ptr[n];
+    a->idx.assign(idx, idx + nnz);
+    a->val.assign(val, val + nnz);
+    return a;
+}
+void orc_csr_info(void* h, size_t* n, size_t* nnz) {
+    *n = C(h)->n;
+    *nnz = C(h)->idx.size();
+}
+void orc_csr_export(void* h, int64_t* ptr, uint32_t* idx, double* val) {
+    Csr* a = C(h);
+    for (size_t i = 0; i <= a->n; ++i) ptr[i] = (int64_t)a->ptr[i];
+    if (idx) std::memcpy(idx, a->idx.data(), a->idx.size() * 4);
+    if (val) std::memcpy(val, a->val.data(), a->val.size() * 8);
+}
+void orc_csr_free(void* h) { delete C(h); }
+int orc_add_element(void* h, const uint32_t* nodes, int m, const double* ke, char* err,
+                    size_t len) {
+    try {
+        C(h)->add_element(nodes, m, ke);
+        return 0;
+    } catch (const std::exception& e) {
+        put_error(err, len, e.what());
+        return -1;
+    }
+}
+void orc_mul(void* h, const double* x, double* y) { C(h)->mul(x, y); }
+void* orc_submatrix(void* h, const int64_t* keep, size_t nkeep) {
+    vector<size_t> k(keep, keep + nkeep);
+    return new Csr(C(h)->submatrix(k));
+}
+void orc_reduced_rhs(void* h, const double* load, const double* t, const int64_t* free,
+                     size_t nfree, double* out) {
+    vector<size_t> f(free, free + nfree);
+    vector<double> r = reduced_rhs(*C(h), load, t, f);
+    std::memcpy(out, r.data(), nfree * 8);
+}
+
+// ---------------------------------------------------------------- elements
+void orc_tet_gradients(const double* p12, double* g12, double* volume) {
+    Vec3 p[4], g[4];
+    for (int c = 0; c < 4; ++c)
+        for (int d = 0; d < 3; ++d) p[c][d] = p12[3 * c + d];
+    tet_gradients(p, g, volume);
+    for (int c = 0; c < 4; ++c)
+        for (int d = 0; d < 3; ++d) g12[3 * c + d] = g[c][d];
+}
+int orc_isotropic(double e, double nu, double* normal9, double* shear3, char* err, size_t len) {
+    try {
+        Stiffness d = isotropic_stiffness(e, nu);
+        std::memcpy(normal9, d.normal, 72);
+        std::memcpy(shear3, d.shear, 24);
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+// The element matrix of 1 tetrahedron: kind 0 = P1 heat (4 x 4, `coef` = 3 conductivities),
+// 1 = P1 elasticity (12 x 12, `coef` = E, nu), 2 = P2 elasticity (30 x 30, `coef` = E, nu).
+int orc_element_matrix(int kind, const double* p12, const double* coef, double* ke) {
+    Vec3 p[4], g[4];
+    double v;
+    for (int c = 0; c < 4; ++c)
+        for (int d = 0; d < 3; ++d) p[c][d] = p12[3 * c + d];
+    tet_gradients(p, g, &v);
+    if (kind == 0) {
+        tet_conduction(g, v, Vec3{coef[0], coef[1], coef[2]}, ke);
+        return 0;
+    }
+    Stiffness d = isotropic_stiffness(coef[0], coef[1]);
+    if (kind == 1)
+        tet4_stiffness(g, v, d, ke);
+    else
+        tet10_stiffness(g, v, d, ke);
+    return 0;
+}
+
+// Assemble all the elements of a mesh into the pattern `h`, in increasing element order
+// (heat.rs:920-927, elastic_tet.rs:183-193). kind as orc_element_matrix; `nodes` are 4 corners
+// (kind 0, 1) or 10 points (kind 2) per element; `coef` has 3 (kind 0) or 2 values per element.
+// The scalar nodes of kinds 1 and 2 become the unknowns 3 node + component.
+int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, size_t nel,
+                 const double* coef, char* err, size_t len) {
+    try {
+        Csr* a = C(h);
+        int mn = kind == 2 ? 10 : 4;
+        int m = kind == 0 ? 4 : 3 * mn;
+        vector<double> ke(m * m);
+        vector<uint32_t> dofs(m);
+        for (size_t e = 0; e < nel; ++e) {
+            const uint32_t* t = nodes + e * mn;
+            Vec3 p[4], g[4];
+            double v;
+            tet_points(xyz, t, p);
+            tet_gradients(p, g, &v);
+            if (kind == 0) {
+                const double* k = coef + 3 * e;
+                tet_conduction(g, v, Vec3{k[0], k[1], k[2]}, ke.data());
+                a->add_element(t, 4, ke.data());
+                continue;
+            }
+            Stiffness d = isotropic_stiffness(coef[2 * e], coef[2 * e + 1]);
+            if (kind == 1)
+                tet4_stiffness(g, v, d, ke.data());
+            else
+                tet10_stiffness(g, v, d, ke.data());
+            for (int k = 0; k < m; ++k) dofs[k] = 3 * t[k / 3] + (uint32_t)(k % 3);
+            a->add_element(dofs.data(), m, ke.data());
+        }
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+
+// tet10.rs:244-272. Writes the edges (2 per edge) and the 10-point tetrahedra; returns the
+// number of edges. `edges` must hold 2 * 6 * ntet values.
+size_t orc_quadratic(const double* xyz, size_t ncorner, const uint32_t* tets, size_t ntet,
+                     uint32_t* edges, uint32_t* tets10) {
+    vector<Vec3> pts = make_points(xyz, ncorner);
+    vector<array<uint32_t, 4>> t(ntet);
+    for (size_t e = 0; e < ntet; ++e)
+        for (int c = 0; c < 4; ++c) t[e][c] = tets[4 * e + c];
+    Quadratic q = quadratic(pts, t);
+    for (size_t k = 0; k < q.edges.size(); ++k) {
+        edges[2 * k] = q.edges[k][0];
+        edges[2 * k + 1] = q.edges[k][1];
+    }
+    for (size_t e = 0; e < ntet; ++e)
+        for (int c = 0; c < 10; ++c) tets10[10 * e + c] = q.tets[e][c];
+    return q.edges.size();
+}
+
+int orc_colour(size_t n, const uint32_t* elements, size_t nel, int m, uint32_t* colour) {
+    int nc = 0;
+    vector<uint32_t> c = colour_elements(n, elements, nel, m, &nc);
+    std::memcpy(colour, c.data(), nel * 4);
+    return nc;
+}
+uint32_t orc_colour_priority(uint32_t e) { return colour_priority(e); }
+
+// ---------------------------------------------------------------- Rect
+void* orc_rect_import(size_t rows, size_t cols, const int64_t* ptr, const uint32_t* idx,
+                      const double* val) {
+    Rect* p = new Rect;
+    p->rows = rows;
+    p->cols = cols;
+    p->ptr.assign(ptr, ptr + rows + 1);
+    size_t nnz = (size_t)ptr[rows];
+    p->idx.assign(idx, idx + nnz);
+    p->val.assign(val, val + nnz);
+    return p;
+}
+void orc_rect_info(void* h, size_t* rows, size_t* cols, size_t* nnz) {
+    *rows = R(h)->rows;
+    *cols = R(h)->cols;
+    *nnz = R(h)->idx.size();
+}
+void orc_rect_export(void* h, int64_t* ptr, uint32_t* idx, double* val) {
+    Rect* p = R(h);
+    for (size_t i = 0; i <= p->rows; ++i) ptr[i] = (int64_t)p->ptr[i];
+    std::memcpy(idx, p->idx.data(), p->idx.size() * 4);
+    std::memcpy(val, p->val.data(), p->val.size() * 8);
+}
+void orc_rect_free(void* h) { delete R(h); }
+void orc_rect_mul(void* h, const double* x, double* y) { R(h)->mul(x, y); }
+void orc_rect_mul_transpose(void* h, const double* x, double* y) { R(h)->mul_transpose(x, y); }
+void* orc_galerkin(void* p, void* a) { return new Csr(R(p)->galerkin(*C(a))); }
+
+// multigrid.rs:329-452. Returns P (a Rect handle) or null; the coarse level's points and
+// components go to `cpoints` (3 per unknown) and `ccomp`, sized like the fine level.
+void* orc_coarsen(void* a, const double* px, size_t nx, const double* py, size_t ny,
+                  const double* pz, size_t nz, const uint32_t* points, const uint8_t* comp,
+                  size_t n, uint32_t* cpoints, uint8_t* ccomp, size_t* cn) {
+    Level fine = make_level(px, nx, py, ny, pz, nz, points, comp, n);
+    Rect* p = new Rect;
+    Level coarse;
+    if (!coarsen(fine, *C(a), p, &coarse)) {
+        delete p;
+        return nullptr;
+    }
+    *cn = coarse.points.size();
+    for (size_t k = 0; k < coarse.points.size(); ++k)
+        for (int d = 0; d < 3; ++d) cpoints[3 * k + d] = coarse.points[k][d];
+    std::memcpy(ccomp, coarse.comp.data(), coarse.comp.size());
+    return p;
+}
+
+// pmultigrid.rs:104-151. Returns P; the coarse points go to `cxyz` (3 per coarse unknown;
+// room for 3 * nfree values).
+void* orc_prolongation(const double* points, size_t npoints, size_t corners,
+                       const uint32_t* edges, size_t nedges, const int64_t* free, size_t nfree,
+                       double* cxyz, size_t* ncoarse) {
+    vector<Vec3> pts = make_points(points, npoints);
+    vector<array<uint32_t, 2>> e(nedges);
+    for (size_t k = 0; k < nedges; ++k) e[k] = {edges[2 * k], edges[2 * k + 1]};
+    vector<size_t> f(free, free + nfree);
+    Rect* p = new Rect;
+    vector<Vec3> xyz;
+    prolongation(pts, corners, e, f, p, &xyz);
+    *ncoarse = xyz.size();
+    for (size_t k = 0; k < xyz.size(); ++k)
+        for (int d = 0; d < 3; ++d) cxyz[3 * k + d] = xyz[k][d];
+    return p;
+}
+
+// ---------------------------------------------------------------- direct
+void orc_nested_dissection(void* a, const double* xyz, int64_t* order) {
+    vector<size_t> o = nested_dissection(*C(a), make_points(xyz, C(a)->n));
+    for (size_t k = 0; k < o.size(); ++k) order[k] = (int64_t)o[k];
+}
+// Factor and solve in place; returns 0 or -1 with the error text. `entries` gets the factor's
+// entries (symbolic.rs:162).
+int orc_direct_solve(void* a, const double* xyz, double* b, uint64_t* entries, char* err,
+                     size_t len) {
+    try {
+        Symbolic sym = analyse(*C(a), nested_dissection(*C(a), make_points(xyz, C(a)->n)));
+        if (entries) *entries = sym.entries();
+        Cholesky ch = factor(sym, *C(a));
+        ch.solve(b);
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+
+// ---------------------------------------------------------------- Solver
+struct OSolver {
+    Solver s;
+};
+
+// unknowns kind 0 = Grid (planes, points, comp), 1 = Points (xyz), 2 = Quadratic (xyz of each
+// unknown, P as a Rect handle, coarse xyz). method -1 none, 0 direct, 1 multigrid.
+// crossover: flops_rule 0 -> Unknowns(unknowns); 1 -> Flops{flops, entries, flat}.
+void* orc_solver_new(void* a, int kind, const double* px, size_t nx, const double* py,
+                     size_t ny, const double* pz, size_t nz, const uint32_t* points,
+                     const uint8_t* comp, const double* xyz, void* p, const double* cxyz,
+                     size_t ncoarse, int method, int flops_rule, size_t unknowns, double flops,
+                     uint64_t entries, int flat, char* err, size_t len) {
+    try {
+        Unknowns u;
+        size_t n = C(a)->n;
+        u.kind = (Unknowns::Kind)kind;
+        if (kind == 0) u.level = make_level(px, nx, py, ny, pz, nz, points, comp, n);
+        if (kind >= 1) u.points = make_points(xyz, n);
+        if (kind == 2) {
+            u.p = *R(p);
+            u.coarse = make_points(cxyz, ncoarse);
+        }
+        Crossover c;
+        c.flops_rule = flops_rule != 0;
+        c.unknowns = unknowns;
+        c.flops = flops;
+        c.entries = entries;
+        c.flat = flat != 0;
+        auto* s = new OSolver;
+        s->s = Solver::make(*C(a), std::move(u), method, c);
+        return s;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return nullptr;
+    }
+}
+void orc_solver_free(void* s) { delete static_cast<OSolver*>(s); }
+int orc_solver_method(void* s) { return (int)static_cast<OSolver*>(s)->s.method(); }
+size_t orc_solver_levels(void* s) {
+    auto* o = static_cast<OSolver*>(s);
+    return o->s.inner == Solver::MG ? o->s.mg.levels() : (o->s.inner == Solver::PMG ? 2 : 1);
+}
+size_t orc_solver_level_size(void* s, size_t l) {
+    auto* o = static_cast<OSolver*>(s);
+    if (o->s.inner == Solver::MG) return o->s.mg.a[l].n;
+    if (o->s.inner == Solver::PMG) return l == 0 ? o->s.a.n : o->s.pmg.coarse_unknowns;
+    return o->s.a.n;
+}
+// `cancel` (may be null) is read before each PCG iteration, as the reference's `cancelled`.
+int orc_solver_solve(void* s, const double* b, double* x, double tol, size_t max_iter,
+                     const volatile int* cancel, size_t* iterations, double* residual,
+                     char* err, size_t len) {
+    auto* o = static_cast<OSolver*>(s);
+    try {
+        if (tol > 0) o->s.tol = tol;
+        if (max_iter > 0) o->s.max_iter = max_iter;
+        Stats st = o->s.solve(b, x, [cancel] { return cancel && *cancel != 0; });
+        *iterations = st.iterations;
+        *residual = st.residual;
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+// z = M^-1 r of the solver's preconditioner (1 V-cycle).
+void orc_solver_precondition(void* s, const double* r, double* z) {
+    auto* o = static_cast<OSolver*>(s);
+    if (o->s.inner == Solver::MG)
+        o->s.mg.apply(r, z);
+    else if (o->s.inner == Solver::PMG)
+        o->s.pmg.apply(o->s.a, r, z);
+}
+
+}  // extern "C"

@@ -1,0 +1,269 @@
+// Oracle (test infrastructure): the element kernels of the path. Restates
+// crates/fem/src/heat.rs:972-1002, 1219-1244, crates/fem/src/hex.rs:58-114 and
+// crates/fem/src/tet10.rs:38-120, 232-272. The 4-node elasticity tetrahedron is this
+// project's own (the reference solves elasticity on tets only with 10 nodes).
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <unordered_map>
+
+#include "oracle.hpp"
+
+namespace orc {
+
+// heat.rs:983-1002
+void tet_gradients(const Vec3 p[4], Vec3 g[4], double* volume) {
+    double e[3][3];
+    for (int k = 0; k < 3; ++k)
+        for (int d = 0; d < 3; ++d) e[k][d] = p[k + 1][d] - p[0][d];
+    auto cross = [](const double* a, const double* b, double* c) {
+        c[0] = a[1] * b[2] - a[2] * b[1];
+        c[1] = a[2] * b[0] - a[0] * b[2];
+        c[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    double det = e[0][0] * (e[1][1] * e[2][2] - e[1][2] * e[2][1]) -
+                 e[0][1] * (e[1][0] * e[2][2] - e[1][2] * e[2][0]) +
+                 e[0][2] * (e[1][0] * e[2][1] - e[1][1] * e[2][0]);
+    double rows[3][3];
+    cross(e[1], e[2], rows[0]);
+    cross(e[2], e[0], rows[1]);
+    cross(e[0], e[1], rows[2]);
+    for (int k = 0; k < 3; ++k)
+        for (int d = 0; d < 3; ++d) g[k + 1][d] = rows[k][d] / det;
+    for (int d = 0; d < 3; ++d) g[0][d] = -(g[1][d] + g[2][d] + g[3][d]);
+    *volume = det / 6.0;
+}
+
+// heat.rs:972-981. The Rust float sum starts from -0.0, the exact additive identity, so it
+// equals ((t0 + t1) + t2).
+void tet_conduction(const Vec3 g[4], double v, const Vec3& k, double ke[16]) {
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double s = k[0] * g[i][0] * g[j][0];
+            s = s + k[1] * g[i][1] * g[j][1];
+            s = s + k[2] * g[i][2] * g[j][2];
+            ke[i * 4 + j] = v * s;
+        }
+}
+
+// heat.rs:1219-1244 with `transient = None`.
+vector<double> reduced_rhs(const Csr& a, const double* load, const double* t,
+                           const vector<size_t>& free) {
+    vector<double> out(free.size());
+    for (size_t k = 0; k < free.size(); ++k) {
+        size_t i = free[k];
+        double r = load[i];
+        for (size_t e = a.ptr[i]; e < a.ptr[i + 1]; ++e) {
+            size_t j = a.idx[e];
+            if (!std::binary_search(free.begin(), free.end(), j)) r -= a.val[e] * t[j];
+        }
+        out[k] = r;
+    }
+    return out;
+}
+
+// hex.rs:69-114
+Stiffness orthotropic_stiffness(const double e[3], const double nu[3], const double g[3]) {
+    for (int i = 0; i < 3; ++i)
+        if (!(std::isfinite(e[i]) && e[i] > 0.0 && std::isfinite(g[i]) && g[i] > 0.0) ||
+            !std::isfinite(nu[i]))
+            throw Error("the moduli must be above 0 and the Poisson ratios finite");
+    double ex = e[0], ey = e[1], ez = e[2];
+    double nxy = nu[0], nxz = nu[1], nyz = nu[2];
+    double s[3][3] = {{1.0 / ex, -nxy / ex, -nxz / ex},
+                      {-nxy / ex, 1.0 / ey, -nyz / ey},
+                      {-nxz / ex, -nyz / ey, 1.0 / ez}};
+    double det = s[0][0] * (s[1][1] * s[2][2] - s[1][2] * s[2][1]) -
+                 s[0][1] * (s[1][0] * s[2][2] - s[1][2] * s[2][0]) +
+                 s[0][2] * (s[1][0] * s[2][1] - s[1][1] * s[2][0]);
+    double minor = s[0][0] * s[1][1] - s[0][1] * s[1][0];
+    if (!(minor > 0.0 && det > 1e-12 * s[0][0] * s[1][1] * s[2][2]))
+        throw Error(
+            "the Poisson ratios give no stable material (for an isotropic material, nu must be "
+            "between -1 and 0.5)");
+    Stiffness d;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            d.normal[i][j] = (s[j1][i1] * s[j2][i2] - s[j1][i2] * s[j2][i1]) / det;
+        }
+    d.shear[0] = g[2];  // G_yz
+    d.shear[1] = g[1];  // G_xz
+    d.shear[2] = g[0];  // G_xy
+    return d;
+}
+
+// hex.rs:58-64
+Stiffness isotropic_stiffness(double e, double nu) {
+    double ee[3] = {e, e, e}, nn[3] = {nu, nu, nu};
+    double gg = e / (2.0 * (1.0 + nu));
+    double g[3] = {gg, gg, gg};
+    return orthotropic_stiffness(ee, nn, g);
+}
+
+// tet10.rs:41: the 2 axes of each shear strain (yz, xz, xy).
+static const int SHEAR[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+// tet10.rs:38
+static const int EDGES[6][2] = {{0, 1}, {1, 2}, {0, 2}, {0, 3}, {1, 3}, {2, 3}};
+
+// The (a, b) term of the B^T D B integrand of 2 node gradients: tet10.rs:101-112.
+static inline double elastic_term(const double* gi, const double* gj, int a, int b,
+                                  const Stiffness& d) {
+    double v = gi[a] * gj[b] * d.normal[a][b];
+    if (a == b) {
+        for (int s = 0; s < 3; ++s) {
+            int p = SHEAR[s][0], q = SHEAR[s][1];
+            if (p == a)
+                v += gi[q] * gj[q] * d.shear[s];
+            else if (q == a)
+                v += gi[p] * gj[p] * d.shear[s];
+        }
+    } else {
+        v += gi[b] * gj[a] * d.shear[3 - a - b];
+    }
+    return v;
+}
+
+// tet10.rs:44-48 and 77-87: the 4-point rule of degree 2 and the gradients of the 10 functions.
+void tet10_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k[900]) {
+    const double A = 0.5854101966249685, B = 0.1381966011250105;
+    std::fill(k, k + 900, 0.0);
+    double w = volume / 4.0;
+    for (int q = 0; q < 4; ++q) {
+        double l[4];
+        for (int c = 0; c < 4; ++c) l[c] = (c == q) ? A : B;
+        double gr[10][3];
+        for (int i = 0; i < 4; ++i)
+            for (int dd = 0; dd < 3; ++dd) gr[i][dd] = (4.0 * l[i] - 1.0) * g[i][dd];
+        for (int e = 0; e < 6; ++e) {
+            int i = EDGES[e][0], j = EDGES[e][1];
+            for (int dd = 0; dd < 3; ++dd)
+                gr[4 + e][dd] = 4.0 * (l[i] * g[j][dd] + l[j] * g[i][dd]);
+        }
+        for (int i = 0; i < 10; ++i)
+            for (int j = 0; j < 10; ++j)
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        k[(3 * i + a) * 30 + 3 * j + b] += w * elastic_term(gr[i], gr[j], a, b, d);
+    }
+}
+
+// The 4-node tetrahedron: constant gradients, 1 point of weight V, same layout as tet10.rs:113.
+void tet4_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k[144]) {
+    std::fill(k, k + 144, 0.0);
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b)
+                    k[(3 * i + a) * 12 + 3 * j + b] += volume * elastic_term(g[i].data(), g[j].data(), a, b, d);
+}
+
+// tet10.rs:244-272: edge points numbered in the order of first sight over (tetrahedron,
+// EDGES order), keyed by the sorted corner pair.
+Quadratic quadratic(const vector<Vec3>& points, const vector<array<uint32_t, 4>>& tets) {
+    Quadratic q;
+    q.corners = points.size();
+    std::unordered_map<uint64_t, uint32_t> of;
+    of.reserve(tets.size() * 2);
+    q.tets.reserve(tets.size());
+    for (const auto& tet : tets) {
+        array<uint32_t, 10> t{};
+        for (int c = 0; c < 4; ++c) t[c] = tet[c];
+        for (int k = 0; k < 6; ++k) {
+            uint32_t a = std::min(tet[EDGES[k][0]], tet[EDGES[k][1]]);
+            uint32_t b = std::max(tet[EDGES[k][0]], tet[EDGES[k][1]]);
+            uint64_t key = ((uint64_t)a << 32) | b;
+            auto it = of.find(key);
+            if (it == of.end()) {
+                q.edges.push_back({a, b});
+                uint32_t id = (uint32_t)(q.corners + q.edges.size() - 1);
+                of.emplace(key, id);
+                t[4 + k] = id;
+            } else {
+                t[4 + k] = it->second;
+            }
+        }
+        q.tets.push_back(t);
+    }
+    q.points = points;
+    for (const auto& e : q.edges) {
+        const Vec3 &p = points[e[0]], &r = points[e[1]];
+        q.points.push_back({0.5 * (p[0] + r[0]), 0.5 * (p[1] + r[1]), 0.5 * (p[2] + r[2])});
+    }
+    return q;
+}
+
+// The priority of an element in the colouring: the "lowbias32" integer hash of C. Wellons
+// (2018), a bijection of 32-bit words.
+uint32_t colour_priority(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+// Jones-Plassmann colouring: M. T. Jones and P. E. Plassmann, A parallel graph coloring
+// heuristic, SIAM J. Sci. Comput. 14 (1993) 654-669. In each round an uncoloured element whose
+// (priority, index) is above that of each uncoloured element it shares a node with takes the
+// smallest colour that no coloured element it shares a node with has. Elements that share a
+// node get different colours, so the scatter of 1 colour has no write conflicts.
+vector<uint32_t> colour_elements(size_t n, const uint32_t* elements, size_t nel, int m,
+                                 int* ncolours) {
+    const uint32_t UNSET = UINT32_MAX;
+    vector<size_t> count(n + 1, 0);
+    for (size_t e = 0; e < nel; ++e)
+        for (int a = 0; a < m; ++a) count[elements[e * m + a] + 1] += 1;
+    for (size_t i = 0; i < n; ++i) count[i + 1] += count[i];
+    vector<uint32_t> of_node(count[n]);
+    vector<size_t> next(count);
+    for (size_t k = 0; k < nel; ++k)
+        for (int a = 0; a < m; ++a) of_node[next[elements[k * m + a]]++] = (uint32_t)k;
+    vector<uint32_t> colour(nel, UNSET);
+    vector<char> selected(nel, 0);
+    size_t left = nel;
+    int most = 0;
+    while (left > 0) {
+        for (size_t e = 0; e < nel; ++e) {
+            selected[e] = 0;
+            if (colour[e] != UNSET) continue;
+            uint64_t me = ((uint64_t)colour_priority((uint32_t)e) << 32) | (uint32_t)e;
+            bool top = true;
+            for (int a = 0; a < m && top; ++a) {
+                uint32_t v = elements[e * m + a];
+                for (size_t t = count[v]; t < count[v + 1]; ++t) {
+                    uint32_t f = of_node[t];
+                    if (f == e || colour[f] != UNSET) continue;
+                    uint64_t other = ((uint64_t)colour_priority(f) << 32) | f;
+                    if (other > me) {
+                        top = false;
+                        break;
+                    }
+                }
+            }
+            selected[e] = top;
+        }
+        for (size_t e = 0; e < nel; ++e) {
+            if (!selected[e]) continue;
+            uint64_t used[4] = {0, 0, 0, 0};
+            for (int a = 0; a < m; ++a) {
+                uint32_t v = elements[e * m + a];
+                for (size_t t = count[v]; t < count[v + 1]; ++t) {
+                    uint32_t c = colour[of_node[t]];
+                    if (c != UNSET && c < 256) used[c >> 6] |= 1ull << (c & 63);
+                }
+            }
+            uint32_t c = 0;
+            while (c < 256 && (used[c >> 6] >> (c & 63) & 1)) ++c;
+            if (c >= 256) throw Error("the elements need more than 256 colours");
+            colour[e] = c;
+            most = std::max(most, (int)c + 1);
+            --left;
+        }
+    }
+    *ncolours = most;
+    return colour;
+}
+
+}  // namespace orc

@@ -1,0 +1,233 @@
+// CPU oracle: a C++17 restatement of the fh-fem iterative solve path of femahoy (crates/fem).
+//
+// TEST INFRASTRUCTURE ONLY. This library is the checker of the CUDA path: only the tests, the
+// smoke check and the CPU-baseline leg of the benchmark load it. The product (libfemgpu.so)
+// never links, calls or falls back to it.
+//
+// Every function cites the reference file:line it restates (paths inside the femahoy project).
+// Floating-point expressions keep the reference's evaluation order, and the build uses
+// -ffp-contract=off, so that element matrices and assembled values are bit-identical with
+// the Rust code (which never fuses a multiply and an add).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#include <array>
+
+namespace orc {
+
+using std::size_t;
+using std::vector;
+using std::array;
+
+constexpr size_t NONE = SIZE_MAX;  // symbolic.rs:14
+
+// A failure with the reference's error text (the Rust `Err(String)`).
+struct Error : std::runtime_error {
+    explicit Error(const std::string& s) : std::runtime_error(s) {}
+};
+
+// ---------------------------------------------------------------- sparse.rs
+// sparse.rs:12-17: square CSR with both triangles, sorted columns per row.
+struct Csr {
+    size_t n = 0;
+    vector<size_t> ptr;
+    vector<uint32_t> idx;
+    vector<double> val;
+    // sparse.rs:68-71
+    bool find(size_t i, size_t j, size_t* at) const;
+    // sparse.rs:75-86
+    void add_element(const uint32_t* nodes, int m, const double* ke);
+    // sparse.rs:89-93
+    vector<double> diagonal() const;
+    // sparse.rs:96-105
+    void mul(const double* x, double* y) const;
+    // sparse.rs:108-135
+    Csr submatrix(const vector<size_t>& keep) const;
+};
+// sparse.rs:22-65: elements are `nel` runs of `m` nodes.
+Csr pattern(size_t n, const uint32_t* elements, size_t nel, int m);
+
+// sparse.rs:202-208
+struct Rect {
+    size_t rows = 0, cols = 0;
+    vector<size_t> ptr;
+    vector<uint32_t> idx;
+    vector<double> val;
+    void mul(const double* x, double* y) const;            // sparse.rs:212-220
+    void mul_transpose(const double* x, double* y) const;  // sparse.rs:223-230
+    Csr galerkin(const Csr& a) const;                       // sparse.rs:233-292
+};
+
+// ---------------------------------------------------------------- elements
+using Vec3 = array<double, 3>;
+// heat.rs:983-1002
+void tet_gradients(const Vec3 p[4], Vec3 g[4], double* volume);
+// heat.rs:972-981
+void tet_conduction(const Vec3 g[4], double v, const Vec3& k, double ke[16]);
+// heat.rs:1219-1244 (steady form: no transient term)
+vector<double> reduced_rhs(const Csr& a, const double* load, const double* t,
+                           const vector<size_t>& free);
+
+// hex.rs:120-124
+struct Stiffness {
+    double normal[3][3];
+    double shear[3];  // G_yz, G_xz, G_xy
+};
+// hex.rs:58-64 then hex.rs:69-114
+Stiffness isotropic_stiffness(double e, double nu);
+Stiffness orthotropic_stiffness(const double e[3], const double nu[3], const double g[3]);
+
+// tet10.rs:90-120: 30 x 30 row-major, unknown 3 node + component.
+void tet10_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k[900]);
+// The linear (4-node) elasticity tetrahedron, which the reference lacks: V B^T D B with the
+// constant gradients of tet_gradients, in the index layout and term order of tet10.rs:99-113.
+void tet4_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k[144]);
+
+// tet10.rs:232-272
+struct Quadratic {
+    vector<Vec3> points;
+    size_t corners = 0;
+    vector<array<uint32_t, 2>> edges;
+    vector<array<uint32_t, 10>> tets;
+};
+Quadratic quadratic(const vector<Vec3>& points, const vector<array<uint32_t, 4>>& tets);
+
+// Element colouring (not in the reference, whose assembly is sequential; sparse.rs:75):
+// Jones-Plassmann with a fixed integer hash as the priority and first-fit colours. The CUDA
+// colouring runs the same rounds, so both give the same colour for each element.
+uint32_t colour_priority(uint32_t e);
+vector<uint32_t> colour_elements(size_t n, const uint32_t* elements, size_t nel, int m,
+                                 int* ncolours);
+
+// ---------------------------------------------------------------- order / symbolic / cholesky
+// order.rs:19-179
+vector<size_t> nested_dissection(const Csr& a, const vector<Vec3>& xyz);
+
+// symbolic.rs:19-192
+struct Symbolic {
+    size_t n = 0;
+    vector<size_t> perm, iperm, start, rows_ptr;
+    vector<uint32_t> rows;
+    vector<size_t> parent, children;
+    size_t supernodes() const { return start.size() - 1; }
+    uint64_t entries() const;  // symbolic.rs:162-170
+    double flops() const;      // symbolic.rs:174-182
+};
+Symbolic analyse(const Csr& a, const vector<size_t>& order);
+
+// cholesky.rs:23-167
+struct Cholesky {
+    Symbolic sym;
+    vector<size_t> offset;
+    vector<double> values;
+    void solve(double* b) const;  // cholesky.rs:125-160
+};
+Cholesky factor(const Symbolic& sym, const Csr& a);  // cholesky.rs:44-122
+
+// ---------------------------------------------------------------- multigrid.rs
+// multigrid.rs:55-59
+struct Level {
+    array<vector<double>, 3> planes;
+    vector<array<uint32_t, 3>> points;
+    vector<uint8_t> comp;
+};
+
+// multigrid.rs:187-324
+struct Lines {
+    vector<uint32_t> order;
+    vector<size_t> start;
+    vector<uint32_t> line, place;
+    size_t band = 0;
+    vector<double> factor;
+    static Lines make(const Level& level, int axis, const Csr& a);
+    void sweep(const Csr& a, const double* b, double* x, bool forward) const;
+};
+
+// multigrid.rs:329-452
+bool coarsen(const Level& fine, const Csr& a, Rect* p, Level* coarse);
+
+// multigrid.rs:73-180 (the Galerkin form: `cells = None`)
+struct Multigrid {
+    vector<Csr> a;
+    vector<Rect> p;
+    vector<array<Lines, 3>> lines;
+    Cholesky coarse;
+    static Multigrid make(const Csr& a, Level level);
+    size_t levels() const { return a.size(); }
+    void apply(const double* r, double* z) const;
+    void cycle(size_t l, const double* b, double* x) const;
+};
+
+// multigrid.rs:683-753
+struct Convergence {
+    size_t iterations;
+    double residual;
+};
+Convergence pcg(const Csr& a, const double* b, double* x,
+                const std::function<void(const double*, double*)>& precondition, double tol,
+                size_t max_iter, const std::function<bool()>& cancelled);
+
+// ---------------------------------------------------------------- pmultigrid.rs
+struct PMultigrid {
+    Rect p;
+    vector<double> diag;
+    Cholesky coarse;
+    size_t coarse_unknowns = 0;
+    static PMultigrid make(const Csr& a, Rect p, const vector<Vec3>& coarse);  // :46-60
+    void apply(const Csr& a, const double* r, double* z) const;               // :63-98
+};
+// pmultigrid.rs:104-151
+void prolongation(const vector<Vec3>& points, size_t corners,
+                  const vector<array<uint32_t, 2>>& edges, const vector<size_t>& free, Rect* p,
+                  vector<Vec3>* xyz);
+
+// ---------------------------------------------------------------- solve.rs
+constexpr size_t STEADY_DIRECT_LIMIT = 3000;    // solve.rs:18
+constexpr size_t TRANSIENT_DIRECT_LIMIT = 40000;  // solve.rs:24
+constexpr double PCG_TOL = 1e-10;               // solve.rs:42
+constexpr size_t PCG_MAX_ITER = 500;            // solve.rs:43
+
+enum class Method { Direct = 0, Multigrid = 1 };  // solve.rs:47-50
+
+// solve.rs:28-39
+struct Crossover {
+    bool flops_rule = false;
+    size_t unknowns = STEADY_DIRECT_LIMIT;
+    double flops = 0.0;
+    uint64_t entries = 0;
+    bool flat = false;
+};
+
+// solve.rs:64-77
+struct Unknowns {
+    enum Kind { Grid = 0, Points = 1, Quadratic = 2 } kind = Grid;
+    Level level;             // Grid
+    vector<Vec3> points;     // Points, Quadratic
+    Rect p;                  // Quadratic
+    vector<Vec3> coarse;     // Quadratic
+};
+
+struct Stats {
+    size_t iterations;
+    double residual;
+};
+
+// solve.rs:58-250
+struct Solver {
+    enum Inner { Direct, MG, PMG } inner = Direct;
+    Csr a;
+    Cholesky chol;
+    Multigrid mg;
+    PMultigrid pmg;
+    size_t max_iter = PCG_MAX_ITER;
+    double tol = PCG_TOL;
+    static Solver make(Csr a, Unknowns unknowns, int method /* -1 none */, Crossover crossover);
+    Method method() const { return inner == Direct ? Method::Direct : Method::Multigrid; }
+    Stats solve(const double* b, double* x, const std::function<bool()>& cancelled) const;
+};
+
+}  // namespace orc
