@@ -1,0 +1,146 @@
+"""ctypes binding of libfemgpu.so (include/femgpu.h). Loading fails loudly when the library is
+missing: there is no CPU path behind this package."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfemgpu.so")
+
+# Status codes (femgpu.h).
+OK, CANCELLED, NOT_CONVERGED, NOT_SPD, NEEDS_GRID, INVALID, CUDA, TOO_LARGE, PATTERN, MATERIAL, \
+    TIMEOUT = range(11)
+
+P1_HEAT, P1_ELASTIC, P2_ELASTIC = 0, 1, 2
+GATHER, COLOUR = 0, 1
+FP64, MIXED = 0, 1
+
+
+class FemError(RuntimeError):
+    """A failure of the library: ``code`` is the femgpu.h status and ``str(e)`` the message (the
+    reference's text where it has one, e.g. "cancelled")."""
+
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+class Unknowns_t(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int),
+        ("planes", C.c_void_p * 3),
+        ("nplanes", C.c_size_t * 3),
+        ("points", C.c_void_p),
+        ("comp", C.c_void_p),
+        ("xyz", C.c_void_p),
+        ("p_cols", C.c_size_t),
+        ("p_ptr", C.c_void_p),
+        ("p_idx", C.c_void_p),
+        ("p_val", C.c_void_p),
+        ("coarse_xyz", C.c_void_p),
+        ("coarse_comp", C.c_void_p),
+    ]
+
+
+class Crossover_t(C.Structure):
+    _fields_ = [("rule", C.c_int), ("unknowns", C.c_size_t), ("flops", C.c_double),
+                ("entries", C.c_uint64), ("flat", C.c_int)]
+
+
+class Options_t(C.Structure):
+    _fields_ = [("precision", C.c_int), ("degree", C.c_int), ("lower", C.c_double),
+                ("sell_c", C.c_int), ("sell_sigma", C.c_int), ("coarsest", C.c_int),
+                ("max_levels", C.c_int), ("graph", C.c_int)]
+
+
+class Stats_t(C.Structure):
+    _fields_ = [("iterations", C.c_size_t), ("residual", C.c_double),
+                ("true_residual", C.c_double), ("seconds", C.c_double),
+                ("launches", C.c_size_t)]
+
+
+_lib = None
+
+# Every symbol of include/femgpu.h with its signature.
+SIGNATURES = {
+    "femgpu_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "femgpu_version": (C.c_char_p, []),
+    "femgpu_assemble": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_size_t,
+                                  C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "femgpu_assemble_device": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_size_t,
+                                         C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "femgpu_pattern": (C.c_int, [C.c_size_t, C.c_size_t, C.c_int, C.c_void_p,
+                                 C.POINTER(C.c_void_p)]),
+    "femgpu_colour": (C.c_int, [C.c_size_t, C.c_size_t, C.c_int, C.c_void_p, C.c_void_p,
+                                C.POINTER(C.c_int)]),
+    "femgpu_quadratic": (C.c_int, [C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_size_t)]),
+    "femgpu_csr_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "femgpu_csr_download": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_csr_upload": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.POINTER(C.c_void_p)]),
+    "femgpu_csr_submatrix": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t,
+                                       C.POINTER(C.c_void_p)]),
+    "femgpu_csr_mul": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_reduced_rhs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_size_t, C.c_void_p]),
+    "femgpu_csr_free": (None, [C.c_void_p]),
+    "femgpu_prolongation": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_size_t,
+                                      C.c_void_p, C.c_size_t, C.c_void_p,
+                                      C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_solver_new": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.c_int,
+                                    C.POINTER(Crossover_t), C.POINTER(Options_t),
+                                    C.POINTER(C.c_void_p)]),
+    "femgpu_solver_set_max_iter": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "femgpu_solver_set_tol": (C.c_int, [C.c_void_p, C.c_double]),
+    "femgpu_solver_method": (C.c_int, [C.c_void_p]),
+    "femgpu_solver_levels": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "femgpu_solver_bytes": (C.c_size_t, [C.c_void_p]),
+    "femgpu_solver_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.POINTER(Stats_t)]),
+    "femgpu_solver_solve_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.POINTER(Stats_t)]),
+    "femgpu_solver_precondition_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_solver_free": (None, [C.c_void_p]),
+    "femgpu_solver_stream": (C.c_void_p, [C.c_void_p]),
+    "femgpu_solver_kernel_time": (C.c_int, [C.c_void_p, C.c_int, C.c_int,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+}
+
+
+def lib():
+    """The loaded library; raises when libfemgpu.so is missing (build it with
+    ``python -m femahoy_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m femahoy_b200.build")
+        handle = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(handle, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status):
+    if status != OK:
+        buf = C.create_string_buffer(1024)
+        lib().femgpu_last_error(buf, 1024)
+        raise FemError(status, buf.value.decode())
+
+
+def ptr(a):
+    """The data pointer of a contiguous numpy array (None for None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)

@@ -1,0 +1,39 @@
+// Device assembly: the interfaces of assemble.cu.
+#pragma once
+#include "common.cuh"
+
+namespace femgpu {
+
+// The elements of each node, in increasing element order: of_node[start[v] .. start[v + 1]].
+struct Incidence {
+    int64_t n = 0, nel = 0;
+    int m = 0;
+    DevBuf<int64_t> start;
+    DevBuf<uint32_t> of_node;
+};
+
+// The result of an assembly: the matrix, the pattern of the nodes (elasticity) and the
+// incidence it was built from.
+struct Assembled {
+    DevCsr matrix;
+    DevCsr node;
+    Incidence inc;
+    int ncolours = 0;
+};
+
+void build_incidence(const uint32_t* d_el, int64_t nel, int m, int64_t n, Incidence* inc,
+                     cudaStream_t s);
+void build_pattern(const uint32_t* d_el, const Incidence& inc, DevCsr* out, cudaStream_t s);
+int colour_elements(const uint32_t* d_el, const Incidence& inc, DevBuf<uint32_t>* colour,
+                    cudaStream_t s);
+void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t nel,
+              const uint32_t* d_el, const double* d_coef, Assembled* out, cudaStream_t s);
+int64_t quadratic(int64_t ncorner, int64_t ntet, const uint32_t* d_tets, uint32_t* d_tets10,
+                  uint32_t* d_edges, cudaStream_t s);
+void submatrix(const DevCsr& a, const int64_t* d_keep, int64_t nkeep, DevCsr* out,
+               cudaStream_t s);
+void reduced_rhs(const DevCsr& a, const double* d_load, const double* d_t, const int64_t* d_free,
+                 int64_t nfree, double* d_out, cudaStream_t s);
+void csr_mul(const DevCsr& a, const double* d_x, double* d_y, cudaStream_t s);
+
+}  // namespace femgpu

@@ -1,0 +1,396 @@
+// The C ABI of femgpu.h: argument checks, host <-> device copies and the translation of
+// failures into status codes with the reference's messages.
+#include <cstring>
+#include <string>
+
+#include "assemble.cuh"
+#include "common.cuh"
+#include "hierarchy.hpp"
+#include "solver.cuh"
+
+struct femgpu_csr {
+    femgpu::DevCsr m;
+};
+
+struct femgpu_solver {
+    femgpu::SolverImpl impl;
+};
+
+namespace femgpu {
+
+static thread_local std::string g_last_error;
+
+void set_last_error(const std::string& s) { g_last_error = s; }
+
+template <class F>
+static int guarded(F f) {
+    try {
+        f();
+        return FEMGPU_OK;
+    } catch (const Failure& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        set_last_error("out of host memory");
+        return FEMGPU_ERR_TOO_LARGE;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return FEMGPU_ERR_INVALID;
+    }
+}
+
+// A stream for calls that have no handle (assembly, utilities).
+static cudaStream_t util_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    if (!s) FG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+
+static void require(bool ok, const char* what) {
+    if (!ok) throw Failure(FEMGPU_ERR_INVALID, what);
+}
+
+}  // namespace femgpu
+
+using namespace femgpu;
+
+extern "C" {
+
+size_t femgpu_last_error(char* buf, size_t len) {
+    const std::string& e = g_last_error;
+    if (buf && len) {
+        size_t k = std::min(len - 1, e.size());
+        std::memcpy(buf, e.data(), k);
+        buf[k] = 0;
+    }
+    return e.size();
+}
+
+const char* femgpu_version(void) { return "femgpu 0.1 (sm_100a)"; }
+
+static int assemble_impl(int kind, int mode, size_t npoints, const double* xyz, size_t nel,
+                         const uint32_t* nodes, const double* coef, femgpu_csr** out,
+                         bool device) {
+    return guarded([&] {
+        require(out != nullptr, "out is null");
+        require(npoints > 0 && nel > 0, "an empty mesh");
+        require(xyz && nodes && coef, "a null mesh array");
+        cudaStream_t s = util_stream();
+        int nn = kind == FEMGPU_P2_ELASTIC ? 10 : 4;
+        int nc = kind == FEMGPU_P1_HEAT ? 3 : 2;
+        DevBuf<double> dx, dc;
+        DevBuf<uint32_t> de;
+        const double* px = xyz;
+        const double* pc = coef;
+        const uint32_t* pe = nodes;
+        if (!device) {
+            dx.upload(xyz, 3 * npoints, s);
+            de.upload(nodes, nn * nel, s);
+            dc.upload(coef, nc * nel, s);
+            px = dx.p;
+            pc = dc.p;
+            pe = de.p;
+        }
+        Assembled a;
+        assemble(kind, mode, (int64_t)npoints, px, (int64_t)nel, pe, pc, &a, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        auto* h = new femgpu_csr;
+        h->m = std::move(a.matrix);
+        *out = h;
+    });
+}
+
+int femgpu_assemble(int kind, int mode, size_t npoints, const double* xyz, size_t nel,
+                    const uint32_t* nodes, const double* coef, femgpu_csr** out) {
+    return assemble_impl(kind, mode, npoints, xyz, nel, nodes, coef, out, false);
+}
+
+int femgpu_assemble_device(int kind, int mode, size_t npoints, const double* xyz, size_t nel,
+                           const uint32_t* nodes, const double* coef, femgpu_csr** out) {
+    return assemble_impl(kind, mode, npoints, xyz, nel, nodes, coef, out, true);
+}
+
+int femgpu_pattern(size_t n, size_t nel, int m, const uint32_t* elements, femgpu_csr** out) {
+    return guarded([&] {
+        require(out && elements && m > 0 && n > 0, "invalid pattern arguments");
+        cudaStream_t s = util_stream();
+        DevBuf<uint32_t> de;
+        de.upload(elements, (size_t)m * nel, s);
+        Incidence inc;
+        build_incidence(de.p, (int64_t)nel, m, (int64_t)n, &inc, s);
+        auto* h = new femgpu_csr;
+        build_pattern(de.p, inc, &h->m, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        *out = h;
+    });
+}
+
+int femgpu_colour(size_t n, size_t nel, int m, const uint32_t* elements, uint32_t* colour,
+                  int* ncolours) {
+    return guarded([&] {
+        require(elements && colour && ncolours && m > 0, "invalid colouring arguments");
+        cudaStream_t s = util_stream();
+        DevBuf<uint32_t> de;
+        de.upload(elements, (size_t)m * nel, s);
+        Incidence inc;
+        build_incidence(de.p, (int64_t)nel, m, (int64_t)n, &inc, s);
+        DevBuf<uint32_t> c;
+        *ncolours = colour_elements(de.p, inc, &c, s);
+        c.download(colour, nel, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int femgpu_quadratic(size_t ncorner, size_t ntet, const uint32_t* tets, uint32_t* tets10,
+                     uint32_t* edges, size_t* nedges) {
+    return guarded([&] {
+        require(tets && tets10 && edges && nedges, "a null array");
+        cudaStream_t s = util_stream();
+        DevBuf<uint32_t> dt, d10(10 * ntet), de(12 * ntet);
+        dt.upload(tets, 4 * ntet, s);
+        int64_t ne = quadratic((int64_t)ncorner, (int64_t)ntet, dt.p, d10.p, de.p, s);
+        d10.download(tets10, 10 * ntet, s);
+        de.download(edges, 2 * ne, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        *nedges = (size_t)ne;
+    });
+}
+
+int femgpu_csr_info(const femgpu_csr* a, size_t* n, size_t* nnz) {
+    return guarded([&] {
+        require(a != nullptr, "null matrix");
+        if (n) *n = (size_t)a->m.n;
+        if (nnz) *nnz = (size_t)a->m.nnz;
+    });
+}
+
+int femgpu_csr_download(const femgpu_csr* a, int64_t* ptr, uint32_t* idx, double* val) {
+    return guarded([&] {
+        require(a != nullptr, "null matrix");
+        cudaStream_t s = util_stream();
+        if (ptr) a->m.ptr.download(ptr, a->m.n + 1, s);
+        if (idx) a->m.idx.download(idx, a->m.nnz, s);
+        if (val) a->m.val.download(val, a->m.nnz, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int femgpu_csr_upload(size_t n, const int64_t* ptr, const uint32_t* idx, const double* val,
+                      femgpu_csr** out) {
+    return guarded([&] {
+        require(out && ptr && (ptr[n] == 0 || (idx && val)), "null CSR arrays");
+        require(ptr[0] == 0, "ptr[0] must be 0");
+        for (size_t i = 0; i < n; ++i) require(ptr[i + 1] >= ptr[i], "ptr must not decrease");
+        cudaStream_t s = util_stream();
+        auto* h = new femgpu_csr;
+        h->m.n = (int64_t)n;
+        h->m.nnz = ptr[n];
+        h->m.ptr.upload(ptr, n + 1, s);
+        h->m.idx.upload(idx, (size_t)ptr[n], s);
+        h->m.val.upload(val, (size_t)ptr[n], s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        *out = h;
+    });
+}
+
+int femgpu_csr_submatrix(const femgpu_csr* a, const int64_t* keep, size_t nkeep,
+                         femgpu_csr** out) {
+    return guarded([&] {
+        require(a && keep && out, "null argument");
+        cudaStream_t s = util_stream();
+        DevBuf<int64_t> dk;
+        dk.upload(keep, nkeep, s);
+        auto* h = new femgpu_csr;
+        try {
+            submatrix(a->m, dk.p, (int64_t)nkeep, &h->m, s);
+            FG_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int femgpu_csr_mul(const femgpu_csr* a, const double* x, double* y) {
+    return guarded([&] {
+        require(a && x && y, "null argument");
+        cudaStream_t s = util_stream();
+        DevBuf<double> dx, dy(a->m.n);
+        dx.upload(x, a->m.n, s);
+        csr_mul(a->m, dx.p, dy.p, s);
+        dy.download(y, a->m.n, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int femgpu_reduced_rhs(const femgpu_csr* a, const double* load, const double* t,
+                       const int64_t* free, size_t nfree, double* out) {
+    return guarded([&] {
+        require(a && load && t && free && out, "null argument");
+        cudaStream_t s = util_stream();
+        DevBuf<double> dl, dt, dout(nfree);
+        DevBuf<int64_t> df;
+        dl.upload(load, a->m.n, s);
+        dt.upload(t, a->m.n, s);
+        df.upload(free, nfree, s);
+        reduced_rhs(a->m, dl.p, dt.p, df.p, (int64_t)nfree, dout.p, s);
+        dout.download(out, nfree, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+void femgpu_csr_free(femgpu_csr* a) { delete a; }
+
+int femgpu_prolongation(size_t npoints, const double* points, size_t corners, size_t nedges,
+                        const uint32_t* edges, size_t nfree, const int64_t* free, size_t* nnz,
+                        size_t* ncoarse, int64_t* p_ptr, uint32_t* p_idx, double* p_val,
+                        double* coarse_xyz) {
+    return guarded([&] {
+        require(points && edges && free, "null argument");
+        for (size_t k = 0; k < nfree; ++k) {
+            require(free[k] >= 0 && (size_t)free[k] < 3 * npoints, "a free unknown out of range");
+            require(k == 0 || free[k] > free[k - 1], "the free unknowns must increase");
+            if ((size_t)(free[k] / 3) >= corners)
+                require((size_t)(free[k] / 3) - corners < nedges, "an edge point out of range");
+        }
+        HostRect p;
+        std::vector<double> xyz;
+        prolongation(points, (int64_t)npoints, (int64_t)corners, edges, (int64_t)nedges, free,
+                     (int64_t)nfree, &p, &xyz);
+        if (nnz) *nnz = p.idx.size();
+        if (ncoarse) *ncoarse = (size_t)p.cols;
+        if (p_ptr) std::memcpy(p_ptr, p.ptr.data(), p.ptr.size() * 8);
+        if (p_idx) std::memcpy(p_idx, p.idx.data(), p.idx.size() * 4);
+        if (p_val) std::memcpy(p_val, p.val.data(), p.val.size() * 8);
+        if (coarse_xyz) std::memcpy(coarse_xyz, xyz.data(), xyz.size() * 8);
+    });
+}
+
+int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
+                      const femgpu_crossover* crossover, const femgpu_options* options,
+                      femgpu_solver** out) {
+    return guarded([&] {
+        require(a && u && out, "null argument");
+        require(method >= -1 && method <= 1, "unknown method");
+        femgpu_crossover c{0, 3000, 0.0, 0, 0};  // Crossover::Unknowns(STEADY_DIRECT_LIMIT)
+        if (crossover) c = *crossover;
+        Options o;
+        if (options) {
+            o.precision = options->precision;
+            o.degree = options->degree;
+            o.lower = options->lower;
+            o.sell_c = options->sell_c;
+            o.coarsest = options->coarsest > 0 ? options->coarsest : 3000;
+            o.max_levels = options->max_levels > 0 ? options->max_levels : 30;
+            o.graph = options->graph != 2;
+        }
+        require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
+        require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,
+                "the SELL chunk height must be 8, 16 or 32");
+        require(o.degree >= 0 && o.degree <= 16, "the Chebyshev degree must be 1 to 16");
+        int64_t n = a->m.n;
+        if (u->kind == FEMGPU_UNKNOWNS_GRID) {
+            require(u->points && u->comp, "a grid level needs its points and components");
+            for (int d = 0; d < 3; ++d) require(u->planes[d] && u->nplanes[d] > 0, "empty planes");
+            for (int64_t k = 0; k < n; ++k)
+                for (int d = 0; d < 3; ++d)
+                    require(u->points[3 * k + d] < u->nplanes[d], "a grid point past its planes");
+        } else if (u->kind == FEMGPU_UNKNOWNS_POINTS) {
+            require(u->xyz != nullptr, "points need coordinates");
+        } else if (u->kind == FEMGPU_UNKNOWNS_QUADRATIC) {
+            require(u->p_ptr && u->p_idx && u->p_val && u->coarse_xyz, "quadratic needs P");
+            require(u->p_ptr[0] == 0, "P ptr[0] must be 0");
+            for (int64_t k = 0; k < u->p_ptr[n]; ++k)
+                require(u->p_idx[k] < u->p_cols, "a column of P past its columns");
+        } else {
+            throw Failure(FEMGPU_ERR_INVALID, "unknown unknowns kind");
+        }
+        auto* s = new femgpu_solver;
+        try {
+            s->impl.create(a->m, *u, method, c, o);
+        } catch (...) {
+            delete s;
+            throw;
+        }
+        *out = s;
+    });
+}
+
+int femgpu_solver_set_max_iter(femgpu_solver* s, size_t max_iter) {
+    return guarded([&] {
+        require(s != nullptr, "null solver");
+        s->impl.max_iter = max_iter;
+    });
+}
+
+int femgpu_solver_set_tol(femgpu_solver* s, double tol) {
+    return guarded([&] {
+        require(s != nullptr && tol >= 0.0, "a tolerance must be 0 or more");
+        s->impl.tol = tol;
+    });
+}
+
+int femgpu_solver_method(const femgpu_solver* s) { return s ? s->impl.method() : -1; }
+
+int femgpu_solver_levels(const femgpu_solver* s, size_t* sizes, int cap) {
+    if (!s) return 0;
+    auto v = s->impl.level_sizes();
+    for (int i = 0; i < (int)v.size() && i < cap; ++i)
+        if (sizes) sizes[i] = (size_t)v[i];
+    return (int)v.size();
+}
+
+size_t femgpu_solver_bytes(const femgpu_solver* s) { return s ? s->impl.bytes() : 0; }
+
+int femgpu_solver_solve(femgpu_solver* s, const double* b, double* x, const volatile int* cancel,
+                        femgpu_stats* stats) {
+    return guarded([&] {
+        require(s && b && x, "null argument");
+        size_t n = s->impl.level_sizes().empty() ? 0 : (size_t)s->impl.level_sizes()[0];
+        cudaStream_t st = s->impl.stream();
+        DevBuf<double> db, dx;
+        db.upload(b, n, st);
+        dx.upload(x, n, st);
+        try {
+            s->impl.solve(db.p, dx.p, cancel, stats);
+        } catch (const Failure&) {
+            dx.download(x, n, st);
+            cudaStreamSynchronize(st);
+            throw;
+        }
+        dx.download(x, n, st);
+        FG_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+int femgpu_solver_solve_device(femgpu_solver* s, const double* b, double* x,
+                               const volatile int* cancel, femgpu_stats* stats) {
+    return guarded([&] {
+        require(s && b && x, "null argument");
+        s->impl.solve(b, x, cancel, stats);
+    });
+}
+
+int femgpu_solver_precondition_device(femgpu_solver* s, const double* r, double* z) {
+    return guarded([&] {
+        require(s && r && z, "null argument");
+        s->impl.precondition(r, z);
+    });
+}
+
+void femgpu_solver_free(femgpu_solver* s) { delete s; }
+
+void* femgpu_solver_stream(const femgpu_solver* s) {
+    return s ? (void*)s->impl.stream() : nullptr;
+}
+
+int femgpu_solver_kernel_time(femgpu_solver* s, int which, int reps, double* ms, double* bytes) {
+    return guarded([&] {
+        require(s && ms && bytes, "null argument");
+        require(which == 0 || which == 1, "which is 0 (smoother step) or 1 (FP64 operator)");
+        s->impl.kernel_time(which, reps, ms, bytes);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,1161 @@
+// The device solver (see solver.cuh).
+//
+// Per PCG iteration (multigrid.rs:721-751) the device runs: q = A p fused with p.q and
+// alpha; x += alpha p, r -= alpha q fused with r.r and the convergence test; the V-cycle;
+// r.z (and z.q) fused with beta; p = z + beta p. The scalars never leave the device; the host
+// reads 1 small struct per iteration to apply the reference's stopping rules. Each iteration
+// is 1 CUDA graph launch.
+//
+// The V-cycle (multigrid.rs:151-179 with the line Gauss-Seidel replaced by Chebyshev-Jacobi):
+// `degree` Chebyshev steps from x = 0 (the first needs no matrix product), the residual, the
+// restriction R = P^T (a gather), the coarser cycle, the prolongation and correction, and
+// `degree` Chebyshev steps. The pre- and post-smoother are the same polynomial in D^-1 A, so
+// the cycle is a symmetric positive definite preconditioner in exact arithmetic. The coarsest
+// level is solved by its inverse, formed on the device from a dense Cholesky factor.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "assemble.cuh"
+#include "solver.cuh"
+
+namespace femgpu {
+
+constexpr int TH = 256;
+constexpr int RED_BLOCKS = NUM_SMS * 4;
+constexpr double PIVOT = 1e-10;  // cholesky.rs:22
+
+// ------------------------------------------------------------------ SELL build
+__global__ void k_slice_entries(const int64_t* __restrict__ ptr, int64_t n, int C, int64_t ns,
+                                int64_t* __restrict__ entries) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < ns;
+         s += (int64_t)gridDim.x * blockDim.x) {
+        int64_t w = 0;
+        for (int r = 0; r < C; ++r) {
+            int64_t i = s * C + r;
+            if (i < n) w = max(w, ptr[i + 1] - ptr[i]);
+        }
+        entries[s] = ((w + 3) / 4) * 4 * C;
+    }
+}
+
+template <class T>
+__global__ void k_sell_fill(const int64_t* __restrict__ ptr, const uint32_t* __restrict__ idx,
+                            const double* __restrict__ val, int64_t n, int C, int64_t ns,
+                            const int64_t* __restrict__ sptr, uint32_t* __restrict__ col,
+                            T* __restrict__ sval) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ns * C;
+         g += (int64_t)gridDim.x * blockDim.x) {
+        int64_t s = g / C;
+        int r = (int)(g % C);
+        int64_t b = sptr[s], width = (sptr[s + 1] - b) / C;
+        int64_t len = g < n ? ptr[g + 1] - ptr[g] : 0;
+        int64_t at = g < n ? ptr[g] : 0;
+        uint32_t self = g < n ? (uint32_t)g : 0u;
+        for (int64_t k = 0; k < width; ++k) {
+            int64_t off = b + 4 * ((k / 4) * C + r) + (k % 4);
+            if (k < len) {
+                col[off] = idx[at + k];
+                sval[off] = (T)val[at + k];
+            } else {
+                col[off] = self;
+                sval[off] = (T)0;
+            }
+        }
+    }
+}
+
+template <class T>
+void make_sell(const DevCsr& a, int C, Sell<T>* out, cudaStream_t s) {
+    out->n = a.n;
+    out->C = C;
+    out->nslices = (a.n + C - 1) / C;
+    DevBuf<int64_t> ent(out->nslices);
+    k_slice_entries<<<blocks_for(out->nslices, TH), TH, 0, s>>>(a.ptr.p, a.n, C, out->nslices,
+                                                                  ent.p);
+    FG_CHECK_LAUNCH();
+    out->slice_ptr.alloc(out->nslices + 1);
+    exclusive_scan(ent.p, out->slice_ptr.p, out->nslices, s);
+    out->entries = fetch(out->slice_ptr.p + out->nslices, s);
+    out->col.alloc(out->entries);
+    out->val.alloc(out->entries);
+    k_sell_fill<T><<<blocks_for(out->nslices * C, TH), TH, 0, s>>>(
+        a.ptr.p, a.idx.p, a.val.p, a.n, C, out->nslices, out->slice_ptr.p, out->col.p,
+        out->val.p);
+    FG_CHECK_LAUNCH();
+}
+template void make_sell<double>(const DevCsr&, int, Sell<double>*, cudaStream_t);
+template void make_sell<float>(const DevCsr&, int, Sell<float>*, cudaStream_t);
+
+// ------------------------------------------------------------------ V-cycle kernels
+#define GRID_STRIDE(i, n)                                                     \
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); \
+         i += (int64_t)gridDim.x * blockDim.x)
+
+// The first Chebyshev step from x = 0: d = c1 D^-1 b, x = d.
+template <class T>
+__global__ void k_cheb_first(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv, T c1,
+                             T* __restrict__ d, T* __restrict__ x, const int* __restrict__ done) {
+    if (*done) return;
+    GRID_STRIDE(i, n) {
+        T v = c1 * dinv[i] * b[i];
+        d[i] = v;
+        x[i] = v;
+    }
+}
+
+// A Chebyshev step: r = b - A x_in, d = c2 d + c1 D^-1 r, x_out = x_in + d.
+template <class T>
+__global__ void __launch_bounds__(TH)
+    k_cheb_step(SellView<T> A, const T* __restrict__ b, const T* __restrict__ xin,
+                const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d, T* __restrict__ xout,
+                const int* __restrict__ done) {
+    if (*done) return;
+    GRID_STRIDE(g, A.nslices * A.C) {
+        T ax = sell_row<T, T, T>(A, g / A.C, (int)(g % A.C), xin);
+        if (g < A.n) {
+            T r = b[g] - ax;
+            T dd = c2 * d[g] + c1 * dinv[g] * r;
+            d[g] = dd;
+            xout[g] = xin[g] + dd;
+        }
+    }
+}
+
+// r = b - A x
+template <class T>
+__global__ void __launch_bounds__(TH)
+    k_residual(SellView<T> A, const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r,
+               const int* __restrict__ done) {
+    if (*done) return;
+    GRID_STRIDE(g, A.nslices * A.C) {
+        T ax = sell_row<T, T, T>(A, g / A.C, (int)(g % A.C), x);
+        if (g < A.n) r[g] = b[g] - ax;
+    }
+}
+
+// bc = P^T r as a gather over the rows of R = P^T (multigrid.rs:166, sparse.rs:223-230).
+template <class T>
+__global__ void k_restrict(int64_t nc, const int64_t* __restrict__ ptr,
+                           const uint32_t* __restrict__ idx, const T* __restrict__ val,
+                           const T* __restrict__ r, T* __restrict__ bc,
+                           const int* __restrict__ done) {
+    if (*done) return;
+    GRID_STRIDE(c, nc) {
+        T s = 0;
+        for (int64_t k = ptr[c]; k < ptr[c + 1]; ++k) s += val[k] * __ldg(r + idx[k]);
+        bc[c] = s;
+    }
+}
+
+// x += P e (multigrid.rs:169-172, sparse.rs:212-220)
+template <class T>
+__global__ void k_prolong(int64_t nf, const int64_t* __restrict__ ptr,
+                          const uint32_t* __restrict__ idx, const T* __restrict__ val,
+                          const T* __restrict__ e, T* __restrict__ x,
+                          const int* __restrict__ done) {
+    if (*done) return;
+    GRID_STRIDE(i, nf) {
+        T s = 0;
+        for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k) s += val[k] * __ldg(e + idx[k]);
+        x[i] += s;
+    }
+}
+
+// x = M b for the symmetric n x n matrix M (the coarsest inverse): 1 warp per row.
+template <class T>
+__global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__ b,
+                       T* __restrict__ x, const int* __restrict__ done) {
+    if (*done) return;
+    int lane = threadIdx.x & 31;
+    int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = w; i < n; i += nw) {
+        const T* row = M + i * n;
+        T s = 0;
+        for (int64_t k = lane; k < n; k += 32) s += row[k] * __ldg(b + k);
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) x[i] = s;
+    }
+}
+
+// x += t
+__global__ void k_add(int64_t n, const double* __restrict__ t, double* __restrict__ x) {
+    GRID_STRIDE(i, n) x[i] += t[i];
+}
+
+template <class S, class D>
+__global__ void k_convert(int64_t n, const S* __restrict__ a, D* __restrict__ b) {
+    GRID_STRIDE(i, n) b[i] = (D)a[i];
+}
+
+// ------------------------------------------------------------------ PCG kernels (FP64)
+struct FinResidual0 {
+    Scalars* sc;
+    __device__ void operator()(double bb, double rr) const {
+        sc->bb = bb;
+        sc->norm_b = sqrt(bb);
+        sc->rr = rr;
+    }
+};
+
+// r = b - A x, with b.b and r.r; also the FP32 copy of r (mixed form).
+__global__ void __launch_bounds__(TH)
+    k_pcg_residual(SellView<double> A, const double* __restrict__ b, const double* __restrict__ x,
+                   double* __restrict__ r, float* __restrict__ r32, double* partial,
+                   unsigned* counter, Scalars* sc) {
+    double bb = 0, rr = 0;
+    GRID_STRIDE(g, A.nslices * A.C) {
+        double ax = sell_row<double, double, double>(A, g / A.C, (int)(g % A.C), x);
+        if (g < A.n) {
+            double bi = b[g], ri = bi - ax;
+            r[g] = ri;
+            if (r32) r32[g] = (float)ri;
+            bb += bi * bi;
+            rr += ri * ri;
+        }
+    }
+    reduce2_finalize<TH>(bb, rr, partial, counter, FinResidual0{sc});
+}
+
+struct FinPq {
+    Scalars* sc;
+    __device__ void operator()(double pq, double) const {
+        sc->pq = pq;
+        sc->alpha = sc->rz / pq;
+    }
+};
+
+// q = A p with p.q and alpha = rz / p.q (multigrid.rs:740-741).
+__global__ void __launch_bounds__(TH)
+    k_pcg_spmv_pq(SellView<double> A, const double* __restrict__ p, double* __restrict__ q,
+                  double* partial, unsigned* counter, Scalars* sc) {
+    if (sc->done) return;
+    double pq = 0;
+    GRID_STRIDE(g, A.nslices * A.C) {
+        double ap = sell_row<double, double, double>(A, g / A.C, (int)(g % A.C), p);
+        if (g < A.n) {
+            q[g] = ap;
+            pq += p[g] * ap;
+        }
+    }
+    reduce2_finalize<TH>(pq, 0.0, partial, counter, FinPq{sc});
+}
+
+struct FinUpdate {
+    Scalars* sc;
+    double tol;
+    __device__ void operator()(double rr, double) const {
+        sc->rr = rr;
+        sc->iters += 1;
+        // multigrid.rs:722-723: |r| / |b| <= tol, on the updated residual.
+        if (sqrt(rr) / sc->norm_b <= tol) sc->done = 1;
+    }
+};
+
+// x += alpha p, r -= alpha q (multigrid.rs:742-745), with r.r and the stopping test.
+__global__ void __launch_bounds__(TH)
+    k_pcg_update(int64_t n, double* __restrict__ x, double* __restrict__ r,
+                 const double* __restrict__ p, const double* __restrict__ q,
+                 float* __restrict__ r32, double* partial, unsigned* counter, Scalars* sc,
+                 double tol) {
+    if (sc->done) return;
+    double alpha = sc->alpha, rr = 0;
+    GRID_STRIDE(i, n) {
+        x[i] += alpha * p[i];
+        double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        if (r32) r32[i] = (float)ri;
+        rr += ri * ri;
+    }
+    reduce2_finalize<TH>(rr, 0.0, partial, counter, FinUpdate{sc, tol});
+}
+
+struct FinDots {
+    Scalars* sc;
+    int flexible, init;
+    __device__ void operator()(double rz, double zq) const {
+        if (init) {
+            sc->beta = 0;
+        } else if (flexible) {
+            // Flexible CG (Y. Notay, Flexible conjugate gradients, SIAM J. Sci. Comput. 22 (2000)
+            // 1444-1460): beta = z_new.(r_new - r_old) / rz_old = -alpha z_new.q / rz_old.
+            sc->beta = -sc->alpha * zq / sc->rz;
+        } else {
+            sc->beta = rz / sc->rz;  // multigrid.rs:747-748
+        }
+        sc->rz = rz;
+        sc->zq = zq;
+    }
+};
+
+template <class TZ>
+__global__ void __launch_bounds__(TH)
+    k_pcg_dots(int64_t n, const double* __restrict__ r, const TZ* __restrict__ z,
+               const double* __restrict__ q, int flexible, int init, double* partial,
+               unsigned* counter, Scalars* sc) {
+    if (sc->done) return;
+    double rz = 0, zq = 0;
+    GRID_STRIDE(i, n) {
+        double zi = (double)z[i];
+        rz += r[i] * zi;
+        if (flexible && !init) zq += zi * q[i];
+    }
+    reduce2_finalize<TH>(rz, zq, partial, counter, FinDots{sc, flexible, init});
+}
+
+// p = z + beta p (multigrid.rs:749-751); p = z on the first call.
+template <class TZ>
+__global__ void k_pcg_p(int64_t n, const TZ* __restrict__ z, double* __restrict__ p,
+                        const Scalars* sc, int init) {
+    if (sc->done) return;
+    double beta = sc->beta;
+    GRID_STRIDE(i, n) p[i] = init ? (double)z[i] : (double)z[i] + beta * p[i];
+}
+
+// ------------------------------------------------------------------ power iteration
+struct FinTwo {
+    double* out;
+    __device__ void operator()(double a, double b) const {
+        out[0] = a;
+        out[1] = b;
+    }
+};
+
+// w = D^-1 A v; sums v.Av and v.Dv (the Rayleigh quotient of D^-1 A in the D inner product).
+__global__ void __launch_bounds__(TH)
+    k_power_step(SellView<double> A, const double* __restrict__ v, const double* __restrict__ dg,
+                 double* __restrict__ w, double* partial, unsigned* counter, double* out) {
+    double vav = 0, vdv = 0;
+    GRID_STRIDE(g, A.nslices * A.C) {
+        double av = sell_row<double, double, double>(A, g / A.C, (int)(g % A.C), v);
+        if (g < A.n) {
+            vav += v[g] * av;
+            vdv += v[g] * dg[g] * v[g];
+            w[g] = av / dg[g];
+        }
+    }
+    reduce2_finalize<TH>(vav, vdv, partial, counter, FinTwo{out});
+}
+
+__global__ void __launch_bounds__(TH)
+    k_norm2(int64_t n, const double* __restrict__ w, double* partial, unsigned* counter,
+            double* out) {
+    double s = 0;
+    GRID_STRIDE(i, n) s += w[i] * w[i];
+    reduce2_finalize<TH>(s, 0.0, partial, counter, FinTwo{out});
+}
+
+__global__ void k_scale_into(int64_t n, const double* __restrict__ w, const double* __restrict__ nrm,
+                             double* __restrict__ v) {
+    double f = 1.0 / sqrt(nrm[0]);
+    GRID_STRIDE(i, n) v[i] = w[i] * f;
+}
+
+__global__ void k_seed(int64_t n, double* __restrict__ v) {
+    GRID_STRIDE(i, n) {
+        uint32_t x = (uint32_t)i * 2654435761u + 12345u;
+        x ^= x >> 16;
+        x *= 0x7feb352dU;
+        x ^= x >> 15;
+        v[i] = 0.5 + (double)(x & 0xffffff) / (double)0x1000000;
+    }
+}
+
+__global__ void k_diagonal(int64_t n, const int64_t* __restrict__ ptr,
+                           const uint32_t* __restrict__ idx, const double* __restrict__ val,
+                           double* __restrict__ dg, int* __restrict__ bad) {
+    GRID_STRIDE(i, n) {
+        double d = 0;
+        for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+            if (idx[k] == (uint32_t)i) d = val[k];
+        dg[i] = d;
+        if (!(d > 0.0)) atomicExch(bad, 1);
+    }
+}
+
+// ------------------------------------------------------------------ dense Cholesky + inverse
+// Column-major n x n; the lower triangle. Blocked right-looking: a 32 x 32 diagonal block in
+// shared memory, the panel below it by rows, then the trailing lower triangle by 32 x 32 tiles.
+__global__ void k_potrf_diag(double* __restrict__ M, int64_t n, int64_t k0, int kb,
+                             const double* __restrict__ diag0, int64_t* __restrict__ status) {
+    __shared__ double A[32][33];
+    __shared__ int stop;
+    int tx = threadIdx.x, ty = threadIdx.y;
+    if (tx < kb && ty < kb) A[tx][ty] = M[(k0 + tx) + (k0 + ty) * n];
+    if (tx == 0 && ty == 0) stop = 0;
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        if (tx == 0 && ty == 0) {
+            double d = A[j][j];
+            if (!(d > PIVOT * fabs(diag0[k0 + j]))) {
+                if (*status == 0) *status = k0 + j + 1;
+                stop = 1;
+            } else {
+                A[j][j] = sqrt(d);
+            }
+        }
+        __syncthreads();
+        if (stop) return;
+        if (ty == 0 && tx > j && tx < kb) A[tx][j] /= A[j][j];
+        __syncthreads();
+        if (ty > j && tx >= ty && tx < kb) A[tx][ty] -= A[tx][j] * A[ty][j];
+        __syncthreads();
+    }
+    if (tx < kb && ty < kb && tx >= ty) M[(k0 + tx) + (k0 + ty) * n] = A[tx][ty];
+}
+
+__global__ void k_trsm_panel(double* __restrict__ M, int64_t n, int64_t k0, int kb,
+                             const int64_t* __restrict__ status) {
+    __shared__ double L[32][33];
+    if (*status) return;
+    for (int t = threadIdx.x; t < 32 * 32; t += blockDim.x) {
+        int i = t % 32, j = t / 32;
+        L[i][j] = (i < kb && j < kb) ? M[(k0 + i) + (k0 + j) * n] : 0.0;
+    }
+    __syncthreads();
+    int64_t i = k0 + kb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double l[32];
+    for (int j = 0; j < kb; ++j) {
+        double s = M[i + (k0 + j) * n];
+        for (int p = 0; p < j; ++p) s -= l[p] * L[j][p];
+        l[j] = s / L[j][j];
+        M[i + (k0 + j) * n] = l[j];
+    }
+}
+
+__global__ void k_syrk(double* __restrict__ M, int64_t n, int64_t k0, int kb,
+                       const int64_t* __restrict__ status) {
+    __shared__ double SA[32][33], SB[32][33];
+    if (*status) return;
+    int64_t t0 = k0 + kb;
+    int64_t b = blockIdx.x;
+    int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
+    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+    while (bi * (bi + 1) / 2 > b) --bi;
+    int64_t bj = b - bi * (bi + 1) / 2;
+    int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 32
+    int64_t ri = t0 + bi * 32 + tx, rj = t0 + bj * 32 + tx;
+    if (ty < kb) {
+        SA[tx][ty] = ri < n ? M[ri + (k0 + ty) * n] : 0.0;
+        SB[tx][ty] = rj < n ? M[rj + (k0 + ty) * n] : 0.0;
+    } else {
+        SA[tx][ty] = 0.0;
+        SB[tx][ty] = 0.0;
+    }
+    __syncthreads();
+    int64_t r = t0 + bi * 32 + tx, c = t0 + bj * 32 + ty;
+    if (r < n && c < n && r >= c) {
+        double acc = 0;
+        for (int p = 0; p < kb; ++p) acc += SA[tx][p] * SB[ty][p];
+        M[r + c * n] -= acc;
+    }
+}
+
+__global__ void k_transpose_lower(const double* __restrict__ L, int64_t n, double* __restrict__ R) {
+    GRID_STRIDE(t, n * n) {
+        int64_t i = t % n, j = t / n;
+        R[i * n + j] = i >= j ? L[i + j * n] : 0.0;
+    }
+}
+
+// Column c of L^-1 (as Y, column-major) by forward substitution: 1 warp per column.
+__global__ void k_inv_forward(const double* __restrict__ Lr, int64_t n, double* __restrict__ Y) {
+    int lane = threadIdx.x & 31;
+    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (c >= n) return;
+    double* y = Y + c * n;
+    for (int64_t k = lane; k < c; k += 32) y[k] = 0.0;
+    for (int64_t i = c; i < n; ++i) {
+        const double* row = Lr + i * n;
+        double s = 0;
+        for (int64_t k = c + lane; k < i; k += 32) s += row[k] * y[k];
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        double v = ((i == c ? 1.0 : 0.0) - s) / row[i];
+        if (lane == 0) y[i] = v;
+        __syncwarp();
+    }
+}
+
+// Column c of L^-T Y: backward substitution with L column-major.
+__global__ void k_inv_backward(const double* __restrict__ L, int64_t n, const double* __restrict__ Y,
+                               double* __restrict__ X) {
+    int lane = threadIdx.x & 31;
+    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (c >= n) return;
+    double* x = X + c * n;
+    const double* y = Y + c * n;
+    for (int64_t i = n - 1; i >= 0; --i) {
+        const double* col = L + i * n;
+        double s = 0;
+        for (int64_t k = i + 1 + lane; k < n; k += 32) s += col[k] * x[k];
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        double v = (y[i] - s) / col[i];
+        if (lane == 0) x[i] = v;
+        __syncwarp();
+    }
+}
+
+// The inverse of the SPD matrix `a` (host CSR, n small) on the device, FP64, row-major (it is
+// symmetric). Fails with the reference's text when a pivot is not positive.
+static void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
+    int64_t n = a.n;
+    std::vector<double> h((size_t)n * n, 0.0), diag(n, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
+            h[i + (int64_t)a.idx[k] * n] = a.val[k];
+            if ((int64_t)a.idx[k] == i) diag[i] = a.val[k];
+        }
+    DevBuf<double> M(n * n), d0(n);
+    M.upload(h.data(), n * n, s);
+    d0.upload(diag.data(), n, s);
+    DevBuf<int64_t> status(1);
+    status.zero(s);
+    for (int64_t k0 = 0; k0 < n; k0 += 32) {
+        int kb = (int)std::min<int64_t>(32, n - k0);
+        k_potrf_diag<<<1, dim3(32, 32), 0, s>>>(M.p, n, k0, kb, d0.p, status.p);
+        int64_t rest = n - k0 - kb;
+        if (rest > 0) {
+            k_trsm_panel<<<(unsigned)((rest + 127) / 128), 128, 0, s>>>(M.p, n, k0, kb, status.p);
+            int64_t T = (rest + 31) / 32;
+            k_syrk<<<(unsigned)(T * (T + 1) / 2), dim3(32, 32), 0, s>>>(M.p, n, k0, kb, status.p);
+        }
+        FG_CHECK_LAUNCH();
+    }
+    int64_t st = fetch(status.p, s);
+    if (st) {
+        char buf[320];
+        std::snprintf(buf, sizeof buf,
+                      "the matrix is not positive definite: the pivot of column %lld is 0 or less "
+                      "to the precision of the arithmetic (its diagonal is %e)",
+                      (long long)(st - 1), diag[st - 1]);
+        throw Failure(FEMGPU_ERR_NOT_SPD, buf);
+    }
+    DevBuf<double> Lr(n * n), Y(n * n);
+    k_transpose_lower<<<blocks_for(n * n, TH), TH, 0, s>>>(M.p, n, Lr.p);
+    k_inv_forward<<<(unsigned)((n * 32 + 127) / 128), 128, 0, s>>>(Lr.p, n, Y.p);
+    inv->alloc(n * n);
+    k_inv_backward<<<(unsigned)((n * 32 + 127) / 128), 128, 0, s>>>(M.p, n, Y.p, inv->p);
+    FG_CHECK_LAUNCH();
+    FG_CUDA(cudaStreamSynchronize(s));
+}
+
+// ------------------------------------------------------------------ helpers
+static void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s) {
+    d->n = h.n;
+    d->nnz = h.nnz();
+    d->ptr.upload(h.ptr.data(), h.n + 1, s);
+    d->idx.upload(h.idx.data(), h.nnz(), s);
+    d->val.upload(h.val.data(), h.nnz(), s);
+}
+
+static HostCsr download_csr(const DevCsr& d, cudaStream_t s) {
+    HostCsr h;
+    h.n = d.n;
+    h.ptr.resize(d.n + 1);
+    h.idx.resize(d.nnz);
+    h.val.resize(d.nnz);
+    d.ptr.download(h.ptr.data(), d.n + 1, s);
+    d.idx.download(h.idx.data(), d.nnz, s);
+    d.val.download(h.val.data(), d.nnz, s);
+    FG_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+static HostRect transpose(const HostRect& p) {
+    HostRect r;
+    r.rows = p.cols;
+    r.cols = p.rows;
+    r.ptr.assign(p.cols + 1, 0);
+    for (uint32_t j : p.idx) r.ptr[j + 1] += 1;
+    for (int64_t j = 0; j < p.cols; ++j) r.ptr[j + 1] += r.ptr[j];
+    r.idx.resize(p.idx.size());
+    r.val.resize(p.idx.size());
+    std::vector<int64_t> next(r.ptr.begin(), r.ptr.end() - 1);
+    for (int64_t i = 0; i < p.rows; ++i)
+        for (int64_t k = p.ptr[i]; k < p.ptr[i + 1]; ++k) {
+            uint32_t j = p.idx[k];
+            r.idx[next[j]] = (uint32_t)i;
+            r.val[next[j]] = p.val[k];
+            next[j]++;
+        }
+    return r;
+}
+
+template <class T>
+static void upload_values(const std::vector<double>& v, DevBuf<T>* d, cudaStream_t s) {
+    std::vector<T> t(v.begin(), v.end());
+    d->upload(t.data(), t.size(), s);
+    FG_CUDA(cudaStreamSynchronize(s));
+}
+
+// lambda_max of D^-1 A by the power method in the D inner product (15 steps), on the device.
+static double lambda_max(const Sell<double>& A, const double* dg, cudaStream_t s,
+                         DevBuf<double>& partial, DevBuf<unsigned>& counter) {
+    int64_t n = A.n;
+    // out[0..1]: v.Av and v.Dv of this step; out[2..3]: |w|^2 (and an unused 0).
+    DevBuf<double> v(n), w(n), out(4);
+    k_seed<<<blocks_for(n, TH), TH, 0, s>>>(n, v.p);
+    double lam = 0;
+    for (int it = 0; it < 15; ++it) {
+        k_power_step<<<RED_BLOCKS, TH, 0, s>>>(A.view(), v.p, dg, w.p, partial.p, counter.p,
+                                                 out.p);
+        k_norm2<<<RED_BLOCKS, TH, 0, s>>>(n, w.p, partial.p, counter.p, out.p + 2);
+        k_scale_into<<<blocks_for(n, TH), TH, 0, s>>>(n, w.p, out.p + 2, v.p);
+        FG_CHECK_LAUNCH();
+        if (it >= 12) {
+            double h[2];
+            FG_CUDA(cudaMemcpyAsync(h, out.p, 16, cudaMemcpyDeviceToHost, s));
+            FG_CUDA(cudaStreamSynchronize(s));
+            lam = std::max(lam, h[0] / h[1]);
+        }
+    }
+    return lam;
+}
+
+static void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
+                      std::vector<double>* c2) {
+    // Y. Saad, Iterative Methods for Sparse Linear Systems, 2nd ed., SIAM 2003, algorithm 12.1,
+    // on the interval [lower, 1.1] x lambda_max of D^-1 A.
+    double hi = 1.1 * lam, lo = lower * lam;
+    double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
+    c1->assign(degree, 0.0);
+    c2->assign(degree, 0.0);
+    (*c1)[0] = 1.0 / theta;
+    double rho = 1.0 / sigma;
+    for (int k = 1; k < degree; ++k) {
+        double rn = 1.0 / (2.0 * sigma - rho);
+        (*c2)[k] = rn * rho;
+        (*c1)[k] = 2.0 * rn / delta;
+        rho = rn;
+    }
+}
+
+// ------------------------------------------------------------------ SolverImpl
+SolverImpl::SolverImpl() {
+    FG_CUDA(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    FG_CUDA(cudaEventCreate(&ev0_));
+    FG_CUDA(cudaEventCreate(&ev1_));
+    partial_.alloc(2 * RED_BLOCKS);
+    counter_.alloc(1);
+    counter_.zero(s_);
+    sc_.alloc(1);
+    done_zero_.alloc(1);
+    done_zero_.zero(s_);
+    FG_CUDA(cudaMallocHost(&h_sc_, sizeof(Scalars)));
+}
+
+SolverImpl::~SolverImpl() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    if (h_sc_) cudaFreeHost(h_sc_);
+    if (ev0_) cudaEventDestroy(ev0_);
+    if (ev1_) cudaEventDestroy(ev1_);
+    if (s_) {
+        cudaStreamSynchronize(s_);
+        cudaStreamDestroy(s_);
+    }
+}
+
+template <class T>
+size_t Hierarchy<T>::bytes() const {
+    size_t b = inv.bytes() + cb.bytes() + cx.bytes();
+    for (const auto& l : levels)
+        b += l.A.bytes() + l.dinv.bytes() + l.pptr.bytes() + l.rptr.bytes() + l.pidx.bytes() +
+             l.ridx.bytes() + l.pval.bytes() + l.rval.bytes() + l.b.bytes() + l.xa.bytes() +
+             l.xb.bytes() + l.d.bytes() + l.r.bytes();
+    return b;
+}
+
+size_t SolverImpl::bytes() const {
+    return A64_.bytes() + a_.ptr.bytes() + a_.idx.bytes() + a_.val.bytes() + H64_.bytes() +
+           H32_.bytes() + dense_inv_.bytes() + 7 * n_ * sizeof(double) + r32_.bytes();
+}
+
+std::vector<int64_t> SolverImpl::level_sizes() const { return sizes_; }
+
+void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
+                        const femgpu_crossover& c, const Options& o) {
+    opt_ = o;
+    n_ = a.n;
+    // The solver's own copy of the matrix (the reference moves `a` into the Solver).
+    a_.n = a.n;
+    a_.nnz = a.nnz;
+    a_.ptr.alloc(a.n + 1);
+    a_.idx.alloc(a.nnz);
+    a_.val.alloc(a.nnz);
+    FG_CUDA(cudaMemcpyAsync(a_.ptr.p, a.ptr.p, a_.ptr.bytes(), cudaMemcpyDeviceToDevice, s_));
+    FG_CUDA(cudaMemcpyAsync(a_.idx.p, a.idx.p, a_.idx.bytes(), cudaMemcpyDeviceToDevice, s_));
+    FG_CUDA(cudaMemcpyAsync(a_.val.p, a.val.p, a_.val.bytes(), cudaMemcpyDeviceToDevice, s_));
+    int C = o.sell_c ? o.sell_c : 32;
+    make_sell<double>(a_, C, &A64_, s_);
+    x_.alloc(n_);
+    r_.alloc(n_);
+    p_.alloc(n_);
+    q_.alloc(n_);
+    b_.alloc(n_);
+    t_.alloc(n_);
+    if (c.rule != 0 && method < 0)
+        throw Failure(FEMGPU_ERR_INVALID,
+                      "Crossover::Flops needs the symbolic analysis of a sparse factor, which this "
+                      "library does not form: force a method");
+    // solve.rs:99-183: the choice of the method.
+    bool direct;
+    if (u.kind == FEMGPU_UNKNOWNS_POINTS) {
+        if (method == FEMGPU_METHOD_MULTIGRID)
+            throw Failure(FEMGPU_ERR_NEEDS_GRID,
+                          "multigrid needs the box grid: a mesh of tetrahedra has the direct solver");
+        direct = true;
+    } else if (method == FEMGPU_METHOD_DIRECT) {
+        direct = true;
+    } else if (method == FEMGPU_METHOD_MULTIGRID) {
+        direct = false;
+    } else {
+        direct = (size_t)a.n <= c.unknowns;
+    }
+    direct_ = direct;
+    HostCsr h = download_csr(a_, s_);
+    if (direct) {
+        dense_direct(h);
+        sizes_ = {n_};
+        return;
+    }
+    if (u.kind == FEMGPU_UNKNOWNS_GRID) {
+        HostLevel lv;
+        for (int d = 0; d < 3; ++d) lv.planes[d].assign(u.planes[d], u.planes[d] + u.nplanes[d]);
+        lv.points.resize(n_);
+        for (int64_t k = 0; k < n_; ++k)
+            for (int d = 0; d < 3; ++d) lv.points[k][d] = u.points[3 * k + d];
+        lv.comp.assign(u.comp, u.comp + n_);
+        build_multigrid(std::move(h), std::move(lv), nullptr);
+    } else {
+        // p-multigrid (pmultigrid.rs:46-98): the first coarse level is P^T A P on the corners,
+        // then geometric levels on the grid of the corner points.
+        HostRect p;
+        p.rows = n_;
+        p.cols = (int64_t)u.p_cols;
+        p.ptr.assign(u.p_ptr, u.p_ptr + n_ + 1);
+        p.idx.assign(u.p_idx, u.p_idx + p.ptr[n_]);
+        p.val.assign(u.p_val, u.p_val + p.ptr[n_]);
+        HostLevel lv = level_of_points(u.coarse_xyz, p.cols, u.coarse_comp);
+        build_multigrid(std::move(h), std::move(lv), &p);
+    }
+}
+
+void SolverImpl::dense_direct(const HostCsr& h) {
+    const int64_t LIMIT = 16384;
+    if (h.n > LIMIT)
+        throw Failure(FEMGPU_ERR_TOO_LARGE,
+                      "the direct solver of this library is a dense Cholesky factor on the device "
+                      "and holds at most 16384 unknowns: use multigrid");
+    dense_inverse(h, &dense_inv_, s_);
+}
+
+template <class T>
+void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps,
+                              Hierarchy<T>* H) {
+    size_t L = mats.size();
+    H->levels.resize(L - 1);
+    int C = opt_.sell_c ? opt_.sell_c : 32;
+    for (size_t l = 0; l + 1 < L; ++l) {
+        MgLevel<T>& lv = H->levels[l];
+        lv.n = mats[l].n;
+        lv.nnz = mats[l].nnz();
+        DevCsr d;
+        upload_csr(mats[l], &d, s_);
+        make_sell<T>(d, C, &lv.A, s_);
+        // The diagonal and lambda_max(D^-1 A) in FP64.
+        DevBuf<double> dg(lv.n);
+        DevBuf<int> bad(1);
+        bad.zero(s_);
+        k_diagonal<<<blocks_for(lv.n, TH), TH, 0, s_>>>(lv.n, d.ptr.p, d.idx.p, d.val.p, dg.p,
+                                                        bad.p);
+        FG_CHECK_LAUNCH();
+        if (fetch(bad.p, s_))
+            throw Failure(FEMGPU_ERR_NOT_SPD,
+                          "the matrix is not positive definite: it has a diagonal entry that is "
+                          "not above 0");
+        Sell<double> a64;
+        const Sell<double>* ap = nullptr;
+        if (l == 0) {
+            ap = &A64_;
+        } else {
+            make_sell<double>(d, C, &a64, s_);
+            ap = &a64;
+        }
+        lv.lambda = lambda_max(*ap, dg.p, s_, partial_, counter_);
+        std::vector<double> hd = dg.to_host(s_);
+        std::vector<double> inv(lv.n);
+        for (int64_t i = 0; i < lv.n; ++i) inv[i] = 1.0 / hd[i];
+        upload_values<T>(inv, &lv.dinv, s_);
+        int deg = opt_.degree > 0 ? opt_.degree : 2;
+        double lower = opt_.lower > 0 ? opt_.lower : 0.3;
+        chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2);
+        // Transfers to the next level.
+        const HostRect& P = ps[l];
+        HostRect R = transpose(P);
+        lv.nc = P.cols;
+        lv.pptr.upload(P.ptr.data(), P.rows + 1, s_);
+        lv.pidx.upload(P.idx.data(), P.idx.size(), s_);
+        upload_values<T>(P.val, &lv.pval, s_);
+        lv.rptr.upload(R.ptr.data(), R.rows + 1, s_);
+        lv.ridx.upload(R.idx.data(), R.idx.size(), s_);
+        upload_values<T>(R.val, &lv.rval, s_);
+        lv.b.alloc(lv.n);
+        lv.xa.alloc(lv.n);
+        lv.xb.alloc(lv.n);
+        lv.d.alloc(lv.n);
+        lv.r.alloc(lv.n);
+        FG_CUDA(cudaStreamSynchronize(s_));
+    }
+    // The coarsest level: its inverse from a dense Cholesky factor on the device.
+    const HostCsr& last = mats.back();
+    H->ncoarse = last.n;
+    DevBuf<double> inv64;
+    dense_inverse(last, &inv64, s_);
+    if constexpr (std::is_same<T, double>::value) {
+        H->inv = std::move(inv64);
+    } else {
+        H->inv.alloc(last.n * last.n);
+        k_convert<double, T><<<blocks_for(last.n * last.n, TH), TH, 0, s_>>>(last.n * last.n,
+                                                                            inv64.p, H->inv.p);
+        FG_CHECK_LAUNCH();
+        FG_CUDA(cudaStreamSynchronize(s_));
+    }
+    H->cb.alloc(last.n);
+    H->cx.alloc(last.n);
+}
+
+void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst) {
+    // multigrid.rs:84-139 (the Galerkin form): coarsen until a level has at most `coarsest`
+    // unknowns, 30 levels, or a coarsening keeps more than 90 % of the unknowns.
+    std::vector<HostCsr> mats;
+    std::vector<HostRect> ps;
+    int threads = host_threads();
+    mats.push_back(std::move(a0));
+    if (pfirst) {
+        // pmultigrid.rs:47: the P1 level is the Galerkin product with the P2 -> P1 prolongation.
+        mats.push_back(galerkin(*pfirst, mats[0], threads));
+        ps.push_back(*pfirst);
+    }
+    size_t coarsest = (size_t)(opt_.coarsest > 0 ? opt_.coarsest : 3000);
+    size_t max_levels = (size_t)(opt_.max_levels > 0 ? opt_.max_levels : 30);
+    for (;;) {
+        const HostCsr& a = mats.back();
+        if ((size_t)a.n <= coarsest || ps.size() >= max_levels) break;
+        HostRect p;
+        HostLevel coarse;
+        if (!coarsen(level, a, &p, &coarse)) break;
+        if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
+        HostCsr ac = galerkin(p, a, threads);
+        mats.push_back(std::move(ac));
+        ps.push_back(std::move(p));
+        level = std::move(coarse);
+    }
+    if ((size_t)mats.back().n > 16384)
+        throw Failure(FEMGPU_ERR_TOO_LARGE,
+                      "the coarsest level has more than 16384 unknowns: the grid does not coarsen");
+    sizes_.clear();
+    for (const auto& m : mats) sizes_.push_back(m.n);
+    if (opt_.precision == FEMGPU_MIXED) {
+        build_levels<float>(mats, ps, &H32_);
+        r32_.alloc(n_);
+    } else {
+        build_levels<double>(mats, ps, &H64_);
+    }
+}
+
+template <class T>
+const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
+    const int* done = &sc_.p->done;
+    if (l == H.levels.size()) {
+        int64_t n = H.ncoarse;
+        k_gemv<T><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, H.inv.p, b, H.cx.p, done);
+        FG_CHECK_LAUNCH();
+        launches_ += 1;
+        return H.cx.p;
+    }
+    MgLevel<T>& L = H.levels[l];
+    int64_t n = L.n;
+    int gb = blocks_for(n, TH, NUM_SMS * 8);
+    int gs = blocks_for(L.A.nslices * L.A.C, TH, NUM_SMS * 8);
+    T* xa = L.xa.p;
+    T* xb = L.xb.p;
+    int deg = (int)L.c1.size();
+    k_cheb_first<T><<<gb, TH, 0, s_>>>(n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
+    for (int k = 1; k < deg; ++k) {
+        k_cheb_step<T><<<gs, TH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k],
+                                          L.d.p, xb, done);
+        std::swap(xa, xb);
+    }
+    k_residual<T><<<gs, TH, 0, s_>>>(L.A.view(), b, xa, L.r.p, done);
+    T* bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
+    k_restrict<T><<<blocks_for(L.nc, TH, NUM_SMS * 8), TH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p,
+                                                                     L.rval.p, L.r.p, bc, done);
+    FG_CHECK_LAUNCH();
+    launches_ += deg + 2;
+    const T* ec = enqueue_vcycle(H, l + 1, bc);
+    k_prolong<T><<<gb, TH, 0, s_>>>(n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
+    for (int k = 0; k < deg; ++k) {
+        k_cheb_step<T><<<gs, TH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k],
+                                          L.d.p, xb, done);
+        std::swap(xa, xb);
+    }
+    FG_CHECK_LAUNCH();
+    launches_ += deg + 1;
+    return xa;
+}
+
+void SolverImpl::enqueue_iteration() {
+    int64_t n = n_;
+    launches_ += 4;
+    int gs = blocks_for(A64_.nslices * A64_.C, TH, RED_BLOCKS);
+    (void)gs;
+    Scalars* sc = sc_.p;
+    bool mixed = opt_.precision == FEMGPU_MIXED;
+    k_pcg_spmv_pq<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), p_.p, q_.p, partial_.p, counter_.p, sc);
+    k_pcg_update<<<RED_BLOCKS, TH, 0, s_>>>(n, x_.p, r_.p, p_.p, q_.p, mixed ? r32_.p : nullptr,
+                                            partial_.p, counter_.p, sc, tol);
+    FG_CHECK_LAUNCH();
+    if (mixed) {
+        zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
+        k_pcg_dots<float><<<RED_BLOCKS, TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 0, partial_.p,
+                                                     counter_.p, sc);
+        k_pcg_p<float><<<blocks_for(n, TH, NUM_SMS * 8), TH, 0, s_>>>(n, zf_, p_.p, sc, 0);
+    } else {
+        zd_ = enqueue_vcycle<double>(H64_, 0, r_.p);
+        k_pcg_dots<double><<<RED_BLOCKS, TH, 0, s_>>>(n, r_.p, zd_, q_.p, 0, 0, partial_.p,
+                                                      counter_.p, sc);
+        k_pcg_p<double><<<blocks_for(n, TH, NUM_SMS * 8), TH, 0, s_>>>(n, zd_, p_.p, sc, 0);
+    }
+    FG_CHECK_LAUNCH();
+}
+
+void SolverImpl::precondition(const double* d_r, double* d_z) {
+    FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
+    if (direct_) {
+        k_gemv<double><<<blocks_for(n_ * 32, TH), TH, 0, s_>>>(n_, dense_inv_.p, d_r, d_z,
+                                                               done_zero_.p);
+    } else if (opt_.precision == FEMGPU_MIXED) {
+        k_convert<double, float><<<blocks_for(n_, TH), TH, 0, s_>>>(n_, d_r, r32_.p);
+        const float* z = enqueue_vcycle<float>(H32_, 0, r32_.p);
+        k_convert<float, double><<<blocks_for(n_, TH), TH, 0, s_>>>(n_, z, d_z);
+    } else {
+        const double* z = enqueue_vcycle<double>(H64_, 0, d_r);
+        FG_CUDA(cudaMemcpyAsync(d_z, z, n_ * 8, cudaMemcpyDeviceToDevice, s_));
+    }
+    FG_CHECK_LAUNCH();
+    FG_CUDA(cudaStreamSynchronize(s_));
+}
+
+void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cancel,
+                       femgpu_stats* st) {
+    int64_t n = n_;
+    bool mixed = opt_.precision == FEMGPU_MIXED;
+    FG_CUDA(cudaEventRecord(ev0_, s_));
+    FG_CUDA(cudaMemcpyAsync(b_.p, d_b, n * 8, cudaMemcpyDeviceToDevice, s_));
+    Scalars init{};
+    FG_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(Scalars), cudaMemcpyHostToDevice, s_));
+    femgpu_stats out{};
+    launches_ = 0;
+    if (direct_) {
+        launches_ = 6;
+        // solve.rs:206-218: x = A^-1 b (with 1 step of refinement in FP64), then the true
+        // residual.
+        k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, dense_inv_.p, b_.p, x_.p,
+                                                              done_zero_.p);
+        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p, nullptr,
+                                                  partial_.p, counter_.p, sc_.p);
+        k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, dense_inv_.p, r_.p, t_.p,
+                                                              done_zero_.p);
+        k_add<<<blocks_for(n, TH), TH, 0, s_>>>(n, t_.p, x_.p);
+        FG_CHECK_LAUNCH();
+        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p, nullptr,
+                                                  partial_.p, counter_.p, sc_.p);
+        FG_CHECK_LAUNCH();
+        FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
+        FG_CUDA(cudaMemcpyAsync(d_x, x_.p, n * 8, cudaMemcpyDeviceToDevice, s_));
+        FG_CUDA(cudaEventRecord(ev1_, s_));
+        FG_CUDA(cudaStreamSynchronize(s_));
+        double bn = std::sqrt(h_sc_->bb), rn = std::sqrt(h_sc_->rr);
+        out.iterations = 0;
+        out.residual = bn > 0.0 ? rn / bn : rn;
+        out.true_residual = out.residual;
+        out.launches = launches_;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev0_, ev1_);
+        out.seconds = ms * 1e-3;
+        if (st) *st = out;
+        return;
+    }
+    // multigrid.rs:692-753
+    FG_CUDA(cudaMemcpyAsync(x_.p, d_x, n * 8, cudaMemcpyDeviceToDevice, s_));
+    k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p,
+                                              mixed ? r32_.p : nullptr, partial_.p, counter_.p,
+                                              sc_.p);
+    FG_CHECK_LAUNCH();
+    launches_ += 3;  // this residual, and r.z and p = z after the first cycle
+    FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
+    FG_CUDA(cudaStreamSynchronize(s_));
+    double norm_b = h_sc_->norm_b;
+    if (norm_b == 0.0) {
+        FG_CUDA(cudaMemsetAsync(d_x, 0, n * 8, s_));
+        FG_CUDA(cudaStreamSynchronize(s_));
+        if (st) *st = out;
+        return;
+    }
+    // z = M^-1 r, p = z, rz = r.z
+    if (mixed) {
+        zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
+        k_pcg_dots<float><<<RED_BLOCKS, TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 1, partial_.p,
+                                                     counter_.p, sc_.p);
+        k_pcg_p<float><<<blocks_for(n, TH), TH, 0, s_>>>(n, zf_, p_.p, sc_.p, 1);
+    } else {
+        zd_ = enqueue_vcycle<double>(H64_, 0, r_.p);
+        k_pcg_dots<double><<<RED_BLOCKS, TH, 0, s_>>>(n, r_.p, zd_, q_.p, 0, 1, partial_.p,
+                                                      counter_.p, sc_.p);
+        k_pcg_p<double><<<blocks_for(n, TH), TH, 0, s_>>>(n, zd_, p_.p, sc_.p, 1);
+    }
+    FG_CHECK_LAUNCH();
+    if (opt_.graph && !exec_) {
+        size_t before = launches_;
+        FG_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
+        enqueue_iteration();
+        FG_CUDA(cudaStreamEndCapture(s_, &graph_));
+        FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+        graph_kernels_ = launches_ - before;
+        launches_ = before;
+    }
+    int status = FEMGPU_OK;
+    std::string message;
+    double residual = std::sqrt(h_sc_->rr) / norm_b;
+    size_t it = 0;
+    int restarts = 0;
+    for (;;) {
+        // multigrid.rs:721-738: the residual test, then the iteration limit, then the cancel.
+        if (residual <= tol) {
+            // The true residual in FP64; with an FP32 preconditioner the recurrence can drift
+            // from it, and then the solve restarts from x (iterative refinement).
+            k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, t_.p, nullptr,
+                                                      partial_.p, counter_.p, sc_.p);
+            FG_CHECK_LAUNCH();
+            launches_ += 1;
+            FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
+            FG_CUDA(cudaStreamSynchronize(s_));
+            double truth = std::sqrt(h_sc_->rr) / norm_b;
+            out.true_residual = truth;
+            if (truth <= tol || !mixed || restarts >= 3 || it >= max_iter) break;
+            ++restarts;
+            FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
+            k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p, r32_.p,
+                                                      partial_.p, counter_.p, sc_.p);
+            zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
+            k_pcg_dots<float><<<RED_BLOCKS, TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 1, partial_.p,
+                                                         counter_.p, sc_.p);
+            k_pcg_p<float><<<blocks_for(n, TH), TH, 0, s_>>>(n, zf_, p_.p, sc_.p, 1);
+            FG_CHECK_LAUNCH();
+            launches_ += 3;
+            residual = truth;
+            continue;
+        }
+        if (it == max_iter) {
+            char buf[200];
+            std::snprintf(buf, sizeof buf,
+                          "conjugate gradients did not converge: the residual is %.2e after %zu "
+                          "iterations",
+                          residual, max_iter);
+            status = FEMGPU_ERR_NOT_CONVERGED;
+            message = buf;
+            break;
+        }
+        if (cancel && *cancel) {
+            status = FEMGPU_ERR_CANCELLED;
+            message = "cancelled";
+            break;
+        }
+        if (exec_) {
+            FG_CUDA(cudaGraphLaunch(exec_, s_));
+            launches_ += graph_kernels_;
+        } else {
+            enqueue_iteration();
+        }
+        FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
+        FG_CUDA(cudaStreamSynchronize(s_));
+        ++it;
+        residual = std::sqrt(h_sc_->rr) / norm_b;
+        if (!(residual == residual)) {
+            status = FEMGPU_ERR_NOT_CONVERGED;
+            message = "conjugate gradients broke down: the residual is not a number";
+            break;
+        }
+    }
+    FG_CUDA(cudaMemcpyAsync(d_x, x_.p, n * 8, cudaMemcpyDeviceToDevice, s_));
+    FG_CUDA(cudaEventRecord(ev1_, s_));
+    FG_CUDA(cudaStreamSynchronize(s_));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0_, ev1_);
+    out.iterations = it;
+    out.residual = residual;
+    out.seconds = ms * 1e-3;
+    out.launches = launches_;
+    if (st) *st = out;
+    if (status != FEMGPU_OK) throw Failure(status, message);
+}
+
+void SolverImpl::kernel_time(int which, int reps, double* ms, double* bytes) {
+    if (reps < 1) reps = 1;
+    bool mixed = opt_.precision == FEMGPU_MIXED;
+    FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
+    auto launch = [&]() {
+        if (which == 1) {
+            k_pcg_spmv_pq<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), p_.p, q_.p, partial_.p,
+                                                     counter_.p, sc_.p);
+        } else if (mixed) {
+            MgLevel<float>& L = H32_.levels.at(0);
+            int gs = blocks_for(L.A.nslices * L.A.C, TH, NUM_SMS * 8);
+            k_cheb_step<float><<<gs, TH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p, 0.5f,
+                                                  0.5f, L.d.p, L.xb.p, done_zero_.p);
+        } else {
+            MgLevel<double>& L = H64_.levels.at(0);
+            int gs = blocks_for(L.A.nslices * L.A.C, TH, NUM_SMS * 8);
+            k_cheb_step<double><<<gs, TH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p, 0.5, 0.5,
+                                                   L.d.p, L.xb.p, done_zero_.p);
+        }
+    };
+    if (which == 0 && (mixed ? H32_.levels.empty() : H64_.levels.empty()))
+        throw Failure(FEMGPU_ERR_INVALID, "the solver has no smoothed level");
+    if (which == 0) {
+        // Defined inputs for the timed launches.
+        if (mixed) {
+            auto& L = H32_.levels[0];
+            L.b.zero(s_); L.xa.zero(s_); L.d.zero(s_);
+        } else {
+            auto& L = H64_.levels[0];
+            L.b.zero(s_); L.xa.zero(s_); L.d.zero(s_);
+        }
+    } else {
+        p_.zero(s_);
+    }
+    for (int w = 0; w < 3; ++w) launch();
+    FG_CHECK_LAUNCH();
+    FG_CUDA(cudaEventRecord(ev0_, s_));
+    for (int k = 0; k < reps; ++k) launch();
+    FG_CUDA(cudaEventRecord(ev1_, s_));
+    FG_CUDA(cudaEventSynchronize(ev1_));
+    float t = 0;
+    FG_CUDA(cudaEventElapsedTime(&t, ev0_, ev1_));
+    *ms = t / reps;
+    if (which == 1) {
+        *bytes = (double)a_.nnz * 12.0 + 2.0 * (double)n_ * 8.0;
+    } else if (mixed) {
+        auto& L = H32_.levels[0];
+        *bytes = (double)L.nnz * 8.0 + 6.0 * (double)L.n * 4.0;
+    } else {
+        auto& L = H64_.levels[0];
+        *bytes = (double)L.nnz * 12.0 + 6.0 * (double)L.n * 8.0;
+    }
+}
+
+}  // namespace femgpu

@@ -1,0 +1,124 @@
+// The solver of a matrix on the device: the reference's `Solver` (solve.rs:58-250) with a
+// dense Cholesky for the direct method and for the coarsest level, and PCG with a geometric or
+// p-multigrid V-cycle of Chebyshev-Jacobi smoothing.
+#pragma once
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "hierarchy.hpp"
+#include "sell.cuh"
+
+namespace femgpu {
+
+template <class T>
+struct Sell {
+    int64_t n = 0, nslices = 0, entries = 0;
+    int C = 32;
+    DevBuf<int64_t> slice_ptr;
+    DevBuf<uint32_t> col;
+    DevBuf<T> val;
+    SellView<T> view() const { return {n, nslices, C, slice_ptr.p, col.p, val.p}; }
+    size_t bytes() const { return slice_ptr.bytes() + col.bytes() + val.bytes(); }
+};
+
+// A SELL-C matrix of `a` with values converted to T.
+template <class T>
+void make_sell(const DevCsr& a, int C, Sell<T>* out, cudaStream_t s);
+
+// The scalars of a PCG solve, in device memory.
+struct Scalars {
+    double bb, rr, rz, pq, alpha, beta, zq, norm_b;
+    int done, iters, status, pad;
+};
+
+template <class T>
+struct MgLevel {
+    int64_t n = 0, nnz = 0;
+    Sell<T> A;
+    DevBuf<T> dinv;
+    // The prolongation P from the next level, and R = P^T (gather form of the restriction).
+    int64_t nc = 0;
+    DevBuf<int64_t> pptr, rptr;
+    DevBuf<uint32_t> pidx, ridx;
+    DevBuf<T> pval, rval;
+    DevBuf<T> b, xa, xb, d, r;
+    std::vector<double> c1, c2;
+    double lambda = 0;
+};
+
+template <class T>
+struct Hierarchy {
+    std::vector<MgLevel<T>> levels;  // all but the coarsest
+    int64_t ncoarse = 0;
+    DevBuf<T> inv;  // the inverse of the coarsest matrix, n x n (symmetric)
+    DevBuf<T> cb, cx;
+    size_t bytes() const;
+};
+
+struct Options {
+    int precision = FEMGPU_FP64;
+    int degree = 0;
+    double lower = 0;
+    int sell_c = 0;
+    int coarsest = 3000;
+    int max_levels = 30;
+    bool graph = true;
+};
+
+class SolverImpl {
+   public:
+    SolverImpl();
+    ~SolverImpl();
+    // solve.rs:92-183
+    void create(const DevCsr& a, const femgpu_unknowns& u, int method, const femgpu_crossover& c,
+                const Options& o);
+    // solve.rs:199-250 on device vectors
+    void solve(const double* d_b, double* d_x, const volatile int* cancel, femgpu_stats* st);
+    void precondition(const double* d_r, double* d_z);
+    int method() const { return direct_ ? FEMGPU_METHOD_DIRECT : FEMGPU_METHOD_MULTIGRID; }
+    std::vector<int64_t> level_sizes() const;
+    size_t bytes() const;
+    // The mean device time (ms) of 1 launch of a kernel of the solve, and its algorithmic bytes.
+    void kernel_time(int which, int reps, double* ms, double* bytes);
+    size_t max_iter = 500;  // PCG_MAX_ITER, solve.rs:43
+    double tol = 1e-10;     // PCG_TOL, solve.rs:42
+    cudaStream_t stream() const { return s_; }
+
+   private:
+    void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst);
+    template <class T>
+    void build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps, Hierarchy<T>* H);
+    template <class T>
+    const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b);
+    void enqueue_iteration();
+    void run_init(const double* d_b);
+    void dense_direct(const HostCsr& a);
+
+    cudaStream_t s_ = nullptr;
+    Options opt_;
+    bool direct_ = false;
+    int64_t n_ = 0;
+    Sell<double> A64_;
+    DevCsr a_;  // the matrix, FP64 CSR
+    Hierarchy<double> H64_;
+    Hierarchy<float> H32_;
+    DevBuf<double> dense_inv_;  // the direct method: A^-1
+    DevBuf<double> x_, r_, p_, q_, b_, z64_, t_;
+    DevBuf<float> r32_;
+    const double* zd_ = nullptr;  // where the V-cycle leaves z (FP64 form)
+    const float* zf_ = nullptr;   // (mixed form)
+    DevBuf<double> partial_;
+    DevBuf<unsigned> counter_;
+    DevBuf<Scalars> sc_;
+    Scalars* h_sc_ = nullptr;
+    DevBuf<int> done_zero_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    std::vector<int64_t> sizes_;
+    size_t launches_ = 0;      // kernels enqueued by the current solve
+    size_t graph_kernels_ = 0; // kernels of 1 iteration graph
+};
+
+}  // namespace femgpu

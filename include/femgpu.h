@@ -1,0 +1,222 @@
+/* femgpu: the fh-fem iterative solve path of femahoy on one B200 (sm_100a), behind a C ABI.
+ *
+ * Each entry point replaces one interface of the Rust crate `fh-fem` (crates/fem/src in the
+ * femahoy project); the comment above it cites the item it replaces. Plain pointers and sizes
+ * only. Functions ending in `_device` take device pointers (CUDA global memory on the current
+ * device); all others take host pointers. Every function returns FEMGPU_OK (0) or a status
+ * code below; femgpu_last_error() gives the message, with the reference's text where the
+ * reference has one ("cancelled", "conjugate gradients did not converge: ...", "the matrix is
+ * not positive definite: ...", "multigrid needs the box grid: ...").
+ *
+ * Threading: a handle is used from one host thread at a time (as the reference's `Solver`,
+ * which is Send + Sync but solves synchronously). Different handles may be used from
+ * different threads; each handle owns its CUDA stream.
+ */
+#ifndef FEMGPU_H
+#define FEMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. Each maps one-to-one onto an error string of the reference. */
+enum {
+    FEMGPU_OK = 0,
+    FEMGPU_ERR_CANCELLED = 1,      /* "cancelled" (multigrid.rs:735-737) */
+    FEMGPU_ERR_NOT_CONVERGED = 2,  /* "conjugate gradients did not converge: ..." (multigrid.rs:729-733) */
+    FEMGPU_ERR_NOT_SPD = 3,        /* "the matrix is not positive definite: ..." (cholesky.rs:92-99) */
+    FEMGPU_ERR_NEEDS_GRID = 4,     /* "multigrid needs the box grid: ..." (solve.rs:133-138) */
+    FEMGPU_ERR_INVALID = 5,        /* an argument out of range; the message names it */
+    FEMGPU_ERR_CUDA = 6,           /* a CUDA runtime error; the message names the call site */
+    FEMGPU_ERR_TOO_LARGE = 7,      /* a size above a documented limit of this library */
+    FEMGPU_ERR_PATTERN = 8,        /* "the pattern holds each element pair" (sparse.rs:80-82) */
+    FEMGPU_ERR_MATERIAL = 9,       /* hex.rs:72-98: the moduli or Poisson ratios give no material */
+    FEMGPU_ERR_TIMEOUT = 10        /* a device-side wait ran out of its iteration limit */
+};
+
+/* Element kinds of the assembly. */
+enum {
+    FEMGPU_P1_HEAT = 0,    /* 4-node tet, 4 x 4 conduction V G^T K G (heat.rs:972-1002) */
+    FEMGPU_P1_ELASTIC = 1, /* 4-node tet, 12 x 12 V B^T D B (this library's own element) */
+    FEMGPU_P2_ELASTIC = 2  /* 10-node tet, 30 x 30, 4-point rule (tet10.rs:90-120) */
+};
+
+/* Assembly modes. */
+enum {
+    FEMGPU_ASSEMBLE_GATHER = 0, /* each row sums its element terms in increasing element order:
+                                   bit-identical with Csr::add_element (sparse.rs:75-86) */
+    FEMGPU_ASSEMBLE_COLOUR = 1  /* elements scattered colour by colour, no atomics: the same
+                                   terms summed in colour order (a few ulp apart) */
+};
+
+/* Solver methods (solve.rs:47-50). -1 lets the crossover choose. */
+enum { FEMGPU_METHOD_NONE = -1, FEMGPU_METHOD_DIRECT = 0, FEMGPU_METHOD_MULTIGRID = 1 };
+
+/* Precision of the iterative solve. */
+enum {
+    FEMGPU_FP64 = 0,  /* plain form: FP64 operator, V-cycle and PCG (Hestenes-Stiefel, as
+                         multigrid.rs:692-753) */
+    FEMGPU_MIXED = 1  /* FP32 V-cycle (values FP32, indices int32) inside FP64 flexible CG; the
+                         outer residual, dots, scalars, update and coarse factor stay FP64 */
+};
+
+typedef struct femgpu_csr femgpu_csr;       /* a device-resident square CSR matrix */
+typedef struct femgpu_solver femgpu_solver; /* solve.rs:58-61 `Solver` */
+
+/* The message of the last failure of this host thread. */
+size_t femgpu_last_error(char* buf, size_t len);
+/* The library version and the device it runs on. */
+const char* femgpu_version(void);
+
+/* ---------------------------------------------------------------- assembly */
+
+/* Csr::pattern + Csr::add_element over all elements (sparse.rs:22-86), as called by
+ * heat.rs:920-927 (P1 heat), elastic_tet.rs:183-193 (P2 elasticity, unknown 3 node + component)
+ * and for P1 elasticity. `xyz` holds 3 coordinates per point; `nodes` 4 (P1) or 10 (P2) point
+ * numbers per element; `coef` 3 conductivities (P1 heat) or E and nu (elasticity) per
+ * element. The result is the full matrix on the device: n = points (heat) or 3 points. */
+int femgpu_assemble(int kind, int mode, size_t npoints, const double* xyz, size_t nel,
+                    const uint32_t* nodes, const double* coef, femgpu_csr** out);
+int femgpu_assemble_device(int kind, int mode, size_t npoints, const double* xyz, size_t nel,
+                           const uint32_t* nodes, const double* coef, femgpu_csr** out);
+
+/* Csr::pattern alone (sparse.rs:22-65) for `nel` elements of `m` nodes each. */
+int femgpu_pattern(size_t n, size_t nel, int m, const uint32_t* elements, femgpu_csr** out);
+
+/* Element colouring for the colour-ordered scatter: elements that share a node get different
+ * colours (Jones-Plassmann with a fixed hash priority; deterministic). No reference
+ * counterpart: the reference assembles sequentially (sparse.rs:75). */
+int femgpu_colour(size_t n, size_t nel, int m, const uint32_t* elements, uint32_t* colour,
+                  int* ncolours);
+
+/* Quadratic::new (tet10.rs:244-272): the 10 points of each tetrahedron, the edge points
+ * numbered from `ncorner` in the order of first sight. `tets10` holds 10 * ntet values and
+ * `edges` 2 * (6 * ntet) values; `nedges` gets the edge count. */
+int femgpu_quadratic(size_t ncorner, size_t ntet, const uint32_t* tets, uint32_t* tets10,
+                     uint32_t* edges, size_t* nedges);
+
+/* The matrix's size and entries; its CSR arrays (ptr n + 1, idx nnz, val nnz) to host. */
+int femgpu_csr_info(const femgpu_csr* a, size_t* n, size_t* nnz);
+int femgpu_csr_download(const femgpu_csr* a, int64_t* ptr, uint32_t* idx, double* val);
+/* A device matrix from host CSR arrays (the Rust `Csr` handed to Solver::new). */
+int femgpu_csr_upload(size_t n, const int64_t* ptr, const uint32_t* idx, const double* val,
+                      femgpu_csr** out);
+/* Csr::submatrix (sparse.rs:108-135): rows and columns `keep` (each index once). */
+int femgpu_csr_submatrix(const femgpu_csr* a, const int64_t* keep, size_t nkeep,
+                         femgpu_csr** out);
+/* Csr::mul (sparse.rs:96-105): y = A x, host vectors. */
+int femgpu_csr_mul(const femgpu_csr* a, const double* x, double* y);
+/* heat::reduced_rhs (heat.rs:1219-1244, steady form): load - A t over the fixed columns, for
+ * the free rows `free` (increasing). Host vectors; `out` holds nfree values. */
+int femgpu_reduced_rhs(const femgpu_csr* a, const double* load, const double* t,
+                       const int64_t* free, size_t nfree, double* out);
+void femgpu_csr_free(femgpu_csr* a);
+
+/* pmultigrid::prolongation (pmultigrid.rs:104-151): P from the free corner unknowns to the
+ * free unknowns of a quadratic mesh. Two calls: with null outputs it writes the sizes
+ * (`nnz`, `ncoarse`); then the CSR arrays of P (rows = nfree) and the coarse points (3 each). */
+int femgpu_prolongation(size_t npoints, const double* points, size_t corners, size_t nedges,
+                        const uint32_t* edges, size_t nfree, const int64_t* free, size_t* nnz,
+                        size_t* ncoarse, int64_t* p_ptr, uint32_t* p_idx, double* p_val,
+                        double* coarse_xyz);
+
+/* ---------------------------------------------------------------- solver */
+
+/* solve.rs:64-77 `Unknowns`. */
+enum { FEMGPU_UNKNOWNS_GRID = 0, FEMGPU_UNKNOWNS_POINTS = 1, FEMGPU_UNKNOWNS_QUADRATIC = 2 };
+
+typedef struct femgpu_unknowns {
+    int kind;
+    /* GRID (multigrid.rs:55-59 `Level`): the planes of each axis, and the grid point (3 values)
+     * and component of each unknown. */
+    const double* planes[3];
+    size_t nplanes[3];
+    const uint32_t* points;
+    const uint8_t* comp;
+    /* POINTS and QUADRATIC: the coordinates of each unknown (3 values each). */
+    const double* xyz;
+    /* QUADRATIC: the prolongation P (rows = unknowns, cols = coarse unknowns) and the point of
+     * each coarse unknown; `coarse_comp` (optional, may be null) gives the component of each
+     * coarse unknown, else it is inferred from the order of the unknowns at each point. */
+    size_t p_cols;
+    const int64_t* p_ptr;
+    const uint32_t* p_idx;
+    const double* p_val;
+    const double* coarse_xyz;
+    const uint8_t* coarse_comp;
+} femgpu_unknowns;
+
+/* solve.rs:28-39 `Crossover`: rule 0 = Unknowns(unknowns); 1 = Flops{flops, entries, flat}. */
+typedef struct femgpu_crossover {
+    int rule;
+    size_t unknowns;
+    double flops;
+    uint64_t entries;
+    int flat;
+} femgpu_crossover;
+
+/* Options of this library (no reference counterpart; zeros pick the defaults). */
+typedef struct femgpu_options {
+    int precision;        /* FEMGPU_FP64 or FEMGPU_MIXED */
+    int degree;           /* Chebyshev degree of each pre- and post-smoothing; 0 = autotuned */
+    double lower;         /* Chebyshev interval lower end as a fraction of lambda_max; 0 = default */
+    int sell_c;           /* SELL chunk height (rows per slice): 0 = autotuned */
+    int sell_sigma;       /* SELL sorting window in rows: 0 = autotuned */
+    int coarsest;         /* the largest level that the dense coarse solve takes; 0 = 3000 */
+    int max_levels;       /* 0 = 30 (multigrid.rs:94) */
+    int graph;            /* 1 = replay each PCG iteration as a CUDA graph (default), 2 = off */
+} femgpu_options;
+
+/* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end
+ * (the reference reports the recurrence residual for PCG and the true one for Cholesky). */
+typedef struct femgpu_stats {
+    size_t iterations;
+    double residual;       /* the reference's definition for the method that ran */
+    double true_residual;  /* |b - A x|_2 / |b|_2 in FP64 on the device */
+    double seconds;        /* device time of the solve (CUDA events) */
+    size_t launches;       /* kernels this library launched for the solve */
+} femgpu_stats;
+
+/* Solver::new (solve.rs:92-183). The solver keeps a copy of `a` on the device (the reference
+ * moves `a` in). `a` may be freed after the call. `cells` (hex elasticity, multigrid.rs:62-68)
+ * is not supported: box-grid hex elements are outside this library. */
+int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* unknowns, int method,
+                      const femgpu_crossover* crossover, const femgpu_options* options,
+                      femgpu_solver** out);
+/* Solver::with_max_iter (solve.rs:187-189). */
+int femgpu_solver_set_max_iter(femgpu_solver* s, size_t max_iter);
+/* The relative residual of each PCG solve; PCG_TOL = 1e-10 (solve.rs:42) by default. */
+int femgpu_solver_set_tol(femgpu_solver* s, double tol);
+/* Solver::method (solve.rs:191-196). */
+int femgpu_solver_method(const femgpu_solver* s);
+/* The number of unknowns of each level (levels[0] = n); returns the level count. */
+int femgpu_solver_levels(const femgpu_solver* s, size_t* sizes, int cap);
+/* Device memory held by the solver, in bytes. */
+size_t femgpu_solver_bytes(const femgpu_solver* s);
+/* Solver::solve (solve.rs:199-250): solve A x = b; `x` holds the start value and gets the
+ * solution. `cancel` (may be null) is read before each PCG iteration, as the reference's
+ * `cancelled` closure; a non-zero value ends the solve with FEMGPU_ERR_CANCELLED. */
+int femgpu_solver_solve(femgpu_solver* s, const double* b, double* x, const volatile int* cancel,
+                        femgpu_stats* stats);
+int femgpu_solver_solve_device(femgpu_solver* s, const double* b, double* x,
+                               const volatile int* cancel, femgpu_stats* stats);
+/* z = M^-1 r: 1 application of the preconditioner (a V-cycle), device vectors. */
+int femgpu_solver_precondition_device(femgpu_solver* s, const double* r, double* z);
+void femgpu_solver_free(femgpu_solver* s);
+
+/* The CUDA stream (a cudaStream_t) on which the solver launches all its work, so that a caller
+ * can order its own work and CUDA events with it. No reference counterpart. */
+void* femgpu_solver_stream(const femgpu_solver* s);
+/* Times `reps` back-to-back launches of 1 kernel of the solve on the solver's stream with CUDA
+ * events: which = 0 the finest Chebyshev smoothing step, 1 the FP64 operator product of PCG
+ * (fused with p.q). Writes the mean device time of a launch (ms) and the algorithmic bytes of 1
+ * launch (values, indices and vectors, each read or written once). No reference counterpart. */
+int femgpu_solver_kernel_time(femgpu_solver* s, int which, int reps, double* ms, double* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEMGPU_H */

@@ -1,0 +1,171 @@
+"""The device solver against the oracle's FP64 direct solve (the reference's multifrontal
+Cholesky) and against the reference's PCG semantics and error texts."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import femahoy_b200 as fg
+import oracle
+from femahoy_b200 import meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(prob):
+    """The device matrix of the free unknowns, the right side, and the oracle's."""
+    kind = {"p1_heat": 0, "p1_elastic": 1, "p2_elastic": 2}[prob.kind]
+    K = fg.Csr.assemble(kind, prob.xyz, prob.nodes, prob.coef)
+    A = K.submatrix(prob.free)
+    rhs = fg.reduced_rhs(K, prob.load, prob.values, prob.free)
+    nodes = prob.nodes if kind == 0 else oracle.dof_elements(prob.nodes)
+    Ko = oracle.pattern(prob.n_unknowns, nodes)
+    Ko.assemble(kind, prob.xyz, prob.nodes, prob.coef)
+    Ao = Ko.submatrix(prob.free)
+    return A, rhs, Ao
+
+
+def _grid(prob):
+    planes, pts, comp = mg.grid_unknowns(prob)
+    return fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+
+
+def _rel(x, y):
+    return np.linalg.norm(x - y) / np.linalg.norm(y)
+
+
+def test_cantilever_fp64_pcg_multigrid():
+    """Config 1: P1 cantilever, 3,000 free unknowns, plain FP64 PCG + MG at 1e-10. The grid is at
+    the coarsest size, so the cycle is the coarse solve (multigrid.rs:94)."""
+    p = mg.cantilever_p1()
+    A, rhs, Ao = _system(p)
+    s = fg.Solver(A, _grid(p), fg.Method.Multigrid).with_tol(1e-10)
+    assert s.method() == fg.Method.Multigrid
+    assert s.levels() == [3000]
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    xd, _ = oracle.direct_solve(Ao, p.xyz[p.free // 3], rhs)
+    assert st.residual <= 1e-10
+    assert st.true_residual <= 1e-10
+    assert _rel(x, xd) <= 1e-8
+    assert 1 <= st.iterations <= 5
+
+
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_heat_multigrid_matches_direct(precision):
+    """Config 2's problem at 24^3: lognormal conductivity; |x - x_chol| / |x_chol| <= 1e-8."""
+    h = mg.heat_cube(24)
+    A, rhs, Ao = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision).with_tol(1e-10)
+    assert len(s.levels()) >= 2
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    xd, _ = oracle.direct_solve(Ao, h.xyz[h.free], rhs)
+    assert st.true_residual <= 1e-10
+    assert _rel(x, xd) <= 1e-8
+    assert st.iterations < 60
+
+
+def test_heat_oracle_pcg_agrees_at_tolerance():
+    """The reference's own PCG-MG (line Gauss-Seidel) and the device solve reach the same
+    temperatures at the same tolerance, within 1e-8 relative."""
+    h = mg.heat_cube(16)
+    A, rhs, Ao = _system(h)
+    planes, pts, comp = mg.grid_unknowns(h)
+    so = oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp, method="multigrid")
+    xo, _, _ = so.solve(rhs, tol=1e-10)
+    for precision in (fg.FP64, fg.MIXED):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision).with_tol(1e-10)
+        x = np.zeros(A.n)
+        s.solve(rhs, x)
+        assert _rel(x, xo) <= 1e-8
+
+
+def test_p2_p_multigrid_matches_direct():
+    """Config 3's problem on a 16 x 4 x 4 beam: p-multigrid P2 -> P1, then geometric levels."""
+    m = mg.box(16, 4, 4, (80.0, 20.0, 20.0))
+    q = fg.Quadratic.new(m.points, m.tets)
+    prob = mg.beam_p2(q.edges, q.tets, mesh=m)
+    A, rhs, Ao = _system(prob)
+    free = prob.free
+    P, coarse = fg.prolongation(prob.xyz, m.n, q.edges, free)
+    u = fg.Unknowns.Quadratic(prob.xyz[free // 3], P, coarse)
+    for precision in (fg.FP64, fg.MIXED):
+        s = fg.Solver(A, u, fg.Method.Multigrid, precision=precision, options=fg.Options(
+            precision=precision, coarsest=200)).with_tol(1e-10)
+        assert len(s.levels()) >= 3
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        xd, _ = oracle.direct_solve(Ao, prob.xyz[free // 3], rhs)
+        assert st.true_residual <= 1e-10
+        assert np.abs(x - xd).max() <= 1e-8 * np.abs(xd).max()
+
+
+def test_direct_method_matches_oracle():
+    h = mg.heat_cube(10)
+    A, rhs, Ao = _system(h)
+    s = fg.Solver(A, _grid(h))  # Crossover::Unknowns(3000) picks the direct solver
+    assert s.method() == fg.Method.Direct
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    xd, _ = oracle.direct_solve(Ao, h.xyz[h.free], rhs)
+    assert st.iterations == 0
+    assert st.residual < 1e-12
+    assert _rel(x, xd) < 1e-12
+
+
+def test_points_refuse_multigrid():
+    h = mg.heat_cube(4)
+    A, _, _ = _system(h)
+    with pytest.raises(fg.FemError, match="^multigrid needs the box grid"):
+        fg.Solver(A, fg.Unknowns.Points(h.xyz[h.free]), fg.Method.Multigrid)
+
+
+def test_not_converged_and_cancelled_texts():
+    """multigrid.rs:729-737 through the device loop."""
+    h = mg.heat_cube(16)
+    A, rhs, _ = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid).with_max_iter(1)
+    with pytest.raises(fg.FemError, match="^conjugate gradients did not converge: the residual is"):
+        s.solve(rhs, np.zeros(A.n))
+    s.with_max_iter(500)
+    flag = ctypes.c_int(1)
+    with pytest.raises(fg.FemError) as e:
+        s.solve(rhs, np.zeros(A.n), cancelled=flag)
+    assert str(e.value) == "cancelled" and e.value.code == 1
+
+
+def test_zero_right_side_gives_zero():
+    """multigrid.rs:704-711: |b| = 0 gives x = 0 and 0 iterations."""
+    h = mg.heat_cube(8)
+    A, _, _ = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid)
+    x = np.ones(A.n)
+    st = s.solve(np.zeros(A.n), x)
+    assert st.iterations == 0 and not x.any()
+
+
+def test_singular_matrix_is_not_positive_definite():
+    """cholesky.rs:547-560 on the direct path of the device."""
+    h = mg.heat_cube(4)
+    K = fg.Csr.assemble(fg.P1_HEAT, h.xyz, h.nodes, h.coef)  # no fixed points: singular
+    planes = h.mesh.planes
+    u = fg.Unknowns.Grid(fg.Level(planes, h.mesh.ijk, np.zeros(h.n_points, np.uint8)))
+    with pytest.raises(fg.FemError, match="not positive definite"):
+        fg.Solver(K, u, fg.Method.Direct)
+
+
+def test_solver_reuse_across_right_sides():
+    """A solver solves many right sides (solve.rs:1-5); the start value is honoured."""
+    h = mg.heat_cube(16)
+    A, rhs, Ao = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=fg.MIXED).with_tol(1e-10)
+    xs = []
+    for k in range(3):
+        x = np.zeros(A.n)
+        s.solve(rhs * (k + 1), x)
+        xs.append(x)
+    assert _rel(xs[1], 2 * xs[0]) < 1e-9 and _rel(xs[2], 3 * xs[0]) < 1e-9
+    x = xs[0].copy()
+    st = s.solve(rhs, x)
+    assert st.iterations == 0
