@@ -284,11 +284,13 @@ int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
             o.coarsest = options->coarsest > 0 ? options->coarsest : 3000;
             o.max_levels = options->max_levels > 0 ? options->max_levels : 30;
             o.graph = options->graph != 2;
+            o.format = options->format;
         }
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,
                 "the SELL chunk height must be 8, 16 or 32");
         require(o.degree >= 0 && o.degree <= 16, "the Chebyshev degree must be 1 to 16");
+        require(o.format == 0 || o.format == 1, "the format is 0 (stencil where possible) or 1");
         int64_t n = a->m.n;
         if (u->kind == FEMGPU_UNKNOWNS_GRID) {
             require(u->points && u->comp, "a grid level needs its points and components");

@@ -116,6 +116,38 @@ bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* pout, HostLevel*
     return true;
 }
 
+void renumber_grid_order(HostRect* p, HostLevel* lv) {
+    size_t n = lv->points.size();
+    std::vector<uint32_t> order(n);
+    for (size_t k = 0; k < n; ++k) order[k] = (uint32_t)k;
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        const auto &pa = lv->points[a], &pb = lv->points[b];
+        return std::make_tuple(pa[2], pa[1], pa[0], lv->comp[a]) <
+               std::make_tuple(pb[2], pb[1], pb[0], lv->comp[b]);
+    });
+    std::vector<uint32_t> fresh(n);
+    for (size_t q = 0; q < n; ++q) fresh[order[q]] = (uint32_t)q;
+    std::vector<std::array<uint32_t, 3>> pts(n);
+    std::vector<uint8_t> comp(n);
+    for (size_t q = 0; q < n; ++q) {
+        pts[q] = lv->points[order[q]];
+        comp[q] = lv->comp[order[q]];
+    }
+    lv->points = std::move(pts);
+    lv->comp = std::move(comp);
+    std::vector<std::pair<uint32_t, double>> row;
+    for (int64_t i = 0; i < p->rows; ++i) {
+        row.clear();
+        for (int64_t k = p->ptr[i]; k < p->ptr[i + 1]; ++k) row.push_back({fresh[p->idx[k]], p->val[k]});
+        std::sort(row.begin(), row.end(),
+                  [](const auto& s, const auto& t) { return s.first < t.first; });
+        for (size_t k = 0; k < row.size(); ++k) {
+            p->idx[p->ptr[i] + k] = row[k].first;
+            p->val[p->ptr[i] + k] = row[k].second;
+        }
+    }
+}
+
 HostCsr galerkin(const HostRect& P, const HostCsr& a, int threads) {
     int64_t nc = P.cols;
     // The transpose of P, row by row, by a counting sort (fine rows in increasing order).

@@ -33,6 +33,12 @@ struct HostLevel {
 // multigrid.rs:329-452: false when no axis has more than 2 planes.
 bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* p, HostLevel* coarse);
 
+// Renumbers the coarse unknowns of `coarse` in grid order (z, then y, then x, then the
+// component) and the columns of `p` with them. The Galerkin matrix of the renumbered P is the
+// same matrix with its rows and columns permuted; in grid order the entries of a box level sit
+// at constant offsets, which the stencil format needs.
+void renumber_grid_order(HostRect* p, HostLevel* coarse);
+
 // sparse.rs:233-292, each coarse row exactly as the reference forms it; rows shared among
 // `threads` host threads.
 HostCsr galerkin(const HostRect& p, const HostCsr& a, int threads);

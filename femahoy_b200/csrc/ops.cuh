@@ -1,0 +1,59 @@
+// The operators of a level, as seen by the kernels: SELL-C (any sparse matrix) or a symmetric
+// stencil (a matrix whose entries sit at a few constant column offsets, as the operators of a
+// box grid in grid order do).
+//
+// Stencil layout: offsets 0 = o_0 < o_1 < ... < o_{K-1}; coef[k n + i] = a(i, i + o_k), 0 where
+// the matrix has no such entry. Row i is then
+//   sum_k coef[k][i] x[i + o_k] + sum_{k >= 1} coef[k][i - o_k] x[i - o_k],
+// the lower entries taken from the rows above (the matrix is symmetric). The columns are
+// implicit: a row reads K coefficients of its own, K - 1 of earlier rows (recently read by
+// other threads, so from L2) and 2K - 1 entries of x; no index is stored.
+#pragma once
+#include "sell.cuh"
+
+namespace femgpu {
+
+constexpr int MAXK = 32;
+
+template <class T>
+struct StencilView {
+    int64_t n;
+    int K;
+    int64_t off[MAXK];
+    const T* __restrict__ coef;
+};
+
+template <class T>
+struct SellOp {
+    SellView<T> v;
+    __device__ __forceinline__ int64_t threads() const { return v.nslices * v.C; }
+    __device__ __forceinline__ bool valid(int64_t g) const { return g < v.n; }
+    template <class TA, class TX>
+    __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
+        return sell_row<T, TX, TA>(v, g / v.C, (int)(g % v.C), x);
+    }
+};
+
+template <class T>
+struct StencilOp {
+    StencilView<T> v;
+    __device__ __forceinline__ int64_t threads() const { return v.n; }
+    __device__ __forceinline__ bool valid(int64_t) const { return true; }
+    template <class TA, class TX>
+    __device__ __forceinline__ TA apply(int64_t i, const TX* __restrict__ x) const {
+        const int64_t n = v.n;
+        const T* __restrict__ c = v.coef;
+        TA acc = (TA)__ldg(c + i) * (TA)__ldg(x + i);
+        for (int k = 1; k < v.K; ++k) {
+            int64_t o = v.off[k];
+            const T* ck = c + k * n;
+            int64_t j = i + o;
+            if (j < n) acc += (TA)__ldg(ck + i) * (TA)__ldg(x + j);
+            int64_t m = i - o;
+            if (m >= 0) acc += (TA)__ldg(ck + m) * (TA)__ldg(x + m);
+        }
+        return acc;
+    }
+};
+
+}  // namespace femgpu

@@ -88,6 +88,75 @@ void make_sell(const DevCsr& a, int C, Sell<T>* out, cudaStream_t s) {
 template void make_sell<double>(const DevCsr&, int, Sell<double>*, cudaStream_t);
 template void make_sell<float>(const DevCsr&, int, Sell<float>*, cudaStream_t);
 
+// The stencil of a symmetric matrix whose entries sit at a few constant offsets col - row:
+// coef[k n + i] = a(i, i + o_k) for the offsets o_k >= 0. Refused (false) when there are more
+// than MAXK such offsets, or when the slots would hold more than 1.5 times the upper entries.
+template <class T>
+static bool make_stencil(const HostCsr& h, Operator<T>* out, cudaStream_t s) {
+    int64_t n = h.n;
+    std::vector<int64_t> offs;
+    offs.reserve(64);
+    int64_t upper = 0;
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) {
+            int64_t o = (int64_t)h.idx[k] - i;
+            if (o < 0) continue;
+            ++upper;
+            if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
+                offs.push_back(o);
+                if ((int)offs.size() > MAXK) return false;
+            }
+        }
+    std::sort(offs.begin(), offs.end());
+    if (offs.empty() || offs[0] != 0) return false;
+    // A symmetric pattern has as many entries below the diagonal as above it.
+    int64_t diag = 0;
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) diag += (int64_t)h.idx[k] == i;
+    if (h.nnz() - upper != upper - diag) return false;
+    int K = (int)offs.size();
+    if ((double)K * n > 1.5 * (double)upper) return false;
+    std::vector<T> coef((size_t)K * n, (T)0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) {
+            int64_t o = (int64_t)h.idx[k] - i;
+            if (o < 0) continue;
+            int slot = (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
+            coef[(size_t)slot * n + i] = (T)h.val[k];
+        }
+    out->stencil = true;
+    out->n = n;
+    out->nnz = h.nnz();
+    out->K = K;
+    out->off = offs;
+    out->coef.upload(coef.data(), coef.size(), s);
+    FG_CUDA(cudaStreamSynchronize(s));
+    return true;
+}
+
+template <class T>
+void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operator<T>* out,
+                   cudaStream_t s) {
+    if (allow && make_stencil<T>(h, out, s)) return;
+    out->stencil = false;
+    out->n = d.n;
+    out->nnz = d.nnz;
+    make_sell<T>(d, C, &out->sell, s);
+}
+template void make_operator<double>(const HostCsr&, const DevCsr&, int, bool, Operator<double>*,
+                                    cudaStream_t);
+template void make_operator<float>(const HostCsr&, const DevCsr&, int, bool, Operator<float>*,
+                                   cudaStream_t);
+
+// Calls f with the kernel-side view of the operator.
+template <class T, class F>
+static void with_op(const Operator<T>& op, F&& f) {
+    if (op.stencil)
+        f(StencilOp<T>{op.sview()});
+    else
+        f(SellOp<T>{op.sell.view()});
+}
+
 // ------------------------------------------------------------------ V-cycle kernels
 #define GRID_STRIDE(i, n)                                                     \
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (n); \
@@ -106,15 +175,15 @@ __global__ void k_cheb_first(int64_t n, const T* __restrict__ b, const T* __rest
 }
 
 // A Chebyshev step: r = b - A x_in, d = c2 d + c1 D^-1 r, x_out = x_in + d.
-template <class T>
+template <class T, class Op>
 __global__ void __launch_bounds__(TH)
-    k_cheb_step(SellView<T> A, const T* __restrict__ b, const T* __restrict__ xin,
+    k_cheb_step(Op A, const T* __restrict__ b, const T* __restrict__ xin,
                 const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d, T* __restrict__ xout,
                 const int* __restrict__ done) {
     if (*done) return;
-    GRID_STRIDE(g, A.nslices * A.C) {
-        T ax = sell_row<T, T, T>(A, g / A.C, (int)(g % A.C), xin);
-        if (g < A.n) {
+    GRID_STRIDE(g, A.threads()) {
+        T ax = A.template apply<T>(g, xin);
+        if (A.valid(g)) {
             T r = b[g] - ax;
             T dd = c2 * d[g] + c1 * dinv[g] * r;
             d[g] = dd;
@@ -124,14 +193,14 @@ __global__ void __launch_bounds__(TH)
 }
 
 // r = b - A x
-template <class T>
+template <class T, class Op>
 __global__ void __launch_bounds__(TH)
-    k_residual(SellView<T> A, const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r,
+    k_residual(Op A, const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r,
                const int* __restrict__ done) {
     if (*done) return;
-    GRID_STRIDE(g, A.nslices * A.C) {
-        T ax = sell_row<T, T, T>(A, g / A.C, (int)(g % A.C), x);
-        if (g < A.n) r[g] = b[g] - ax;
+    GRID_STRIDE(g, A.threads()) {
+        T ax = A.template apply<T>(g, x);
+        if (A.valid(g)) r[g] = b[g] - ax;
     }
 }
 
@@ -201,14 +270,15 @@ struct FinResidual0 {
 };
 
 // r = b - A x, with b.b and r.r; also the FP32 copy of r (mixed form).
+template <class Op>
 __global__ void __launch_bounds__(TH)
-    k_pcg_residual(SellView<double> A, const double* __restrict__ b, const double* __restrict__ x,
+    k_pcg_residual(Op A, const double* __restrict__ b, const double* __restrict__ x,
                    double* __restrict__ r, float* __restrict__ r32, double* partial,
                    unsigned* counter, Scalars* sc) {
     double bb = 0, rr = 0;
-    GRID_STRIDE(g, A.nslices * A.C) {
-        double ax = sell_row<double, double, double>(A, g / A.C, (int)(g % A.C), x);
-        if (g < A.n) {
+    GRID_STRIDE(g, A.threads()) {
+        double ax = A.template apply<double>(g, x);
+        if (A.valid(g)) {
             double bi = b[g], ri = bi - ax;
             r[g] = ri;
             if (r32) r32[g] = (float)ri;
@@ -228,14 +298,15 @@ struct FinPq {
 };
 
 // q = A p with p.q and alpha = rz / p.q (multigrid.rs:740-741).
+template <class Op>
 __global__ void __launch_bounds__(TH)
-    k_pcg_spmv_pq(SellView<double> A, const double* __restrict__ p, double* __restrict__ q,
+    k_pcg_spmv_pq(Op A, const double* __restrict__ p, double* __restrict__ q,
                   double* partial, unsigned* counter, Scalars* sc) {
     if (sc->done) return;
     double pq = 0;
-    GRID_STRIDE(g, A.nslices * A.C) {
-        double ap = sell_row<double, double, double>(A, g / A.C, (int)(g % A.C), p);
-        if (g < A.n) {
+    GRID_STRIDE(g, A.threads()) {
+        double ap = A.template apply<double>(g, p);
+        if (A.valid(g)) {
             q[g] = ap;
             pq += p[g] * ap;
         }
@@ -324,13 +395,14 @@ struct FinTwo {
 };
 
 // w = D^-1 A v; sums v.Av and v.Dv (the Rayleigh quotient of D^-1 A in the D inner product).
+template <class Op>
 __global__ void __launch_bounds__(TH)
-    k_power_step(SellView<double> A, const double* __restrict__ v, const double* __restrict__ dg,
+    k_power_step(Op A, const double* __restrict__ v, const double* __restrict__ dg,
                  double* __restrict__ w, double* partial, unsigned* counter, double* out) {
     double vav = 0, vdv = 0;
-    GRID_STRIDE(g, A.nslices * A.C) {
-        double av = sell_row<double, double, double>(A, g / A.C, (int)(g % A.C), v);
-        if (g < A.n) {
+    GRID_STRIDE(g, A.threads()) {
+        double av = A.template apply<double>(g, v);
+        if (A.valid(g)) {
             vav += v[g] * av;
             vdv += v[g] * dg[g] * v[g];
             w[g] = av / dg[g];
@@ -592,7 +664,7 @@ static void upload_values(const std::vector<double>& v, DevBuf<T>* d, cudaStream
 }
 
 // lambda_max of D^-1 A by the power method in the D inner product (15 steps), on the device.
-static double lambda_max(const Sell<double>& A, const double* dg, cudaStream_t s,
+static double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
                          DevBuf<double>& partial, DevBuf<unsigned>& counter) {
     int64_t n = A.n;
     // out[0..1]: v.Av and v.Dv of this step; out[2..3]: |w|^2 (and an unused 0).
@@ -600,8 +672,9 @@ static double lambda_max(const Sell<double>& A, const double* dg, cudaStream_t s
     k_seed<<<blocks_for(n, TH), TH, 0, s>>>(n, v.p);
     double lam = 0;
     for (int it = 0; it < 15; ++it) {
-        k_power_step<<<RED_BLOCKS, TH, 0, s>>>(A.view(), v.p, dg, w.p, partial.p, counter.p,
-                                                 out.p);
+        with_op(A, [&](auto op) {
+            k_power_step<<<RED_BLOCKS, TH, 0, s>>>(op, v.p, dg, w.p, partial.p, counter.p, out.p);
+        });
         k_norm2<<<RED_BLOCKS, TH, 0, s>>>(n, w.p, partial.p, counter.p, out.p + 2);
         k_scale_into<<<blocks_for(n, TH), TH, 0, s>>>(n, w.p, out.p + 2, v.p);
         FG_CHECK_LAUNCH();
@@ -670,7 +743,7 @@ size_t Hierarchy<T>::bytes() const {
 }
 
 size_t SolverImpl::bytes() const {
-    return A64_.bytes() + a_.ptr.bytes() + a_.idx.bytes() + a_.val.bytes() + H64_.bytes() +
+    return A64_.bytes() + op64_.bytes() + a_.ptr.bytes() + a_.idx.bytes() + a_.val.bytes() + H64_.bytes() +
            H32_.bytes() + dense_inv_.bytes() + 7 * n_ * sizeof(double) + r32_.bytes();
 }
 
@@ -722,6 +795,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         sizes_ = {n_};
         return;
     }
+    make_operator<double>(h, a_, C, opt_.format == 0, &op64_, s_);
     if (u.kind == FEMGPU_UNKNOWNS_GRID) {
         HostLevel lv;
         for (int d = 0; d < 3; ++d) lv.planes[d].assign(u.planes[d], u.planes[d] + u.nplanes[d]);
@@ -765,7 +839,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         lv.nnz = mats[l].nnz();
         DevCsr d;
         upload_csr(mats[l], &d, s_);
-        make_sell<T>(d, C, &lv.A, s_);
+        make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
         // The diagonal and lambda_max(D^-1 A) in FP64.
         DevBuf<double> dg(lv.n);
         DevBuf<int> bad(1);
@@ -777,12 +851,12 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
             throw Failure(FEMGPU_ERR_NOT_SPD,
                           "the matrix is not positive definite: it has a diagonal entry that is "
                           "not above 0");
-        Sell<double> a64;
-        const Sell<double>* ap = nullptr;
+        Operator<double> a64;
+        const Operator<double>* ap = nullptr;
         if (l == 0) {
-            ap = &A64_;
+            ap = &op64_;
         } else {
-            make_sell<double>(d, C, &a64, s_);
+            make_operator<double>(mats[l], d, C, opt_.format == 0, &a64, s_);
             ap = &a64;
         }
         lv.lambda = lambda_max(*ap, dg.p, s_, partial_, counter_);
@@ -849,6 +923,7 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
         HostLevel coarse;
         if (!coarsen(level, a, &p, &coarse)) break;
         if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
+        if (opt_.format == 0) renumber_grid_order(&p, &coarse);
         HostCsr ac = galerkin(p, a, threads);
         mats.push_back(std::move(ac));
         ps.push_back(std::move(p));
@@ -880,17 +955,19 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     MgLevel<T>& L = H.levels[l];
     int64_t n = L.n;
     int gb = blocks_for(n, TH, NUM_SMS * 8);
-    int gs = blocks_for(L.A.nslices * L.A.C, TH, NUM_SMS * 8);
+    int gs = blocks_for(L.A.threads(), TH, NUM_SMS * 8);
     T* xa = L.xa.p;
     T* xb = L.xb.p;
     int deg = (int)L.c1.size();
     k_cheb_first<T><<<gb, TH, 0, s_>>>(n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
     for (int k = 1; k < deg; ++k) {
-        k_cheb_step<T><<<gs, TH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k],
-                                          L.d.p, xb, done);
+        with_op(L.A, [&](auto op) {
+            k_cheb_step<T><<<gs, TH, 0, s_>>>(op, b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k], L.d.p,
+                                              xb, done);
+        });
         std::swap(xa, xb);
     }
-    k_residual<T><<<gs, TH, 0, s_>>>(L.A.view(), b, xa, L.r.p, done);
+    with_op(L.A, [&](auto op) { k_residual<T><<<gs, TH, 0, s_>>>(op, b, xa, L.r.p, done); });
     T* bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
     k_restrict<T><<<blocks_for(L.nc, TH, NUM_SMS * 8), TH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p,
                                                                      L.rval.p, L.r.p, bc, done);
@@ -899,8 +976,10 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     const T* ec = enqueue_vcycle(H, l + 1, bc);
     k_prolong<T><<<gb, TH, 0, s_>>>(n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
     for (int k = 0; k < deg; ++k) {
-        k_cheb_step<T><<<gs, TH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k],
-                                          L.d.p, xb, done);
+        with_op(L.A, [&](auto op) {
+            k_cheb_step<T><<<gs, TH, 0, s_>>>(op, b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k], L.d.p,
+                                              xb, done);
+        });
         std::swap(xa, xb);
     }
     FG_CHECK_LAUNCH();
@@ -911,11 +990,11 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
 void SolverImpl::enqueue_iteration() {
     int64_t n = n_;
     launches_ += 4;
-    int gs = blocks_for(A64_.nslices * A64_.C, TH, RED_BLOCKS);
-    (void)gs;
     Scalars* sc = sc_.p;
     bool mixed = opt_.precision == FEMGPU_MIXED;
-    k_pcg_spmv_pq<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), p_.p, q_.p, partial_.p, counter_.p, sc);
+    with_op(op64_, [&](auto op) {
+        k_pcg_spmv_pq<<<RED_BLOCKS, TH, 0, s_>>>(op, p_.p, q_.p, partial_.p, counter_.p, sc);
+    });
     k_pcg_update<<<RED_BLOCKS, TH, 0, s_>>>(n, x_.p, r_.p, p_.p, q_.p, mixed ? r32_.p : nullptr,
                                             partial_.p, counter_.p, sc, tol);
     FG_CHECK_LAUNCH();
@@ -966,14 +1045,14 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         // residual.
         k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, dense_inv_.p, b_.p, x_.p,
                                                               done_zero_.p);
-        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p, nullptr,
-                                                  partial_.p, counter_.p, sc_.p);
+        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p,
+                                                  nullptr, partial_.p, counter_.p, sc_.p);
         k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, dense_inv_.p, r_.p, t_.p,
                                                               done_zero_.p);
         k_add<<<blocks_for(n, TH), TH, 0, s_>>>(n, t_.p, x_.p);
         FG_CHECK_LAUNCH();
-        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p, nullptr,
-                                                  partial_.p, counter_.p, sc_.p);
+        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p,
+                                                  nullptr, partial_.p, counter_.p, sc_.p);
         FG_CHECK_LAUNCH();
         FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
         FG_CUDA(cudaMemcpyAsync(d_x, x_.p, n * 8, cudaMemcpyDeviceToDevice, s_));
@@ -992,9 +1071,10 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
     }
     // multigrid.rs:692-753
     FG_CUDA(cudaMemcpyAsync(x_.p, d_x, n * 8, cudaMemcpyDeviceToDevice, s_));
-    k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p,
-                                              mixed ? r32_.p : nullptr, partial_.p, counter_.p,
-                                              sc_.p);
+    with_op(op64_, [&](auto op) {
+        k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(op, b_.p, x_.p, r_.p, mixed ? r32_.p : nullptr,
+                                                  partial_.p, counter_.p, sc_.p);
+    });
     FG_CHECK_LAUNCH();
     launches_ += 3;  // this residual, and r.z and p = z after the first cycle
     FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
@@ -1038,8 +1118,9 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         if (residual <= tol) {
             // The true residual in FP64; with an FP32 preconditioner the recurrence can drift
             // from it, and then the solve restarts from x (iterative refinement).
-            k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, t_.p, nullptr,
-                                                      partial_.p, counter_.p, sc_.p);
+            k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(SellOp<double>{A64_.view()}, b_.p, x_.p,
+                                                      t_.p, nullptr, partial_.p, counter_.p,
+                                                      sc_.p);
             FG_CHECK_LAUNCH();
             launches_ += 1;
             FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
@@ -1049,8 +1130,9 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
             if (truth <= tol || !mixed || restarts >= 3 || it >= max_iter) break;
             ++restarts;
             FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
-            k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), b_.p, x_.p, r_.p, r32_.p,
-                                                      partial_.p, counter_.p, sc_.p);
+            k_pcg_residual<<<RED_BLOCKS, TH, 0, s_>>>(SellOp<double>{A64_.view()}, b_.p, x_.p,
+                                                      r_.p, r32_.p, partial_.p, counter_.p,
+                                                      sc_.p);
             zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
             k_pcg_dots<float><<<RED_BLOCKS, TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 1, partial_.p,
                                                          counter_.p, sc_.p);
@@ -1110,18 +1192,24 @@ void SolverImpl::kernel_time(int which, int reps, double* ms, double* bytes) {
     FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
     auto launch = [&]() {
         if (which == 1) {
-            k_pcg_spmv_pq<<<RED_BLOCKS, TH, 0, s_>>>(A64_.view(), p_.p, q_.p, partial_.p,
-                                                     counter_.p, sc_.p);
+            with_op(op64_, [&](auto op) {
+                k_pcg_spmv_pq<<<RED_BLOCKS, TH, 0, s_>>>(op, p_.p, q_.p, partial_.p, counter_.p,
+                                                         sc_.p);
+            });
         } else if (mixed) {
             MgLevel<float>& L = H32_.levels.at(0);
-            int gs = blocks_for(L.A.nslices * L.A.C, TH, NUM_SMS * 8);
-            k_cheb_step<float><<<gs, TH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p, 0.5f,
-                                                  0.5f, L.d.p, L.xb.p, done_zero_.p);
+            int gs = blocks_for(L.A.threads(), TH, NUM_SMS * 8);
+            with_op(L.A, [&](auto op) {
+                k_cheb_step<float><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5f, 0.5f,
+                                                      L.d.p, L.xb.p, done_zero_.p);
+            });
         } else {
             MgLevel<double>& L = H64_.levels.at(0);
-            int gs = blocks_for(L.A.nslices * L.A.C, TH, NUM_SMS * 8);
-            k_cheb_step<double><<<gs, TH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p, 0.5, 0.5,
-                                                   L.d.p, L.xb.p, done_zero_.p);
+            int gs = blocks_for(L.A.threads(), TH, NUM_SMS * 8);
+            with_op(L.A, [&](auto op) {
+                k_cheb_step<double><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5, 0.5,
+                                                       L.d.p, L.xb.p, done_zero_.p);
+            });
         }
     };
     if (which == 0 && (mixed ? H32_.levels.empty() : H64_.levels.empty()))
@@ -1147,14 +1235,16 @@ void SolverImpl::kernel_time(int which, int reps, double* ms, double* bytes) {
     float t = 0;
     FG_CUDA(cudaEventElapsedTime(&t, ev0_, ev1_));
     *ms = t / reps;
+    // A smoothing step streams the operator, x, y and 4 more vectors (b, D^-1, d read and
+    // written); the PCG product the operator, p and q.
     if (which == 1) {
-        *bytes = (double)a_.nnz * 12.0 + 2.0 * (double)n_ * 8.0;
+        *bytes = op64_.stream_bytes();
     } else if (mixed) {
         auto& L = H32_.levels[0];
-        *bytes = (double)L.nnz * 8.0 + 6.0 * (double)L.n * 4.0;
+        *bytes = L.A.stream_bytes() + 4.0 * (double)L.n * sizeof(float);
     } else {
         auto& L = H64_.levels[0];
-        *bytes = (double)L.nnz * 12.0 + 6.0 * (double)L.n * 8.0;
+        *bytes = L.A.stream_bytes() + 4.0 * (double)L.n * sizeof(double);
     }
 }
 

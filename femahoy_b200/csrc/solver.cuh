@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "hierarchy.hpp"
+#include "ops.cuh"
 #include "sell.cuh"
 
 namespace femgpu {
@@ -26,6 +27,40 @@ struct Sell {
 template <class T>
 void make_sell(const DevCsr& a, int C, Sell<T>* out, cudaStream_t s);
 
+// The operator of a level: a symmetric stencil when the level's entries sit at a few constant
+// column offsets (the operators of a box grid in grid order), else SELL-C.
+template <class T>
+struct Operator {
+    bool stencil = false;
+    int64_t n = 0, nnz = 0;
+    Sell<T> sell;
+    int K = 0;
+    std::vector<int64_t> off;
+    DevBuf<T> coef;
+    int64_t threads() const { return stencil ? n : sell.nslices * sell.C; }
+    StencilView<T> sview() const {
+        StencilView<T> v{};
+        v.n = n;
+        v.K = K;
+        for (int k = 0; k < K; ++k) v.off[k] = off[k];
+        v.coef = coef.p;
+        return v;
+    }
+    size_t bytes() const { return sell.bytes() + coef.bytes(); }
+    // The bytes one product reads and writes, each value once: the stored coefficients (and
+    // indices), x and y.
+    double stream_bytes() const {
+        if (stencil) return (double)K * n * sizeof(T) + 2.0 * n * sizeof(T);
+        return (double)nnz * (sizeof(T) + 4) + 2.0 * n * sizeof(T);
+    }
+};
+
+// The operator of the host matrix `h` (also on the device as `d`): a stencil if `allow` and
+// the offsets fit, else SELL-C.
+template <class T>
+void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operator<T>* out,
+                   cudaStream_t s);
+
 // The scalars of a PCG solve, in device memory.
 struct Scalars {
     double bb, rr, rz, pq, alpha, beta, zq, norm_b;
@@ -35,7 +70,7 @@ struct Scalars {
 template <class T>
 struct MgLevel {
     int64_t n = 0, nnz = 0;
-    Sell<T> A;
+    Operator<T> A;
     DevBuf<T> dinv;
     // The prolongation P from the next level, and R = P^T (gather form of the restriction).
     int64_t nc = 0;
@@ -61,6 +96,7 @@ struct Options {
     int degree = 0;
     double lower = 0;
     int sell_c = 0;
+    int format = 0;  // 0: stencil where possible, else SELL; 1: SELL only
     int coarsest = 3000;
     int max_levels = 30;
     bool graph = true;
@@ -99,7 +135,8 @@ class SolverImpl {
     Options opt_;
     bool direct_ = false;
     int64_t n_ = 0;
-    Sell<double> A64_;
+    Sell<double> A64_;          // the matrix exactly (the true residual, the direct method)
+    Operator<double> op64_;     // the FP64 operator of PCG
     DevCsr a_;  // the matrix, FP64 CSR
     Hierarchy<double> H64_;
     Hierarchy<float> H32_;

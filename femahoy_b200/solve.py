@@ -95,6 +95,7 @@ class Stats:
     residual: float
     true_residual: float = 0.0
     seconds: float = 0.0
+    launches: int = 0
 
 
 @dataclass
@@ -108,10 +109,11 @@ class Options:
     coarsest: int = 0
     max_levels: int = 0
     graph: int = 0
+    format: int = 0  # 0: stencil where the level allows it, else SELL-C; 1: SELL-C only
 
     def _c(self):
         return L.Options_t(self.precision, self.degree, self.lower, self.sell_c, 0, self.coarsest,
-                           self.max_levels, self.graph)
+                           self.max_levels, self.graph, self.format)
 
 
 class Solver:
@@ -212,7 +214,7 @@ class Solver:
             flag = C.byref(C.c_int(1))
         st = L.Stats_t()
         L.check(L.lib().femgpu_solver_solve(self._h, L.ptr(b), L.ptr(x), flag, C.byref(st)))
-        return Stats(st.iterations, st.residual, st.true_residual, st.seconds)
+        return Stats(st.iterations, st.residual, st.true_residual, st.seconds, st.launches)
 
     def solve_device(self, b_ptr: int, x_ptr: int, cancel=None) -> Stats:
         """The same on device vectors (raw CUDA pointers, e.g. torch ``data_ptr()``)."""
@@ -220,7 +222,7 @@ class Solver:
         flag = C.byref(cancel) if isinstance(cancel, C.c_int) else None
         L.check(L.lib().femgpu_solver_solve_device(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr),
                                                    flag, C.byref(st)))
-        return Stats(st.iterations, st.residual, st.true_residual, st.seconds)
+        return Stats(st.iterations, st.residual, st.true_residual, st.seconds, st.launches)
 
 
 def prolongation(points, corners, edges, free):

@@ -168,6 +168,9 @@ typedef struct femgpu_options {
     int coarsest;         /* the largest level that the dense coarse solve takes; 0 = 3000 */
     int max_levels;       /* 0 = 30 (multigrid.rs:94) */
     int graph;            /* 1 = replay each PCG iteration as a CUDA graph (default), 2 = off */
+    int format;           /* 0 = a symmetric stencil for each level whose entries sit at a few
+                             constant column offsets (box grids in grid order), SELL-C for the
+                             others; 1 = SELL-C for every level */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end
