@@ -41,7 +41,7 @@ UNIT = "DOF-solves/s"
 def args():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cells", type=int, default=N_CELLS)
@@ -74,7 +74,7 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.file,
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.file,
                 stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None

@@ -345,6 +345,17 @@ int femgpu_solver_levels(const femgpu_solver* s, size_t* sizes, int cap) {
 
 size_t femgpu_solver_bytes(const femgpu_solver* s) { return s ? s->impl.bytes() : 0; }
 
+size_t femgpu_solver_describe(const femgpu_solver* s, char* buf, size_t len) {
+    if (!s) return 0;
+    std::string d = s->impl.describe();
+    if (buf && len) {
+        size_t k = std::min(len - 1, d.size());
+        std::memcpy(buf, d.data(), k);
+        buf[k] = 0;
+    }
+    return d.size();
+}
+
 int femgpu_solver_solve(femgpu_solver* s, const double* b, double* x, const volatile int* cancel,
                         femgpu_stats* stats) {
     return guarded([&] {

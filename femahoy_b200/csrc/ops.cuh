@@ -56,4 +56,36 @@ struct StencilOp {
     }
 };
 
+// The same with K known at compile time: the K own coefficients, the K - 1 coefficients of the
+// rows above and the 2K - 1 entries of x are all loaded before the first product, so a thread
+// has 4K - 2 independent loads in flight (the runtime-K loop issues them 4 at a time). Loads
+// past either end are predicated off and count 0.
+template <class T, int K>
+struct StencilOpK {
+    StencilView<T> v;
+    __device__ __forceinline__ int64_t threads() const { return v.n; }
+    __device__ __forceinline__ bool valid(int64_t) const { return true; }
+    template <class TA, class TX>
+    __device__ __forceinline__ TA apply(int64_t i, const TX* __restrict__ x) const {
+        const int64_t n = v.n;
+        const T* __restrict__ c = v.coef;
+        T cu[K], cl[K];
+        TX xu[K], xl[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int64_t o = v.off[k];
+            const int64_t j = i + o, m = i - o;
+            cu[k] = __ldg(c + k * n + i);
+            xu[k] = j < n ? __ldg(x + j) : (TX)0;
+            const bool low = k > 0 && m >= 0;
+            cl[k] = low ? __ldg(c + k * n + m) : (T)0;
+            xl[k] = low ? __ldg(x + m) : (TX)0;
+        }
+        TA acc = 0;
+#pragma unroll
+        for (int k = 0; k < K; ++k) acc += (TA)cu[k] * (TA)xu[k] + (TA)cl[k] * (TA)xl[k];
+        return acc;
+    }
+};
+
 }  // namespace femgpu

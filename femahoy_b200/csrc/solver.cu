@@ -14,7 +14,10 @@
 // level is solved by its inverse, formed on the device from a dense Cholesky factor.
 #include <algorithm>
 #include <cmath>
+#include <atomic>
+#include <chrono>
 #include <cstring>
+#include <thread>
 #include <type_traits>
 
 #include "assemble.cuh"
@@ -149,13 +152,20 @@ template void make_operator<float>(const HostCsr&, const DevCsr&, int, bool, Ope
                                    cudaStream_t);
 
 // Calls f with the kernel-side view of the operator.
+// The stencils of the box-grid hierarchies have K = 8 (the finest P1 level: the 15-point Kuhn
+// stencil) and K = 14 (Galerkin levels: 27 points); these get unrolled kernels.
 template <class T, class F>
 static void with_op(const Operator<T>& op, F&& f) {
-    if (op.stencil)
-        f(StencilOp<T>{op.sview()});
-    else
+    if (!op.stencil)
         f(SellOp<T>{op.sell.view()});
+    else if (op.unrolled && op.K == 8)
+        f(StencilOpK<T, 8>{op.sview()});
+    else if (op.unrolled && op.K == 14)
+        f(StencilOpK<T, 14>{op.sview()});
+    else
+        f(StencilOp<T>{op.sview()});
 }
+
 
 // ------------------------------------------------------------------ V-cycle kernels
 #define GRID_STRIDE(i, n)                                                     \
@@ -242,8 +252,16 @@ __global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__
     int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = w; i < n; i += nw) {
         const T* row = M + i * n;
-        T s = 0;
-        for (int64_t k = lane; k < n; k += 32) s += row[k] * __ldg(b + k);
+        T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        int64_t k = lane;
+        for (; k + 96 < n; k += 128) {
+            s0 += row[k] * __ldg(b + k);
+            s1 += row[k + 32] * __ldg(b + k + 32);
+            s2 += row[k + 64] * __ldg(b + k + 64);
+            s3 += row[k + 96] * __ldg(b + k + 96);
+        }
+        for (; k < n; k += 32) s0 += row[k] * __ldg(b + k);
+        T s = (s0 + s1) + (s2 + s3);
         for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) x[i] = s;
     }
@@ -383,6 +401,16 @@ __global__ void k_pcg_p(int64_t n, const TZ* __restrict__ z, double* __restrict_
     if (sc->done) return;
     double beta = sc->beta;
     GRID_STRIDE(i, n) p[i] = init ? (double)z[i] : (double)z[i] + beta * p[i];
+}
+
+// The end of a device-side PCG iteration: continue unless the solve converged, reached its
+// iteration limit, broke down (a NaN residual) or was cancelled (multigrid.rs:721-738, in the
+// same order of tests).
+__global__ void k_loop_control(cudaGraphConditionalHandle h, const Scalars* sc,
+                               const volatile int* cancel) {
+    double rr = sc->rr;
+    bool go = !sc->done && sc->iters < sc->max_iter && rr == rr && !*cancel;
+    cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
 // ------------------------------------------------------------------ power iteration
@@ -663,6 +691,42 @@ static void upload_values(const std::vector<double>& v, DevBuf<T>* d, cudaStream
     FG_CUDA(cudaStreamSynchronize(s));
 }
 
+// The autotuner's choice for a stencil operator: times y = b - A x with the runtime-K and the
+// compile-time-K kernels (5 launches each after 2 warm-up launches, CUDA events) and keeps the
+// faster. The choice depends on the level's size and on how the L2 serves its offsets.
+template <class T>
+static void tune_operator(Operator<T>* op, cudaStream_t s) {
+    if (!op->stencil || (op->K != 8 && op->K != 14)) return;
+    int64_t n = op->n;
+    DevBuf<T> x(n), b(n), r(n);
+    x.zero(s);
+    b.zero(s);
+    DevBuf<int> done(1);
+    done.zero(s);
+    cudaEvent_t e0, e1;
+    FG_CUDA(cudaEventCreate(&e0));
+    FG_CUDA(cudaEventCreate(&e1));
+    int gs = blocks_for(n, TH, NUM_SMS * 8);
+    for (int variant = 0; variant < 2; ++variant) {
+        op->unrolled = variant == 1;
+        auto launch = [&] {
+            with_op(*op, [&](auto o) { k_residual<T><<<gs, TH, 0, s>>>(o, b.p, x.p, r.p, done.p); });
+        };
+        launch();
+        launch();
+        FG_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < 5; ++k) launch();
+        FG_CUDA(cudaEventRecord(e1, s));
+        FG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        op->probe_ms[variant] = ms / 5;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    op->unrolled = op->probe_ms[1] < op->probe_ms[0];
+}
+
 // lambda_max of D^-1 A by the power method in the D inner product (15 steps), on the device.
 static double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
                          DevBuf<double>& partial, DevBuf<unsigned>& counter) {
@@ -718,12 +782,16 @@ SolverImpl::SolverImpl() {
     done_zero_.alloc(1);
     done_zero_.zero(s_);
     FG_CUDA(cudaMallocHost(&h_sc_, sizeof(Scalars)));
+    FG_CUDA(cudaHostAlloc(&h_cancel_, sizeof(int), cudaHostAllocMapped));
+    *h_cancel_ = 0;
+    FG_CUDA(cudaHostGetDevicePointer(&d_cancel_, h_cancel_, 0));
 }
 
 SolverImpl::~SolverImpl() {
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
     if (h_sc_) cudaFreeHost(h_sc_);
+    if (h_cancel_) cudaFreeHost(h_cancel_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
     if (s_) {
@@ -748,6 +816,45 @@ size_t SolverImpl::bytes() const {
 }
 
 std::vector<int64_t> SolverImpl::level_sizes() const { return sizes_; }
+
+template <class T>
+static std::string describe_op(const Operator<T>& op) {
+    char buf[200];
+    if (!op.stencil) {
+        std::snprintf(buf, sizeof buf, "sell C=%d nnz=%lld", op.sell.C, (long long)op.nnz);
+    } else {
+        std::snprintf(buf, sizeof buf, "stencil K=%d %s (probe %.1f / %.1f us) nnz=%lld", op.K,
+                      op.unrolled ? "unrolled" : "loop", op.probe_ms[0] * 1e3,
+                      op.probe_ms[1] * 1e3, (long long)op.nnz);
+    }
+    return buf;
+}
+
+std::string SolverImpl::describe() const {
+    std::string out;
+    char buf[256];
+    std::snprintf(buf, sizeof buf, "method=%s precision=%s n=%lld\n",
+                  direct_ ? "direct" : "multigrid",
+                  opt_.precision == FEMGPU_MIXED ? "mixed" : "fp64", (long long)n_);
+    out += buf;
+    if (direct_) return out;
+    out += "outer fp64: " + describe_op(op64_) + "\n";
+    auto levels = [&](const auto& H, const char* t) {
+        for (size_t l = 0; l < H.levels.size(); ++l) {
+            const auto& L = H.levels[l];
+            std::snprintf(buf, sizeof buf, "level %zu %s n=%lld lambda=%.4f degree=%zu: ", l, t,
+                          (long long)L.n, L.lambda, L.c1.size());
+            out += buf + describe_op(L.A) + "\n";
+        }
+        std::snprintf(buf, sizeof buf, "coarsest n=%lld dense inverse\n", (long long)H.ncoarse);
+        out += buf;
+    };
+    if (opt_.precision == FEMGPU_MIXED)
+        levels(H32_, "fp32");
+    else
+        levels(H64_, "fp64");
+    return out;
+}
 
 void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
                         const femgpu_crossover& c, const Options& o) {
@@ -796,6 +903,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         return;
     }
     make_operator<double>(h, a_, C, opt_.format == 0, &op64_, s_);
+    tune_operator(&op64_, s_);
     if (u.kind == FEMGPU_UNKNOWNS_GRID) {
         HostLevel lv;
         for (int d = 0; d < 3; ++d) lv.planes[d].assign(u.planes[d], u.planes[d] + u.nplanes[d]);
@@ -840,6 +948,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         DevCsr d;
         upload_csr(mats[l], &d, s_);
         make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
+        tune_operator(&lv.A, s_);
         // The diagonal and lambda_max(D^-1 A) in FP64.
         DevBuf<double> dg(lv.n);
         DevBuf<int> bad(1);
@@ -1012,6 +1121,53 @@ void SolverImpl::enqueue_iteration() {
     FG_CHECK_LAUNCH();
 }
 
+// The whole PCG loop as 1 graph: a WHILE conditional node whose body is 1 iteration followed by
+// k_loop_control, so the device runs iteration after iteration with no host round trip.
+void SolverImpl::build_loop_graph() {
+    FG_CUDA(cudaGraphCreate(&graph_, 0));
+    FG_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond_;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    FG_CUDA(cudaGraphAddNode(&node, graph_, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    size_t before = launches_;
+    FG_CUDA(cudaStreamBeginCaptureToGraph(s_, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+    enqueue_iteration();
+    k_loop_control<<<1, 1, 0, s_>>>(cond_, sc_.p, d_cancel_);
+    FG_CUDA(cudaStreamEndCapture(s_, &body));
+    FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+    graph_kernels_ = launches_ - before + 1;
+    launches_ = before;
+}
+
+void SolverImpl::run_device_loop(const volatile int* cancel) {
+    int before = h_sc_->iters;
+    *(volatile int*)h_cancel_ = 0;
+    std::atomic<bool> stop{false};
+    std::thread watcher;
+    if (cancel) {
+        // Mirrors the caller's flag into the mapped flag the device reads each iteration.
+        watcher = std::thread([&] {
+            while (!stop.load(std::memory_order_relaxed)) {
+                if (*cancel) *(volatile int*)h_cancel_ = 1;
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+            }
+        });
+    }
+    cudaError_t e = cudaGraphLaunch(exec_, s_);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
+    stop.store(true);
+    if (watcher.joinable()) watcher.join();
+    FG_CUDA(e);
+    launches_ += graph_kernels_ * (size_t)(h_sc_->iters - before);
+}
+
 void SolverImpl::precondition(const double* d_r, double* d_z) {
     FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
     if (direct_) {
@@ -1036,6 +1192,7 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
     FG_CUDA(cudaEventRecord(ev0_, s_));
     FG_CUDA(cudaMemcpyAsync(b_.p, d_b, n * 8, cudaMemcpyDeviceToDevice, s_));
     Scalars init{};
+    init.max_iter = (int)std::min<size_t>(max_iter, 0x7fffffff);
     FG_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(Scalars), cudaMemcpyHostToDevice, s_));
     femgpu_stats out{};
     launches_ = 0;
@@ -1099,15 +1256,7 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         k_pcg_p<double><<<blocks_for(n, TH), TH, 0, s_>>>(n, zd_, p_.p, sc_.p, 1);
     }
     FG_CHECK_LAUNCH();
-    if (opt_.graph && !exec_) {
-        size_t before = launches_;
-        FG_CUDA(cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal));
-        enqueue_iteration();
-        FG_CUDA(cudaStreamEndCapture(s_, &graph_));
-        FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
-        graph_kernels_ = launches_ - before;
-        launches_ = before;
-    }
+    if (opt_.graph && !exec_) build_loop_graph();
     int status = FEMGPU_OK;
     std::string message;
     double residual = std::sqrt(h_sc_->rr) / norm_b;
@@ -1158,14 +1307,14 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
             break;
         }
         if (exec_) {
-            FG_CUDA(cudaGraphLaunch(exec_, s_));
-            launches_ += graph_kernels_;
+            run_device_loop(cancel);
+            it = (size_t)h_sc_->iters;
         } else {
             enqueue_iteration();
+            FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
+            FG_CUDA(cudaStreamSynchronize(s_));
+            ++it;
         }
-        FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
-        FG_CUDA(cudaStreamSynchronize(s_));
-        ++it;
         residual = std::sqrt(h_sc_->rr) / norm_b;
         if (!(residual == residual)) {
             status = FEMGPU_ERR_NOT_CONVERGED;

@@ -3,6 +3,7 @@
 // p-multigrid V-cycle of Chebyshev-Jacobi smoothing.
 #pragma once
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -32,6 +33,8 @@ void make_sell(const DevCsr& a, int C, Sell<T>* out, cudaStream_t s);
 template <class T>
 struct Operator {
     bool stencil = false;
+    bool unrolled = false;  // the compile-time-K kernel (K = 8 or 14), chosen by timing
+    double probe_ms[2] = {0, 0};  // the timed product: runtime K, compile-time K
     int64_t n = 0, nnz = 0;
     Sell<T> sell;
     int K = 0;
@@ -64,7 +67,7 @@ void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operato
 // The scalars of a PCG solve, in device memory.
 struct Scalars {
     double bb, rr, rz, pq, alpha, beta, zq, norm_b;
-    int done, iters, status, pad;
+    int done, iters, status, max_iter;
 };
 
 template <class T>
@@ -114,6 +117,8 @@ class SolverImpl {
     void precondition(const double* d_r, double* d_z);
     int method() const { return direct_ ? FEMGPU_METHOD_DIRECT : FEMGPU_METHOD_MULTIGRID; }
     std::vector<int64_t> level_sizes() const;
+    // A text description of the levels: size, format, K, kernel choice, lambda_max.
+    std::string describe() const;
     size_t bytes() const;
     // The mean device time (ms) of 1 launch of a kernel of the solve, and its algorithmic bytes.
     void kernel_time(int which, int reps, double* ms, double* bytes);
@@ -128,6 +133,9 @@ class SolverImpl {
     template <class T>
     const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b);
     void enqueue_iteration();
+    void build_loop_graph();
+    // Runs PCG iterations on the device until convergence, max_iter, a NaN or a cancel.
+    void run_device_loop(const volatile int* cancel);
     void run_init(const double* d_b);
     void dense_direct(const HostCsr& a);
 
@@ -152,6 +160,9 @@ class SolverImpl {
     DevBuf<int> done_zero_;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
+    cudaGraphConditionalHandle cond_ = 0;
+    int* h_cancel_ = nullptr;  // pinned and mapped: the device reads it each iteration
+    int* d_cancel_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     std::vector<int64_t> sizes_;
     size_t launches_ = 0;      // kernels enqueued by the current solve

@@ -198,6 +198,12 @@ class Solver:
     def device_bytes(self):
         return L.lib().femgpu_solver_bytes(self._h)
 
+    def describe(self):
+        """The levels, their storage formats and the kernels the autotuner chose."""
+        buf = C.create_string_buffer(8192)
+        L.lib().femgpu_solver_describe(self._h, buf, 8192)
+        return buf.value.decode()
+
     def solve(self, b, x=None, cancelled=None) -> Stats:
         """solve.rs:199-250: solve A x = b; ``x`` (numpy, updated in place) holds the start
         value. ``cancelled`` is a callable or a ctypes int flag read before each iteration;

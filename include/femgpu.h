@@ -197,6 +197,10 @@ int femgpu_solver_set_tol(femgpu_solver* s, double tol);
 int femgpu_solver_method(const femgpu_solver* s);
 /* The number of unknowns of each level (levels[0] = n); returns the level count. */
 int femgpu_solver_levels(const femgpu_solver* s, size_t* sizes, int cap);
+/* A text description of the solver (method, precision, and for each level its size, storage
+ * format and the kernel variant the autotuner chose); returns the full length. No reference
+ * counterpart. */
+size_t femgpu_solver_describe(const femgpu_solver* s, char* buf, size_t len);
 /* Device memory held by the solver, in bytes. */
 size_t femgpu_solver_bytes(const femgpu_solver* s);
 /* Solver::solve (solve.rs:199-250): solve A x = b; `x` holds the start value and gets the

@@ -169,3 +169,36 @@ def test_solver_reuse_across_right_sides():
     x = xs[0].copy()
     st = s.solve(rhs, x)
     assert st.iterations == 0
+
+
+def test_cancel_during_the_device_loop():
+    """A flag raised by another host thread while the device runs the PCG loop ends the solve
+    with "cancelled" before the iteration limit (multigrid.rs:735, polled each iteration)."""
+    import threading
+    import time
+
+    h = mg.heat_cube(48)
+    A, rhs, _ = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid)
+    s.solve(rhs, np.zeros(A.n))  # builds the loop graph
+    s.with_tol(1e-300).with_max_iter(100000)
+    flag = ctypes.c_int(0)
+    timer = threading.Timer(0.05, lambda: setattr(flag, "value", 1))
+    timer.start()
+    t0 = time.perf_counter()
+    with pytest.raises(fg.FemError) as e:
+        s.solve(rhs, np.zeros(A.n), cancelled=flag)
+    timer.cancel()
+    assert str(e.value) == "cancelled"
+    assert time.perf_counter() - t0 < 30.0
+
+
+def test_nan_right_side_breaks_down_with_an_error():
+    """A NaN in the right side stops the device loop at once instead of running to max_iter."""
+    h = mg.heat_cube(8)
+    A, rhs, _ = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid)
+    bad = rhs.copy()
+    bad[3] = np.nan
+    with pytest.raises(fg.FemError):
+        s.solve(bad, np.zeros(A.n))
