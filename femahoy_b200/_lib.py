@@ -88,6 +88,9 @@ SIGNATURES = {
     "femgpu_reduced_rhs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_size_t, C.c_void_p]),
     "femgpu_csr_free": (None, [C.c_void_p]),
+    "femgpu_reduced_rhs_noalloc": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                             C.c_void_p, C.c_void_p]),
     "femgpu_prolongation": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_size_t,
                                       C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.c_void_p,

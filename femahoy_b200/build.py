@@ -30,6 +30,7 @@ UNITS = [
     ("assemble.cu", ["-fmad=false"]),
     ("solver.cu", []),
     ("capi.cu", []),
+    ("noalloc.cu", ["-fmad=false"]),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"])]
 

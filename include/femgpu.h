@@ -115,6 +115,32 @@ int femgpu_reduced_rhs(const femgpu_csr* a, const double* load, const double* t,
                        const int64_t* free, size_t nfree, double* out);
 void femgpu_csr_free(femgpu_csr* a);
 
+/* The largest matrix (rows) that femgpu_reduced_rhs_noalloc takes. */
+#define FEMGPU_NOALLOC_MAX_ROWS 4194304
+
+/* femgpu_reduced_rhs for callers that cannot allocate device memory. No counterpart in the
+ * reference: it is this library's own addition.
+ *
+ * Some callers must not call cudaMalloc or cudaFree: code that shares the GPU with other work in
+ * flight (a loop serving many solves on several streams) would be stalled by cudaFree, which
+ * waits for the whole device, and code whose device memory is held by its own pool allocator
+ * cannot count on a new allocation succeeding. This entry point allocates nothing: every pointer
+ * is a device pointer owned by the caller (the CSR arrays of the n x n matrix: ptr n + 1, idx and
+ * val ptr[n]; load and t n values; free nfree increasing rows; out nfree values), and its only
+ * scratch, a row-to-place map, is a fixed array inside the library of FEMGPU_NOALLOC_MAX_ROWS
+ * entries (16 MiB held on every GPU that loads the library until the process exits). A larger n
+ * fails with FEMGPU_ERR_TOO_LARGE. The result is the allocating entry point's, bit for bit.
+ *
+ * `stream` is a cudaStream_t (null: the default stream). The call checks the free list on the
+ * device and waits for that check, then queues the right side on `stream` and returns;
+ * synchronize the stream before reading `out`. The first call on each device looks up the
+ * scratch's device address; make that first call before any stream capture. All calls share the
+ * scratch, which keeps the last call's contents (each call clears what it uses); calls whose
+ * work overlaps on the GPU race on it, so order them on one stream or one host thread. */
+int femgpu_reduced_rhs_noalloc(size_t n, const int64_t* ptr, const uint32_t* idx,
+                               const double* val, const double* load, const double* t,
+                               const int64_t* free, size_t nfree, double* out, void* stream);
+
 /* pmultigrid::prolongation (pmultigrid.rs:104-151): P from the free corner unknowns to the
  * free unknowns of a quadratic mesh. Two calls: with null outputs it writes the sizes
  * (`nnz`, `ncoarse`); then the CSR arrays of P (rows = nfree) and the coarse points (3 each). */

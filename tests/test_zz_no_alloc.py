@@ -1,0 +1,77 @@
+"""femgpu_reduced_rhs_noalloc against femgpu_reduced_rhs, through the C ABI.
+
+The no-allocation entry point exists for callers that must not call cudaMalloc or cudaFree:
+code that shares the GPU with other work in flight (cudaFree waits for the whole device and
+would stall it) and code whose device memory is held by its own pool allocator. Such a caller
+owns every buffer; here torch plays that caller and allocates the inputs and outputs, while the
+entry point itself allocates nothing and keeps its scratch in a fixed array in the library.
+
+The two calls in a row use matrices of different sizes, so the second call must clear what the
+first left in the shared scratch. This file sorts last so that a run stopping at the first
+failure has run every other test; it also passes alone in a fresh process.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+import femahoy_b200 as fg
+from femahoy_b200 import _lib
+from femahoy_b200 import meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems():
+    heat = mg.heat_cube(12)
+    K1 = fg.Csr.assemble(fg.P1_HEAT, heat.xyz, heat.nodes, heat.coef)
+    beam = mg.cantilever_p1(dims=(10, 2, 2), lengths=(25.0, 5.0, 5.0))
+    K2 = fg.Csr.assemble(fg.P1_ELASTIC, beam.xyz, beam.nodes, beam.coef)
+    rng = np.random.default_rng(7)
+    t2 = np.where(beam.fixed, rng.uniform(-0.1, 0.1, beam.n_unknowns), 0.0)
+    return [(K1, heat.load, heat.values, heat.free), (K2, beam.load, t2, beam.free)]
+
+
+def _noalloc(torch, K, load, t, free):
+    """The caller's device buffers, 1 call of the entry point, and the result."""
+    ptr, idx, val = K.arrays()
+    dev = "cuda"
+    d_ptr = torch.from_numpy(ptr).to(dev)
+    d_idx = torch.from_numpy(idx.view(np.int32)).to(dev)
+    d_val = torch.from_numpy(val).to(dev)
+    d_load = torch.from_numpy(np.ascontiguousarray(load, dtype=np.float64)).to(dev)
+    d_t = torch.from_numpy(np.ascontiguousarray(t, dtype=np.float64)).to(dev)
+    d_free = torch.from_numpy(np.ascontiguousarray(free, dtype=np.int64)).to(dev)
+    d_out = torch.full((len(free),), np.nan, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    stream.synchronize()
+    rc = fg.lib().femgpu_reduced_rhs_noalloc(
+        K.n, ctypes.c_void_p(d_ptr.data_ptr()), ctypes.c_void_p(d_idx.data_ptr()),
+        ctypes.c_void_p(d_val.data_ptr()), ctypes.c_void_p(d_load.data_ptr()),
+        ctypes.c_void_p(d_t.data_ptr()), ctypes.c_void_p(d_free.data_ptr()), len(free),
+        ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+    _lib.check(rc)
+    stream.synchronize()
+    return d_out.cpu().numpy()
+
+
+def test_noalloc_right_side_equals_the_allocating_one_twice_in_a_row():
+    torch = pytest.importorskip("torch")
+    for K, load, t, free in _problems():
+        expected = fg.reduced_rhs(K, load, t, free)
+        got = _noalloc(torch, K, load, t, free)
+        # The same sums in the same order: equal bit for bit (the other right-side tests are
+        # bit-exact too).
+        assert np.array_equal(got.view(np.uint64), expected.view(np.uint64))
+
+
+def test_noalloc_refuses_a_matrix_past_its_scratch():
+    max_rows = 4194304
+    rc = fg.lib().femgpu_reduced_rhs_noalloc(max_rows + 1, ctypes.c_void_p(8),
+                                             ctypes.c_void_p(8), ctypes.c_void_p(8),
+                                             ctypes.c_void_p(8), ctypes.c_void_p(8),
+                                             ctypes.c_void_p(8), 1, ctypes.c_void_p(8), None)
+    assert rc == 7  # FEMGPU_ERR_TOO_LARGE, before any device work
+    buf = ctypes.create_string_buffer(256)
+    fg.lib().femgpu_last_error(buf, 256)
+    assert b"4194304" in buf.value
