@@ -49,6 +49,12 @@ def args():
     p.add_argument("--profile", action="store_true",
                    help="only the timed mixed-precision solves (the command profiled by ncu)")
     p.add_argument("--format", type=int, default=0, help="0: stencil where possible, 1: SELL")
+    p.add_argument("--breakdown", action="store_true",
+                   help="print each solver's levels and the device time of each kernel of 1 "
+                        "PCG iteration (kernels launched one by one), then exit")
+    p.add_argument("--graph", type=int, default=0,
+                   help="0/1: the PCG loop as 1 CUDA graph; 2: kernels launched one by one (so "
+                        "that a profiler lists each kernel of the loop)")
     return p.parse_args()
 
 
@@ -253,7 +259,8 @@ def run_ours(opt, rank, world, local):
     def make(precision):
         t = time.perf_counter()
         s = fg.Solver(A, unknowns, fg.Method.Multigrid,
-                      options=fg.Options(precision=precision, format=opt.format)).with_tol(TOL)
+                      options=fg.Options(precision=precision, format=opt.format,
+                                         graph=opt.graph)).with_tol(TOL)
         return s, time.perf_counter() - t
 
     b = torch.from_numpy(rhs).cuda()
@@ -286,6 +293,21 @@ def run_ours(opt, rank, world, local):
         ms = e0.elapsed_time(e1)
         return ms, lat, its, launches, res, clk
 
+    if opt.breakdown:
+        for precision in (fg.MIXED, fg.FP64):
+            s, _ = make(precision)
+            for _ in range(3):
+                with torch.cuda.stream(torch.cuda.ExternalStream(
+                        lib.femgpu_solver_stream(s.handle))):
+                    x.zero_()
+                st = s.solve_device(b.data_ptr(), x.data_ptr())
+            if rank == 0:
+                print(f"== {'mixed' if precision == fg.MIXED else 'fp64'}: {st.iterations} "
+                      f"iterations, {st.seconds * 1e3:.3f} ms per solve (CUDA graph)")
+                print(s.describe())
+                print(s.breakdown(), flush=True)
+            del s
+        return
     mixed, setup_mixed = make(fg.MIXED)
     clocks = Clocks(torch.cuda.current_device())
     ms, lat, its, launches, res, clk = timed(mixed, opt.steps, opt.warmup, clocks)

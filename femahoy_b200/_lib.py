@@ -104,6 +104,7 @@ SIGNATURES = {
     "femgpu_solver_levels": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "femgpu_solver_bytes": (C.c_size_t, [C.c_void_p]),
     "femgpu_solver_describe": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "femgpu_solver_breakdown": (C.c_size_t, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "femgpu_solver_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.POINTER(Stats_t)]),
     "femgpu_solver_solve_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -360,20 +360,7 @@ int femgpu_solver_solve(femgpu_solver* s, const double* b, double* x, const vola
                         femgpu_stats* stats) {
     return guarded([&] {
         require(s && b && x, "null argument");
-        size_t n = s->impl.level_sizes().empty() ? 0 : (size_t)s->impl.level_sizes()[0];
-        cudaStream_t st = s->impl.stream();
-        DevBuf<double> db, dx;
-        db.upload(b, n, st);
-        dx.upload(x, n, st);
-        try {
-            s->impl.solve(db.p, dx.p, cancel, stats);
-        } catch (const Failure&) {
-            dx.download(x, n, st);
-            cudaStreamSynchronize(st);
-            throw;
-        }
-        dx.download(x, n, st);
-        FG_CUDA(cudaStreamSynchronize(st));
+        s->impl.solve_host(b, x, cancel, stats);
     });
 }
 
@@ -393,6 +380,18 @@ int femgpu_solver_precondition_device(femgpu_solver* s, const double* r, double*
 }
 
 void femgpu_solver_free(femgpu_solver* s) { delete s; }
+
+size_t femgpu_solver_breakdown(femgpu_solver* s, char* buf, size_t len) {
+    std::string d;
+    int rc = guarded([&] { d = s->impl.breakdown(); });
+    if (rc != FEMGPU_OK) return 0;
+    if (buf && len) {
+        size_t k = std::min(len - 1, d.size());
+        std::memcpy(buf, d.data(), k);
+        buf[k] = 0;
+    }
+    return d.size();
+}
 
 void* femgpu_solver_stream(const femgpu_solver* s) {
     return s ? (void*)s->impl.stream() : nullptr;

@@ -98,20 +98,31 @@ __device__ __forceinline__ void reduce2_finalize(double a, double b, double* par
     __syncthreads();
     if (!last) return;
     __threadfence();
-    if (threadIdx.x < 32) {
-        double ta = 0, tb = 0;
-        for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
-            ta += ((volatile double*)partial)[2 * k];
-            tb += ((volatile double*)partial)[2 * k + 1];
+    // The last block sums the partials of every block: each thread a strided subset in a
+    // fixed order, then the block tree; the same order every launch.
+    double ta = 0, tb = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += THREADS) {
+        ta += ((volatile double*)partial)[2 * k];
+        tb += ((volatile double*)partial)[2 * k + 1];
+    }
+    for (int o = 16; o; o >>= 1) {
+        ta += __shfl_xor_sync(0xffffffffu, ta, o);
+        tb += __shfl_xor_sync(0xffffffffu, tb, o);
+    }
+    __syncthreads();
+    if (lane == 0) {
+        sa[w] = ta;
+        sb[w] = tb;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double fa = 0, fb = 0;
+        for (int k = 0; k < THREADS / 32; ++k) {
+            fa += sa[k];
+            fb += sb[k];
         }
-        for (int o = 16; o; o >>= 1) {
-            ta += __shfl_xor_sync(0xffffffffu, ta, o);
-            tb += __shfl_xor_sync(0xffffffffu, tb, o);
-        }
-        if (threadIdx.x == 0) {
-            fin(ta, tb);
-            *counter = 0;
-        }
+        fin(fa, fb);
+        *counter = 0;
     }
 }
 

@@ -43,9 +43,9 @@ struct Operator {
     int64_t threads() const { return stencil ? n : sell.nslices * sell.C; }
     StencilView<T> sview() const {
         StencilView<T> v{};
-        v.n = n;
+        v.n = (int)n;
         v.K = K;
-        for (int k = 0; k < K; ++k) v.off[k] = off[k];
+        for (int k = 0; k < K; ++k) v.off[k] = (int)off[k];
         v.coef = coef.p;
         return v;
     }
@@ -114,11 +114,15 @@ class SolverImpl {
                 const Options& o);
     // solve.rs:199-250 on device vectors
     void solve(const double* d_b, double* d_x, const volatile int* cancel, femgpu_stats* st);
+    void solve_host(const double* h_b, double* h_x, const volatile int* cancel, femgpu_stats* st);
     void precondition(const double* d_r, double* d_z);
     int method() const { return direct_ ? FEMGPU_METHOD_DIRECT : FEMGPU_METHOD_MULTIGRID; }
     std::vector<int64_t> level_sizes() const;
     // A text description of the levels: size, format, K, kernel choice, lambda_max.
     std::string describe() const;
+    // The device time of each kernel of 1 PCG iteration (kernels launched one by one, a CUDA
+    // event after each), as text.
+    std::string breakdown();
     size_t bytes() const;
     // The mean device time (ms) of 1 launch of a kernel of the solve, and its algorithmic bytes.
     void kernel_time(int which, int reps, double* ms, double* bytes);
@@ -165,6 +169,9 @@ class SolverImpl {
     int* d_cancel_ = nullptr;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     std::vector<int64_t> sizes_;
+    // While breakdown() runs: the label and the event recorded after each kernel.
+    std::vector<std::pair<std::string, cudaEvent_t>>* trace_ = nullptr;
+    void mark(const std::string& label);
     size_t launches_ = 0;      // kernels enqueued by the current solve
     size_t graph_kernels_ = 0; // kernels of 1 iteration graph
 };

@@ -198,6 +198,12 @@ class Solver:
     def device_bytes(self):
         return L.lib().femgpu_solver_bytes(self._h)
 
+    def breakdown(self):
+        """The device time of each kernel of 1 PCG iteration (overwrites the solver's vectors)."""
+        buf = C.create_string_buffer(16384)
+        L.lib().femgpu_solver_breakdown(self._h, buf, 16384)
+        return buf.value.decode()
+
     def describe(self):
         """The levels, their storage formats and the kernels the autotuner chose."""
         buf = C.create_string_buffer(8192)

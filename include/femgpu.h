@@ -227,6 +227,10 @@ int femgpu_solver_levels(const femgpu_solver* s, size_t* sizes, int cap);
  * format and the kernel variant the autotuner chose); returns the full length. No reference
  * counterpart. */
 size_t femgpu_solver_describe(const femgpu_solver* s, char* buf, size_t len);
+/* Runs 1 PCG iteration with its kernels launched one by one and a CUDA event after each, and
+ * writes the device time of each kernel as text (1 line each); returns the full length. The
+ * solver's vectors are overwritten; solve again afterwards. No reference counterpart. */
+size_t femgpu_solver_breakdown(femgpu_solver* s, char* buf, size_t len);
 /* Device memory held by the solver, in bytes. */
 size_t femgpu_solver_bytes(const femgpu_solver* s);
 /* Solver::solve (solve.rs:199-250): solve A x = b; `x` holds the start value and gets the
