@@ -56,6 +56,13 @@ class Options_t(C.Structure):
                 ("max_levels", C.c_int), ("graph", C.c_int), ("format", C.c_int)]
 
 
+class BatchStats_t(C.Structure):
+    _fields_ = [("max_iterations", C.c_size_t), ("mean_iterations", C.c_double),
+                ("max_residual", C.c_double), ("max_true_residual", C.c_double),
+                ("seconds", C.c_double), ("launches", C.c_size_t),
+                ("not_converged", C.c_size_t), ("restarts", C.c_size_t)]
+
+
 class Stats_t(C.Structure):
     _fields_ = [("iterations", C.c_size_t), ("residual", C.c_double),
                 ("true_residual", C.c_double), ("seconds", C.c_double),
@@ -114,6 +121,32 @@ SIGNATURES = {
     "femgpu_solver_stream": (C.c_void_p, [C.c_void_p]),
     "femgpu_solver_kernel_time": (C.c_int, [C.c_void_p, C.c_int, C.c_int,
                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "femgpu_server_new": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(C.c_void_p)]),
+    "femgpu_server_reserve": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "femgpu_server_put": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p]),
+    "femgpu_server_has": (C.c_int, [C.c_void_p, C.c_uint64]),
+    "femgpu_server_submit": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_uint64)]),
+    "femgpu_server_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.POINTER(Stats_t),
+                                     C.POINTER(C.c_double)]),
+    "femgpu_server_resident_bytes": (C.c_size_t, [C.c_void_p]),
+    "femgpu_server_resident_count": (C.c_size_t, [C.c_void_p]),
+    "femgpu_server_free": (None, [C.c_void_p]),
+    "femgpu_batch_new": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                   C.POINTER(C.c_void_p)]),
+    "femgpu_batch_set_tol": (C.c_int, [C.c_void_p, C.c_double]),
+    "femgpu_batch_set_max_iter": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "femgpu_batch_systems": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_batch_levels": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.POINTER(BatchStats_t)]),
+    "femgpu_batch_solve_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.POINTER(BatchStats_t)]),
+    "femgpu_batch_segments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]),
+    "femgpu_batch_bytes": (C.c_size_t, [C.c_void_p]),
+    "femgpu_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "femgpu_batch_free": (None, [C.c_void_p]),
 }
 
 

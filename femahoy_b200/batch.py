@@ -1,0 +1,140 @@
+"""Batches: many small systems with several right sides each, solved together on 1 GPU
+(include/femgpu.h ``femgpu_batch_*``).
+
+``Batch(matrices, unknowns, nrhs)`` builds each system's multigrid hierarchy and combines the
+systems level by level into block-diagonal operators; ``solve(b)`` runs every (system, right
+side) pair as its own PCG solve in 1 device-side loop. ``b`` and the result are lists of
+``(rows, nrhs)`` arrays, one per system.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+from .solve import Options, Unknowns, unknowns_c
+from .sparse import Csr
+
+
+@dataclass
+class BatchStats:
+    max_iterations: int
+    mean_iterations: float
+    max_residual: float
+    max_true_residual: float
+    seconds: float
+    launches: int
+    not_converged: int
+    restarts: int
+
+
+class Batch:
+    def __init__(self, matrices: list[Csr], unknowns: list[Unknowns], nrhs=16, *,
+                 precision=L.MIXED, options: Options | None = None):
+        if len(matrices) != len(unknowns):
+            raise L.FemError(L.INVALID, "1 unknowns description per matrix")
+        opts = options or Options(precision=precision)
+        keep = []
+        us = (L.Unknowns_t * len(matrices))()
+        for k, u in enumerate(unknowns):
+            us[k] = unknowns_c(u, keep)
+        hs = (C.c_void_p * len(matrices))(*[m.handle for m in matrices])
+        oc = opts._c()
+        h = C.c_void_p()
+        L.check(L.lib().femgpu_batch_new(len(matrices), hs, us, nrhs, C.byref(oc), C.byref(h)))
+        self._h = h.value
+        self.nrhs = nrhs
+        count = L.lib().femgpu_batch_systems(self._h, None)
+        off = np.zeros(count + 1, dtype=np.uint64)
+        L.lib().femgpu_batch_systems(self._h, L.ptr(off))
+        self.offsets = off.astype(np.int64)
+        self.rows = int(self.offsets[-1])
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            L.lib().femgpu_batch_free(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def count(self):
+        return len(self.offsets) - 1
+
+    def with_tol(self, tol):
+        L.check(L.lib().femgpu_batch_set_tol(self._h, tol))
+        return self
+
+    def with_max_iter(self, m):
+        L.check(L.lib().femgpu_batch_set_max_iter(self._h, m))
+        return self
+
+    def levels(self):
+        k = L.lib().femgpu_batch_levels(self._h, None)
+        out = np.zeros(k, dtype=np.uint64)
+        L.lib().femgpu_batch_levels(self._h, L.ptr(out))
+        return [int(v) for v in out]
+
+    def device_bytes(self):
+        return L.lib().femgpu_batch_bytes(self._h)
+
+    def stream(self):
+        return L.lib().femgpu_batch_stream(self._h)
+
+    def pack(self, parts):
+        """The interleaved vector of per-system (rows, nrhs) arrays."""
+        out = np.empty((self.rows, self.nrhs))
+        for k, p in enumerate(parts):
+            out[self.offsets[k]:self.offsets[k + 1]] = np.asarray(p).reshape(-1, self.nrhs)
+        return out
+
+    def unpack(self, v):
+        v = np.asarray(v).reshape(self.rows, self.nrhs)
+        return [v[self.offsets[k]:self.offsets[k + 1]].copy() for k in range(self.count)]
+
+    def solve_packed(self, b, x=None, cancel=None):
+        """Solves with interleaved host vectors (rows x nrhs); x (the start value, zeros when
+        None) gets the solution. Returns (x, BatchStats)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x is None else x
+        st = L.BatchStats_t()
+        flag = None if cancel is None else C.byref(cancel)
+        L.check(L.lib().femgpu_batch_solve(self._h, L.ptr(b), L.ptr(x), flag, C.byref(st)))
+        return x, _stats(st)
+
+    def solve(self, parts, cancel=None):
+        x, st = self.solve_packed(self.pack(parts), cancel=cancel)
+        return self.unpack(x), st
+
+    def solve_device(self, b, x, cancel=None):
+        """Device tensors (torch, float64, rows * nrhs values, contiguous) on the batch's stream."""
+        st = L.BatchStats_t()
+        flag = None if cancel is None else C.byref(cancel)
+        L.check(L.lib().femgpu_batch_solve_device(self._h, C.c_void_p(b.data_ptr()),
+                                                  C.c_void_p(x.data_ptr()), flag, C.byref(st)))
+        return _stats(st)
+
+    def segments(self):
+        """Per (system, right side) of the last solve: iterations, true residual, recurrence
+        residual, status (0 converged, 1 iteration limit, 2 broke down), each (count, nrhs)."""
+        n = self.count * self.nrhs
+        it = np.zeros(n, dtype=np.uint64)
+        tr = np.zeros(n)
+        rr = np.zeros(n)
+        stt = np.zeros(n, dtype=np.int32)
+        L.check(L.lib().femgpu_batch_segments(self._h, L.ptr(it), L.ptr(tr), L.ptr(rr),
+                                              L.ptr(stt)))
+        shape = (self.count, self.nrhs)
+        return (it.astype(np.int64).reshape(shape), tr.reshape(shape), rr.reshape(shape),
+                stt.reshape(shape))
+
+
+def _stats(st):
+    return BatchStats(st.max_iterations, st.mean_iterations, st.max_residual,
+                      st.max_true_residual, st.seconds, st.launches, st.not_converged,
+                      st.restarts)

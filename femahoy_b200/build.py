@@ -31,6 +31,8 @@ UNITS = [
     ("solver.cu", []),
     ("capi.cu", []),
     ("noalloc.cu", ["-fmad=false"]),
+    ("server.cu", []),
+    ("batch.cu", []),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"])]
 

@@ -8,14 +8,6 @@
 #include "hierarchy.hpp"
 #include "solver.cuh"
 
-struct femgpu_csr {
-    femgpu::DevCsr m;
-};
-
-struct femgpu_solver {
-    femgpu::SolverImpl impl;
-};
-
 namespace femgpu {
 
 static thread_local std::string g_last_error;

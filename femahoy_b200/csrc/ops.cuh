@@ -15,6 +15,11 @@ namespace femgpu {
 
 constexpr int MAXK = 32;
 
+// a b + c with 1 rounding, so that every product kernel below sums in the same way whatever
+// the compiler contracts.
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // Row numbers and offsets are 32-bit (a stencil is built only when n plus the largest offset
 // fits): with 64-bit row arithmetic the products ran 2.4 times slower on B200, the extra integer
 // work, not the memory, setting their time.
@@ -51,8 +56,8 @@ struct StencilOp {
             const int o = v.off[k];
             const T* __restrict__ ck = c + (size_t)k * n;
             const int j = i + o, m = i - o;
-            if (j < n) acc += (TA)__ldg(ck + i) * (TA)__ldg(x + j);
-            if (m >= 0) acc += (TA)__ldg(ck + m) * (TA)__ldg(x + m);
+            if (j < n) acc = fmadd((TA)__ldg(ck + i), (TA)__ldg(x + j), acc);
+            if (m >= 0) acc = fmadd((TA)__ldg(ck + m), (TA)__ldg(x + m), acc);
         }
         return acc;
     }
@@ -71,15 +76,18 @@ struct StencilOpK {
     __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
         const int i = (int)g, n = v.n;
         const T* __restrict__ c = v.coef;
-        TA acc = 0;
+        // The same fused multiply-adds in the same order as StencilOp: a term past either end
+        // adds 0 * 0 = +0, which changes no nonzero sum, so both kernels give the same bits and
+        // the autotuner's choice between them (made by timing) cannot change a result.
+        TA acc = (TA)__ldg(c + i) * (TA)__ldg(x + i);
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
+        for (int k = 1; k < K; ++k) {
             const int o = v.off[k];
             const T* __restrict__ ck = c + (size_t)k * n;
             const int j = i + o, m = i - o;
-            TA a = (TA)__ldg(ck + i) * (j < n ? (TA)__ldg(x + j) : (TA)0);
-            if (k > 0) a += (m >= 0 ? (TA)__ldg(ck + m) : (TA)0) * (m >= 0 ? (TA)__ldg(x + m) : (TA)0);
-            acc += a;
+            const bool up = j < n, lo = m >= 0;
+            acc = fmadd(up ? (TA)__ldg(ck + i) : (TA)0, up ? (TA)__ldg(x + j) : (TA)0, acc);
+            acc = fmadd(lo ? (TA)__ldg(ck + m) : (TA)0, lo ? (TA)__ldg(x + m) : (TA)0, acc);
         }
         return acc;
     }

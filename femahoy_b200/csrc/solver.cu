@@ -682,7 +682,7 @@ __global__ void k_inv_backward(const double* __restrict__ L, int64_t n, const do
 
 // The inverse of the SPD matrix `a` (host CSR, n small) on the device, FP64, row-major (it is
 // symmetric). Fails with the reference's text when a pivot is not positive.
-static void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
     int64_t n = a.n;
     std::vector<double> h((size_t)n * n, 0.0), diag(n, 0.0);
     for (int64_t i = 0; i < n; ++i)
@@ -725,7 +725,7 @@ static void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s)
 }
 
 // ------------------------------------------------------------------ helpers
-static void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s) {
+void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s) {
     d->n = h.n;
     d->nnz = h.nnz();
     d->ptr.upload(h.ptr.data(), h.n + 1, s);
@@ -733,7 +733,7 @@ static void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s) {
     d->val.upload(h.val.data(), h.nnz(), s);
 }
 
-static HostCsr download_csr(const DevCsr& d, cudaStream_t s) {
+HostCsr download_csr(const DevCsr& d, cudaStream_t s) {
     HostCsr h;
     h.n = d.n;
     h.ptr.resize(d.n + 1);
@@ -746,7 +746,7 @@ static HostCsr download_csr(const DevCsr& d, cudaStream_t s) {
     return h;
 }
 
-static HostRect transpose(const HostRect& p) {
+HostRect transpose(const HostRect& p) {
     HostRect r;
     r.rows = p.cols;
     r.cols = p.rows;
@@ -816,8 +816,8 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
 }
 
 // lambda_max of D^-1 A by the power method in the D inner product (15 steps), on the device.
-static double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
-                         DevBuf<double>& partial) {
+double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
+                  DevBuf<double>& partial) {
     int64_t n = A.n;
     // out[0..1]: v.Av and v.Dv of this step; out[2..3]: |w|^2 (and an unused 0).
     DevBuf<double> v(n), w(n), out(4);
@@ -843,8 +843,8 @@ static double lambda_max(const Operator<double>& A, const double* dg, cudaStream
     return lam;
 }
 
-static void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
-                      std::vector<double>* c2) {
+void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
+               std::vector<double>* c2) {
     // Y. Saad, Iterative Methods for Sparse Linear Systems, 2nd ed., SIAM 2003, algorithm 12.1,
     // on the interval [lower, 1.1] x lambda_max of D^-1 A.
     double hi = 1.1 * lam, lo = lower * lam;

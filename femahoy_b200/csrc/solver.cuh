@@ -64,6 +64,16 @@ template <class T>
 void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operator<T>* out,
                    cudaStream_t s);
 
+// Setup helpers shared by the solvers (solver.cu).
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s);
+void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s);
+HostCsr download_csr(const DevCsr& d, cudaStream_t s);
+HostRect transpose(const HostRect& p);
+double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
+                  DevBuf<double>& partial);
+void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
+               std::vector<double>* c2);
+
 // The scalars of a PCG solve, in device memory.
 struct Scalars {
     double bb, rr, rz, pq, alpha, beta, zq, norm_b;
@@ -177,3 +187,12 @@ class SolverImpl {
 };
 
 }  // namespace femgpu
+
+// The handles of include/femgpu.h.
+struct femgpu_csr {
+    femgpu::DevCsr m;
+};
+
+struct femgpu_solver {
+    femgpu::SolverImpl impl;
+};

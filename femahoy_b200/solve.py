@@ -116,6 +116,41 @@ class Options:
                            self.max_levels, self.graph, self.format)
 
 
+def unknowns_c(unknowns: "Unknowns", keep: list) -> L.Unknowns_t:
+    """The femgpu_unknowns of ``unknowns``; the arrays it points into are appended to ``keep``,
+    which must outlive the call that reads it."""
+    u = L.Unknowns_t()
+    u.kind = unknowns.kind
+    if unknowns.kind == 0:
+        lv = unknowns.level
+        planes = [L.arr(p, np.float64) for p in lv.planes]
+        pts = L.arr(lv.points, np.uint32).reshape(-1, 3)
+        comp = L.arr(lv.comp, np.uint8)
+        keep += planes + [pts, comp]
+        for d in range(3):
+            u.planes[d] = planes[d].ctypes.data
+            u.nplanes[d] = len(planes[d])
+        u.points = pts.ctypes.data
+        u.comp = comp.ctypes.data
+    else:
+        xyz = L.arr(unknowns.points, np.float64).reshape(-1, 3)
+        keep.append(xyz)
+        u.xyz = xyz.ctypes.data
+    if unknowns.kind == 2:
+        p = unknowns.p
+        pp, pi, pv = L.arr(p.ptr, np.int64), L.arr(p.idx, np.uint32), L.arr(p.val, np.float64)
+        cx = L.arr(unknowns.coarse, np.float64).reshape(-1, 3)
+        keep += [pp, pi, pv, cx]
+        u.p_cols = p.cols
+        u.p_ptr, u.p_idx, u.p_val = pp.ctypes.data, pi.ctypes.data, pv.ctypes.data
+        u.coarse_xyz = cx.ctypes.data
+        if unknowns.coarse_comp is not None:
+            cc = L.arr(unknowns.coarse_comp, np.uint8)
+            keep.append(cc)
+            u.coarse_comp = cc.ctypes.data
+    return u
+
+
 class Solver:
     """solve.rs:58-250 on the device."""
 
@@ -127,37 +162,9 @@ class Solver:
         crossover = crossover or Crossover.Unknowns(STEADY_DIRECT_LIMIT)
         opts = options or Options()
         opts.precision = precision if options is None else opts.precision
-        u = L.Unknowns_t()
-        u.kind = unknowns.kind
         keep = []  # arrays that must live through the call
+        u = unknowns_c(unknowns, keep)
         n = a.n
-        if unknowns.kind == 0:
-            lv = unknowns.level
-            planes = [L.arr(p, np.float64) for p in lv.planes]
-            pts = L.arr(lv.points, np.uint32).reshape(-1, 3)
-            comp = L.arr(lv.comp, np.uint8)
-            keep += planes + [pts, comp]
-            for d in range(3):
-                u.planes[d] = planes[d].ctypes.data
-                u.nplanes[d] = len(planes[d])
-            u.points = pts.ctypes.data
-            u.comp = comp.ctypes.data
-        else:
-            xyz = L.arr(unknowns.points, np.float64).reshape(-1, 3)
-            keep.append(xyz)
-            u.xyz = xyz.ctypes.data
-        if unknowns.kind == 2:
-            p = unknowns.p
-            pp, pi, pv = L.arr(p.ptr, np.int64), L.arr(p.idx, np.uint32), L.arr(p.val, np.float64)
-            cx = L.arr(unknowns.coarse, np.float64).reshape(-1, 3)
-            keep += [pp, pi, pv, cx]
-            u.p_cols = p.cols
-            u.p_ptr, u.p_idx, u.p_val = pp.ctypes.data, pi.ctypes.data, pv.ctypes.data
-            u.coarse_xyz = cx.ctypes.data
-            if unknowns.coarse_comp is not None:
-                cc = L.arr(unknowns.coarse_comp, np.uint8)
-                keep.append(cc)
-                u.coarse_comp = cc.ctypes.data
         m = -1 if method is None else int(method)
         h = C.c_void_p()
         cr = crossover._c()

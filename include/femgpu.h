@@ -253,6 +253,85 @@ void* femgpu_solver_stream(const femgpu_solver* s);
  * launch (values, indices and vectors, each read or written once). No reference counterpart. */
 int femgpu_solver_kernel_time(femgpu_solver* s, int which, int reps, double* ms, double* bytes);
 
+/* ---------------------------------------------------------------- serving */
+
+/* A server of solve requests. No reference counterpart: the reference's callers solve 1 model
+ * at a time (heat.rs:661-676, elastic_tet.rs:293-337). `slots` host threads each run 1 solve at
+ * a time on its solver's own CUDA stream, so up to `slots` requests are on the device together
+ * and a request that arrives while others run starts when a slot is free. The resident solvers
+ * (operators and hierarchies, keyed by the caller's 64-bit key, e.g. a mesh id) count against
+ * `budget_bytes` of device memory; idle ones are freed least recently used first when room is
+ * needed. 1 solver runs 1 request at a time; requests for 1 key run in submission order. */
+typedef struct femgpu_server femgpu_server;
+int femgpu_server_new(int slots, size_t budget_bytes, femgpu_server** out);
+/* Frees idle resident solvers until `bytes` more fit; FEMGPU_ERR_TOO_LARGE if the busy ones
+ * leave no room. Call it before building a solver that the server is to hold. */
+int femgpu_server_reserve(femgpu_server* s, size_t bytes);
+/* Hands `solver` to the server under `key`; the server owns it from then on (do not free it).
+ * On an error the caller keeps it. */
+int femgpu_server_put(femgpu_server* s, uint64_t key, femgpu_solver* solver);
+/* 1 if a solver is resident under `key`. */
+int femgpu_server_has(femgpu_server* s, uint64_t key);
+/* Queues Solver::solve (solve.rs:199) of the solver under `key`: b and the start value x are
+ * host arrays that must stay valid until the ticket is waited for; x gets the solution. */
+int femgpu_server_submit(femgpu_server* s, uint64_t key, const double* b, double* x,
+                         uint64_t* ticket);
+/* Waits for a ticket: its status (the solve's), stats, and the seconds from submission to the
+ * end of the solve. */
+int femgpu_server_wait(femgpu_server* s, uint64_t ticket, femgpu_stats* stats, double* latency_s);
+size_t femgpu_server_resident_bytes(femgpu_server* s);
+size_t femgpu_server_resident_count(femgpu_server* s);
+void femgpu_server_free(femgpu_server* s);
+
+/* ---------------------------------------------------------------- batches */
+
+/* Many small systems, each with `nrhs` right sides, solved together. No reference counterpart:
+ * the reference's callers solve 1 model at a time; each (system, right side) pair, a segment,
+ * is the reference's PCG with the multigrid V-cycle (multigrid.rs:692-753) with its own
+ * scalars and stopping test. Each system keeps its own hierarchy (multigrid.rs:84-139, down to
+ * `options->coarsest` unknowns, 1024 when 0) and the systems' levels are combined into
+ * block-diagonal operators, so 1 launch of each kernel serves all systems; the loop is 1 CUDA
+ * graph on the device. Vectors hold the right sides interleaved: value (row, k) of system s is
+ * at (offsets[s] + row) * nrhs + k, offsets from femgpu_batch_systems. */
+typedef struct femgpu_batch femgpu_batch;
+
+typedef struct femgpu_batch_stats {
+    size_t max_iterations;    /* the most iterations of a segment */
+    double mean_iterations;
+    double max_residual;      /* the largest recurrence residual |r| / |b| of a segment */
+    double max_true_residual; /* the largest |b - A x| / |b| in FP64 of a segment */
+    double seconds;           /* device time of the solve (CUDA events) */
+    size_t launches;          /* kernels this library launched for the solve */
+    size_t not_converged;     /* segments that hit the iteration limit or broke down */
+    size_t restarts;          /* restarts from x of the segments whose true residual drifted */
+} femgpu_batch_stats;
+
+/* `count` systems with grid unknowns (FEMGPU_UNKNOWNS_GRID; else FEMGPU_ERR_NEEDS_GRID);
+ * nrhs = 1, 4 or 16. Honours options->precision, degree, lower, coarsest and max_levels. */
+int femgpu_batch_new(int count, const femgpu_csr* const* a, const femgpu_unknowns* unknowns,
+                     int nrhs, const femgpu_options* options, femgpu_batch** out);
+int femgpu_batch_set_tol(femgpu_batch* b, double tol);           /* default PCG_TOL, 1e-10 */
+int femgpu_batch_set_max_iter(femgpu_batch* b, size_t max_iter); /* default PCG_MAX_ITER, 500 */
+/* The number of systems; `offsets` (may be null) gets count + 1 row offsets. */
+int femgpu_batch_systems(const femgpu_batch* b, size_t* offsets);
+/* The number of levels; `sizes` (may be null) gets the combined unknowns of each. */
+int femgpu_batch_levels(const femgpu_batch* b, size_t* sizes);
+/* Solves every segment from the start value in x (host arrays of rows * nrhs values). A segment
+ * that hits the iteration limit or breaks down makes the call return FEMGPU_ERR_NOT_CONVERGED
+ * naming the first such segment, with every x written; femgpu_batch_segments tells which. */
+int femgpu_batch_solve(femgpu_batch* b, const double* rhs, double* x, const volatile int* cancel,
+                       femgpu_batch_stats* stats);
+/* As femgpu_batch_solve on device arrays, on the batch's stream. */
+int femgpu_batch_solve_device(femgpu_batch* b, const double* rhs, double* x,
+                              const volatile int* cancel, femgpu_batch_stats* stats);
+/* Per segment (system s, right side k at s * nrhs + k) of the last solve: iterations, true and
+ * recurrence residuals, status (0 converged, 1 iteration limit, 2 broke down). Any may be null. */
+int femgpu_batch_segments(const femgpu_batch* b, size_t* iterations, double* true_residual,
+                          double* residual, int* status);
+size_t femgpu_batch_bytes(const femgpu_batch* b);
+void* femgpu_batch_stream(const femgpu_batch* b);
+void femgpu_batch_free(femgpu_batch* b);
+
 #ifdef __cplusplus
 }
 #endif
