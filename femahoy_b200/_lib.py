@@ -144,6 +144,8 @@ SIGNATURES = {
                                             C.POINTER(BatchStats_t)]),
     "femgpu_batch_segments": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p]),
+    "femgpu_batch_kernel_time": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double)]),
     "femgpu_batch_bytes": (C.c_size_t, [C.c_void_p]),
     "femgpu_batch_stream": (C.c_void_p, [C.c_void_p]),
     "femgpu_batch_free": (None, [C.c_void_p]),

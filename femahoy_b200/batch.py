@@ -83,6 +83,12 @@ class Batch:
     def device_bytes(self):
         return L.lib().femgpu_batch_bytes(self._h)
 
+    def kernel_time(self, reps=50):
+        """(ms, bytes) of 1 launch of the finest Chebyshev step over all right sides."""
+        ms, nb = C.c_double(), C.c_double()
+        L.check(L.lib().femgpu_batch_kernel_time(self._h, reps, C.byref(ms), C.byref(nb)))
+        return ms.value, nb.value
+
     def stream(self):
         return L.lib().femgpu_batch_stream(self._h)
 

@@ -1,23 +1,29 @@
 // Batched solves: many small systems of uneven sizes, each with several right sides, in 1 set
 // of launches (no counterpart in the reference, whose callers solve 1 model at a time).
 //
-// The systems are combined level by level into block-diagonal operators: each system keeps the
-// reference's own hierarchy (plane coarsening and Galerkin products, multigrid.rs:84-139, down
-// to `coarsest` unknowns), the shallower hierarchies are padded with identity transfers to a
-// common depth, and the deepest level is solved by a dense inverse per system. So 1 launch of
-// each V-cycle kernel covers every system. The right sides are interleaved, R per row
-// (x[row * R + col]): the R threads of a row share each matrix entry, so 1 read of the
-// operator serves all R solves. Every (system, right side) pair, a segment, is its own
-// conjugate gradient solve with its own scalars and stopping test (multigrid.rs:692-753; the
-// flexible form with the FP32 cycle); the sums of each segment are reduced over chunks of rows
-// that never cross a system, in a fixed order, so a result does not depend on the timing. The
-// iteration is 1 CUDA graph body under a WHILE node that runs until every segment has stopped.
+// Each system, a member, keeps the reference's own hierarchy (plane coarsening and Galerkin
+// products, multigrid.rs:84-139, down to `coarsest` unknowns). Inside the batch the members are
+// ordered by depth, deepest first, so that the members that have a level l form a prefix of the
+// order, and those that go on below l a shorter prefix. Level l is then 1 vector over the
+// members that have it: first the rows of the members that smooth at l and go on (1
+// block-diagonal SELL operator, 1 launch of each smoothing kernel for all of them), then the
+// rows of the members whose deepest level l is, solved by a dense inverse each. The right sides
+// are interleaved, R per row (x[row * R + col]): the R threads of a row share each matrix entry,
+// so 1 read of the operator serves all R solves. Every (member, right side) pair, a segment, is
+// its own conjugate gradient solve with its own scalars and stopping test (multigrid.rs:692-753;
+// the flexible form with the FP32 cycle); the sums of each segment are reduced over chunks of
+// rows that never cross a member, in a fixed order, so a result does not depend on the timing.
+// The iteration is 1 CUDA graph body under a WHILE node that runs until every segment has
+// stopped. The caller's vectors are in the caller's member order; they are permuted into the
+// batch's order at the start of a solve and back at the end.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <numeric>
 #include <thread>
+#include <type_traits>
 
 #include "common.cuh"
 #include "hierarchy.hpp"
@@ -26,6 +32,8 @@
 namespace femgpu {
 
 constexpr int BTH = 256;
+constexpr int DTH = 128;  // rows of a dense tile
+constexpr int DJ = 64;    // right-side rows staged in shared memory at a time
 
 // ------------------------------------------------------------------ operator with R columns
 // (A x)[row][col] for the SELL matrix A and the column `col` of the interleaved x.
@@ -106,31 +114,68 @@ __global__ void k_bgather(int64_t rows, const int64_t* __restrict__ ptr,
         out[t] = s;
 }
 
-// The deepest level: out = inv_b in for the rows of system b (1 block per system).
+// The members whose deepest level this is: out = M in for each, M its (symmetric) inverse. A
+// block takes DTH rows i of 1 member; thread i reads M[j][i] = M[i][j] for j = 0, 1, ..., so
+// a warp reads 32 consecutive entries of a row of M at a time, and the right sides of DJ rows
+// j at a time sit in shared memory, read by all threads at once.
 template <class T, int R>
-__global__ void k_bdense(const int64_t* __restrict__ off, const int64_t* __restrict__ ioff,
-                         const T* __restrict__ inv, const T* __restrict__ in, T* __restrict__ out) {
-    const int b = blockIdx.x;
-    const int64_t r0 = off[b], m = off[b + 1] - r0;
-    const T* M = inv + ioff[b];
-    for (int64_t t = threadIdx.x; t < m * R; t += blockDim.x) {
-        const int64_t i = t / R;
-        const int col = (int)(t % R);
-        T s = 0;
-        for (int64_t j = 0; j < m; ++j) s += M[i * m + j] * in[(r0 + j) * R + col];
-        out[(r0 + i) * R + col] = s;
+__global__ void __launch_bounds__(DTH)
+    k_bdense(const int2* __restrict__ tiles, const int64_t* __restrict__ off,
+             const int64_t* __restrict__ ioff, const T* __restrict__ inv,
+             const T* __restrict__ in, T* __restrict__ out) {
+    __shared__ T s_in[DJ * R];
+    const int2 tl = tiles[blockIdx.x];
+    const int64_t r0 = off[tl.x], m = off[tl.x + 1] - r0;
+    const T* __restrict__ M = inv + ioff[tl.x];
+    const int64_t i = tl.y + threadIdx.x;
+    T acc[R];
+#pragma unroll
+    for (int c = 0; c < R; ++c) acc[c] = 0;
+    for (int64_t j0 = 0; j0 < m; j0 += DJ) {
+        const int jn = (int)min((int64_t)DJ, m - j0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < jn * R; t += DTH) s_in[t] = in[(r0 + j0) * R + t];
+        __syncthreads();
+        if (i < m) {
+#pragma unroll 4
+            for (int jj = 0; jj < jn; ++jj) {
+                const T mv = __ldg(M + (j0 + jj) * m + i);
+#pragma unroll
+                for (int c = 0; c < R; ++c) acc[c] += mv * s_in[jj * R + c];
+            }
+        }
+    }
+    if (i < m) {
+#pragma unroll
+        for (int c = 0; c < R; ++c) out[(r0 + i) * R + c] = acc[c];
     }
 }
 
+// out[row] = in[map[row]] (gather) or out[map[row]] = in[row] (scatter), R columns: the
+// caller's member order to the batch's and back.
+template <int R>
+__global__ void k_bpermute(int64_t n, const int* __restrict__ map, const double* __restrict__ in,
+                           double* __restrict__ out, int scatter) {
+    const int64_t t = elem_of_thread();
+    if (t >= n * R) return;
+    const int64_t row = t / R;
+    const int col = (int)(t % R);
+    const int64_t other = (int64_t)map[row] * R + col;
+    if (scatter)
+        out[other] = in[t];
+    else
+        out[t] = in[other];
+}
+
 // ------------------------------------------------------------------ PCG over segments
-// A block of the PCG kernels takes 1 chunk: rows [row0, row1) of system `sys`. Thread t takes
+// A block of the PCG kernels takes 1 chunk: rows [row0, row1) of member `sys`. Thread t takes
 // column t % R and rows row0 + t / R, row0 + t / R + BTH / R, ...
 struct Chunk {
     int sys;
     int row0, row1;
 };
 
-// The per-segment scalars (arrays of B R; segment s = system s / R, right side s % R).
+// The per-segment scalars (arrays of B R; segment s = member s / R, right side s % R).
 struct BatchScalars {
     double *bb, *rr, *rz, *pq, *alpha, *beta, *truth;
     int *done, *iters, *status;  // status: 0 running or converged, 1 iteration limit, 2 NaN
@@ -269,23 +314,38 @@ __global__ void k_bzero_empty(const Chunk* __restrict__ chunks, const double* __
 enum FinishKind { FIN_START = 0, FIN_PQ = 1, FIN_UPDATE = 2, FIN_DOTS = 3, FIN_TRUTH = 4,
                   FIN_RESTART = 5 };
 
-// The sums of each segment over the chunks of its system (in chunk order), then its scalars.
-// FIN_START: the first residual (stop at once if |r| <= tol |b| or b = 0, multigrid.rs:
-// 704-723); FIN_PQ: alpha; FIN_UPDATE: the stopping test and the iteration limit (multigrid.rs:
-// 721-733); FIN_DOTS: beta; FIN_TRUTH: the true residual |b - A x| / |b|; FIN_RESTART: the
-// segments whose true residual drifted above tol run again from x (iterative refinement).
+// 1 block per member: the sums of each of its R segments over the member's chunks (a fixed
+// tree), then the segment's scalars. FIN_START: the first residual (stop at once if
+// |r| <= tol |b| or b = 0, multigrid.rs:704-723); FIN_PQ: alpha; FIN_UPDATE: the stopping test
+// and the iteration limit (multigrid.rs:721-733); FIN_DOTS: beta; FIN_TRUTH: the true residual
+// |b - A x| / |b|; FIN_RESTART: the segments whose true residual drifted above tol run again
+// from x (iterative refinement).
 template <int R>
-__global__ void k_bfinish(int kind, int nseg, const int* __restrict__ cstart,
-                          const double* __restrict__ partial, BatchScalars sc, double tol,
-                          int max_iter, int flexible, int init) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nseg) return;
-    const int sys = s / R, col = s % R;
+__global__ void __launch_bounds__(BTH)
+    k_bfinish(int kind, const int* __restrict__ cstart, const double* __restrict__ partial,
+              BatchScalars sc, double tol, int max_iter, int flexible, int init) {
+    __shared__ double sa[BTH], sb[BTH];
+    const int sys = blockIdx.x;
+    const int col = threadIdx.x % R, lane = threadIdx.x / R;
     double a = 0, b = 0;
-    for (int c = cstart[sys]; c < cstart[sys + 1]; ++c) {
+    for (int c = cstart[sys] + lane; c < cstart[sys + 1]; c += BTH / R) {
         a += partial[((int64_t)c * R + col) * 2];
         b += partial[((int64_t)c * R + col) * 2 + 1];
     }
+    sa[threadIdx.x] = a;
+    sb[threadIdx.x] = b;
+    __syncthreads();
+    for (int st = (BTH / R) / 2; st > 0; st >>= 1) {
+        if (lane < st) {
+            sa[threadIdx.x] += sa[threadIdx.x + st * R];
+            sb[threadIdx.x] += sb[threadIdx.x + st * R];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x >= R) return;
+    a = sa[threadIdx.x];
+    b = sb[threadIdx.x];
+    const int s = sys * R + col;
     switch (kind) {
         case FIN_START:
             sc.bb[s] = a;
@@ -365,24 +425,24 @@ struct SystemHierarchy {
     std::vector<HostRect> ps;
 };
 
+// Level l: rows [0, ns) of the members that smooth here and go on to level l + 1, then rows
+// [ns, n) of the members whose deepest level this is.
 template <class T>
 struct BatchLevel {
-    int64_t n = 0, nc = 0;
-    Sell<T> A;
-    DevBuf<T> dinv;
-    DevBuf<int64_t> pptr, rptr;
+    int64_t n = 0, ns = 0, nc = 0;  // rows, smoothed rows, rows of the next level
+    Sell<T> A;                       // ns rows
+    DevBuf<T> dinv;                  // ns
+    DevBuf<int64_t> pptr, rptr;      // P: ns x nc, R = P^T: nc x ns
     DevBuf<uint32_t> pidx, ridx;
     DevBuf<T> pval, rval;
-    DevBuf<T> b, xa, xb, d, r;
+    DevBuf<T> b, xa, xb;             // n R
+    DevBuf<T> d, r;                  // ns R
     std::vector<double> c1, c2;
     double lambda = 0;
-};
-
-template <class T>
-struct BatchCoarse {
-    int64_t n = 0;
-    DevBuf<int64_t> off, ioff;
-    DevBuf<T> inv, b, x;
+    int ndense = 0, ntiles = 0;
+    DevBuf<int64_t> doff, dioff;     // ndense + 1: first row (in the level), first inverse entry
+    DevBuf<int2> tiles;              // (dense member, first row of the tile)
+    DevBuf<T> inv;
 };
 
 class BatchImpl {
@@ -396,19 +456,22 @@ class BatchImpl {
     void solve_host(const double* h_b, double* h_x, const volatile int* cancel,
                     femgpu_batch_stats* st);
     void set_max_iter(int m) { max_iter_ = m; }
+    // Per segment in the caller's member order.
     void segments(size_t* iterations, double* truth, double* residual, int* status) const;
     const std::vector<int64_t>& offsets() const { return offsets_; }
     std::vector<int64_t> level_sizes() const { return sizes_; }
     size_t bytes() const;
     cudaStream_t stream() const { return s_; }
+    // The mean device time (ms) of 1 launch of the finest level's Chebyshev step over all
+    // right sides, and its algorithmic bytes.
+    void kernel_time(int reps, double* ms, double* bytes);
     double tol = 1e-10;  // PCG_TOL, solve.rs:42
 
    private:
     template <class T>
-    void build_levels(std::vector<SystemHierarchy>& H, size_t depth,
-                      std::vector<BatchLevel<T>>* levels, BatchCoarse<T>* coarse);
+    void build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchLevel<T>>* levels);
     template <class T, int R>
-    const T* vcycle(std::vector<BatchLevel<T>>& Ls, BatchCoarse<T>& Cc, size_t l, const T* b);
+    const T* vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b);
     template <int R>
     void finish(int kind, int init);
     template <int R>
@@ -417,6 +480,8 @@ class BatchImpl {
     void iteration();
     template <int R>
     void run(const volatile int* cancel);
+    void permute(const double* in, double* out, int scatter);
+    void solve_loaded(const volatile int* cancel, femgpu_batch_stats* st);
     void launch_loop(const volatile int* cancel);
     bool any_running();
     void collect(femgpu_batch_stats* st);
@@ -430,18 +495,18 @@ class BatchImpl {
     Options opt_;
     int B_ = 0, R_ = 1, nchunks_ = 0, max_iter_ = 500, graph_max_iter_ = -1;
     int64_t n_ = 0;
-    std::vector<int64_t> offsets_, sizes_;
-    Sell<double> A64_;  // the block-diagonal finest matrix, exactly
+    std::vector<int64_t> offsets_, sizes_;  // the caller's member order
+    std::vector<int> order_;                // batch position -> caller's member
+    DevBuf<int> map_;                       // batch row -> caller's row
+    Sell<double> A64_;  // the block-diagonal finest matrix (batch order), exactly
     std::vector<BatchLevel<float>> L32_;
     std::vector<BatchLevel<double>> L64_;
-    BatchCoarse<float> C32_;
-    BatchCoarse<double> C64_;
     DevBuf<char> chunks_;
     DevBuf<int> cstart_;
     DevBuf<double> partial_;
     DevBuf<double> bb_, rr_, rz_, pq_, alpha_, beta_, truth_;
     DevBuf<int> done_, iters_, status_, loops_;
-    DevBuf<double> x_, r_, p_, q_, b_;
+    DevBuf<double> x_, r_, p_, q_, b_, stage_;
     DevBuf<float> r32_;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t exec_ = nullptr;
@@ -456,18 +521,7 @@ class BatchImpl {
 
 namespace {
 
-HostRect identity(int64_t n) {
-    HostRect p;
-    p.rows = p.cols = n;
-    p.ptr.resize(n + 1);
-    p.idx.resize(n);
-    p.val.assign(n, 1.0);
-    for (int64_t i = 0; i <= n; ++i) p.ptr[i] = i;
-    for (int64_t i = 0; i < n; ++i) p.idx[i] = (uint32_t)i;
-    return p;
-}
-
-// The block-diagonal matrix of the systems' matrices.
+// The block-diagonal matrix of the members' matrices.
 HostCsr combine(const std::vector<const HostCsr*>& parts) {
     HostCsr out;
     int64_t n = 0, nnz = 0;
@@ -495,7 +549,7 @@ HostCsr combine(const std::vector<const HostCsr*>& parts) {
     return out;
 }
 
-// The block-diagonal transfer of the systems' transfers.
+// The block-diagonal transfer of the members' transfers.
 HostRect combine_rect(const std::vector<const HostRect*>& parts) {
     HostRect out;
     for (auto* p : parts) {
@@ -547,7 +601,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     R_ = nrhs;
     B_ = (int)a.size();
     if (B_ < 1) throw Failure(FEMGPU_ERR_INVALID, "an empty batch");
-    // Each system's hierarchy on the host (multigrid.rs:84-139), the systems shared among the
+    // Each member's hierarchy on the host (multigrid.rs:84-139), the members shared among the
     // host threads.
     std::vector<HostCsr> fine(B_);
     for (int b = 0; b < B_; ++b) {
@@ -609,45 +663,44 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     for (int b = 0; b < B_; ++b)
         if (codes[b] != FEMGPU_OK)
             throw Failure(codes[b], "system " + std::to_string(b) + ": " + errors[b]);
-    // Pad to the common depth: a level past a system's own repeats its deepest matrix, with the
-    // identity as the transfer.
-    size_t depth = 0;
-    for (auto& h : H) depth = std::max(depth, h.mats.size());
-    for (auto& h : H)
-        while (h.mats.size() < depth) {
-            HostCsr last = h.mats.back();
-            h.ps.push_back(identity(last.n));
-            h.mats.push_back(std::move(last));
-        }
+    // The caller's row offsets, then the batch order: deepest first (stable).
     offsets_.assign(B_ + 1, 0);
     for (int b = 0; b < B_; ++b) offsets_[b + 1] = offsets_[b] + H[b].mats[0].n;
     n_ = offsets_[B_];
     if (n_ * R_ >= 0x7fffffff)
         throw Failure(FEMGPU_ERR_TOO_LARGE, "a batch of 2^31 values or more per vector");
+    order_.resize(B_);
+    std::iota(order_.begin(), order_.end(), 0);
+    std::stable_sort(order_.begin(), order_.end(),
+                     [&](int x, int y) { return H[x].mats.size() > H[y].mats.size(); });
+    std::vector<SystemHierarchy> Hs(B_);
+    for (int k = 0; k < B_; ++k) Hs[k] = std::move(H[order_[k]]);
+    std::vector<int> map(n_);
+    std::vector<int64_t> boff(B_ + 1, 0);  // the batch order's row offsets
+    for (int k = 0; k < B_; ++k) {
+        const int64_t m = Hs[k].mats[0].n;
+        boff[k + 1] = boff[k] + m;
+        for (int64_t i = 0; i < m; ++i) map[boff[k] + i] = (int)(offsets_[order_[k]] + i);
+    }
+    map_.upload(map.data(), map.size(), s_);
     // The exact finest operator (FP64) of the PCG loop and the true residual.
     {
         std::vector<const HostCsr*> parts;
-        for (auto& h : H) parts.push_back(&h.mats[0]);
+        for (auto& h : Hs) parts.push_back(&h.mats[0]);
         HostCsr f = combine(parts);
         DevCsr d;
         upload_csr(f, &d, s_);
         make_sell<double>(d, 32, &A64_, s_);
         FG_CUDA(cudaStreamSynchronize(s_));
     }
-    sizes_.clear();
-    for (size_t l = 0; l < depth; ++l) {
-        int64_t s = 0;
-        for (auto& h : H) s += h.mats[l].n;
-        sizes_.push_back(s);
-    }
-    // The chunks of the PCG kernels: up to 4 rows per thread, rows of 1 system each.
+    // The chunks of the PCG kernels: up to 4 rows per thread, rows of 1 member each.
     const int chunk_rows = 4 * BTH / R_;
     std::vector<Chunk> ch;
     std::vector<int> cstart(B_ + 1, 0);
-    for (int b = 0; b < B_; ++b) {
-        cstart[b] = (int)ch.size();
-        for (int64_t r = offsets_[b]; r < offsets_[b + 1]; r += chunk_rows)
-            ch.push_back({b, (int)r, (int)std::min<int64_t>(r + chunk_rows, offsets_[b + 1])});
+    for (int k = 0; k < B_; ++k) {
+        cstart[k] = (int)ch.size();
+        for (int64_t r = boff[k]; r < boff[k + 1]; r += chunk_rows)
+            ch.push_back({k, (int)r, (int)std::min<int64_t>(r + chunk_rows, boff[k + 1])});
     }
     cstart[B_] = (int)ch.size();
     nchunks_ = (int)ch.size();
@@ -658,146 +711,171 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     // The block sums: of the chunks (R columns, 2 values) and of the power iteration.
     partial_.alloc(std::max(2 * (size_t)nchunks_ * R_, 2 * (size_t)(n_ / BTH + 64)));
     if (opt_.precision == FEMGPU_MIXED)
-        build_levels<float>(H, depth, &L32_, &C32_);
+        build_levels<float>(Hs, &L32_);
     else
-        build_levels<double>(H, depth, &L64_, &C64_);
+        build_levels<double>(Hs, &L64_);
     const size_t S = (size_t)B_ * R_;
     for (auto* v : {&bb_, &rr_, &rz_, &pq_, &alpha_, &beta_, &truth_}) v->alloc(S);
     for (auto* v : {&done_, &iters_, &status_}) v->alloc(S);
     loops_.alloc(1);
-    for (auto* v : {&x_, &r_, &p_, &q_, &b_}) v->alloc((size_t)n_ * R_);
+    for (auto* v : {&x_, &r_, &p_, &q_, &b_, &stage_}) v->alloc((size_t)n_ * R_);
     if (opt_.precision == FEMGPU_MIXED) r32_.alloc((size_t)n_ * R_);
     FG_CUDA(cudaStreamSynchronize(s_));
 }
 
 template <class T>
-void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, size_t depth,
-                             std::vector<BatchLevel<T>>* levels, BatchCoarse<T>* coarse) {
-    levels->resize(depth - 1);
+void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchLevel<T>>* levels) {
+    const size_t depth = H[0].mats.size();  // the deepest member comes first
+    levels->resize(depth);
     const int deg = opt_.degree > 0 ? opt_.degree : 2;
     const double lower = opt_.lower > 0 ? opt_.lower : 0.3;
-    for (size_t l = 0; l + 1 < depth; ++l) {
+    sizes_.clear();
+    for (size_t l = 0; l < depth; ++l) {
         BatchLevel<T>& L = (*levels)[l];
-        std::vector<const HostCsr*> mats;
-        std::vector<const HostRect*> ps;
-        for (auto& h : H) {
-            mats.push_back(&h.mats[l]);
-            ps.push_back(&h.ps[l]);
+        // Members [0, S) smooth at l and go on; [S, K) end at l (the order is by depth).
+        int K = 0, S = 0;
+        while (K < B_ && H[K].mats.size() > l) ++K;
+        while (S < K && H[S].mats.size() > l + 1) ++S;
+        for (int k = 0; k < K; ++k) L.n += H[k].mats[l].n;
+        for (int k = 0; k < S; ++k) L.ns += H[k].mats[l].n;
+        sizes_.push_back(L.n);
+        if (S > 0) {
+            std::vector<const HostCsr*> mats;
+            std::vector<const HostRect*> ps;
+            for (int k = 0; k < S; ++k) {
+                mats.push_back(&H[k].mats[l]);
+                ps.push_back(&H[k].ps[l]);
+            }
+            HostCsr A = combine(mats);
+            HostRect P = combine_rect(ps);
+            DevCsr d;
+            upload_csr(A, &d, s_);
+            make_sell<T>(d, 32, &L.A, s_);
+            // The diagonal, and lambda_max of the block-diagonal D^-1 A: the largest of the
+            // members'.
+            std::vector<double> dg(A.n, 0.0), inv(A.n);
+            for (int64_t i = 0; i < A.n; ++i)
+                for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
+                    if ((int64_t)A.idx[k] == i) dg[i] = A.val[k];
+            for (int64_t i = 0; i < A.n; ++i) {
+                if (!(dg[i] > 0.0))
+                    throw Failure(FEMGPU_ERR_NOT_SPD,
+                                  "the matrix is not positive definite: it has a diagonal entry "
+                                  "that is not above 0");
+                inv[i] = 1.0 / dg[i];
+            }
+            Operator<double> op;
+            op.n = A.n;
+            op.nnz = A.nnz();
+            make_sell<double>(d, 32, &op.sell, s_);
+            DevBuf<double> ddg;
+            ddg.upload(dg.data(), A.n, s_);
+            L.lambda = lambda_max(op, ddg.p, s_, partial_);
+            chebyshev(L.lambda, deg, lower, &L.c1, &L.c2);
+            std::vector<T> tv(inv.begin(), inv.end());
+            L.dinv.upload(tv.data(), tv.size(), s_);
+            HostRect Rt = transpose(P);
+            L.nc = P.cols;
+            L.pptr.upload(P.ptr.data(), P.rows + 1, s_);
+            L.pidx.upload(P.idx.data(), P.idx.size(), s_);
+            std::vector<T> pv(P.val.begin(), P.val.end()), rv(Rt.val.begin(), Rt.val.end());
+            L.pval.upload(pv.data(), pv.size(), s_);
+            L.rptr.upload(Rt.ptr.data(), Rt.rows + 1, s_);
+            L.ridx.upload(Rt.idx.data(), Rt.idx.size(), s_);
+            L.rval.upload(rv.data(), rv.size(), s_);
+            L.d.alloc((size_t)L.ns * R_);
+            L.r.alloc((size_t)L.ns * R_);
         }
-        HostCsr A = combine(mats);
-        HostRect P = combine_rect(ps);
-        L.n = A.n;
-        DevCsr d;
-        upload_csr(A, &d, s_);
-        make_sell<T>(d, 32, &L.A, s_);
-        // The diagonal, and lambda_max of the block-diagonal D^-1 A: the largest of the
-        // systems'.
-        std::vector<double> dg(A.n, 0.0), inv(A.n);
-        for (int64_t i = 0; i < A.n; ++i)
-            for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
-                if ((int64_t)A.idx[k] == i) dg[i] = A.val[k];
-        for (int64_t i = 0; i < A.n; ++i) {
-            if (!(dg[i] > 0.0))
-                throw Failure(FEMGPU_ERR_NOT_SPD,
-                              "the matrix is not positive definite: it has a diagonal entry that "
-                              "is not above 0");
-            inv[i] = 1.0 / dg[i];
+        // The members that end here: a dense inverse each, from a dense Cholesky factor on the
+        // device, made exactly symmetric (the kernel reads it by columns).
+        L.ndense = K - S;
+        if (L.ndense > 0) {
+            std::vector<int64_t> off(L.ndense + 1), ioff(L.ndense + 1, 0);
+            std::vector<int2> tiles;
+            off[0] = L.ns;
+            for (int j = 0; j < L.ndense; ++j) {
+                const int64_t m = H[S + j].mats[l].n;
+                off[j + 1] = off[j] + m;
+                ioff[j + 1] = ioff[j] + m * m;
+                for (int64_t t = 0; t < m; t += DTH) tiles.push_back({j, (int)t});
+            }
+            L.ntiles = (int)tiles.size();
+            L.inv.alloc(ioff[L.ndense]);
+            for (int j = 0; j < L.ndense; ++j) {
+                const int64_t m = off[j + 1] - off[j];
+                DevBuf<double> inv64;
+                dense_inverse(H[S + j].mats[l], &inv64, s_);
+                std::vector<double> h((size_t)(m * m));
+                inv64.download(h.data(), m * m, s_);
+                FG_CUDA(cudaStreamSynchronize(s_));
+                std::vector<T> t((size_t)(m * m));
+                for (int64_t r = 0; r < m; ++r)
+                    for (int64_t c = 0; c < m; ++c)
+                        t[r * m + c] = (T)(0.5 * (h[r * m + c] + h[c * m + r]));
+                FG_CUDA(cudaMemcpyAsync(L.inv.p + ioff[j], t.data(), m * m * sizeof(T),
+                                        cudaMemcpyHostToDevice, s_));
+                FG_CUDA(cudaStreamSynchronize(s_));
+            }
+            L.doff.upload(off.data(), off.size(), s_);
+            L.dioff.upload(ioff.data(), ioff.size(), s_);
+            L.tiles.upload(tiles.data(), tiles.size(), s_);
         }
-        Operator<double> op;
-        op.n = A.n;
-        op.nnz = A.nnz();
-        make_sell<double>(d, 32, &op.sell, s_);
-        DevBuf<double> ddg;
-        ddg.upload(dg.data(), A.n, s_);
-        L.lambda = lambda_max(op, ddg.p, s_, partial_);
-        chebyshev(L.lambda, deg, lower, &L.c1, &L.c2);
-        std::vector<T> tv(inv.begin(), inv.end());
-        L.dinv.upload(tv.data(), tv.size(), s_);
-        HostRect Rt = transpose(P);
-        L.nc = P.cols;
-        L.pptr.upload(P.ptr.data(), P.rows + 1, s_);
-        L.pidx.upload(P.idx.data(), P.idx.size(), s_);
-        std::vector<T> pv(P.val.begin(), P.val.end()), rv(Rt.val.begin(), Rt.val.end());
-        L.pval.upload(pv.data(), pv.size(), s_);
-        L.rptr.upload(Rt.ptr.data(), Rt.rows + 1, s_);
-        L.ridx.upload(Rt.idx.data(), Rt.idx.size(), s_);
-        L.rval.upload(rv.data(), rv.size(), s_);
-        for (auto* v : {&L.b, &L.xa, &L.xb, &L.d, &L.r}) v->alloc((size_t)A.n * R_);
+        for (auto* v : {&L.b, &L.xa, &L.xb}) v->alloc((size_t)L.n * R_);
         FG_CUDA(cudaStreamSynchronize(s_));
     }
-    // The deepest level: a dense inverse per system, from a dense Cholesky factor on the device.
-    std::vector<int64_t> off(B_ + 1, 0), ioff(B_ + 1, 0);
-    for (int b = 0; b < B_; ++b) {
-        const int64_t m = H[b].mats[depth - 1].n;
-        off[b + 1] = off[b] + m;
-        ioff[b + 1] = ioff[b] + m * m;
-    }
-    coarse->n = off[B_];
-    coarse->inv.alloc(ioff[B_]);
-    for (int b = 0; b < B_; ++b) {
-        DevBuf<double> inv64;
-        dense_inverse(H[b].mats[depth - 1], &inv64, s_);
-        const int64_t mm = ioff[b + 1] - ioff[b];
-        std::vector<double> h(mm);
-        inv64.download(h.data(), mm, s_);
-        FG_CUDA(cudaStreamSynchronize(s_));
-        std::vector<T> t(h.begin(), h.end());
-        FG_CUDA(cudaMemcpyAsync(coarse->inv.p + ioff[b], t.data(), mm * sizeof(T),
-                                cudaMemcpyHostToDevice, s_));
-        FG_CUDA(cudaStreamSynchronize(s_));
-    }
-    coarse->off.upload(off.data(), off.size(), s_);
-    coarse->ioff.upload(ioff.data(), ioff.size(), s_);
-    coarse->b.alloc((size_t)coarse->n * R_);
-    coarse->x.alloc((size_t)coarse->n * R_);
-    FG_CUDA(cudaStreamSynchronize(s_));
 }
 
 // ------------------------------------------------------------------ the cycle and the loop
 // The V-cycle from level l on the right sides b; returns where the correction is.
 template <class T, int R>
-const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, BatchCoarse<T>& Cc, size_t l,
-                           const T* b) {
-    if (l == Ls.size()) {
-        k_bdense<T, R><<<B_, BTH, 0, s_>>>(Cc.off.p, Cc.ioff.p, Cc.inv.p, b, Cc.x.p);
-        FG_CHECK_LAUNCH();
-        launches_ += 1;
-        return Cc.x.p;
-    }
+const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b) {
     BatchLevel<T>& L = Ls[l];
-    const int g = (int)((L.n * R + BTH - 1) / BTH);
     T* xa = L.xa.p;
     T* xb = L.xb.p;
-    const int deg = (int)L.c1.size();
-    k_bcheb_first<T, R><<<g, BTH, 0, s_>>>(L.n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa);
-    for (int k = 1; k < deg; ++k) {
-        k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k],
-                                              (T)L.c2[k], L.d.p, xb);
-        std::swap(xa, xb);
+    if (L.ns > 0) {
+        const int g = (int)((L.ns * R + BTH - 1) / BTH);
+        const int deg = (int)L.c1.size();
+        k_bcheb_first<T, R><<<g, BTH, 0, s_>>>(L.ns, b, L.dinv.p, (T)L.c1[0], L.d.p, xa);
+        for (int k = 1; k < deg; ++k) {
+            k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k],
+                                                  (T)L.c2[k], L.d.p, xb);
+            std::swap(xa, xb);
+        }
+        k_bresidual<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.r.p);
+        T* bc = Ls[l + 1].b.p;
+        const int gc = (int)((L.nc * R + BTH - 1) / BTH);
+        k_bgather<T, R><<<gc, BTH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p, bc, 0);
+        FG_CHECK_LAUNCH();
+        launches_ += deg + 2;
+        const T* ec = vcycle<T, R>(Ls, l + 1, bc);
+        k_bgather<T, R><<<g, BTH, 0, s_>>>(L.ns, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, 1);
+        for (int k = 0; k < deg; ++k) {
+            k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k],
+                                                  (T)L.c2[k], L.d.p, xb);
+            std::swap(xa, xb);
+        }
+        FG_CHECK_LAUNCH();
+        launches_ += deg + 1;
     }
-    k_bresidual<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.r.p);
-    T* bc = l + 1 == Ls.size() ? Cc.b.p : Ls[l + 1].b.p;
-    const int gc = (int)((L.nc * R + BTH - 1) / BTH);
-    k_bgather<T, R><<<gc, BTH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p, bc, 0);
-    FG_CHECK_LAUNCH();
-    launches_ += deg + 2;
-    const T* ec = vcycle<T, R>(Ls, Cc, l + 1, bc);
-    k_bgather<T, R><<<g, BTH, 0, s_>>>(L.n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, 1);
-    for (int k = 0; k < deg; ++k) {
-        k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k],
-                                              (T)L.c2[k], L.d.p, xb);
-        std::swap(xa, xb);
+    if (L.ndense > 0) {
+        k_bdense<T, R><<<L.ntiles, DTH, 0, s_>>>(L.tiles.p, L.doff.p, L.dioff.p, L.inv.p, b, xa);
+        FG_CHECK_LAUNCH();
+        launches_ += 1;
     }
-    FG_CHECK_LAUNCH();
-    launches_ += deg + 1;
     return xa;
 }
 
+// The recurrence's stopping target. The mixed form promises the true FP64 residual at tol, and a
+// segment whose recurrence stops just under tol may sit a rounding drift (a few parts in 1000)
+// above it and need a restart, which re-runs the whole batch's cycle for a few segments; the
+// recurrence of the mixed form therefore stops at 0.98 tol. The FP64 form stops at tol on the
+// recurrence as the reference does (multigrid.rs:721-723).
 template <int R>
 void BatchImpl::finish(int kind, int init) {
-    const int S = B_ * R;
-    k_bfinish<R><<<(S + 127) / 128, 128, 0, s_>>>(kind, S, cstart_.p, partial_.p, scalars(), tol,
-                                                  max_iter_, opt_.precision == FEMGPU_MIXED, init);
+    const bool mixed = opt_.precision == FEMGPU_MIXED;
+    const double target = (mixed && kind != FIN_RESTART) ? 0.98 * tol : tol;
+    k_bfinish<R><<<B_, BTH, 0, s_>>>(kind, cstart_.p, partial_.p, scalars(), target, max_iter_,
+                                     mixed, init);
     FG_CHECK_LAUNCH();
     launches_ += 1;
 }
@@ -807,13 +885,13 @@ template <int R>
 void BatchImpl::precondition_and_dots(int init) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     if (mixed) {
-        const float* z = vcycle<float, R>(L32_, C32_, 0, r32_.p);
+        const float* z = vcycle<float, R>(L32_, 0, r32_.p);
         k_bpcg_dots<R, float><<<nchunks_, BTH, 0, s_>>>(chunks(), r_.p, z, q_.p, 1, init,
                                                         done_.p, partial_.p);
         finish<R>(FIN_DOTS, init);
         k_bpcg_p<R, float><<<nchunks_, BTH, 0, s_>>>(chunks(), z, p_.p, scalars(), init);
     } else {
-        const double* z = vcycle<double, R>(L64_, C64_, 0, r_.p);
+        const double* z = vcycle<double, R>(L64_, 0, r_.p);
         k_bpcg_dots<R, double><<<nchunks_, BTH, 0, s_>>>(chunks(), r_.p, z, q_.p, 0, init,
                                                          done_.p, partial_.p);
         finish<R>(FIN_DOTS, init);
@@ -871,9 +949,9 @@ void BatchImpl::launch_loop(const volatile int* cancel) {
 template <int R>
 void BatchImpl::run(const volatile int* cancel) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
-    launches_ = 0;
     restarts_ = 0;
     if (!exec_) {
+        const size_t before = launches_;
         FG_CUDA(cudaGraphCreate(&graph_, 0));
         FG_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault));
         cudaGraphNodeParams cp{};
@@ -890,10 +968,10 @@ void BatchImpl::run(const volatile int* cancel) {
         k_bloop_control<<<1, BTH, 0, s_>>>(cond_, done_.p, B_ * R, d_cancel_, loops_.p);
         FG_CUDA(cudaStreamEndCapture(s_, &body));
         FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
-        graph_kernels_ = launches_ + 1;
+        graph_kernels_ = launches_ - before + 1;
         graph_max_iter_ = max_iter_;
         graph_tol_ = tol;
-        launches_ = 0;
+        launches_ = before;
     }
     FG_CUDA(cudaMemsetAsync(loops_.p, 0, sizeof(int), s_));
     // r = b - A x and the first test (multigrid.rs:692-723), x = 0 where b = 0, then
@@ -923,6 +1001,29 @@ void BatchImpl::run(const volatile int* cancel) {
     }
 }
 
+void BatchImpl::permute(const double* in, double* out, int scatter) {
+    const int64_t e = n_ * R_;
+    const int g = (int)((e + BTH - 1) / BTH);
+    if (R_ == 16)
+        k_bpermute<16><<<g, BTH, 0, s_>>>(n_, map_.p, in, out, scatter);
+    else if (R_ == 4)
+        k_bpermute<4><<<g, BTH, 0, s_>>>(n_, map_.p, in, out, scatter);
+    else
+        k_bpermute<1><<<g, BTH, 0, s_>>>(n_, map_.p, in, out, scatter);
+    FG_CHECK_LAUNCH();
+    launches_ += 1;
+}
+
+// The solve on b_ and x_ (the batch's order), already loaded.
+void BatchImpl::solve_loaded(const volatile int* cancel, femgpu_batch_stats* st) {
+    if (R_ == 16)
+        run<16>(cancel);
+    else if (R_ == 4)
+        run<4>(cancel);
+    else
+        run<1>(cancel);
+}
+
 void BatchImpl::solve_device(const double* d_b, double* d_x, const volatile int* cancel,
                              femgpu_batch_stats* st) {
     if (exec_ && (max_iter_ != graph_max_iter_ || tol != graph_tol_)) {
@@ -931,37 +1032,41 @@ void BatchImpl::solve_device(const double* d_b, double* d_x, const volatile int*
         exec_ = nullptr;
         graph_ = nullptr;
     }
-    const size_t bytes = (size_t)n_ * R_ * sizeof(double);
+    launches_ = 0;
     FG_CUDA(cudaEventRecord(ev0_, s_));
-    if (d_b != b_.p) FG_CUDA(cudaMemcpyAsync(b_.p, d_b, bytes, cudaMemcpyDeviceToDevice, s_));
-    if (d_x != x_.p) FG_CUDA(cudaMemcpyAsync(x_.p, d_x, bytes, cudaMemcpyDeviceToDevice, s_));
-    if (R_ == 16)
-        run<16>(cancel);
-    else if (R_ == 4)
-        run<4>(cancel);
-    else
-        run<1>(cancel);
-    if (d_x != x_.p) FG_CUDA(cudaMemcpyAsync(d_x, x_.p, bytes, cudaMemcpyDeviceToDevice, s_));
+    permute(d_b, b_.p, 0);
+    permute(d_x, x_.p, 0);
+    solve_loaded(cancel, st);
+    permute(x_.p, d_x, 1);
     FG_CUDA(cudaEventRecord(ev1_, s_));
     FG_CUDA(cudaStreamSynchronize(s_));
     if (cancel && *cancel) throw Failure(FEMGPU_ERR_CANCELLED, "cancelled");
     collect(st);
 }
 
+// Host vectors go through the batch's own staging vector, so a solve allocates nothing.
 void BatchImpl::solve_host(const double* h_b, double* h_x, const volatile int* cancel,
                            femgpu_batch_stats* st) {
     const size_t bytes = (size_t)n_ * R_ * sizeof(double);
-    FG_CUDA(cudaMemcpyAsync(b_.p, h_b, bytes, cudaMemcpyHostToDevice, s_));
-    FG_CUDA(cudaMemcpyAsync(x_.p, h_x, bytes, cudaMemcpyHostToDevice, s_));
-    try {
-        solve_device(b_.p, x_.p, cancel, st);
-    } catch (const Failure&) {
-        cudaMemcpyAsync(h_x, x_.p, bytes, cudaMemcpyDeviceToHost, s_);
-        cudaStreamSynchronize(s_);
-        throw;
+    if (exec_ && (max_iter_ != graph_max_iter_ || tol != graph_tol_)) {
+        cudaGraphExecDestroy(exec_);
+        cudaGraphDestroy(graph_);
+        exec_ = nullptr;
+        graph_ = nullptr;
     }
-    FG_CUDA(cudaMemcpyAsync(h_x, x_.p, bytes, cudaMemcpyDeviceToHost, s_));
+    launches_ = 0;
+    FG_CUDA(cudaEventRecord(ev0_, s_));
+    FG_CUDA(cudaMemcpyAsync(stage_.p, h_b, bytes, cudaMemcpyHostToDevice, s_));
+    permute(stage_.p, b_.p, 0);
+    FG_CUDA(cudaMemcpyAsync(stage_.p, h_x, bytes, cudaMemcpyHostToDevice, s_));
+    permute(stage_.p, x_.p, 0);
+    solve_loaded(cancel, st);
+    permute(x_.p, stage_.p, 1);
+    FG_CUDA(cudaMemcpyAsync(h_x, stage_.p, bytes, cudaMemcpyDeviceToHost, s_));
+    FG_CUDA(cudaEventRecord(ev1_, s_));
     FG_CUDA(cudaStreamSynchronize(s_));
+    if (cancel && *cancel) throw Failure(FEMGPU_ERR_CANCELLED, "cancelled");
+    collect(st);
 }
 
 void BatchImpl::segments(size_t* iterations, double* truth, double* residual,
@@ -975,12 +1080,15 @@ void BatchImpl::segments(size_t* iterations, double* truth, double* residual,
     rr_.download(rr.data(), S, s_);
     bb_.download(bb.data(), S, s_);
     FG_CUDA(cudaStreamSynchronize(s_));
-    for (int s = 0; s < S; ++s) {
-        if (iterations) iterations[s] = (size_t)it[s];
-        if (truth) truth[s] = tr[s];
-        if (residual) residual[s] = bb[s] > 0 ? std::sqrt(rr[s]) / std::sqrt(bb[s]) : 0.0;
-        if (status) status[s] = stt[s];
-    }
+    for (int k = 0; k < B_; ++k)
+        for (int c = 0; c < R_; ++c) {
+            const int s = k * R_ + c;           // the batch's segment
+            const int o = order_[k] * R_ + c;   // the caller's
+            if (iterations) iterations[o] = (size_t)it[s];
+            if (truth) truth[o] = tr[s];
+            if (residual) residual[o] = bb[s] > 0 ? std::sqrt(rr[s]) / std::sqrt(bb[s]) : 0.0;
+            if (status) status[o] = stt[s];
+        }
 }
 
 void BatchImpl::collect(femgpu_batch_stats* st) {
@@ -988,7 +1096,7 @@ void BatchImpl::collect(femgpu_batch_stats* st) {
     std::vector<size_t> it(S);
     std::vector<double> tr(S), res(S);
     std::vector<int> stt(S);
-    segments(it.data(), tr.data(), res.data(), stt.data());
+    segments(it.data(), tr.data(), res.data(), stt.data());  // the caller's order
     const int loops = fetch(loops_.p, s_);
     femgpu_batch_stats out{};
     size_t total = 0;
@@ -1027,18 +1135,61 @@ void BatchImpl::collect(femgpu_batch_stats* st) {
     }
 }
 
+void BatchImpl::kernel_time(int reps, double* ms, double* bytes) {
+    const bool mixed = opt_.precision == FEMGPU_MIXED;
+    const int64_t ns = mixed ? L32_[0].ns : L64_[0].ns;
+    if (ns == 0) throw Failure(FEMGPU_ERR_INVALID, "no member smooths at the finest level");
+    reps = std::max(1, reps);
+    auto go = [&](auto& L, auto r) {
+        using T = typename std::remove_reference<decltype(*L.dinv.p)>::type;
+        constexpr int R = decltype(r)::value;
+        const int g = (int)((L.ns * R + BTH - 1) / BTH);
+        for (int k = 0; k < reps + 5; ++k) {
+            if (k == 5) FG_CUDA(cudaEventRecord(ev0_, s_));
+            k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p, (T)0.5,
+                                                  (T)0.5, L.d.p, L.xb.p);
+        }
+        FG_CHECK_LAUNCH();
+        FG_CUDA(cudaEventRecord(ev1_, s_));
+        FG_CUDA(cudaEventSynchronize(ev1_));
+        float t = 0;
+        FG_CUDA(cudaEventElapsedTime(&t, ev0_, ev1_));
+        *ms = t / reps;
+        // Each value and index of the level once, and per right side b, x, d (read), d and
+        // x_out (written) and the row's D^-1.
+        *bytes = (double)L.A.bytes() - (double)L.A.slice_ptr.bytes() +
+                 (double)L.ns * sizeof(T) * (5.0 * R + 1.0);
+    };
+    auto pick = [&](auto& L) {
+        FG_CUDA(cudaMemsetAsync(L.xa.p, 0, L.xa.bytes(), s_));
+        FG_CUDA(cudaMemsetAsync(L.b.p, 0, L.b.bytes(), s_));
+        FG_CUDA(cudaMemsetAsync(L.d.p, 0, L.d.bytes(), s_));
+        if (R_ == 16)
+            go(L, std::integral_constant<int, 16>());
+        else if (R_ == 4)
+            go(L, std::integral_constant<int, 4>());
+        else
+            go(L, std::integral_constant<int, 1>());
+    };
+    if (mixed)
+        pick(L32_[0]);
+    else
+        pick(L64_[0]);
+}
+
 size_t BatchImpl::bytes() const {
-    size_t b = A64_.bytes() + partial_.bytes() + chunks_.bytes() + cstart_.bytes();
-    auto levels = [&](const auto& Ls, const auto& C) {
+    size_t b = A64_.bytes() + partial_.bytes() + chunks_.bytes() + cstart_.bytes() + map_.bytes();
+    auto levels = [&](const auto& Ls) {
         for (const auto& L : Ls)
             b += L.A.bytes() + L.dinv.bytes() + L.pptr.bytes() + L.rptr.bytes() + L.pidx.bytes() +
                  L.ridx.bytes() + L.pval.bytes() + L.rval.bytes() + L.b.bytes() + L.xa.bytes() +
-                 L.xb.bytes() + L.d.bytes() + L.r.bytes();
-        b += C.off.bytes() + C.ioff.bytes() + C.inv.bytes() + C.b.bytes() + C.x.bytes();
+                 L.xb.bytes() + L.d.bytes() + L.r.bytes() + L.doff.bytes() + L.dioff.bytes() +
+                 L.tiles.bytes() + L.inv.bytes();
     };
-    levels(L32_, C32_);
-    levels(L64_, C64_);
-    b += x_.bytes() + r_.bytes() + p_.bytes() + q_.bytes() + b_.bytes() + r32_.bytes();
+    levels(L32_);
+    levels(L64_);
+    b += x_.bytes() + r_.bytes() + p_.bytes() + q_.bytes() + b_.bytes() + stage_.bytes() +
+         r32_.bytes();
     return b;
 }
 
@@ -1158,6 +1309,13 @@ int femgpu_batch_segments(const femgpu_batch* b, size_t* iterations, double* tru
     return batch_guarded([&] {
         if (!b) throw Failure(FEMGPU_ERR_INVALID, "null batch");
         b->impl.segments(iterations, true_residual, residual, status);
+    });
+}
+
+int femgpu_batch_kernel_time(femgpu_batch* b, int reps, double* ms, double* bytes) {
+    return batch_guarded([&] {
+        if (!b || !ms || !bytes) throw Failure(FEMGPU_ERR_INVALID, "null argument");
+        b->impl.kernel_time(reps, ms, bytes);
     });
 }
 

@@ -328,6 +328,11 @@ int femgpu_batch_solve_device(femgpu_batch* b, const double* rhs, double* x,
  * recurrence residuals, status (0 converged, 1 iteration limit, 2 broke down). Any may be null. */
 int femgpu_batch_segments(const femgpu_batch* b, size_t* iterations, double* true_residual,
                           double* residual, int* status);
+/* Times `reps` back-to-back launches of the finest level's Chebyshev step over all right sides
+ * on the batch's stream (CUDA events); writes the mean device time of a launch (ms) and its
+ * algorithmic bytes (values and indices once; b, x, d read, d, x written per right side). The
+ * level's work vectors are overwritten. No reference counterpart. */
+int femgpu_batch_kernel_time(femgpu_batch* b, int reps, double* ms, double* bytes);
 size_t femgpu_batch_bytes(const femgpu_batch* b);
 void* femgpu_batch_stream(const femgpu_batch* b);
 void femgpu_batch_free(femgpu_batch* b);
