@@ -254,6 +254,48 @@ __global__ void k_prolong(int64_t nf, const int64_t* __restrict__ ptr,
     x[i] += s;
 }
 
+// A transfer in offset form: out = M in, or out += M in (accumulate). KC > 0: K known at
+// compile time (8 for P, 27 for R), so that all of a row's weight and x loads are in flight at
+// once; KC = 0 reads K from the view.
+template <class T, int KC>
+__global__ void __launch_bounds__(TH)
+    k_transfer(OffsetView<T> M, const T* __restrict__ in, T* __restrict__ out, int accumulate,
+               const int* __restrict__ done) {
+    if (*done) return;
+    const int i = row_of_thread();
+    if (i >= M.rows) return;
+    const int b = M.base[i];
+    const int K = KC > 0 ? KC : M.K;
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < (KC > 0 ? KC : MAXK); ++k) {
+        if (KC == 0 && k >= K) break;
+        const int j = b + M.off[k];
+        const bool in_range = j < M.cols;
+        const T w = __ldg(M.w + (size_t)k * M.rows + i);
+        const T v = in_range ? __ldg(in + j) : (T)0;
+        s = fmadd(w, v, s);
+    }
+    if (accumulate)
+        out[i] += s;
+    else
+        out[i] = s;
+}
+
+template <class T>
+static void launch_transfer(const OffsetTransfer<T>& M, const T* in, T* out, int accumulate,
+                            const int* done, cudaStream_t s) {
+    const int g = row_blocks(M.rows);
+    const auto v = M.view();
+    if (v.K == 8)
+        k_transfer<T, 8><<<g, TH, 0, s>>>(v, in, out, accumulate, done);
+    else if (v.K == 27)
+        k_transfer<T, 27><<<g, TH, 0, s>>>(v, in, out, accumulate, done);
+    else
+        k_transfer<T, 0><<<g, TH, 0, s>>>(v, in, out, accumulate, done);
+    FG_CHECK_LAUNCH();
+}
+
 // x = M b for the symmetric n x n matrix M (the coarsest inverse): 1 warp per row.
 template <class T>
 __global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__ b,
@@ -896,8 +938,8 @@ size_t Hierarchy<T>::bytes() const {
     size_t b = inv.bytes() + cb.bytes() + cx.bytes();
     for (const auto& l : levels)
         b += l.A.bytes() + l.dinv.bytes() + l.pptr.bytes() + l.rptr.bytes() + l.pidx.bytes() +
-             l.ridx.bytes() + l.pval.bytes() + l.rval.bytes() + l.b.bytes() + l.xa.bytes() +
-             l.xb.bytes() + l.d.bytes() + l.r.bytes();
+             l.ridx.bytes() + l.pval.bytes() + l.rval.bytes() + l.Po.bytes() + l.Ro.bytes() +
+             l.b.bytes() + l.xa.bytes() + l.xb.bytes() + l.d.bytes() + l.r.bytes();
     return b;
 }
 
@@ -935,7 +977,13 @@ std::string SolverImpl::describe() const {
             const auto& L = H.levels[l];
             std::snprintf(buf, sizeof buf, "level %zu %s n=%lld lambda=%.4f degree=%zu: ", l, t,
                           (long long)L.n, L.lambda, L.c1.size());
-            out += buf + describe_op(L.A) + "\n";
+            out += buf + describe_op(L.A);
+            std::snprintf(buf, sizeof buf, "; P %s, R %s\n",
+                          L.Po.ok ? ("offsets K=" + std::to_string(L.Po.off.size())).c_str()
+                                  : "CSR",
+                          L.Ro.ok ? ("offsets K=" + std::to_string(L.Ro.off.size())).c_str()
+                                  : "CSR");
+            out += buf;
         }
         std::snprintf(buf, sizeof buf, "coarsest n=%lld dense inverse\n", (long long)H.ncoarse);
         out += buf;
@@ -1028,6 +1076,46 @@ void SolverImpl::dense_direct(const HostCsr& h) {
     dense_inverse(h, &dense_inv_, s_);
 }
 
+// The offset form of a transfer when its entries sit at no more than 32 distinct offsets from
+// each row's first (smallest) column, which they do for the plane coarsening of a box grid in
+// grid order; else `out->ok` stays false and the transfer stays CSR.
+template <class T>
+static void make_offset(const HostRect& M, OffsetTransfer<T>* out, cudaStream_t s) {
+    out->ok = false;
+    if (M.rows >= 0x7fffffff || M.cols >= 0x7fffffff) return;
+    std::vector<int> base(M.rows, 0);
+    std::vector<int64_t> offs;
+    for (int64_t i = 0; i < M.rows; ++i) {
+        if (M.ptr[i] == M.ptr[i + 1]) continue;
+        uint32_t b = M.idx[M.ptr[i]];
+        for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) b = std::min(b, M.idx[k]);
+        base[i] = (int)b;
+        for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
+            const int64_t o = (int64_t)M.idx[k] - b;
+            if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
+                if (offs.size() == MAXK) return;
+                offs.push_back(o);
+            }
+        }
+    }
+    std::sort(offs.begin(), offs.end());
+    const int K = (int)offs.size();
+    std::vector<T> w((size_t)K * M.rows, (T)0);
+    for (int64_t i = 0; i < M.rows; ++i)
+        for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
+            const int64_t o = (int64_t)M.idx[k] - base[i];
+            const int slot = (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
+            w[(size_t)slot * M.rows + i] = (T)M.val[k];
+        }
+    out->rows = M.rows;
+    out->cols = M.cols;
+    out->off.assign(offs.begin(), offs.end());
+    out->base.upload(base.data(), base.size(), s);
+    out->w.upload(w.data(), w.size(), s);
+    FG_CUDA(cudaStreamSynchronize(s));
+    out->ok = true;
+}
+
 template <class T>
 void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps,
                               Hierarchy<T>* H) {
@@ -1075,12 +1163,20 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
             throw Failure(FEMGPU_ERR_TOO_LARGE, "a prolongation with 2^31 entries or more");
         HostRect R = transpose(P);
         lv.nc = P.cols;
-        lv.pptr.upload(P.ptr.data(), P.rows + 1, s_);
-        lv.pidx.upload(P.idx.data(), P.idx.size(), s_);
-        upload_values<T>(P.val, &lv.pval, s_);
-        lv.rptr.upload(R.ptr.data(), R.rows + 1, s_);
-        lv.ridx.upload(R.idx.data(), R.idx.size(), s_);
-        upload_values<T>(R.val, &lv.rval, s_);
+        if (opt_.format == 0) {
+            make_offset<T>(P, &lv.Po, s_);
+            make_offset<T>(R, &lv.Ro, s_);
+        }
+        if (!lv.Po.ok) {
+            lv.pptr.upload(P.ptr.data(), P.rows + 1, s_);
+            lv.pidx.upload(P.idx.data(), P.idx.size(), s_);
+            upload_values<T>(P.val, &lv.pval, s_);
+        }
+        if (!lv.Ro.ok) {
+            lv.rptr.upload(R.ptr.data(), R.rows + 1, s_);
+            lv.ridx.upload(R.idx.data(), R.idx.size(), s_);
+            upload_values<T>(R.val, &lv.rval, s_);
+        }
         lv.b.alloc(lv.n);
         lv.xa.alloc(lv.n);
         lv.xb.alloc(lv.n);
@@ -1178,13 +1274,19 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     with_op(L.A, [&](auto op) { k_residual<T><<<gs, TH, 0, s_>>>(op, b, xa, L.r.p, done); });
     mark(tag + "residual");
     T* bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
-    k_restrict<T><<<row_blocks(L.nc), TH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p,
-                                                                     L.rval.p, L.r.p, bc, done);
+    if (L.Ro.ok)
+        launch_transfer(L.Ro, (const T*)L.r.p, bc, 0, done, s_);
+    else
+        k_restrict<T><<<row_blocks(L.nc), TH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p,
+                                                       bc, done);
     FG_CHECK_LAUNCH();
     mark(tag + "restrict");
     launches_ += deg + 2;
     const T* ec = enqueue_vcycle(H, l + 1, bc);
-    k_prolong<T><<<gb, TH, 0, s_>>>(n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
+    if (L.Po.ok)
+        launch_transfer(L.Po, ec, xa, 1, done, s_);
+    else
+        k_prolong<T><<<gb, TH, 0, s_>>>(n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
     mark(tag + "prolong + correct");
     for (int k = 0; k < deg; ++k) {
         with_op(L.A, [&](auto op) {

@@ -80,13 +80,47 @@ struct Scalars {
     int done, iters, status, max_iter;
 };
 
+// A transfer (P or R = P^T) of a box grid in grid order: the entries of row i sit at K
+// constant offsets from the row's first column, y[i] = sum_k w[k][i] x[base[i] + off[k]], with
+// w = 0 where the row has no entry (at most 8 offsets for P, the corners of a coarse cell, and
+// 27 for R). The weights are read coalesced and no column index is stored.
+template <class T>
+struct OffsetView {
+    int rows, cols, K;
+    int off[32];
+    const int* __restrict__ base;
+    const T* __restrict__ w;
+};
+
+template <class T>
+struct OffsetTransfer {
+    bool ok = false;
+    int64_t rows = 0, cols = 0;
+    std::vector<int> off;
+    DevBuf<int> base;
+    DevBuf<T> w;
+    OffsetView<T> view() const {
+        OffsetView<T> v{};
+        v.rows = (int)rows;
+        v.cols = (int)cols;
+        v.K = (int)off.size();
+        for (size_t k = 0; k < off.size(); ++k) v.off[k] = off[k];
+        v.base = base.p;
+        v.w = w.p;
+        return v;
+    }
+    size_t bytes() const { return base.bytes() + w.bytes(); }
+};
+
 template <class T>
 struct MgLevel {
     int64_t n = 0, nnz = 0;
     Operator<T> A;
     DevBuf<T> dinv;
-    // The prolongation P from the next level, and R = P^T (gather form of the restriction).
+    // The prolongation P from the next level, and R = P^T (gather form of the restriction):
+    // in offset form where they fit (Po, Ro), else CSR.
     int64_t nc = 0;
+    OffsetTransfer<T> Po, Ro;
     DevBuf<int64_t> pptr, rptr;
     DevBuf<uint32_t> pidx, ridx;
     DevBuf<T> pval, rval;
