@@ -49,6 +49,11 @@ def args():
     p.add_argument("--profile", action="store_true",
                    help="only the timed mixed-precision solves (the command profiled by ncu)")
     p.add_argument("--format", type=int, default=0, help="0: stencil where possible, 1: SELL")
+    p.add_argument("--tail", type=int, default=0,
+                   help="> 0: levels of at most this many rows run as 1 fused cooperative "
+                        "kernel (0: none, the default)")
+    p.add_argument("--degree", type=int, default=0,
+                   help="Chebyshev degree of each pre- and post-smoothing (0: the default, 2)")
     p.add_argument("--breakdown", action="store_true",
                    help="print each solver's levels and the device time of each kernel of 1 "
                         "PCG iteration (kernels launched one by one), then exit")
@@ -268,7 +273,8 @@ def run_ours(opt, rank, world, local):
         t = time.perf_counter()
         s = fg.Solver(A, unknowns, fg.Method.Multigrid,
                       options=fg.Options(precision=precision, format=opt.format,
-                                         graph=opt.graph)).with_tol(TOL)
+                                         graph=opt.graph, tail=opt.tail,
+                                         degree=opt.degree)).with_tol(TOL)
         return s, time.perf_counter() - t
 
     b = torch.from_numpy(rhs).cuda()

@@ -277,6 +277,7 @@ int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
             o.max_levels = options->max_levels > 0 ? options->max_levels : 30;
             o.graph = options->graph != 2;
             o.format = options->format;
+            o.tail = options->tail;
         }
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,

@@ -42,6 +42,23 @@ struct SellOp {
     }
 };
 
+// Row i of the stencil product with K read at run time.
+template <class T, class TA, class TX>
+__device__ __forceinline__ TA stencil_apply(const StencilView<T>& v, int i,
+                                            const TX* __restrict__ x) {
+    const int n = v.n;
+    const T* __restrict__ c = v.coef;
+    TA acc = (TA)__ldg(c + i) * (TA)__ldg(x + i);
+    for (int k = 1; k < v.K; ++k) {
+        const int o = v.off[k];
+        const T* __restrict__ ck = c + (size_t)k * n;
+        const int j = i + o, m = i - o;
+        if (j < n) acc = fmadd((TA)__ldg(ck + i), (TA)__ldg(x + j), acc);
+        if (m >= 0) acc = fmadd((TA)__ldg(ck + m), (TA)__ldg(x + m), acc);
+    }
+    return acc;
+}
+
 template <class T>
 struct StencilOp {
     StencilView<T> v;
@@ -49,17 +66,29 @@ struct StencilOp {
     __device__ __forceinline__ bool valid(int64_t) const { return true; }
     template <class TA, class TX>
     __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
-        const int i = (int)g, n = v.n;
-        const T* __restrict__ c = v.coef;
-        TA acc = (TA)__ldg(c + i) * (TA)__ldg(x + i);
-        for (int k = 1; k < v.K; ++k) {
-            const int o = v.off[k];
-            const T* __restrict__ ck = c + (size_t)k * n;
-            const int j = i + o, m = i - o;
-            if (j < n) acc = fmadd((TA)__ldg(ck + i), (TA)__ldg(x + j), acc);
-            if (m >= 0) acc = fmadd((TA)__ldg(ck + m), (TA)__ldg(x + m), acc);
-        }
-        return acc;
+        return stencil_apply<T, TA, TX>(v, (int)g, x);
+    }
+};
+
+// The same products through a reference to a view held elsewhere (shared memory), so that the
+// view is not copied per thread.
+template <class T>
+struct StencilRefOp {
+    const StencilView<T>& v;
+    __device__ __forceinline__ bool valid(int64_t) const { return true; }
+    template <class TA, class TX>
+    __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
+        return stencil_apply<T, TA, TX>(v, (int)g, x);
+    }
+};
+
+template <class T>
+struct SellRefOp {
+    const SellView<T>& v;
+    __device__ __forceinline__ bool valid(int64_t g) const { return g < v.n; }
+    template <class TA, class TX>
+    __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
+        return sell_row<T, TX, TA>(v, g / v.C, (int)(g % v.C), x);
     }
 };
 

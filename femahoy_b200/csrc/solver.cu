@@ -20,6 +20,8 @@
 #include <thread>
 #include <type_traits>
 
+#include <cooperative_groups.h>
+
 #include "assemble.cuh"
 #include "solver.cuh"
 
@@ -183,19 +185,100 @@ static void with_op(const Operator<T>& op, F&& f) {
 // long on B200.
 __device__ __forceinline__ int row_of_thread() { return (int)(blockIdx.x * blockDim.x + threadIdx.x); }
 
+// ------------------------------------------------------------------ V-cycle rows
+// The work of 1 row of each V-cycle step, shared by the separate kernels below and by the fused
+// kernel of the coarse levels (k_tail), so that both give the same bits.
+
 // The first Chebyshev step from x = 0: d = c1 D^-1 b, x = d.
 template <class T>
-__global__ void k_cheb_first(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv, T c1,
-                             T* __restrict__ d, T* __restrict__ x, const int* __restrict__ done) {
-    if (*done) return;
-    const int i = row_of_thread();
-    if (i >= n) return;
+__device__ __forceinline__ void cheb_first_row(int i, const T* __restrict__ b,
+                                               const T* __restrict__ dinv, T c1,
+                                               T* __restrict__ d, T* __restrict__ x) {
     T v = c1 * dinv[i] * b[i];
     d[i] = v;
     x[i] = v;
 }
 
 // A Chebyshev step: r = b - A x_in, d = c2 d + c1 D^-1 r, x_out = x_in + d.
+template <class T, class Op>
+__device__ __forceinline__ void cheb_step_row(const Op& A, int g, const T* __restrict__ b,
+                                              const T* __restrict__ xin,
+                                              const T* __restrict__ dinv, T c1, T c2,
+                                              T* __restrict__ d, T* __restrict__ xout) {
+    T ax = A.template apply<T>(g, xin);
+    if (!A.valid(g)) return;
+    T r = b[g] - ax;
+    T dd = c2 * d[g] + c1 * dinv[g] * r;
+    d[g] = dd;
+    xout[g] = xin[g] + dd;
+}
+
+template <class T, class Op>
+__device__ __forceinline__ void residual_row(const Op& A, int g, const T* __restrict__ b,
+                                             const T* __restrict__ x, T* __restrict__ r) {
+    T ax = A.template apply<T>(g, x);
+    if (A.valid(g)) r[g] = b[g] - ax;
+}
+
+// Row i of a CSR transfer times x (multigrid.rs:166-172, sparse.rs:212-230).
+template <class T>
+__device__ __forceinline__ T csr_row(int i, const int64_t* __restrict__ ptr,
+                                     const uint32_t* __restrict__ idx, const T* __restrict__ val,
+                                     const T* __restrict__ x) {
+    const int e = (int)ptr[i + 1];
+    T s = 0;
+    for (int k = (int)ptr[i]; k < e; ++k) s += val[k] * __ldg(x + idx[k]);
+    return s;
+}
+
+// Row i of a transfer in offset form times x. KC > 0: K known at compile time (8 for P, 27 for
+// R), so that all of a row's weight and x loads are in flight at once; KC = 0 reads K from the
+// view. The terms are fused multiply-adds in increasing offset (= column) order either way.
+template <class T, int KC>
+__device__ __forceinline__ T offset_row(const OffsetView<T>& M, int i, const T* __restrict__ x) {
+    const int b = M.base[i];
+    const int K = KC > 0 ? KC : M.K;
+    T s = 0;
+#pragma unroll
+    for (int k = 0; k < (KC > 0 ? KC : MAXK); ++k) {
+        if (KC == 0 && k >= K) break;
+        const int j = b + M.off[k];
+        const T w = __ldg(M.w + (size_t)k * M.rows + i);
+        const T v = j < M.cols ? __ldg(x + j) : (T)0;
+        s = fmadd(w, v, s);
+    }
+    return s;
+}
+
+// Row i of x = M b for the n x n matrix M, by 1 warp (lane `lane`): 4 lane-strided partial sums,
+// then a butterfly over the warp; every lane ends with the sum.
+template <class T>
+__device__ __forceinline__ T gemv_warp_row(const T* __restrict__ M, const T* __restrict__ b,
+                                           int64_t n, int64_t i, int lane) {
+    const T* row = M + i * n;
+    T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    int64_t k = lane;
+    for (; k + 96 < n; k += 128) {
+        s0 += row[k] * __ldg(b + k);
+        s1 += row[k + 32] * __ldg(b + k + 32);
+        s2 += row[k + 64] * __ldg(b + k + 64);
+        s3 += row[k + 96] * __ldg(b + k + 96);
+    }
+    for (; k < n; k += 32) s0 += row[k] * __ldg(b + k);
+    T s = (s0 + s1) + (s2 + s3);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+template <class T>
+__global__ void k_cheb_first(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv, T c1,
+                             T* __restrict__ d, T* __restrict__ x, const int* __restrict__ done) {
+    if (*done) return;
+    const int i = row_of_thread();
+    if (i >= n) return;
+    cheb_first_row(i, b, dinv, c1, d, x);
+}
+
 template <class T, class Op>
 __global__ void __launch_bounds__(TH)
     k_cheb_step(Op A, const T* __restrict__ b, const T* __restrict__ xin,
@@ -204,12 +287,7 @@ __global__ void __launch_bounds__(TH)
     if (*done) return;
     const int g = row_of_thread();
     if (g >= A.threads()) return;
-    T ax = A.template apply<T>(g, xin);
-    if (!A.valid(g)) return;
-    T r = b[g] - ax;
-    T dd = c2 * d[g] + c1 * dinv[g] * r;
-    d[g] = dd;
-    xout[g] = xin[g] + dd;
+    cheb_step_row(A, g, b, xin, dinv, c1, c2, d, xout);
 }
 
 // r = b - A x
@@ -220,8 +298,7 @@ __global__ void __launch_bounds__(TH)
     if (*done) return;
     const int g = row_of_thread();
     if (g >= A.threads()) return;
-    T ax = A.template apply<T>(g, x);
-    if (A.valid(g)) r[g] = b[g] - ax;
+    residual_row(A, g, b, x, r);
 }
 
 // bc = P^T r as a gather over the rows of R = P^T (multigrid.rs:166, sparse.rs:223-230).
@@ -233,10 +310,7 @@ __global__ void k_restrict(int64_t nc, const int64_t* __restrict__ ptr,
     if (*done) return;
     const int c = row_of_thread();
     if (c >= nc) return;
-    const int e = (int)ptr[c + 1];
-    T s = 0;
-    for (int k = (int)ptr[c]; k < e; ++k) s += val[k] * __ldg(r + idx[k]);
-    bc[c] = s;
+    bc[c] = csr_row(c, ptr, idx, val, r);
 }
 
 // x += P e (multigrid.rs:169-172, sparse.rs:212-220)
@@ -248,15 +322,10 @@ __global__ void k_prolong(int64_t nf, const int64_t* __restrict__ ptr,
     if (*done) return;
     const int i = row_of_thread();
     if (i >= nf) return;
-    const int end = (int)ptr[i + 1];
-    T s = 0;
-    for (int k = (int)ptr[i]; k < end; ++k) s += val[k] * __ldg(e + idx[k]);
-    x[i] += s;
+    x[i] += csr_row(i, ptr, idx, val, e);
 }
 
-// A transfer in offset form: out = M in, or out += M in (accumulate). KC > 0: K known at
-// compile time (8 for P, 27 for R), so that all of a row's weight and x loads are in flight at
-// once; KC = 0 reads K from the view.
+// A transfer in offset form: out = M in, or out += M in (accumulate).
 template <class T, int KC>
 __global__ void __launch_bounds__(TH)
     k_transfer(OffsetView<T> M, const T* __restrict__ in, T* __restrict__ out, int accumulate,
@@ -264,18 +333,7 @@ __global__ void __launch_bounds__(TH)
     if (*done) return;
     const int i = row_of_thread();
     if (i >= M.rows) return;
-    const int b = M.base[i];
-    const int K = KC > 0 ? KC : M.K;
-    T s = 0;
-#pragma unroll
-    for (int k = 0; k < (KC > 0 ? KC : MAXK); ++k) {
-        if (KC == 0 && k >= K) break;
-        const int j = b + M.off[k];
-        const bool in_range = j < M.cols;
-        const T w = __ldg(M.w + (size_t)k * M.rows + i);
-        const T v = in_range ? __ldg(in + j) : (T)0;
-        s = fmadd(w, v, s);
-    }
+    const T s = offset_row<T, KC>(M, i, in);
     if (accumulate)
         out[i] += s;
     else
@@ -305,19 +363,111 @@ __global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = w; i < n; i += nw) {
-        const T* row = M + i * n;
-        T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-        int64_t k = lane;
-        for (; k + 96 < n; k += 128) {
-            s0 += row[k] * __ldg(b + k);
-            s1 += row[k + 32] * __ldg(b + k + 32);
-            s2 += row[k + 64] * __ldg(b + k + 64);
-            s3 += row[k + 96] * __ldg(b + k + 96);
-        }
-        for (; k < n; k += 32) s0 += row[k] * __ldg(b + k);
-        T s = (s0 + s1) + (s2 + s3);
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        T s = gemv_warp_row(M, b, n, i, lane);
         if (lane == 0) x[i] = s;
+    }
+}
+
+// ------------------------------------------------------------------ fused coarse levels
+namespace cg = cooperative_groups;
+
+constexpr int TAIL_MAXLEVELS = 8;
+static_assert(sizeof(TailLevel<float>) % sizeof(int) == 0 &&
+                  sizeof(TailLevel<double>) % sizeof(int) == 0,
+              "the descriptors are copied to shared memory as ints");
+
+// 1 smoothing step of a level of the fused kernel, over all its rows.
+template <class T>
+__device__ __forceinline__ void tail_smooth(const TailLevel<T>& L, const T* __restrict__ b,
+                                            const T* xin, T* xout, T c1, T c2, int tid,
+                                            int nth) {
+    if (L.stencil) {
+        const StencilRefOp<T> A{L.sv};
+        for (int i = tid; i < L.n; i += nth) cheb_step_row(A, i, b, xin, L.dinv, c1, c2, L.d, xout);
+    } else {
+        const SellRefOp<T> A{L.sell};
+        for (int i = tid; i < L.n; i += nth) cheb_step_row(A, i, b, xin, L.dinv, c1, c2, L.d, xout);
+    }
+}
+
+// The V-cycle from the first fused level down to the coarsest and back, as 1 cooperative
+// kernel: the steps of the separate kernels (the same row functions, so the same bits), each
+// over all rows of its level, with a grid-wide barrier between steps. On the small levels a
+// step is a few microseconds of launch and drain for well under a microsecond of work; here it
+// costs 1 barrier.
+template <class T>
+__global__ void __launch_bounds__(TH)
+    k_tail(const TailLevel<T>* __restrict__ Ls, int nl, const T* __restrict__ b0,
+           const T* __restrict__ inv, int64_t nco, T* __restrict__ cx,
+           const int* __restrict__ done) {
+    if (*done) return;  // the same value in every block: all leave, or none
+    // The levels' descriptors in shared memory, read by all threads of the block.
+    __shared__ TailLevel<T> sL[TAIL_MAXLEVELS];
+    {
+        const int words = nl * (int)(sizeof(TailLevel<T>) / sizeof(int));
+        const int* src = reinterpret_cast<const int*>(Ls);
+        int* dst = reinterpret_cast<int*>(sL);
+        for (int k = threadIdx.x; k < words; k += blockDim.x) dst[k] = src[k];
+        __syncthreads();
+    }
+    cg::grid_group grid = cg::this_grid();
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nth = gridDim.x * blockDim.x;
+    for (int l = 0; l < nl; ++l) {
+        const TailLevel<T>& L = sL[l];
+        const T* b = l == 0 ? b0 : L.b;
+        T* xa = L.xa;
+        T* xb = L.xb;
+        for (int i = tid; i < L.n; i += nth) cheb_first_row(i, b, L.dinv, L.c1[0], L.d, xa);
+        grid.sync();
+        for (int k = 1; k < L.deg; ++k) {
+            tail_smooth(L, b, xa, xb, L.c1[k], L.c2[k], tid, nth);
+            grid.sync();
+            T* t = xa;
+            xa = xb;
+            xb = t;
+        }
+        if (L.stencil) {
+            const StencilRefOp<T> A{L.sv};
+            for (int i = tid; i < L.n; i += nth) residual_row(A, i, b, xa, L.r);
+        } else {
+            const SellRefOp<T> A{L.sell};
+            for (int i = tid; i < L.n; i += nth) residual_row(A, i, b, xa, L.r);
+        }
+        grid.sync();
+        for (int j = tid; j < L.nc; j += nth)
+            L.bc[j] = L.r_offset ? offset_row<T, 0>(L.Ro, j, L.r)
+                                 : csr_row(j, L.rptr, L.ridx, L.rval, L.r);
+        grid.sync();
+    }
+    {
+        const int lane = threadIdx.x & 31;
+        const T* bc = sL[nl - 1].bc;
+        for (int64_t i = tid >> 5; i < nco; i += nth >> 5) {
+            const T s = gemv_warp_row(inv, bc, nco, i, lane);
+            if (lane == 0) cx[i] = s;
+        }
+        grid.sync();
+    }
+    const T* e = cx;
+    for (int l = nl - 1; l >= 0; --l) {
+        const TailLevel<T>& L = sL[l];
+        const T* b = l == 0 ? b0 : L.b;
+        // Where the pre-smoothing left x: after deg - 1 swaps.
+        T* xa = (L.deg - 1) % 2 ? L.xb : L.xa;
+        T* xb = (L.deg - 1) % 2 ? L.xa : L.xb;
+        for (int i = tid; i < L.n; i += nth)
+            xa[i] += L.p_offset ? offset_row<T, 0>(L.Po, i, e)
+                                : csr_row(i, L.pptr, L.pidx, L.pval, e);
+        grid.sync();
+        for (int k = 0; k < L.deg; ++k) {
+            tail_smooth(L, b, xa, xb, L.c1[k], L.c2[k], tid, nth);
+            grid.sync();
+            T* t = xa;
+            xa = xb;
+            xb = t;
+        }
+        e = xa;
     }
 }
 
@@ -940,7 +1090,7 @@ size_t Hierarchy<T>::bytes() const {
         b += l.A.bytes() + l.dinv.bytes() + l.pptr.bytes() + l.rptr.bytes() + l.pidx.bytes() +
              l.ridx.bytes() + l.pval.bytes() + l.rval.bytes() + l.Po.bytes() + l.Ro.bytes() +
              l.b.bytes() + l.xa.bytes() + l.xb.bytes() + l.d.bytes() + l.r.bytes();
-    return b;
+    return b + tail.bytes();
 }
 
 size_t SolverImpl::bytes() const {
@@ -987,6 +1137,12 @@ std::string SolverImpl::describe() const {
         }
         std::snprintf(buf, sizeof buf, "coarsest n=%lld dense inverse\n", (long long)H.ncoarse);
         out += buf;
+        if (H.tail_from >= 0 && tail_on_) {
+            std::snprintf(buf, sizeof buf,
+                          "levels %d.. and the coarsest solve: 1 cooperative kernel, %d blocks\n",
+                          H.tail_from, H.tail_grid);
+            out += buf;
+        }
     };
     if (opt_.precision == FEMGPU_MIXED)
         levels(H32_, "fp32");
@@ -1116,6 +1272,77 @@ static void make_offset(const HostRect& M, OffsetTransfer<T>* out, cudaStream_t 
     out->ok = true;
 }
 
+// The descriptors of the fused kernel for the levels from the first one of at most `tail` rows
+// down (tail <= 0: none), and its grid: as many blocks as fit on the GPU at once (a cooperative
+// launch needs them all resident), no more than the largest of those levels has rows for.
+// Measured on the 128^3 heat cube (levels 36k, 4.9k, coarsest 729): about 7 us per step of the
+// fused kernel, a grid-wide barrier included, against about 4 us per separate launch in the
+// loop's CUDA graph; so it is off unless asked for.
+template <class T>
+static void build_tail(Hierarchy<T>* H, int tail, cudaStream_t s) {
+    H->tail_from = -1;
+    if (tail <= 0 || H->levels.empty()) return;
+    const int64_t limit = tail;
+    size_t from = 0;
+    while (from < H->levels.size() && H->levels[from].n > limit) ++from;
+    if (from == H->levels.size()) return;
+    std::vector<TailLevel<T>> d;
+    int64_t rows = H->ncoarse;
+    if (H->levels.size() - from > (size_t)TAIL_MAXLEVELS) return;
+    for (size_t l = from; l < H->levels.size(); ++l) {
+        const MgLevel<T>& L = H->levels[l];
+        if (L.c1.size() > (size_t)TAIL_MAXDEG || L.n >= 0x7fffffff) return;
+        TailLevel<T> t{};
+        t.n = (int)L.n;
+        t.nc = (int)L.nc;
+        t.stencil = L.A.stencil ? 1 : 0;
+        t.deg = (int)L.c1.size();
+        if (L.A.stencil)
+            t.sv = L.A.sview();
+        else
+            t.sell = L.A.sell.view();
+        t.p_offset = L.Po.ok ? 1 : 0;
+        t.r_offset = L.Ro.ok ? 1 : 0;
+        if (L.Po.ok) {
+            t.Po = L.Po.view();
+        } else {
+            t.pptr = L.pptr.p;
+            t.pidx = L.pidx.p;
+            t.pval = L.pval.p;
+        }
+        if (L.Ro.ok) {
+            t.Ro = L.Ro.view();
+        } else {
+            t.rptr = L.rptr.p;
+            t.ridx = L.ridx.p;
+            t.rval = L.rval.p;
+        }
+        t.dinv = L.dinv.p;
+        t.b = L.b.p;
+        t.xa = L.xa.p;
+        t.xb = L.xb.p;
+        t.d = L.d.p;
+        t.r = L.r.p;
+        t.bc = l + 1 == H->levels.size() ? H->cb.p : H->levels[l + 1].b.p;
+        for (size_t k = 0; k < L.c1.size(); ++k) {
+            t.c1[k] = (T)L.c1[k];
+            t.c2[k] = (T)L.c2[k];
+        }
+        d.push_back(t);
+        rows = std::max(rows, L.n);
+    }
+    int per_sm = 0, dev = 0, sms = 0;
+    FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tail<T>, TH, 0));
+    FG_CUDA(cudaGetDevice(&dev));
+    FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return;
+    H->tail.upload(d.data(), d.size(), s);
+    FG_CUDA(cudaStreamSynchronize(s));
+    H->tail_grid =
+        (int)std::max<int64_t>(1, std::min<int64_t>((rows + TH - 1) / TH, (int64_t)per_sm * sms));
+    H->tail_from = (int)from;
+}
+
 template <class T>
 void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps,
                               Hierarchy<T>* H) {
@@ -1200,6 +1427,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
     }
     H->cb.alloc(last.n);
     H->cx.alloc(last.n);
+    build_tail(H, opt_.tail, s_);
 }
 
 void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst) {
@@ -1252,6 +1480,27 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
         mark("coarsest dense solve n=" + std::to_string(n));
         launches_ += 1;
         return H.cx.p;
+    }
+    if ((int)l == H.tail_from && tail_on_) {
+        // This level and all below it, and the coarsest solve: 1 cooperative kernel.
+        const TailLevel<T>* tl = H.tail.p;
+        int nl = (int)(H.levels.size() - l);
+        const T* b0 = b;
+        const T* inv = H.inv.p;
+        int64_t nco = H.ncoarse;
+        T* cx = H.cx.p;
+        void* args[] = {(void*)&tl, (void*)&nl, (void*)&b0, (void*)&inv,
+                        (void*)&nco, (void*)&cx, (void*)&done};
+        FG_CUDA(cudaLaunchCooperativeKernel((const void*)k_tail<T>, dim3(H.tail_grid), dim3(TH),
+                                            args, 0, s_));
+        mark("L" + std::to_string(l) + " and below, fused, with the coarsest solve");
+        launches_ += 1;
+        // Where the kernel leaves this level's x: the same swaps as the separate steps below.
+        MgLevel<T>& L = H.levels[l];
+        T* xa = L.xa.p;
+        T* xb = L.xb.p;
+        for (size_t k = 1; k < 2 * L.c1.size(); ++k) std::swap(xa, xb);
+        return xa;
     }
     MgLevel<T>& L = H.levels[l];
     int64_t n = L.n;
@@ -1342,25 +1591,48 @@ void SolverImpl::enqueue_iteration() {
 // The whole PCG loop as 1 graph: a WHILE conditional node whose body is 1 iteration followed by
 // k_loop_control, so the device runs iteration after iteration with no host round trip.
 void SolverImpl::build_loop_graph() {
-    FG_CUDA(cudaGraphCreate(&graph_, 0));
-    FG_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1, cudaGraphCondAssignDefault));
-    cudaGraphNodeParams cp{};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = cond_;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t node;
-    FG_CUDA(cudaGraphAddNode(&node, graph_, nullptr, 0, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    size_t before = launches_;
-    FG_CUDA(cudaStreamBeginCaptureToGraph(s_, body, nullptr, nullptr, 0,
-                                          cudaStreamCaptureModeThreadLocal));
-    enqueue_iteration();
-    k_loop_control<<<1, 1, 0, s_>>>(cond_, sc_.p, d_cancel_);
-    FG_CUDA(cudaStreamEndCapture(s_, &body));
-    FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
-    graph_kernels_ = launches_ - before + 1;
-    launches_ = before;
+    for (int attempt = 0;; ++attempt) {
+        const size_t before = launches_;
+        try {
+            FG_CUDA(cudaGraphCreate(&graph_, 0));
+            FG_CUDA(cudaGraphConditionalHandleCreate(&cond_, graph_, 1,
+                                                     cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp{};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond_;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            FG_CUDA(cudaGraphAddNode(&node, graph_, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            FG_CUDA(cudaStreamBeginCaptureToGraph(s_, body, nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+            enqueue_iteration();
+            k_loop_control<<<1, 1, 0, s_>>>(cond_, sc_.p, d_cancel_);
+            FG_CUDA(cudaStreamEndCapture(s_, &body));
+            FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
+            graph_kernels_ = launches_ - before + 1;
+            launches_ = before;
+            return;
+        } catch (const Failure&) {
+            // A capture that failed (a cooperative launch that the graph did not take, for
+            // one) ends here; the loop is captured again with every step its own launch.
+            cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+            cudaStreamIsCapturing(s_, &st);
+            if (st != cudaStreamCaptureStatusNone) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(s_, &g);
+            }
+            cudaGetLastError();
+            if (exec_) cudaGraphExecDestroy(exec_);
+            if (graph_) cudaGraphDestroy(graph_);
+            exec_ = nullptr;
+            graph_ = nullptr;
+            launches_ = before;
+            if (attempt > 0 || !tail_on_) throw;
+            tail_on_ = false;
+        }
+    }
 }
 
 void SolverImpl::run_device_loop(const volatile int* cancel) {

@@ -129,12 +129,34 @@ struct MgLevel {
     double lambda = 0;
 };
 
+// 1 level of the fused kernel of the coarse levels (k_tail): its operator (a stencil read with
+// the runtime-K product, or SELL), smoother, transfers and vectors.
+constexpr int TAIL_MAXDEG = 8;
+template <class T>
+struct TailLevel {
+    int n, nc, stencil, deg, p_offset, r_offset;
+    StencilView<T> sv;
+    SellView<T> sell;
+    OffsetView<T> Po, Ro;
+    const int64_t *pptr, *rptr;
+    const uint32_t *pidx, *ridx;
+    const T *pval, *rval;
+    const T* dinv;
+    const T* b;  // the level's right side (the first level's comes as an argument)
+    T *xa, *xb, *d, *r, *bc;
+    T c1[TAIL_MAXDEG], c2[TAIL_MAXDEG];
+};
+
 template <class T>
 struct Hierarchy {
     std::vector<MgLevel<T>> levels;  // all but the coarsest
     int64_t ncoarse = 0;
     DevBuf<T> inv;  // the inverse of the coarsest matrix, n x n (symmetric)
     DevBuf<T> cb, cx;
+    // The levels from `tail_from` down, and the coarsest solve, run as 1 cooperative kernel
+    // (-1: none) of `tail_grid` blocks.
+    int tail_from = -1, tail_grid = 0;
+    DevBuf<TailLevel<T>> tail;
     size_t bytes() const;
 };
 
@@ -147,6 +169,7 @@ struct Options {
     int coarsest = 3000;
     int max_levels = 30;
     bool graph = true;
+    int tail = 0;  // levels of at most this many rows run fused (<= 0: none)
 };
 
 class SolverImpl {
@@ -216,6 +239,7 @@ class SolverImpl {
     // While breakdown() runs: the label and the event recorded after each kernel.
     std::vector<std::pair<std::string, cudaEvent_t>>* trace_ = nullptr;
     void mark(const std::string& label);
+    bool tail_on_ = true;      // the fused coarse levels (off if a graph would not take them)
     size_t launches_ = 0;      // kernels enqueued by the current solve
     size_t graph_kernels_ = 0; // kernels of 1 iteration graph
 };

@@ -197,6 +197,10 @@ typedef struct femgpu_options {
     int format;           /* 0 = a symmetric stencil for each level whose entries sit at a few
                              constant column offsets (box grids in grid order), SELL-C for the
                              others; 1 = SELL-C for every level */
+    int tail;             /* > 0: the levels of at most this many rows, and the coarsest solve,
+                             run as 1 cooperative kernel with a grid-wide barrier between steps;
+                             0 (default) = every step its own launch (faster on B200 for the
+                             box grids measured) */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end

@@ -202,3 +202,29 @@ def test_nan_right_side_breaks_down_with_an_error():
     bad[3] = np.nan
     with pytest.raises(fg.FemError):
         s.solve(bad, np.zeros(A.n))
+
+
+@pytest.mark.parametrize("kind", ["heat", "elastic"])
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_fused_coarse_levels_give_the_same_bits(kind, precision):
+    """The small levels run as 1 cooperative kernel (the same row functions as the separate
+    kernels): the solution is bit for bit the one of the separate launches, for stencil levels
+    (heat) and SELL levels (elasticity)."""
+    if kind == "heat":
+        p = mg.heat_cube(40, seed=7)
+    else:
+        p = mg.cantilever_p1(dims=(48, 8, 8), lengths=(120.0, 20.0, 20.0))
+    A, rhs, _ = _system(p)
+    xs, its = [], []
+    for tail in (65536, 0):
+        s = fg.Solver(A, _grid(p), fg.Method.Multigrid, precision=precision,
+                      options=fg.Options(precision=precision, tail=tail, coarsest=200))
+        s = s.with_tol(1e-10)
+        assert ("cooperative kernel" in s.describe()) == (tail > 0)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1e-10
+        xs.append(x)
+        its.append(st.iterations)
+    assert its[0] == its[1]
+    assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
