@@ -35,6 +35,20 @@ static int row_blocks(int64_t rows) {
 }
 constexpr double PIVOT = 1e-10;  // cholesky.rs:22
 
+// Times a phase of the setup: the host time from its start until the solver's stream has
+// finished the phase's device work.
+struct PhaseTimer {
+    SolverImpl* solver;
+    const char* name;
+    cudaStream_t s;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    ~PhaseTimer() {
+        cudaStreamSynchronize(s);
+        solver->phase(name, std::chrono::duration<double>(std::chrono::steady_clock::now() - t0)
+                                .count());
+    }
+};
+
 // ------------------------------------------------------------------ SELL build
 __global__ void k_slice_entries(const int64_t* __restrict__ ptr, int64_t n, int C, int64_t ns,
                                 int64_t* __restrict__ entries) {
@@ -1148,7 +1162,22 @@ std::string SolverImpl::describe() const {
         levels(H32_, "fp32");
     else
         levels(H64_, "fp64");
+    out += "setup seconds:";
+    for (const auto& p : setup_s_) {
+        std::snprintf(buf, sizeof buf, " %s %.3f;", p.first.c_str(), p.second);
+        out += buf;
+    }
+    out += "\n";
     return out;
+}
+
+void SolverImpl::phase(const std::string& name, double seconds) {
+    for (auto& p : setup_s_)
+        if (p.first == name) {
+            p.second += seconds;
+            return;
+        }
+    setup_s_.emplace_back(name, seconds);
 }
 
 void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
@@ -1193,14 +1222,21 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         direct = (size_t)a.n <= c.unknowns;
     }
     direct_ = direct;
-    HostCsr h = download_csr(a_, s_);
+    HostCsr h;
+    {
+        PhaseTimer t{this, "matrix to host", s_};
+        h = download_csr(a_, s_);
+    }
     if (direct) {
         dense_direct(h);
         sizes_ = {n_};
         return;
     }
-    make_operator<double>(h, a_, C, opt_.format == 0, &op64_, s_);
-    tune_operator(&op64_, s_);
+    {
+        PhaseTimer t{this, "outer operator and autotuner", s_};
+        make_operator<double>(h, a_, C, opt_.format == 0, &op64_, s_);
+        tune_operator(&op64_, s_);
+    }
     if (u.kind == FEMGPU_UNKNOWNS_GRID) {
         HostLevel lv;
         for (int d = 0; d < 3; ++d) lv.planes[d].assign(u.planes[d], u.planes[d] + u.nplanes[d]);
@@ -1354,9 +1390,13 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         lv.n = mats[l].n;
         lv.nnz = mats[l].nnz();
         DevCsr d;
-        upload_csr(mats[l], &d, s_);
-        make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
-        tune_operator(&lv.A, s_);
+        {
+            PhaseTimer t{this, "level operators and autotuner", s_};
+            upload_csr(mats[l], &d, s_);
+            make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
+            tune_operator(&lv.A, s_);
+        }
+        PhaseTimer t_lam{this, "diagonals and lambda_max", s_};
         // The diagonal and lambda_max(D^-1 A) in FP64.
         DevBuf<double> dg(lv.n);
         DevBuf<int> bad(1);
@@ -1384,6 +1424,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         int deg = opt_.degree > 0 ? opt_.degree : 2;
         double lower = opt_.lower > 0 ? opt_.lower : 0.3;
         chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2);
+        PhaseTimer t_tr{this, "transfers", s_};
         // Transfers to the next level.
         const HostRect& P = ps[l];
         if ((int64_t)P.idx.size() >= 0x7fffffff || P.rows >= 0x7fffffff)
@@ -1412,6 +1453,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         FG_CUDA(cudaStreamSynchronize(s_));
     }
     // The coarsest level: its inverse from a dense Cholesky factor on the device.
+    PhaseTimer t_dense{this, "coarsest dense inverse", s_};
     const HostCsr& last = mats.back();
     H->ncoarse = last.n;
     DevBuf<double> inv64;
@@ -1449,9 +1491,13 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
         if ((size_t)a.n <= coarsest || ps.size() >= max_levels) break;
         HostRect p;
         HostLevel coarse;
-        if (!coarsen(level, a, &p, &coarse)) break;
-        if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
-        if (opt_.format == 0) renumber_grid_order(&p, &coarse);
+        {
+            PhaseTimer t{this, "coarsening (host)", s_};
+            if (!coarsen(level, a, &p, &coarse)) break;
+            if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
+            if (opt_.format == 0) renumber_grid_order(&p, &coarse);
+        }
+        PhaseTimer t_g{this, "Galerkin products (host)", s_};
         HostCsr ac = galerkin(p, a, threads);
         mats.push_back(std::move(ac));
         ps.push_back(std::move(p));

@@ -196,6 +196,8 @@ class SolverImpl {
     size_t max_iter = 500;  // PCG_MAX_ITER, solve.rs:43
     double tol = 1e-10;     // PCG_TOL, solve.rs:42
     cudaStream_t stream() const { return s_; }
+    // Adds `seconds` to the setup phase `name`.
+    void phase(const std::string& name, double seconds);
 
    private:
     void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst);
@@ -240,6 +242,8 @@ class SolverImpl {
     std::vector<std::pair<std::string, cudaEvent_t>>* trace_ = nullptr;
     void mark(const std::string& label);
     bool tail_on_ = true;      // the fused coarse levels (off if a graph would not take them)
+    // Seconds of each phase of the setup, in the order first met (reported by describe()).
+    std::vector<std::pair<std::string, double>> setup_s_;
     size_t launches_ = 0;      // kernels enqueued by the current solve
     size_t graph_kernels_ = 0; // kernels of 1 iteration graph
 };
