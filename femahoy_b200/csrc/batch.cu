@@ -32,8 +32,7 @@
 namespace femgpu {
 
 constexpr int BTH = 256;
-constexpr int DTH = 128;  // rows of a dense tile
-constexpr int DJ = 64;    // right-side rows staged in shared memory at a time
+constexpr int DTH = 32;   // rows of a dense tile
 
 // ------------------------------------------------------------------ operator with R columns
 // (A x)[row][col] for the SELL matrix A and the column `col` of the interleaved x.
@@ -96,6 +95,82 @@ __global__ void __launch_bounds__(BTH)
     r[t] = b[t] - sell_row_cols<T, R>(A, (int)(t / R), (int)(t % R), x);
 }
 
+// ------------------------------------------------------------------ 3x3-block operators
+// Elasticity levels: the 3 rows of a node have the same columns, which come in node triples.
+// Stored as SELL over block rows (slices of B3C block rows, blocks of 9 values, row-major, and
+// 1 block column each; padding blocks are 0 and point at the block row itself). The R threads
+// of a block row load each x block (3 rows of R values) once for the 3 rows.
+constexpr int B3C = 32;
+
+template <class T>
+struct BSell3View {
+    int64_t nb;                             // block rows
+    const int64_t* __restrict__ slice_ptr;  // in blocks; nslices + 1
+    const uint32_t* __restrict__ col;       // block column per block
+    const T* __restrict__ val;              // 9 per block
+};
+
+// (A x)[3 br + a][col] for a = 0, 1, 2.
+template <class T, int R>
+__device__ __forceinline__ void bsell3_rows(const BSell3View<T>& A, int br, int col,
+                                            const T* __restrict__ x, T* acc) {
+    const int s = br / B3C, r = br % B3C;
+    const int64_t b = A.slice_ptr[s], e = A.slice_ptr[s + 1];
+    const int w = (int)((e - b) / B3C);
+    acc[0] = acc[1] = acc[2] = 0;
+    for (int k = 0; k < w; ++k) {
+        const int64_t blk = b + (int64_t)k * B3C + r;
+        const uint32_t J = __ldg(A.col + blk);
+        const T* v = A.val + blk * 9;
+        const T x0 = __ldg(x + ((size_t)3 * J) * R + col);
+        const T x1 = __ldg(x + ((size_t)3 * J + 1) * R + col);
+        const T x2 = __ldg(x + ((size_t)3 * J + 2) * R + col);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            acc[a] += __ldg(v + 3 * a) * x0;
+            acc[a] += __ldg(v + 3 * a + 1) * x1;
+            acc[a] += __ldg(v + 3 * a + 2) * x2;
+        }
+    }
+}
+
+// The Chebyshev step of k_bcheb_step on a 3x3-block operator.
+template <class T, int R>
+__global__ void __launch_bounds__(BTH)
+    k_bcheb_step3(BSell3View<T> A, const T* __restrict__ b, const T* __restrict__ xin,
+                  const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d,
+                  T* __restrict__ xout) {
+    const int64_t t = elem_of_thread();
+    if (t >= A.nb * R) return;
+    const int br = (int)(t / R), col = (int)(t % R);
+    T acc[3];
+    bsell3_rows<T, R>(A, br, col, xin, acc);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int64_t row = 3 * (int64_t)br + a, i = row * R + col;
+        T r = b[i] - acc[a];
+        T dd = c2 * d[i] + c1 * dinv[row] * r;
+        d[i] = dd;
+        xout[i] = xin[i] + dd;
+    }
+}
+
+template <class T, int R>
+__global__ void __launch_bounds__(BTH)
+    k_bresidual3(BSell3View<T> A, const T* __restrict__ b, const T* __restrict__ x,
+                 T* __restrict__ r) {
+    const int64_t t = elem_of_thread();
+    if (t >= A.nb * R) return;
+    const int br = (int)(t / R), col = (int)(t % R);
+    T acc[3];
+    bsell3_rows<T, R>(A, br, col, x, acc);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int64_t i = (3 * (int64_t)br + a) * R + col;
+        r[i] = b[i] - acc[a];
+    }
+}
+
 // out = M in (accumulate: out += M in) for a CSR transfer M, R columns.
 template <class T, int R>
 __global__ void k_bgather(int64_t rows, const int64_t* __restrict__ ptr,
@@ -115,39 +190,61 @@ __global__ void k_bgather(int64_t rows, const int64_t* __restrict__ ptr,
 }
 
 // The members whose deepest level this is: out = M in for each, M its (symmetric) inverse. A
-// block takes DTH rows i of 1 member; thread i reads M[j][i] = M[i][j] for j = 0, 1, ..., so
-// a warp reads 32 consecutive entries of a row of M at a time, and the right sides of DJ rows
-// j at a time sit in shared memory, read by all threads at once.
+// block takes DTH = 32 rows i of 1 member; its DW warps split the columns j into DW contiguous
+// ranges, lane i reading M[j][i] = M[i][j] (32 consecutive entries of a row of M per warp) and
+// the R right-side values of row j (1 broadcast load per 4 values), so that 8 warps' loads are
+// in flight per tile; the DW partial sums are added in warp order through shared memory.
+constexpr int DW = 8;
+
 template <class T, int R>
-__global__ void __launch_bounds__(DTH)
+__device__ __forceinline__ void dense_accumulate(T mv, const T* __restrict__ xin, T* acc) {
+    if constexpr (R % 4 == 0) {
+        using V = typename Vec4<T>::type;
+#pragma unroll
+        for (int c = 0; c < R; c += 4) {
+            const V v = load4(xin + c);
+            acc[c] += mv * v.x;
+            acc[c + 1] += mv * v.y;
+            acc[c + 2] += mv * v.z;
+            acc[c + 3] += mv * v.w;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < R; ++c) acc[c] += mv * __ldg(xin + c);
+    }
+}
+
+template <class T, int R>
+__global__ void __launch_bounds__(32 * DW)
     k_bdense(const int2* __restrict__ tiles, const int64_t* __restrict__ off,
              const int64_t* __restrict__ ioff, const T* __restrict__ inv,
              const T* __restrict__ in, T* __restrict__ out) {
-    __shared__ T s_in[DJ * R];
+    __shared__ T part[DW][DTH][R + 1];
     const int2 tl = tiles[blockIdx.x];
     const int64_t r0 = off[tl.x], m = off[tl.x + 1] - r0;
     const T* __restrict__ M = inv + ioff[tl.x];
-    const int64_t i = tl.y + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t i = tl.y + lane;
+    const int64_t j0 = m * w / DW, j1 = m * (w + 1) / DW;
     T acc[R];
 #pragma unroll
     for (int c = 0; c < R; ++c) acc[c] = 0;
-    for (int64_t j0 = 0; j0 < m; j0 += DJ) {
-        const int jn = (int)min((int64_t)DJ, m - j0);
-        __syncthreads();
-        for (int t = threadIdx.x; t < jn * R; t += DTH) s_in[t] = in[(r0 + j0) * R + t];
-        __syncthreads();
-        if (i < m) {
-#pragma unroll 4
-            for (int jj = 0; jj < jn; ++jj) {
-                const T mv = __ldg(M + (j0 + jj) * m + i);
-#pragma unroll
-                for (int c = 0; c < R; ++c) acc[c] += mv * s_in[jj * R + c];
-            }
-        }
-    }
     if (i < m) {
+#pragma unroll 4
+        for (int64_t j = j0; j < j1; ++j)
+            dense_accumulate<T, R>(__ldg(M + j * m + i), in + (r0 + j) * R, acc);
+    }
 #pragma unroll
-        for (int c = 0; c < R; ++c) out[(r0 + i) * R + c] = acc[c];
+    for (int c = 0; c < R; ++c) part[w][lane][c] = acc[c];
+    __syncthreads();
+    for (int t = threadIdx.x; t < DTH * R; t += 32 * DW) {
+        const int row = t / R, c = t % R;
+        if (tl.y + row < m) {
+            T sum = 0;
+#pragma unroll
+            for (int q = 0; q < DW; ++q) sum += part[q][row][c];
+            out[(r0 + tl.y + row) * R + c] = sum;
+        }
     }
 }
 
@@ -237,6 +334,55 @@ __global__ void __launch_bounds__(BTH)
             double ap = sell_row_cols<double, R>(A, row, col, p);
             q[t] = ap;
             pq += p[t] * ap;
+        }
+    chunk_partial<R>(pq, 0.0, partial);
+}
+
+// k_bpcg_residual and k_bpcg_spmv on the 3x3-block form of the exact operator: a chunk's rows
+// are whole nodes (multiples of 3), and a thread takes block rows of 1 column.
+template <int R>
+__global__ void __launch_bounds__(BTH)
+    k_bpcg_residual3(BSell3View<double> A, const Chunk* __restrict__ chunks,
+                     const double* __restrict__ b, const double* __restrict__ x,
+                     double* __restrict__ r, float* __restrict__ r32,
+                     double* __restrict__ partial) {
+    const Chunk ch = chunks[blockIdx.x];
+    const int col = threadIdx.x % R;
+    double bb = 0, rr = 0;
+    for (int br = ch.row0 / 3 + threadIdx.x / R; br < ch.row1 / 3; br += BTH / R) {
+        double acc[3];
+        bsell3_rows<double, R>(A, br, col, x, acc);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int64_t t = (3 * (int64_t)br + a) * R + col;
+            const double ri = b[t] - acc[a];
+            if (r) r[t] = ri;
+            if (r32) r32[t] = (float)ri;
+            bb += b[t] * b[t];
+            rr += ri * ri;
+        }
+    }
+    chunk_partial<R>(bb, rr, partial);
+}
+
+template <int R>
+__global__ void __launch_bounds__(BTH)
+    k_bpcg_spmv3(BSell3View<double> A, const Chunk* __restrict__ chunks,
+                 const double* __restrict__ p, double* __restrict__ q,
+                 const int* __restrict__ done, double* __restrict__ partial) {
+    const Chunk ch = chunks[blockIdx.x];
+    const int col = threadIdx.x % R;
+    double pq = 0;
+    if (!done[ch.sys * R + col])
+        for (int br = ch.row0 / 3 + threadIdx.x / R; br < ch.row1 / 3; br += BTH / R) {
+            double acc[3];
+            bsell3_rows<double, R>(A, br, col, p, acc);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int64_t t = (3 * (int64_t)br + a) * R + col;
+                q[t] = acc[a];
+                pq += p[t] * acc[a];
+            }
         }
     chunk_partial<R>(pq, 0.0, partial);
 }
@@ -430,7 +576,12 @@ struct SystemHierarchy {
 template <class T>
 struct BatchLevel {
     int64_t n = 0, ns = 0, nc = 0;  // rows, smoothed rows, rows of the next level
-    Sell<T> A;                       // ns rows
+    Sell<T> A;                       // ns rows (when the level has no 3x3-block form)
+    bool block3 = false;             // the 3x3-block form A3 instead of A
+    DevBuf<int64_t> b3ptr;
+    DevBuf<uint32_t> b3col;
+    DevBuf<T> b3val;
+    BSell3View<T> view3() const { return {ns / 3, b3ptr.p, b3col.p, b3val.p}; }
     DevBuf<T> dinv;                  // ns
     DevBuf<int64_t> pptr, rptr;      // P: ns x nc, R = P^T: nc x ns
     DevBuf<uint32_t> pidx, ridx;
@@ -480,6 +631,8 @@ class BatchImpl {
     void iteration();
     template <int R>
     void run(const volatile int* cancel);
+    template <int R>
+    void residual(double* r, float* r32);
     void permute(const double* in, double* out, int scatter);
     void solve_loaded(const volatile int* cancel, femgpu_batch_stats* st);
     void launch_loop(const volatile int* cancel);
@@ -499,6 +652,11 @@ class BatchImpl {
     std::vector<int> order_;                // batch position -> caller's member
     DevBuf<int> map_;                       // batch row -> caller's row
     Sell<double> A64_;  // the block-diagonal finest matrix (batch order), exactly
+    bool fine3_ = false;  // ... in 3x3-block form instead (every member elastic)
+    DevBuf<int64_t> f3ptr_;
+    DevBuf<uint32_t> f3col_;
+    DevBuf<double> f3val_;
+    BSell3View<double> fine3() const { return {n_ / 3, f3ptr_.p, f3col_.p, f3val_.p}; }
     std::vector<BatchLevel<float>> L32_;
     std::vector<BatchLevel<double>> L64_;
     DevBuf<char> chunks_;
@@ -570,6 +728,59 @@ HostRect combine_rect(const std::vector<const HostRect*>& parts) {
         off += p->cols;
     }
     return out;
+}
+
+// The 3x3-block SELL form of `a`, if every node's 3 rows have the same columns and the
+// columns come in aligned triples; false (and nothing built) otherwise.
+template <class T>
+bool make_bsell3(const HostCsr& a, std::vector<int64_t>* sptr, std::vector<uint32_t>* cols,
+                 std::vector<T>* vals) {
+    if (a.n % 3 != 0 || a.n / 3 >= 0x7fffffff) return false;
+    const int64_t nb = a.n / 3;
+    std::vector<int> width(nb);
+    for (int64_t I = 0; I < nb; ++I) {
+        const int64_t r0 = 3 * I;
+        const int64_t len = a.ptr[r0 + 1] - a.ptr[r0];
+        if (len % 3 != 0) return false;
+        for (int q = 1; q < 3; ++q) {
+            if (a.ptr[r0 + q + 1] - a.ptr[r0 + q] != len) return false;
+            for (int64_t k = 0; k < len; ++k)
+                if (a.idx[a.ptr[r0 + q] + k] != a.idx[a.ptr[r0] + k]) return false;
+        }
+        for (int64_t k = 0; k < len; k += 3) {
+            const uint32_t c = a.idx[a.ptr[r0] + k];
+            if (c % 3 != 0 || a.idx[a.ptr[r0] + k + 1] != c + 1 ||
+                a.idx[a.ptr[r0] + k + 2] != c + 2)
+                return false;
+        }
+        width[I] = (int)(len / 3);
+    }
+    const int64_t nslices = (nb + B3C - 1) / B3C;
+    sptr->assign(nslices + 1, 0);
+    for (int64_t sl = 0; sl < nslices; ++sl) {
+        int w = 0;
+        for (int64_t I = sl * B3C; I < std::min(nb, (sl + 1) * B3C); ++I) w = std::max(w, width[I]);
+        (*sptr)[sl + 1] = (*sptr)[sl] + (int64_t)w * B3C;
+    }
+    cols->assign((*sptr)[nslices], 0);
+    vals->assign((size_t)(*sptr)[nslices] * 9, (T)0);
+    for (int64_t I = 0; I < nb; ++I) {
+        const int64_t sl = I / B3C, r = I % B3C, base = (*sptr)[sl];
+        const int w = (int)(((*sptr)[sl + 1] - base) / B3C);
+        for (int k = 0; k < w; ++k) {
+            const int64_t blk = base + (int64_t)k * B3C + r;
+            if (k < width[I]) {
+                const int64_t e = a.ptr[3 * I] + 3 * k;
+                (*cols)[blk] = a.idx[e] / 3;
+                for (int q = 0; q < 3; ++q)
+                    for (int c = 0; c < 3; ++c)
+                        (*vals)[(size_t)blk * 9 + 3 * q + c] = (T)a.val[a.ptr[3 * I + q] + 3 * k + c];
+            } else {
+                (*cols)[blk] = (uint32_t)I;  // padding: value 0, the block row's own x
+            }
+        }
+    }
+    return true;
 }
 
 }  // namespace
@@ -688,13 +899,24 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
         std::vector<const HostCsr*> parts;
         for (auto& h : Hs) parts.push_back(&h.mats[0]);
         HostCsr f = combine(parts);
-        DevCsr d;
-        upload_csr(f, &d, s_);
-        make_sell<double>(d, 32, &A64_, s_);
+        std::vector<int64_t> bp;
+        std::vector<uint32_t> bc;
+        std::vector<double> bv;
+        if (opt_.format == 0 && make_bsell3<double>(f, &bp, &bc, &bv)) {
+            fine3_ = true;
+            f3ptr_.upload(bp.data(), bp.size(), s_);
+            f3col_.upload(bc.data(), bc.size(), s_);
+            f3val_.upload(bv.data(), bv.size(), s_);
+        } else {
+            DevCsr d;
+            upload_csr(f, &d, s_);
+            make_sell<double>(d, 32, &A64_, s_);
+        }
         FG_CUDA(cudaStreamSynchronize(s_));
     }
-    // The chunks of the PCG kernels: up to 4 rows per thread, rows of 1 member each.
-    const int chunk_rows = 4 * BTH / R_;
+    // The chunks of the PCG kernels: rows of 1 member each; up to 4 rows per thread, or 2 block
+    // rows (6 rows) per thread with the 3x3-block operator, whose chunks hold whole nodes.
+    const int chunk_rows = fine3_ ? 3 * 2 * (BTH / R_) : 4 * BTH / R_;
     std::vector<Chunk> ch;
     std::vector<int> cstart(B_ + 1, 0);
     for (int k = 0; k < B_; ++k) {
@@ -750,7 +972,19 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             HostRect P = combine_rect(ps);
             DevCsr d;
             upload_csr(A, &d, s_);
-            make_sell<T>(d, 32, &L.A, s_);
+            {
+                std::vector<int64_t> bp;
+                std::vector<uint32_t> bc;
+                std::vector<T> bv;
+                if (opt_.format == 0 && make_bsell3<T>(A, &bp, &bc, &bv)) {
+                    L.block3 = true;
+                    L.b3ptr.upload(bp.data(), bp.size(), s_);
+                    L.b3col.upload(bc.data(), bc.size(), s_);
+                    L.b3val.upload(bv.data(), bv.size(), s_);
+                } else {
+                    make_sell<T>(d, 32, &L.A, s_);
+                }
+            }
             // The diagonal, and lambda_max of the block-diagonal D^-1 A: the largest of the
             // members'.
             std::vector<double> dg(A.n, 0.0), inv(A.n);
@@ -836,12 +1070,23 @@ const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b)
         const int g = (int)((L.ns * R + BTH - 1) / BTH);
         const int deg = (int)L.c1.size();
         k_bcheb_first<T, R><<<g, BTH, 0, s_>>>(L.ns, b, L.dinv.p, (T)L.c1[0], L.d.p, xa);
+        const int g3 = (int)((L.ns / 3 * R + BTH - 1) / BTH);
+        auto step = [&](const T* xin, T* xout, int k) {
+            if (L.block3)
+                k_bcheb_step3<T, R><<<g3, BTH, 0, s_>>>(L.view3(), b, xin, L.dinv.p, (T)L.c1[k],
+                                                         (T)L.c2[k], L.d.p, xout);
+            else
+                k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xin, L.dinv.p, (T)L.c1[k],
+                                                      (T)L.c2[k], L.d.p, xout);
+        };
         for (int k = 1; k < deg; ++k) {
-            k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k],
-                                                  (T)L.c2[k], L.d.p, xb);
+            step(xa, xb, k);
             std::swap(xa, xb);
         }
-        k_bresidual<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.r.p);
+        if (L.block3)
+            k_bresidual3<T, R><<<g3, BTH, 0, s_>>>(L.view3(), b, xa, L.r.p);
+        else
+            k_bresidual<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.r.p);
         T* bc = Ls[l + 1].b.p;
         const int gc = (int)((L.nc * R + BTH - 1) / BTH);
         k_bgather<T, R><<<gc, BTH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p, bc, 0);
@@ -850,15 +1095,15 @@ const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b)
         const T* ec = vcycle<T, R>(Ls, l + 1, bc);
         k_bgather<T, R><<<g, BTH, 0, s_>>>(L.ns, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, 1);
         for (int k = 0; k < deg; ++k) {
-            k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.dinv.p, (T)L.c1[k],
-                                                  (T)L.c2[k], L.d.p, xb);
+            step(xa, xb, k);
             std::swap(xa, xb);
         }
         FG_CHECK_LAUNCH();
         launches_ += deg + 1;
     }
     if (L.ndense > 0) {
-        k_bdense<T, R><<<L.ntiles, DTH, 0, s_>>>(L.tiles.p, L.doff.p, L.dioff.p, L.inv.p, b, xa);
+        k_bdense<T, R><<<L.ntiles, 32 * DW, 0, s_>>>(L.tiles.p, L.doff.p, L.dioff.p, L.inv.p,
+                                                     b, xa);
         FG_CHECK_LAUNCH();
         launches_ += 1;
     }
@@ -905,8 +1150,12 @@ void BatchImpl::precondition_and_dots(int init) {
 template <int R>
 void BatchImpl::iteration() {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
-    k_bpcg_spmv<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), p_.p, q_.p, done_.p,
-                                             partial_.p);
+    if (fine3_)
+        k_bpcg_spmv3<R><<<nchunks_, BTH, 0, s_>>>(fine3(), chunks(), p_.p, q_.p, done_.p,
+                                                  partial_.p);
+    else
+        k_bpcg_spmv<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), p_.p, q_.p, done_.p,
+                                                 partial_.p);
     finish<R>(FIN_PQ, 0);
     k_bpcg_update<R><<<nchunks_, BTH, 0, s_>>>(chunks(), x_.p, r_.p, p_.p, q_.p,
                                                mixed ? r32_.p : nullptr, scalars(), partial_.p);
@@ -946,6 +1195,18 @@ void BatchImpl::launch_loop(const volatile int* cancel) {
     FG_CUDA(e);
 }
 
+// r = b - A x with the FP64 exact operator and its sums (b.b, r.r) per chunk.
+template <int R>
+void BatchImpl::residual(double* r, float* r32) {
+    if (fine3_)
+        k_bpcg_residual3<R><<<nchunks_, BTH, 0, s_>>>(fine3(), chunks(), b_.p, x_.p, r, r32,
+                                                      partial_.p);
+    else
+        k_bpcg_residual<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), b_.p, x_.p, r, r32,
+                                                     partial_.p);
+    FG_CHECK_LAUNCH();
+}
+
 template <int R>
 void BatchImpl::run(const volatile int* cancel) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
@@ -976,8 +1237,7 @@ void BatchImpl::run(const volatile int* cancel) {
     FG_CUDA(cudaMemsetAsync(loops_.p, 0, sizeof(int), s_));
     // r = b - A x and the first test (multigrid.rs:692-723), x = 0 where b = 0, then
     // z = M^-1 r, p = z.
-    k_bpcg_residual<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), b_.p, x_.p, r_.p,
-                                                 mixed ? r32_.p : nullptr, partial_.p);
+    residual<R>(r_.p, mixed ? r32_.p : nullptr);
     finish<R>(FIN_START, 0);
     k_bzero_empty<R><<<nchunks_, BTH, 0, s_>>>(chunks(), bb_.p, x_.p);
     FG_CHECK_LAUNCH();
@@ -988,9 +1248,7 @@ void BatchImpl::run(const volatile int* cancel) {
         if (cancel && *cancel) return;
         // The true residual of each segment in FP64. With the FP32 cycle the recurrence can
         // drift from it; the segments that drifted above tol run again from x (at most 3 times).
-        k_bpcg_residual<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), b_.p, x_.p,
-                                                     mixed ? r_.p : nullptr,
-                                                     mixed ? r32_.p : nullptr, partial_.p);
+        residual<R>(mixed ? r_.p : nullptr, mixed ? r32_.p : nullptr);
         finish<R>(FIN_TRUTH, 0);
         launches_ += 1;
         if (!mixed || restarts_ >= 3) break;
@@ -1144,10 +1402,15 @@ void BatchImpl::kernel_time(int reps, double* ms, double* bytes) {
         using T = typename std::remove_reference<decltype(*L.dinv.p)>::type;
         constexpr int R = decltype(r)::value;
         const int g = (int)((L.ns * R + BTH - 1) / BTH);
+        const int g3 = (int)((L.ns / 3 * R + BTH - 1) / BTH);
         for (int k = 0; k < reps + 5; ++k) {
             if (k == 5) FG_CUDA(cudaEventRecord(ev0_, s_));
-            k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p, (T)0.5,
-                                                  (T)0.5, L.d.p, L.xb.p);
+            if (L.block3)
+                k_bcheb_step3<T, R><<<g3, BTH, 0, s_>>>(L.view3(), L.b.p, L.xa.p, L.dinv.p,
+                                                         (T)0.5, (T)0.5, L.d.p, L.xb.p);
+            else
+                k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), L.b.p, L.xa.p, L.dinv.p,
+                                                      (T)0.5, (T)0.5, L.d.p, L.xb.p);
         }
         FG_CHECK_LAUNCH();
         FG_CUDA(cudaEventRecord(ev1_, s_));
@@ -1157,8 +1420,9 @@ void BatchImpl::kernel_time(int reps, double* ms, double* bytes) {
         *ms = t / reps;
         // Each value and index of the level once, and per right side b, x, d (read), d and
         // x_out (written) and the row's D^-1.
-        *bytes = (double)L.A.bytes() - (double)L.A.slice_ptr.bytes() +
-                 (double)L.ns * sizeof(T) * (5.0 * R + 1.0);
+        const double mat = L.block3 ? (double)L.b3col.bytes() + (double)L.b3val.bytes()
+                                    : (double)L.A.bytes() - (double)L.A.slice_ptr.bytes();
+        *bytes = mat + (double)L.ns * sizeof(T) * (5.0 * R + 1.0);
     };
     auto pick = [&](auto& L) {
         FG_CUDA(cudaMemsetAsync(L.xa.p, 0, L.xa.bytes(), s_));
@@ -1178,10 +1442,12 @@ void BatchImpl::kernel_time(int reps, double* ms, double* bytes) {
 }
 
 size_t BatchImpl::bytes() const {
-    size_t b = A64_.bytes() + partial_.bytes() + chunks_.bytes() + cstart_.bytes() + map_.bytes();
+    size_t b = A64_.bytes() + f3ptr_.bytes() + f3col_.bytes() + f3val_.bytes() +
+               partial_.bytes() + chunks_.bytes() + cstart_.bytes() + map_.bytes();
     auto levels = [&](const auto& Ls) {
         for (const auto& L : Ls)
-            b += L.A.bytes() + L.dinv.bytes() + L.pptr.bytes() + L.rptr.bytes() + L.pidx.bytes() +
+            b += L.A.bytes() + L.b3ptr.bytes() + L.b3col.bytes() + L.b3val.bytes() +
+                 L.dinv.bytes() + L.pptr.bytes() + L.rptr.bytes() + L.pidx.bytes() +
                  L.ridx.bytes() + L.pval.bytes() + L.rval.bytes() + L.b.bytes() + L.xa.bytes() +
                  L.xb.bytes() + L.d.bytes() + L.r.bytes() + L.doff.bytes() + L.dioff.bytes() +
                  L.tiles.bytes() + L.inv.bytes();
@@ -1238,10 +1504,11 @@ int femgpu_batch_new(int count, const femgpu_csr* const* a, const femgpu_unknown
             us.push_back(&u[b]);
         }
         Options o;
-        o.format = 1;
+        o.format = 0;
         o.coarsest = 0;
         if (options) {
             o.precision = options->precision;
+            o.format = options->format;
             o.degree = options->degree;
             o.lower = options->lower;
             o.coarsest = options->coarsest;
