@@ -847,6 +847,9 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
                 HostLevel coarse;
                 if (!coarsen(lv, m, &p, &coarse)) break;
                 if (coarse.points.size() * 10 > (size_t)m.n * 9) break;
+                // Grid order (z, y, x, component): the 3 unknowns of a node are consecutive,
+                // which the 3x3-block operators need.
+                if (o.format == 0) renumber_grid_order(&p, &coarse);
                 HostCsr ac = galerkin(p, m, 1);
                 H[b].mats.push_back(std::move(ac));
                 H[b].ps.push_back(std::move(p));
