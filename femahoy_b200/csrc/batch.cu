@@ -189,60 +189,103 @@ __global__ void k_bgather(int64_t rows, const int64_t* __restrict__ ptr,
         out[t] = s;
 }
 
-// The members whose deepest level this is: out = M in for each, M its (symmetric) inverse. A
-// block takes DTH = 32 rows i of 1 member; its DW warps split the columns j into DW contiguous
-// ranges, lane i reading M[j][i] = M[i][j] (32 consecutive entries of a row of M per warp) and
-// the R right-side values of row j (1 broadcast load per 4 values), so that 8 warps' loads are
-// in flight per tile; the DW partial sums are added in warp order through shared memory.
+// The members whose deepest level this is: out = M in for each, M its inverse, stored in tiles
+// of DTH = 32 rows, each tile by column (the 32 entries of column j of the tile contiguous). A
+// block takes 1 tile; its DW warps split the columns j into DW contiguous ranges. A warp takes
+// its columns 32 at a time: lane q brings the R right-side values of column j + q into the
+// warp's shared buffer (the next 32 already loading into registers while this 32 is used), then
+// lane i (row i of the tile) adds M[i][j] times the buffered values, the loads of M 8 columns
+// ahead. The DW partial sums are added in warp order through shared memory.
 constexpr int DW = 8;
 
 template <class T, int R>
-__device__ __forceinline__ void dense_accumulate(T mv, const T* __restrict__ xin, T* acc) {
-    if constexpr (R % 4 == 0) {
-        using V = typename Vec4<T>::type;
+struct DenseChunk {
+    static constexpr int V = R % 4 == 0 ? R / 4 : R;  // loads of a row: 4-vectors, or scalars
+    typename std::conditional<R % 4 == 0, typename Vec4<T>::type, T>::type v[V];
+    __device__ __forceinline__ void load(const T* __restrict__ row, bool ok) {
 #pragma unroll
-        for (int c = 0; c < R; c += 4) {
-            const V v = load4(xin + c);
-            acc[c] += mv * v.x;
-            acc[c + 1] += mv * v.y;
-            acc[c + 2] += mv * v.z;
-            acc[c + 3] += mv * v.w;
+        for (int k = 0; k < V; ++k) {
+            if constexpr (R % 4 == 0) {
+                if (ok) {
+                    v[k] = load4(row + 4 * k);
+                } else {
+                    v[k].x = v[k].y = v[k].z = v[k].w = 0;
+                }
+            } else {
+                v[k] = ok ? __ldg(row + k) : (T)0;
+            }
         }
-    } else {
-#pragma unroll
-        for (int c = 0; c < R; ++c) acc[c] += mv * __ldg(xin + c);
     }
-}
+    __device__ __forceinline__ void store(T* dst) const {
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            if constexpr (R % 4 == 0) {
+                dst[4 * k] = v[k].x;
+                dst[4 * k + 1] = v[k].y;
+                dst[4 * k + 2] = v[k].z;
+                dst[4 * k + 3] = v[k].w;
+            } else {
+                dst[k] = v[k];
+            }
+        }
+    }
+};
 
 template <class T, int R>
 __global__ void __launch_bounds__(32 * DW)
     k_bdense(const int2* __restrict__ tiles, const int64_t* __restrict__ off,
              const int64_t* __restrict__ ioff, const T* __restrict__ inv,
              const T* __restrict__ in, T* __restrict__ out) {
-    __shared__ T part[DW][DTH][R + 1];
+    // Per warp a buffer of 32 right-side rows; reused at the end for the partial sums.
+    constexpr int STAGE = DW * 32 * R, PART = DW * DTH * (R + 1);
+    __shared__ T smem[STAGE > PART ? STAGE : PART];
     const int2 tl = tiles[blockIdx.x];
     const int64_t r0 = off[tl.x], m = off[tl.x + 1] - r0;
-    const T* __restrict__ M = inv + ioff[tl.x];
+    const T* __restrict__ Mt = inv + ioff[tl.x] + (int64_t)tl.y * m;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t i = tl.y + lane;
+    const bool row_ok = tl.y + lane < m;
     const int64_t j0 = m * w / DW, j1 = m * (w + 1) / DW;
+    T* buf = smem + w * 32 * R;
     T acc[R];
 #pragma unroll
     for (int c = 0; c < R; ++c) acc[c] = 0;
-    if (i < m) {
-#pragma unroll 4
-        for (int64_t j = j0; j < j1; ++j)
-            dense_accumulate<T, R>(__ldg(M + j * m + i), in + (r0 + j) * R, acc);
-    }
+    DenseChunk<T, R> next;
+    next.load(in + (r0 + j0 + lane) * R, j0 + lane < j1);
+    for (int64_t jc = j0; jc < j1; jc += 32) {
+        __syncwarp();
+        next.store(buf + lane * R);
+        __syncwarp();
+        if (jc + 32 < j1) next.load(in + (r0 + jc + 32 + lane) * R, jc + 32 + lane < j1);
+        const int nj = (int)min((int64_t)32, j1 - jc);
+        if (row_ok) {
+            int q = 0;
+            for (; q + 8 <= nj; q += 8) {
+                T mv[8];
 #pragma unroll
-    for (int c = 0; c < R; ++c) part[w][lane][c] = acc[c];
+                for (int u = 0; u < 8; ++u) mv[u] = __ldg(Mt + 32 * (jc + q + u) + lane);
+#pragma unroll
+                for (int u = 0; u < 8; ++u)
+#pragma unroll
+                    for (int c = 0; c < R; ++c) acc[c] += mv[u] * buf[(q + u) * R + c];
+            }
+            for (; q < nj; ++q) {
+                const T mv = __ldg(Mt + 32 * (jc + q) + lane);
+#pragma unroll
+                for (int c = 0; c < R; ++c) acc[c] += mv * buf[q * R + c];
+            }
+        }
+    }
+    __syncthreads();
+    T* part = smem;  // [DW][DTH][R + 1]
+#pragma unroll
+    for (int c = 0; c < R; ++c) part[(w * DTH + lane) * (R + 1) + c] = acc[c];
     __syncthreads();
     for (int t = threadIdx.x; t < DTH * R; t += 32 * DW) {
         const int row = t / R, c = t % R;
         if (tl.y + row < m) {
             T sum = 0;
 #pragma unroll
-            for (int q = 0; q < DW; ++q) sum += part[q][row][c];
+            for (int q = 0; q < DW; ++q) sum += part[(q * DTH + row) * (R + 1) + c];
             out[(r0 + tl.y + row) * R + c] = sum;
         }
     }
@@ -1024,7 +1067,7 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             L.r.alloc((size_t)L.ns * R_);
         }
         // The members that end here: a dense inverse each, from a dense Cholesky factor on the
-        // device, made exactly symmetric (the kernel reads it by columns).
+        // device, made exactly symmetric, stored in tiles of DTH rows (k_bdense's layout).
         L.ndense = K - S;
         if (L.ndense > 0) {
             std::vector<int64_t> off(L.ndense + 1), ioff(L.ndense + 1, 0);
@@ -1033,7 +1076,8 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             for (int j = 0; j < L.ndense; ++j) {
                 const int64_t m = H[S + j].mats[l].n;
                 off[j + 1] = off[j] + m;
-                ioff[j + 1] = ioff[j] + m * m;
+                // Row tiles of DTH rows (the last padded with zero rows), each stored by column.
+                ioff[j + 1] = ioff[j] + (m + DTH - 1) / DTH * DTH * m;
                 for (int64_t t = 0; t < m; t += DTH) tiles.push_back({j, (int)t});
             }
             L.ntiles = (int)tiles.size();
@@ -1045,11 +1089,13 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
                 std::vector<double> h((size_t)(m * m));
                 inv64.download(h.data(), m * m, s_);
                 FG_CUDA(cudaStreamSynchronize(s_));
-                std::vector<T> t((size_t)(m * m));
+                const int64_t mt = ioff[j + 1] - ioff[j];
+                std::vector<T> t((size_t)mt, (T)0);
                 for (int64_t r = 0; r < m; ++r)
                     for (int64_t c = 0; c < m; ++c)
-                        t[r * m + c] = (T)(0.5 * (h[r * m + c] + h[c * m + r]));
-                FG_CUDA(cudaMemcpyAsync(L.inv.p + ioff[j], t.data(), m * m * sizeof(T),
+                        t[(r / DTH) * DTH * m + c * DTH + r % DTH] =
+                            (T)(0.5 * (h[r * m + c] + h[c * m + r]));
+                FG_CUDA(cudaMemcpyAsync(L.inv.p + ioff[j], t.data(), mt * sizeof(T),
                                         cudaMemcpyHostToDevice, s_));
                 FG_CUDA(cudaStreamSynchronize(s_));
             }
