@@ -52,6 +52,8 @@ def args():
     p.add_argument("--tail", type=int, default=0,
                    help="> 0: levels of at most this many rows run as 1 fused cooperative "
                         "kernel (0: none, the default)")
+    p.add_argument("--launch", type=int, default=0,
+                   help="0: programmatic dependent launch in the PCG loop (default), 1: plain")
     p.add_argument("--degree", type=int, default=0,
                    help="Chebyshev degree of each pre- and post-smoothing (0: the default, 2)")
     p.add_argument("--breakdown", action="store_true",
@@ -274,7 +276,7 @@ def run_ours(opt, rank, world, local):
         s = fg.Solver(A, unknowns, fg.Method.Multigrid,
                       options=fg.Options(precision=precision, format=opt.format,
                                          graph=opt.graph, tail=opt.tail,
-                                         degree=opt.degree)).with_tol(TOL)
+                                         degree=opt.degree, launch=opt.launch)).with_tol(TOL)
         return s, time.perf_counter() - t
 
     b = torch.from_numpy(rhs).cuda()

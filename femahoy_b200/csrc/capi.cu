@@ -278,6 +278,7 @@ int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
             o.graph = options->graph != 2;
             o.format = options->format;
             o.tail = options->tail;
+            o.pdl = options->launch == 0 ? 1 : 0;
         }
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,

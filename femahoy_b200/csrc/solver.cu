@@ -35,6 +35,31 @@ static int row_blocks(int64_t rows) {
 }
 constexpr double PIVOT = 1e-10;  // cholesky.rs:22
 
+// Programmatic dependent launch. The kernels of a PCG iteration are launched so that each may
+// start while the one before it drains; every such kernel first waits (griddepcontrol.wait) for
+// the completion and the memory of the kernel before it, so it reads what it would have read
+// without the attribute. On the short kernels of the coarse levels the launch latency this
+// hides is most of their time.
+// (An explicit early trigger, griddepcontrol.launch_dependents after the wait, measured no
+// better on the 128^3 heat solve; the blocks trigger when they exit.)
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static void launch(bool pdl, void (*kernel)(KArgs...), int grid, int block, cudaStream_t s,
+                   Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? &attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    FG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
+
 // Times a phase of the setup: the host time from its start until the solver's stream has
 // finished the phase's device work.
 struct PhaseTimer {
@@ -287,6 +312,7 @@ __device__ __forceinline__ T gemv_warp_row(const T* __restrict__ M, const T* __r
 template <class T>
 __global__ void k_cheb_first(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv, T c1,
                              T* __restrict__ d, T* __restrict__ x, const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     const int i = row_of_thread();
     if (i >= n) return;
@@ -298,6 +324,7 @@ __global__ void __launch_bounds__(TH)
     k_cheb_step(Op A, const T* __restrict__ b, const T* __restrict__ xin,
                 const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d, T* __restrict__ xout,
                 const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     const int g = row_of_thread();
     if (g >= A.threads()) return;
@@ -309,6 +336,7 @@ template <class T, class Op>
 __global__ void __launch_bounds__(TH)
     k_residual(Op A, const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r,
                const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     const int g = row_of_thread();
     if (g >= A.threads()) return;
@@ -321,6 +349,7 @@ __global__ void k_restrict(int64_t nc, const int64_t* __restrict__ ptr,
                            const uint32_t* __restrict__ idx, const T* __restrict__ val,
                            const T* __restrict__ r, T* __restrict__ bc,
                            const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     const int c = row_of_thread();
     if (c >= nc) return;
@@ -333,6 +362,7 @@ __global__ void k_prolong(int64_t nf, const int64_t* __restrict__ ptr,
                           const uint32_t* __restrict__ idx, const T* __restrict__ val,
                           const T* __restrict__ e, T* __restrict__ x,
                           const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     const int i = row_of_thread();
     if (i >= nf) return;
@@ -344,6 +374,7 @@ template <class T, int KC>
 __global__ void __launch_bounds__(TH)
     k_transfer(OffsetView<T> M, const T* __restrict__ in, T* __restrict__ out, int accumulate,
                const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     const int i = row_of_thread();
     if (i >= M.rows) return;
@@ -356,22 +387,22 @@ __global__ void __launch_bounds__(TH)
 
 template <class T>
 static void launch_transfer(const OffsetTransfer<T>& M, const T* in, T* out, int accumulate,
-                            const int* done, cudaStream_t s) {
+                            const int* done, cudaStream_t s, bool pdl) {
     const int g = row_blocks(M.rows);
     const auto v = M.view();
     if (v.K == 8)
-        k_transfer<T, 8><<<g, TH, 0, s>>>(v, in, out, accumulate, done);
+        launch(pdl, k_transfer<T, 8>, g, TH, s, v, in, out, accumulate, done);
     else if (v.K == 27)
-        k_transfer<T, 27><<<g, TH, 0, s>>>(v, in, out, accumulate, done);
+        launch(pdl, k_transfer<T, 27>, g, TH, s, v, in, out, accumulate, done);
     else
-        k_transfer<T, 0><<<g, TH, 0, s>>>(v, in, out, accumulate, done);
-    FG_CHECK_LAUNCH();
+        launch(pdl, k_transfer<T, 0>, g, TH, s, v, in, out, accumulate, done);
 }
 
 // x = M b for the symmetric n x n matrix M (the coarsest inverse): 1 warp per row.
 template <class T>
 __global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__ b,
                        T* __restrict__ x, const int* __restrict__ done) {
+    pdl_wait();
     if (*done) return;
     int lane = threadIdx.x & 31;
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -525,6 +556,7 @@ __device__ __forceinline__ void block_partial(double a, double b, double* __rest
 template <class Fin>
 __global__ void __launch_bounds__(TH) k_finish(const double* __restrict__ partial, int nblocks,
                                                 Fin fin) {
+    pdl_wait();
     if (fin.skip()) return;
     __shared__ double sa[TH / 32], sb[TH / 32];
     double a = 0, b = 0;
@@ -568,6 +600,7 @@ template <class Op>
 __global__ void __launch_bounds__(TH)
     k_pcg_residual(Op A, const double* __restrict__ b, const double* __restrict__ x,
                    double* __restrict__ r, float* __restrict__ r32, double* __restrict__ partial) {
+    pdl_wait();
     double bb = 0, rr = 0;
     const int g = row_of_thread();
     if (g < A.threads()) {
@@ -597,6 +630,7 @@ template <class Op>
 __global__ void __launch_bounds__(TH)
     k_pcg_spmv_pq(Op A, const double* __restrict__ p, double* __restrict__ q,
                   double* __restrict__ partial, const Scalars* __restrict__ sc) {
+    pdl_wait();
     if (sc->done) return;
     double pq = 0;
     const int g = row_of_thread();
@@ -628,6 +662,7 @@ __global__ void __launch_bounds__(TH)
                  const double* __restrict__ p, const double* __restrict__ q,
                  float* __restrict__ r32, double* __restrict__ partial,
                  const Scalars* __restrict__ sc) {
+    pdl_wait();
     if (sc->done) return;
     const double alpha = sc->alpha;
     double rr = 0;
@@ -666,6 +701,7 @@ __global__ void __launch_bounds__(TH)
     k_pcg_dots(int64_t n, const double* __restrict__ r, const TZ* __restrict__ z,
                const double* __restrict__ q, int flexible, int init,
                double* __restrict__ partial, const Scalars* __restrict__ sc) {
+    pdl_wait();
     if (sc->done) return;
     double rz = 0, zq = 0;
     const int i = row_of_thread();
@@ -681,6 +717,7 @@ __global__ void __launch_bounds__(TH)
 template <class TZ>
 __global__ void k_pcg_p(int64_t n, const TZ* __restrict__ z, double* __restrict__ p,
                         const Scalars* sc, int init) {
+    pdl_wait();
     if (sc->done) return;
     const double beta = sc->beta;
     const int i = row_of_thread();
@@ -1183,6 +1220,7 @@ void SolverImpl::phase(const std::string& name, double seconds) {
 void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
                         const femgpu_crossover& c, const Options& o) {
     opt_ = o;
+    pdl_ = o.pdl != 0;
     n_ = a.n;
     // The solver's own copy of the matrix (the reference moves `a` into the Solver).
     a_.n = a.n;
@@ -1521,7 +1559,7 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     const int* done = &sc_.p->done;
     if (l == H.levels.size()) {
         int64_t n = H.ncoarse;
-        k_gemv<T><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, H.inv.p, b, H.cx.p, done);
+        launch(pdl_, k_gemv<T>, blocks_for(n * 32, TH), TH, s_, n, H.inv.p, b, H.cx.p, done);
         FG_CHECK_LAUNCH();
         mark("coarsest dense solve n=" + std::to_string(n));
         launches_ += 1;
@@ -1556,37 +1594,39 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     T* xb = L.xb.p;
     int deg = (int)L.c1.size();
     std::string tag = "L" + std::to_string(l) + " ";
-    k_cheb_first<T><<<gb, TH, 0, s_>>>(n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
+    launch(pdl_, k_cheb_first<T>, gb, TH, s_, n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
     mark(tag + "smooth (first, no product)");
     for (int k = 1; k < deg; ++k) {
         with_op(L.A, [&](auto op) {
-            k_cheb_step<T><<<gs, TH, 0, s_>>>(op, b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k], L.d.p,
-                                              xb, done);
+            launch(pdl_, k_cheb_step<T, decltype(op)>, gs, TH, s_, op, b, xa, L.dinv.p,
+                   (T)L.c1[k], (T)L.c2[k], L.d.p, xb, done);
         });
         mark(tag + "smooth pre");
         std::swap(xa, xb);
     }
-    with_op(L.A, [&](auto op) { k_residual<T><<<gs, TH, 0, s_>>>(op, b, xa, L.r.p, done); });
+    with_op(L.A, [&](auto op) {
+        launch(pdl_, k_residual<T, decltype(op)>, gs, TH, s_, op, b, xa, L.r.p, done);
+    });
     mark(tag + "residual");
     T* bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
     if (L.Ro.ok)
-        launch_transfer(L.Ro, (const T*)L.r.p, bc, 0, done, s_);
+        launch_transfer(L.Ro, (const T*)L.r.p, bc, 0, done, s_, pdl_);
     else
-        k_restrict<T><<<row_blocks(L.nc), TH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p,
+        launch(pdl_, k_restrict<T>, row_blocks(L.nc), TH, s_, L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p,
                                                        bc, done);
     FG_CHECK_LAUNCH();
     mark(tag + "restrict");
     launches_ += deg + 2;
     const T* ec = enqueue_vcycle(H, l + 1, bc);
     if (L.Po.ok)
-        launch_transfer(L.Po, ec, xa, 1, done, s_);
+        launch_transfer(L.Po, ec, xa, 1, done, s_, pdl_);
     else
-        k_prolong<T><<<gb, TH, 0, s_>>>(n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
+        launch(pdl_, k_prolong<T>, gb, TH, s_, n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
     mark(tag + "prolong + correct");
     for (int k = 0; k < deg; ++k) {
         with_op(L.A, [&](auto op) {
-            k_cheb_step<T><<<gs, TH, 0, s_>>>(op, b, xa, L.dinv.p, (T)L.c1[k], (T)L.c2[k], L.d.p,
-                                              xb, done);
+            launch(pdl_, k_cheb_step<T, decltype(op)>, gs, TH, s_, op, b, xa, L.dinv.p,
+                   (T)L.c1[k], (T)L.c2[k], L.d.p, xb, done);
         });
         mark(tag + "smooth post");
         std::swap(xa, xb);
@@ -1603,32 +1643,32 @@ void SolverImpl::enqueue_iteration() {
     bool mixed = opt_.precision == FEMGPU_MIXED;
     const int nbq = row_blocks(op64_.threads()), nbn = row_blocks(n);
     with_op(op64_, [&](auto op) {
-        k_pcg_spmv_pq<<<nbq, TH, 0, s_>>>(op, p_.p, q_.p, partial_.p, sc);
+        launch(pdl_, k_pcg_spmv_pq<decltype(op)>, nbq, TH, s_, op, p_.p, q_.p, partial_.p, sc);
     });
     mark("pcg q = A p, p.q partials (fp64)");
-    k_finish<<<1, TH, 0, s_>>>(partial_.p, nbq, FinPq{sc});
+    launch(pdl_, k_finish<FinPq>, 1, TH, s_, partial_.p, nbq, FinPq{sc});
     mark("pcg alpha");
-    k_pcg_update<<<nbn, TH, 0, s_>>>(n, x_.p, r_.p, p_.p, q_.p, mixed ? r32_.p : nullptr,
+    launch(pdl_, k_pcg_update, nbn, TH, s_, n, x_.p, r_.p, p_.p, q_.p, mixed ? r32_.p : nullptr,
                                      partial_.p, sc);
     mark("pcg x, r update, r.r partials");
-    k_finish<<<1, TH, 0, s_>>>(partial_.p, nbn, FinUpdate{sc, tol});
+    launch(pdl_, k_finish<FinUpdate>, 1, TH, s_, partial_.p, nbn, FinUpdate{sc, tol});
     FG_CHECK_LAUNCH();
     mark("pcg stopping test");
     if (mixed) {
         zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
-        k_pcg_dots<float><<<nbn, TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 0, partial_.p, sc);
+        launch(pdl_, k_pcg_dots<float>, nbn, TH, s_, n, r_.p, zf_, q_.p, 1, 0, partial_.p, sc);
         mark("pcg r.z, z.q partials");
-        k_finish<<<1, TH, 0, s_>>>(partial_.p, nbn, FinDots{sc, 1, 0});
+        launch(pdl_, k_finish<FinDots>, 1, TH, s_, partial_.p, nbn, FinDots{sc, 1, 0});
         mark("pcg beta");
-        k_pcg_p<float><<<nbn, TH, 0, s_>>>(n, zf_, p_.p, sc, 0);
+        launch(pdl_, k_pcg_p<float>, nbn, TH, s_, n, zf_, p_.p, sc, 0);
         mark("pcg p = z + beta p");
     } else {
         zd_ = enqueue_vcycle<double>(H64_, 0, r_.p);
-        k_pcg_dots<double><<<nbn, TH, 0, s_>>>(n, r_.p, zd_, q_.p, 0, 0, partial_.p, sc);
+        launch(pdl_, k_pcg_dots<double>, nbn, TH, s_, n, r_.p, zd_, q_.p, 0, 0, partial_.p, sc);
         mark("pcg r.z partials");
-        k_finish<<<1, TH, 0, s_>>>(partial_.p, nbn, FinDots{sc, 0, 0});
+        launch(pdl_, k_finish<FinDots>, 1, TH, s_, partial_.p, nbn, FinDots{sc, 0, 0});
         mark("pcg beta");
-        k_pcg_p<double><<<nbn, TH, 0, s_>>>(n, zd_, p_.p, sc, 0);
+        launch(pdl_, k_pcg_p<double>, nbn, TH, s_, n, zd_, p_.p, sc, 0);
         mark("pcg p = z + beta p");
     }
     FG_CHECK_LAUNCH();
@@ -1637,7 +1677,7 @@ void SolverImpl::enqueue_iteration() {
 // The whole PCG loop as 1 graph: a WHILE conditional node whose body is 1 iteration followed by
 // k_loop_control, so the device runs iteration after iteration with no host round trip.
 void SolverImpl::build_loop_graph() {
-    for (int attempt = 0;; ++attempt) {
+    for (;;) {
         const size_t before = launches_;
         try {
             FG_CUDA(cudaGraphCreate(&graph_, 0));
@@ -1675,8 +1715,14 @@ void SolverImpl::build_loop_graph() {
             exec_ = nullptr;
             graph_ = nullptr;
             launches_ = before;
-            if (attempt > 0 || !tail_on_) throw;
-            tail_on_ = false;
+            // Give up the fused coarse levels first, then the programmatic launches.
+            if (tail_on_ && H32_.tail_from + H64_.tail_from > -2) {
+                tail_on_ = false;
+            } else if (pdl_) {
+                pdl_ = false;
+            } else {
+                throw;
+            }
         }
     }
 }

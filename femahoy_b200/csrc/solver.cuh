@@ -170,6 +170,7 @@ struct Options {
     int max_levels = 30;
     bool graph = true;
     int tail = 0;  // levels of at most this many rows run fused (<= 0: none)
+    int pdl = 1;   // programmatic dependent launch between the iteration's kernels
 };
 
 class SolverImpl {
@@ -242,6 +243,7 @@ class SolverImpl {
     std::vector<std::pair<std::string, cudaEvent_t>>* trace_ = nullptr;
     void mark(const std::string& label);
     bool tail_on_ = true;      // the fused coarse levels (off if a graph would not take them)
+    bool pdl_ = true;          // programmatic dependent launch of the iteration's kernels
     // Seconds of each phase of the setup, in the order first met (reported by describe()).
     std::vector<std::pair<std::string, double>> setup_s_;
     size_t launches_ = 0;      // kernels enqueued by the current solve

@@ -201,6 +201,9 @@ typedef struct femgpu_options {
                              run as 1 cooperative kernel with a grid-wide barrier between steps;
                              0 (default) = every step its own launch (faster on B200 for the
                              box grids measured) */
+    int launch;           /* 0 = each kernel of a PCG iteration may start while the one before
+                             it drains, waiting on the device for its results (programmatic
+                             dependent launch; default); 1 = plain stream-ordered launches */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end

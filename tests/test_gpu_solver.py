@@ -228,3 +228,20 @@ def test_fused_coarse_levels_give_the_same_bits(kind, precision):
         its.append(st.iterations)
     assert its[0] == its[1]
     assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
+
+
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_programmatic_launches_give_the_same_bits(precision):
+    """Each kernel of the loop waits on the device for the one before it, so the launches that
+    may start early compute what the plain stream-ordered launches compute, bit for bit."""
+    h = mg.heat_cube(32, seed=3)
+    A, rhs, _ = _system(h)
+    xs = []
+    for launch in (0, 1):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision,
+                      options=fg.Options(precision=precision, launch=launch)).with_tol(1e-10)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1e-10
+        xs.append(x)
+    assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
