@@ -66,6 +66,7 @@ __device__ __forceinline__ int64_t elem_of_thread() {
 template <class T, int R>
 __global__ void k_bcheb_first(int64_t n, const T* __restrict__ b, const T* __restrict__ dinv,
                               T c1, T* __restrict__ d, T* __restrict__ x) {
+    pdl_wait();
     const int64_t t = elem_of_thread();
     if (t >= n * R) return;
     T v = c1 * dinv[t / R] * b[t];
@@ -78,6 +79,7 @@ template <class T, int R>
 __global__ void __launch_bounds__(BTH)
     k_bcheb_step(SellView<T> A, const T* __restrict__ b, const T* __restrict__ xin,
                  const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d, T* __restrict__ xout) {
+    pdl_wait();
     const int64_t t = elem_of_thread();
     if (t >= A.n * R) return;
     const int row = (int)(t / R), col = (int)(t % R);
@@ -90,6 +92,7 @@ __global__ void __launch_bounds__(BTH)
 template <class T, int R>
 __global__ void __launch_bounds__(BTH)
     k_bresidual(SellView<T> A, const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r) {
+    pdl_wait();
     const int64_t t = elem_of_thread();
     if (t >= A.n * R) return;
     r[t] = b[t] - sell_row_cols<T, R>(A, (int)(t / R), (int)(t % R), x);
@@ -140,6 +143,7 @@ __global__ void __launch_bounds__(BTH)
     k_bcheb_step3(BSell3View<T> A, const T* __restrict__ b, const T* __restrict__ xin,
                   const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d,
                   T* __restrict__ xout) {
+    pdl_wait();
     const int64_t t = elem_of_thread();
     if (t >= A.nb * R) return;
     const int br = (int)(t / R), col = (int)(t % R);
@@ -159,6 +163,7 @@ template <class T, int R>
 __global__ void __launch_bounds__(BTH)
     k_bresidual3(BSell3View<T> A, const T* __restrict__ b, const T* __restrict__ x,
                  T* __restrict__ r) {
+    pdl_wait();
     const int64_t t = elem_of_thread();
     if (t >= A.nb * R) return;
     const int br = (int)(t / R), col = (int)(t % R);
@@ -176,6 +181,7 @@ template <class T, int R>
 __global__ void k_bgather(int64_t rows, const int64_t* __restrict__ ptr,
                           const uint32_t* __restrict__ idx, const T* __restrict__ val,
                           const T* __restrict__ in, T* __restrict__ out, int accumulate) {
+    pdl_wait();
     const int64_t t = elem_of_thread();
     if (t >= rows * R) return;
     const int64_t row = t / R;
@@ -236,6 +242,7 @@ __global__ void __launch_bounds__(32 * DW)
     k_bdense(const int2* __restrict__ tiles, const int64_t* __restrict__ off,
              const int64_t* __restrict__ ioff, const T* __restrict__ inv,
              const T* __restrict__ in, T* __restrict__ out) {
+    pdl_wait();
     // Per warp a buffer of 32 right-side rows; reused at the end for the partial sums.
     constexpr int STAGE = DW * 32 * R, PART = DW * DTH * (R + 1);
     __shared__ T smem[STAGE > PART ? STAGE : PART];
@@ -348,6 +355,7 @@ __global__ void __launch_bounds__(BTH)
                     const double* __restrict__ b, const double* __restrict__ x,
                     double* __restrict__ r, float* __restrict__ r32,
                     double* __restrict__ partial) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     double bb = 0, rr = 0;
@@ -368,6 +376,7 @@ __global__ void __launch_bounds__(BTH)
     k_bpcg_spmv(SellView<double> A, const Chunk* __restrict__ chunks, const double* __restrict__ p,
                 double* __restrict__ q, const int* __restrict__ done,
                 double* __restrict__ partial) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     double pq = 0;
@@ -389,6 +398,7 @@ __global__ void __launch_bounds__(BTH)
                      const double* __restrict__ b, const double* __restrict__ x,
                      double* __restrict__ r, float* __restrict__ r32,
                      double* __restrict__ partial) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     double bb = 0, rr = 0;
@@ -413,6 +423,7 @@ __global__ void __launch_bounds__(BTH)
     k_bpcg_spmv3(BSell3View<double> A, const Chunk* __restrict__ chunks,
                  const double* __restrict__ p, double* __restrict__ q,
                  const int* __restrict__ done, double* __restrict__ partial) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     double pq = 0;
@@ -437,6 +448,7 @@ __global__ void __launch_bounds__(BTH)
                   double* __restrict__ r, const double* __restrict__ p,
                   const double* __restrict__ q, float* __restrict__ r32, BatchScalars sc,
                   double* __restrict__ partial) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     const int seg = ch.sys * R + col;
@@ -461,6 +473,7 @@ __global__ void __launch_bounds__(BTH)
     k_bpcg_dots(const Chunk* __restrict__ chunks, const double* __restrict__ r,
                 const TZ* __restrict__ z, const double* __restrict__ q, int flexible, int init,
                 const int* __restrict__ done, double* __restrict__ partial) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     double rz = 0, zq = 0;
@@ -478,6 +491,7 @@ __global__ void __launch_bounds__(BTH)
 template <int R, class TZ>
 __global__ void k_bpcg_p(const Chunk* __restrict__ chunks, const TZ* __restrict__ z,
                          double* __restrict__ p, BatchScalars sc, int init) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     const int seg = ch.sys * R + col;
@@ -493,6 +507,7 @@ __global__ void k_bpcg_p(const Chunk* __restrict__ chunks, const TZ* __restrict_
 template <int R>
 __global__ void k_bzero_empty(const Chunk* __restrict__ chunks, const double* __restrict__ bb,
                               double* __restrict__ x) {
+    pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     if (bb[ch.sys * R + col] != 0.0) return;
@@ -513,6 +528,7 @@ template <int R>
 __global__ void __launch_bounds__(BTH)
     k_bfinish(int kind, const int* __restrict__ cstart, const double* __restrict__ partial,
               BatchScalars sc, double tol, int max_iter, int flexible, int init) {
+    pdl_wait();
     __shared__ double sa[BTH], sb[BTH];
     const int sys = blockIdx.x;
     const int col = threadIdx.x % R, lane = threadIdx.x / R;
@@ -1118,31 +1134,31 @@ const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b)
     if (L.ns > 0) {
         const int g = (int)((L.ns * R + BTH - 1) / BTH);
         const int deg = (int)L.c1.size();
-        k_bcheb_first<T, R><<<g, BTH, 0, s_>>>(L.ns, b, L.dinv.p, (T)L.c1[0], L.d.p, xa);
+        launch(true, k_bcheb_first<T, R>, g, BTH, s_, L.ns, b, L.dinv.p, (T)L.c1[0], L.d.p, xa);
         const int g3 = (int)((L.ns / 3 * R + BTH - 1) / BTH);
         auto step = [&](const T* xin, T* xout, int k) {
             if (L.block3)
-                k_bcheb_step3<T, R><<<g3, BTH, 0, s_>>>(L.view3(), b, xin, L.dinv.p, (T)L.c1[k],
-                                                         (T)L.c2[k], L.d.p, xout);
+                launch(true, k_bcheb_step3<T, R>, g3, BTH, s_, L.view3(), b, xin, L.dinv.p,
+                       (T)L.c1[k], (T)L.c2[k], L.d.p, xout);
             else
-                k_bcheb_step<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xin, L.dinv.p, (T)L.c1[k],
-                                                      (T)L.c2[k], L.d.p, xout);
+                launch(true, k_bcheb_step<T, R>, g, BTH, s_, L.A.view(), b, xin, L.dinv.p,
+                       (T)L.c1[k], (T)L.c2[k], L.d.p, xout);
         };
         for (int k = 1; k < deg; ++k) {
             step(xa, xb, k);
             std::swap(xa, xb);
         }
         if (L.block3)
-            k_bresidual3<T, R><<<g3, BTH, 0, s_>>>(L.view3(), b, xa, L.r.p);
+            launch(true, k_bresidual3<T, R>, g3, BTH, s_, L.view3(), b, xa, L.r.p);
         else
-            k_bresidual<T, R><<<g, BTH, 0, s_>>>(L.A.view(), b, xa, L.r.p);
+            launch(true, k_bresidual<T, R>, g, BTH, s_, L.A.view(), b, xa, L.r.p);
         T* bc = Ls[l + 1].b.p;
         const int gc = (int)((L.nc * R + BTH - 1) / BTH);
-        k_bgather<T, R><<<gc, BTH, 0, s_>>>(L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p, bc, 0);
+        launch(true, k_bgather<T, R>, gc, BTH, s_, L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p, bc, 0);
         FG_CHECK_LAUNCH();
         launches_ += deg + 2;
         const T* ec = vcycle<T, R>(Ls, l + 1, bc);
-        k_bgather<T, R><<<g, BTH, 0, s_>>>(L.ns, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, 1);
+        launch(true, k_bgather<T, R>, g, BTH, s_, L.ns, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, 1);
         for (int k = 0; k < deg; ++k) {
             step(xa, xb, k);
             std::swap(xa, xb);
@@ -1151,8 +1167,8 @@ const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b)
         launches_ += deg + 1;
     }
     if (L.ndense > 0) {
-        k_bdense<T, R><<<L.ntiles, 32 * DW, 0, s_>>>(L.tiles.p, L.doff.p, L.dioff.p, L.inv.p,
-                                                     b, xa);
+        launch(true, k_bdense<T, R>, L.ntiles, 32 * DW, s_, L.tiles.p, L.doff.p, L.dioff.p,
+               L.inv.p, b, xa);
         FG_CHECK_LAUNCH();
         launches_ += 1;
     }
@@ -1168,8 +1184,8 @@ template <int R>
 void BatchImpl::finish(int kind, int init) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     const double target = (mixed && kind != FIN_RESTART) ? 0.98 * tol : tol;
-    k_bfinish<R><<<B_, BTH, 0, s_>>>(kind, cstart_.p, partial_.p, scalars(), target, max_iter_,
-                                     mixed, init);
+    launch(true, k_bfinish<R>, B_, BTH, s_, kind, cstart_.p, partial_.p, scalars(), target,
+           max_iter_, (int)mixed, init);
     FG_CHECK_LAUNCH();
     launches_ += 1;
 }
@@ -1180,16 +1196,16 @@ void BatchImpl::precondition_and_dots(int init) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     if (mixed) {
         const float* z = vcycle<float, R>(L32_, 0, r32_.p);
-        k_bpcg_dots<R, float><<<nchunks_, BTH, 0, s_>>>(chunks(), r_.p, z, q_.p, 1, init,
-                                                        done_.p, partial_.p);
+        launch(true, k_bpcg_dots<R, float>, nchunks_, BTH, s_, chunks(), r_.p, z, q_.p, 1, init,
+               done_.p, partial_.p);
         finish<R>(FIN_DOTS, init);
-        k_bpcg_p<R, float><<<nchunks_, BTH, 0, s_>>>(chunks(), z, p_.p, scalars(), init);
+        launch(true, k_bpcg_p<R, float>, nchunks_, BTH, s_, chunks(), z, p_.p, scalars(), init);
     } else {
         const double* z = vcycle<double, R>(L64_, 0, r_.p);
-        k_bpcg_dots<R, double><<<nchunks_, BTH, 0, s_>>>(chunks(), r_.p, z, q_.p, 0, init,
-                                                         done_.p, partial_.p);
+        launch(true, k_bpcg_dots<R, double>, nchunks_, BTH, s_, chunks(), r_.p, z, q_.p, 0, init,
+               done_.p, partial_.p);
         finish<R>(FIN_DOTS, init);
-        k_bpcg_p<R, double><<<nchunks_, BTH, 0, s_>>>(chunks(), z, p_.p, scalars(), init);
+        launch(true, k_bpcg_p<R, double>, nchunks_, BTH, s_, chunks(), z, p_.p, scalars(), init);
     }
     FG_CHECK_LAUNCH();
     launches_ += 2;
@@ -1200,14 +1216,14 @@ template <int R>
 void BatchImpl::iteration() {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     if (fine3_)
-        k_bpcg_spmv3<R><<<nchunks_, BTH, 0, s_>>>(fine3(), chunks(), p_.p, q_.p, done_.p,
-                                                  partial_.p);
+        launch(true, k_bpcg_spmv3<R>, nchunks_, BTH, s_, fine3(), chunks(), p_.p, q_.p, done_.p,
+               partial_.p);
     else
-        k_bpcg_spmv<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), p_.p, q_.p, done_.p,
-                                                 partial_.p);
+        launch(true, k_bpcg_spmv<R>, nchunks_, BTH, s_, A64_.view(), chunks(), p_.p, q_.p,
+               done_.p, partial_.p);
     finish<R>(FIN_PQ, 0);
-    k_bpcg_update<R><<<nchunks_, BTH, 0, s_>>>(chunks(), x_.p, r_.p, p_.p, q_.p,
-                                               mixed ? r32_.p : nullptr, scalars(), partial_.p);
+    launch(true, k_bpcg_update<R>, nchunks_, BTH, s_, chunks(), x_.p, r_.p, p_.p, q_.p,
+           mixed ? r32_.p : nullptr, scalars(), partial_.p);
     finish<R>(FIN_UPDATE, 0);
     FG_CHECK_LAUNCH();
     launches_ += 2;
@@ -1248,11 +1264,11 @@ void BatchImpl::launch_loop(const volatile int* cancel) {
 template <int R>
 void BatchImpl::residual(double* r, float* r32) {
     if (fine3_)
-        k_bpcg_residual3<R><<<nchunks_, BTH, 0, s_>>>(fine3(), chunks(), b_.p, x_.p, r, r32,
-                                                      partial_.p);
+        launch(true, k_bpcg_residual3<R>, nchunks_, BTH, s_, fine3(), chunks(), b_.p, x_.p, r,
+               r32, partial_.p);
     else
-        k_bpcg_residual<R><<<nchunks_, BTH, 0, s_>>>(A64_.view(), chunks(), b_.p, x_.p, r, r32,
-                                                     partial_.p);
+        launch(true, k_bpcg_residual<R>, nchunks_, BTH, s_, A64_.view(), chunks(), b_.p, x_.p, r,
+               r32, partial_.p);
     FG_CHECK_LAUNCH();
 }
 

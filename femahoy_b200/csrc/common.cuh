@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "femgpu.h"
@@ -107,6 +108,31 @@ struct DevCsr {
 // Exclusive prefix sum of `n` counts into `out` (n + 1 values; out[n] = total), on `s`.
 void exclusive_scan(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 void exclusive_scan32(const uint32_t* in, int64_t* out, int64_t n, cudaStream_t s);
+
+// Programmatic dependent launch. The kernels of a PCG iteration are launched so that each may
+// start while the one before it drains; every such kernel first waits (griddepcontrol.wait) for
+// the completion and the memory of the kernel before it, so it reads what it would have read
+// without the attribute. On the short kernels of the coarse levels the launch latency this
+// hides is most of their time.
+// (An explicit early trigger, griddepcontrol.launch_dependents after the wait, measured no
+// better on the 128^3 heat solve; the blocks trigger when they exit.)
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static void launch(bool pdl, void (*kernel)(KArgs...), int grid, int block, cudaStream_t s,
+                   Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? &attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    FG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
 
 // A scalar from device memory.
 template <class T>

@@ -35,31 +35,6 @@ static int row_blocks(int64_t rows) {
 }
 constexpr double PIVOT = 1e-10;  // cholesky.rs:22
 
-// Programmatic dependent launch. The kernels of a PCG iteration are launched so that each may
-// start while the one before it drains; every such kernel first waits (griddepcontrol.wait) for
-// the completion and the memory of the kernel before it, so it reads what it would have read
-// without the attribute. On the short kernels of the coarse levels the launch latency this
-// hides is most of their time.
-// (An explicit early trigger, griddepcontrol.launch_dependents after the wait, measured no
-// better on the 128^3 heat solve; the blocks trigger when they exit.)
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-
-template <typename... KArgs, typename... Args>
-static void launch(bool pdl, void (*kernel)(KArgs...), int grid, int block, cudaStream_t s,
-                   Args&&... args) {
-    cudaLaunchConfig_t cfg{};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr{};
-    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr.val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = pdl ? &attr : nullptr;
-    cfg.numAttrs = pdl ? 1 : 0;
-    FG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
-}
-
 // Times a phase of the setup: the host time from its start until the solver's stream has
 // finished the phase's device work.
 struct PhaseTimer {
