@@ -59,10 +59,12 @@ def args():
     p.add_argument("--breakdown", action="store_true",
                    help="print each solver's levels and the device time of each kernel of 1 "
                         "PCG iteration (kernels launched one by one), then exit")
-    p.add_argument("--workload", default="heat", choices=["heat", "batch", "serve"],
-                   help="heat: 1 right side of the 128^3 heat cube (the headline line); batch: "
-                        "256 cantilevers x 16 load cases in 1 batched solve; serve: a Poisson "
-                        "stream of solve requests through the server")
+    p.add_argument("--workload", default="heat",
+                   choices=["heat", "cantilever", "p2beam", "batch", "serve"],
+                   help="heat: 1 right side of the 128^3 heat cube (the headline line); "
+                        "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
+                        "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
+                        "serve: a Poisson stream of solve requests through the server")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -133,6 +135,60 @@ def build_problem(cells):
     return mg.heat_cube(cells, seed=SEED)
 
 
+def build_system(opt):
+    """The device system of a single-solver workload: (A, rhs, unknowns, facts). `facts` holds
+    the workload's text, tolerance, assembly and reduction seconds, and a maker of the oracle's
+    solver for the CPU baseline (reference algorithm, FP64)."""
+    import femahoy_b200 as fg
+    from femahoy_b200 import meshgen as mg
+    import oracle
+    if opt.workload == "cantilever":
+        prob = mg.cantilever_p1()
+        kind, tol = fg.P1_ELASTIC, 1e-10
+        text = ("P1 elasticity cantilever 100x10x10 mm as 40x4x4 hexes x 6 Kuhn tets (3,000 free "
+                "unknowns), E 210 GPa, nu 0.3, clamped at x = 0, 1 MPa on the top face, to 1e-10, "
+                "FP64 and mixed PCG-MG")
+    elif opt.workload == "p2beam":
+        box = mg.box(200, 20, 20, (200.0, 20.0, 20.0))
+        q = fg.Quadratic.new(box.points, box.tets)
+        prob = mg.beam_p2(q.edges, q.tets, mesh=box, seed=SEED)
+        kind, tol = fg.P2_ELASTIC, TOL
+        text = (f"P2 elasticity box beam 200x20x20 mm as 200x20x20 hexes x 6 Kuhn tets (10-node), "
+                f"E 70 GPa, nu 0.33, clamped at x = 0, random traction on x = L (seed {SEED}), "
+                f"p-multigrid P2 -> P1 then geometric levels, to 1e-8")
+    else:
+        prob = build_problem(opt.cells)
+        kind, tol = fg.P1_HEAT, TOL
+        text = (f"P1 heat, {opt.cells}^3 Kuhn box (6 tets/hex), lognormal k seed {SEED}, 1 RHS "
+                f"to 1e-8, mixed precision PCG-MG")
+    t0 = time.perf_counter()
+    K = fg.Csr.assemble(kind, prob.xyz, prob.nodes, prob.coef)
+    assemble_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    A = K.submatrix(prob.free)
+    rhs = fg.reduced_rhs(K, prob.load, prob.values, prob.free)
+    reduce_s = time.perf_counter() - t0
+    del K
+    if opt.workload == "p2beam":
+        P, coarse = fg.prolongation(prob.xyz, box.n, q.edges, prob.free)
+        unknowns = fg.Unknowns.Quadratic(prob.xyz[prob.free // 3], P, coarse)
+
+        def oracle_solver(Ao):
+            Po = oracle.Rect.from_arrays(P.rows, P.cols, P.ptr, P.idx, P.val)
+            return oracle.Solver(Ao, "quadratic", xyz=prob.xyz[prob.free // 3], p=Po,
+                                 coarse=coarse, method="multigrid")
+    else:
+        planes, pts, comp = mg.grid_unknowns(prob)
+        unknowns = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+
+        def oracle_solver(Ao):
+            return oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp,
+                                 method="multigrid")
+    facts = {"text": text, "tol": tol, "assemble_s": assemble_s, "reduce_s": reduce_s,
+             "oracle_solver": oracle_solver}
+    return A, rhs, unknowns, facts
+
+
 def measured_peak():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -153,17 +209,17 @@ def profiled_traffic():
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-def oracle_solve_rate(A, rhs, planes, pts, comp, budget_s=60.0):
-    """The oracle's PCG with the reference's line Gauss-Seidel multigrid (FP64, 1 thread) on
-    the same system: (DOF-solves/s, iterations, solve seconds, setup seconds)."""
+def oracle_solve_rate(A, rhs, make_solver, tol):
+    """The oracle's PCG with the reference's multigrid (FP64, 1 thread) on the same system:
+    (DOF-solves/s, iterations, solve seconds, setup seconds, residual)."""
     import oracle
     ptr, idx, val = A.arrays()
     Ao = oracle.Csr.from_arrays(A.n, ptr, idx, val)
     t0 = time.perf_counter()
-    so = oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp, method="multigrid")
+    so = make_solver(Ao)
     setup = time.perf_counter() - t0
     t0 = time.perf_counter()
-    _, it, res = so.solve(rhs, tol=TOL)
+    _, it, res = so.solve(rhs, tol=tol)
     solve = time.perf_counter() - t0
     return A.n / solve, it, solve, setup, res
 
@@ -266,26 +322,18 @@ def run_ours(opt, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    h = build_problem(opt.cells)
     lib = fg.lib()
-    t0 = time.perf_counter()
-    K = fg.Csr.assemble(fg.P1_HEAT, h.xyz, h.nodes, h.coef)
-    assemble_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    A = K.submatrix(h.free)
-    rhs = fg.reduced_rhs(K, h.load, h.values, h.free)
-    reduce_s = time.perf_counter() - t0
+    A, rhs, unknowns, facts = build_system(opt)
+    tol = facts["tol"]
+    assemble_s, reduce_s = facts["assemble_s"], facts["reduce_s"]
     n_free = A.n
-    del K
-    planes, pts, comp = mg.grid_unknowns(h)
-    unknowns = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
 
     def make(precision):
         t = time.perf_counter()
         s = fg.Solver(A, unknowns, fg.Method.Multigrid,
                       options=fg.Options(precision=precision, format=opt.format,
                                          graph=opt.graph, tail=opt.tail,
-                                         degree=opt.degree, launch=opt.launch)).with_tol(TOL)
+                                         degree=opt.degree, launch=opt.launch)).with_tol(tol)
         return s, time.perf_counter() - t
 
     b = torch.from_numpy(rhs).cuda()
@@ -345,13 +393,15 @@ def run_ours(opt, rank, world, local):
                               "launches": launches, "true_residual": max(res)}), flush=True)
         return
 
-    # The dominant kernel alone: the finest FP32 Chebyshev step (SpMV + smoother update).
+    # The dominant kernel alone: the finest FP32 Chebyshev step (SpMV + smoother update). A
+    # problem at or below the coarsest size (the cantilever) has no smoothing level: its solve
+    # is the dense coarse product and a few PCG kernels, launch- and latency-bound.
     kms, kbytes = ctypes.c_double(), ctypes.c_double()
-    fg._lib.check(lib.femgpu_solver_kernel_time(mixed.handle, 0, 50, ctypes.byref(kms),
-                                                ctypes.byref(kbytes)))
+    roof_ok = lib.femgpu_solver_kernel_time(mixed.handle, 0, 50, ctypes.byref(kms),
+                                            ctypes.byref(kbytes)) == 0
     peak, peak_kind = measured_peak()
-    achieved = kbytes.value / (kms.value * 1e-3) / 1e9
-    traffic = profiled_traffic()
+    achieved = kbytes.value / (kms.value * 1e-3) / 1e9 if roof_ok else None
+    traffic = profiled_traffic() if opt.workload == "heat" and opt.cells == N_CELLS else None
 
     # e2e: the same solve through the host C ABI from pinned host memory (copies inside).
     hb = torch.from_numpy(rhs).pin_memory()
@@ -389,11 +439,12 @@ def run_ours(opt, rank, world, local):
     cpu = None
     if rank == 0 and world == 1 and not opt.no_cpu_baseline:
         try:
-            rate, cit, csolve, csetup, cres = oracle_solve_rate(A, rhs, planes, pts, comp)
+            rate, cit, csolve, csetup, cres = oracle_solve_rate(A, rhs, facts["oracle_solver"],
+                                                                tol)
             cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                   "sample": f"1 full solve of the same {opt.cells}^3 system by the oracle "
-                             f"(reference algorithm: FP64 PCG + line Gauss-Seidel MG), "
-                             f"{cit} iterations, {csolve:.1f} s (setup {csetup:.1f} s "
+                   "sample": f"1 full solve of the same system by the oracle (reference "
+                             f"algorithm: FP64 PCG + the reference's multigrid smoothers), "
+                             f"{cit} iterations, {csolve:.2f} s (setup {csetup:.1f} s "
                              f"excluded)"}
         except Exception as e:  # the baseline is reported, never the product
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port",
@@ -406,10 +457,10 @@ def run_ours(opt, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer",
         "data": "synthetic",
         "config": {
-            "workload": f"P1 heat, {opt.cells}^3 Kuhn box (6 tets/hex), lognormal k seed {SEED}, "
-                        f"1 RHS to 1e-8, mixed precision PCG-MG",
-            "free_dofs": n_free, "tol": TOL, "levels": levels,
-            "flush": "inputs larger than L2 (the FP64 operator alone is 0.4 GB)",
+            "workload": facts["text"],
+            "free_dofs": n_free, "tol": tol, "levels": levels,
+            "flush": ("inputs larger than L2" if mixed_bytes > (256 << 20) else
+                      "none: the whole problem fits L2; launch- and latency-bound"),
             "parallelism": f"replicas x{world}",
         },
         "latency_ms": {"p50": float(np.percentile(lat_ms, 50)),
@@ -425,11 +476,14 @@ def run_ours(opt, rank, world, local):
         "including_setup": world * n_free / (assemble_s + reduce_s + setup_mixed
                                              + ms_max / opt.steps / 1e3),
         "device_bytes": mixed_bytes,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "kernel": "k_cheb_step<float> (finest level)",
-                     "bytes_per_launch": kbytes.value, "launch_ms": kms.value,
-                     "traffic": traffic.get("bytes_per_launch") if traffic else None},
+        "roofline": ({"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                      "frac": achieved / peak, "peak_kind": peak_kind,
+                      "kernel": "k_cheb_step<float> (finest level)",
+                      "bytes_per_launch": kbytes.value, "launch_ms": kms.value,
+                      "traffic": traffic.get("bytes_per_launch") if traffic else None}
+                     if roof_ok else
+                     {"bound": "latency", "achieved": None, "peak": peak, "unit": "GB/s",
+                      "frac": None, "note": "no smoothing level: launch- and latency-bound"}),
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * 8 * n_free,
                 "d2h_bytes_per_step": 8 * n_free},
