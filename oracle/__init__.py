@@ -40,6 +40,7 @@ def _load():
         "orc_csr_free": (None, [P]),
         "orc_add_element": (I, [P, P, I, P, P, S]),
         "orc_mul": (None, [P, P, P]),
+        "orc_set_threads": (None, [C.c_int]),
         "orc_submatrix": (P, [P, P, S]),
         "orc_reduced_rhs": (None, [P, P, P, P, S, P]),
         "orc_tet_gradients": (None, [P, P, P]),
@@ -158,6 +159,12 @@ class Csr:
         if _lib.orc_assemble(self.h, kind, _p(xyz), _p(nodes), nodes.shape[0], _p(coef), err,
                              512):
             raise OracleError(err.value.decode())
+
+
+def set_threads(n):
+    """Host threads of the restatement's matrix products and PCG dot products (1: the
+    reference's single thread, the default)."""
+    _lib.orc_set_threads(int(n))
 
 
 def pattern(n, elements):

@@ -49,6 +49,8 @@ void tet_points(const double* xyz, const uint32_t* t, Vec3 p[4]) {
 
 extern "C" {
 
+void orc_set_threads(int n) { set_threads(n); }
+
 // ---------------------------------------------------------------- Csr
 void* orc_pattern(size_t n, const uint32_t* elements, size_t nel, int m) {
     return new Csr(pattern(n, elements, nel, m));

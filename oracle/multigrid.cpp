@@ -4,6 +4,7 @@
 // crates/fem/src/solve.rs:87-250 (the solver dispatch).
 #include <algorithm>
 #include <cmath>
+#include <thread>
 #include <tuple>
 
 #include "oracle.hpp"
@@ -273,6 +274,22 @@ void Multigrid::cycle(size_t l, const double* b, double* x) const {
 
 static double dot(const double* u, const double* v, size_t n) {
     if (n == 0) return -0.0;
+    const size_t t = (size_t)threads();
+    if (t > 1 && n >= 65536) {
+        // The all-cores baseline: fixed chunks, their sums added in chunk order.
+        std::vector<double> part(t, 0.0);
+        std::vector<std::thread> pool;
+        for (size_t k = 0; k < t; ++k)
+            pool.emplace_back([&, k] {
+                double s = 0.0;
+                for (size_t i = n * k / t; i < n * (k + 1) / t; ++i) s += u[i] * v[i];
+                part[k] = s;
+            });
+        for (auto& th : pool) th.join();
+        double s = 0.0;
+        for (double p : part) s += p;
+        return s;
+    }
     double s = u[0] * v[0];
     for (size_t i = 1; i < n; ++i) s += u[i] * v[i];
     return s;

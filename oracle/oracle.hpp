@@ -32,6 +32,11 @@ struct Error : std::runtime_error {
 
 // ---------------------------------------------------------------- sparse.rs
 // sparse.rs:12-17: square CSR with both triangles, sorted columns per row.
+// Host threads of the parallel parts of the restatement: the matrix product and the PCG dot
+// products (the reference runs on 1 thread; 1 is the default and gives its arithmetic).
+void set_threads(int n);
+int threads();
+
 struct Csr {
     size_t n = 0;
     vector<size_t> ptr;

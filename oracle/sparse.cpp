@@ -1,6 +1,7 @@
 // Oracle (test infrastructure): restatement of crates/fem/src/sparse.rs.
 #include <algorithm>
 #include <numeric>
+#include <thread>
 
 #include "oracle.hpp"
 
@@ -82,12 +83,28 @@ vector<double> Csr::diagonal() const {
 }
 
 // sparse.rs:96-105
+static int g_threads = 1;
+void set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+int threads() { return g_threads; }
+
+// Each row is summed by 1 thread in column order, so the product is the same on any number of
+// threads.
 void Csr::mul(const double* x, double* y) const {
-    for (size_t i = 0; i < n; ++i) {
-        double s = 0.0;
-        for (size_t k = ptr[i]; k < ptr[i + 1]; ++k) s += val[k] * x[idx[k]];
-        y[i] = s;
+    auto rows = [&](size_t lo, size_t hi) {
+        for (size_t i = lo; i < hi; ++i) {
+            double s = 0.0;
+            for (size_t k = ptr[i]; k < ptr[i + 1]; ++k) s += val[k] * x[idx[k]];
+            y[i] = s;
+        }
+    };
+    const size_t t = (size_t)g_threads;
+    if (t <= 1 || n < 65536) {
+        rows(0, n);
+        return;
     }
+    std::vector<std::thread> pool;
+    for (size_t k = 0; k < t; ++k) pool.emplace_back(rows, n * k / t, n * (k + 1) / t);
+    for (auto& th : pool) th.join();
 }
 
 // sparse.rs:137-148
