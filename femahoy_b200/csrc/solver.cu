@@ -166,6 +166,19 @@ void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operato
     out->stencil = false;
     out->n = d.n;
     out->nnz = d.nnz;
+    // Elasticity levels (node-major unknowns, grid order): the 3x3-block form, 40 bytes per 9
+    // FP32 entries instead of 72.
+    std::vector<int64_t> bp;
+    std::vector<uint32_t> bc;
+    std::vector<T> bv;
+    if (allow && make_bsell3<T>(h, &bp, &bc, &bv)) {
+        out->block3 = true;
+        out->b3ptr.upload(bp.data(), bp.size(), s);
+        out->b3col.upload(bc.data(), bc.size(), s);
+        out->b3val.upload(bv.data(), bv.size(), s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        return;
+    }
     make_sell<T>(d, C, &out->sell, s);
 }
 template void make_operator<double>(const HostCsr&, const DevCsr&, int, bool, Operator<double>*,
@@ -178,7 +191,9 @@ template void make_operator<float>(const HostCsr&, const DevCsr&, int, bool, Ope
 // stencil) and K = 14 (Galerkin levels: 27 points); these get unrolled kernels.
 template <class T, class F>
 static void with_op(const Operator<T>& op, F&& f) {
-    if (!op.stencil)
+    if (op.block3)
+        f(Block3Op<T>{op.b3view(), (int)op.n});
+    else if (!op.stencil)
         f(SellOp<T>{op.sell.view()});
     else if (op.unrolled && op.K == 8)
         f(StencilOpK<T, 8>{op.sview()});
@@ -1129,7 +1144,9 @@ std::vector<int64_t> SolverImpl::level_sizes() const { return sizes_; }
 template <class T>
 static std::string describe_op(const Operator<T>& op) {
     char buf[200];
-    if (!op.stencil) {
+    if (op.block3) {
+        std::snprintf(buf, sizeof buf, "3x3-block sell C=%d nnz=%lld", B3C, (long long)op.nnz);
+    } else if (!op.stencil) {
         std::snprintf(buf, sizeof buf, "sell C=%d nnz=%lld", op.sell.C, (long long)op.nnz);
     } else {
         std::snprintf(buf, sizeof buf, "stencil K=%d %s (probe %.1f / %.1f us) nnz=%lld", op.K,
@@ -1340,7 +1357,9 @@ static void build_tail(Hierarchy<T>* H, int tail, cudaStream_t s) {
     if (H->levels.size() - from > (size_t)TAIL_MAXLEVELS) return;
     for (size_t l = from; l < H->levels.size(); ++l) {
         const MgLevel<T>& L = H->levels[l];
-        if (L.c1.size() > (size_t)TAIL_MAXDEG || L.n >= 0x7fffffff) return;
+        // The fused kernel reads stencil and SELL levels; a 3x3-block level keeps separate
+        // launches.
+        if (L.c1.size() > (size_t)TAIL_MAXDEG || L.n >= 0x7fffffff || L.A.block3) return;
         TailLevel<T> t{};
         t.n = (int)L.n;
         t.nc = (int)L.nc;

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "block3.cuh"
 #include "hierarchy.hpp"
 #include "ops.cuh"
 #include "sell.cuh"
@@ -33,6 +34,7 @@ void make_sell(const DevCsr& a, int C, Sell<T>* out, cudaStream_t s);
 template <class T>
 struct Operator {
     bool stencil = false;
+    bool block3 = false;  // the 3x3-block form (elasticity), else SELL-C, when not a stencil
     bool unrolled = false;  // the compile-time-K kernel (K = 8 or 14), chosen by timing
     double probe_ms[2] = {0, 0};  // the timed product: runtime K, compile-time K
     int64_t n = 0, nnz = 0;
@@ -40,7 +42,15 @@ struct Operator {
     int K = 0;
     std::vector<int64_t> off;
     DevBuf<T> coef;
-    int64_t threads() const { return stencil ? n : sell.nslices * sell.C; }
+    DevBuf<int64_t> b3ptr;
+    DevBuf<uint32_t> b3col;
+    DevBuf<T> b3val;
+    BSell3View<T> b3view() const { return {n / 3, b3ptr.p, b3col.p, b3val.p}; }
+    int64_t threads() const {
+        if (stencil) return n;
+        if (block3) return 3 * ((n / 3 + B3C - 1) / B3C) * B3C;
+        return sell.nslices * sell.C;
+    }
     StencilView<T> sview() const {
         StencilView<T> v{};
         v.n = (int)n;
@@ -49,11 +59,14 @@ struct Operator {
         v.coef = coef.p;
         return v;
     }
-    size_t bytes() const { return sell.bytes() + coef.bytes(); }
+    size_t bytes() const {
+        return sell.bytes() + coef.bytes() + b3ptr.bytes() + b3col.bytes() + b3val.bytes();
+    }
     // The bytes one product reads and writes, each value once: the stored coefficients (and
     // indices), x and y.
     double stream_bytes() const {
         if (stencil) return (double)K * n * sizeof(T) + 2.0 * n * sizeof(T);
+        if (block3) return (double)nnz / 9 * (9 * sizeof(T) + 4) + 2.0 * n * sizeof(T);
         return (double)nnz * (sizeof(T) + 4) + 2.0 * n * sizeof(T);
     }
 };

@@ -216,9 +216,13 @@ def test_fused_coarse_levels_give_the_same_bits(kind, precision):
         p = mg.cantilever_p1(dims=(48, 8, 8), lengths=(120.0, 20.0, 20.0))
     A, rhs, _ = _system(p)
     xs, its = [], []
+    # Elasticity in scalar SELL form (the fused kernel reads stencils and SELL; 3x3-block levels
+    # keep separate launches).
+    fmt = 0 if kind == "heat" else 1
     for tail in (65536, 0):
         s = fg.Solver(A, _grid(p), fg.Method.Multigrid, precision=precision,
-                      options=fg.Options(precision=precision, tail=tail, coarsest=200))
+                      options=fg.Options(precision=precision, tail=tail, coarsest=200,
+                                         format=fmt))
         s = s.with_tol(1e-10)
         assert ("cooperative kernel" in s.describe()) == (tail > 0)
         x = np.zeros(A.n)
@@ -245,3 +249,21 @@ def test_programmatic_launches_give_the_same_bits(precision):
         assert st.true_residual <= 1e-10
         xs.append(x)
     assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
+
+
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_block_operators_match_sell_for_elasticity(precision):
+    """Elasticity levels in 3x3-block form (each node's 3 rows share their block columns) solve
+    to the same solution as in scalar SELL form, both against the direct oracle."""
+    p = mg.cantilever_p1(dims=(48, 8, 8), lengths=(120.0, 20.0, 20.0))
+    A, rhs, Ao = _system(p)
+    xd, _ = oracle.direct_solve(Ao, p.xyz[p.free // 3], rhs)
+    for fmt in (0, 1):
+        s = fg.Solver(A, _grid(p), fg.Method.Multigrid, precision=precision,
+                      options=fg.Options(precision=precision, coarsest=200, format=fmt))
+        s = s.with_tol(1e-10)
+        assert ("3x3-block" in s.describe()) == (fmt == 0)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1.2e-10
+        assert _rel(x, xd) <= 1e-6
