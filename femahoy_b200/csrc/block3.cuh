@@ -5,7 +5,9 @@
 // in FP32 (36 of values, 4 of index) against 72 for the same 9 entries in scalar SELL.
 #pragma once
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include "hierarchy.hpp"
@@ -53,31 +55,50 @@ struct Block3Op {
     }
 };
 
-// The 3x3-block SELL form of `a`, if every node's 3 rows have the same columns and the
-// columns come in aligned triples; false (and nothing built) otherwise.
+// Runs f(lo, hi) over [0, n) split among the host threads.
+template <class F>
+inline void parallel_ranges(int64_t n, F&& f) {
+    const int64_t t = std::max<int64_t>(1, std::min<int64_t>(host_threads(), n / 4096));
+    if (t == 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (int64_t k = 0; k < t; ++k) pool.emplace_back([&, k] { f(n * k / t, n * (k + 1) / t); });
+    for (auto& th : pool) th.join();
+}
+
+// The 3x3-block SELL form of `a`, if every node's 3 rows have the same columns and the columns
+// come in aligned triples; false (and nothing built) otherwise. The block rows are checked and
+// filled on all host threads.
 template <class T>
 inline bool make_bsell3(const HostCsr& a, std::vector<int64_t>* sptr, std::vector<uint32_t>* cols,
-                 std::vector<T>* vals) {
+                        std::vector<T>* vals) {
     if (a.n % 3 != 0 || a.n / 3 >= 0x7fffffff) return false;
     const int64_t nb = a.n / 3;
     std::vector<int> width(nb);
-    for (int64_t I = 0; I < nb; ++I) {
-        const int64_t r0 = 3 * I;
-        const int64_t len = a.ptr[r0 + 1] - a.ptr[r0];
-        if (len % 3 != 0) return false;
-        for (int q = 1; q < 3; ++q) {
-            if (a.ptr[r0 + q + 1] - a.ptr[r0 + q] != len) return false;
-            for (int64_t k = 0; k < len; ++k)
-                if (a.idx[a.ptr[r0 + q] + k] != a.idx[a.ptr[r0] + k]) return false;
+    std::atomic<bool> ok{true};
+    parallel_ranges(nb, [&](int64_t lo, int64_t hi) {
+        for (int64_t I = lo; I < hi && ok.load(std::memory_order_relaxed); ++I) {
+            const int64_t r0 = 3 * I;
+            const int64_t len = a.ptr[r0 + 1] - a.ptr[r0];
+            bool good = len % 3 == 0;
+            for (int q = 1; q < 3 && good; ++q) {
+                if (a.ptr[r0 + q + 1] - a.ptr[r0 + q] != len) good = false;
+                for (int64_t k = 0; k < len && good; ++k)
+                    if (a.idx[a.ptr[r0 + q] + k] != a.idx[a.ptr[r0] + k]) good = false;
+            }
+            for (int64_t k = 0; k < len && good; k += 3) {
+                const uint32_t c = a.idx[a.ptr[r0] + k];
+                if (c % 3 != 0 || a.idx[a.ptr[r0] + k + 1] != c + 1 ||
+                    a.idx[a.ptr[r0] + k + 2] != c + 2)
+                    good = false;
+            }
+            if (!good) ok.store(false);
+            width[I] = (int)(len / 3);
         }
-        for (int64_t k = 0; k < len; k += 3) {
-            const uint32_t c = a.idx[a.ptr[r0] + k];
-            if (c % 3 != 0 || a.idx[a.ptr[r0] + k + 1] != c + 1 ||
-                a.idx[a.ptr[r0] + k + 2] != c + 2)
-                return false;
-        }
-        width[I] = (int)(len / 3);
-    }
+    });
+    if (!ok.load()) return false;
     const int64_t nslices = (nb + B3C - 1) / B3C;
     sptr->assign(nslices + 1, 0);
     for (int64_t sl = 0; sl < nslices; ++sl) {
@@ -87,24 +108,26 @@ inline bool make_bsell3(const HostCsr& a, std::vector<int64_t>* sptr, std::vecto
     }
     cols->assign((*sptr)[nslices], 0);
     vals->assign((size_t)(*sptr)[nslices] * 9, (T)0);
-    for (int64_t I = 0; I < nb; ++I) {
-        const int64_t sl = I / B3C, r = I % B3C, base = (*sptr)[sl];
-        const int w = (int)(((*sptr)[sl + 1] - base) / B3C);
-        for (int k = 0; k < w; ++k) {
-            const int64_t blk = base + (int64_t)k * B3C + r;
-            if (k < width[I]) {
-                const int64_t e = a.ptr[3 * I] + 3 * k;
-                (*cols)[blk] = a.idx[e] / 3;
-                for (int q = 0; q < 3; ++q)
-                    for (int c = 0; c < 3; ++c)
-                        (*vals)[(size_t)blk * 9 + 3 * q + c] = (T)a.val[a.ptr[3 * I + q] + 3 * k + c];
-            } else {
-                (*cols)[blk] = (uint32_t)I;  // padding: value 0, the block row's own x
+    parallel_ranges(nb, [&](int64_t lo, int64_t hi) {
+        for (int64_t I = lo; I < hi; ++I) {
+            const int64_t sl = I / B3C, r = I % B3C, base = (*sptr)[sl];
+            const int w = (int)(((*sptr)[sl + 1] - base) / B3C);
+            for (int k = 0; k < w; ++k) {
+                const int64_t blk = base + (int64_t)k * B3C + r;
+                if (k < width[I]) {
+                    const int64_t e = a.ptr[3 * I] + 3 * k;
+                    (*cols)[blk] = a.idx[e] / 3;
+                    for (int q = 0; q < 3; ++q)
+                        for (int c = 0; c < 3; ++c)
+                            (*vals)[(size_t)blk * 9 + 3 * q + c] =
+                                (T)a.val[a.ptr[3 * I + q] + 3 * k + c];
+                } else {
+                    (*cols)[blk] = (uint32_t)I;  // padding: value 0, the block row's own x
+                }
             }
         }
-    }
+    });
     return true;
 }
-
 
 }  // namespace femgpu

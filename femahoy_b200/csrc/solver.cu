@@ -17,6 +17,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <type_traits>
 
@@ -1049,7 +1050,8 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
 }
 
 // lambda_max of D^-1 A by the power method in the D inner product (15 steps), on the device.
-double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
+template <class T>
+double lambda_max(const Operator<T>& A, const double* dg, cudaStream_t s,
                   DevBuf<double>& partial) {
     int64_t n = A.n;
     // out[0..1]: v.Av and v.Dv of this step; out[2..3]: |w|^2 (and an unused 0).
@@ -1075,6 +1077,10 @@ double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
     }
     return lam;
 }
+template double lambda_max<double>(const Operator<double>&, const double*, cudaStream_t,
+                                   DevBuf<double>&);
+template double lambda_max<float>(const Operator<float>&, const double*, cudaStream_t,
+                                  DevBuf<double>&);
 
 void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
                std::vector<double>* c2) {
@@ -1306,29 +1312,45 @@ static void make_offset(const HostRect& M, OffsetTransfer<T>* out, cudaStream_t 
     out->ok = false;
     if (M.rows >= 0x7fffffff || M.cols >= 0x7fffffff) return;
     std::vector<int> base(M.rows, 0);
+    // The rows' bases and each thread's set of offsets (giving up past MAXK), then their union.
+    std::mutex m;
     std::vector<int64_t> offs;
-    for (int64_t i = 0; i < M.rows; ++i) {
-        if (M.ptr[i] == M.ptr[i + 1]) continue;
-        uint32_t b = M.idx[M.ptr[i]];
-        for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) b = std::min(b, M.idx[k]);
-        base[i] = (int)b;
-        for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
-            const int64_t o = (int64_t)M.idx[k] - b;
-            if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
-                if (offs.size() == MAXK) return;
-                offs.push_back(o);
+    std::atomic<bool> fits{true};
+    parallel_ranges(M.rows, [&](int64_t lo, int64_t hi) {
+        std::vector<int64_t> mine;
+        for (int64_t i = lo; i < hi && fits.load(std::memory_order_relaxed); ++i) {
+            if (M.ptr[i] == M.ptr[i + 1]) continue;
+            uint32_t b = M.idx[M.ptr[i]];
+            for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) b = std::min(b, M.idx[k]);
+            base[i] = (int)b;
+            for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
+                const int64_t o = (int64_t)M.idx[k] - b;
+                if (std::find(mine.begin(), mine.end(), o) == mine.end()) {
+                    if (mine.size() == MAXK) {
+                        fits.store(false);
+                        return;
+                    }
+                    mine.push_back(o);
+                }
             }
         }
-    }
+        std::lock_guard<std::mutex> g(m);
+        for (int64_t o : mine)
+            if (std::find(offs.begin(), offs.end(), o) == offs.end()) offs.push_back(o);
+    });
+    if (!fits.load() || offs.size() > (size_t)MAXK) return;
     std::sort(offs.begin(), offs.end());
     const int K = (int)offs.size();
     std::vector<T> w((size_t)K * M.rows, (T)0);
-    for (int64_t i = 0; i < M.rows; ++i)
-        for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
-            const int64_t o = (int64_t)M.idx[k] - base[i];
-            const int slot = (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
-            w[(size_t)slot * M.rows + i] = (T)M.val[k];
-        }
+    parallel_ranges(M.rows, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i)
+            for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
+                const int64_t o = (int64_t)M.idx[k] - base[i];
+                const int slot =
+                    (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
+                w[(size_t)slot * M.rows + i] = (T)M.val[k];
+            }
+    });
     out->rows = M.rows;
     out->cols = M.cols;
     out->off.assign(offs.begin(), offs.end());
@@ -1440,15 +1462,10 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
             throw Failure(FEMGPU_ERR_NOT_SPD,
                           "the matrix is not positive definite: it has a diagonal entry that is "
                           "not above 0");
-        Operator<double> a64;
-        const Operator<double>* ap = nullptr;
-        if (l == 0) {
-            ap = &op64_;
-        } else {
-            make_operator<double>(mats[l], d, C, opt_.format == 0, &a64, s_);
-            ap = &a64;
-        }
-        lv.lambda = lambda_max(*ap, dg.p, s_, partial_);
+        // The finest level's lambda_max from the exact FP64 operator; a coarser level's from
+        // its own (FP32 in the mixed form, the products accumulated in FP64).
+        lv.lambda = l == 0 ? lambda_max(op64_, dg.p, s_, partial_)
+                           : lambda_max(lv.A, dg.p, s_, partial_);
         std::vector<double> hd = dg.to_host(s_);
         std::vector<double> inv(lv.n);
         for (int64_t i = 0; i < lv.n; ++i) inv[i] = 1.0 / hd[i];

@@ -82,7 +82,8 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s);
 void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s);
 HostCsr download_csr(const DevCsr& d, cudaStream_t s);
 HostRect transpose(const HostRect& p);
-double lambda_max(const Operator<double>& A, const double* dg, cudaStream_t s,
+template <class T>
+double lambda_max(const Operator<T>& A, const double* dg, cudaStream_t s,
                   DevBuf<double>& partial);
 void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
                std::vector<double>* c2);
