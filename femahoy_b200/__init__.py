@@ -4,18 +4,21 @@ coarse Cholesky) on one B200, behind the C ABI of include/femgpu.h (libfemgpu.so
 
 The Python names mirror the reference crate: ``Csr`` (sparse.rs), ``Solver``, ``Unknowns``,
 ``Method``, ``Crossover``, ``Stats`` (solve.rs), ``Level`` (multigrid.rs), ``prolongation``
-(pmultigrid.rs), ``Quadratic`` (tet10.rs) and ``reduced_rhs`` (heat.rs).
+(pmultigrid.rs), ``Quadratic`` (tet10.rs) and ``reduced_rhs`` (heat.rs); ``Recovery`` and
+``Peak`` are the post-solve loop of elastic_tet.rs:367-427.
 """
 from ._lib import (COLOUR, FP64, GATHER, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC, FemError,
                    LIB_PATH, lib)
 from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT_LIMIT,
                     Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
                     prolongation, reduced_rhs)
+from .recover import Peak, Recovery
 from .sparse import Csr, Rect, colour
 
 __all__ = [
     "COLOUR", "FP64", "GATHER", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "FemError",
     "LIB_PATH", "lib", "PCG_MAX_ITER", "PCG_TOL", "STEADY_DIRECT_LIMIT",
     "TRANSIENT_DIRECT_LIMIT", "Crossover", "Level", "Method", "Options", "Quadratic", "Solver",
-    "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour",
+    "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
+    "Recovery",
 ]

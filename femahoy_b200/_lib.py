@@ -70,6 +70,13 @@ class Stats_t(C.Structure):
                 ("launches", C.c_size_t)]
 
 
+class Peak_t(C.Structure):
+    _fields_ = [("mises", C.c_double), ("element", C.c_int64), ("local", C.c_int32),
+                ("point", C.c_uint32), ("singular", C.c_int32), ("pad", C.c_int32),
+                ("regular_mises", C.c_double), ("regular_element", C.c_int64),
+                ("regular_local", C.c_int32), ("regular_point", C.c_uint32)]
+
+
 _lib = None
 
 # Every symbol of include/femgpu.h with its signature.
@@ -150,6 +157,18 @@ SIGNATURES = {
     "femgpu_batch_bytes": (C.c_size_t, [C.c_void_p]),
     "femgpu_batch_stream": (C.c_void_p, [C.c_void_p]),
     "femgpu_batch_free": (None, [C.c_void_p]),
+    "femgpu_recovery_new": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                      C.c_void_p, C.POINTER(C.c_void_p)]),
+    "femgpu_recovery_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_recovery_run_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_recovery_last_time": (C.c_int, [C.c_void_p, C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]),
+    "femgpu_recovery_bytes": (C.c_size_t, [C.c_void_p]),
+    "femgpu_recovery_stream": (C.c_void_p, [C.c_void_p]),
+    "femgpu_recovery_free": (None, [C.c_void_p]),
 }
 
 

@@ -1,0 +1,105 @@
+"""Post-solve recovery of P2 elasticity (include/femgpu.h ``femgpu_recovery_*``): the strain and
+the stress at the 10 points of each cell, their mean at each point, the von Mises and principal
+stresses of the means, and the peak von Mises stress of each part, as the loop of
+crates/fem/src/elastic_tet.rs:367-427 and elastic_tet.rs:482-483.
+
+``Recovery(xyz, tets10, coef)`` keeps the mesh side on the device (a record of constants per
+cell and the cells of each point); ``run(u)`` recovers from the full displacement (3 values per
+point). Stress order xx, yy, zz, xy, yz, xz; strain as tensor components in the same order.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclass
+class Peak:
+    """The reference's ``Peak`` of 1 part (crates/fem/src/elastic.rs:186-195), with the cell
+    and the point of each value. ``regular_element`` -1 is ``None``."""
+    mises: float
+    element: int
+    local: int
+    point: int
+    singular: bool
+    regular_mises: float
+    regular_element: int
+    regular_local: int
+    regular_point: int
+
+    @classmethod
+    def of(cls, p):
+        return cls(p.mises, p.element, p.local, p.point, bool(p.singular), p.regular_mises,
+                   p.regular_element, p.regular_local, p.regular_point)
+
+
+class Recovery:
+    def __init__(self, xyz, tets10, coef, *, expansion=None, part=None, nparts=1,
+                 singular=None):
+        xyz = L.arr(xyz, np.float64).reshape(-1, 3)
+        t10 = L.arr(tets10, np.uint32).reshape(-1, 10)
+        coef = L.arr(coef, np.float64).reshape(-1, 2)
+        exp = None if expansion is None else L.arr(expansion, np.float64).reshape(-1, 3)
+        part = None if part is None else L.arr(part, np.uint32)
+        sing = None if singular is None else L.arr(singular, np.uint8)
+        h = C.c_void_p()
+        L.check(L.lib().femgpu_recovery_new(len(xyz), L.ptr(xyz), len(t10), L.ptr(t10),
+                                            L.ptr(coef), L.ptr(exp), L.ptr(part), nparts,
+                                            L.ptr(sing), C.byref(h)))
+        self._h = h.value
+        self._free = L.lib().femgpu_recovery_free
+        self.npoints = len(xyz)
+        self.ncells = len(t10)
+        self.nparts = nparts
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._free(h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def run(self, u, dtemp=None, *, peaks=True, principal=True):
+        """Host arrays in and out: a dict of stress (n, 6), strain (n, 6), mises (n,),
+        principal (n, 3) or None, and peaks (a list of Peak, 1 per part) or None."""
+        n = self.npoints
+        u = L.arr(u, np.float64).reshape(-1)
+        if len(u) != 3 * n:
+            raise L.FemError(L.INVALID, "u holds 3 values per point")
+        dt = None if dtemp is None else L.arr(dtemp, np.float64)
+        stress, strain, mises = np.empty((n, 6)), np.empty((n, 6)), np.empty(n)
+        pr = np.empty((n, 3)) if principal else None
+        pk = (L.Peak_t * self.nparts)() if peaks else None
+        L.check(L.lib().femgpu_recovery_run(self._h, L.ptr(u), L.ptr(dt), L.ptr(stress),
+                                            L.ptr(strain), L.ptr(mises), L.ptr(pr),
+                                            C.cast(pk, C.c_void_p) if peaks else None))
+        return {"stress": stress, "strain": strain, "mises": mises, "principal": pr,
+                "peaks": [Peak.of(p) for p in pk] if peaks else None}
+
+    def run_device(self, u, stress, strain, *, dtemp=None, mises=None, principal=None,
+                   peaks=True):
+        """Device buffers (torch CUDA float64 tensors, contiguous) in and out; returns the list
+        of Peak or None. Returns when the results are written."""
+        def dp(t):
+            return None if t is None else C.c_void_p(t.data_ptr())
+        pk = (L.Peak_t * self.nparts)() if peaks else None
+        L.check(L.lib().femgpu_recovery_run_device(
+            self._h, dp(u), dp(dtemp), dp(stress), dp(strain), dp(mises), dp(principal),
+            C.cast(pk, C.c_void_p) if peaks else None))
+        return [Peak.of(p) for p in pk] if peaks else None
+
+    def last_time(self):
+        """(ms, algorithmic bytes) of the recovery kernels of the last run (CUDA events)."""
+        ms, by = C.c_double(), C.c_double()
+        L.check(L.lib().femgpu_recovery_last_time(self._h, C.byref(ms), C.byref(by)))
+        return ms.value, by.value
+
+    def bytes(self):
+        return int(L.lib().femgpu_recovery_bytes(self._h))

@@ -344,6 +344,62 @@ size_t femgpu_batch_bytes(const femgpu_batch* b);
 void* femgpu_batch_stream(const femgpu_batch* b);
 void femgpu_batch_free(femgpu_batch* b);
 
+/* ---------------------------------------------------------------- post-solve recovery */
+
+/* The strain and the stress of a solved P2 elasticity model at the 10 points of each cell,
+ * the mean at each point, and the peak of each part: the loop of elastic_tet.rs:367-427 with
+ * Tet10::strain_stress (tet10.rs:142-169), and the von Mises and principal stresses of the
+ * means (elastic_tet.rs:482-483; elastic.rs:977-1002). Materials are isotropic, E and nu per
+ * cell as in femgpu_assemble. Stress order xx, yy, zz, xy, yz, xz (elastic.rs:967-970); strain
+ * as tensor components in the same order (elastic.rs:972-975). The sums at each point run in
+ * increasing cell order, so stress, strain, mises and the peaks are bit-identical with the
+ * reference; the principal stresses call acos and cos and agree to a few ulp. */
+typedef struct femgpu_recovery femgpu_recovery;
+
+/* The reference's `Peak` of 1 part (elastic.rs:186-195, set by elastic_tet.rs:405-416): the
+ * largest von Mises stress over the 10 points of the part's cells, first in (cell, point) order
+ * on ties, and the same over the regular points (neither the point nor a corner of its cell
+ * singular). A part with no cell keeps mises -inf and element -1; regular_element -1 is the
+ * reference's `None`. */
+typedef struct femgpu_peak {
+    double mises;
+    int64_t element;         /* the cell */
+    int32_t local;           /* which of its 10 points (tet10.rs:216-228 order) */
+    uint32_t point;          /* that point's number */
+    int32_t singular;        /* 1: the point or a corner of the cell is singular (`why`) */
+    int32_t pad;
+    double regular_mises;
+    int64_t regular_element;
+    int32_t regular_local;
+    uint32_t regular_point;
+} femgpu_peak;
+
+/* The mesh side of the loop, kept on the device: points (3 coordinates each), the 10 points of
+ * each cell (corners first, as Quadratic, tet10.rs:232-272), E and nu per cell, the thermal
+ * expansion alpha_x, alpha_y, alpha_z per cell (NULL: none; D alpha as elastic_tet.rs:164-170),
+ * the part of each cell (NULL: all in part 0; nparts >= 1, at most 2048) and the singular mask
+ * of each point (NULL: none; the reference's `singular_points`). */
+int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uint32_t* tets10,
+                        const double* coef, const double* expansion, const uint32_t* part,
+                        size_t nparts, const uint8_t* singular, femgpu_recovery** out);
+/* One recovery from the full displacement `u` (3 per point; the solution at the free unknowns
+ * and the prescribed values elsewhere, elastic_tet.rs:349-351) and the temperature change of
+ * each point (NULL: none; only corners are read). Outputs may be NULL to skip them: stress and
+ * strain 6 per point, mises 1, principal 3 (largest first), peaks nparts. Host pointers. */
+int femgpu_recovery_run(femgpu_recovery* r, const double* u, const double* dtemp, double* stress,
+                        double* strain, double* mises, double* principal, femgpu_peak* peaks);
+/* The same with u, dtemp, stress, strain, mises and principal in device memory (stress and
+ * strain required); peaks stays a host array. Returns when the results are written. */
+int femgpu_recovery_run_device(femgpu_recovery* r, const double* u, const double* dtemp,
+                               double* stress, double* strain, double* mises, double* principal,
+                               femgpu_peak* peaks);
+/* The device time of the recovery kernels of the last run in ms (CUDA events), and the
+ * algorithmic bytes they move: the cell records, the incidence and u once, the outputs once. */
+int femgpu_recovery_last_time(const femgpu_recovery* r, double* ms, double* bytes);
+size_t femgpu_recovery_bytes(const femgpu_recovery* r);
+void* femgpu_recovery_stream(const femgpu_recovery* r);
+void femgpu_recovery_free(femgpu_recovery* r);
+
 #ifdef __cplusplus
 }
 #endif

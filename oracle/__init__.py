@@ -69,6 +69,7 @@ def _load():
         "orc_solver_level_size": (S, [P, S]),
         "orc_solver_solve": (I, [P, P, P, D, S, P, P, P, P, S]),
         "orc_solver_precondition": (None, [P, P, P]),
+        "orc_recover": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -215,6 +216,40 @@ def quadratic(xyz, tets):
     t10 = np.empty((len(tets), 10), np.uint32)
     ne = _lib.orc_quadratic(_p(xyz), len(xyz), _p(tets), len(tets), _p(edges), _p(t10))
     return edges[:ne].copy(), t10
+
+
+class Peak(C.Structure):
+    """elastic_tet.rs:367-427 ``Peak`` of 1 part (the layout of ``femgpu_peak``)."""
+    _fields_ = [("mises", C.c_double), ("element", C.c_int64), ("local", C.c_int32),
+                ("point", C.c_uint32), ("singular", C.c_int32), ("pad", C.c_int32),
+                ("regular_mises", C.c_double), ("regular_element", C.c_int64),
+                ("regular_local", C.c_int32), ("regular_point", C.c_uint32)]
+
+
+def recover(xyz, tets10, coef, u, *, expansion=None, dtemp=None, part=None, nparts=1,
+            singular=None):
+    """elastic_tet.rs:367-427 and 482-483: the mean strain and stress at each point of the
+    quadratic mesh, their von Mises and principal stresses, and the peaks of each part. Returns a
+    dict of arrays: stress (n, 6), strain (n, 6), mises (n,), principal (n, 3), peaks (list)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    t10 = np.ascontiguousarray(tets10, dtype=np.uint32)
+    coef = np.ascontiguousarray(coef, dtype=np.float64)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    opt = lambda a, t: None if a is None else np.ascontiguousarray(a, dtype=t)
+    expansion, dtemp = opt(expansion, np.float64), opt(dtemp, np.float64)
+    part, singular = opt(part, np.uint32), opt(singular, np.uint8)
+    n = len(xyz)
+    stress, strain = np.empty((n, 6)), np.empty((n, 6))
+    mises, principal = np.empty(n), np.empty((n, 3))
+    peaks = (Peak * nparts)()
+    err = C.create_string_buffer(512)
+    st = _lib.orc_recover(n, _p(xyz), len(t10), _p(t10), _p(coef), _p(expansion), _p(dtemp),
+                          _p(u), _p(part), nparts, _p(singular), _p(stress), _p(strain),
+                          _p(mises), _p(principal), C.cast(peaks, C.c_void_p), err, 512)
+    if st:
+        raise OracleError(err.value.decode())
+    return {"stress": stress, "strain": strain, "mises": mises, "principal": principal,
+            "peaks": list(peaks)}
 
 
 def colour(n, elements):

@@ -363,4 +363,22 @@ void orc_solver_precondition(void* s, const double* r, double* z) {
         o->s.pmg.apply(o->s.a, r, z);
 }
 
+// elastic_tet.rs:367-427 and 482-483 (see recover_tet10). Optional arrays may be null;
+// `peaks` holds nparts entries.
+int orc_recover(size_t npoints, const double* xyz, size_t nel, const uint32_t* tets10,
+                const double* coef, const double* expansion, const double* dtemp,
+                const double* u, const uint32_t* part, size_t nparts, const uint8_t* singular,
+                double* stress, double* strain, double* mises_out, double* principal_out,
+                void* peaks, char* err, size_t len) {
+    try {
+        recover_tet10(npoints, xyz, nel, tets10, coef, expansion, dtemp, u, part, nparts,
+                      singular, stress, strain, mises_out, principal_out,
+                      static_cast<RecoveryPeak*>(peaks));
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+
 }  // extern "C"

@@ -108,6 +108,34 @@ uint32_t colour_priority(uint32_t e);
 vector<uint32_t> colour_elements(size_t n, const uint32_t* elements, size_t nel, int m,
                                  int* ncolours);
 
+// ---------------------------------------------------------------- post-solve recovery
+// elastic_tet.rs:367-427: the peak von Mises stress of a part over the 10 points of its cells,
+// and the same over the points that are not singular (the reference's `Peak`). A part with no
+// cells keeps mises -inf and element -1; regular_element -1 is the reference's `None`.
+struct RecoveryPeak {
+    double mises;
+    int64_t element;
+    int32_t local;
+    uint32_t point;
+    int32_t singular;
+    int32_t pad;
+    double regular_mises;
+    int64_t regular_element;
+    int32_t regular_local;
+    uint32_t regular_point;
+};
+// elastic_tet.rs:367-427 and 482-483 for isotropic materials (E, nu per cell as the assembly):
+// the mean strain (tensor components) and stress (xx, yy, zz, xy, yz, xz) at each point, the
+// von Mises and principal stresses of the mean, and the peaks of each part.
+void recover_tet10(size_t npoints, const double* xyz, size_t nel, const uint32_t* tets10,
+                   const double* coef, const double* expansion, const double* dtemp,
+                   const double* u, const uint32_t* part, size_t nparts, const uint8_t* singular,
+                   double* stress, double* strain, double* mises_out, double* principal_out,
+                   RecoveryPeak* peaks);
+// elastic.rs:977-1002
+double mises(const double s[6]);
+void principal(const double s[6], double out[3]);
+
 // ---------------------------------------------------------------- order / symbolic / cholesky
 // order.rs:19-179
 vector<size_t> nested_dissection(const Csr& a, const vector<Vec3>& xyz);

@@ -62,3 +62,23 @@ def test_reference_constants():
 def test_invalid_arguments_fail_before_the_device():
     with np.testing.assert_raises(fg.FemError):
         fg.prolongation(np.zeros((4, 3)), 4, np.zeros((0, 2), np.uint32), np.array([50]))
+
+
+def test_recovery_arguments_fail_before_the_device():
+    """femgpu_recovery_new checks its sizes on the host: no part, more than 2048 parts, an
+    empty mesh, a null array."""
+    from femahoy_b200.recover import Recovery
+    xyz = np.zeros((10, 3))
+    t10 = np.arange(10, dtype=np.uint32)[None, :]
+    coef = np.array([[1.0, 0.3]])
+    for kw, what in [(dict(nparts=0), "no part"), (dict(nparts=4096), "2048 parts")]:
+        with np.testing.assert_raises(fg.FemError) as e:
+            Recovery(xyz, t10, coef, **kw)
+        assert what in str(e.exception)
+    with np.testing.assert_raises(fg.FemError) as e:
+        Recovery(np.zeros((0, 3)), t10[:0], coef[:0])
+    assert "empty mesh" in str(e.exception)
+    h = ctypes.c_void_p()
+    st = fg.lib().femgpu_recovery_new(10, None, 1, None, None, None, None, 1, None,
+                                      ctypes.byref(h))
+    assert st == _lib.INVALID
