@@ -3,23 +3,32 @@
 // each point, the peak von Mises stress of each part) and the von Mises and principal stresses of
 // the means (elastic_tet.rs:482-483).
 //
-// Layout in HBM. Setup writes one 224-byte record per cell: the gradients of its 4 volume
-// coordinates (tet_gradients, heat.rs:983-1002), its stiffness D (hex.rs:58-114) and D alpha
-// (elastic_tet.rs:164-170). The incidence of the assembly lists the cells of each point in
-// increasing order. A recovery is one thread per point: it walks its cells in that order,
-// evaluates Tet10::strain_stress (tet10.rs:142-169) at its own volume coordinates in each, and
-// sums. The reference adds the same terms to the same point in the same order, so the means
-// are bit-identical with it. Each (cell, point) pair is evaluated exactly once, by the thread of
-// its point. The unit is compiled with -fmad=false, so no multiply and add are fused.
+// Layout in HBM, written once at setup: per cell a 128-byte record (the gradients of its 4
+// volume coordinates, tet_gradients of heat.rs:983-1002, and its material number); per distinct
+// material (E, nu, alpha) a 128-byte entry (D of hex.rs:58-114 and D alpha of
+// elastic_tet.rs:164-170); the incidence of the assembly (the cells of each point in increasing
+// order) and, beside it, the place (0-9) of the point in each of those cells. A recovery first
+// copies u into 32 bytes per point, so that each point's displacement is 1 aligned 32-byte load.
 //
-// Peaks: the thread that evaluates pair (cell e, point c) writes its von Mises stress to
-// vm[10 e + c]. Each block reduces a contiguous range of pairs per part in shared memory, then
-// 1 thread per part combines the blocks: the largest value, and among equal values the smallest
-// index, which is the first in the reference's (cell, point) order. Maximum and minimum are
-// exact, so no order of the reduction changes the result.
+// One thread per point walks its cells in increasing order, evaluates Tet10::strain_stress
+// (tet10.rs:142-169) at its own volume coordinates in each, and sums. The reference adds the same
+// terms to the same point in the same order, so the means are bit-identical with it. Each
+// (cell, point) pair, a "visit", is evaluated exactly once, by the thread of its point. The unit
+// is compiled with -fmad=false, so no multiply and add are fused.
+//
+// Peaks: the thread of each visit folds its von Mises stress into 3 running maxima of its part,
+// each a 128-bit word updated by compare-and-swap: (value, ~key) for the peak and for the
+// regular peak, where key = 10 cell + place orders the visits as the reference's loop, and
+// (~key, value) for the first regular visit. The maximum of such words is the largest value and,
+// among equal values, the smallest key: the reference's first strict maximum. Maxima are exact,
+// so no order of the updates changes the result. With few parts the maxima live in shared memory
+// per block and are folded into global memory at the end of the block.
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <vector>
 
 #include "assemble.cuh"
 #include "common.cuh"
@@ -27,29 +36,46 @@
 
 namespace femgpu {
 
-// One cell's constants: 27 values and a pad, 224 bytes (7 sectors of 32 bytes).
-struct CellRecord {
-    double g[4][3];
-    double normal[3][3];
+// One cell: the gradients of its 4 volume coordinates, its material, and its part with the
+// `near` flag in the top bit (128 bytes, 4 aligned 32-byte loads).
+struct alignas(32) CellRecord {
+    double g[12];
+    uint32_t mat;
+    uint32_t tag;
+    double pad[3];
+};
+static_assert(sizeof(CellRecord) == 128, "the cell record is 128 bytes");
+
+// One material: D (normal 3 x 3 row-major, then G_yz, G_xz, G_xy) and D alpha (128 bytes).
+struct alignas(32) MaterialEntry {
+    double normal[9];
     double shear[3];
     double thermal[3];
     double pad;
 };
-static_assert(sizeof(CellRecord) == 224, "the cell record is 224 bytes");
+static_assert(sizeof(MaterialEntry) == 128, "the material entry is 128 bytes");
 
 constexpr int MAX_PARTS = 2048;
-constexpr int PEAK_THREADS = 256;
-constexpr int PEAK_BLOCKS = 2 * NUM_SMS;
+constexpr int SMEM_PARTS = 64;  // parts whose maxima a block keeps in shared memory
 constexpr uint64_t NONE = ~0ull;
 constexpr uint32_t NEAR_BIT = 0x80000000u;
-
-struct PeakPartial {
-    uint64_t max_all, key_all, max_reg, key_reg, first_reg;
-};
+typedef unsigned __int128 u128;
 
 // tet10.rs:38, packed 4 bits per edge: the first and the second corner of edge k.
 constexpr uint32_t EDGE_FIRST = 0x210010u;   // 0, 1, 0, 0, 1, 2
 constexpr uint32_t EDGE_SECOND = 0x333221u;  // 1, 2, 2, 3, 3, 3
+
+__device__ __forceinline__ int edge_corner(int k, int which) {
+    return (int)(((which ? EDGE_SECOND : EDGE_FIRST) >> (4 * k)) & 0xfu);
+}
+
+// A 32-byte load through the read-only path; p is 32-byte aligned and not written by the kernel.
+__device__ __forceinline__ void ld32(const double* p, double& a, double& b, double& c,
+                                     double& d) {
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+        : "=d"(a), "=d"(b), "=d"(c), "=d"(d)
+        : "l"(p));
+}
 
 __device__ __forceinline__ bool is_nan_bits(uint64_t b) {
     return (b & 0x7fffffffffffffffull) > 0x7ff0000000000000ull;
@@ -87,15 +113,39 @@ __device__ __forceinline__ void principal3(const double s[6], double out[3]) {
     out[2] = s3;
 }
 
-// Setup: the record, and the part and the `near` flag of each cell (a corner is singular:
-// elastic_tet.rs:395). Flags: 2 no stable material, 3 a part past the last.
+// Setup: D and D alpha of each distinct material (E, nu, alpha_x, alpha_y, alpha_z). Flag 2: no
+// stable material (hex.rs:72-98).
+__global__ void k_recover_materials(const double* __restrict__ in, int64_t nmat,
+                                    MaterialEntry* __restrict__ out, int* __restrict__ bad) {
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < nmat;
+         m += (int64_t)gridDim.x * blockDim.x) {
+        const double* v = in + 5 * m;
+        Stiffness D;
+        if (!isotropic_stiffness(v[0], v[1], &D)) atomicExch(bad, 2);
+        MaterialEntry r;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            double s = -0.0;  // the Rust float sum starts from -0.0
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                r.normal[3 * i + j] = D.normal[i][j];
+                s += D.normal[i][j] * v[2 + j];
+            }
+            r.thermal[i] = s;
+            r.shear[i] = D.shear[i];
+        }
+        r.pad = 0.0;
+        out[m] = r;
+    }
+}
+
+// Setup: the record of each cell, with its part and `near` flag (a corner is singular:
+// elastic_tet.rs:395). Flag 3: a part past the last.
 __global__ void k_recover_cells(const double* __restrict__ xyz, const uint32_t* __restrict__ t10,
-                                const double* __restrict__ coef,
-                                const double* __restrict__ expansion,
+                                const uint32_t* __restrict__ mat,
                                 const uint32_t* __restrict__ part, uint32_t nparts,
                                 const uint8_t* __restrict__ singular, int64_t nel,
-                                CellRecord* __restrict__ rec, uint32_t* __restrict__ tag,
-                                int* __restrict__ bad) {
+                                CellRecord* __restrict__ rec, int* __restrict__ bad) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
          e += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t* t = t10 + 10 * e;
@@ -104,62 +154,82 @@ __global__ void k_recover_cells(const double* __restrict__ xyz, const uint32_t* 
         for (int k = 0; k < 4; ++k)
 #pragma unroll
             for (int d = 0; d < 3; ++d) p[k][d] = xyz[3 * (int64_t)t[k] + d];
+        double g[4][3], volume;
+        tet_gradients(p, g, &volume);
         CellRecord r;
-        double volume;
-        tet_gradients(p, r.g, &volume);
-        Stiffness D;
-        if (!isotropic_stiffness(coef[2 * e], coef[2 * e + 1], &D)) atomicExch(bad, 2);
-        double alpha[3] = {0.0, 0.0, 0.0};
-        if (expansion)
 #pragma unroll
-            for (int k = 0; k < 3; ++k) alpha[k] = expansion[3 * e + k];
+        for (int k = 0; k < 4; ++k)
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            double s = -0.0;  // the Rust float sum starts from -0.0
-#pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                r.normal[i][j] = D.normal[i][j];
-                s += D.normal[i][j] * alpha[j];
-            }
-            r.thermal[i] = s;
-            r.shear[i] = D.shear[i];
-        }
-        r.pad = 0.0;
-        rec[e] = r;
+            for (int d = 0; d < 3; ++d) r.g[3 * k + d] = g[k][d];
         uint32_t pt = part ? part[e] : 0u;
         if (pt >= nparts) atomicExch(bad, 3);
         bool near = false;
         if (singular)
 #pragma unroll
             for (int k = 0; k < 4; ++k) near = near || singular[t[k]] != 0;
-        tag[e] = (pt & ~NEAR_BIT) | (near ? NEAR_BIT : 0u);
+        r.mat = mat[e];
+        r.tag = (pt & ~NEAR_BIT) | (near ? NEAR_BIT : 0u);
+        r.pad[0] = r.pad[1] = r.pad[2] = 0.0;
+        rec[e] = r;
     }
 }
 
-// Tet10::strain_stress (tet10.rs:142-169) of cell `r` at its point c, followed by reorder and
-// tensor_strain (elastic.rs:967-975): sig and eps in the order xx, yy, zz, xy, yz, xz.
-__device__ __forceinline__ void strain_stress_at(const CellRecord* __restrict__ rp,
-                                                 const uint32_t* __restrict__ t, int c,
-                                                 const double* __restrict__ u,
-                                                 const double* __restrict__ dtemp,
-                                                 double sig[6], double eps[6]) {
-    const double2* r2 = reinterpret_cast<const double2*>(rp);
-    double w[28];
-#pragma unroll
-    for (int k = 0; k < 14; ++k) {
-        double2 v = __ldg(r2 + k);
-        w[2 * k] = v.x;
-        w[2 * k + 1] = v.y;
+// Setup: the place of point v in each of its cells. A cell that names the point twice is listed
+// twice and takes its places in order, as the reference's loop over the 10 points.
+__global__ void k_visit_places(const uint32_t* __restrict__ t10, const int64_t* __restrict__ start,
+                               const uint32_t* __restrict__ of_node, int64_t npoints,
+                               uint8_t* __restrict__ place) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < npoints;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t last = 0xffffffffu;
+        int lastc = -1;
+        for (int64_t k = start[v]; k < start[v + 1]; ++k) {
+            const uint32_t e = of_node[k];
+            const uint32_t* t = t10 + 10 * (int64_t)e;
+            int c = e == last ? lastc + 1 : 0;
+            while (c < 10 && t[c] != (uint32_t)v) ++c;
+            // c < 10: the incidence was built from these cells.
+            place[k] = (uint8_t)c;
+            last = e;
+            lastc = c;
+        }
     }
-    // w[0..12) g, w[12..21) normal, w[21..24) shear, w[24..27) thermal.
-    double l[4] = {0.0, 0.0, 0.0, 0.0};  // node_coordinates (tet10.rs:216-228)
+}
+
+// u (3 per point) into 4 per point, the 4th 0.
+__global__ void k_pad_u(const double* __restrict__ u, int64_t npoints, double* __restrict__ u4) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < npoints;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        const double a = u[3 * v], b = u[3 * v + 1], c = u[3 * v + 2];
+        double2* o = reinterpret_cast<double2*>(u4 + 4 * v);
+        o[0] = make_double2(a, b);
+        o[1] = make_double2(c, 0.0);
+    }
+}
+
+// Tet10::strain_stress (tet10.rs:142-169) of cell e (record rp, points t) at its point c,
+// followed by reorder and tensor_strain (elastic.rs:967-975): sig and eps in the order xx, yy,
+// zz, xy, yz, xz.
+__device__ __forceinline__ void strain_stress_at(const CellRecord* __restrict__ rp,
+                                                 const MaterialEntry* __restrict__ mats,
+                                                 const uint32_t t[10], int c,
+                                                 const double* __restrict__ u4,
+                                                 const double* __restrict__ dtemp,
+                                                 double sig[6], double eps[6], uint32_t* tag) {
+    const double* rd = reinterpret_cast<const double*>(rp);
+    double g[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ld32(rd + 4 * k, g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+    const uint2 mt = __ldg(reinterpret_cast<const uint2*>(rd + 12));
+    const uint32_t mat = mt.x;
+    *tag = mt.y;
+    // node_coordinates (tet10.rs:216-228)
+    double l[4];
     if (c < 4) {
-        l[0] = c == 0 ? 1.0 : 0.0;
-        l[1] = c == 1 ? 1.0 : 0.0;
-        l[2] = c == 2 ? 1.0 : 0.0;
-        l[3] = c == 3 ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) l[k] = k == c ? 1.0 : 0.0;
     } else {
-        int i = (EDGE_FIRST >> (4 * (c - 4))) & 0xf, j = (EDGE_SECOND >> (4 * (c - 4))) & 0xf;
+        const int i = edge_corner(c - 4, 0), j = edge_corner(c - 4, 1);
 #pragma unroll
         for (int k = 0; k < 4; ++k) l[k] = (k == i || k == j) ? 0.5 : 0.0;
     }
@@ -169,34 +239,39 @@ __device__ __forceinline__ void strain_stress_at(const CellRecord* __restrict__ 
         // The gradient of function i at l (tet10.rs:77-87).
         double gi[3];
         if (i < 4) {
+            const double f = 4.0 * l[i] - 1.0;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) gi[d] = (4.0 * l[i] - 1.0) * w[3 * i + d];
+            for (int d = 0; d < 3; ++d) gi[d] = f * g[3 * i + d];
         } else {
-            const int a = kEdges[i - 4][0], b = kEdges[i - 4][1];
+            const int a = edge_corner(i - 4, 0), b = edge_corner(i - 4, 1);
 #pragma unroll
-            for (int d = 0; d < 3; ++d) gi[d] = 4.0 * (l[a] * w[3 * b + d] + l[b] * w[3 * a + d]);
+            for (int d = 0; d < 3; ++d) gi[d] = 4.0 * (l[a] * g[3 * b + d] + l[b] * g[3 * a + d]);
         }
-        const int64_t base = 3 * (int64_t)t[i];
-        double ui[3] = {u[base], u[base + 1], u[base + 2]};
+        double ui[3], unused;
+        ld32(u4 + 4 * (int64_t)t[i], ui[0], ui[1], ui[2], unused);
 #pragma unroll
         for (int a = 0; a < 3; ++a) e[a] += gi[a] * ui[a];
-#pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            const int a = kShear[s][0], b = kShear[s][1];
-            e[3 + s] += gi[a] * ui[b] + gi[b] * ui[a];
-        }
+        // SHEAR (tet10.rs:41): yz, xz, xy
+        e[3] += gi[1] * ui[2] + gi[2] * ui[1];
+        e[4] += gi[0] * ui[2] + gi[2] * ui[0];
+        e[5] += gi[0] * ui[1] + gi[1] * ui[0];
     }
     double dt = -0.0;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) dt += l[k] * (dtemp ? dtemp[t[k]] : 0.0);
+    for (int k = 0; k < 4; ++k) dt += l[k] * (dtemp ? __ldg(dtemp + t[k]) : 0.0);
+    const double* md = reinterpret_cast<const double*>(mats + mat);
+    double w[16];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ld32(md + 4 * k, w[4 * k], w[4 * k + 1], w[4 * k + 2], w[4 * k + 3]);
+    // w[0..9) normal, w[9..12) shear, w[12..15) thermal.
     double s[6];
 #pragma unroll
     for (int a = 0; a < 3; ++a)  // hex.rs:128-139
-        s[a] = w[12 + 3 * a] * e[0] + w[12 + 3 * a + 1] * e[1] + w[12 + 3 * a + 2] * e[2];
+        s[a] = w[3 * a] * e[0] + w[3 * a + 1] * e[1] + w[3 * a + 2] * e[2];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) s[3 + k] = w[21 + k] * e[3 + k];
+    for (int k = 0; k < 3; ++k) s[3 + k] = w[9 + k] * e[3 + k];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) s[a] -= w[24 + a] * dt;
+    for (int a = 0; a < 3; ++a) s[a] -= w[12 + a] * dt;
     sig[0] = s[0];
     sig[1] = s[1];
     sig[2] = s[2];
@@ -211,41 +286,80 @@ __device__ __forceinline__ void strain_stress_at(const CellRecord* __restrict__ 
     eps[5] = 0.5 * e[4];
 }
 
+// max(*a, v) by compare-and-swap. The high half of *a never decreases, so a v whose high half
+// is below it is below *a and needs no atomic.
+__device__ __forceinline__ void fold_max(u128* a, u128 v) {
+    const unsigned long long vh = (unsigned long long)(v >> 64);
+    const unsigned long long ch =
+        *(reinterpret_cast<volatile unsigned long long*>(a) + 1);  // little-endian: high half
+    if (vh < ch) return;
+    u128 old = atomicCAS(a, (u128)0, (u128)0);  // an atomic read (0 stays 0)
+    while (v > old) {
+        const u128 prev = atomicCAS(a, old, v);
+        if (prev == old) break;
+        old = prev;  // another thread raised it: compare again
+    }
+}
+
 // One thread per point: the sums of elastic_tet.rs:396-403 over the point's cells in
-// increasing order, the means of elastic_tet.rs:419-425, and elastic_tet.rs:482-483.
-template <bool PEAKS>
-__global__ void __launch_bounds__(128)
-    k_recover_points(const CellRecord* __restrict__ rec, const uint32_t* __restrict__ t10,
-                     const int64_t* __restrict__ start, const uint32_t* __restrict__ of_node,
-                     const double* __restrict__ u, const double* __restrict__ dtemp,
-                     int64_t npoints, double* __restrict__ stress, double* __restrict__ strain,
+// increasing order, the means of elastic_tet.rs:419-425, and elastic_tet.rs:482-483. With
+// PEAKS, the peaks of elastic_tet.rs:405-416 into `peak` (3 words per part: peak, regular peak,
+// first regular visit), through shared memory when SMEM.
+template <bool PEAKS, bool SMEM>
+__global__ void __launch_bounds__(128, 4)
+    k_recover_points(const CellRecord* __restrict__ rec, const MaterialEntry* __restrict__ mats,
+                     const uint32_t* __restrict__ t10, const int64_t* __restrict__ start,
+                     const uint32_t* __restrict__ of_node, const uint8_t* __restrict__ place,
+                     const double* __restrict__ u4, const double* __restrict__ dtemp,
+                     const uint8_t* __restrict__ singular, int64_t npoints, int nparts,
+                     double* __restrict__ stress, double* __restrict__ strain,
                      double* __restrict__ mises_out, double* __restrict__ principal_out,
-                     double* __restrict__ vm) {
+                     u128* __restrict__ peak) {
+    extern __shared__ u128 peak_s[];
+    u128* fold = SMEM ? peak_s : peak;
+    if (PEAKS && SMEM) {
+        for (int i = threadIdx.x; i < 3 * nparts; i += blockDim.x) peak_s[i] = 0;
+        __syncthreads();
+    }
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < npoints;
          v += (int64_t)gridDim.x * blockDim.x) {
         double ss[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         double se[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         const int64_t b = start[v], end = start[v + 1];
-        uint32_t last = 0xffffffffu;
-        int lastc = -1;
+        const bool sing_v = PEAKS && singular && singular[v];
         for (int64_t k = b; k < end; ++k) {
-            const uint32_t e = of_node[k];
-            const uint32_t* t = t10 + 10 * (int64_t)e;
-            // The point's place in the cell; a cell that names the point twice is listed twice
-            // and takes its places in order, as the reference's loop over c.
-            int c = e == last ? lastc + 1 : 0;
-            while (c < 10 && t[c] != (uint32_t)v) ++c;
-            if (c >= 10) continue;  // not reached: the incidence lists exactly these places
-            last = e;
-            lastc = c;
+            const uint32_t e = __ldg(of_node + k);
+            const int c = __ldg(place + k);
+            const uint2* row = reinterpret_cast<const uint2*>(t10 + 10 * (int64_t)e);
+            uint32_t t[10];
+#pragma unroll
+            for (int q = 0; q < 5; ++q) {
+                const uint2 w = __ldg(row + q);
+                t[2 * q] = w.x;
+                t[2 * q + 1] = w.y;
+            }
             double sig[6], eps[6];
-            strain_stress_at(rec + e, t, c, u, dtemp, sig, eps);
+            uint32_t tg;
+            strain_stress_at(rec + e, mats, t, c, u4, dtemp, sig, eps, &tg);
 #pragma unroll
             for (int i = 0; i < 6; ++i) {
                 ss[i] += sig[i];
                 se[i] += eps[i];
             }
-            if (PEAKS) vm[10 * (int64_t)e + c] = mises6(sig);
+            if (PEAKS) {
+                const unsigned long long bits =
+                    (unsigned long long)__double_as_longlong(mises6(sig));
+                const unsigned long long key = 10ull * e + c;
+                const int p = (int)(tg & ~NEAR_BIT);
+                const bool reg = !(tg & NEAR_BIT) && !sing_v;
+                const bool nan = is_nan_bits(bits);
+                const u128 vk = ((u128)bits << 64) | (u128)(NONE - key);
+                if (!nan) fold_max(fold + 3 * p, vk);
+                if (reg) {
+                    if (!nan) fold_max(fold + 3 * p + 1, vk);
+                    fold_max(fold + 3 * p + 2, ((u128)(NONE - key) << 64) | (u128)bits);
+                }
+            }
         }
         int64_t count = end - b;
         const double cnt = (double)(count > 1 ? count : 1);
@@ -264,103 +378,46 @@ __global__ void __launch_bounds__(128)
             for (int i = 0; i < 3; ++i) principal_out[3 * v + i] = pr[i];
         }
     }
-}
-
-// Each block: the pairs [10 e0, 10 e1) of its range of cells, per part in shared memory
-// (5 x nparts words). Pass A takes the maxima and the first regular pair; pass B the smallest
-// pair index at each maximum.
-__global__ void __launch_bounds__(PEAK_THREADS)
-    k_peak_blocks(const double* __restrict__ vm, const uint32_t* __restrict__ tag,
-                  const uint32_t* __restrict__ t10, const uint8_t* __restrict__ singular,
-                  int64_t nel, int nparts, int64_t chunk, PeakPartial* __restrict__ partial) {
-    extern __shared__ unsigned long long sm[];
-    unsigned long long* mall = sm;
-    unsigned long long* kall = sm + nparts;
-    unsigned long long* mreg = sm + 2 * nparts;
-    unsigned long long* kreg = sm + 3 * nparts;
-    unsigned long long* freg = sm + 4 * nparts;
-    for (int p = threadIdx.x; p < nparts; p += blockDim.x) {
-        mall[p] = 0;
-        mreg[p] = 0;
-        kall[p] = NONE;
-        kreg[p] = NONE;
-        freg[p] = NONE;
-    }
-    __syncthreads();
-    const int64_t e0 = blockIdx.x * chunk;
-    const int64_t e1 = e0 + chunk < nel ? e0 + chunk : nel;
-    for (int pass = 0; pass < 2; ++pass) {
-        for (int64_t i = 10 * e0 + threadIdx.x; i < 10 * e1; i += blockDim.x) {
-            const uint32_t tg = tag[i / 10];
-            const int p = (int)(tg & ~NEAR_BIT);
-            const bool reg = !(tg & NEAR_BIT) && !(singular && singular[t10[i]]);
-            const unsigned long long bits = (unsigned long long)__double_as_longlong(vm[i]);
-            const bool nan = is_nan_bits(bits);
-            if (pass == 0) {
-                if (!nan) atomicMax(&mall[p], bits);
-                if (reg) {
-                    if (!nan) atomicMax(&mreg[p], bits);
-                    atomicMin(&freg[p], (unsigned long long)i);
-                }
-            } else if (!nan) {
-                if (bits == mall[p]) atomicMin(&kall[p], (unsigned long long)i);
-                if (reg && bits == mreg[p]) atomicMin(&kreg[p], (unsigned long long)i);
-            }
-        }
+    if (PEAKS && SMEM) {
         __syncthreads();
-    }
-    for (int p = threadIdx.x; p < nparts; p += blockDim.x)
-        partial[(int64_t)blockIdx.x * nparts + p] =
-            PeakPartial{mall[p], kall[p], mreg[p], kreg[p], freg[p]};
-}
-
-__device__ __forceinline__ void combine(uint64_t m, uint64_t k, uint64_t* bm, uint64_t* bk) {
-    if (k == NONE) return;
-    if (*bk == NONE || m > *bm || (m == *bm && k < *bk)) {
-        *bm = m;
-        *bk = k;
+        for (int i = threadIdx.x; i < 3 * nparts; i += blockDim.x)
+            if (peak_s[i] != 0) fold_max(peak + i, peak_s[i]);
     }
 }
 
-// 1 thread per part: the blocks combined, and the reference's Peak (elastic_tet.rs:405-416):
-// the first regular pair stays the regular peak when its value is NaN, since no value is
-// greater than NaN.
-__global__ void k_peak_final(const PeakPartial* __restrict__ partial, int nblocks, int nparts,
-                             const double* __restrict__ vm, const uint32_t* __restrict__ t10,
-                             const uint32_t* __restrict__ tag,
+// 1 thread per part: the reference's Peak (elastic_tet.rs:405-416) from the 3 maxima. The first
+// regular visit stays the regular peak when its value is NaN, since no value is greater than NaN.
+__global__ void k_peak_final(const u128* __restrict__ peak, int nparts,
+                             const uint32_t* __restrict__ t10, const CellRecord* __restrict__ rec,
                              const uint8_t* __restrict__ singular, femgpu_peak* __restrict__ out) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nparts) return;
-    uint64_t mall = 0, kall = NONE, mreg = 0, kreg = NONE, freg = NONE;
-    for (int b = 0; b < nblocks; ++b) {
-        const PeakPartial q = partial[(int64_t)b * nparts + p];
-        combine(q.max_all, q.key_all, &mall, &kall);
-        combine(q.max_reg, q.key_reg, &mreg, &kreg);
-        if (q.first_reg < freg) freg = q.first_reg;
-    }
+    const u128 all = peak[3 * p], reg = peak[3 * p + 1], first = peak[3 * p + 2];
     femgpu_peak o;
     memset(&o, 0, sizeof(o));
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
-    if (kall == NONE) {
+    if (all == 0) {
         o.mises = -inf;
         o.element = -1;
     } else {
-        o.mises = __longlong_as_double((long long)mall);
-        o.element = (int64_t)(kall / 10);
-        o.local = (int32_t)(kall % 10);
-        o.point = t10[kall];
-        o.singular = ((tag[kall / 10] & NEAR_BIT) || (singular && singular[o.point])) ? 1 : 0;
+        const uint64_t key = NONE - (uint64_t)all;
+        o.mises = __longlong_as_double((long long)(uint64_t)(all >> 64));
+        o.element = (int64_t)(key / 10);
+        o.local = (int32_t)(key % 10);
+        o.point = t10[key];
+        o.singular =
+            ((rec[key / 10].tag & NEAR_BIT) || (singular && singular[o.point])) ? 1 : 0;
     }
     uint64_t rk = NONE;
     double rm = -inf;
-    if (freg != NONE) {
-        const uint64_t fb = (uint64_t)__double_as_longlong(vm[freg]);
-        if (is_nan_bits(fb)) {
-            rk = freg;
-            rm = vm[freg];
+    if (first != 0) {
+        const uint64_t fbits = (uint64_t)first;
+        if (is_nan_bits(fbits)) {
+            rk = NONE - (uint64_t)(first >> 64);
+            rm = __longlong_as_double((long long)fbits);
         } else {
-            rk = kreg;
-            rm = __longlong_as_double((long long)mreg);
+            rk = NONE - (uint64_t)reg;
+            rm = __longlong_as_double((long long)(uint64_t)(reg >> 64));
         }
     }
     if (rk == NONE) {
@@ -380,19 +437,18 @@ __global__ void k_peak_final(const PeakPartial* __restrict__ partial, int nblock
 using namespace femgpu;
 
 struct femgpu_recovery {
-    int64_t npoints = 0, nel = 0;
+    int64_t npoints = 0, nel = 0, nmat = 0;
     int nparts = 1;
     bool has_singular = false;
     Incidence inc;
+    DevBuf<uint8_t> place;
     DevBuf<uint32_t> t10;
     DevBuf<CellRecord> rec;
-    DevBuf<uint32_t> tag;
+    DevBuf<MaterialEntry> mats;
     DevBuf<uint8_t> singular;
-    DevBuf<double> vm;
-    DevBuf<PeakPartial> partial;
+    DevBuf<double> u4;
+    DevBuf<u128> peak;
     DevBuf<femgpu_peak> dpeaks;
-    int peak_blocks = 1;
-    int64_t chunk = 1;
     // Device copies for the host-pointer form.
     DevBuf<double> du, ddt, dstress, dstrain, dmises, dprincipal;
     cudaStream_t s = nullptr;
@@ -407,28 +463,30 @@ struct femgpu_recovery {
     void run(const double* u, const double* dtemp, double* stress, double* strain,
              double* mises, double* principal, femgpu_peak* peaks) {
         const bool want_peaks = peaks != nullptr;
-        if (want_peaks && vm.count < (size_t)(10 * nel)) vm.alloc(10 * nel);
+        const uint8_t* sing = has_singular ? singular.p : nullptr;
         FG_CUDA(cudaEventRecord(ev0, s));
+        k_pad_u<<<blocks_for(npoints, 256), 256, 0, s>>>(u, npoints, u4.p);
+        FG_CHECK_LAUNCH();
         const int grid = blocks_for(npoints, 128, NUM_SMS * 64);
-        if (want_peaks)
-            k_recover_points<true><<<grid, 128, 0, s>>>(rec.p, t10.p, inc.start.p, inc.of_node.p,
-                                                        u, dtemp, npoints, stress, strain, mises,
-                                                        principal, vm.p);
-        else
-            k_recover_points<false><<<grid, 128, 0, s>>>(rec.p, t10.p, inc.start.p,
-                                                         inc.of_node.p, u, dtemp, npoints,
-                                                         stress, strain, mises, principal,
-                                                         nullptr);
+        if (!want_peaks) {
+            k_recover_points<false, false><<<grid, 128, 0, s>>>(
+                rec.p, mats.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p, dtemp, sing,
+                npoints, nparts, stress, strain, mises, principal, nullptr);
+        } else {
+            peak.zero(s);
+            if (nparts <= SMEM_PARTS)
+                k_recover_points<true, true><<<grid, 128, 3 * sizeof(u128) * nparts, s>>>(
+                    rec.p, mats.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p, dtemp, sing,
+                    npoints, nparts, stress, strain, mises, principal, peak.p);
+            else
+                k_recover_points<true, false><<<grid, 128, 0, s>>>(
+                    rec.p, mats.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p, dtemp, sing,
+                    npoints, nparts, stress, strain, mises, principal, peak.p);
+        }
         FG_CHECK_LAUNCH();
         if (want_peaks) {
-            const size_t smem = 5 * sizeof(unsigned long long) * (size_t)nparts;
-            k_peak_blocks<<<peak_blocks, PEAK_THREADS, smem, s>>>(
-                vm.p, tag.p, t10.p, has_singular ? singular.p : nullptr, nel, nparts, chunk,
-                partial.p);
-            FG_CHECK_LAUNCH();
-            k_peak_final<<<(nparts + 127) / 128, 128, 0, s>>>(
-                partial.p, peak_blocks, nparts, vm.p, t10.p, tag.p,
-                has_singular ? singular.p : nullptr, dpeaks.p);
+            k_peak_final<<<(nparts + 127) / 128, 128, 0, s>>>(peak.p, nparts, t10.p, rec.p, sing,
+                                                               dpeaks.p);
             FG_CHECK_LAUNCH();
         }
         FG_CUDA(cudaEventRecord(ev1, s));
@@ -437,14 +495,13 @@ struct femgpu_recovery {
         float ms = 0.f;
         FG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
         last_ms = ms;
-        // The cell records, the cells' point numbers, the incidence and u once; the outputs once;
-        // for the peaks the pair values written and read once and the cell tags.
-        double bytes = nel * (sizeof(CellRecord) + 10.0 * 4) + (npoints + 1) * 8.0 +
-                       10.0 * nel * 4 + npoints * 24.0 + (dtemp ? npoints * 8.0 : 0.0) +
-                       npoints * 96.0 + (mises ? npoints * 8.0 : 0.0) +
-                       (principal ? npoints * 24.0 : 0.0);
-        if (want_peaks) bytes += nel * (80.0 + 80.0 + 4.0) + (has_singular ? nel * 10.0 : 0.0);
-        last_bytes = bytes;
+        // Each array once: u read, written padded and read padded; the cell records and point
+        // numbers; the incidence with its places; the outputs.
+        last_bytes = npoints * (24.0 + 32.0 + 32.0) + nel * (sizeof(CellRecord) + 40.0) +
+                     nmat * (double)sizeof(MaterialEntry) + (npoints + 1) * 8.0 +
+                     10.0 * nel * 5.0 + (dtemp ? npoints * 8.0 : 0.0) + npoints * 96.0 +
+                     (mises ? npoints * 8.0 : 0.0) + (principal ? npoints * 24.0 : 0.0) +
+                     (want_peaks && has_singular ? npoints * 1.0 : 0.0);
     }
 };
 
@@ -495,24 +552,46 @@ int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uin
         r->nparts = (int)nparts;
         r->t10.upload(tets10, 10 * nel, s);
         build_incidence(r->t10.p, r->nel, 10, r->npoints, &r->inc, s);
-        DevBuf<double> dxyz, dcoef, dexp;
-        DevBuf<uint32_t> dpart;
+        r->place.alloc(10 * nel);
+        k_visit_places<<<blocks_for(r->npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
+            r->t10.p, r->inc.start.p, r->inc.of_node.p, r->npoints, r->place.p);
+        FG_CHECK_LAUNCH();
+        // The distinct materials (E, nu, alpha) by their bits, numbered in order of first sight.
+        std::map<std::array<uint64_t, 5>, uint32_t> seen;
+        std::vector<uint32_t> mat(nel);
+        std::vector<double> table;
+        for (size_t e = 0; e < nel; ++e) {
+            double v[5] = {coef[2 * e], coef[2 * e + 1], 0.0, 0.0, 0.0};
+            if (expansion)
+                for (int k = 0; k < 3; ++k) v[2 + k] = expansion[3 * e + k];
+            std::array<uint64_t, 5> key;
+            std::memcpy(key.data(), v, sizeof(v));
+            auto it = seen.emplace(key, (uint32_t)seen.size());
+            if (it.second) table.insert(table.end(), v, v + 5);
+            mat[e] = it.first->second;
+        }
+        r->nmat = (int64_t)seen.size();
+        DevBuf<double> dxyz, dtable;
+        DevBuf<uint32_t> dpart, dmat;
         dxyz.upload(xyz, 3 * npoints, s);
-        dcoef.upload(coef, 2 * nel, s);
-        if (expansion) dexp.upload(expansion, 3 * nel, s);
+        dtable.upload(table.data(), table.size(), s);
+        dmat.upload(mat.data(), nel, s);
         if (part) dpart.upload(part, nel, s);
         if (singular) {
             r->singular.upload(singular, npoints, s);
             r->has_singular = true;
         }
+        r->mats.alloc(r->nmat);
         r->rec.alloc(nel);
-        r->tag.alloc(nel);
+        r->u4.alloc(4 * npoints);
         DevBuf<int> bad(1);
         bad.zero(s);
+        k_recover_materials<<<blocks_for(r->nmat, 128), 128, 0, s>>>(dtable.p, r->nmat, r->mats.p,
+                                                                     bad.p);
+        FG_CHECK_LAUNCH();
         k_recover_cells<<<blocks_for(r->nel, 128, NUM_SMS * 32), 128, 0, s>>>(
-            dxyz.p, r->t10.p, dcoef.p, expansion ? dexp.p : nullptr, part ? dpart.p : nullptr,
-            (uint32_t)nparts, singular ? r->singular.p : nullptr, r->nel, r->rec.p, r->tag.p,
-            bad.p);
+            dxyz.p, r->t10.p, dmat.p, part ? dpart.p : nullptr, (uint32_t)nparts,
+            singular ? r->singular.p : nullptr, r->nel, r->rec.p, bad.p);
         FG_CHECK_LAUNCH();
         int b = fetch(bad.p, s);
         if (b == 2)
@@ -520,14 +599,8 @@ int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uin
                           "the Poisson ratios give no stable material (for an isotropic material, "
                           "nu must be between -1 and 0.5)");
         if (b == 3) throw Failure(FEMGPU_ERR_INVALID, "a cell names a part past the last");
-        r->chunk = (r->nel + PEAK_BLOCKS - 1) / PEAK_BLOCKS;
-        r->peak_blocks = (int)((r->nel + r->chunk - 1) / r->chunk);
-        r->partial.alloc((size_t)r->peak_blocks * nparts);
+        r->peak.alloc(3 * nparts);
         r->dpeaks.alloc(nparts);
-        const size_t smem = 5 * sizeof(unsigned long long) * nparts;
-        if (smem > 48 * 1024)
-            FG_CUDA(cudaFuncSetAttribute(k_peak_blocks,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         FG_CUDA(cudaStreamSynchronize(s));
         *out = r.release();
     });
@@ -574,8 +647,9 @@ int femgpu_recovery_last_time(const femgpu_recovery* r, double* ms, double* byte
 
 size_t femgpu_recovery_bytes(const femgpu_recovery* r) {
     if (!r) return 0;
-    return r->t10.bytes() + r->rec.bytes() + r->tag.bytes() + r->singular.bytes() +
-           r->vm.bytes() + r->partial.bytes() + r->dpeaks.bytes() + r->inc.start.bytes() +
+    return r->t10.bytes() + r->rec.bytes() + r->mats.bytes() + r->singular.bytes() +
+           r->place.bytes() + r->u4.bytes() + r->peak.bytes() + r->dpeaks.bytes() +
+           r->inc.start.bytes() +
            r->inc.of_node.bytes() + r->du.bytes() + r->ddt.bytes() + r->dstress.bytes() +
            r->dstrain.bytes() + r->dmises.bytes() + r->dprincipal.bytes();
 }

@@ -244,6 +244,12 @@ def test_gpu_recovery_is_bit_identical_to_the_oracle():
 
 
 @pytest.mark.gpu
+def test_gpu_recovery_many_parts():
+    """More parts than a block keeps in shared memory (64): the maxima go to global memory."""
+    check_parity(random_case(dims=(4, 4, 3), seed=15, nparts=100))
+
+
+@pytest.mark.gpu
 def test_gpu_recovery_without_options():
     """No expansion, no temperature change, 1 part, no singular points."""
     c = random_case(dims=(3, 3, 2), seed=12, nparts=1)
