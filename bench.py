@@ -60,11 +60,12 @@ def args():
                    help="print each solver's levels and the device time of each kernel of 1 "
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
-                   choices=["heat", "cantilever", "p2beam", "batch", "serve"],
+                   choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
-                        "serve: a Poisson stream of solve requests through the server")
+                        "serve: a Poisson stream of solve requests through the server; "
+                        "recover: the stress recovery of the solved 200x20x20 P2 beam")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -94,6 +95,8 @@ class Clocks:
         self.proc = None
 
     def start(self):
+        """Starts the sampler and returns once it has written its first sample (at most 15 s):
+        nvidia-smi's own start-up then lies outside the timed region."""
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
@@ -101,6 +104,12 @@ class Clocks:
                 stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 15.0 and self.proc.poll() is None:
+            if os.path.getsize(self.file.name) > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -926,13 +935,138 @@ def _plumbing(world):
     return dist, barrier, max_over_ranks
 
 
+# ------------------------------------------------------------------ the recovery workload
+RECOVER_METRIC = "recovered points/s (P2 strain, stress, von Mises, principal, peaks)"
+
+
+def run_recover(opt, rank, world, local):
+    """The post-solve recovery of the 200x20x20 P2 beam (elastic_tet.rs:367-427, 482-483): the
+    beam solved once (mixed, 1e-8), then a step is 1 recovery of all 674,081 points from the
+    resident displacement: mean strain and stress, von Mises and principal stresses, and the
+    peaks of 4 parts (cells split by x) with the edges of the clamped face singular. e2e is the
+    same through the host C ABI (u from host memory, the results back)."""
+    import torch
+    import femahoy_b200 as fg
+    from femahoy_b200 import meshgen as mg
+    from femahoy_b200.recover import Recovery
+    torch.cuda.set_device(local)
+    dist, barrier, max_over_ranks = _plumbing(world)
+    box = mg.box(200, 20, 20, (200.0, 20.0, 20.0))
+    q = fg.Quadratic.new(box.points, box.tets)
+    prob = mg.beam_p2(q.edges, q.tets, mesh=box, seed=SEED)
+    K = fg.Csr.assemble(fg.P2_ELASTIC, prob.xyz, prob.nodes, prob.coef)
+    A = K.submatrix(prob.free)
+    rhs = fg.reduced_rhs(K, prob.load, prob.values, prob.free)
+    del K
+    P, coarse = fg.prolongation(prob.xyz, box.n, q.edges, prob.free)
+    unknowns = fg.Unknowns.Quadratic(prob.xyz[prob.free // 3], P, coarse)
+    solver = fg.Solver(A, unknowns, fg.Method.Multigrid,
+                       options=fg.Options(precision=fg.MIXED)).with_tol(TOL)
+    x = np.zeros(A.n)
+    solver.solve(rhs, x)
+    del solver
+    u = prob.values.copy()
+    u[prob.free] = x
+    xyz, t10 = prob.xyz, prob.nodes
+    n, ne = len(xyz), len(t10)
+    nparts = 4
+    part = (4 * np.arange(ne) // ne).astype(np.uint32)
+    on = lambda d, v: xyz[:, d] == v
+    singular = (on(0, 0.0) & (on(1, 0.0) | on(1, 20.0) | on(2, 0.0) | on(2, 20.0))).astype(
+        np.uint8)
+    t0 = time.perf_counter()
+    rec = Recovery(xyz, t10, prob.coef, part=part, nparts=nparts, singular=singular)
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(fg.lib().femgpu_recovery_stream(rec.handle))
+    dev = torch.device("cuda", local)
+    ud = torch.from_numpy(u).to(dev)
+    st = torch.empty((n, 6), dtype=torch.float64, device=dev)
+    sn, mi, pr = torch.empty_like(st), torch.empty(n, dtype=torch.float64, device=dev), \
+        torch.empty((n, 3), dtype=torch.float64, device=dev)
+
+    def step():
+        return rec.run_device(ud, st, sn, mises=mi, principal=pr)
+
+    for _ in range(opt.warmup):
+        step()
+    barrier()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    kms = []
+    e0.record(stream)
+    for _ in range(opt.steps):
+        step()
+        kms.append(rec.last_time())
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * n * opt.steps / (ms / 1e3)
+    # The recovery kernels alone (CUDA events around them on the recovery stream).
+    kernel_ms = float(np.median([k for k, _ in kms]))
+    kbytes = kms[-1][1]
+    peak, peak_kind = measured_peak()
+    achieved = kbytes / (kernel_ms * 1e-3) / 1e9
+    # e2e: the host form, u from pinned host memory and all results back to it.
+    hu = torch.from_numpy(u).pin_memory().numpy()
+    for _ in range(opt.warmup):
+        rec.run(hu)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(opt.steps):
+        out = rec.run(hu)
+    e2e_s = time.perf_counter() - t0
+    e2e_value = world * n * opt.steps / e2e_s
+    cpu = None
+    if rank == 0 and world == 1 and not opt.no_cpu_baseline:
+        import oracle
+        t0 = time.perf_counter()
+        ref = oracle.recover(xyz, t10, prob.coef, u, part=part, nparts=nparts,
+                             singular=singular)
+        cpu_s = time.perf_counter() - t0
+        same = all(np.array_equal(out[k].view(np.uint64), ref[k].view(np.uint64))
+                   for k in ("stress", "strain", "mises"))
+        cpu = {"value": n / cpu_s, "unit": "points/s", "cores": 1, "kind": "port",
+               "sample": f"1 full recovery of the same beam by the oracle ({cpu_s:.2f} s); "
+                         f"bits identical with the GPU's: {same}"}
+    line = {
+        "metric": RECOVER_METRIC, "value": value, "unit": "points/s", "n_gpus": world,
+        "steps": opt.steps, "warmup": opt.warmup, "ms_per_step": ms / opt.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"stress recovery of the 200x20x20 P2 beam (480,000 10-node "
+                               f"tets, {n} points) after its solve to 1e-8; 4 parts, "
+                               f"clamped-face edges singular",
+                   "points": n, "cells": ne, "flush": "inputs larger than L2",
+                   "parallelism": f"replicas x{world}"},
+        "setup_s": setup_s,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "kernel": "k_pad_u + k_recover_points<peaks> + k_peak_final",
+                     "bytes_per_launch": kbytes, "launch_ms": kernel_ms, "traffic": None},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": (6 + 6 + 1 + 3) * 8 * n},
+        "gpu_launches": 3 * opt.steps,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     opt = args()
     rank, world, local = dist_env()
     if opt.impl == "reference":
         run_reference(opt, rank, world)
         return
-    if opt.workload == "batch":
+    if opt.workload == "recover":
+        run_recover(opt, rank, world, local)
+    elif opt.workload == "batch":
         run_batch(opt, rank, world, local)
     elif opt.workload == "serve":
         run_serve(opt, rank, world, local)
