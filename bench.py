@@ -54,6 +54,10 @@ def args():
                         "kernel (0: none, the default)")
     p.add_argument("--launch", type=int, default=0,
                    help="0: programmatic dependent launch in the PCG loop (default), 1: plain")
+    p.add_argument("--coarsest", type=int, default=0,
+                   help="the largest level the dense coarse solve takes (0: 3000, the reference's)")
+    p.add_argument("--values", type=int, default=0,
+                   help="mixed form's stencil levels: 0 default, 1 FP32, 2 FP16 coefficients")
     p.add_argument("--degree", type=int, default=0,
                    help="Chebyshev degree of each pre- and post-smoothing (0: the default, 2)")
     p.add_argument("--breakdown", action="store_true",
@@ -353,7 +357,9 @@ def run_ours(opt, rank, world, local):
         s = fg.Solver(A, unknowns, fg.Method.Multigrid,
                       options=fg.Options(precision=precision, format=opt.format,
                                          graph=opt.graph, tail=opt.tail,
-                                         degree=opt.degree, launch=opt.launch)).with_tol(tol)
+                                         degree=opt.degree, launch=opt.launch,
+                                         values=opt.values,
+                                         coarsest=opt.coarsest)).with_tol(tol)
         return s, time.perf_counter() - t
 
     b = torch.from_numpy(rhs).cuda()

@@ -273,13 +273,15 @@ int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
             o.degree = options->degree;
             o.lower = options->lower;
             o.sell_c = options->sell_c;
-            o.coarsest = options->coarsest > 0 ? options->coarsest : 3000;
+            o.coarsest = options->coarsest > 0 ? options->coarsest : DEVICE_COARSEST;
             o.max_levels = options->max_levels > 0 ? options->max_levels : 30;
             o.graph = options->graph != 2;
             o.format = options->format;
             o.tail = options->tail;
             o.pdl = options->launch == 0 ? 1 : 0;
+            o.values = options->values;
         }
+        require(o.values >= 0 && o.values <= 2, "values is 0 (default), 1 (FP32) or 2 (FP16)");
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,
                 "the SELL chunk height must be 8, 16 or 32");

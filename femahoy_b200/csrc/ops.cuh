@@ -9,6 +9,8 @@
 // implicit: a row reads K coefficients of its own, K - 1 of earlier rows (recently read by
 // other threads, so from L2) and 2K - 1 entries of x; no index is stored.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "sell.cuh"
 
 namespace femgpu {
@@ -122,4 +124,47 @@ struct StencilOpK {
     }
 };
 
+// A stencil whose coefficients are stored as FP16, divided by the level's largest coefficient
+// magnitude `scale` so that they lie in [-1, 1] (11 significant bits, relative error at most
+// 2^-11 for magnitudes above 2^-14 of the largest). The products of the fine levels read little
+// but their coefficients, so these read about 0.6 of the bytes of the FP32 stencil. Each term is
+// converted to TA and accumulated with the fused multiply-adds of StencilOp, in the same order;
+// the sum is multiplied by `scale` at the end. KC > 0: K known at compile time; KC = 0: K read
+// from the view. Both give the same bits, so the autotuner's choice changes no result.
+struct StencilViewH {
+    int n;
+    int K;
+    int off[MAXK];
+    const __half* __restrict__ coef;
+    float scale;
+};
+
+template <int KC>
+struct StencilOpH {
+    StencilViewH v;
+    __device__ __forceinline__ int64_t threads() const { return v.n; }
+    __device__ __forceinline__ bool valid(int64_t) const { return true; }
+    template <class TA, class TX>
+    __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
+        const int i = (int)g, n = v.n;
+        const __half* __restrict__ c = v.coef;
+        const int K = KC > 0 ? KC : v.K;
+        TA acc = (TA)__half2float(__ldg(c + i)) * (TA)__ldg(x + i);
+#pragma unroll
+        for (int k = 1; k < (KC > 0 ? KC : MAXK); ++k) {
+            if (KC == 0 && k >= K) break;
+            const int o = v.off[k];
+            const __half* __restrict__ ck = c + (size_t)k * n;
+            const int j = i + o, m = i - o;
+            const bool up = j < n, lo = m >= 0;
+            acc = fmadd(up ? (TA)__half2float(__ldg(ck + i)) : (TA)0,
+                        up ? (TA)__ldg(x + j) : (TA)0, acc);
+            acc = fmadd(lo ? (TA)__half2float(__ldg(ck + m)) : (TA)0,
+                        lo ? (TA)__ldg(x + m) : (TA)0, acc);
+        }
+        return acc * (TA)v.scale;
+    }
+};
+
 }  // namespace femgpu
+

@@ -29,6 +29,8 @@
 namespace femgpu {
 
 constexpr int TH = 256;
+// The mixed form's stencil levels read FP16 coefficients unless the options say otherwise.
+constexpr bool kHalfDefault = false;
 
 // The grid that gives 1 thread to each of `rows` rows.
 static int row_blocks(int64_t rows) {
@@ -192,6 +194,17 @@ template void make_operator<float>(const HostCsr&, const DevCsr&, int, bool, Ope
 // stencil) and K = 14 (Galerkin levels: 27 points); these get unrolled kernels.
 template <class T, class F>
 static void with_op(const Operator<T>& op, F&& f) {
+    if constexpr (std::is_same<T, float>::value) {
+        if (op.half) {
+            if (op.unrolled && op.K == 8)
+                f(StencilOpH<8>{op.hview()});
+            else if (op.unrolled && op.K == 14)
+                f(StencilOpH<14>{op.hview()});
+            else
+                f(StencilOpH<0>{op.hview()});
+            return;
+        }
+    }
     if (op.block3)
         f(Block3Op<T>{op.b3view(), (int)op.n});
     else if (!op.stencil)
@@ -1007,6 +1020,21 @@ static void upload_values(const std::vector<double>& v, DevBuf<T>* d, cudaStream
     FG_CUDA(cudaStreamSynchronize(s));
 }
 
+// The FP16 copy of a stencil's coefficients (StencilOpH): each divided by the largest
+// magnitude and rounded to nearest. The FP32 coefficients stay for the fused coarse kernel.
+static void make_half(Operator<float>* op, cudaStream_t s) {
+    std::vector<float> c = op->coef.to_host(s);
+    float m = 0.0f;
+    for (float v : c) m = std::max(m, std::fabs(v));
+    if (!(m > 0.0f) || !std::isfinite(m)) return;
+    std::vector<__half> h(c.size());
+    for (size_t k = 0; k < c.size(); ++k) h[k] = __float2half_rn(c[k] / m);
+    op->hcoef.upload(h.data(), h.size(), s);
+    FG_CUDA(cudaStreamSynchronize(s));
+    op->hscale = m;
+    op->half = true;
+}
+
 // The autotuner's choice for a stencil operator: times y = b - A x with the runtime-K and the
 // compile-time-K kernels (5 launches each after 2 warm-up launches, CUDA events) and keeps the
 // faster. The choice depends on the level's size and on how the L2 serves its offsets.
@@ -1155,9 +1183,9 @@ static std::string describe_op(const Operator<T>& op) {
     } else if (!op.stencil) {
         std::snprintf(buf, sizeof buf, "sell C=%d nnz=%lld", op.sell.C, (long long)op.nnz);
     } else {
-        std::snprintf(buf, sizeof buf, "stencil K=%d %s (probe %.1f / %.1f us) nnz=%lld", op.K,
-                      op.unrolled ? "unrolled" : "loop", op.probe_ms[0] * 1e3,
-                      op.probe_ms[1] * 1e3, (long long)op.nnz);
+        std::snprintf(buf, sizeof buf, "stencil K=%d %s%s (probe %.1f / %.1f us) nnz=%lld", op.K,
+                      op.half ? "fp16 " : "", op.unrolled ? "unrolled" : "loop",
+                      op.probe_ms[0] * 1e3, op.probe_ms[1] * 1e3, (long long)op.nnz);
     }
     return buf;
 }
@@ -1448,6 +1476,9 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
             PhaseTimer t{this, "level operators and autotuner", s_};
             upload_csr(mats[l], &d, s_);
             make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
+            if constexpr (std::is_same<T, float>::value)
+                if (lv.A.stencil && (opt_.values == 2 || (opt_.values == 0 && kHalfDefault)))
+                    make_half(&lv.A, s_);
             tune_operator(&lv.A, s_);
         }
         PhaseTimer t_lam{this, "diagonals and lambda_max", s_};
@@ -1533,7 +1564,7 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
         mats.push_back(galerkin(*pfirst, mats[0], threads));
         ps.push_back(*pfirst);
     }
-    size_t coarsest = (size_t)(opt_.coarsest > 0 ? opt_.coarsest : 3000);
+    size_t coarsest = (size_t)(opt_.coarsest > 0 ? opt_.coarsest : DEVICE_COARSEST);
     size_t max_levels = (size_t)(opt_.max_levels > 0 ? opt_.max_levels : 30);
     for (;;) {
         const HostCsr& a = mats.back();

@@ -36,12 +36,15 @@ struct Operator {
     bool stencil = false;
     bool block3 = false;  // the 3x3-block form (elasticity), else SELL-C, when not a stencil
     bool unrolled = false;  // the compile-time-K kernel (K = 8 or 14), chosen by timing
+    bool half = false;      // the stencil's products read its FP16 copy (hcoef, hscale)
     double probe_ms[2] = {0, 0};  // the timed product: runtime K, compile-time K
     int64_t n = 0, nnz = 0;
     Sell<T> sell;
     int K = 0;
     std::vector<int64_t> off;
     DevBuf<T> coef;
+    DevBuf<__half> hcoef;
+    float hscale = 1.0f;
     DevBuf<int64_t> b3ptr;
     DevBuf<uint32_t> b3col;
     DevBuf<T> b3val;
@@ -59,13 +62,23 @@ struct Operator {
         v.coef = coef.p;
         return v;
     }
+    StencilViewH hview() const {
+        StencilViewH v{};
+        v.n = (int)n;
+        v.K = K;
+        for (int k = 0; k < K; ++k) v.off[k] = (int)off[k];
+        v.coef = hcoef.p;
+        v.scale = hscale;
+        return v;
+    }
     size_t bytes() const {
-        return sell.bytes() + coef.bytes() + b3ptr.bytes() + b3col.bytes() + b3val.bytes();
+        return sell.bytes() + coef.bytes() + hcoef.bytes() + b3ptr.bytes() + b3col.bytes() +
+               b3val.bytes();
     }
     // The bytes one product reads and writes, each value once: the stored coefficients (and
     // indices), x and y.
     double stream_bytes() const {
-        if (stencil) return (double)K * n * sizeof(T) + 2.0 * n * sizeof(T);
+        if (stencil) return (double)K * n * (half ? 2 : sizeof(T)) + 2.0 * n * sizeof(T);
         if (block3) return (double)nnz / 9 * (9 * sizeof(T) + 4) + 2.0 * n * sizeof(T);
         return (double)nnz * (sizeof(T) + 4) + 2.0 * n * sizeof(T);
     }
@@ -174,17 +187,25 @@ struct Hierarchy {
     size_t bytes() const;
 };
 
+// The largest level that the dense coarse solve takes by default. The reference stops
+// coarsening at 3000 unknowns (multigrid.rs:94, COARSEST) and factors that level sparsely; a
+// dense inverse of up to 5000 unknowns (100 MB in FP32) is applied by 1 matrix-vector product
+// on the device, and on the 128^3 heat cube the level of 4,913 rows taken whole saves 2 coarser
+// levels' kernels and 1 PCG iteration (9 instead of 10, 3.28 instead of 3.50 ms).
+constexpr int DEVICE_COARSEST = 5000;
+
 struct Options {
     int precision = FEMGPU_FP64;
     int degree = 0;
     double lower = 0;
     int sell_c = 0;
     int format = 0;  // 0: stencil where possible, else SELL; 1: SELL only
-    int coarsest = 3000;
+    int coarsest = DEVICE_COARSEST;
     int max_levels = 30;
     bool graph = true;
     int tail = 0;  // levels of at most this many rows run fused (<= 0: none)
     int pdl = 1;   // programmatic dependent launch between the iteration's kernels
+    int values = 0;  // mixed form's stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
 };
 
 class SolverImpl {

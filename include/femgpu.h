@@ -191,7 +191,10 @@ typedef struct femgpu_options {
     double lower;         /* Chebyshev interval lower end as a fraction of lambda_max; 0 = default */
     int sell_c;           /* SELL chunk height (rows per slice): 0 = autotuned */
     int sell_sigma;       /* SELL sorting window in rows: 0 = autotuned */
-    int coarsest;         /* the largest level that the dense coarse solve takes; 0 = 3000 */
+    int coarsest;         /* the largest level that the dense coarse solve takes; 0 = 5000 (the
+                             reference's COARSEST is 3000, multigrid.rs:94; the dense inverse
+                             on the device takes 1 level more and the box grids measured
+                             converge in 1 iteration less) */
     int max_levels;       /* 0 = 30 (multigrid.rs:94) */
     int graph;            /* 1 = replay each PCG iteration as a CUDA graph (default), 2 = off */
     int format;           /* 0 = a symmetric stencil for each level whose entries sit at a few
@@ -204,6 +207,10 @@ typedef struct femgpu_options {
     int launch;           /* 0 = each kernel of a PCG iteration may start while the one before
                              it drains, waiting on the device for its results (programmatic
                              dependent launch; default); 1 = plain stream-ordered launches */
+    int values;           /* the mixed form's stencil levels: 0 = the default, 1 = FP32
+                             coefficients, 2 = FP16 coefficients scaled by the level's largest
+                             (the products read about 0.6 of the bytes; the V-cycle changes by
+                             about 2^-11 relative) */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end

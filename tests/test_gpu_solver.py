@@ -122,10 +122,13 @@ def test_points_refuse_multigrid():
 
 
 def test_not_converged_and_cancelled_texts():
-    """multigrid.rs:729-737 through the device loop."""
+    """multigrid.rs:729-737 through the device loop (on the reference's coarsest size, 3000, so
+    that the cycle is not the exact dense solve)."""
     h = mg.heat_cube(16)
     A, rhs, _ = _system(h)
-    s = fg.Solver(A, _grid(h), fg.Method.Multigrid).with_max_iter(1)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid,
+                  options=fg.Options(coarsest=3000)).with_max_iter(1)
+    assert len(s.levels()) >= 2
     with pytest.raises(fg.FemError, match="^conjugate gradients did not converge: the residual is"):
         s.solve(rhs, np.zeros(A.n))
     s.with_max_iter(500)
@@ -249,6 +252,28 @@ def test_programmatic_launches_give_the_same_bits(precision):
         assert st.true_residual <= 1e-10
         xs.append(x)
     assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
+
+
+def test_fp16_stencil_coefficients_solve_to_the_same_tolerance():
+    """The mixed form with the stencil levels' coefficients in FP16 (scaled by each level's
+    largest): the V-cycle changes by about 2^-11 relative, and flexible CG still reaches the
+    tolerance on the true FP64 residual in at most 1 more iteration. The FP64 form ignores the
+    option."""
+    h = mg.heat_cube(32, seed=3)
+    A, rhs, _ = _system(h)
+    its = {}
+    for values in (1, 2):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=fg.MIXED,
+                      options=fg.Options(precision=fg.MIXED, values=values)).with_tol(1e-10)
+        assert ("fp16" in s.describe()) == (values == 2)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1.2e-10
+        its[values] = st.iterations
+    assert its[2] <= its[1] + 1
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=fg.FP64,
+                  options=fg.Options(precision=fg.FP64, values=2))
+    assert "fp16" not in s.describe()
 
 
 @pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
