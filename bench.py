@@ -64,12 +64,14 @@ def args():
                    help="print each solver's levels and the device time of each kernel of 1 "
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
-                   choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover"],
+                   choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover",
+                            "transient"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
                         "serve: a Poisson stream of solve requests through the server; "
-                        "recover: the stress recovery of the solved 200x20x20 P2 beam")
+                        "recover: the stress recovery of the solved 200x20x20 P2 beam; "
+                        "transient: backward-Euler steps of the 128^3 heat cube")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -941,6 +943,91 @@ def _plumbing(world):
     return dist, barrier, max_over_ranks
 
 
+# ------------------------------------------------------------------ the transient workload
+TRANSIENT_METRIC = "DOF-steps/s of backward-Euler transient heat (1 resident operator)"
+
+
+def run_transient(opt, rank, world, local):
+    """The transient loop of heat.rs:686-733 on the 128^3 heat cube: lumped capacity 1 per unit
+    volume, dt = 1e-3, from T = 0 with the fixed temperatures of the steady problem; a step is 1
+    time step (right side, 1 warm-started solve to 1e-8, the temperatures), mixed form. The
+    call is the public host API (load and temperatures in, the last temperatures and 1 frame
+    per 10 steps out), so value and e2e are the same measurement; the device time of the solves
+    is reported beside it. The CPU baseline runs the oracle's loop for 2 steps."""
+    import torch
+    import femahoy_b200 as fg
+    from femahoy_b200 import meshgen as mg
+    from femahoy_b200.transient import Transient
+    torch.cuda.set_device(local)
+    dist, barrier, max_over_ranks = _plumbing(world)
+    h = build_problem(opt.cells)
+    K = fg.Csr.assemble(fg.P1_HEAT, h.xyz, h.nodes, h.coef)
+    cap = mg.lumped_capacity(h.mesh, capacity=1.0)
+    planes, pts, comp = mg.grid_unknowns(h)
+    u = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+    dt = 1e-3
+    t0 = time.perf_counter()
+    tr = Transient(K, cap, dt, h.free, u, fg.Method.Multigrid,
+                   options=fg.Options(precision=fg.MIXED))
+    tr.solver.with_tol(TOL)
+    setup_s = time.perf_counter() - t0
+    every = 10
+    tr.run(opt.warmup, h.load, h.values, output_every=every)
+    barrier()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    t0 = time.perf_counter()
+    frames, energies, t, st = tr.run(opt.steps, h.load, h.values, output_every=every)
+    torch.cuda.synchronize()
+    wall = max_over_ranks(time.perf_counter() - t0)
+    clk = clocks.stop()
+    n_free = tr.nfree
+    value = world * n_free * opt.steps / wall
+    cpu = None
+    if rank == 0 and world == 1 and not opt.no_cpu_baseline:
+        import oracle
+        k = oracle.pattern(h.n_points, h.nodes)
+        k.assemble(0, h.xyz, h.nodes, h.coef)
+        t1 = time.perf_counter()
+        of, oe, its = oracle.transient(
+            k, cap, dt, h.free, h.load, h.values, 2,
+            lambda a: oracle.Solver(a, "grid", planes=planes, points=pts, comp=comp,
+                                    method="multigrid"), tol=TOL)
+        cpu_s = time.perf_counter() - t1
+        cpu = {"value": n_free * 2 / cpu_s, "unit": "DOF-steps/s", "cores": 1, "kind": "port",
+               "sample": f"the oracle's loop (the reference's algorithm, FP64 PCG + line "
+                         f"Gauss-Seidel multigrid) for 2 steps, {its} PCG iterations, "
+                         f"{cpu_s:.1f} s including its hierarchy setup"}
+    imb = max(abs(e.stored - h.load.sum() - e.fixed) / e.gross for e in energies)
+    line = {
+        "metric": TRANSIENT_METRIC, "value": value, "unit": "DOF-steps/s", "n_gpus": world,
+        "steps": opt.steps, "warmup": opt.warmup, "ms_per_step": 1e3 * wall / opt.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
+        "config": {"workload": f"transient P1 heat, {opt.cells}^3 Kuhn box, lognormal k (seed "
+                               f"{SEED}), lumped capacity 1, dt 1e-3, from T = 0, each step "
+                               f"solved to 1e-8 from the last temperatures",
+                   "free_dofs": n_free, "flush": "inputs larger than L2",
+                   "parallelism": f"replicas x{world}"},
+        "pcg_iterations_per_step": st.iterations / opt.steps,
+        "device_solve_ms_per_step": 1e3 * st.seconds / opt.steps,
+        "energy_imbalance": imb, "setup_s": setup_s,
+        "roofline": {"bound": "hbm", "achieved": None, "peak": measured_peak()[0],
+                     "unit": "GB/s", "frac": None,
+                     "note": "the per-step solve is the heat solve of the default line"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": "DOF-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 8 * h.n_points // every},
+        "gpu_launches": st.launches,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ------------------------------------------------------------------ the recovery workload
 RECOVER_METRIC = "recovered points/s (P2 strain, stress, von Mises, principal, peaks)"
 
@@ -1072,6 +1159,8 @@ def main():
         return
     if opt.workload == "recover":
         run_recover(opt, rank, world, local)
+    elif opt.workload == "transient":
+        run_transient(opt, rank, world, local)
     elif opt.workload == "batch":
         run_batch(opt, rank, world, local)
     elif opt.workload == "serve":

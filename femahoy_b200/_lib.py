@@ -70,6 +70,10 @@ class Stats_t(C.Structure):
                 ("launches", C.c_size_t)]
 
 
+class Energy_t(C.Structure):
+    _fields_ = [("stored", C.c_double), ("fixed", C.c_double), ("gross", C.c_double)]
+
+
 class Peak_t(C.Structure):
     _fields_ = [("mises", C.c_double), ("element", C.c_int64), ("local", C.c_int32),
                 ("point", C.c_uint32), ("singular", C.c_int32), ("pad", C.c_int32),
@@ -157,6 +161,15 @@ SIGNATURES = {
     "femgpu_batch_bytes": (C.c_size_t, [C.c_void_p]),
     "femgpu_batch_stream": (C.c_void_p, [C.c_void_p]),
     "femgpu_batch_free": (None, [C.c_void_p]),
+    "femgpu_transient_new": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                       C.c_size_t, C.POINTER(Unknowns_t), C.c_int,
+                                       C.POINTER(Crossover_t), C.POINTER(Options_t),
+                                       C.POINTER(C.c_void_p)]),
+    "femgpu_transient_solver": (C.c_void_p, [C.c_void_p]),
+    "femgpu_transient_run": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                       C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(Stats_t)]),
+    "femgpu_transient_free": (None, [C.c_void_p]),
     "femgpu_recovery_new": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),

@@ -293,12 +293,13 @@ __device__ __forceinline__ T offset_row(const OffsetView<T>& M, int i, const T* 
     return s;
 }
 
-// Row i of x = M b for the n x n matrix M, by 1 warp (lane `lane`): 4 lane-strided partial sums,
-// then a butterfly over the warp; every lane ends with the sum.
+// Row i of x = M b for the n x n matrix M stored with leading dimension ld, by 1 warp (lane
+// `lane`): 4 lane-strided partial sums, then a butterfly over the warp; every lane ends with the
+// sum.
 template <class T>
 __device__ __forceinline__ T gemv_warp_row(const T* __restrict__ M, const T* __restrict__ b,
-                                           int64_t n, int64_t i, int lane) {
-    const T* row = M + i * n;
+                                           int64_t n, int64_t ld, int64_t i, int lane) {
+    const T* row = M + i * ld;
     T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
     int64_t k = lane;
     for (; k + 96 < n; k += 128) {
@@ -308,6 +309,63 @@ __device__ __forceinline__ T gemv_warp_row(const T* __restrict__ M, const T* __r
         s3 += row[k + 96] * __ldg(b + k + 96);
     }
     for (; k < n; k += 32) s0 += row[k] * __ldg(b + k);
+    T s = (s0 + s1) + (s2 + s3);
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+// The leading dimension of a coarsest inverse: n rounded up to 32 elements, so that every row
+// starts on a 128-byte boundary. The padding columns, and the coarse right side past n, are 0.
+__host__ __device__ __forceinline__ int64_t dense_ld(int64_t n) { return (n + 31) / 32 * 32; }
+
+template <class T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+    typedef float4 type;
+};
+template <>
+struct Vec16<double> {
+    typedef double2 type;
+};
+__device__ __forceinline__ float dot_add(float4 m, float4 x, float s) {
+    s += m.x * x.x;
+    s += m.y * x.y;
+    s += m.z * x.z;
+    s += m.w * x.w;
+    return s;
+}
+__device__ __forceinline__ double dot_add(double2 m, double2 x, double s) {
+    s += m.x * x.x;
+    s += m.y * x.y;
+    return s;
+}
+
+// The same row with M at leading dimension dense_ld(n) and b padded to it with zeros: 16-byte
+// loads of M and b, 4 per lane in flight (2 KB per warp), against the 128 bytes of 4 scalar
+// loads: the coarsest product of the box grids (4,913 rows, 96 MB in FP32) is bound by the
+// bytes a warp keeps in flight. 4 partial sums over 16-byte chunks, then the butterfly.
+template <class T>
+__device__ __forceinline__ T gemv_warp_row_padded(const T* __restrict__ M,
+                                                  const T* __restrict__ b, int64_t ld, int64_t i,
+                                                  int lane) {
+    typedef typename Vec16<T>::type VT;
+    const VT* row = reinterpret_cast<const VT*>(M + i * ld);
+    const VT* bv = reinterpret_cast<const VT*>(b);
+    const int64_t nc = ld / (int64_t)(sizeof(VT) / sizeof(T));
+    T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    int64_t c = lane;
+    for (; c + 96 < nc; c += 128) {
+        const VT m0 = __ldg(row + c), m1 = __ldg(row + c + 32), m2 = __ldg(row + c + 64),
+                 m3 = __ldg(row + c + 96);
+        const VT x0 = __ldg(bv + c), x1 = __ldg(bv + c + 32), x2 = __ldg(bv + c + 64),
+                 x3 = __ldg(bv + c + 96);
+        s0 = dot_add(m0, x0, s0);
+        s1 = dot_add(m1, x1, s1);
+        s2 = dot_add(m2, x2, s2);
+        s3 = dot_add(m3, x3, s3);
+    }
+    for (; c < nc; c += 32) s0 = dot_add(__ldg(row + c), __ldg(bv + c), s0);
     T s = (s0 + s1) + (s2 + s3);
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     return s;
@@ -402,9 +460,12 @@ static void launch_transfer(const OffsetTransfer<T>& M, const T* in, T* out, int
         launch(pdl, k_transfer<T, 0>, g, TH, s, v, in, out, accumulate, done);
 }
 
-// x = M b for the symmetric n x n matrix M (the coarsest inverse): 1 warp per row.
-template <class T>
-__global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__ b,
+// x = M b for the symmetric n x n matrix M (a dense inverse) at leading dimension ld: 1 warp per
+// row. PADDED: ld = dense_ld(n) and b padded to it (the coarsest level of a hierarchy, whose
+// right side is the hierarchy's own padded vector); else scalar loads (the direct method, and a
+// hierarchy of no smoothed level, whose right side is the caller's vector).
+template <class T, bool PADDED>
+__global__ void k_gemv(int64_t n, int64_t ld, const T* __restrict__ M, const T* __restrict__ b,
                        T* __restrict__ x, const int* __restrict__ done) {
     pdl_wait();
     if (*done) return;
@@ -412,7 +473,7 @@ __global__ void k_gemv(int64_t n, const T* __restrict__ M, const T* __restrict__
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = w; i < n; i += nw) {
-        T s = gemv_warp_row(M, b, n, i, lane);
+        T s = PADDED ? gemv_warp_row_padded(M, b, ld, i, lane) : gemv_warp_row(M, b, n, ld, i, lane);
         if (lane == 0) x[i] = s;
     }
 }
@@ -493,7 +554,7 @@ __global__ void __launch_bounds__(TH)
         const int lane = threadIdx.x & 31;
         const T* bc = sL[nl - 1].bc;
         for (int64_t i = tid >> 5; i < nco; i += nth >> 5) {
-            const T s = gemv_warp_row(inv, bc, nco, i, lane);
+            const T s = gemv_warp_row_padded(inv, bc, dense_ld(nco), i, lane);
             if (lane == 0) cx[i] = s;
         }
         grid.sync();
@@ -528,6 +589,15 @@ __global__ void k_add(int64_t n, const double* __restrict__ t, double* __restric
 template <class S, class D>
 __global__ void k_convert(int64_t n, const S* __restrict__ a, D* __restrict__ b) {
     GRID_STRIDE(i, n) b[i] = (D)a[i];
+}
+
+// The n x n matrix a (row-major) into b at leading dimension ld, the padding columns 0.
+template <class S, class D>
+__global__ void k_convert_pad(int64_t n, int64_t ld, const S* __restrict__ a, D* __restrict__ b) {
+    GRID_STRIDE(k, n * ld) {
+        const int64_t i = k / ld, j = k % ld;
+        b[k] = j < n ? (D)a[i * n + j] : (D)0;
+    }
 }
 
 // ------------------------------------------------------------------ reductions
@@ -1538,16 +1608,15 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
     H->ncoarse = last.n;
     DevBuf<double> inv64;
     dense_inverse(last, &inv64, s_);
-    if constexpr (std::is_same<T, double>::value) {
-        H->inv = std::move(inv64);
-    } else {
-        H->inv.alloc(last.n * last.n);
-        k_convert<double, T><<<blocks_for(last.n * last.n, TH), TH, 0, s_>>>(last.n * last.n,
-                                                                            inv64.p, H->inv.p);
-        FG_CHECK_LAUNCH();
-        FG_CUDA(cudaStreamSynchronize(s_));
-    }
-    H->cb.alloc(last.n);
+    // Rows at leading dimension dense_ld(n), the padding 0; the right side padded with zeros.
+    const int64_t ld = dense_ld(last.n);
+    H->inv.alloc(last.n * ld);
+    k_convert_pad<double, T><<<blocks_for(last.n * ld, TH), TH, 0, s_>>>(last.n, ld, inv64.p,
+                                                                         H->inv.p);
+    FG_CHECK_LAUNCH();
+    H->cb.alloc(ld);
+    H->cb.zero(s_);
+    FG_CUDA(cudaStreamSynchronize(s_));
     H->cx.alloc(last.n);
     build_tail(H, opt_.tail, s_);
 }
@@ -1601,7 +1670,12 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     const int* done = &sc_.p->done;
     if (l == H.levels.size()) {
         int64_t n = H.ncoarse;
-        launch(pdl_, k_gemv<T>, blocks_for(n * 32, TH), TH, s_, n, H.inv.p, b, H.cx.p, done);
+        if (b == H.cb.p)
+            launch(pdl_, k_gemv<T, true>, blocks_for(n * 32, TH), TH, s_, n, dense_ld(n),
+                   H.inv.p, b, H.cx.p, done);
+        else
+            launch(pdl_, k_gemv<T, false>, blocks_for(n * 32, TH), TH, s_, n, dense_ld(n),
+                   H.inv.p, b, H.cx.p, done);
         FG_CHECK_LAUNCH();
         mark("coarsest dense solve n=" + std::to_string(n));
         launches_ += 1;
@@ -1812,7 +1886,7 @@ void SolverImpl::solve_host(const double* h_b, double* h_x, const volatile int* 
 void SolverImpl::precondition(const double* d_r, double* d_z) {
     FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
     if (direct_) {
-        k_gemv<double><<<blocks_for(n_ * 32, TH), TH, 0, s_>>>(n_, dense_inv_.p, d_r, d_z,
+        k_gemv<double, false><<<blocks_for(n_ * 32, TH), TH, 0, s_>>>(n_, n_, dense_inv_.p, d_r, d_z,
                                                                done_zero_.p);
     } else if (opt_.precision == FEMGPU_MIXED) {
         k_convert<double, float><<<blocks_for(n_, TH), TH, 0, s_>>>(n_, d_r, r32_.p);
@@ -1841,13 +1915,13 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         launches_ = 8;
         // solve.rs:206-218: x = A^-1 b (with 1 step of refinement in FP64), then the true
         // residual.
-        k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, dense_inv_.p, b_.p, x_.p,
+        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, b_.p, x_.p,
                                                               done_zero_.p);
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
             SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p, nullptr, partial_.p);
         k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                    FinResidual0{sc_.p});
-        k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, dense_inv_.p, r_.p, t_.p,
+        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, r_.p, t_.p,
                                                               done_zero_.p);
         k_add<<<blocks_for(n, TH), TH, 0, s_>>>(n, t_.p, x_.p);
         FG_CHECK_LAUNCH();

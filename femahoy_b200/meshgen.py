@@ -145,6 +145,17 @@ def heat_cube(n=128, seed=1234, source=1.0) -> Problem:
                    xyz=mesh.points, seed=seed)
 
 
+def lumped_capacity(mesh, capacity=1.0):
+    """crates/fem/src/heat.rs:417-423: each corner of a tetrahedron takes capacity V/4, summed
+    in tetrahedron order."""
+    vol = tet_volumes(mesh.points, mesh.tets)
+    out = np.zeros(mesh.n)
+    share = capacity * vol / 4.0
+    for c in range(4):
+        np.add.at(out, mesh.tets[:, c], share)
+    return out
+
+
 def tet_volumes(points, tets):
     p = points[tets]
     e = p[:, 1:, :] - p[:, :1, :]

@@ -180,9 +180,16 @@ class Solver:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
+        if h and not getattr(self, "_owner", None):
             L.lib().femgpu_solver_free(h)
             self._h = None
+
+    @classmethod
+    def _borrowed(cls, handle, n, owner):
+        """The solver of another handle (a transient loop's), freed with its owner."""
+        s = cls.__new__(cls)
+        s._h, s.n, s._owner = handle, n, owner
+        return s
 
     @property
     def handle(self):

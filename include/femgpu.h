@@ -351,6 +351,48 @@ size_t femgpu_batch_bytes(const femgpu_batch* b);
 void* femgpu_batch_stream(const femgpu_batch* b);
 void femgpu_batch_free(femgpu_batch* b);
 
+/* ---------------------------------------------------------------- transient heat */
+
+/* The backward-Euler loop of a transient heat model with lumped capacity (heat.rs:686-733): 1
+ * operator, K + C/dt on the free points, solved once per time step from the last temperatures.
+ * The matrix, its solver and the vectors stay on the device for the whole run. */
+typedef struct femgpu_transient femgpu_transient;
+
+/* The energy terms of heat.rs:535-547 that the loop forms, for a step with no radiation:
+ * stored = sum of the rates C (T - T_prev) / dt; fixed = sum over the fixed points of
+ * q = (K T)_i + rate_i - load_i; gross = sum of |rate| and |q|. The caller adds its own source,
+ * flux and convection terms. Summed on the device in a fixed order (deterministic; not the
+ * reference's point order, so they agree to rounding). */
+typedef struct femgpu_energy {
+    double stored;
+    double fixed;
+    double gross;
+} femgpu_energy;
+
+/* heat.rs:688-703: `k` the full conductivity matrix (femgpu_assemble, P1 heat), `capacity` the
+ * lumped capacity of each point, `dt` the step, `free` the free points (increasing) and
+ * `unknowns` their grid level, as for femgpu_solver_new (whose method, crossover and options
+ * these are). A NULL crossover is Unknowns(16384): the reference's TRANSIENT_DIRECT_LIMIT is
+ * 40,000 (solve.rs:24), and the direct solver of this library holds 16,384 unknowns. */
+int femgpu_transient_new(const femgpu_csr* k, const double* capacity, double dt,
+                         const int64_t* free, size_t nfree, const femgpu_unknowns* unknowns,
+                         int method, const femgpu_crossover* crossover,
+                         const femgpu_options* options, femgpu_transient** out);
+/* The solver of the loop, for femgpu_solver_set_tol / _set_max_iter / _describe. It belongs to
+ * the transient handle. */
+femgpu_solver* femgpu_transient_solver(femgpu_transient* t);
+/* heat.rs:709-733 for `steps` steps: `temperature` (n) holds the start values (the fixed points
+ * keep theirs) and gets the last step's; `load` (n) is the constant load of each point. The
+ * steps s with s % output_every == 0 or s == steps write their temperatures to `frames`
+ * (n each, in order; NULL skips them) and their energies to `energies` (NULL skips them).
+ * "cancelled" between steps and between PCG iterations, as the reference. `stats` sums the
+ * iterations, device seconds and launches of all steps. Host pointers. */
+int femgpu_transient_run(femgpu_transient* t, size_t steps, const double* load,
+                         double* temperature, size_t output_every, double* frames,
+                         femgpu_energy* energies, const volatile int* cancel,
+                         femgpu_stats* stats);
+void femgpu_transient_free(femgpu_transient* t);
+
 /* ---------------------------------------------------------------- post-solve recovery */
 
 /* The strain and the stress of a solved P2 elasticity model at the 10 points of each cell,

@@ -70,6 +70,9 @@ def _load():
         "orc_solver_solve": (I, [P, P, P, D, S, P, P, P, P, S]),
         "orc_solver_precondition": (None, [P, P, P]),
         "orc_recover": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
+        "orc_add_capacity": (I, [P, P, D, P, S]),
+        "orc_reduced_rhs_transient": (None, [P, P, P, P, S, P, D, P]),
+        "orc_transient_energy": (None, [S, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -148,6 +151,24 @@ class Csr:
         free = np.ascontiguousarray(free, dtype=np.int64)
         out = np.empty(len(free))
         _lib.orc_reduced_rhs(self.h, _p(load), _p(t), _p(free), len(free), _p(out))
+        return out
+
+    def add_capacity(self, capacity, dt):
+        """heat.rs:691-696: capacity / dt added to each diagonal entry, in place."""
+        capacity = np.ascontiguousarray(capacity, dtype=np.float64)
+        err = C.create_string_buffer(512)
+        if _lib.orc_add_capacity(self.h, _p(capacity), dt, err, 512):
+            raise OracleError(err.value.decode())
+
+    def reduced_rhs_transient(self, load, t, free, capacity, dt):
+        """heat.rs:1219-1244 with Some((capacity, dt))."""
+        load = np.ascontiguousarray(load, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        free = np.ascontiguousarray(free, dtype=np.int64)
+        capacity = np.ascontiguousarray(capacity, dtype=np.float64)
+        out = np.empty(len(free))
+        _lib.orc_reduced_rhs_transient(self.h, _p(load), _p(t), _p(free), len(free),
+                                       _p(capacity), dt, _p(out))
         return out
 
     def assemble(self, kind, xyz, nodes, coef):
@@ -424,3 +445,44 @@ class Solver:
         z = np.zeros(self.n)
         _lib.orc_solver_precondition(self.h, _p(r), _p(z))
         return z
+
+
+def transient_energy(kt, rate, load, fixed):
+    """heat.rs:535-547 for a transient step with no radiation, summed in point order: (stored,
+    fixed, the sum of |rate| and |q| over the points)."""
+    kt, rate, load = (np.ascontiguousarray(a, dtype=np.float64) for a in (kt, rate, load))
+    fixed = np.ascontiguousarray(fixed, dtype=np.uint8)
+    out = np.empty(3)
+    _lib.orc_transient_energy(len(kt), _p(kt), _p(rate), _p(load), _p(fixed), _p(out))
+    return tuple(out)
+
+
+def transient(k, capacity, dt, free, load, t0, steps, make_solver, output_every=1, tol=1e-10):
+    """heat.rs:686-733: backward Euler with the lumped capacity. ``k`` is the full conductivity
+    matrix (a Csr), ``make_solver(a)`` the solver of the free unknowns of K + C/dt. Returns the
+    temperatures and the energies (stored, fixed, |rate| + |q| summed) of the steps s with
+    s % output_every == 0 or s == steps, and the PCG iterations of all steps."""
+    n = k.n
+    ptr, idx, val = k.arrays()
+    a_full = Csr.from_arrays(n, ptr, idx, val)
+    a_full.add_capacity(capacity, dt)
+    solver = make_solver(a_full.submatrix(free))
+    capacity = np.asarray(capacity, dtype=np.float64)
+    t = np.array(t0, dtype=np.float64, copy=True)
+    x = t[free].copy()
+    fixed = np.ones(n, np.uint8)
+    fixed[free] = 0
+    frames, energies, iterations = [], [], 0
+    for s in range(1, steps + 1):
+        previous = t.copy()
+        rhs = a_full.reduced_rhs_transient(load, t, free, capacity, dt)
+        x, it, _ = solver.solve(rhs, x, tol=tol)
+        iterations += it
+        t[free] = x
+        kt = k.mul(t)
+        rate = capacity * (t - previous) / dt
+        if s % max(output_every, 1) == 0 or s == steps:
+            frames.append(t.copy())
+            energies.append(transient_energy(kt, rate, load, fixed))
+    return frames, energies, iterations
+

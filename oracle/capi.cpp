@@ -363,6 +363,28 @@ void orc_solver_precondition(void* s, const double* r, double* z) {
         o->s.pmg.apply(o->s.a, r, z);
 }
 
+// heat.rs:691-696 on the matrix `h`; -1 and the reference's text when a row has no diagonal.
+int orc_add_capacity(void* h, const double* capacity, double dt, char* err, size_t len) {
+    try {
+        add_capacity(C(h), capacity, dt);
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+// heat.rs:1219-1244 with the capacity term of a transient step.
+void orc_reduced_rhs_transient(void* h, const double* load, const double* t, const int64_t* free,
+                               size_t nfree, const double* capacity, double dt, double* out) {
+    vector<size_t> f(free, free + nfree);
+    vector<double> r = reduced_rhs(*C(h), load, t, f, capacity, dt);
+    std::copy(r.begin(), r.end(), out);
+}
+void orc_transient_energy(size_t n, const double* kt, const double* rate, const double* load,
+                          const uint8_t* fixed, double* out) {
+    transient_energy(n, kt, rate, load, fixed, out);
+}
+
 // elastic_tet.rs:367-427 and 482-483 (see recover_tet10). Optional arrays may be null;
 // `peaks` holds nparts entries.
 int orc_recover(size_t npoints, const double* xyz, size_t nel, const uint32_t* tets10,

@@ -46,13 +46,14 @@ void tet_conduction(const Vec3 g[4], double v, const Vec3& k, double ke[16]) {
         }
 }
 
-// heat.rs:1219-1244 with `transient = None`.
+// heat.rs:1219-1244; `capacity` null is `transient = None`, else Some((capacity, dt)).
 vector<double> reduced_rhs(const Csr& a, const double* load, const double* t,
-                           const vector<size_t>& free) {
+                           const vector<size_t>& free, const double* capacity, double dt) {
     vector<double> out(free.size());
     for (size_t k = 0; k < free.size(); ++k) {
         size_t i = free[k];
         double r = load[i];
+        if (capacity) r += capacity[i] / dt * t[i];
         for (size_t e = a.ptr[i]; e < a.ptr[i + 1]; ++e) {
             size_t j = a.idx[e];
             if (!std::binary_search(free.begin(), free.end(), j)) r -= a.val[e] * t[j];
@@ -266,4 +267,33 @@ vector<uint32_t> colour_elements(size_t n, const uint32_t* elements, size_t nel,
     return colour;
 }
 
+// heat.rs:691-696
+void add_capacity(Csr* a, const double* capacity, double dt) {
+    for (size_t i = 0; i < a->n; ++i) {
+        size_t d;
+        if (!a->find(i, i, &d)) throw Error("a diagonal");
+        a->val[d] += capacity[i] / dt;
+    }
+}
+
+// heat.rs:535-547 with rad = 0 (the transient path of heat.rs:717-733 passes no radiation).
+void transient_energy(size_t n, const double* kt, const double* rate, const double* load,
+                      const uint8_t* fixed, double out[3]) {
+    double stored = 0.0, fix = 0.0, gross = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        stored += rate[i];
+        gross += std::fabs(rate[i]);
+        gross += 0.0;  // |rad[i]|
+        if (fixed[i]) {
+            double q = kt[i] + rate[i] - load[i] - 0.0;
+            fix += q;
+            gross += std::fabs(q);
+        }
+    }
+    out[0] = stored;
+    out[1] = fix;
+    out[2] = gross;
+}
+
 }  // namespace orc
+

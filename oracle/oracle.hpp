@@ -75,7 +75,14 @@ void tet_gradients(const Vec3 p[4], Vec3 g[4], double* volume);
 void tet_conduction(const Vec3 g[4], double v, const Vec3& k, double ke[16]);
 // heat.rs:1219-1244 (steady form: no transient term)
 vector<double> reduced_rhs(const Csr& a, const double* load, const double* t,
-                           const vector<size_t>& free);
+                           const vector<size_t>& free, const double* capacity = nullptr,
+                           double dt = 0.0);
+// heat.rs:691-696: a_full = K with capacity / dt added to each diagonal entry.
+void add_capacity(Csr* a, const double* capacity, double dt);
+// heat.rs:535-547 for a transient step with no radiation: out = {stored, fixed, the sum of
+// |rate| and |q| over the points}, each summed in point order.
+void transient_energy(size_t n, const double* kt, const double* rate, const double* load,
+                      const uint8_t* fixed, double out[3]);
 
 // hex.rs:120-124
 struct Stiffness {
