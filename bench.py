@@ -54,6 +54,8 @@ def args():
                         "kernel (0: none, the default)")
     p.add_argument("--launch", type=int, default=0,
                    help="0: programmatic dependent launch in the PCG loop (default), 1: plain")
+    p.add_argument("--lower", type=float, default=0.0,
+                   help="Chebyshev interval's lower end as a fraction of lambda_max (0: 0.3)")
     p.add_argument("--coarsest", type=int, default=0,
                    help="the largest level the dense coarse solve takes (0: 3000, the reference's)")
     p.add_argument("--values", type=int, default=0,
@@ -361,7 +363,8 @@ def run_ours(opt, rank, world, local):
                                          graph=opt.graph, tail=opt.tail,
                                          degree=opt.degree, launch=opt.launch,
                                          values=opt.values,
-                                         coarsest=opt.coarsest)).with_tol(tol)
+                                         coarsest=opt.coarsest,
+                                         lower=opt.lower)).with_tol(tol)
         return s, time.perf_counter() - t
 
     b = torch.from_numpy(rhs).cuda()
