@@ -58,6 +58,8 @@ def args():
                    help="Chebyshev interval's lower end as a fraction of lambda_max (0: 0.3)")
     p.add_argument("--coarsest", type=int, default=0,
                    help="the largest level the dense coarse solve takes (0: 3000, the reference's)")
+    p.add_argument("--tiles", type=int, default=0,
+                   help="finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on")
     p.add_argument("--values", type=int, default=0,
                    help="mixed form's stencil levels: 0 default, 1 FP32, 2 FP16 coefficients")
     p.add_argument("--degree", type=int, default=0,
@@ -362,7 +364,7 @@ def run_ours(opt, rank, world, local):
                       options=fg.Options(precision=precision, format=opt.format,
                                          graph=opt.graph, tail=opt.tail,
                                          degree=opt.degree, launch=opt.launch,
-                                         values=opt.values,
+                                         values=opt.values, tiles=opt.tiles,
                                          coarsest=opt.coarsest,
                                          lower=opt.lower)).with_tol(tol)
         return s, time.perf_counter() - t

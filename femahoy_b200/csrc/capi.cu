@@ -280,7 +280,9 @@ int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
             o.tail = options->tail;
             o.pdl = options->launch == 0 ? 1 : 0;
             o.values = options->values;
+            o.tiles = options->tiles;
         }
+        require(o.tiles >= 0 && o.tiles <= 2, "tiles is 0 (autotuned), 1 (off) or 2 (on)");
         require(o.values >= 0 && o.values <= 2, "values is 0 (default), 1 (FP32) or 2 (FP16)");
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,

@@ -134,6 +134,23 @@ static void launch(bool pdl, void (*kernel)(KArgs...), int grid, int block, cuda
     FG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
 }
 
+// The same with `smem` bytes of dynamic shared memory.
+template <typename... KArgs, typename... Args>
+static void launch_smem(bool pdl, void (*kernel)(KArgs...), int grid, int block, size_t smem,
+                        cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr{};
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? &attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    FG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
+
 // A scalar from device memory.
 template <class T>
 T fetch(const T* d, cudaStream_t s) {

@@ -2,8 +2,9 @@
 // stencil (a matrix whose entries sit at a few constant column offsets, as the operators of a
 // box grid in grid order do).
 //
-// Stencil layout: offsets 0 = o_0 < o_1 < ... < o_{K-1}; coef[k n + i] = a(i, i + o_k), 0 where
-// the matrix has no such entry. Row i is then
+// Stencil layout: offsets 0 = o_0 < o_1 < ... < o_{K-1}; coef[k ld + i] = a(i, i + o_k), 0 where
+// the matrix has no such entry (ld >= n: each offset's array starts on a 4 KB boundary, the
+// padding 0). Row i is then
 //   sum_k coef[k][i] x[i + o_k] + sum_{k >= 1} coef[k][i - o_k] x[i - o_k],
 // the lower entries taken from the rows above (the matrix is symmetric). The columns are
 // implicit: a row reads K coefficients of its own, K - 1 of earlier rows (recently read by
@@ -17,6 +18,14 @@ namespace femgpu {
 
 constexpr int MAXK = 32;
 
+// The rows of a stencil tile streamed into shared memory by the bulk-copy kernels, and the
+// stride of a stencil's coefficient arrays: n rounded up to whole tiles, so that every array and
+// tile starts on a 4 KB boundary and every tile is 1 full copy.
+constexpr int STENCIL_TILE = 1024;
+__host__ __device__ __forceinline__ int64_t stencil_ld(int64_t n) {
+    return (n + STENCIL_TILE - 1) / STENCIL_TILE * STENCIL_TILE;
+}
+
 // a b + c with 1 rounding, so that every product kernel below sums in the same way whatever
 // the compiler contracts.
 __device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
@@ -29,6 +38,7 @@ template <class T>
 struct StencilView {
     int n;
     int K;
+    int ld;
     int off[MAXK];
     const T* __restrict__ coef;
 };
@@ -53,7 +63,7 @@ __device__ __forceinline__ TA stencil_apply(const StencilView<T>& v, int i,
     TA acc = (TA)__ldg(c + i) * (TA)__ldg(x + i);
     for (int k = 1; k < v.K; ++k) {
         const int o = v.off[k];
-        const T* __restrict__ ck = c + (size_t)k * n;
+        const T* __restrict__ ck = c + (size_t)k * v.ld;
         const int j = i + o, m = i - o;
         if (j < n) acc = fmadd((TA)__ldg(ck + i), (TA)__ldg(x + j), acc);
         if (m >= 0) acc = fmadd((TA)__ldg(ck + m), (TA)__ldg(x + m), acc);
@@ -114,7 +124,7 @@ struct StencilOpK {
 #pragma unroll
         for (int k = 1; k < K; ++k) {
             const int o = v.off[k];
-            const T* __restrict__ ck = c + (size_t)k * n;
+            const T* __restrict__ ck = c + (size_t)k * v.ld;
             const int j = i + o, m = i - o;
             const bool up = j < n, lo = m >= 0;
             acc = fmadd(up ? (TA)__ldg(ck + i) : (TA)0, up ? (TA)__ldg(x + j) : (TA)0, acc);
@@ -134,6 +144,7 @@ struct StencilOpK {
 struct StencilViewH {
     int n;
     int K;
+    int ld;
     int off[MAXK];
     const __half* __restrict__ coef;
     float scale;
@@ -154,7 +165,7 @@ struct StencilOpH {
         for (int k = 1; k < (KC > 0 ? KC : MAXK); ++k) {
             if (KC == 0 && k >= K) break;
             const int o = v.off[k];
-            const __half* __restrict__ ck = c + (size_t)k * n;
+            const __half* __restrict__ ck = c + (size_t)k * v.ld;
             const int j = i + o, m = i - o;
             const bool up = j < n, lo = m >= 0;
             acc = fmadd(up ? (TA)__half2float(__ldg(ck + i)) : (TA)0,

@@ -144,18 +144,21 @@ static bool make_stencil(const HostCsr& h, Operator<T>* out, cudaStream_t s) {
     if (h.nnz() - upper != upper - diag) return false;
     int K = (int)offs.size();
     if ((double)K * n > 1.5 * (double)upper) return false;
-    std::vector<T> coef((size_t)K * n, (T)0);
+    const int64_t ld = stencil_ld(n);
+    if (ld + offs.back() >= (int64_t)0x7fffffff) return false;
+    std::vector<T> coef((size_t)K * ld, (T)0);
     for (int64_t i = 0; i < n; ++i)
         for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) {
             int64_t o = (int64_t)h.idx[k] - i;
             if (o < 0) continue;
             int slot = (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
-            coef[(size_t)slot * n + i] = (T)h.val[k];
+            coef[(size_t)slot * ld + i] = (T)h.val[k];
         }
     out->stencil = true;
     out->n = n;
     out->nnz = h.nnz();
     out->K = K;
+    out->ld = ld;
     out->off = offs;
     out->coef.upload(coef.data(), coef.size(), s);
     FG_CUDA(cudaStreamSynchronize(s));
@@ -403,6 +406,160 @@ __global__ void __launch_bounds__(TH)
     const int g = row_of_thread();
     if (g >= A.threads()) return;
     residual_row(A, g, b, x, r);
+}
+
+// ------------------------------------------------------------------ stencil tiles by bulk copy
+// The finest level's Chebyshev steps and residuals with the row-own arrays streamed into shared
+// memory. Each block of 1024 threads takes tiles of STENCIL_TILE rows, 1 row per thread. One
+// thread issues 1D bulk copies (cp.async.bulk, no multicast) of the tile's K coefficient
+// arrays, b, and for a step D^-1 and d, completing on an mbarrier; the next tile's copies run
+// while this tile computes (2 stages). The rows' x neighbours, and the coefficients of rows
+// above the tile, come from L1/L2 as in StencilOpK. The arithmetic is StencilOpK's and
+// cheb_step_row's / residual_row's in the same order on the same values, so the bits are those
+// of the kernels it replaces. A partial last tile reads global memory directly. Every wait on an
+// mbarrier has an iteration limit: on running out, the kernel sets *timeout, waits (bounded) for
+// its copies in flight and returns.
+constexpr int BULK_TH = STENCIL_TILE;
+constexpr unsigned BULK_SPIN = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(
+                     smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, unsigned bytes,
+                                          uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        "selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for phase `parity` of `bar`, at most BULK_SPIN polls: false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (unsigned k = 0; k < BULK_SPIN; ++k)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+template <int K, bool STEP>
+__global__ void __launch_bounds__(BULK_TH, 2)
+    k_stencil_tiles(StencilView<float> v, const float* __restrict__ b,
+                    const float* __restrict__ xin, const float* __restrict__ dinv, float c1,
+                    float c2, float* __restrict__ d, float* __restrict__ out,
+                    const int* __restrict__ done, int* __restrict__ timeout) {
+    constexpr int NA = K + (STEP ? 3 : 1);  // coefficients, b (, D^-1, d)
+    constexpr unsigned TILE_BYTES = STENCIL_TILE * sizeof(float);
+    extern __shared__ __align__(128) float tiles[];  // [2][NA][STENCIL_TILE]
+    __shared__ uint64_t bar[2];
+    pdl_wait();
+    if (*done) return;
+    const int n = v.n;
+    const int nfull = n / STENCIL_TILE;
+    const int ntiles = (n + STENCIL_TILE - 1) / STENCIL_TILE;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    auto issue = [&](int t, int s) {
+        float* base = tiles + (size_t)s * NA * STENCIL_TILE;
+        const size_t r0 = (size_t)t * STENCIL_TILE;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect(&bar[s], NA * TILE_BYTES);
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            bulk_copy(base + k * STENCIL_TILE, v.coef + (size_t)k * v.ld + r0, TILE_BYTES,
+                      &bar[s]);
+        bulk_copy(base + K * STENCIL_TILE, b + r0, TILE_BYTES, &bar[s]);
+        if (STEP) {
+            bulk_copy(base + (K + 1) * STENCIL_TILE, dinv + r0, TILE_BYTES, &bar[s]);
+            bulk_copy(base + (K + 2) * STENCIL_TILE, d + r0, TILE_BYTES, &bar[s]);
+        }
+    };
+    // pending[s]: stage s has copies issued and not yet waited for, completing phase parity[s].
+    int t = blockIdx.x;
+    if (threadIdx.x == 0 && t < nfull) issue(t, 0);
+    bool pending[2] = {t < nfull, false};
+    unsigned parity[2] = {0, 0};
+    int j = 0;
+    for (; t < ntiles; t += gridDim.x, ++j) {
+        const int s = j & 1;
+        const int tn = t + gridDim.x;
+        if (tn < nfull) {
+            if (threadIdx.x == 0) issue(tn, s ^ 1);
+            pending[s ^ 1] = true;
+            parity[s ^ 1] = ((j + 1) >> 1) & 1;
+        }
+        const int r0 = t * STENCIL_TILE;
+        const int i = r0 + threadIdx.x;
+        const bool full = t < nfull;
+        if (full) {
+            const bool ok = mbar_wait(&bar[s], (j >> 1) & 1);
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) atomicExch(timeout, 1);
+                break;
+            }
+            pending[s] = false;
+        }
+        const float* own = tiles + (size_t)s * NA * STENCIL_TILE;
+        if (i < n) {
+            const int li = threadIdx.x;
+            const float* __restrict__ c = v.coef;
+            // StencilOpK<float, K>::apply on the same values.
+            float acc = (full ? own[li] : __ldg(c + i)) * __ldg(xin + i);
+#pragma unroll
+            for (int k = 1; k < K; ++k) {
+                const int o = v.off[k];
+                const float* __restrict__ ck = c + (size_t)k * v.ld;
+                const int jj = i + o, m = i - o;
+                const bool up = jj < n, lo = m >= 0;
+                const float cu = up ? (full ? own[k * STENCIL_TILE + li] : __ldg(ck + i)) : 0.0f;
+                acc = fmadd(cu, up ? __ldg(xin + jj) : 0.0f, acc);
+                const float cl =
+                    lo ? ((full && m >= r0) ? own[k * STENCIL_TILE + (m - r0)] : __ldg(ck + m))
+                       : 0.0f;
+                acc = fmadd(cl, lo ? __ldg(xin + m) : 0.0f, acc);
+            }
+            const float bi = full ? own[K * STENCIL_TILE + li] : b[i];
+            if (STEP) {
+                const float di = full ? own[(K + 1) * STENCIL_TILE + li] : dinv[i];
+                const float dd0 = full ? own[(K + 2) * STENCIL_TILE + li] : d[i];
+                // cheb_step_row
+                float r = bi - acc;
+                float dd = c2 * dd0 + c1 * di * r;
+                d[i] = dd;
+                out[i] = xin[i] + dd;
+            } else {
+                out[i] = bi - acc;  // residual_row
+            }
+        }
+        __syncthreads();
+    }
+    // After a timeout: wait, again bounded, for the copies still in flight into this block's
+    // shared memory before the block exits.
+    if (threadIdx.x == 0)
+        for (int s = 0; s < 2; ++s)
+            if (pending[s]) mbar_wait(&bar[s], parity[s]);
 }
 
 // bc = P^T r as a gather over the rows of R = P^T (multigrid.rs:166, sparse.rs:223-230).
@@ -1147,6 +1304,71 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
     op->unrolled = op->probe_ms[1] < op->probe_ms[0];
 }
 
+// The launch of the tile kernels: persistent blocks, 2 per SM, 2 stages of NA tiles each.
+template <bool STEP>
+static size_t tile_smem() {
+    return 2 * (size_t)(8 + (STEP ? 3 : 1)) * STENCIL_TILE * sizeof(float);
+}
+static int tile_grid(int64_t n) {
+    int64_t tiles = (n + STENCIL_TILE - 1) / STENCIL_TILE;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, 2 * NUM_SMS));
+}
+static void tile_attributes() {
+    static bool done = false;
+    if (done) return;
+    FG_CUDA(cudaFuncSetAttribute(k_stencil_tiles<8, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_smem<true>()));
+    FG_CUDA(cudaFuncSetAttribute(k_stencil_tiles<8, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tile_smem<false>()));
+    done = true;
+}
+
+// Whether a finest FP32 stencil level (K = 8, large enough to fill the GPU with tiles) takes the
+// tile kernels: mode 2 yes, mode 1 no, mode 0 when its residual by tiles is faster than by the
+// kernel the autotuner chose (the same timing as tune_operator). A probe whose copies time out
+// keeps the direct kernels.
+static void tune_tiles(Operator<float>* op, int mode, cudaStream_t s) {
+    op->bulk = false;
+    if (mode == 1 || !op->stencil || op->half || op->K != 8) return;
+    int64_t n = op->n;
+    if (n < (int64_t)STENCIL_TILE * NUM_SMS) return;
+    tile_attributes();
+    DevBuf<float> x(n), b(n), r(n);
+    x.zero(s);
+    b.zero(s);
+    DevBuf<int> done(1), timeout(1);
+    done.zero(s);
+    timeout.zero(s);
+    const StencilView<float> v = op->sview();
+    auto probe = [&]() {
+        k_stencil_tiles<8, false><<<tile_grid(n), BULK_TH, tile_smem<false>(), s>>>(
+            v, b.p, x.p, nullptr, 0.f, 0.f, nullptr, r.p, done.p, timeout.p);
+    };
+    cudaEvent_t e0, e1;
+    FG_CUDA(cudaEventCreate(&e0));
+    FG_CUDA(cudaEventCreate(&e1));
+    for (int w = 0; w < 10; ++w) probe();
+    FG_CHECK_LAUNCH();
+    double best = 1e30;
+    for (int round = 0; round < 4; ++round) {
+        FG_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < 5; ++k) probe();
+        FG_CUDA(cudaEventRecord(e1, s));
+        FG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, (double)ms / 5);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    op->probe_ms[2] = best;
+    if (fetch(timeout.p, s)) return;
+    const double direct = op->unrolled ? op->probe_ms[1] : op->probe_ms[0];
+    op->bulk = mode == 2 || best < direct;
+}
+
 // lambda_max of D^-1 A by the power method in the D inner product (15 steps), on the device.
 template <class T>
 double lambda_max(const Operator<T>& A, const double* dg, cudaStream_t s,
@@ -1253,9 +1475,10 @@ static std::string describe_op(const Operator<T>& op) {
     } else if (!op.stencil) {
         std::snprintf(buf, sizeof buf, "sell C=%d nnz=%lld", op.sell.C, (long long)op.nnz);
     } else {
-        std::snprintf(buf, sizeof buf, "stencil K=%d %s%s (probe %.1f / %.1f us) nnz=%lld", op.K,
-                      op.half ? "fp16 " : "", op.unrolled ? "unrolled" : "loop",
-                      op.probe_ms[0] * 1e3, op.probe_ms[1] * 1e3, (long long)op.nnz);
+        std::snprintf(buf, sizeof buf, "stencil K=%d %s%s (probe %.1f / %.1f us)%s nnz=%lld",
+                      op.K, op.half ? "fp16 " : "", op.unrolled ? "unrolled" : "loop",
+                      op.probe_ms[0] * 1e3, op.probe_ms[1] * 1e3,
+                      op.bulk ? ", steps from bulk-copied tiles" : "", (long long)op.nnz);
     }
     return buf;
 }
@@ -1550,6 +1773,8 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
                 if (lv.A.stencil && (opt_.values == 2 || (opt_.values == 0 && kHalfDefault)))
                     make_half(&lv.A, s_);
             tune_operator(&lv.A, s_);
+            if constexpr (std::is_same<T, float>::value)
+                if (l == 0) tune_tiles(&lv.A, opt_.tiles, s_);
         }
         PhaseTimer t_lam{this, "diagonals and lambda_max", s_};
         // The diagonal and lambda_max(D^-1 A) in FP64.
@@ -1665,6 +1890,41 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
     }
 }
 
+// A Chebyshev step and the residual of level L: by tiles when the autotuner chose them.
+template <class T>
+void SolverImpl::enqueue_step(MgLevel<T>& L, const T* b, const T* xin, T c1, T c2, T* xout) {
+    const int* done = &sc_.p->done;
+    if constexpr (std::is_same<T, float>::value) {
+        if (L.A.bulk) {
+            launch_smem(pdl_, k_stencil_tiles<8, true>, tile_grid(L.n), BULK_TH,
+                        tile_smem<true>(), s_, L.A.sview(), b, xin, (const float*)L.dinv.p, c1,
+                        c2, L.d.p, xout, done, &sc_.p->bulk_timeout);
+            return;
+        }
+    }
+    with_op(L.A, [&](auto op) {
+        launch(pdl_, k_cheb_step<T, decltype(op)>, row_blocks(L.A.threads()), TH, s_, op, b,
+               xin, L.dinv.p, c1, c2, L.d.p, xout, done);
+    });
+}
+
+template <class T>
+void SolverImpl::enqueue_residual(MgLevel<T>& L, const T* b, const T* x) {
+    const int* done = &sc_.p->done;
+    if constexpr (std::is_same<T, float>::value) {
+        if (L.A.bulk) {
+            launch_smem(pdl_, k_stencil_tiles<8, false>, tile_grid(L.n), BULK_TH,
+                        tile_smem<false>(), s_, L.A.sview(), b, x, (const float*)nullptr, 0.f,
+                        0.f, (float*)nullptr, L.r.p, done, &sc_.p->bulk_timeout);
+            return;
+        }
+    }
+    with_op(L.A, [&](auto op) {
+        launch(pdl_, k_residual<T, decltype(op)>, row_blocks(L.A.threads()), TH, s_, op, b, x,
+               L.r.p, done);
+    });
+}
+
 template <class T>
 const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     const int* done = &sc_.p->done;
@@ -1705,7 +1965,6 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     MgLevel<T>& L = H.levels[l];
     int64_t n = L.n;
     const int gb = row_blocks(n);
-    const int gs = row_blocks(L.A.threads());
     T* xa = L.xa.p;
     T* xb = L.xb.p;
     int deg = (int)L.c1.size();
@@ -1713,16 +1972,11 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     launch(pdl_, k_cheb_first<T>, gb, TH, s_, n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
     mark(tag + "smooth (first, no product)");
     for (int k = 1; k < deg; ++k) {
-        with_op(L.A, [&](auto op) {
-            launch(pdl_, k_cheb_step<T, decltype(op)>, gs, TH, s_, op, b, xa, L.dinv.p,
-                   (T)L.c1[k], (T)L.c2[k], L.d.p, xb, done);
-        });
+        enqueue_step(L, b, xa, (T)L.c1[k], (T)L.c2[k], xb);
         mark(tag + "smooth pre");
         std::swap(xa, xb);
     }
-    with_op(L.A, [&](auto op) {
-        launch(pdl_, k_residual<T, decltype(op)>, gs, TH, s_, op, b, xa, L.r.p, done);
-    });
+    enqueue_residual(L, b, xa);
     mark(tag + "residual");
     T* bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
     if (L.Ro.ok)
@@ -1740,10 +1994,7 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
         launch(pdl_, k_prolong<T>, gb, TH, s_, n, L.pptr.p, L.pidx.p, L.pval.p, ec, xa, done);
     mark(tag + "prolong + correct");
     for (int k = 0; k < deg; ++k) {
-        with_op(L.A, [&](auto op) {
-            launch(pdl_, k_cheb_step<T, decltype(op)>, gs, TH, s_, op, b, xa, L.dinv.p,
-                   (T)L.c1[k], (T)L.c2[k], L.d.p, xb, done);
-        });
+        enqueue_step(L, b, xa, (T)L.c1[k], (T)L.c2[k], xb);
         mark(tag + "smooth post");
         std::swap(xa, xb);
     }
@@ -2057,6 +2308,13 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
     out.seconds = ms * 1e-3;
     out.launches = launches_;
     if (st) *st = out;
+    if (status == FEMGPU_OK && !H32_.levels.empty() && H32_.levels[0].A.bulk) {
+        // The Scalars were read back after the last kernel of the solve.
+        if (h_sc_->bulk_timeout) {
+            status = FEMGPU_ERR_TIMEOUT;
+            message = "a bulk copy of a stencil tile did not complete within its wait limit";
+        }
+    }
     if (status != FEMGPU_OK) throw Failure(status, message);
 }
 
@@ -2128,10 +2386,15 @@ void SolverImpl::kernel_time(int which, int reps, double* ms, double* bytes) {
         } else if (mixed) {
             MgLevel<float>& L = H32_.levels.at(0);
             int gs = row_blocks(L.A.threads());
-            with_op(L.A, [&](auto op) {
-                k_cheb_step<float><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5f, 0.5f,
-                                                      L.d.p, L.xb.p, done_zero_.p);
-            });
+            if (L.A.bulk)
+                k_stencil_tiles<8, true><<<tile_grid(L.n), BULK_TH, tile_smem<true>(), s_>>>(
+                    L.A.sview(), L.b.p, L.xa.p, L.dinv.p, 0.5f, 0.5f, L.d.p, L.xb.p,
+                    done_zero_.p, &sc_.p->bulk_timeout);
+            else
+                with_op(L.A, [&](auto op) {
+                    k_cheb_step<float><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5f,
+                                                          0.5f, L.d.p, L.xb.p, done_zero_.p);
+                });
         } else {
             MgLevel<double>& L = H64_.levels.at(0);
             int gs = row_blocks(L.A.threads());

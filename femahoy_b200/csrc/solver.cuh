@@ -37,10 +37,12 @@ struct Operator {
     bool block3 = false;  // the 3x3-block form (elasticity), else SELL-C, when not a stencil
     bool unrolled = false;  // the compile-time-K kernel (K = 8 or 14), chosen by timing
     bool half = false;      // the stencil's products read its FP16 copy (hcoef, hscale)
-    double probe_ms[2] = {0, 0};  // the timed product: runtime K, compile-time K
+    bool bulk = false;      // its smoothing steps and residuals stream tiles by bulk copies
+    double probe_ms[3] = {0, 0, 0};  // the timed product: runtime K, compile-time K, tiles
     int64_t n = 0, nnz = 0;
     Sell<T> sell;
     int K = 0;
+    int64_t ld = 0;  // the stride of each offset's coefficient array (stencil_ld(n))
     std::vector<int64_t> off;
     DevBuf<T> coef;
     DevBuf<__half> hcoef;
@@ -58,6 +60,7 @@ struct Operator {
         StencilView<T> v{};
         v.n = (int)n;
         v.K = K;
+        v.ld = (int)ld;
         for (int k = 0; k < K; ++k) v.off[k] = (int)off[k];
         v.coef = coef.p;
         return v;
@@ -66,6 +69,7 @@ struct Operator {
         StencilViewH v{};
         v.n = (int)n;
         v.K = K;
+        v.ld = (int)ld;
         for (int k = 0; k < K; ++k) v.off[k] = (int)off[k];
         v.coef = hcoef.p;
         v.scale = hscale;
@@ -105,6 +109,7 @@ void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
 struct Scalars {
     double bb, rr, rz, pq, alpha, beta, zq, norm_b;
     int done, iters, status, max_iter;
+    int bulk_timeout;  // a bulk-copy wait of the stencil tile kernels ran out of its limit
 };
 
 // A transfer (P or R = P^T) of a box grid in grid order: the entries of row i sit at K
@@ -206,6 +211,7 @@ struct Options {
     int tail = 0;  // levels of at most this many rows run fused (<= 0: none)
     int pdl = 1;   // programmatic dependent launch between the iteration's kernels
     int values = 0;  // mixed form's stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
+    int tiles = 0;   // finest FP32 stencil steps by bulk-copied tiles: 0 tuned, 1 off, 2 on
 };
 
 class SolverImpl {
@@ -241,6 +247,10 @@ class SolverImpl {
     void build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps, Hierarchy<T>* H);
     template <class T>
     const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b);
+    template <class T>
+    void enqueue_step(MgLevel<T>& L, const T* b, const T* xin, T c1, T c2, T* xout);
+    template <class T>
+    void enqueue_residual(MgLevel<T>& L, const T* b, const T* x);
     void enqueue_iteration();
     void build_loop_graph();
     // Runs PCG iterations on the device until convergence, max_iter, a NaN or a cancel.

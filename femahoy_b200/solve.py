@@ -113,11 +113,12 @@ class Options:
     tail: int = 0    # > 0: levels of at most this many rows run as 1 fused kernel (0: none)
     launch: int = 0  # 0: programmatic dependent launch in the PCG loop; 1: plain launches
     values: int = 0  # mixed stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
+    tiles: int = 0   # finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on
 
     def _c(self):
         return L.Options_t(self.precision, self.degree, self.lower, self.sell_c, 0, self.coarsest,
                            self.max_levels, self.graph, self.format, self.tail, self.launch,
-                           self.values)
+                           self.values, self.tiles)
 
 
 def unknowns_c(unknowns: "Unknowns", keep: list) -> L.Unknowns_t:

@@ -211,6 +211,10 @@ typedef struct femgpu_options {
                              coefficients, 2 = FP16 coefficients scaled by the level's largest
                              (the products read about 0.6 of the bytes; the V-cycle changes by
                              about 2^-11 relative) */
+    int tiles;            /* the mixed form's finest stencil level (K = 8): 0 = the autotuner
+                             chooses by timing whether its smoothing steps and residuals stream
+                             each tile's own arrays into shared memory by bulk copies or read
+                             them directly; 1 = directly; 2 = bulk copies (the same bits) */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end

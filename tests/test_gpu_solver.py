@@ -254,6 +254,27 @@ def test_programmatic_launches_give_the_same_bits(precision):
     assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
 
 
+@pytest.mark.parametrize("precision", [fg.MIXED])
+def test_tile_kernels_give_the_same_bits(precision):
+    """The finest FP32 stencil steps and residuals with each tile's own arrays brought into
+    shared memory by bulk copies compute what the direct kernels compute, bit for bit (a level of
+    180,000 rows: enough tiles to fill the GPU)."""
+    h = mg.heat_cube(56, seed=5)
+    A, rhs, _ = _system(h)
+    xs, its = [], []
+    for tiles in (1, 2):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision,
+                      options=fg.Options(precision=precision, tiles=tiles)).with_tol(1e-10)
+        assert ("bulk-copied tiles" in s.describe()) == (tiles == 2)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1e-10
+        xs.append(x)
+        its.append(st.iterations)
+    assert its[0] == its[1]
+    assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
+
+
 def test_fp16_stencil_coefficients_solve_to_the_same_tolerance():
     """The mixed form with the stencil levels' coefficients in FP16 (scaled by each level's
     largest): the V-cycle changes by about 2^-11 relative, and flexible CG still reaches the
