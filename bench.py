@@ -418,7 +418,7 @@ def run_ours(opt, rank, world, local):
     clocks = Clocks(torch.cuda.current_device())
     ms, lat, its, launches, res, clk = timed(mixed, opt.steps, opt.warmup, clocks)
     ms_max = max_over_ranks(ms)
-    value = world * n_free * opt.steps / (ms_max / 1e3)
+    value = replica_value(world, n_free, opt.steps, ms_max)
     if opt.profile:
         if rank == 0:
             print(json.dumps({"profile": True, "value": value, "unit": UNIT,
@@ -457,7 +457,7 @@ def run_ours(opt, rank, world, local):
     e1.record(stream)
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * n_free * opt.steps / (e2e_ms / 1e3)
+    e2e_value = replica_value(world, n_free, opt.steps, e2e_ms)
     mixed_bytes = mixed.device_bytes()
     levels = mixed.levels()
     del mixed
@@ -466,7 +466,7 @@ def run_ours(opt, rank, world, local):
     plain, setup_fp64 = make(fg.FP64)
     ms64, lat64, its64, _, res64, _ = timed(plain, opt.steps, opt.warmup)
     ms64 = max_over_ranks(ms64)
-    value64 = world * n_free * opt.steps / (ms64 / 1e3)
+    value64 = replica_value(world, n_free, opt.steps, ms64)
     del plain
 
     cpu = None
@@ -925,27 +925,35 @@ def run_serve(opt, rank, world, local):
         dist.destroy_process_group()
 
 
-def _plumbing(world):
+def _plumbing(world, backend="nccl"):
     """The process group (N > 1), a barrier that also synchronizes the device, and the max over
-    ranks of a number."""
+    ranks of a number. The path does not shard: the N ranks are independent replicas, and these
+    are the only collectives (gloo runs the same steps on the host, for the CPU tests)."""
     import torch
     import torch.distributed as dist
     if world > 1 and not dist.is_initialized():
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    on_gpu = backend == "nccl"
 
     def barrier():
         if world > 1:
             dist.barrier()
-        torch.cuda.synchronize()
+        if on_gpu:
+            torch.cuda.synchronize()
 
     def max_over_ranks(v):
         if world == 1:
             return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device="cuda" if on_gpu else "cpu")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
     return dist, barrier, max_over_ranks
+
+
+def replica_value(world, units, steps, ms_max):
+    """The whole-job figure of N replicas: all ranks' units over the slowest rank's time."""
+    return world * units * steps / (ms_max / 1e3)
 
 
 # ------------------------------------------------------------------ the transient workload
