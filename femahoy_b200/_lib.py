@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libfemgpu.so")
 OK, CANCELLED, NOT_CONVERGED, NOT_SPD, NEEDS_GRID, INVALID, CUDA, TOO_LARGE, PATTERN, MATERIAL, \
     TIMEOUT = range(11)
 
-P1_HEAT, P1_ELASTIC, P2_ELASTIC = 0, 1, 2
+P1_HEAT, P1_ELASTIC, P2_ELASTIC, P2_MASS = 0, 1, 2, 3
 GATHER, COLOUR = 0, 1
 FP64, MIXED = 0, 1
 
@@ -73,6 +73,11 @@ class Stats_t(C.Structure):
 
 class Energy_t(C.Structure):
     _fields_ = [("stored", C.c_double), ("fixed", C.c_double), ("gross", C.c_double)]
+
+
+class ModesStats_t(C.Structure):
+    _fields_ = [("iterations", C.c_size_t), ("solves", C.c_size_t),
+                ("pcg_iterations", C.c_size_t), ("shift", C.c_double), ("seconds", C.c_double)]
 
 
 class Peak_t(C.Structure):
@@ -162,6 +167,12 @@ SIGNATURES = {
     "femgpu_batch_bytes": (C.c_size_t, [C.c_void_p]),
     "femgpu_batch_stream": (C.c_void_p, [C.c_void_p]),
     "femgpu_batch_free": (None, [C.c_void_p]),
+    "femgpu_modes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_double,
+                               C.POINTER(Unknowns_t), C.c_int, C.POINTER(Crossover_t),
+                               C.POINTER(Options_t), C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.POINTER(ModesStats_t)]),
+    "femgpu_dense_generalized": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                           C.c_void_p]),
     "femgpu_transient_new": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
                                        C.c_size_t, C.POINTER(Unknowns_t), C.c_int,
                                        C.POINTER(Crossover_t), C.POINTER(Options_t),

@@ -3,8 +3,8 @@
     python -m femahoy_b200.build
 
 Each translation unit is compiled to an object under femahoy_b200/_build/ and linked with nvcc
-into femahoy_b200/libfemgpu.so. assemble.cu, noalloc.cu, recover.cu and transient.cu are
-compiled with -fmad=false so that the element arithmetic keeps the reference's separate roundings;
+into femahoy_b200/libfemgpu.so. assemble.cu, noalloc.cu, recover.cu, transient.cu and modes.cu
+are compiled with -fmad=false so that the element arithmetic keeps the reference's separate roundings;
 hierarchy.cpp with -ffp-contract=off for the same reason.
 """
 from __future__ import annotations
@@ -35,8 +35,10 @@ UNITS = [
     ("batch.cu", []),
     ("recover.cu", ["-fmad=false"]),
     ("transient.cu", ["-fmad=false"]),
+    ("modes.cu", ["-fmad=false"]),
 ]
-CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"])]
+CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
+             ("dense_eigen.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"])]
 
 
 def _nvcc():

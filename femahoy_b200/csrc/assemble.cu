@@ -311,7 +311,23 @@ struct ElasticShared {
     int pos[NN];
 };
 
-template <int NN, int WARPS>
+// tet10.rs:181-205: the scalar of the consistent mass of points i and j, in units of V / 420.
+__device__ __forceinline__ double tet10_mass_scalar(int i, int j) {
+    if (i < 4 && j < 4) return i == j ? 6.0 : 1.0;
+    if (i < 4 || j < 4) {
+        const int c = i < 4 ? i : j, e = i < 4 ? j - 4 : i - 4;
+        return (kEdges[e][0] == c || kEdges[e][1] == c) ? -4.0 : -6.0;
+    }
+    const int a0 = kEdges[i - 4][0], a1 = kEdges[i - 4][1];
+    const int b0 = kEdges[j - 4][0], b1 = kEdges[j - 4][1];
+    const int shared = (a0 == b0 || a0 == b1) + (a1 == b0 || a1 == b1);
+    return shared == 2 ? 32.0 : (shared == 1 ? 16.0 : 8.0);
+}
+
+// MASS: the consistent mass of the 10-node tetrahedron (tet10.rs:173-212) with the density
+// coef[e], in place of the stiffness: entry (3i + a, 3j + b) = density V / 420 scalar(i, j) for
+// a = b, 0 else.
+template <int NN, int WARPS, bool MASS = false>
 __global__ void __launch_bounds__(32 * WARPS)
     k_gather_elastic(const double* __restrict__ xyz, const uint32_t* __restrict__ el,
                      const double* __restrict__ coef, const int64_t* __restrict__ start,
@@ -349,10 +365,12 @@ __global__ void __launch_bounds__(32 * WARPS)
             load_corners(xyz, nodes, p);
             tet_gradients(p, g, &vol);
             Stiffness D;
-            if (!isotropic_stiffness(coef[2 * (int64_t)e], coef[2 * (int64_t)e + 1], &D)) {
+            if (!MASS &&
+                !isotropic_stiffness(coef[2 * (int64_t)e], coef[2 * (int64_t)e + 1], &D)) {
                 if (lane == 0) atomicExch(bad, 2);
             }
-            if (NQ == 4) {
+            if (MASS) {
+            } else if (NQ == 4) {
                 if (lane < 4) {
                     double tab[10][3];
                     tet10_gradients(g, lane, tab);
@@ -369,13 +387,19 @@ __global__ void __launch_bounds__(32 * WARPS)
             while (an < NN && nodes[an] != (uint32_t)v) ++an;
             __syncwarp();
             double wq = NQ == 4 ? vol / 4.0 : vol;
+            const double wm = MASS ? coef[e] * vol / 420.0 : 0.0;
             for (int o = lane; o < OUT; o += 32) {
                 int a = o / (3 * NN);
                 int rem = o % (3 * NN);
                 int j = rem / 3, b = rem % 3;
                 double k = 0.0;
+                if (MASS) {
+                    k = a == b ? wm * tet10_mass_scalar(an, j) : 0.0;
+                } else {
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) k += wq * elastic_term(S.gr[q][an], S.gr[q][j], a, b, D);
+                    for (int q = 0; q < NQ; ++q)
+                        k += wq * elastic_term(S.gr[q][an], S.gr[q][j], a, b, D);
+                }
                 buf[a * rowlen + 3 * S.pos[j] + b] += k;
             }
             __syncwarp();
@@ -599,9 +623,11 @@ __global__ void k_colour_fill(const uint32_t* __restrict__ colour, int64_t nel,
 // ------------------------------------------------------------------ assemble
 void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t nel,
               const uint32_t* d_el, const double* d_coef, Assembled* out, cudaStream_t s) {
-    if (kind < 0 || kind > 2) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
+    if (kind < 0 || kind > 3) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
     if (mode < 0 || mode > 1) throw Failure(FEMGPU_ERR_INVALID, "unknown assembly mode");
-    int nn = kind == FEMGPU_P2_ELASTIC ? 10 : 4;
+    if (kind == FEMGPU_P2_MASS && mode != FEMGPU_ASSEMBLE_GATHER)
+        throw Failure(FEMGPU_ERR_INVALID, "the mass assembles by rows (FEMGPU_ASSEMBLE_GATHER)");
+    int nn = kind >= FEMGPU_P2_ELASTIC ? 10 : 4;
     if (npoints >= 0xffffffffLL / 3)
         throw Failure(FEMGPU_ERR_TOO_LARGE, "more points than 32-bit unknown numbers hold");
     build_incidence(d_el, nel, nn, npoints, &out->inc, s);
@@ -627,6 +653,10 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
                 K.idx.p, K.val.p, bad.p);
         } else if (kind == FEMGPU_P1_ELASTIC) {
             k_gather_elastic<4, 4><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
+                d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints,
+                out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
+        } else if (kind == FEMGPU_P2_MASS) {
+            k_gather_elastic<10, 4, true><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
                 d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints,
                 out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
         } else {

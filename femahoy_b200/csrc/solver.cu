@@ -2166,14 +2166,14 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         launches_ = 8;
         // solve.rs:206-218: x = A^-1 b (with 1 step of refinement in FP64), then the true
         // residual.
-        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, b_.p, x_.p,
-                                                              done_zero_.p);
+        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, b_.p,
+                                                                     x_.p, done_zero_.p);
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
             SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p, nullptr, partial_.p);
         k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                    FinResidual0{sc_.p});
-        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, r_.p, t_.p,
-                                                              done_zero_.p);
+        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, r_.p,
+                                                                     t_.p, done_zero_.p);
         k_add<<<blocks_for(n, TH), TH, 0, s_>>>(n, t_.p, x_.p);
         FG_CHECK_LAUNCH();
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(

@@ -52,8 +52,9 @@ class Csr:
     def assemble(cls, kind, points, nodes, coef, mode=L.GATHER):
         """Csr::pattern + Csr::add_element over every element on the device. ``kind``:
         femahoy_b200.P1_HEAT (``coef`` (T, 3) conductivities), P1_ELASTIC or P2_ELASTIC
-        (``coef`` (T, 2) E and nu; unknown 3 node + component). ``mode`` GATHER gives the
-        reference's values bit for bit; COLOUR scatters colour by colour."""
+        (``coef`` (T, 2) E and nu; unknown 3 node + component), P2_MASS (``coef`` (T,) the
+        density). ``mode`` GATHER gives the reference's values bit for bit; COLOUR scatters
+        colour by colour (not for the mass)."""
         x = L.arr(points, np.float64)
         e = L.arr(nodes, np.uint32)
         c = L.arr(coef, np.float64)

@@ -41,7 +41,9 @@ enum {
 enum {
     FEMGPU_P1_HEAT = 0,    /* 4-node tet, 4 x 4 conduction V G^T K G (heat.rs:972-1002) */
     FEMGPU_P1_ELASTIC = 1, /* 4-node tet, 12 x 12 V B^T D B (this library's own element) */
-    FEMGPU_P2_ELASTIC = 2  /* 10-node tet, 30 x 30, 4-point rule (tet10.rs:90-120) */
+    FEMGPU_P2_ELASTIC = 2, /* 10-node tet, 30 x 30, 4-point rule (tet10.rs:90-120) */
+    FEMGPU_P2_MASS = 3     /* 10-node tet consistent mass, 30 x 30 (tet10.rs:173-212), coef = the
+                              density per element, as modes.rs:470-476; gather mode only */
 };
 
 /* Assembly modes. */
@@ -396,6 +398,40 @@ int femgpu_transient_run(femgpu_transient* t, size_t steps, const double* load,
                          femgpu_energy* energies, const volatile int* cancel,
                          femgpu_stats* stats);
 void femgpu_transient_free(femgpu_transient* t);
+
+/* ---------------------------------------------------------------- modes */
+
+/* The lowest eigenpairs of K x = lambda M x of an elastic model by shift-invert subspace
+ * iteration with Rayleigh-Ritz (eigen.rs:81-177) as modes.rs:180-216 runs it: K - shift M is
+ * formed on the device and solved by this library's solver (the dense factor or PCG with
+ * multigrid, resident for all the solves); the p = max(2 count, count + 8) subspace vectors and
+ * their images stay on the device; the p x p Rayleigh-Ritz problem is solved on the host
+ * (femgpu_dense_generalized). */
+typedef struct femgpu_modes_stats {
+    size_t iterations;      /* subspace iterations */
+    size_t solves;          /* solves of (K - shift M) x = M y */
+    size_t pcg_iterations;  /* summed over the solves (0 with the direct method) */
+    double shift;           /* the shift used */
+    double seconds;         /* device time of the solves */
+} femgpu_modes_stats;
+
+/* eigen.rs:81-177. `k` and `m` are the free-unknown submatrices of the stiffness and the mass
+ * (the same pattern, as modes.rs:183-185 forms them; femgpu_assemble with FEMGPU_P2_ELASTIC and
+ * FEMGPU_P2_MASS, then femgpu_csr_submatrix); `shift` NaN takes modes.rs:186-191's
+ * -1e-8 mean(K_ii / M_ii). `unknowns`, `method`, `crossover` (NULL: Unknowns(16384)) and
+ * `options` are those of femgpu_solver_new for K - shift M. `values` gets `count` eigenvalues
+ * ascending, `vectors` (NULL skips them) count x n M-orthonormal vectors. At most 64 modes; the
+ * reference's texts for too many modes, non-convergence in 120 iterations and "cancelled"
+ * (between iterations and between PCG iterations). Host pointers. */
+int femgpu_modes(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
+                 const femgpu_unknowns* unknowns, int method, const femgpu_crossover* crossover,
+                 const femgpu_options* options, const volatile int* cancel, double* values,
+                 double* vectors, femgpu_modes_stats* stats);
+/* eigen.rs:183-269 on the host: K q = lambda M q for dense symmetric row-major n x n matrices,
+ * M positive definite, n <= 4096; the eigenvalues ascending and the vectors as the columns of
+ * q with Q^T M Q = I (the cyclic Jacobi method of eigen.rs:274-331 inside). No device use. */
+int femgpu_dense_generalized(const double* k, const double* m, size_t n, double* values,
+                             double* q);
 
 /* ---------------------------------------------------------------- post-solve recovery */
 

@@ -71,6 +71,8 @@ def _load():
         "orc_solver_precondition": (None, [P, P, P]),
         "orc_recover": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
         "orc_add_capacity": (I, [P, P, D, P, S]),
+        "orc_dense_generalized": (I, [P, P, I, P, P, P, S]),
+        "orc_dense_jacobi": (None, [P, I, P, P]),
         "orc_reduced_rhs_transient": (None, [P, P, P, P, S, P, D, P]),
         "orc_transient_energy": (None, [S, P, P, P, P, P]),
     }
@@ -214,7 +216,7 @@ def tet_gradients(p):
 def element_matrix(kind, p, coef):
     p = np.ascontiguousarray(p, dtype=np.float64).reshape(12)
     coef = np.ascontiguousarray(coef, dtype=np.float64)
-    m = {0: 4, 1: 12, 2: 30}[kind]
+    m = {0: 4, 1: 12, 2: 30, 3: 30}[kind]
     ke = np.empty(m * m)
     _lib.orc_element_matrix(kind, _p(p), _p(coef), _p(ke))
     return ke.reshape(m, m)
@@ -485,4 +487,85 @@ def transient(k, capacity, dt, free, load, t0, steps, make_solver, output_every=
             frames.append(t.copy())
             energies.append(transient_energy(kt, rate, load, fixed))
     return frames, energies, iterations
+
+
+def dense_jacobi(a):
+    """eigen.rs:274-331: (ascending eigenvalues, eigenvectors as columns) of a symmetric matrix."""
+    a = np.array(a, dtype=np.float64, copy=True)
+    n = a.shape[0]
+    values, v = np.empty(n), np.empty((n, n))
+    _lib.orc_dense_jacobi(_p(a), n, _p(values), _p(v))
+    return values, v
+
+
+def dense_generalized(k, m):
+    """eigen.rs:183-269: K q = lambda M q, ascending, with Q^T M Q = I."""
+    k = np.ascontiguousarray(k, dtype=np.float64)
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    n = k.shape[0]
+    values, q = np.empty(n), np.empty((n, n))
+    err = C.create_string_buffer(512)
+    if _lib.orc_dense_generalized(_p(k), _p(m), n, _p(values), _p(q), err, 512):
+        raise OracleError(err.value.decode())
+    return values, q
+
+
+EIGEN_TOL = 1e-6   # eigen.rs:34
+EIGEN_MAX_ITER = 120  # eigen.rs:40
+MODES_SHIFT = 1e-8  # modes.rs:93
+
+
+def subspace_vectors(n, count):
+    """eigen.rs:48-50"""
+    return min(max(2 * count, count + 8), n)
+
+
+def start_vectors(mdiag, p):
+    """eigen.rs:96-113: the diagonal of M, then xorshift vectors (seed 0x9e3779b97f4a7c15)."""
+    n = len(mdiag)
+    x = np.empty((p, n))
+    x[0] = mdiag
+    seed = 0x9E3779B97F4A7C15
+    mask = (1 << 64) - 1
+    for j in range(1, p):
+        for i in range(n):
+            seed ^= (seed << 13) & mask
+            seed ^= seed >> 7
+            seed ^= (seed << 17) & mask
+            x[j, i] = (seed >> 11) / float(1 << 53) - 0.5
+    return x
+
+
+def subspace(k, m, shift, count, solve):
+    """eigen.rs:81-177 with ``k``, ``m`` oracle Csr and ``solve(b, x0) -> x`` the solve of
+    (K - shift M) x = b from the start value x0. Returns (values, vectors (count, n),
+    iterations)."""
+    n = k.n
+    if count == 0 or count > n:
+        raise OracleError(f"the model has {n} unknowns, so it has 1 to {n} modes, not {count}")
+    p = subspace_vectors(n, count)
+    ptr, idx, val = m.arrays()
+    mdiag = np.zeros(n)
+    for i in range(n):
+        for e in range(ptr[i], ptr[i + 1]):
+            if idx[e] == i:
+                mdiag[i] = val[e]
+    x = start_vectors(mdiag, p)
+    mu = None
+    for iteration in range(1, EIGEN_MAX_ITER + 1):
+        y = np.stack([m.mul(x[j]) for j in range(p)])
+        bar = np.stack([solve(y[j], x[j] / mu[j] if mu is not None else np.zeros(n))
+                        for j in range(p)])
+        mb = np.stack([m.mul(bar[j]) for j in range(p)])
+        kr = 0.5 * (bar @ y.T + (bar @ y.T).T)
+        mr = bar @ mb.T  # eigen.rs:140-146 forms i <= j and mirrors it
+        mr = np.triu(mr) + np.triu(mr, 1).T
+        converged = iteration > 1 and all(
+            np.sqrt(max(1.0 - kr[i, i] ** 2 / mr[i, i], 0.0)) <= EIGEN_TOL for i in range(count))
+        mu, q = dense_generalized(kr, mr)
+        x = q.T @ bar
+        if converged:
+            return mu[:count] + shift, x[:count], iteration
+    raise OracleError(f"the subspace iteration did not converge in {EIGEN_MAX_ITER} iterations:"
+                      " ask for fewer modes")
 

@@ -129,6 +129,10 @@ int orc_element_matrix(int kind, const double* p12, const double* coef, double* 
         tet_conduction(g, v, Vec3{coef[0], coef[1], coef[2]}, ke);
         return 0;
     }
+    if (kind == 3) {
+        tet10_mass(v, coef[0], ke);
+        return 0;
+    }
     Stiffness d = isotropic_stiffness(coef[0], coef[1]);
     if (kind == 1)
         tet4_stiffness(g, v, d, ke);
@@ -137,15 +141,31 @@ int orc_element_matrix(int kind, const double* p12, const double* coef, double* 
     return 0;
 }
 
+// eigen.rs:183-269 (row-major n x n); -1 and the reference's text on failure.
+int orc_dense_generalized(const double* k, const double* m, int n, double* values, double* q,
+                          char* err, size_t len) {
+    std::string e;
+    if (!dense_generalized(k, m, n, values, q, &e)) {
+        put_error(err, len, e.c_str());
+        return -1;
+    }
+    return 0;
+}
+// eigen.rs:274-331; `a` is overwritten.
+void orc_dense_jacobi(double* a, int n, double* values, double* v) {
+    dense_jacobi(a, n, values, v);
+}
+
 // Assemble all the elements of a mesh into the pattern `h`, in increasing element order
-// (heat.rs:920-927, elastic_tet.rs:183-193). kind as orc_element_matrix; `nodes` are 4 corners
-// (kind 0, 1) or 10 points (kind 2) per element; `coef` has 3 (kind 0) or 2 values per element.
+// (heat.rs:920-927, elastic_tet.rs:183-193, modes.rs:470-476). kind as orc_element_matrix;
+// `nodes` are 4 corners (kind 0, 1) or 10 points (kind 2, 3) per element; `coef` has 3 (kind 0),
+// 2 (kinds 1, 2) or 1 (kind 3: the density) values per element.
 // The scalar nodes of kinds 1 and 2 become the unknowns 3 node + component.
 int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, size_t nel,
                  const double* coef, char* err, size_t len) {
     try {
         Csr* a = C(h);
-        int mn = kind == 2 ? 10 : 4;
+        int mn = kind >= 2 ? 10 : 4;
         int m = kind == 0 ? 4 : 3 * mn;
         vector<double> ke(m * m);
         vector<uint32_t> dofs(m);
@@ -161,11 +181,15 @@ int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, si
                 a->add_element(t, 4, ke.data());
                 continue;
             }
-            Stiffness d = isotropic_stiffness(coef[2 * e], coef[2 * e + 1]);
-            if (kind == 1)
-                tet4_stiffness(g, v, d, ke.data());
-            else
-                tet10_stiffness(g, v, d, ke.data());
+            if (kind == 3) {
+                tet10_mass(v, coef[e], ke.data());  // modes.rs:475: the density per element
+            } else {
+                Stiffness d = isotropic_stiffness(coef[2 * e], coef[2 * e + 1]);
+                if (kind == 1)
+                    tet4_stiffness(g, v, d, ke.data());
+                else
+                    tet10_stiffness(g, v, d, ke.data());
+            }
             for (int k = 0; k < m; ++k) dofs[k] = 3 * t[k / 3] + (uint32_t)(k % 3);
             a->add_element(dofs.data(), m, ke.data());
         }

@@ -99,6 +99,15 @@ void tet10_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double 
 // constant gradients of tet_gradients, in the index layout and term order of tet10.rs:99-113.
 void tet4_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k[144]);
 
+// tet10.rs:173-212
+void tet10_mass(double volume, double density, double m[900]);
+
+// eigen.rs:183-269 and 274-331: the dense generalized and standard symmetric eigenproblems.
+// Returns false with `err` set when M is not positive definite.
+bool dense_generalized(const double* k, const double* m, int n, double* values, double* q,
+                       std::string* err);
+void dense_jacobi(double* a, int n, double* values, double* v);
+
 // tet10.rs:232-272
 struct Quadratic {
     vector<Vec3> points;
