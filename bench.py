@@ -69,13 +69,14 @@ def args():
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
                    choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover",
-                            "transient"],
+                            "transient", "modes"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
                         "serve: a Poisson stream of solve requests through the server; "
                         "recover: the stress recovery of the solved 200x20x20 P2 beam; "
-                        "transient: backward-Euler steps of the 128^3 heat cube")
+                        "transient: backward-Euler steps of the 128^3 heat cube; "
+                        "modes: 10 lowest modes of a 100x10x10 P2 beam")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -1041,6 +1042,95 @@ def run_transient(opt, rank, world, local):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ the modes workload
+MODES_METRIC = "modes analyses/s (10 lowest modes, shift-invert subspace iteration)"
+
+
+def run_modes(opt, rank, world, local):
+    """The 10 lowest modes of the 100x10x10 P2 beam (200x20x20 mm, aluminium: E 70 GPa, nu 0.33,
+    density 2.7e-9 t/mm^3, clamped at x = 0): K and M assembled on the device, K - shift M solved
+    by p-multigrid PCG (mixed) 20 times per subspace iteration (p = 20). A step is 1 whole
+    analysis. The CPU baseline solves 1 system of the oracle (the reference's p-multigrid PCG) and
+    scales it by the device analysis's solve count, an estimate that leaves out the oracle's
+    projections."""
+    import torch
+    import femahoy_b200 as fg
+    from femahoy_b200 import meshgen as mg
+    from femahoy_b200.modes import modes
+    torch.cuda.set_device(local)
+    dist, barrier, max_over_ranks = _plumbing(world)
+    box = mg.box(100, 10, 10, (200.0, 20.0, 20.0))
+    q = fg.Quadratic.new(box.points, box.tets)
+    prob = mg.beam_p2(q.edges, q.tets, mesh=box, seed=SEED)
+    density = np.full(len(q.tets), 2.7e-9)
+    free = prob.free
+    t0 = time.perf_counter()
+    Kf = fg.Csr.assemble(fg.P2_ELASTIC, prob.xyz, prob.nodes, prob.coef).submatrix(free)
+    Mf = fg.Csr.assemble(fg.P2_MASS, prob.xyz, prob.nodes, density).submatrix(free)
+    P, coarse = fg.prolongation(prob.xyz, box.n, q.edges, free)
+    u = fg.Unknowns.Quadratic(prob.xyz[free // 3], P, coarse)
+    assemble_s = time.perf_counter() - t0
+    opts = fg.Options(precision=fg.MIXED)
+    for _ in range(max(1, opt.warmup)):
+        values, _, st = modes(Kf, Mf, 10, u, fg.Method.Multigrid, options=opts, vectors=False)
+    barrier()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(opt.steps):
+        values, _, st = modes(Kf, Mf, 10, u, fg.Method.Multigrid, options=opts, vectors=False)
+    torch.cuda.synchronize()
+    wall = max_over_ranks(time.perf_counter() - t0)
+    clk = clocks.stop()
+    value = world * opt.steps / wall
+    cpu = None
+    if rank == 0 and world == 1 and not opt.no_cpu_baseline:
+        import oracle
+        Ko = oracle.Csr.from_arrays(Kf.n, *Kf.arrays())
+        Mo = oracle.Csr.from_arrays(Mf.n, *Mf.arrays())
+        ptr, idx, val = Ko.arrays()
+        Ao = oracle.Csr.from_arrays(Ko.n, ptr, idx, val - st.shift * Mo.arrays()[2])
+        Po = oracle.Rect.from_arrays(P.rows, P.cols, P.ptr, P.idx, P.val)
+        so = oracle.Solver(Ao, "quadratic", xyz=prob.xyz[free // 3], p=Po, coarse=coarse,
+                           method="multigrid")
+        y = Mo.mul(np.random.default_rng(1).standard_normal(Ko.n))
+        t1 = time.perf_counter()
+        _, its, _ = so.solve(y, tol=1e-10)
+        one = time.perf_counter() - t1
+        cpu = {"value": 1.0 / (one * st.solves), "unit": "analyses/s", "cores": 1,
+               "kind": "port",
+               "sample": f"1 solve of K - shift M by the oracle (the reference's p-multigrid PCG, "
+                         f"{its} iterations, {one:.1f} s) times the device analysis's "
+                         f"{st.solves} solves"}
+    line = {
+        "metric": MODES_METRIC, "value": value, "unit": "analyses/s", "n_gpus": world,
+        "steps": opt.steps, "warmup": opt.warmup, "ms_per_step": 1e3 * wall / opt.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
+        "config": {"workload": "10 lowest modes of the 100x10x10 P2 beam (60,000 10-node tets, "
+                               f"{Kf.n} free unknowns), clamped at x = 0",
+                   "free_dofs": Kf.n, "subspace_vectors": 20,
+                   "flush": "inputs larger than L2", "parallelism": f"replicas x{world}"},
+        "eigenvalues": [float(v) for v in values],
+        "subspace_iterations": st.iterations, "solves": st.solves,
+        "pcg_iterations": st.pcg_iterations, "solve_seconds": st.seconds,
+        "assembly_s": assemble_s,
+        "roofline": {"bound": "hbm", "achieved": None, "peak": measured_peak()[0],
+                     "unit": "GB/s", "frac": None,
+                     "note": "the solves are the p-multigrid PCG of the p2beam line"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": value, "unit": "analyses/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 80},
+        "gpu_launches": None,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ------------------------------------------------------------------ the recovery workload
 RECOVER_METRIC = "recovered points/s (P2 strain, stress, von Mises, principal, peaks)"
 
@@ -1174,6 +1264,8 @@ def main():
         run_recover(opt, rank, world, local)
     elif opt.workload == "transient":
         run_transient(opt, rank, world, local)
+    elif opt.workload == "modes":
+        run_modes(opt, rank, world, local)
     elif opt.workload == "batch":
         run_batch(opt, rank, world, local)
     elif opt.workload == "serve":
