@@ -327,7 +327,9 @@ __device__ __forceinline__ double tet10_mass_scalar(int i, int j) {
 // MASS: the consistent mass of the 10-node tetrahedron (tet10.rs:173-212) with the density
 // coef[e], in place of the stiffness: entry (3i + a, 3j + b) = density V / 420 scalar(i, j) for
 // a = b, 0 else.
-template <int NN, int WARPS, bool MASS = false>
+// ORTHO: coef holds the 9 constants of an orthotropic material per element
+// (orthotropic_stiffness), else E and nu. Flags: 2 no stable material, 3 a modulus not above 0.
+template <int NN, int WARPS, bool MASS = false, bool ORTHO = false>
 __global__ void __launch_bounds__(32 * WARPS)
     k_gather_elastic(const double* __restrict__ xyz, const uint32_t* __restrict__ el,
                      const double* __restrict__ coef, const int64_t* __restrict__ start,
@@ -365,8 +367,11 @@ __global__ void __launch_bounds__(32 * WARPS)
             load_corners(xyz, nodes, p);
             tet_gradients(p, g, &vol);
             Stiffness D;
-            if (!MASS &&
-                !isotropic_stiffness(coef[2 * (int64_t)e], coef[2 * (int64_t)e + 1], &D)) {
+            if (ORTHO) {
+                const int st = orthotropic_stiffness(coef + 9 * (int64_t)e, &D);
+                if (st && lane == 0) atomicExch(bad, st == 1 ? 3 : 2);
+            } else if (!MASS &&
+                       !isotropic_stiffness(coef[2 * (int64_t)e], coef[2 * (int64_t)e + 1], &D)) {
                 if (lane == 0) atomicExch(bad, 2);
             }
             if (MASS) {
@@ -623,10 +628,12 @@ __global__ void k_colour_fill(const uint32_t* __restrict__ colour, int64_t nel,
 // ------------------------------------------------------------------ assemble
 void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t nel,
               const uint32_t* d_el, const double* d_coef, Assembled* out, cudaStream_t s) {
-    if (kind < 0 || kind > 3) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
+    if (kind < 0 || kind > 4) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
     if (mode < 0 || mode > 1) throw Failure(FEMGPU_ERR_INVALID, "unknown assembly mode");
-    if (kind == FEMGPU_P2_MASS && mode != FEMGPU_ASSEMBLE_GATHER)
-        throw Failure(FEMGPU_ERR_INVALID, "the mass assembles by rows (FEMGPU_ASSEMBLE_GATHER)");
+    if (kind >= FEMGPU_P2_MASS && mode != FEMGPU_ASSEMBLE_GATHER)
+        throw Failure(FEMGPU_ERR_INVALID,
+                      "the mass and orthotropic materials assemble by rows "
+                      "(FEMGPU_ASSEMBLE_GATHER)");
     int nn = kind >= FEMGPU_P2_ELASTIC ? 10 : 4;
     if (npoints >= 0xffffffffLL / 3)
         throw Failure(FEMGPU_ERR_TOO_LARGE, "more points than 32-bit unknown numbers hold");
@@ -653,6 +660,11 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
                 K.idx.p, K.val.p, bad.p);
         } else if (kind == FEMGPU_P1_ELASTIC) {
             k_gather_elastic<4, 4><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
+                d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints,
+                out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
+        } else if (kind == FEMGPU_P2_ELASTIC_ORTHO) {
+            k_gather_elastic<10, 4, false, true><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0,
+                                                   s>>>(
                 d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints,
                 out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
         } else if (kind == FEMGPU_P2_MASS) {
@@ -718,6 +730,9 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
         throw Failure(FEMGPU_ERR_MATERIAL,
                       "the Poisson ratios give no stable material (for an isotropic material, "
                       "nu must be between -1 and 0.5)");
+    if (b == 3)
+        throw Failure(FEMGPU_ERR_MATERIAL,
+                      "the moduli must be above 0 and the Poisson ratios finite");
 }
 
 // ------------------------------------------------------------------ Quadratic (tet10.rs:244)

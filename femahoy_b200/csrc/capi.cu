@@ -69,7 +69,9 @@ static int assemble_impl(int kind, int mode, size_t npoints, const double* xyz, 
         require(xyz && nodes && coef, "a null mesh array");
         cudaStream_t s = util_stream();
         int nn = kind >= FEMGPU_P2_ELASTIC ? 10 : 4;
-        int nc = kind == FEMGPU_P1_HEAT ? 3 : (kind == FEMGPU_P2_MASS ? 1 : 2);
+        int nc = kind == FEMGPU_P1_HEAT
+                     ? 3
+                     : (kind == FEMGPU_P2_MASS ? 1 : (kind == FEMGPU_P2_ELASTIC_ORTHO ? 9 : 2));
         DevBuf<double> dx, dc;
         DevBuf<uint32_t> de;
         const double* px = xyz;

@@ -81,6 +81,40 @@ __device__ __forceinline__ bool isotropic_stiffness(double e, double nu, Stiffne
     return true;
 }
 
+// hex.rs:69-114 for an orthotropic material, c = E_x, E_y, E_z, nu_xy, nu_xz, nu_yz, G_xy,
+// G_xz, G_yz (the fields of Orthotropic, hex.rs:47-55). Returns 0, or 1 when a modulus is not
+// above 0 or a ratio not finite (hex.rs:72-79), 2 when the constants give no stable material
+// (hex.rs:88-98).
+__device__ __forceinline__ int orthotropic_stiffness(const double* c, Stiffness* d) {
+    const double ex = c[0], ey = c[1], ez = c[2];
+    const double nxy = c[3], nxz = c[4], nyz = c[5];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        ok = ok && isfinite(c[k]) && c[k] > 0.0 && isfinite(c[6 + k]) && c[6 + k] > 0.0 &&
+             isfinite(c[3 + k]);
+    if (!ok) return 1;
+    double s[3][3] = {{1.0 / ex, -nxy / ex, -nxz / ex},
+                      {-nxy / ex, 1.0 / ey, -nyz / ey},
+                      {-nxz / ex, -nyz / ey, 1.0 / ez}};
+    double det = s[0][0] * (s[1][1] * s[2][2] - s[1][2] * s[2][1]) -
+                 s[0][1] * (s[1][0] * s[2][2] - s[1][2] * s[2][0]) +
+                 s[0][2] * (s[1][0] * s[2][1] - s[1][1] * s[2][0]);
+    double minor = s[0][0] * s[1][1] - s[0][1] * s[1][0];
+    if (!(minor > 0.0 && det > 1e-12 * s[0][0] * s[1][1] * s[2][2])) return 2;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            int i1 = (i + 1) % 3, i2 = (i + 2) % 3, j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+            d->normal[i][j] = (s[j1][i1] * s[j2][i2] - s[j1][i2] * s[j2][i1]) / det;
+        }
+    d->shear[0] = c[8];  // G_yz
+    d->shear[1] = c[7];  // G_xz
+    d->shear[2] = c[6];  // G_xy
+    return 0;
+}
+
 // tet10.rs:101-112: the (a, b) term of B^T D B between 2 function gradients.
 __device__ __forceinline__ double elastic_term(const double* gi, const double* gj, int a, int b,
                                                const Stiffness& d) {

@@ -42,8 +42,11 @@ enum {
     FEMGPU_P1_HEAT = 0,    /* 4-node tet, 4 x 4 conduction V G^T K G (heat.rs:972-1002) */
     FEMGPU_P1_ELASTIC = 1, /* 4-node tet, 12 x 12 V B^T D B (this library's own element) */
     FEMGPU_P2_ELASTIC = 2, /* 10-node tet, 30 x 30, 4-point rule (tet10.rs:90-120) */
-    FEMGPU_P2_MASS = 3     /* 10-node tet consistent mass, 30 x 30 (tet10.rs:173-212), coef = the
+    FEMGPU_P2_MASS = 3,    /* 10-node tet consistent mass, 30 x 30 (tet10.rs:173-212), coef = the
                               density per element, as modes.rs:470-476; gather mode only */
+    FEMGPU_P2_ELASTIC_ORTHO = 4 /* as FEMGPU_P2_ELASTIC with an orthotropic material per element
+                                   (Orthotropic::stiffness, hex.rs:69-117): coef = E_x, E_y,
+                                   E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz; gather mode only */
 };
 
 /* Assembly modes. */

@@ -175,7 +175,9 @@ class Csr:
 
     def assemble(self, kind, xyz, nodes, coef):
         """Add every element, in increasing element order (heat.rs:920-927,
-        elastic_tet.rs:183-193). kind 0 = P1 heat, 1 = P1 elasticity, 2 = P2 elasticity."""
+        elastic_tet.rs:183-193, modes.rs:470-476). kind 0 = P1 heat, 1 = P1 elasticity, 2 = P2
+        elasticity (E, nu), 3 = P2 mass (density), 4 = P2 elasticity of an orthotropic material
+        (E_x, E_y, E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz)."""
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
         coef = np.ascontiguousarray(coef, dtype=np.float64)
@@ -216,7 +218,7 @@ def tet_gradients(p):
 def element_matrix(kind, p, coef):
     p = np.ascontiguousarray(p, dtype=np.float64).reshape(12)
     coef = np.ascontiguousarray(coef, dtype=np.float64)
-    m = {0: 4, 1: 12, 2: 30, 3: 30}[kind]
+    m = {0: 4, 1: 12, 2: 30, 3: 30, 4: 30}[kind]
     ke = np.empty(m * m)
     _lib.orc_element_matrix(kind, _p(p), _p(coef), _p(ke))
     return ke.reshape(m, m)

@@ -133,6 +133,10 @@ int orc_element_matrix(int kind, const double* p12, const double* coef, double* 
         tet10_mass(v, coef[0], ke);
         return 0;
     }
+    if (kind == 4) {
+        tet10_stiffness(g, v, orthotropic_stiffness(coef, coef + 3, coef + 6), ke);
+        return 0;
+    }
     Stiffness d = isotropic_stiffness(coef[0], coef[1]);
     if (kind == 1)
         tet4_stiffness(g, v, d, ke);
@@ -183,6 +187,9 @@ int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, si
             }
             if (kind == 3) {
                 tet10_mass(v, coef[e], ke.data());  // modes.rs:475: the density per element
+            } else if (kind == 4) {
+                const double* c = coef + 9 * e;  // Orthotropic {e, nu, g} (hex.rs:47-55)
+                tet10_stiffness(g, v, orthotropic_stiffness(c, c + 3, c + 6), ke.data());
             } else {
                 Stiffness d = isotropic_stiffness(coef[2 * e], coef[2 * e + 1]);
                 if (kind == 1)

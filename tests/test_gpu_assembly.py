@@ -155,3 +155,27 @@ def test_bad_material_is_the_reference_error():
     coef = np.tile([70e3, 0.6], (len(m.tets), 1))
     with pytest.raises(fg.FemError, match="Poisson ratios give no stable material"):
         fg.Csr.assemble(fg.P1_ELASTIC, m.points, m.tets, coef)
+
+
+def test_orthotropic_p2_assembly_is_bit_identical():
+    """Orthotropic::stiffness (hex.rs:69-117) per element on the device: the same bits as the
+    oracle for random stable constants; a modulus below 0 gives the reference's text."""
+    m = mg.box(4, 2, 2, (40.0, 10.0, 10.0))
+    q = fg.Quadratic.new(m.points, m.tets)
+    rng = np.random.default_rng(8)
+    ne = len(q.tets)
+    e = rng.uniform(50e3, 200e3, (ne, 3))
+    nu = rng.uniform(0.1, 0.3, (ne, 3))
+    g = rng.uniform(20e3, 80e3, (ne, 3))
+    coef = np.hstack([e, nu, g])
+    K = fg.Csr.assemble(fg.P2_ELASTIC_ORTHO, q.points, q.tets, coef)
+    Ko = oracle.pattern(3 * len(q.points), oracle.dof_elements(q.tets))
+    Ko.assemble(4, q.points, q.tets, coef)
+    for a, b in zip(K.arrays(), Ko.arrays()):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    bad = coef.copy()
+    bad[3, 1] = -1.0
+    with pytest.raises(fg.FemError) as err:
+        fg.Csr.assemble(fg.P2_ELASTIC_ORTHO, q.points, q.tets, bad)
+    assert err.value.code == fg._lib.MATERIAL and "moduli must be above 0" in str(err.value)
+

@@ -205,3 +205,14 @@ def test_colouring_separates_elements_that_share_a_node():
     for c in range(nc):
         nodes = m.tets[col == c].ravel()
         assert len(np.unique(nodes)) == len(nodes)
+
+
+def test_orthotropic_with_equal_constants_is_the_isotropic_element():
+    """hex.rs:58-64: Orthotropic::isotropic is the orthotropic law with E, nu and
+    G = E / (2 (1 + nu)) on every axis: the same 30 x 30 element, bit for bit."""
+    p = np.array([[0.0, 0.0, 0.0], [2.0, 0.1, 0.0], [0.3, 1.5, 0.2], [0.1, 0.4, 0.9]])
+    e, nu = 70e3, 0.33
+    g = e / (2.0 * (1.0 + nu))
+    iso = oracle.element_matrix(2, p, np.array([e, nu]))
+    ortho = oracle.element_matrix(4, p, np.array([e, e, e, nu, nu, nu, g, g, g]))
+    assert np.array_equal(iso, ortho)
