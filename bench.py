@@ -69,14 +69,15 @@ def args():
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
                    choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover",
-                            "transient", "modes"],
+                            "transient", "modes", "hexheat"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
                         "serve: a Poisson stream of solve requests through the server; "
                         "recover: the stress recovery of the solved 200x20x20 P2 beam; "
                         "transient: backward-Euler steps of the 128^3 heat cube; "
-                        "modes: 10 lowest modes of a 100x10x10 P2 beam")
+                        "modes: 10 lowest modes of a 100x10x10 P2 beam; hexheat: the 128^3 "
+                        "heat cube on box cells")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -168,6 +169,12 @@ def build_system(opt):
         text = ("P1 elasticity cantilever 100x10x10 mm as 40x4x4 hexes x 6 Kuhn tets (3,000 free "
                 "unknowns), E 210 GPa, nu 0.3, clamped at x = 0, 1 MPa on the top face, to 1e-10, "
                 "FP64 and mixed PCG-MG")
+    elif opt.workload == "hexheat":
+        prob = mg.heat_cube_hex(opt.cells, seed=SEED)
+        kind, tol = fg.HEX8_HEAT, TOL
+        text = (f"P1 heat on box cells (the reference's box-grid model), {opt.cells}^3 hex "
+                f"cells of the unit cube, lognormal k seed {SEED}, 1 RHS to 1e-8, mixed "
+                f"precision PCG-MG")
     elif opt.workload == "p2beam":
         box = mg.box(200, 20, 20, (200.0, 20.0, 20.0))
         q = fg.Quadratic.new(box.points, box.tets)

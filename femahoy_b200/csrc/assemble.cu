@@ -298,6 +298,65 @@ __global__ void k_gather_heat(const double* __restrict__ xyz, const uint32_t* __
     }
 }
 
+// ------------------------------------------------------------------ gather: hex8 heat
+// heat.rs:1246-1273: entry (p, q) of the 8 x 8 conduction matrix of a box cell of sides s with
+// conductivities k, the corners in VTK order (bit b of axis e of corner p in kHexBits): the sum
+// over the axes d of k_d times, for each axis e in order, 1/h or -1/h (e = d) or h/3 or h/6.
+__device__ __constant__ const int kHexBits[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                                    {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+
+__device__ __forceinline__ double hex_conduction_entry(const double s[3], const double k[3], int p,
+                                                       int q) {
+    double v = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double term = k[d];
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            const bool same = kHexBits[p][e] == kHexBits[q][e];
+            term *= e == d ? (same ? 1.0 / s[e] : -1.0 / s[e]) : (same ? s[e] / 3.0 : s[e] / 6.0);
+        }
+        v += term;
+    }
+    return v;
+}
+
+// One thread per row, as k_gather_heat, for box cells (heat.rs:820-826): the cell's sides are
+// its corner 6 minus its corner 0, the plane spacings of the grid.
+__global__ void k_gather_hex_heat(const double* __restrict__ xyz, const uint32_t* __restrict__ el,
+                                  const double* __restrict__ coef,
+                                  const int64_t* __restrict__ start,
+                                  const uint32_t* __restrict__ of_node, int64_t n,
+                                  const int64_t* __restrict__ ptr,
+                                  const uint32_t* __restrict__ idx, double* __restrict__ val,
+                                  int* __restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r0 = ptr[i], r1 = ptr[i + 1];
+        for (int64_t t = start[i]; t < start[i + 1]; ++t) {
+            uint32_t e = of_node[t];
+            const uint32_t* nodes = el + 8 * (int64_t)e;
+            double s[3], k[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                s[d] = xyz[3 * (int64_t)nodes[6] + d] - xyz[3 * (int64_t)nodes[0] + d];
+                k[d] = coef[3 * (int64_t)e + d];
+            }
+            int a = 0;
+            while (a < 8 && nodes[a] != (uint32_t)i) ++a;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                int64_t at = lower_bound(idx, r0, r1, nodes[b]);
+                if (at >= r1 || idx[at] != nodes[b]) {
+                    atomicExch(bad, 1);
+                    continue;
+                }
+                val[at] += hex_conduction_entry(s, k, a, b);
+            }
+        }
+    }
+}
+
 // ------------------------------------------------------------------ gather: elasticity
 // One warp per node v, for its 3 rows 3v + c. The element matrix rows 3 a + c of each element
 // of v, in increasing element order; the lanes share the 3 x 3 m outputs of one element, each
@@ -628,13 +687,14 @@ __global__ void k_colour_fill(const uint32_t* __restrict__ colour, int64_t nel,
 // ------------------------------------------------------------------ assemble
 void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t nel,
               const uint32_t* d_el, const double* d_coef, Assembled* out, cudaStream_t s) {
-    if (kind < 0 || kind > 4) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
+    if (kind < 0 || kind > 5) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
     if (mode < 0 || mode > 1) throw Failure(FEMGPU_ERR_INVALID, "unknown assembly mode");
     if (kind >= FEMGPU_P2_MASS && mode != FEMGPU_ASSEMBLE_GATHER)
         throw Failure(FEMGPU_ERR_INVALID,
-                      "the mass and orthotropic materials assemble by rows "
+                      "the mass, orthotropic materials and box cells assemble by rows "
                       "(FEMGPU_ASSEMBLE_GATHER)");
-    int nn = kind >= FEMGPU_P2_ELASTIC ? 10 : 4;
+    const bool scalar = kind == FEMGPU_P1_HEAT || kind == FEMGPU_HEX8_HEAT;
+    int nn = kind == FEMGPU_HEX8_HEAT ? 8 : (kind >= FEMGPU_P2_ELASTIC ? 10 : 4);
     if (npoints >= 0xffffffffLL / 3)
         throw Failure(FEMGPU_ERR_TOO_LARGE, "more points than 32-bit unknown numbers hold");
     build_incidence(d_el, nel, nn, npoints, &out->inc, s);
@@ -642,7 +702,7 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
     DevBuf<int> bad(1);
     bad.zero(s);
     DevCsr& K = out->matrix;
-    if (kind == FEMGPU_P1_HEAT) {
+    if (scalar) {
         K.n = out->node.n;
         K.nnz = out->node.nnz;
         K.ptr = std::move(out->node.ptr);
@@ -656,6 +716,10 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
     if (mode == FEMGPU_ASSEMBLE_GATHER) {
         if (kind == FEMGPU_P1_HEAT) {
             k_gather_heat<<<blocks_for(npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
+                d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints, K.ptr.p,
+                K.idx.p, K.val.p, bad.p);
+        } else if (kind == FEMGPU_HEX8_HEAT) {
+            k_gather_hex_heat<<<blocks_for(npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
                 d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints, K.ptr.p,
                 K.idx.p, K.val.p, bad.p);
         } else if (kind == FEMGPU_P1_ELASTIC) {

@@ -145,6 +145,42 @@ def heat_cube(n=128, seed=1234, source=1.0) -> Problem:
                    xyz=mesh.points, seed=seed)
 
 
+# The corners of a box cell in VTK order: (0,0,0), (1,0,0), (1,1,0), (0,1,0), (0,0,1), (1,0,1),
+# (1,1,1), (0,1,1).
+HEX_BITS = [(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]
+
+
+def box_cells(mesh):
+    """The box cells of a BoxMesh's grid (nx ny nz, in grid order), 8 corners each in VTK order,
+    as the reference's grid meshes (crates/fem/src/heat.rs:804-826)."""
+    nx, ny, nz = mesh.dims
+    ck, cj, ci = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    ci, cj, ck = ci.ravel(), cj.ravel(), ck.ravel()
+    cols = [(ci + a) + (nx + 1) * ((cj + b) + (ny + 1) * (ck + c)) for a, b, c in HEX_BITS]
+    return np.stack(cols, axis=1).astype(np.uint32)
+
+
+def heat_cube_hex(n=64, seed=1234, source=1.0) -> "Problem":
+    """P1 heat conduction on the box cells of the unit cube (the reference's box-grid heat
+    model): conductivity exp(N(0, 1)) per cell (numpy PCG64, ``seed``), T = 1 on x = 0 and
+    T = 0 on x = 1, a uniform volume source lumped V/8 to each corner (heat.rs:417-423)."""
+    mesh = box(n, n, n)
+    cells = box_cells(mesh)
+    rng = np.random.default_rng(seed)
+    k = np.exp(rng.standard_normal(len(cells)))
+    coef = np.repeat(k[:, None], 3, axis=1)
+    fixed = (mesh.ijk[:, 0] == 0) | (mesh.ijk[:, 0] == n)
+    values = np.where(mesh.ijk[:, 0] == 0, 1.0, 0.0)
+    values[~fixed] = 0.0
+    p = mesh.points
+    vol = np.prod(p[cells[:, 6]] - p[cells[:, 0]], axis=1)
+    load = np.zeros(mesh.n)
+    for c in range(8):
+        np.add.at(load, cells[:, c], source * vol / 8.0)
+    return Problem("hex_heat", mesh, cells, coef, mesh.n, 1, fixed, values, load,
+                   xyz=mesh.points, seed=seed)
+
+
 def lumped_capacity(mesh, capacity=1.0):
     """crates/fem/src/heat.rs:417-423: each corner of a tetrahedron takes capacity V/4, summed
     in tetrahedron order."""

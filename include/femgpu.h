@@ -44,9 +44,14 @@ enum {
     FEMGPU_P2_ELASTIC = 2, /* 10-node tet, 30 x 30, 4-point rule (tet10.rs:90-120) */
     FEMGPU_P2_MASS = 3,    /* 10-node tet consistent mass, 30 x 30 (tet10.rs:173-212), coef = the
                               density per element, as modes.rs:470-476; gather mode only */
-    FEMGPU_P2_ELASTIC_ORTHO = 4 /* as FEMGPU_P2_ELASTIC with an orthotropic material per element
-                                   (Orthotropic::stiffness, hex.rs:69-117): coef = E_x, E_y,
-                                   E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz; gather mode only */
+    FEMGPU_P2_ELASTIC_ORTHO = 4, /* as FEMGPU_P2_ELASTIC with an orthotropic material per
+                                    element (Orthotropic::stiffness, hex.rs:69-117): coef = E_x,
+                                    E_y, E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz; gather
+                                    mode only */
+    FEMGPU_HEX8_HEAT = 5 /* box cell of the grid, 8 corners in VTK order, 8 x 8 conduction
+                            (heat.rs:1246-1273) as heat.rs:820-826 assembles it; coef = the 3
+                            conductivities; the sides are corner 6 minus corner 0; gather mode
+                            only */
 };
 
 /* Assembly modes. */

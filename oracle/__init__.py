@@ -177,7 +177,8 @@ class Csr:
         """Add every element, in increasing element order (heat.rs:920-927,
         elastic_tet.rs:183-193, modes.rs:470-476). kind 0 = P1 heat, 1 = P1 elasticity, 2 = P2
         elasticity (E, nu), 3 = P2 mass (density), 4 = P2 elasticity of an orthotropic material
-        (E_x, E_y, E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz)."""
+        (E_x, E_y, E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz), 5 = box cells of 8 corners in
+        VTK order (the 3 conductivities)."""
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         nodes = np.ascontiguousarray(nodes, dtype=np.uint32)
         coef = np.ascontiguousarray(coef, dtype=np.float64)

@@ -169,6 +169,20 @@ int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, si
                  const double* coef, char* err, size_t len) {
     try {
         Csr* a = C(h);
+        if (kind == 5) {  // heat.rs:820-826: box cells, the sides from corners 0 and 6
+            double ke[64];
+            for (size_t e = 0; e < nel; ++e) {
+                const uint32_t* t = nodes + 8 * e;
+                double s[3], k[3];
+                for (int d = 0; d < 3; ++d) {
+                    s[d] = xyz[3 * (size_t)t[6] + d] - xyz[3 * (size_t)t[0] + d];
+                    k[d] = coef[3 * e + d];
+                }
+                hex_conduction(s, k, ke);
+                a->add_element(t, 8, ke);
+            }
+            return 0;
+        }
         int mn = kind >= 2 ? 10 : 4;
         int m = kind == 0 ? 4 : 3 * mn;
         vector<double> ke(m * m);

@@ -295,5 +295,25 @@ void transient_energy(size_t n, const double* kt, const double* rate, const doub
     out[2] = gross;
 }
 
+// heat.rs:1246-1273: the 8 x 8 conduction matrix of a box cell of sides s, VTK corner order.
+void hex_conduction(const double s[3], const double k[3], double ke[64]) {
+    static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int p = 0; p < 8; ++p)
+        for (int q = 0; q < 8; ++q) {
+            double v = 0.0;
+            for (int d = 0; d < 3; ++d) {
+                double term = k[d];
+                for (int e = 0; e < 3; ++e) {
+                    bool same = BITS[p][e] == BITS[q][e];
+                    term *= e == d ? (same ? 1.0 / s[e] : -1.0 / s[e])
+                                   : (same ? s[e] / 3.0 : s[e] / 6.0);
+                }
+                v += term;
+            }
+            ke[p * 8 + q] = v;
+        }
+}
+
 }  // namespace orc
 

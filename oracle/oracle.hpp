@@ -101,6 +101,8 @@ void tet4_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k
 
 // tet10.rs:173-212
 void tet10_mass(double volume, double density, double m[900]);
+// heat.rs:1246-1273
+void hex_conduction(const double s[3], const double k[3], double ke[64]);
 
 // eigen.rs:183-269 and 274-331: the dense generalized and standard symmetric eigenproblems.
 // Returns false with `err` set when M is not positive definite.
