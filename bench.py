@@ -79,7 +79,7 @@ def args():
                         "modes: 10 lowest modes of a 100x10x10 P2 beam; hexheat: the 128^3 "
                         "heat cube on box cells")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
-    p.add_argument("--rates", default="10,50,200",
+    p.add_argument("--rates", default="10,50,200,500",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
     p.add_argument("--requests", type=int, default=40, help="serve: requests per rate")
     p.add_argument("--graph", type=int, default=0,
