@@ -82,6 +82,8 @@ def args():
     p.add_argument("--rates", default="10,50,200,500",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
     p.add_argument("--requests", type=int, default=40, help="serve: requests per rate")
+    p.add_argument("--builders", type=int, default=3,
+                   help="serve: threads that build new meshes' solvers side by side")
     p.add_argument("--graph", type=int, default=0,
                    help="0/1: the PCG loop as 1 CUDA graph; 2: kernels launched one by one (so "
                         "that a profiler lists each kernel of the loop)")
@@ -798,8 +800,9 @@ def serve_setup(kind, prob, box):
 def run_serve(opt, rank, world, local):
     """Replays the request stream at each arrival rate through a fresh server. At its Poisson
     arrival time a request whose mesh is resident goes straight to the server; one that names a
-    new mesh waits for a builder thread (1 build at a time: assembly and hierarchy) that hands
-    the solver to the server and then submits the requests that waited for it. A request's
+    new mesh waits for 1 of `--builders` builder threads (each builds 1 mesh at a time: assembly
+    and hierarchy) that hands the solver to the server and then submits the requests that waited
+    for it. A request's
     latency runs from its arrival to the end of its solve (the server's own clock from
     submission to the end of the solve, plus the time before submission)."""
     import queue
@@ -848,8 +851,8 @@ def run_serve(opt, rank, world, local):
             submitted.append((i, mid, t, server.submit(mid, b), resident))
 
         def builder():
-            # 1 build at a time: assembly and hierarchy of a new mesh, then the requests that
-            # waited for it go to the server.
+            # 1 build at a time per thread: assembly and hierarchy of a new mesh, then the
+            # requests that waited for it go to the server.
             while True:
                 mid = builds.get()
                 if mid is None:
@@ -861,8 +864,9 @@ def run_serve(opt, rank, world, local):
                     for i in pending.pop(mid):
                         submit(i, mid, False)
 
-        worker = threading.Thread(target=builder)
-        worker.start()
+        workers = [threading.Thread(target=builder) for _ in range(opt.builders)]
+        for w in workers:
+            w.start()
         start = time.perf_counter()
         for i, (mid, _) in enumerate(reqs):
             wait = start + arrivals[i] - time.perf_counter()
@@ -876,8 +880,10 @@ def run_serve(opt, rank, world, local):
                 else:
                     pending[mid] = [i]
                     builds.put(mid)
-        builds.put(None)
-        worker.join()
+        for _ in workers:
+            builds.put(None)
+        for w in workers:
+            w.join()
         records = []
         for i, mid, t_sub, ticket, resident in sorted(submitted):
             x, st, solve_s = server.wait(ticket)
