@@ -69,7 +69,7 @@ def args():
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
                    choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover",
-                            "transient", "modes", "hexheat"],
+                            "transient", "modes", "hexheat", "hexbeam"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
@@ -77,7 +77,8 @@ def args():
                         "recover: the stress recovery of the solved 200x20x20 P2 beam; "
                         "transient: backward-Euler steps of the 128^3 heat cube; "
                         "modes: 10 lowest modes of a 100x10x10 P2 beam; hexheat: the 128^3 "
-                        "heat cube on box cells")
+                        "heat cube on box cells; hexbeam: a cantilever of 256x32x32 box cells "
+                        "with incompatible modes (2 materials)")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200,500",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -177,6 +178,15 @@ def build_system(opt):
         text = (f"P1 heat on box cells (the reference's box-grid model), {opt.cells}^3 hex "
                 f"cells of the unit cube, lognormal k seed {SEED}, 1 RHS to 1e-8, mixed "
                 f"precision PCG-MG")
+    elif opt.workload == "hexbeam":
+        nx, ny = 2 * opt.cells, max(1, opt.cells // 4)
+        prob = mg.hex_cantilever(nx=nx, ny=ny, nz=ny, length=8.0, width=1.0, depth=1.0,
+                                 e=1000.0, nu=0.3, load=-1.0, seed=SEED)
+        kind, tol = fg.HEX8_ELASTIC, TOL
+        text = (f"elasticity on box cells with incompatible modes (the reference's box-grid "
+                f"elastic model), a {nx}x{ny}x{ny} cell cantilever 8x1x1, isotropic (E 1000, nu "
+                f"0.3) and orthotropic cells (seed {SEED}), clamped at x = 0, a tip load, 1 RHS "
+                f"to 1e-8, mixed precision PCG-MG")
     elif opt.workload == "p2beam":
         box = mg.box(200, 20, 20, (200.0, 20.0, 20.0))
         q = fg.Quadratic.new(box.points, box.tets)

@@ -7,7 +7,7 @@ The Python names mirror the reference crate: ``Csr`` (sparse.rs), ``Solver``, ``
 (pmultigrid.rs), ``Quadratic`` (tet10.rs) and ``reduced_rhs`` (heat.rs); ``Recovery`` and
 ``Peak`` are the post-solve loop of elastic_tet.rs:367-427.
 """
-from ._lib import (COLOUR, FP64, GATHER, HEX8_HEAT, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
+from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
                    P2_ELASTIC_ORTHO, P2_MASS, FemError, LIB_PATH, lib)
 from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT_LIMIT,
                     Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
@@ -16,7 +16,7 @@ from .recover import Peak, Recovery
 from .sparse import Csr, Rect, colour
 
 __all__ = [
-    "COLOUR", "FP64", "GATHER", "HEX8_HEAT", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "P2_ELASTIC_ORTHO", "P2_MASS",
+    "COLOUR", "FP64", "GATHER", "HEX8_ELASTIC", "HEX8_HEAT", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "P2_ELASTIC_ORTHO", "P2_MASS",
     "FemError",
     "LIB_PATH", "lib", "PCG_MAX_ITER", "PCG_TOL", "STEADY_DIRECT_LIMIT",
     "TRANSIENT_DIRECT_LIMIT", "Crossover", "Level", "Method", "Options", "Quadratic", "Solver",

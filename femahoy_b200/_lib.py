@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libfemgpu.so")
 OK, CANCELLED, NOT_CONVERGED, NOT_SPD, NEEDS_GRID, INVALID, CUDA, TOO_LARGE, PATTERN, MATERIAL, \
     TIMEOUT = range(11)
 
-P1_HEAT, P1_ELASTIC, P2_ELASTIC, P2_MASS, P2_ELASTIC_ORTHO, HEX8_HEAT = 0, 1, 2, 3, 4, 5
+P1_HEAT, P1_ELASTIC, P2_ELASTIC, P2_MASS, P2_ELASTIC_ORTHO, HEX8_HEAT, HEX8_ELASTIC = range(7)
 GATHER, COLOUR = 0, 1
 FP64, MIXED = 0, 1
 

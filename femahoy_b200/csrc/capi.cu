@@ -68,10 +68,13 @@ static int assemble_impl(int kind, int mode, size_t npoints, const double* xyz, 
         require(npoints > 0 && nel > 0, "an empty mesh");
         require(xyz && nodes && coef, "a null mesh array");
         cudaStream_t s = util_stream();
-        int nn = kind == FEMGPU_HEX8_HEAT ? 8 : (kind >= FEMGPU_P2_ELASTIC ? 10 : 4);
+        int nn = kind >= FEMGPU_HEX8_HEAT ? 8 : (kind >= FEMGPU_P2_ELASTIC ? 10 : 4);
         int nc = (kind == FEMGPU_P1_HEAT || kind == FEMGPU_HEX8_HEAT)
                      ? 3
-                     : (kind == FEMGPU_P2_MASS ? 1 : (kind == FEMGPU_P2_ELASTIC_ORTHO ? 9 : 2));
+                     : (kind == FEMGPU_P2_MASS
+                            ? 1
+                            : (kind == FEMGPU_P2_ELASTIC_ORTHO || kind == FEMGPU_HEX8_ELASTIC ? 9
+                                                                                             : 2));
         DevBuf<double> dx, dc;
         DevBuf<uint32_t> de;
         const double* px = xyz;

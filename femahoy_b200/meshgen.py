@@ -181,6 +181,57 @@ def heat_cube_hex(n=64, seed=1234, source=1.0) -> "Problem":
                    xyz=mesh.points, seed=seed)
 
 
+def orthotropic(e, nu=None, g=None):
+    """The 9 constants (Ex, Ey, Ez, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz) of a material with its
+    axes on x, y and z (crates/fem/src/hex.rs:47-55); with one modulus and one ratio, the
+    isotropic material (hex.rs:57-65: G = E / (2 (1 + nu)))."""
+    if np.isscalar(e):
+        return np.array([e] * 3 + [nu] * 3 + [e / (2.0 * (1.0 + nu))] * 3, dtype=np.float64)
+    return np.concatenate([np.asarray(e, float), np.asarray(nu, float), np.asarray(g, float)])
+
+
+def graded_planes(n, length, grade):
+    """n cells over ``length`` whose widths grow geometrically, the last ``grade`` times the
+    first."""
+    if n < 2 or grade == 1.0:
+        return length * np.arange(n + 1) / n
+    w = grade ** (np.arange(n) / (n - 1))
+    return np.concatenate([[0.0], np.cumsum(w)]) * (length / w.sum())
+
+
+def hex_cantilever(nx=24, ny=2, nz=2, length=6.0, width=0.5, depth=0.5, e=1000.0, nu=0.3,
+                   load=-1.0, grade=1.0, seed=None) -> Problem:
+    """A cantilever of box cells (the reference's box-grid elastic model, elastic.rs:352-391):
+    every unknown fixed at x = 0, a total force ``load`` along z on the face x = ``length``
+    (each face cell gives a quarter of its share to each of its 4 corners). ``grade`` makes the
+    cells along x and z grow geometrically (last / first = grade); with ``seed``, about half the
+    cells (numpy PCG64) take an orthotropic material (E, E/2, E/4; 0.25, 0.3, 0.35; G = 0.3 E,
+    0.25 E, 0.2 E) in place of the isotropic (e, nu)."""
+    mesh = box(nx, ny, nz, (length, width, depth))
+    mesh.planes[0] = graded_planes(nx, length, grade)
+    mesh.planes[2] = graded_planes(nz, depth, grade)
+    for d in range(3):
+        mesh.points[:, d] = mesh.planes[d][mesh.ijk[:, d]]
+    cells = box_cells(mesh)
+    coef = np.tile(orthotropic(e, nu), (len(cells), 1))
+    if seed is not None:
+        pick = np.random.default_rng(seed).random(len(cells)) < 0.5
+        coef[pick] = orthotropic([e, e / 2.0, e / 4.0], [0.25, 0.3, 0.35],
+                                 [0.3 * e, 0.25 * e, 0.2 * e])
+    n = mesh.n
+    fixed = np.repeat(mesh.ijk[:, 0] == 0, 3)
+    force = np.zeros(3 * n)
+    ci = np.arange(len(cells)) % nx
+    end = cells[ci == nx - 1]
+    p = mesh.points
+    area = (p[end[:, 2], 1] - p[end[:, 1], 1]) * (p[end[:, 5], 2] - p[end[:, 1], 2])
+    share = load * area / (width * depth) / 4.0
+    for c in (1, 2, 5, 6):  # the corners on the cell's x = high face
+        np.add.at(force, 3 * end[:, c].astype(np.int64) + 2, share)
+    return Problem("hex_elastic", mesh, cells, coef, n, 3, fixed, np.zeros(3 * n), force,
+                   xyz=mesh.points, seed=seed)
+
+
 def lumped_capacity(mesh, capacity=1.0):
     """crates/fem/src/heat.rs:417-423: each corner of a tetrahedron takes capacity V/4, summed
     in tetrahedron order."""

@@ -53,8 +53,10 @@ class Csr:
         """Csr::pattern + Csr::add_element over every element on the device. ``kind``:
         femahoy_b200.P1_HEAT (``coef`` (T, 3) conductivities), P1_ELASTIC or P2_ELASTIC
         (``coef`` (T, 2) E and nu; unknown 3 node + component), P2_MASS (``coef`` (T,) the
-        density). ``mode`` GATHER gives the reference's values bit for bit; COLOUR scatters
-        colour by colour (not for the mass)."""
+        density), P2_ELASTIC_ORTHO (``coef`` (T, 9) orthotropic constants), HEX8_HEAT (box
+        cells, ``coef`` (T, 3) conductivities) or HEX8_ELASTIC (box cells with incompatible
+        modes, ``coef`` (T, 9) orthotropic constants). ``mode`` GATHER gives the reference's
+        values bit for bit; COLOUR scatters colour by colour (P1 and P2 elasticity, P1 heat)."""
         x = L.arr(points, np.float64)
         e = L.arr(nodes, np.uint32)
         c = L.arr(coef, np.float64)

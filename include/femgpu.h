@@ -48,10 +48,16 @@ enum {
                                     element (Orthotropic::stiffness, hex.rs:69-117): coef = E_x,
                                     E_y, E_z, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz; gather
                                     mode only */
-    FEMGPU_HEX8_HEAT = 5 /* box cell of the grid, 8 corners in VTK order, 8 x 8 conduction
-                            (heat.rs:1246-1273) as heat.rs:820-826 assembles it; coef = the 3
-                            conductivities; the sides are corner 6 minus corner 0; gather mode
-                            only */
+    FEMGPU_HEX8_HEAT = 5, /* box cell of the grid, 8 corners in VTK order, 8 x 8 conduction
+                             (heat.rs:1246-1273) as heat.rs:820-826 assembles it; coef = the 3
+                             conductivities; the sides are corner 6 minus corner 0; gather mode
+                             only */
+    FEMGPU_HEX8_ELASTIC = 6 /* box cell of the grid, 8 corners in VTK order: the 24 x 24
+                               stiffness of the 8-node hex with its 9 incompatible modes condensed
+                               (Hex::new, hex.rs:218-297), as elastic.rs:386-391 assembles it;
+                               coef = the 9 orthotropic constants of FEMGPU_P2_ELASTIC_ORTHO; the
+                               sides are corner 6 minus corner 0 (above 0); unknown 3 node +
+                               component; gather mode only */
 };
 
 /* Assembly modes. */

@@ -46,6 +46,7 @@ def _load():
         "orc_tet_gradients": (None, [P, P, P]),
         "orc_isotropic": (I, [D, D, P, P, P, S]),
         "orc_element_matrix": (I, [I, P, P, P]),
+        "orc_hex8_stiffness": (I, [P, P, P, P, S]),
         "orc_assemble": (I, [P, I, P, P, S, P, P, S]),
         "orc_quadratic": (S, [P, S, P, S, P, P]),
         "orc_colour": (I, [S, P, S, I, P]),
@@ -223,6 +224,28 @@ def element_matrix(kind, p, coef):
     ke = np.empty(m * m)
     _lib.orc_element_matrix(kind, _p(p), _p(coef), _p(ke))
     return ke.reshape(m, m)
+
+
+def orthotropic(e, nu=None, g=None):
+    """The 9 constants (Ex, Ey, Ez, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz) of an orthotropic
+    material (hex.rs:47-55); with one modulus and a ratio, the isotropic material
+    (hex.rs:57-65: G = E / (2 (1 + nu)))."""
+    if np.isscalar(e):
+        return np.array([e] * 3 + [nu] * 3 + [e / (2.0 * (1.0 + nu))] * 3)
+    return np.concatenate([np.asarray(e, float), np.asarray(nu, float), np.asarray(g, float)])
+
+
+def hex8_stiffness(size, c):
+    """hex.rs:218-297: the 24 x 24 stiffness of the 8 corners (unknown 3 corner + component) of a
+    box cell with the side lengths ``size``, its 9 incompatible modes condensed, for the
+    orthotropic constants ``c`` (``orthotropic``)."""
+    size = np.ascontiguousarray(size, dtype=np.float64).reshape(3)
+    c = np.ascontiguousarray(c, dtype=np.float64).reshape(9)
+    kc = np.empty(576)
+    err = C.create_string_buffer(512)
+    if _lib.orc_hex8_stiffness(_p(size), _p(c), _p(kc), err, 512):
+        raise OracleError(err.value.decode())
+    return kc.reshape(24, 24)
 
 
 def isotropic(e, nu):

@@ -145,6 +145,18 @@ int orc_element_matrix(int kind, const double* p12, const double* coef, double* 
     return 0;
 }
 
+// hex.rs:218-297: the condensed 24 x 24 stiffness of a box cell with the sides `size` and the
+// orthotropic constants `c` (Ex, Ey, Ez, nu_xy, nu_xz, nu_yz, G_xy, G_xz, G_yz).
+int orc_hex8_stiffness(const double* size, const double* c, double* kc, char* err, size_t len) {
+    try {
+        hex8_stiffness(size, orthotropic_stiffness(c, c + 3, c + 6), kc);
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+
 // eigen.rs:183-269 (row-major n x n); -1 and the reference's text on failure.
 int orc_dense_generalized(const double* k, const double* m, int n, double* values, double* q,
                           char* err, size_t len) {
@@ -162,8 +174,9 @@ void orc_dense_jacobi(double* a, int n, double* values, double* v) {
 
 // Assemble all the elements of a mesh into the pattern `h`, in increasing element order
 // (heat.rs:920-927, elastic_tet.rs:183-193, modes.rs:470-476). kind as orc_element_matrix;
-// `nodes` are 4 corners (kind 0, 1) or 10 points (kind 2, 3) per element; `coef` has 3 (kind 0),
-// 2 (kinds 1, 2) or 1 (kind 3: the density) values per element.
+// `nodes` are 4 corners (kind 0, 1), 10 points (kind 2, 3, 4) or 8 box corners (kind 5, 6) per
+// element; `coef` has 3 (kinds 0, 5), 2 (kinds 1, 2), 1 (kind 3: the density) or 9 (kinds 4, 6:
+// an orthotropic material) values per element.
 // The scalar nodes of kinds 1 and 2 become the unknowns 3 node + component.
 int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, size_t nel,
                  const double* coef, char* err, size_t len) {
@@ -180,6 +193,21 @@ int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, si
                 }
                 hex_conduction(s, k, ke);
                 a->add_element(t, 8, ke);
+            }
+            return 0;
+        }
+        if (kind == 6) {  // elastic.rs:386-391: box cells, Hex::new per cell
+            vector<double> kc(576);
+            uint32_t dofs[24];
+            for (size_t e = 0; e < nel; ++e) {
+                const uint32_t* t = nodes + 8 * e;
+                const double* c = coef + 9 * e;  // Orthotropic {e, nu, g} (hex.rs:47-55)
+                double s[3];
+                for (int d = 0; d < 3; ++d)
+                    s[d] = xyz[3 * (size_t)t[6] + d] - xyz[3 * (size_t)t[0] + d];
+                hex8_stiffness(s, orthotropic_stiffness(c, c + 3, c + 6), kc.data());
+                for (int k = 0; k < 24; ++k) dofs[k] = 3 * t[k / 3] + (uint32_t)(k % 3);
+                a->add_element(dofs, 24, kc.data());
             }
             return 0;
         }

@@ -315,5 +315,78 @@ void hex_conduction(const double s[3], const double k[3], double ke[64]) {
         }
 }
 
+// hex.rs:146-160: the gradients of the 8 corner functions and the 3 mode functions at the local
+// point xi of a box of sides `size`.
+static void hex_gradients(const double size[3], const double xi[3], double g[11][3]) {
+    static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int i = 0; i < 11; ++i)
+        for (int d = 0; d < 3; ++d) g[i][d] = 0.0;
+    for (int n = 0; n < 8; ++n) {
+        double s[3], f[3];
+        for (int d = 0; d < 3; ++d) {
+            s[d] = BITS[n][d] == 1 ? 1.0 : -1.0;
+            f[d] = 0.5 * (1.0 + s[d] * xi[d]);
+        }
+        for (int d = 0; d < 3; ++d) g[n][d] = s[d] / size[d] * f[(d + 1) % 3] * f[(d + 2) % 3];
+    }
+    for (int d = 0; d < 3; ++d) g[8 + d][d] = -4.0 * xi[d] / size[d];
+}
+
+// hex.rs:218-297 (the stiffness part of Hex::new): the 33 x 33 matrix of the 8 corner and 3 mode
+// functions over the 2-point Gauss rule, then the 9 modes condensed with the Cholesky factor of
+// their block (hex.rs:355-389): the 24 x 24 stiffness of the corners, row-major.
+void hex8_stiffness(const double size[3], const Stiffness& d, double kc[576]) {
+    static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    double k[33][33];
+    for (int i = 0; i < 33; ++i)
+        for (int j = 0; j < 33; ++j) k[i][j] = 0.0;
+    const double jac = size[0] * size[1] * size[2] / 8.0;
+    const double p = 1.0 / std::sqrt(3.0);
+    for (int gp = 0; gp < 8; ++gp) {
+        double xi[3], g[11][3];
+        for (int e = 0; e < 3; ++e) xi[e] = BITS[gp][e] == 1 ? p : -p;
+        hex_gradients(size, xi, g);
+        for (int i = 0; i < 11; ++i)
+            for (int j = 0; j < 11; ++j)
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b)
+                        k[3 * i + a][3 * j + b] += jac * elastic_term(g[i], g[j], a, b, d);
+    }
+    double l[9][9] = {};
+    for (int j = 0; j < 9; ++j) {  // cholesky9
+        double dd = k[24 + j][24 + j];
+        for (int c = 0; c < j; ++c) dd -= l[j][c] * l[j][c];
+        dd = std::sqrt(dd);
+        l[j][j] = dd;
+        for (int i = j + 1; i < 9; ++i) {
+            double v = k[24 + i][24 + j];
+            for (int c = 0; c < j; ++c) v -= l[i][c] * l[j][c];
+            l[i][j] = v / dd;
+        }
+    }
+    double mode[9][24];
+    for (int c = 0; c < 24; ++c) {  // solve9 on each column of K_mu
+        double b[9];
+        for (int i = 0; i < 9; ++i) b[i] = k[24 + i][c];
+        for (int i = 0; i < 9; ++i) {
+            for (int q = 0; q < i; ++q) b[i] -= l[i][q] * b[q];
+            b[i] /= l[i][i];
+        }
+        for (int i = 8; i >= 0; --i) {
+            for (int q = i + 1; q < 9; ++q) b[i] -= l[q][i] * b[q];
+            b[i] /= l[i][i];
+        }
+        for (int i = 0; i < 9; ++i) mode[i][c] = b[i];
+    }
+    for (int r = 0; r < 24; ++r)
+        for (int c = 0; c < 24; ++c) {
+            double v = k[r][c];
+            for (int i = 0; i < 9; ++i) v -= k[r][24 + i] * mode[i][c];
+            kc[r * 24 + c] = v;
+        }
+}
+
 }  // namespace orc
 

@@ -103,6 +103,8 @@ void tet4_stiffness(const Vec3 g[4], double volume, const Stiffness& d, double k
 void tet10_mass(double volume, double density, double m[900]);
 // heat.rs:1246-1273
 void hex_conduction(const double s[3], const double k[3], double ke[64]);
+// hex.rs:218-297, 355-389: the condensed 24 x 24 stiffness of a box cell
+void hex8_stiffness(const double size[3], const Stiffness& d, double kc[576]);
 
 // eigen.rs:183-269 and 274-331: the dense generalized and standard symmetric eigenproblems.
 // Returns false with `err` set when M is not positive definite.

@@ -1,0 +1,124 @@
+"""Elasticity on the box cells of the grid: the 8-node hex with 9 incompatible modes condensed
+(crates/fem/src/hex.rs:218-311), assembled as elastic.rs:386-391 does for the box-grid models.
+
+CPU: the oracle's element against the reference's own unit tests of it (hex.rs:443-526: the
+stiffness is symmetric, a rigid motion has no force, one cell holds a pure bending field with
+the exact energy) and a cantilever of box cells against beam theory. GPU: the device assembly bit
+for bit against the oracle, and the grid multigrid solve against the oracle's direct solution."""
+import numpy as np
+import pytest
+
+import oracle
+from femahoy_b200 import meshgen as mg
+
+SIZE = np.array([2.0, 0.5, 0.1])  # hex.rs:402
+
+
+def nodal(f, size=SIZE):
+    """hex.rs:453-460: the corner displacements of the field f of the position."""
+    u = np.empty(24)
+    for n, b in enumerate(mg.HEX_BITS):
+        u[3 * n:3 * n + 3] = f(np.asarray(b, float) * size)
+    return u
+
+
+def test_oracle_hex_stiffness_is_symmetric_and_rigid_motions_have_no_force():
+    """hex.rs:462-489 (the strain check of the rigid motions needs the recovery, not built)."""
+    k = oracle.hex8_stiffness(SIZE, oracle.orthotropic(200.0, 0.3))
+    assert np.all(np.abs(k - k.T) <= 1e-12 * np.maximum(np.abs(k), 1.0))
+    motions = [lambda x: [1.0, 0.0, 0.0], lambda x: [0.0, 1.0, 0.0], lambda x: [0.0, 0.0, 1.0],
+               lambda x: [-x[1], x[0], 0.0], lambda x: [0.0, -x[2], x[1]],
+               lambda x: [x[2], 0.0, -x[0]]]
+    scale = np.abs(k).max()
+    for m in motions:
+        f = k @ nodal(m)
+        assert np.abs(f).max() < 1e-12 * scale
+
+
+def test_oracle_one_cell_bends_with_the_exact_curvature():
+    """hex.rs:521-545: u^T K u equals E I kappa^2 L for the pure bending field (nu = 0)."""
+    e, kappa = 1000.0, 1e-3
+    k = oracle.hex8_stiffness(SIZE, oracle.orthotropic(e, 0.0))
+    u = nodal(lambda x: [-kappa * x[0] * (x[2] - SIZE[2] / 2.0), 0.0, kappa * x[0] ** 2 / 2.0])
+    ku = u @ (k @ u)
+    exact = e * SIZE[1] * SIZE[2] ** 3 / 12.0 * kappa ** 2 * SIZE[0]
+    assert abs(ku - exact) < 1e-9 * exact
+
+
+def test_oracle_orthotropic_box_cell_rejects_unstable_materials():
+    with pytest.raises(oracle.OracleError, match="no stable material"):
+        oracle.hex8_stiffness(SIZE, oracle.orthotropic(1.0, 0.5))
+    with pytest.raises(oracle.OracleError, match="moduli must be above 0"):
+        oracle.hex8_stiffness(SIZE, oracle.orthotropic([1.0, -1.0, 1.0], [0.3] * 3, [1.0] * 3))
+
+
+def test_oracle_box_cantilever_matches_beam_theory():
+    """A cantilever of box cells, 2 cells through the depth: the incompatible modes hold the
+    bending, so the tip deflection is near P L^3 / (3 E I) (the plain trilinear hex locks far
+    below it). Clamped at x = 0, a tip load on x = L."""
+    c = mg.hex_cantilever(nx=24, ny=2, nz=2, length=6.0, width=0.5, depth=0.5, load=-1.0)
+    k = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    k.assemble(6, c.xyz, c.nodes, c.coef)
+    a = k.submatrix(c.free)
+    rhs = k.reduced_rhs(c.load, c.values, c.free)
+    x, _ = oracle.direct_solve(a, c.xyz[c.free // 3], rhs)
+    u = np.zeros(3 * c.mesh.n)
+    u[c.free] = x
+    tip = (c.mesh.ijk[:, 0] == 24)
+    w = u[3 * np.nonzero(tip)[0] + 2].mean()
+    e, i = 1000.0, 0.5 * 0.5 ** 3 / 12.0
+    beam = -1.0 * 6.0 ** 3 / (3.0 * e * i)
+    assert 0.97 < w / beam < 1.05
+
+
+@pytest.mark.gpu
+def test_gpu_box_cell_elastic_assembly_is_bit_identical():
+    """Graded cells of 2 materials (isotropic and orthotropic) in the x and z directions: the
+    element classes differ, and each entry is the sum in cell order."""
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=10, ny=3, nz=4, length=3.0, width=0.6, depth=0.4, load=-1.0,
+                          grade=1.3, seed=7)
+    K = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef)
+    Ko = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    Ko.assemble(6, c.xyz, c.nodes, c.coef)
+    for a, b in zip(K.arrays(), Ko.arrays()):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.gpu
+def test_gpu_box_cell_elastic_rejects_bad_materials():
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=2, ny=1, nz=1)
+    coef = c.coef.copy()
+    coef[1] = oracle.orthotropic(1.0, 0.5)
+    with pytest.raises(fg.FemError, match="no stable material"):
+        fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, coef)
+    coef[1] = oracle.orthotropic(-1.0, 0.3)
+    with pytest.raises(fg.FemError, match="moduli must be above 0"):
+        fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, coef)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_box_cantilever_solves(precision):
+    """PCG with the grid V-cycle on a box-cell cantilever against the oracle's direct solution
+    (1e-8 relative) and its own true residual."""
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=48, ny=6, nz=6, length=6.0, width=0.75, depth=0.75, load=-1.0,
+                          grade=1.1, seed=3)
+    K = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef)
+    A = K.submatrix(c.free)
+    rhs = fg.reduced_rhs(K, c.load, c.values, c.free)
+    planes, pts, comp = mg.grid_unknowns(c)
+    s = fg.Solver(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), fg.Method.Multigrid,
+                  precision=precision,
+                  options=fg.Options(precision=precision, coarsest=600)).with_tol(1e-10)
+    assert s.levels()[0] == A.n and len(s.levels()) >= 2
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    assert st.true_residual <= 1.2e-10
+    Ko = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    Ko.assemble(6, c.xyz, c.nodes, c.coef)
+    xd, _ = oracle.direct_solve(Ko.submatrix(c.free), c.xyz[c.free // 3],
+                                Ko.reduced_rhs(c.load, c.values, c.free))
+    assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
