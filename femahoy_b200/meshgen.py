@@ -232,6 +232,19 @@ def hex_cantilever(nx=24, ny=2, nz=2, length=6.0, width=0.5, depth=0.5, e=1000.0
                    xyz=mesh.points, seed=seed)
 
 
+def hex_classes(prob):
+    """The element classes of the box cells of ``prob``: (origin (C, 3) the lowest grid point
+    of each cell, cls (C,) its class, keys (K, 12) the 3 sides and 9 material constants of each
+    class). Cells whose 12 numbers are equal bit for bit share a class (and a matrix)."""
+    cells = prob.nodes
+    p = prob.xyz
+    keys = np.concatenate([p[cells[:, 6]] - p[cells[:, 0]], prob.coef], axis=1)
+    raw = np.ascontiguousarray(keys).view(np.dtype((np.void, 96))).ravel()
+    _, first, cls = np.unique(raw, return_index=True, return_inverse=True)
+    return (prob.mesh.ijk[cells[:, 0]].astype(np.uint32), cls.astype(np.uint32).ravel(),
+            keys[first])
+
+
 def lumped_capacity(mesh, capacity=1.0):
     """crates/fem/src/heat.rs:417-423: each corner of a tetrahedron takes capacity V/4, summed
     in tetrahedron order."""

@@ -59,11 +59,13 @@ def _load():
         "orc_rect_mul_transpose": (None, [P, P, P]),
         "orc_galerkin": (P, [P, P]),
         "orc_coarsen": (P, [P, P, S, P, S, P, S, P, P, S, P, P, P]),
+        "orc_by_cells": (P, [P, P, S, P, S, P, S, P, P, S, S, P, P, P, S, P, P, P]),
         "orc_prolongation": (P, [P, S, S, P, S, P, S, P, P]),
         "orc_nested_dissection": (None, [P, P, P]),
         "orc_direct_solve": (I, [P, P, P, P, P, S]),
         "orc_solver_new": (P, [P, I, P, S, P, S, P, S, P, P, P, P, P, S, I, I, S, D,
-                               C.c_uint64, I, P, S]),
+                               C.c_uint64, I, S, P, P, P, S, P, S]),
+        "orc_solver_level_matrix": (P, [P, S]),
         "orc_solver_free": (None, [P]),
         "orc_solver_method": (I, [P]),
         "orc_solver_levels": (S, [P]),
@@ -377,6 +379,25 @@ def coarsen(a: Csr, planes, points, comp):
     return Rect(h), cp[:cn.value].copy(), cc[:cn.value].copy()
 
 
+def by_cells(a: Csr, planes, points, comp, cells):
+    """multigrid.rs:458-608 after coarsen: (coarse matrix, coarse points, coarse comp) or None.
+    ``cells`` as for Solver."""
+    px, py, pz, pts, cmp_ = _level_args(planes, points, comp)
+    n = len(pts)
+    origin = np.ascontiguousarray(cells[0], dtype=np.uint32)
+    cls = np.ascontiguousarray(cells[1], dtype=np.uint32)
+    table = np.ascontiguousarray(cells[2], dtype=np.float64)
+    cp = np.empty((n, 3), np.uint32)
+    cc = np.empty(n, np.uint8)
+    cn = C.c_size_t()
+    h = _lib.orc_by_cells(a.h, _p(px), len(px), _p(py), len(py), _p(pz), len(pz), _p(pts),
+                          _p(cmp_), n, len(origin), _p(origin), _p(cls), _p(table),
+                          table.size // 576, _p(cp), _p(cc), C.byref(cn))
+    if not h:
+        return None
+    return Csr(h), cp[:cn.value].copy(), cc[:cn.value].copy()
+
+
 def prolongation(points, corners, edges, free):
     """pmultigrid.rs:104-151: (P, coarse xyz)."""
     pts = np.ascontiguousarray(points, dtype=np.float64)
@@ -413,8 +434,18 @@ class Solver:
     'quadratic' (xyz, p: Rect, coarse xyz). ``method``: None, 'direct' or 'multigrid'."""
 
     def __init__(self, a: Csr, kind, *, planes=None, points=None, comp=None, xyz=None, p=None,
-                 coarse=None, method=None, crossover=("unknowns", 3000)):
+                 coarse=None, method=None, crossover=("unknowns", 3000), cells=None):
+        """``cells`` (grid only, multigrid.rs:62-68): (origin (C, 3) the lowest grid point of
+        each cell, cls (C,) its class, matrices (K, 24, 24) of the classes); the coarse
+        matrices then come from the cells (multigrid.rs:458-608)."""
         err = C.create_string_buffer(512)
+        nce = ncl = 0
+        origin = cls = table = None
+        if cells is not None:
+            origin = np.ascontiguousarray(cells[0], dtype=np.uint32)
+            cls = np.ascontiguousarray(cells[1], dtype=np.uint32)
+            table = np.ascontiguousarray(cells[2], dtype=np.float64)
+            nce, ncl = len(origin), table.size // 576
         k = {"grid": 0, "points": 1, "quadratic": 2}[kind]
         m = {None: -1, "direct": 0, "multigrid": 1}[method]
         px = py = pz = pts = cmp_ = xyz_ = cx = None
@@ -435,7 +466,8 @@ class Solver:
             fl, en, flat = crossover[1], crossover[2], int(crossover[3])
         self.h = _lib.orc_solver_new(a.h, k, _p(px), nx, _p(py), ny, _p(pz), nz, _p(pts),
                                      _p(cmp_), _p(xyz_), p.h if p is not None else None, _p(cx),
-                                     nc, m, fr, un, fl, en, flat, err, 512)
+                                     nc, m, fr, un, fl, en, flat, nce, _p(origin), _p(cls),
+                                     _p(table), ncl, err, 512)
         if not self.h:
             raise OracleError(err.value.decode())
         self.n = a.n
@@ -451,6 +483,13 @@ class Solver:
     def levels(self):
         return [_lib.orc_solver_level_size(self.h, i)
                 for i in range(_lib.orc_solver_levels(self.h))]
+
+    def level_matrix(self, level):
+        """The matrix of multigrid level ``level`` (0 = the system's)."""
+        h = _lib.orc_solver_level_matrix(self.h, level)
+        if not h:
+            raise OracleError(f"no multigrid level {level}")
+        return Csr(h)
 
     def solve(self, b, x=None, tol=0.0, max_iter=0, cancel=None):
         """Returns (x, iterations, residual); raises OracleError with the reference text."""

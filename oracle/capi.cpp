@@ -322,6 +322,33 @@ void* orc_coarsen(void* a, const double* px, size_t nx, const double* py, size_t
     return p;
 }
 
+// multigrid.rs:458-608 after coarsen (multigrid.rs:329-452): the coarse matrix from the cells
+// (origin 3 per cell, its class, 576 values per class), or null; the coarse level as
+// orc_coarsen writes it.
+void* orc_by_cells(void* a, const double* px, size_t nx, const double* py, size_t ny,
+                   const double* pz, size_t nz, const uint32_t* points, const uint8_t* comp,
+                   size_t n, size_t ncells, const uint32_t* origin, const uint32_t* cls,
+                   const double* table, size_t nclass, uint32_t* cpoints, uint8_t* ccomp,
+                   size_t* cn) {
+    Level fine = make_level(px, nx, py, ny, pz, nz, points, comp, n);
+    Cells cells;
+    cells.origin.resize(ncells);
+    for (size_t i = 0; i < ncells; ++i)
+        for (int d = 0; d < 3; ++d) cells.origin[i][d] = origin[3 * i + d];
+    cells.cls.assign(cls, cls + ncells);
+    cells.table.assign(table, table + 576 * nclass);
+    Rect p;
+    Level coarse;
+    if (!coarsen(fine, *C(a), &p, &coarse)) return nullptr;
+    Cells next;
+    Csr* out = new Csr(by_cells(fine, cells, coarse, &next));
+    *cn = coarse.points.size();
+    for (size_t k = 0; k < coarse.points.size(); ++k)
+        for (int d = 0; d < 3; ++d) cpoints[3 * k + d] = coarse.points[k][d];
+    std::memcpy(ccomp, coarse.comp.data(), coarse.comp.size());
+    return out;
+}
+
 // pmultigrid.rs:104-151. Returns P; the coarse points go to `cxyz` (3 per coarse unknown;
 // room for 3 * nfree values).
 void* orc_prolongation(const double* points, size_t npoints, size_t corners,
@@ -373,12 +400,23 @@ void* orc_solver_new(void* a, int kind, const double* px, size_t nx, const doubl
                      size_t ny, const double* pz, size_t nz, const uint32_t* points,
                      const uint8_t* comp, const double* xyz, void* p, const double* cxyz,
                      size_t ncoarse, int method, int flops_rule, size_t unknowns, double flops,
-                     uint64_t entries, int flat, char* err, size_t len) {
+                     uint64_t entries, int flat, size_t ncells, const uint32_t* origin,
+                     const uint32_t* cls, const double* table, size_t nclass, char* err,
+                     size_t len) {
     try {
         Unknowns u;
         size_t n = C(a)->n;
         u.kind = (Unknowns::Kind)kind;
         if (kind == 0) u.level = make_level(px, nx, py, ny, pz, nz, points, comp, n);
+        if (kind == 0 && ncells) {  // multigrid.rs:62-68: the cells of a displacement model
+            u.cells.origin.resize(ncells);
+            for (size_t i = 0; i < ncells; ++i)
+                for (int d = 0; d < 3; ++d) u.cells.origin[i][d] = origin[3 * i + d];
+            u.cells.cls.assign(cls, cls + ncells);
+            for (size_t i = 0; i < ncells; ++i)
+                if (cls[i] >= nclass) throw Error("a cell class is out of range");
+            u.cells.table.assign(table, table + 576 * nclass);
+        }
         if (kind >= 1) u.points = make_points(xyz, n);
         if (kind == 2) {
             u.p = *R(p);
@@ -399,6 +437,12 @@ void* orc_solver_new(void* a, int kind, const double* px, size_t nx, const doubl
     }
 }
 void orc_solver_free(void* s) { delete static_cast<OSolver*>(s); }
+// A copy of the matrix of multigrid level `l` (null when the solver has no such level).
+void* orc_solver_level_matrix(void* s, size_t l) {
+    auto* o = static_cast<OSolver*>(s);
+    if (o->s.inner != Solver::MG || l >= o->s.mg.a.size()) return nullptr;
+    return new Csr(o->s.mg.a[l]);
+}
 int orc_solver_method(void* s) { return (int)static_cast<OSolver*>(s)->s.method(); }
 size_t orc_solver_levels(void* s) {
     auto* o = static_cast<OSolver*>(s);

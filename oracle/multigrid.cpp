@@ -223,10 +223,203 @@ static vector<Vec3> level_xyz(const Level& level) {
     return xyz;
 }
 
-// multigrid.rs:84-139 with `cells = None`.
-Multigrid Multigrid::make(const Csr& a0, Level level) {
+// The local bits of the 8 corners of a cell in VTK order (hex.rs:34-43).
+static const int CORNER[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                 {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+
+// multigrid.rs:616-652: the modes of a coarse cell to keep (3 d + c for the mode along axis d of
+// component c): a Cholesky factor of the Gram matrix of each component's 11 functions, corners
+// first, skipping a pivot below 1e-6 of its diagonal.
+static array<bool, 9> kept_modes(const double gram[3][11][11]) {
+    array<bool, 9> keep{};
+    for (int c = 0; c < 3; ++c) {
+        const auto& g = gram[c];
+        double l[11][11] = {};
+        bool used[11] = {};
+        for (int j = 0; j < 11; ++j) {
+            double d = g[j][j];
+            for (int k = 0; k < j; ++k)
+                if (used[k]) d -= l[j][k] * l[j][k];
+            if (!(d > 1e-6 * g[j][j])) continue;
+            used[j] = true;
+            d = std::sqrt(d);
+            l[j][j] = d;
+            for (int i = j + 1; i < 11; ++i) {
+                double v = g[i][j];
+                for (int k = 0; k < j; ++k)
+                    if (used[k]) v -= l[i][k] * l[j][k];
+                l[i][j] = v / d;
+            }
+            if (j >= 8) keep[3 * (j - 8) + c] = true;
+        }
+    }
+    return keep;
+}
+
+// multigrid.rs:654-681: symmetric Gauss elimination of the kept modes with energy from the
+// 33 x 33 matrix `k`; the 24 x 24 block of the corners.
+static void condense_modes(double* k, const array<bool, 9>& keep, double* out) {
+    for (int m = 24; m < 33; ++m) {
+        if (!keep[m - 24]) continue;
+        const double pivot = k[m * 33 + m];
+        double scale = 0.0;
+        for (int i = 0; i < 33; ++i) scale = std::fmax(scale, std::fabs(k[i * 33 + i]));
+        if (!(pivot > 1e-12 * scale)) continue;
+        for (int i = 0; i < 33; ++i) {
+            const double f = k[i * 33 + m] / pivot;
+            if (i == m || f == 0.0) continue;
+            for (int j = 0; j < 33; ++j) k[i * 33 + j] -= f * k[m * 33 + j];
+        }
+    }
+    for (int r = 0; r < 24; ++r)
+        for (int c = 0; c < 24; ++c) out[r * 24 + c] = k[r * 33 + c];
+}
+
+// multigrid.rs:458-608. The fine cells of each coarse cell are summed in increasing fine-cell
+// order (the reference groups them by an unstable sort, which leaves that order open).
+Csr by_cells(const Level& fine, const Cells& cells, const Level& coarse, Cells* next) {
+    size_t fd[3], cd[3];
+    for (int d = 0; d < 3; ++d) {
+        fd[d] = fine.planes[d].size();
+        cd[d] = coarse.planes[d].size();
+    }
+    auto index = [](const array<uint32_t, 3>& q, size_t c, const size_t* dims) {
+        return c + 3 * (q[0] + dims[0] * (q[1] + dims[1] * (size_t)q[2]));
+    };
+    vector<bool> free(3 * fd[0] * fd[1] * fd[2], false);
+    for (size_t k = 0; k < fine.points.size(); ++k) free[index(fine.points[k], fine.comp[k], fd)] = true;
+    vector<uint32_t> number(3 * cd[0] * cd[1] * cd[2], UINT32_MAX);
+    for (size_t k = 0; k < coarse.points.size(); ++k)
+        number[index(coarse.points[k], coarse.comp[k], cd)] = (uint32_t)k;
+    // The kept planes of each axis (multigrid.rs:341-346) and the coarse cell of each fine one.
+    array<vector<uint32_t>, 3> interval;
+    for (int d = 0; d < 3; ++d) {
+        vector<size_t> keep;
+        if (fd[d] <= 2) {
+            for (size_t i = 0; i < fd[d]; ++i) keep.push_back(i);
+        } else {
+            for (size_t i = 0; i < fd[d]; i += 2) keep.push_back(i);
+            if (keep.back() != fd[d] - 1) keep.push_back(fd[d] - 1);
+        }
+        size_t c = 0;
+        for (size_t i = 0; i < fd[d]; ++i) {
+            while (c + 2 < keep.size() && keep[c + 1] <= i) ++c;
+            interval[d].push_back((uint32_t)c);
+        }
+    }
+    const size_t nf = cells.origin.size();
+    vector<std::pair<uint32_t, array<uint32_t, 3>>> order(nf);
+    for (size_t f = 0; f < nf; ++f) {
+        const auto& o = cells.origin[f];
+        order[f] = {(uint32_t)f, {interval[0][o[0]], interval[1][o[1]], interval[2][o[2]]}};
+    }
+    std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) {
+        return std::tie(a.second[2], a.second[1], a.second[0]) <
+               std::tie(b.second[2], b.second[1], b.second[0]);
+    });
+    next->origin.clear();
+    next->cls.clear();
+    next->table.clear();
+    vector<double> k(33 * 33);
+    size_t start = 0;
+    while (start < order.size()) {
+        const auto cc = order[start].second;
+        size_t end = start;
+        while (end < order.size() && order[end].second == cc) ++end;
+        double lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = coarse.planes[d][cc[d]];
+            hi[d] = coarse.planes[d][cc[d] + 1];
+        }
+        std::fill(k.begin(), k.end(), 0.0);
+        double gram[3][11][11] = {};
+        for (size_t t = start; t < end; ++t) {
+            const uint32_t f = order[t].first;
+            const double* kf = cells.element(f);
+            const auto& o = cells.origin[f];
+            double phi[8][3][11] = {};
+            for (int n = 0; n < 8; ++n) {
+                array<uint32_t, 3> q;
+                double xi[3];
+                for (int d = 0; d < 3; ++d) {
+                    q[d] = o[d] + (uint32_t)CORNER[n][d];
+                    xi[d] = 2.0 * (fine.planes[d][q[d]] - lo[d]) / (hi[d] - lo[d]) - 1.0;
+                }
+                double corner[8];
+                for (int m = 0; m < 8; ++m) {  // hex.rs:164-178
+                    double v = 1.0;
+                    for (int d = 0; d < 3; ++d)
+                        v *= CORNER[m][d] == 1 ? 0.5 * (1.0 + xi[d]) : 0.5 * (1.0 - xi[d]);
+                    corner[m] = v;
+                }
+                for (int c = 0; c < 3; ++c) {
+                    if (!free[index(q, c, fd)]) continue;
+                    double* fn = phi[n][c];
+                    for (int m = 0; m < 8; ++m) fn[m] = corner[m];
+                    for (int d = 0; d < 3; ++d) fn[8 + d] = 1.0 - xi[d] * xi[d];
+                    for (int a = 0; a < 11; ++a)
+                        for (int b = 0; b < 11; ++b) gram[c][a][b] += fn[a] * fn[b];
+                }
+            }
+            double kt[24][33] = {};  // Kf T
+            for (int r = 0; r < 24; ++r)
+                for (int m = 0; m < 8; ++m)
+                    for (int c = 0; c < 3; ++c) {
+                        const double v = kf[r * 24 + 3 * m + c];
+                        if (v != 0.0)
+                            for (int a = 0; a < 11; ++a) kt[r][3 * a + c] += v * phi[m][c][a];
+                    }
+            for (int n = 0; n < 8; ++n)  // K += T^T kt
+                for (int c = 0; c < 3; ++c)
+                    for (int a = 0; a < 11; ++a) {
+                        const double w = phi[n][c][a];
+                        if (w == 0.0) continue;
+                        double* out = k.data() + (3 * a + c) * 33;
+                        for (int j = 0; j < 33; ++j) out[j] += w * kt[3 * n + c][j];
+                    }
+        }
+        const size_t at = next->table.size();
+        next->table.resize(at + 576);
+        condense_modes(k.data(), kept_modes(gram), next->table.data() + at);
+        next->cls.push_back((uint32_t)next->origin.size());
+        next->origin.push_back(cc);
+        start = end;
+    }
+    // Assemble on the coarse unknowns (the kept corners of each coarse cell).
+    const size_t ncells = next->origin.size();
+    vector<vector<std::pair<int, uint32_t>>> ids(ncells);
+    vector<uint32_t> globals;
+    vector<size_t> gstart{0};
+    for (size_t e = 0; e < ncells; ++e) {
+        for (int n = 0; n < 8; ++n) {
+            array<uint32_t, 3> q;
+            for (int d = 0; d < 3; ++d) q[d] = next->origin[e][d] + (uint32_t)CORNER[n][d];
+            for (int c = 0; c < 3; ++c) {
+                const uint32_t g = number[index(q, c, cd)];
+                if (g != UINT32_MAX) ids[e].push_back({3 * n + c, g});
+            }
+        }
+        for (const auto& rg : ids[e]) globals.push_back(rg.second);
+        gstart.push_back(globals.size());
+    }
+    Csr a = pattern_lists(coarse.points.size(), globals, gstart);
+    vector<double> ke;
+    for (size_t e = 0; e < ncells; ++e) {
+        ke.clear();
+        const double* m = next->table.data() + 576 * e;
+        for (const auto& r : ids[e])
+            for (const auto& c : ids[e]) ke.push_back(m[r.first * 24 + c.first]);
+        a.add_element(globals.data() + gstart[e], (int)ids[e].size(), ke.data());
+    }
+    return a;
+}
+
+// multigrid.rs:84-139.
+Multigrid Multigrid::make(const Csr& a0, Level level, const Cells* cells) {
     Multigrid mg;
     mg.a.push_back(a0);
+    Cells stored;
+    bool have = false;
     for (;;) {
         const Csr& a = mg.a.back();
         if (a.n <= COARSEST || mg.p.size() >= 30) break;
@@ -236,7 +429,15 @@ Multigrid Multigrid::make(const Csr& a0, Level level) {
         if (coarse.points.size() * 10 > a.n * 9) break;
         mg.lines.push_back({Lines::make(level, 0, a), Lines::make(level, 1, a),
                             Lines::make(level, 2, a)});
-        Csr ac = p.galerkin(a);
+        Csr ac;
+        if (cells && !cells->empty()) {
+            Cells nxt;
+            ac = by_cells(level, have ? stored : *cells, coarse, &nxt);
+            stored = std::move(nxt);
+            have = true;
+        } else {
+            ac = p.galerkin(a);
+        }
         mg.a.push_back(std::move(ac));
         mg.p.push_back(std::move(p));
         level = std::move(coarse);
@@ -473,7 +674,7 @@ Solver Solver::make(Csr a, Unknowns unknowns, int method, Crossover crossover) {
         s.chol = factor(sym, a);
         s.inner = Direct;
     } else {
-        s.mg = Multigrid::make(a, std::move(unknowns.level));
+        s.mg = Multigrid::make(a, std::move(unknowns.level), &unknowns.cells);
         s.inner = MG;
     }
     s.a = std::move(a);

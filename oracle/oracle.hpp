@@ -55,6 +55,8 @@ struct Csr {
 };
 // sparse.rs:22-65: elements are `nel` runs of `m` nodes.
 Csr pattern(size_t n, const uint32_t* elements, size_t nel, int m);
+// The same for elements of different sizes: element k is nodes[start[k] .. start[k + 1]].
+Csr pattern_lists(size_t n, const vector<uint32_t>& nodes, const vector<size_t>& start);
 
 // sparse.rs:202-208
 struct Rect {
@@ -203,13 +205,28 @@ struct Lines {
 // multigrid.rs:329-452
 bool coarsen(const Level& fine, const Csr& a, Rect* p, Level* coarse);
 
-// multigrid.rs:73-180 (the Galerkin form: `cells = None`)
+// multigrid.rs:62-68 `Cells`: the lowest grid point of each cell of a displacement model and
+// its 24 x 24 matrix (row-major, unknown 3 n + c for corner n in VTK order), here the class
+// matrix table + 576 cls[i].
+struct Cells {
+    vector<array<uint32_t, 3>> origin;
+    vector<uint32_t> cls;
+    vector<double> table;
+    const double* element(size_t i) const { return table.data() + 576 * (size_t)cls[i]; }
+    bool empty() const { return origin.empty(); }
+};
+
+// multigrid.rs:458-608: the coarse matrix of a displacement from the cells, and the coarse
+// cells with their matrices for the next level.
+Csr by_cells(const Level& fine, const Cells& cells, const Level& coarse, Cells* next);
+
+// multigrid.rs:73-180; with `cells` the coarse matrices come from the cells.
 struct Multigrid {
     vector<Csr> a;
     vector<Rect> p;
     vector<array<Lines, 3>> lines;
     Cholesky coarse;
-    static Multigrid make(const Csr& a, Level level);
+    static Multigrid make(const Csr& a, Level level, const Cells* cells = nullptr);
     size_t levels() const { return a.size(); }
     void apply(const double* r, double* z) const;
     void cycle(size_t l, const double* b, double* x) const;
@@ -259,6 +276,7 @@ struct Crossover {
 struct Unknowns {
     enum Kind { Grid = 0, Points = 1, Quadratic = 2 } kind = Grid;
     Level level;             // Grid
+    Cells cells;             // Grid: solve.rs:97 `cells` (empty: None)
     vector<Vec3> points;     // Points, Quadratic
     Rect p;                  // Quadratic
     vector<Vec3> coarse;     // Quadratic

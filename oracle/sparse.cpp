@@ -8,7 +8,49 @@
 namespace orc {
 
 // sparse.rs:22-65. Counting sort of the elements of each node, then for each row a mark
-// de-duplication of the nodes of its elements, plus the row itself, and a sort.
+// de-duplication of the nodes of its elements, plus the row itself, and a sort. Element k is
+// nodes[start[k] .. start[k + 1]].
+Csr pattern_lists(size_t n, const vector<uint32_t>& nodes, const vector<size_t>& start) {
+    const size_t nel = start.size() - 1;
+    vector<size_t> count(n + 1, 0);
+    for (uint32_t v : nodes) count[v + 1] += 1;
+    for (size_t i = 0; i < n; ++i) count[i + 1] += count[i];
+    vector<uint32_t> of_node(count[n]);
+    vector<size_t> next(count);
+    for (size_t k = 0; k < nel; ++k)
+        for (size_t t = start[k]; t < start[k + 1]; ++t) {
+            uint32_t v = nodes[t];
+            of_node[next[v]] = (uint32_t)k;
+            next[v] += 1;
+        }
+    Csr out;
+    out.n = n;
+    out.ptr.reserve(n + 1);
+    out.ptr.push_back(0);
+    vector<size_t> mark(n, SIZE_MAX);
+    vector<uint32_t> row;
+    for (size_t i = 0; i < n; ++i) {
+        row.clear();
+        mark[i] = i;
+        row.push_back((uint32_t)i);
+        for (size_t t = count[i]; t < count[i + 1]; ++t) {
+            const size_t k = of_node[t];
+            for (size_t b = start[k]; b < start[k + 1]; ++b) {
+                uint32_t v = nodes[b];
+                if (mark[v] != i) {
+                    mark[v] = i;
+                    row.push_back(v);
+                }
+            }
+        }
+        std::sort(row.begin(), row.end());
+        out.idx.insert(out.idx.end(), row.begin(), row.end());
+        out.ptr.push_back(out.idx.size());
+    }
+    out.val.assign(out.idx.size(), 0.0);
+    return out;
+}
+
 Csr pattern(size_t n, const uint32_t* elements, size_t nel, int m) {
     vector<size_t> count(n + 1, 0);
     for (size_t e = 0; e < nel; ++e)

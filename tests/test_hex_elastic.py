@@ -71,6 +71,84 @@ def test_oracle_box_cantilever_matches_beam_theory():
     assert 0.97 < w / beam < 1.05
 
 
+def class_table(c):
+    """The cells of a box-cell problem for the cell-based coarse matrices: (origin, class,
+    the oracle's matrix of each class)."""
+    origin, cls, keys = mg.hex_classes(c)
+    return origin, cls, np.stack([oracle.hex8_stiffness(k[:3], k[3:]) for k in keys])
+
+
+def dense(csr):
+    ptr, idx, val = csr.arrays()
+    a = np.zeros((len(ptr) - 1, len(ptr) - 1))
+    for i in range(len(ptr) - 1):
+        a[i, idx[ptr[i]:ptr[i + 1]]] = val[ptr[i]:ptr[i + 1]]
+    return a
+
+
+def test_oracle_coarse_cell_is_the_condensed_product_and_bends_exactly():
+    """multigrid.rs:458-681 on 1 coarse cell of 2 x 2 x 2 fine cells, every unknown free: the
+    coarse matrix is T^T K T of the coarse cell's 8 corner and 9 mode fields at the fine
+    corners (formed here in numpy) with the modes condensed; it has no force for a rigid
+    motion, and it holds a pure bending field with the exact energy, as 1 cell does."""
+    size = (2.0, 0.5, 0.1)
+    c = mg.hex_cantilever(nx=2, ny=2, nz=2, length=size[0], width=size[1], depth=size[2],
+                          e=1000.0, nu=0.0)
+    n = c.mesh.n
+    k = oracle.pattern(3 * n, oracle.dof_elements(c.nodes))
+    k.assemble(6, c.xyz, c.nodes, c.coef)
+    free = np.arange(3 * n)
+    ac, cp, cc = oracle.by_cells(k, c.mesh.planes, c.mesh.ijk[free // 3].astype(np.uint32),
+                                 (free % 3).astype(np.uint8), class_table(c))
+    corner = [tuple(b) for b in mg.HEX_BITS]
+    perm = np.array([3 * corner.index(tuple(int(v) for v in p)) + q for p, q in zip(cp, cc)])
+    got = np.zeros((24, 24))
+    got[np.ix_(perm, perm)] = dense(ac)
+    xi = 2.0 * c.xyz / np.asarray(size) - 1.0
+    t = np.zeros((3 * n, 33))
+    for m, b in enumerate(mg.HEX_BITS):
+        f = np.prod([np.where(b[d], 0.5 * (1 + xi[:, d]), 0.5 * (1 - xi[:, d]))
+                     for d in range(3)], axis=0)
+        for q in range(3):
+            t[q::3, 3 * m + q] = f
+    for d in range(3):
+        for q in range(3):
+            t[q::3, 24 + 3 * d + q] = 1.0 - xi[:, d] ** 2
+    kc = t.T @ dense(k) @ t
+    want = kc[:24, :24] - kc[:24, 24:] @ np.linalg.solve(kc[24:, 24:], kc[24:, :24])
+    assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+    assert np.abs(got - got.T).max() <= 1e-13 * np.abs(got).max()
+    corners = np.asarray(mg.HEX_BITS, float) * np.asarray(size)
+    for f in [lambda x: [1.0, 0.0, 0.0], lambda x: [0.0, 1.0, 0.0], lambda x: [0.0, 0.0, 1.0],
+              lambda x: [-x[1], x[0], 0.0], lambda x: [0.0, -x[2], x[1]],
+              lambda x: [x[2], 0.0, -x[0]]]:
+        u = np.concatenate([f(x) for x in corners])
+        assert np.abs(got @ u).max() < 1e-12 * np.abs(got).max()
+    kappa = 1e-3
+    u = np.concatenate([[-kappa * x[0] * (x[2] - size[2] / 2.0), 0.0, kappa * x[0] ** 2 / 2.0]
+                        for x in corners])
+    exact = 1000.0 * size[1] * size[2] ** 3 / 12.0 * kappa ** 2 * size[0]
+    assert abs(u @ got @ u - exact) < 1e-9 * exact
+
+
+def test_oracle_cell_multigrid_solves_the_cantilever():
+    """multigrid.rs:84-139 with cells: every coarse level from the cells of the one above; PCG
+    with it reaches the direct solution."""
+    c = mg.hex_cantilever(nx=48, ny=6, nz=6, length=6.0, width=0.75, depth=0.75, load=-1.0,
+                          grade=1.1, seed=3)
+    k = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    k.assemble(6, c.xyz, c.nodes, c.coef)
+    a = k.submatrix(c.free)
+    rhs = k.reduced_rhs(c.load, c.values, c.free)
+    planes, pts, comp = mg.grid_unknowns(c)
+    s = oracle.Solver(a, "grid", planes=planes, points=pts, comp=comp, method="multigrid",
+                      cells=class_table(c))
+    assert len(s.levels()) >= 2
+    x, it, res = s.solve(rhs, tol=1e-10)
+    xd, _ = oracle.direct_solve(a, c.xyz[c.free // 3], rhs)
+    assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
+
+
 @pytest.mark.gpu
 def test_gpu_box_cell_elastic_assembly_is_bit_identical():
     """Graded cells of 2 materials (isotropic and orthotropic) in the x and z directions: the
