@@ -79,6 +79,9 @@ def args():
                         "modes: 10 lowest modes of a 100x10x10 P2 beam; hexheat: the 128^3 "
                         "heat cube on box cells; hexbeam: a cantilever of 256x32x32 box cells "
                         "with incompatible modes (2 materials)")
+    p.add_argument("--by-cells", action="store_true",
+                   help="hexbeam: the coarse matrices from the cells, as the reference forms "
+                        "them (default: Galerkin products, fewer iterations here)")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
     p.add_argument("--rates", default="10,50,200,500",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
@@ -186,7 +189,8 @@ def build_system(opt):
         text = (f"elasticity on box cells with incompatible modes (the reference's box-grid "
                 f"elastic model), a {nx}x{ny}x{ny} cell cantilever 8x1x1, isotropic (E 1000, nu "
                 f"0.3) and orthotropic cells (seed {SEED}), clamped at x = 0, a tip load, 1 RHS "
-                f"to 1e-8, mixed precision PCG-MG")
+                f"to 1e-8, mixed precision PCG-MG, coarse matrices "
+                f"{'from the cells' if opt.by_cells else 'by Galerkin products'}")
     elif opt.workload == "p2beam":
         box = mg.box(200, 20, 20, (200.0, 20.0, 20.0))
         q = fg.Quadratic.new(box.points, box.tets)
@@ -219,12 +223,21 @@ def build_system(opt):
     else:
         planes, pts, comp = mg.grid_unknowns(prob)
         unknowns = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+        cells = None
+        if opt.workload == "hexbeam" and opt.by_cells:
+            # elastic.rs:518-537: the coarse matrices from the cells, as the reference solves
+            # its box-grid elastic models.
+            t0 = time.perf_counter()
+            origin, cls, keys = mg.hex_classes(prob)
+            cells = fg.Cells(origin, cls, fg.hex_elements(keys))
+            assemble_s += time.perf_counter() - t0
 
         def oracle_solver(Ao):
+            oc = None if cells is None else (cells.origin, cells.cls, cells.matrices)
             return oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp,
-                                 method="multigrid")
+                                 method="multigrid", cells=oc)
     facts = {"text": text, "tol": tol, "assemble_s": assemble_s, "reduce_s": reduce_s,
-             "oracle_solver": oracle_solver}
+             "oracle_solver": oracle_solver, "cells": cells if opt.workload != "p2beam" else None}
     return A, rhs, unknowns, facts
 
 
@@ -380,7 +393,7 @@ def run_ours(opt, rank, world, local):
 
     def make(precision):
         t = time.perf_counter()
-        s = fg.Solver(A, unknowns, fg.Method.Multigrid,
+        s = fg.Solver(A, unknowns, fg.Method.Multigrid, cells=facts["cells"],
                       options=fg.Options(precision=precision, format=opt.format,
                                          graph=opt.graph, tail=opt.tail,
                                          degree=opt.degree, launch=opt.launch,

@@ -10,8 +10,8 @@ The Python names mirror the reference crate: ``Csr`` (sparse.rs), ``Solver``, ``
 from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
                    P2_ELASTIC_ORTHO, P2_MASS, FemError, LIB_PATH, lib)
 from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT_LIMIT,
-                    Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
-                    prolongation, reduced_rhs)
+                    Cells, Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
+                    coarse_matrix, hex_elements, prolongation, reduced_rhs)
 from .recover import Peak, Recovery
 from .sparse import Csr, Rect, colour
 
@@ -19,7 +19,8 @@ __all__ = [
     "COLOUR", "FP64", "GATHER", "HEX8_ELASTIC", "HEX8_HEAT", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "P2_ELASTIC_ORTHO", "P2_MASS",
     "FemError",
     "LIB_PATH", "lib", "PCG_MAX_ITER", "PCG_TOL", "STEADY_DIRECT_LIMIT",
-    "TRANSIENT_DIRECT_LIMIT", "Crossover", "Level", "Method", "Options", "Quadratic", "Solver",
+    "TRANSIENT_DIRECT_LIMIT", "Cells", "Crossover", "Level", "Method", "Options", "Quadratic",
+    "Solver", "coarse_matrix", "hex_elements",
     "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
     "Recovery",
 ]

@@ -50,6 +50,11 @@ class Crossover_t(C.Structure):
                 ("entries", C.c_uint64), ("flat", C.c_int)]
 
 
+class Cells_t(C.Structure):
+    _fields_ = [("count", C.c_size_t), ("origin", C.c_void_p), ("cls", C.c_void_p),
+                ("matrices", C.c_void_p), ("nclass", C.c_size_t)]
+
+
 class Options_t(C.Structure):
     _fields_ = [("precision", C.c_int), ("degree", C.c_int), ("lower", C.c_double),
                 ("sell_c", C.c_int), ("sell_sigma", C.c_int), ("coarsest", C.c_int),
@@ -123,6 +128,13 @@ SIGNATURES = {
     "femgpu_solver_new": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.c_int,
                                     C.POINTER(Crossover_t), C.POINTER(Options_t),
                                     C.POINTER(C.c_void_p)]),
+    "femgpu_solver_new_cells": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.c_int,
+                                          C.POINTER(Crossover_t), C.POINTER(Options_t),
+                                          C.POINTER(Cells_t), C.POINTER(C.c_void_p)]),
+    "femgpu_hex_elements": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p]),
+    "femgpu_coarse_matrix": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.POINTER(Cells_t),
+                                       C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                       C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_solver_set_max_iter": (C.c_int, [C.c_void_p, C.c_size_t]),
     "femgpu_solver_set_tol": (C.c_int, [C.c_void_p, C.c_double]),
     "femgpu_solver_method": (C.c_int, [C.c_void_p]),

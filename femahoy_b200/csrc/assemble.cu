@@ -686,6 +686,15 @@ __global__ void __launch_bounds__(32 * WARPS)
     }
 }
 
+void hex_elements(const double* d_keys, int64_t n, double* d_table, cudaStream_t s) {
+    DevBuf<int> bad(1);
+    bad.zero(s);
+    k_hex_condense<<<(unsigned)std::min<int64_t>(n, NUM_SMS * 16), HEX_THREADS, 0, s>>>(
+        d_keys, n, d_table, bad.p);
+    FG_CHECK_LAUNCH();
+    assembly_flag(fetch(bad.p, s));
+}
+
 // The classes of the cells: the cells in order, each compared with the last new class first
 // (a grid's neighbours mostly share it), then looked up by its 12 words.
 struct KeyHash {
@@ -1056,7 +1065,10 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
             FG_CHECK_LAUNCH();
         }
     }
-    int b = fetch(bad.p, s);
+    assembly_flag(fetch(bad.p, s));
+}
+
+void assembly_flag(int b) {
     if (b == 1) throw Failure(FEMGPU_ERR_PATTERN, "the pattern holds each element pair");
     if (b == 2)
         throw Failure(FEMGPU_ERR_MATERIAL,

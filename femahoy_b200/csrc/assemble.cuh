@@ -35,5 +35,10 @@ void submatrix(const DevCsr& a, const int64_t* d_keep, int64_t nkeep, DevCsr* ou
 void reduced_rhs(const DevCsr& a, const double* d_load, const double* d_t, const int64_t* d_free,
                  int64_t nfree, double* d_out, cudaStream_t s);
 void csr_mul(const DevCsr& a, const double* d_x, double* d_y, cudaStream_t s);
+// Hex::new (hex.rs:218-297) for `n` box cells given by their 12 numbers each (the 3 sides, the
+// 9 orthotropic constants): 576 values per cell into d_table.
+void hex_elements(const double* d_keys, int64_t n, double* d_table, cudaStream_t s);
+// Throws the error of an assembly's device flag (0: none).
+void assembly_flag(int b);
 
 }  // namespace femgpu

@@ -264,9 +264,106 @@ int femgpu_prolongation(size_t npoints, const double* points, size_t corners, si
     });
 }
 
+static HostCells host_cells(const femgpu_cells* c, const femgpu_unknowns* u) {
+    HostCells h;
+    if (!c || !c->count) return h;
+    require(u->kind == FEMGPU_UNKNOWNS_GRID, "cells need grid unknowns");
+    require(c->origin && c->cls && c->matrices && c->nclass > 0, "a null cell array");
+    h.origin.resize(c->count);
+    for (size_t i = 0; i < c->count; ++i) {
+        for (int d = 0; d < 3; ++d) {
+            require(c->origin[3 * i + d] + 1 < u->nplanes[d], "a cell past the planes");
+            h.origin[i][d] = c->origin[3 * i + d];
+        }
+        require(c->cls[i] < c->nclass, "a cell class past the matrices");
+    }
+    h.cls.assign(c->cls, c->cls + c->count);
+    h.table.assign(c->matrices, c->matrices + 576 * c->nclass);
+    return h;
+}
+
+static HostLevel host_level(const femgpu_unknowns* u, int64_t n) {
+    require(u->points && u->comp, "a grid level needs its points and components");
+    HostLevel lv;
+    for (int d = 0; d < 3; ++d) {
+        require(u->planes[d] && u->nplanes[d] > 0, "empty planes");
+        lv.planes[d].assign(u->planes[d], u->planes[d] + u->nplanes[d]);
+    }
+    lv.points.resize(n);
+    for (int64_t k = 0; k < n; ++k)
+        for (int d = 0; d < 3; ++d) {
+            require(u->points[3 * k + d] < u->nplanes[d], "a grid point past its planes");
+            lv.points[k][d] = u->points[3 * k + d];
+        }
+    lv.comp.assign(u->comp, u->comp + n);
+    return lv;
+}
+
+static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int method,
+                           const femgpu_crossover* crossover, const femgpu_options* options,
+                           const femgpu_cells* cells, femgpu_solver** out);
+
 int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
                       const femgpu_crossover* crossover, const femgpu_options* options,
                       femgpu_solver** out) {
+    return solver_new_impl(a, u, method, crossover, options, nullptr, out);
+}
+
+int femgpu_solver_new_cells(const femgpu_csr* a, const femgpu_unknowns* u, int method,
+                            const femgpu_crossover* crossover, const femgpu_options* options,
+                            const femgpu_cells* cells, femgpu_solver** out) {
+    return solver_new_impl(a, u, method, crossover, options, cells, out);
+}
+
+int femgpu_hex_elements(size_t count, const double* keys, double* matrices) {
+    return guarded([&] {
+        require(count > 0 && keys && matrices, "null or empty cell keys");
+        cudaStream_t s = util_stream();
+        DevBuf<double> dk, dt(576 * count);
+        dk.upload(keys, 12 * count, s);
+        hex_elements(dk.p, (int64_t)count, dt.p, s);
+        dt.download(matrices, 576 * count, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int femgpu_coarse_matrix(const femgpu_csr* a, const femgpu_unknowns* u,
+                         const femgpu_cells* cells, int level, size_t* n, size_t* nnz,
+                         int64_t* ptr, uint32_t* idx, double* val) {
+    return guarded([&] {
+        require(a && u && n && nnz, "null argument");
+        require(u->kind == FEMGPU_UNKNOWNS_GRID, "coarse matrices need grid unknowns");
+        require(level >= 1, "level 1 is the first coarse level");
+        HostCsr m = download_csr(a->m, util_stream());
+        HostLevel lv = host_level(u, m.n);
+        HostCells stored, first = host_cells(cells, u);
+        const int threads = host_threads();
+        for (int l = 1; l <= level; ++l) {
+            HostRect p;
+            HostLevel coarse;
+            require(coarsen(lv, m, &p, &coarse), "the grid does not coarsen that far");
+            if (!first.empty()) {
+                HostCells nxt;
+                m = by_cells(lv, stored.empty() ? first : stored, coarse, &nxt, threads);
+                stored = std::move(nxt);
+            } else {
+                m = galerkin(p, m, threads);
+            }
+            lv = std::move(coarse);
+        }
+        *n = (size_t)m.n;
+        *nnz = (size_t)m.nnz();
+        if (!ptr) return;
+        require(idx && val, "null output arrays");
+        std::copy(m.ptr.begin(), m.ptr.end(), ptr);
+        std::copy(m.idx.begin(), m.idx.end(), idx);
+        std::copy(m.val.begin(), m.val.end(), val);
+    });
+}
+
+static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int method,
+                           const femgpu_crossover* crossover, const femgpu_options* options,
+                           const femgpu_cells* cells, femgpu_solver** out) {
     return guarded([&] {
         require(a && u && out, "null argument");
         require(method >= -1 && method <= 1, "unknown method");
@@ -311,9 +408,10 @@ int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* u, int method,
         } else {
             throw Failure(FEMGPU_ERR_INVALID, "unknown unknowns kind");
         }
+        HostCells hc = host_cells(cells, u);
         auto* s = new femgpu_solver;
         try {
-            s->impl.create(a->m, *u, method, c, o);
+            s->impl.create(a->m, *u, method, c, o, hc.empty() ? nullptr : &hc);
         } catch (...) {
             delete s;
             throw;

@@ -43,6 +43,26 @@ void renumber_grid_order(HostRect* p, HostLevel* coarse);
 // `threads` host threads.
 HostCsr galerkin(const HostRect& p, const HostCsr& a, int threads);
 
+// multigrid.rs:62-68 `Cells`: the cells of a box-grid displacement level, each by its lowest
+// grid point and the class of its 24 x 24 matrix (row-major, unknown 3 n + c for corner n in
+// VTK order): matrix i is table + 576 cls[i].
+struct HostCells {
+    std::vector<std::array<uint32_t, 3>> origin;
+    std::vector<uint32_t> cls;
+    std::vector<double> table;
+    bool empty() const { return origin.empty(); }
+};
+
+// multigrid.rs:458-608: the coarse matrix of a displacement from its cells. Each coarse cell
+// sums the energy of its fine cells for its 8 trilinear corner fields and its 9 incompatible
+// modes (those that the Gram factor of the fields at the free fine unknowns keeps,
+// multigrid.rs:616-652) and condenses the modes (multigrid.rs:654-681); the coarse cells are
+// assembled on the unknowns of `coarse`. `next` gets the coarse cells for the next level. The
+// coarse cells' matrices are formed on `threads` host threads; the fine cells of a coarse cell
+// are summed in increasing order.
+HostCsr by_cells(const HostLevel& fine, const HostCells& cells, const HostLevel& coarse,
+                 HostCells* next, int threads);
+
 // pmultigrid.rs:104-151
 void prolongation(const double* points, int64_t npoints, int64_t corners, const uint32_t* edges,
                   int64_t nedges, const int64_t* free, int64_t nfree, HostRect* p,

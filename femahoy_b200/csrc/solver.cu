@@ -1537,7 +1537,7 @@ void SolverImpl::phase(const std::string& name, double seconds) {
 }
 
 void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
-                        const femgpu_crossover& c, const Options& o) {
+                        const femgpu_crossover& c, const Options& o, const HostCells* cells) {
     opt_ = o;
     pdl_ = o.pdl != 0;
     n_ = a.n;
@@ -1601,7 +1601,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         for (int64_t k = 0; k < n_; ++k)
             for (int d = 0; d < 3; ++d) lv.points[k][d] = u.points[3 * k + d];
         lv.comp.assign(u.comp, u.comp + n_);
-        build_multigrid(std::move(h), std::move(lv), nullptr);
+        build_multigrid(std::move(h), std::move(lv), nullptr, cells);
     } else {
         // p-multigrid (pmultigrid.rs:46-98): the first coarse level is P^T A P on the corners,
         // then geometric levels on the grid of the corner points.
@@ -1612,7 +1612,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         p.idx.assign(u.p_idx, u.p_idx + p.ptr[n_]);
         p.val.assign(u.p_val, u.p_val + p.ptr[n_]);
         HostLevel lv = level_of_points(u.coarse_xyz, p.cols, u.coarse_comp);
-        build_multigrid(std::move(h), std::move(lv), &p);
+        build_multigrid(std::move(h), std::move(lv), &p, nullptr);
     }
 }
 
@@ -1846,9 +1846,11 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
     build_tail(H, opt_.tail, s_);
 }
 
-void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst) {
-    // multigrid.rs:84-139 (the Galerkin form): coarsen until a level has at most `coarsest`
-    // unknowns, 30 levels, or a coarsening keeps more than 90 % of the unknowns.
+void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
+                                 const HostCells* cells) {
+    // multigrid.rs:84-139: coarsen until a level has at most `coarsest` unknowns, 30 levels, or
+    // a coarsening keeps more than 90 % of the unknowns. The coarse matrices are the Galerkin
+    // products, or with cells the cell-condensed matrices (each level's cells from the last).
     std::vector<HostCsr> mats;
     std::vector<HostRect> ps;
     int threads = host_threads();
@@ -1860,6 +1862,7 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
     }
     size_t coarsest = (size_t)(opt_.coarsest > 0 ? opt_.coarsest : DEVICE_COARSEST);
     size_t max_levels = (size_t)(opt_.max_levels > 0 ? opt_.max_levels : 30);
+    HostCells stored;  // the cells of the last coarse level
     for (;;) {
         const HostCsr& a = mats.back();
         if ((size_t)a.n <= coarsest || ps.size() >= max_levels) break;
@@ -1871,8 +1874,16 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
             if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
             if (opt_.format == 0) renumber_grid_order(&p, &coarse);
         }
-        PhaseTimer t_g{this, "Galerkin products (host)", s_};
-        HostCsr ac = galerkin(p, a, threads);
+        HostCsr ac;
+        if (cells && !cells->empty()) {
+            PhaseTimer t_c{this, "coarse matrices from the cells (host)", s_};
+            HostCells nxt;
+            ac = by_cells(level, stored.empty() ? *cells : stored, coarse, &nxt, threads);
+            stored = std::move(nxt);
+        } else {
+            PhaseTimer t_g{this, "Galerkin products (host)", s_};
+            ac = galerkin(p, a, threads);
+        }
         mats.push_back(std::move(ac));
         ps.push_back(std::move(p));
         level = std::move(coarse);

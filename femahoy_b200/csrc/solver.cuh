@@ -219,8 +219,10 @@ class SolverImpl {
     SolverImpl();
     ~SolverImpl();
     // solve.rs:92-183
+    // `cells` (may be null): the cells of a box-grid displacement model, whose coarse matrices
+    // then come from the cells (multigrid.rs:107-119).
     void create(const DevCsr& a, const femgpu_unknowns& u, int method, const femgpu_crossover& c,
-                const Options& o);
+                const Options& o, const HostCells* cells = nullptr);
     // solve.rs:199-250 on device vectors
     void solve(const double* d_b, double* d_x, const volatile int* cancel, femgpu_stats* st);
     void solve_host(const double* h_b, double* h_x, const volatile int* cancel, femgpu_stats* st);
@@ -242,7 +244,8 @@ class SolverImpl {
     void phase(const std::string& name, double seconds);
 
    private:
-    void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst);
+    void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
+                         const HostCells* cells);
     template <class T>
     void build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps, Hierarchy<T>* H);
     template <class T>

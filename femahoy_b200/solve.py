@@ -156,14 +156,58 @@ def unknowns_c(unknowns: "Unknowns", keep: list) -> L.Unknowns_t:
     return u
 
 
+@dataclass
+class Cells:
+    """multigrid.rs:62-68: the box cells of a displacement model on grid unknowns, each by its
+    lowest grid point ``origin`` (C, 3) and the class ``cls`` (C,) of its 24 x 24 matrix among
+    ``matrices`` (K, 24, 24) (unknown 3 n + c for corner n in VTK order)."""
+
+    origin: np.ndarray
+    cls: np.ndarray
+    matrices: np.ndarray
+
+    def _c(self, keep):
+        o = L.arr(self.origin, np.uint32).reshape(-1, 3)
+        c = L.arr(self.cls, np.uint32).ravel()
+        m = L.arr(self.matrices, np.float64).reshape(-1, 576)
+        keep += [o, c, m]
+        return L.Cells_t(len(o), o.ctypes.data, c.ctypes.data, m.ctypes.data, len(m))
+
+
+def hex_elements(keys):
+    """Hex::new (hex.rs:218-297) on the device for each row of ``keys`` (K, 12): the 3 sides and
+    the 9 orthotropic constants of a box cell. Returns (K, 24, 24)."""
+    k = L.arr(keys, np.float64).reshape(-1, 12)
+    out = np.empty((len(k), 24, 24))
+    L.check(L.lib().femgpu_hex_elements(len(k), k.ctypes.data, out.ctypes.data))
+    return out
+
+
+def coarse_matrix(a: Csr, unknowns: Unknowns, level: int, cells: Cells | None = None):
+    """The matrix (ptr, idx, val) of multigrid level ``level`` as the solver forms it (the
+    Galerkin products, or with ``cells`` the cell-condensed matrices), its unknowns numbered as
+    multigrid.rs:329-452 numbers them."""
+    keep = []
+    u = unknowns_c(unknowns, keep)
+    cc = C.byref(cells._c(keep)) if cells is not None else None
+    n, nnz = C.c_size_t(), C.c_size_t()
+    L.check(L.lib().femgpu_coarse_matrix(a.handle, C.byref(u), cc, level, C.byref(n),
+                                         C.byref(nnz), None, None, None))
+    ptr = np.empty(n.value + 1, np.int64)
+    idx = np.empty(nnz.value, np.uint32)
+    val = np.empty(nnz.value, np.float64)
+    L.check(L.lib().femgpu_coarse_matrix(a.handle, C.byref(u), cc, level, C.byref(n),
+                                         C.byref(nnz), ptr.ctypes.data, idx.ctypes.data,
+                                         val.ctypes.data))
+    return ptr, idx, val
+
+
 class Solver:
     """solve.rs:58-250 on the device."""
 
     def __init__(self, a: Csr, unknowns: Unknowns, method: Method | None = None,
-                 crossover: Crossover | None = None, cells=None, *, precision=L.FP64,
-                 options: Options | None = None):
-        if cells is not None:
-            raise L.FemError(L.INVALID, "cells (hex elasticity) are outside this library")
+                 crossover: Crossover | None = None, cells: Cells | None = None, *,
+                 precision=L.FP64, options: Options | None = None):
         crossover = crossover or Crossover.Unknowns(STEADY_DIRECT_LIMIT)
         opts = options or Options()
         opts.precision = precision if options is None else opts.precision
@@ -174,8 +218,9 @@ class Solver:
         h = C.c_void_p()
         cr = crossover._c()
         oc = opts._c()
-        L.check(L.lib().femgpu_solver_new(a.handle, C.byref(u), m, C.byref(cr), C.byref(oc),
-                                          C.byref(h)))
+        cc = C.byref(cells._c(keep)) if cells is not None else None
+        L.check(L.lib().femgpu_solver_new_cells(a.handle, C.byref(u), m, C.byref(cr),
+                                                C.byref(oc), cc, C.byref(h)))
         self._h = h.value
         self.n = n
 

@@ -243,12 +243,43 @@ typedef struct femgpu_stats {
     size_t launches;       /* kernels this library launched for the solve */
 } femgpu_stats;
 
-/* Solver::new (solve.rs:92-183). The solver keeps a copy of `a` on the device (the reference
- * moves `a` in). `a` may be freed after the call. `cells` (hex elasticity, multigrid.rs:62-68)
- * is not supported: box-grid hex elements are outside this library. */
+/* multigrid.rs:62-68 `Cells`: the box cells of a displacement model on grid unknowns, each by
+ * its lowest grid point `origin` (3 values per cell) and its 24 x 24 matrix (row-major, unknown
+ * 3 n + c for corner n in VTK order and component c), given by class: cell i has the matrix
+ * matrices + 576 cls[i] (a per-cell table is cls[i] = i). The reference's `element` closure
+ * gives Hex::new per cell (elastic.rs:499-521); femgpu_hex_elements makes the class matrices. */
+typedef struct femgpu_cells {
+    size_t count;
+    const uint32_t* origin;
+    const uint32_t* cls;
+    const double* matrices;
+    size_t nclass;
+} femgpu_cells;
+
+/* Solver::new (solve.rs:92-183) with `cells` = None. The solver keeps a copy of `a` on the
+ * device (the reference moves `a` in). `a` may be freed after the call. */
 int femgpu_solver_new(const femgpu_csr* a, const femgpu_unknowns* unknowns, int method,
                       const femgpu_crossover* crossover, const femgpu_options* options,
                       femgpu_solver** out);
+/* Solver::new with `cells` (may be null): grid unknowns whose multigrid coarse matrices come
+ * from the cells (multigrid.rs:107-119, 458-608) instead of the Galerkin products. The cell
+ * arrays may be freed after the call. */
+int femgpu_solver_new_cells(const femgpu_csr* a, const femgpu_unknowns* unknowns, int method,
+                            const femgpu_crossover* crossover, const femgpu_options* options,
+                            const femgpu_cells* cells, femgpu_solver** out);
+/* Hex::new (hex.rs:218-297) of `count` box cells on the device: `keys` holds 12 values per cell
+ * (its 3 sides, then the 9 orthotropic constants of FEMGPU_P2_ELASTIC_ORTHO); `matrices` gets
+ * the condensed 24 x 24 stiffness of each (576 values, row-major), bit-identical with the
+ * reference's. */
+int femgpu_hex_elements(size_t count, const double* keys, double* matrices);
+/* The matrix of multigrid level `level` (>= 1) that the solver of (a, unknowns, cells) forms
+ * (cells may be null: the Galerkin products), with the coarse unknowns in the reference's
+ * numbering of multigrid.rs:329-452; `level` coarsenings regardless of the size limits. Two
+ * calls: with null arrays it writes n and nnz; then the CSR arrays. No reference counterpart:
+ * for checking the hierarchy against the reference. */
+int femgpu_coarse_matrix(const femgpu_csr* a, const femgpu_unknowns* unknowns,
+                         const femgpu_cells* cells, int level, size_t* n, size_t* nnz,
+                         int64_t* ptr, uint32_t* idx, double* val);
 /* Solver::with_max_iter (solve.rs:187-189). */
 int femgpu_solver_set_max_iter(femgpu_solver* s, size_t max_iter);
 /* The relative residual of each PCG solve; PCG_TOL = 1e-10 (solve.rs:42) by default. */

@@ -200,3 +200,77 @@ def test_gpu_box_cantilever_solves(precision):
     xd, _ = oracle.direct_solve(Ko.submatrix(c.free), c.xyz[c.free // 3],
                                 Ko.reduced_rhs(c.load, c.values, c.free))
     assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
+
+
+def cells_of(c, fg):
+    """The device's cells of a box-cell problem: the class matrices from femgpu_hex_elements."""
+    origin, cls, keys = mg.hex_classes(c)
+    return fg.Cells(origin, cls, fg.hex_elements(keys)), keys
+
+
+@pytest.mark.gpu
+def test_gpu_hex_elements_are_bit_identical():
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=6, ny=2, nz=3, grade=1.4, seed=11)
+    cells, keys = cells_of(c, fg)
+    want = np.stack([oracle.hex8_stiffness(k[:3], k[3:]) for k in keys])
+    assert np.array_equal(cells.matrices.view(np.uint64), want.view(np.uint64))
+    with pytest.raises(fg.FemError, match="side not above 0"):
+        bad = keys[:1].copy()
+        bad[0, 1] = 0.0
+        fg.hex_elements(bad)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level", [1, 2])
+def test_gpu_coarse_matrices_from_cells_are_bit_identical(level):
+    """multigrid.rs:458-608: the library's coarse matrices (host threads) equal the oracle's bit
+    for bit on a graded cantilever of 2 materials; level 2 is formed from level 1's cells."""
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=64, ny=8, nz=12, length=8.0, width=1.0, depth=1.5, load=-1.0,
+                          grade=1.3, seed=9)
+    K = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef)
+    A = K.submatrix(c.free)
+    planes, pts, comp = mg.grid_unknowns(c)
+    cells, _ = cells_of(c, fg)
+    got = fg.coarse_matrix(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), level, cells)
+    Ko = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    Ko.assemble(6, c.xyz, c.nodes, c.coef)
+    so = oracle.Solver(Ko.submatrix(c.free), "grid", planes=planes, points=pts, comp=comp,
+                       method="multigrid", cells=class_table(c))
+    want = so.level_matrix(level).arrays()
+    for a, b in zip(got, want):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    # The Galerkin form through the same entry, against the oracle's P^T A P.
+    gal = fg.coarse_matrix(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), 1)
+    sg = oracle.Solver(Ko.submatrix(c.free), "grid", planes=planes, points=pts, comp=comp,
+                       method="multigrid")
+    for a, b in zip(gal, sg.level_matrix(1).arrays()):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_box_cantilever_solves_with_cells(precision):
+    """PCG with the cell-based V-cycle (the reference's box-grid elastic solver) against the
+    oracle's direct solution (1e-8 relative) and its own true residual."""
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=48, ny=6, nz=6, length=6.0, width=0.75, depth=0.75, load=-1.0,
+                          grade=1.1, seed=3)
+    K = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef)
+    A = K.submatrix(c.free)
+    rhs = fg.reduced_rhs(K, c.load, c.values, c.free)
+    planes, pts, comp = mg.grid_unknowns(c)
+    cells, _ = cells_of(c, fg)
+    s = fg.Solver(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), fg.Method.Multigrid,
+                  cells=cells, precision=precision,
+                  options=fg.Options(precision=precision, coarsest=600)).with_tol(1e-10)
+    assert len(s.levels()) >= 2
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    assert st.true_residual <= 1.2e-10
+    Ko = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    Ko.assemble(6, c.xyz, c.nodes, c.coef)
+    xd, _ = oracle.direct_solve(Ko.submatrix(c.free), c.xyz[c.free // 3],
+                                Ko.reduced_rhs(c.load, c.values, c.free))
+    assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
