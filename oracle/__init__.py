@@ -47,6 +47,9 @@ def _load():
         "orc_isotropic": (I, [D, D, P, P, P, S]),
         "orc_element_matrix": (I, [I, P, P, P]),
         "orc_hex8_stiffness": (I, [P, P, P, P, S]),
+        "orc_hex8_element": (I, [P, P, P, P, P, P, P, P, S]),
+        "orc_hex8_strain_stress": (I, [P, P, P, P, P, P, P, P, P, S]),
+        "orc_recover_hex": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
         "orc_assemble": (I, [P, I, P, P, S, P, P, S]),
         "orc_quadratic": (S, [P, S, P, S, P, P]),
         "orc_colour": (I, [S, P, S, I, P]),
@@ -277,11 +280,35 @@ class Peak(C.Structure):
                 ("regular_local", C.c_int32), ("regular_point", C.c_uint32)]
 
 
+def hex8_element(size, c, alpha=(0.0, 0.0, 0.0)):
+    """hex.rs:218-309: (k (24, 24), load (24, 8), mode_u (9, 24), mode_t (9, 8)) of a box
+    cell."""
+    size, c, alpha = (np.ascontiguousarray(v, dtype=np.float64) for v in (size, c, alpha))
+    k, load, mu, mt = np.empty(576), np.empty(192), np.empty(216), np.empty(72)
+    err = C.create_string_buffer(512)
+    if _lib.orc_hex8_element(_p(size), _p(c), _p(alpha), _p(k), _p(load), _p(mu), _p(mt), err,
+                             512):
+        raise OracleError(err.value.decode())
+    return k.reshape(24, 24), load.reshape(24, 8), mu.reshape(9, 24), mt.reshape(9, 8)
+
+
+def hex8_strain_stress(size, c, xi, u, t, alpha=(0.0, 0.0, 0.0)):
+    """hex.rs:311-335: (engineering strain, stress), both xx, yy, zz, yz, xz, xy."""
+    a = [np.ascontiguousarray(v, dtype=np.float64) for v in (size, c, alpha, xi, u, t)]
+    e, s = np.empty(6), np.empty(6)
+    err = C.create_string_buffer(512)
+    if _lib.orc_hex8_strain_stress(*[_p(v) for v in a], _p(e), _p(s), err, 512):
+        raise OracleError(err.value.decode())
+    return e, s
+
+
 def recover(xyz, tets10, coef, u, *, expansion=None, dtemp=None, part=None, nparts=1,
-            singular=None):
+            singular=None, hex=False):
     """elastic_tet.rs:367-427 and 482-483: the mean strain and stress at each point of the
     quadratic mesh, their von Mises and principal stresses, and the peaks of each part. Returns a
-    dict of arrays: stress (n, 6), strain (n, 6), mises (n,), principal (n, 3), peaks (list)."""
+    dict of arrays: stress (n, 6), strain (n, 6), mises (n,), principal (n, 3), peaks (list).
+    ``hex``: the box grid's loop (elastic.rs:615-660) over box cells (``tets10`` then holds 8
+    corners per cell and ``coef`` 9 orthotropic constants per cell)."""
     xyz = np.ascontiguousarray(xyz, dtype=np.float64)
     t10 = np.ascontiguousarray(tets10, dtype=np.uint32)
     coef = np.ascontiguousarray(coef, dtype=np.float64)
@@ -294,9 +321,10 @@ def recover(xyz, tets10, coef, u, *, expansion=None, dtemp=None, part=None, npar
     mises, principal = np.empty(n), np.empty((n, 3))
     peaks = (Peak * nparts)()
     err = C.create_string_buffer(512)
-    st = _lib.orc_recover(n, _p(xyz), len(t10), _p(t10), _p(coef), _p(expansion), _p(dtemp),
-                          _p(u), _p(part), nparts, _p(singular), _p(stress), _p(strain),
-                          _p(mises), _p(principal), C.cast(peaks, C.c_void_p), err, 512)
+    fn = _lib.orc_recover_hex if hex else _lib.orc_recover
+    st = fn(n, _p(xyz), len(t10), _p(t10), _p(coef), _p(expansion), _p(dtemp),
+            _p(u), _p(part), nparts, _p(singular), _p(stress), _p(strain),
+            _p(mises), _p(principal), C.cast(peaks, C.c_void_p), err, 512)
     if st:
         raise OracleError(err.value.decode())
     return {"stress": stress, "strain": strain, "mises": mises, "principal": principal,

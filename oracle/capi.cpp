@@ -519,5 +519,50 @@ int orc_recover(size_t npoints, const double* xyz, size_t nel, const uint32_t* t
         return -1;
     }
 }
+// elastic.rs:615-660 and 709-710 (see recover_hex8), as orc_recover.
+int orc_recover_hex(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                    const double* coef, const double* expansion, const double* dtemp,
+                    const double* u, const uint32_t* part, size_t nparts, const uint8_t* singular,
+                    double* stress, double* strain, double* mises_out, double* principal_out,
+                    void* peaks, char* err, size_t len) {
+    try {
+        recover_hex8(npoints, xyz, nel, hexes, coef, expansion, dtemp, u, part, nparts, singular,
+                     stress, strain, mises_out, principal_out, static_cast<RecoveryPeak*>(peaks));
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+// hex.rs:218-335 for 1 box cell: its load (24 x 8) and mode matrices (9 x 24, 9 x 8), and the
+// strain and stress at xi for the corner values u and t.
+int orc_hex8_element(const double* size, const double* c, const double* alpha, double* k,
+                     double* load, double* mode_u, double* mode_t, char* err, size_t len) {
+    try {
+        HexElement h;
+        hex8_element(size, orthotropic_stiffness(c, c + 3, c + 6), alpha, &h);
+        std::memcpy(k, h.k, sizeof(h.k));
+        std::memcpy(load, h.load, sizeof(h.load));
+        std::memcpy(mode_u, h.mode_u, sizeof(h.mode_u));
+        std::memcpy(mode_t, h.mode_t, sizeof(h.mode_t));
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
+int orc_hex8_strain_stress(const double* size, const double* c, const double* alpha,
+                           const double* xi, const double* u, const double* t, double* e,
+                           double* s, char* err, size_t len) {
+    try {
+        HexElement h;
+        hex8_element(size, orthotropic_stiffness(c, c + 3, c + 6), alpha, &h);
+        hex8_strain_stress(h, xi, u, t, e, s);
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
 
 }  // extern "C"

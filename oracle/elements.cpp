@@ -333,59 +333,137 @@ static void hex_gradients(const double size[3], const double xi[3], double g[11]
     for (int d = 0; d < 3; ++d) g[8 + d][d] = -4.0 * xi[d] / size[d];
 }
 
-// hex.rs:218-297 (the stiffness part of Hex::new): the 33 x 33 matrix of the 8 corner and 3 mode
-// functions over the 2-point Gauss rule, then the 9 modes condensed with the Cholesky factor of
-// their block (hex.rs:355-389): the 24 x 24 stiffness of the corners, row-major.
-void hex8_stiffness(const double size[3], const Stiffness& d, double kc[576]) {
+// hex.rs:164-178: the values of the 8 corner functions at xi (a product from 1.0).
+static void hex_shape(const double xi[3], double n[8]) {
     static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
                                    {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
-    double k[33][33];
-    for (int i = 0; i < 33; ++i)
+    for (int c = 0; c < 8; ++c) {
+        double v = 1.0;
+        for (int d = 0; d < 3; ++d) v *= BITS[c][d] == 1 ? 0.5 * (1.0 + xi[d]) : 0.5 * (1.0 - xi[d]);
+        n[c] = v;
+    }
+}
+
+// hex.rs:218-309: Hex::new. The 33 x 33 stiffness and the 33 x 8 thermal load of the 8 corner
+// and 3 mode functions over the 2-point Gauss rule, then the 9 modes condensed with the Cholesky
+// factor of their block (hex.rs:355-389).
+void hex8_element(const double size[3], const Stiffness& d, const double alpha[3], HexElement* h) {
+    static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int d3 = 0; d3 < 3; ++d3) h->size[d3] = size[d3];
+    h->d = d;
+    for (int i = 0; i < 3; ++i) {  // the Rust float sum starts from -0.0
+        double s = -0.0;
+        for (int j = 0; j < 3; ++j) s += d.normal[i][j] * alpha[j];
+        h->thermal[i] = s;
+    }
+    double k[33][33], l[33][8];
+    for (int i = 0; i < 33; ++i) {
         for (int j = 0; j < 33; ++j) k[i][j] = 0.0;
+        for (int c = 0; c < 8; ++c) l[i][c] = 0.0;
+    }
     const double jac = size[0] * size[1] * size[2] / 8.0;
     const double p = 1.0 / std::sqrt(3.0);
     for (int gp = 0; gp < 8; ++gp) {
-        double xi[3], g[11][3];
+        double xi[3], g[11][3], n[8];
         for (int e = 0; e < 3; ++e) xi[e] = BITS[gp][e] == 1 ? p : -p;
         hex_gradients(size, xi, g);
-        for (int i = 0; i < 11; ++i)
+        hex_shape(xi, n);
+        for (int i = 0; i < 11; ++i) {
             for (int j = 0; j < 11; ++j)
                 for (int a = 0; a < 3; ++a)
                     for (int b = 0; b < 3; ++b)
                         k[3 * i + a][3 * j + b] += jac * elastic_term(g[i], g[j], a, b, d);
+            for (int a = 0; a < 3; ++a)
+                for (int c = 0; c < 8; ++c) l[3 * i + a][c] += jac * g[i][a] * h->thermal[a] * n[c];
+        }
     }
-    double l[9][9] = {};
+    double ch[9][9] = {};
     for (int j = 0; j < 9; ++j) {  // cholesky9
         double dd = k[24 + j][24 + j];
-        for (int c = 0; c < j; ++c) dd -= l[j][c] * l[j][c];
+        for (int c = 0; c < j; ++c) dd -= ch[j][c] * ch[j][c];
         dd = std::sqrt(dd);
-        l[j][j] = dd;
+        ch[j][j] = dd;
         for (int i = j + 1; i < 9; ++i) {
             double v = k[24 + i][24 + j];
-            for (int c = 0; c < j; ++c) v -= l[i][c] * l[j][c];
-            l[i][j] = v / dd;
+            for (int c = 0; c < j; ++c) v -= ch[i][c] * ch[j][c];
+            ch[i][j] = v / dd;
         }
     }
-    double mode[9][24];
-    for (int c = 0; c < 24; ++c) {  // solve9 on each column of K_mu
-        double b[9];
-        for (int i = 0; i < 9; ++i) b[i] = k[24 + i][c];
+    auto solve9 = [&](double b[9]) {
         for (int i = 0; i < 9; ++i) {
-            for (int q = 0; q < i; ++q) b[i] -= l[i][q] * b[q];
-            b[i] /= l[i][i];
+            for (int q = 0; q < i; ++q) b[i] -= ch[i][q] * b[q];
+            b[i] /= ch[i][i];
         }
         for (int i = 8; i >= 0; --i) {
-            for (int q = i + 1; q < 9; ++q) b[i] -= l[q][i] * b[q];
-            b[i] /= l[i][i];
+            for (int q = i + 1; q < 9; ++q) b[i] -= ch[q][i] * b[q];
+            b[i] /= ch[i][i];
         }
-        for (int i = 0; i < 9; ++i) mode[i][c] = b[i];
+    };
+    for (int c = 0; c < 24; ++c) {
+        double b[9];
+        for (int i = 0; i < 9; ++i) b[i] = k[24 + i][c];
+        solve9(b);
+        for (int i = 0; i < 9; ++i) h->mode_u[i * 24 + c] = b[i];
     }
-    for (int r = 0; r < 24; ++r)
+    for (int c = 0; c < 8; ++c) {
+        double b[9];
+        for (int i = 0; i < 9; ++i) b[i] = l[24 + i][c];
+        solve9(b);
+        for (int i = 0; i < 9; ++i) h->mode_t[i * 8 + c] = b[i];
+    }
+    for (int r = 0; r < 24; ++r) {
         for (int c = 0; c < 24; ++c) {
             double v = k[r][c];
-            for (int i = 0; i < 9; ++i) v -= k[r][24 + i] * mode[i][c];
-            kc[r * 24 + c] = v;
+            for (int i = 0; i < 9; ++i) v -= k[r][24 + i] * h->mode_u[i * 24 + c];
+            h->k[r * 24 + c] = v;
         }
+        for (int c = 0; c < 8; ++c) {
+            double v = l[r][c];
+            for (int i = 0; i < 9; ++i) v -= k[r][24 + i] * h->mode_t[i * 8 + c];
+            h->load[r * 8 + c] = v;
+        }
+    }
+}
+
+void hex8_stiffness(const double size[3], const Stiffness& d, double kc[576]) {
+    const double zero[3] = {0.0, 0.0, 0.0};
+    HexElement h;
+    hex8_element(size, d, zero, &h);
+    for (int i = 0; i < 576; ++i) kc[i] = h.k[i];
+}
+
+// hex.rs:311-335: the engineering strain and the stress (xx, yy, zz, yz, xz, xy) at the local
+// point xi from the corner displacements u and the corner temperature changes t.
+void hex8_strain_stress(const HexElement& h, const double xi[3], const double u[24],
+                        const double t[8], double e[6], double s[6]) {
+    static const int SH[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+    double all[11][3];
+    for (int n = 0; n < 8; ++n)
+        for (int a = 0; a < 3; ++a) all[n][a] = u[3 * n + a];
+    for (int i = 0; i < 9; ++i) {
+        double a = 0.0;
+        for (int c = 0; c < 8; ++c) a += h.mode_t[i * 8 + c] * t[c];
+        for (int c = 0; c < 24; ++c) a -= h.mode_u[i * 24 + c] * u[c];
+        all[8 + i / 3][i % 3] = a;
+    }
+    double g[11][3], n[8];
+    hex_gradients(h.size, xi, g);
+    for (int a = 0; a < 6; ++a) e[a] = 0.0;
+    for (int i = 0; i < 11; ++i) {
+        for (int a = 0; a < 3; ++a) e[a] += g[i][a] * all[i][a];
+        for (int q = 0; q < 3; ++q) {
+            const int a = SH[q][0], b = SH[q][1];
+            e[3 + q] += g[i][a] * all[i][b] + g[i][b] * all[i][a];
+        }
+    }
+    hex_shape(xi, n);
+    double dt = -0.0;
+    for (int c = 0; c < 8; ++c) dt += n[c] * t[c];
+    for (int a = 0; a < 3; ++a)  // hex.rs:128-139
+        s[a] = h.d.normal[a][0] * e[0] + h.d.normal[a][1] * e[1] + h.d.normal[a][2] * e[2];
+    for (int q = 0; q < 3; ++q) s[3 + q] = h.d.shear[q] * e[3 + q];
+    for (int a = 0; a < 3; ++a) s[a] -= h.thermal[a] * dt;
 }
 
 }  // namespace orc

@@ -107,6 +107,18 @@ void tet10_mass(double volume, double density, double m[900]);
 void hex_conduction(const double s[3], const double k[3], double ke[64]);
 // hex.rs:218-297, 355-389: the condensed 24 x 24 stiffness of a box cell
 void hex8_stiffness(const double size[3], const Stiffness& d, double kc[576]);
+// hex.rs:186-309 `Hex`: the box cell's condensed stiffness, its load of a unit temperature
+// change at each corner, and the mode amplitudes a = mode_t T - mode_u u.
+struct HexElement {
+    double size[3];
+    Stiffness d;
+    double thermal[3];
+    double k[576], load[192], mode_u[216], mode_t[72];
+};
+void hex8_element(const double size[3], const Stiffness& d, const double alpha[3], HexElement* h);
+// hex.rs:311-335
+void hex8_strain_stress(const HexElement& h, const double xi[3], const double u[24],
+                        const double t[8], double e[6], double s[6]);
 
 // eigen.rs:183-269 and 274-331: the dense generalized and standard symmetric eigenproblems.
 // Returns false with `err` set when M is not positive definite.
@@ -154,6 +166,13 @@ void recover_tet10(size_t npoints, const double* xyz, size_t nel, const uint32_t
                    const double* u, const uint32_t* part, size_t nparts, const uint8_t* singular,
                    double* stress, double* strain, double* mises_out, double* principal_out,
                    RecoveryPeak* peaks);
+// elastic.rs:615-660 and 709-710 for box cells (8 corners in VTK order, 9 orthotropic constants
+// per cell): as recover_tet10 over the 8 corners of each cell.
+void recover_hex8(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                  const double* coef, const double* expansion, const double* dtemp,
+                  const double* u, const uint32_t* part, size_t nparts, const uint8_t* singular,
+                  double* stress, double* strain, double* mises_out, double* principal_out,
+                  RecoveryPeak* peaks);
 // elastic.rs:977-1002
 double mises(const double s[6]);
 void principal(const double s[6], double out[3]);

@@ -197,4 +197,87 @@ void recover_tet10(size_t npoints, const double* xyz, size_t nel, const uint32_t
     }
 }
 
+// elastic.rs:615-660 (the box grid): the strain and the stress at the 8 corners of each cell
+// (Hex::strain_stress, hex.rs:311-335, at xi = -1 or 1 per axis), their mean at each point and
+// the peaks of each part, over the cells in increasing order; `coef` holds the 9 orthotropic
+// constants of each cell, `expansion` (NULL: 0) its 3 expansion coefficients. mises_out and
+// principal_out are elastic.rs:709-710.
+void recover_hex8(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                  const double* coef, const double* expansion, const double* dtemp,
+                  const double* u, const uint32_t* part, size_t nparts, const uint8_t* singular,
+                  double* stress, double* strain, double* mises_out, double* principal_out,
+                  RecoveryPeak* peaks) {
+    static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    vector<uint32_t> count(npoints, 0);
+    for (size_t i = 0; i < 6 * npoints; ++i) stress[i] = strain[i] = 0.0;
+    const double inf = std::numeric_limits<double>::infinity();
+    vector<bool> has_regular(nparts, false);
+    for (size_t p = 0; peaks && p < nparts; ++p) {
+        peaks[p] = RecoveryPeak{};
+        peaks[p].mises = -inf;
+        peaks[p].element = -1;
+        peaks[p].regular_mises = -inf;
+        peaks[p].regular_element = -1;
+    }
+    HexElement h;
+    for (size_t e = 0; e < nel; ++e) {
+        const uint32_t* nodes = hexes + 8 * e;
+        double size[3], alpha[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < 3; ++d) {
+            size[d] = xyz[3 * (size_t)nodes[6] + d] - xyz[3 * (size_t)nodes[0] + d];
+            if (expansion) alpha[d] = expansion[3 * e + d];
+        }
+        const double* c9 = coef + 9 * e;
+        hex8_element(size, orthotropic_stiffness(c9, c9 + 3, c9 + 6), alpha, &h);
+        double ue[24], te[8];
+        for (int r = 0; r < 24; ++r) ue[r] = u[3 * (size_t)nodes[r / 3] + r % 3];
+        for (int c = 0; c < 8; ++c) te[c] = dtemp ? dtemp[nodes[c]] : 0.0;
+        bool near = false;
+        if (singular)
+            for (int c = 0; c < 8; ++c) near = near || singular[nodes[c]];
+        size_t pt = part ? part[e] : 0;
+        for (int c = 0; c < 8; ++c) {
+            double xi[3], eng[6], sig0[6], sig[6], eps[6];
+            for (int d = 0; d < 3; ++d) xi[d] = BITS[c][d] == 1 ? 1.0 : -1.0;
+            hex8_strain_stress(h, xi, ue, te, eng, sig0);
+            tensor_strain(eng, eps);
+            reorder_stress(sig0, sig);
+            size_t node = nodes[c];
+            for (int i = 0; i < 6; ++i) {
+                stress[6 * node + i] += sig[i];
+                strain[6 * node + i] += eps[i];
+            }
+            count[node] += 1;
+            if (!peaks) continue;
+            double vm = mises(sig);
+            RecoveryPeak& pk = peaks[pt];
+            bool why = (singular && singular[node]) || near;
+            if (vm > pk.mises) {
+                pk.mises = vm;
+                pk.element = (int64_t)e;
+                pk.local = c;
+                pk.point = (uint32_t)node;
+                pk.singular = why ? 1 : 0;
+            }
+            if (!why && (!has_regular[pt] || vm > pk.regular_mises)) {
+                has_regular[pt] = true;
+                pk.regular_mises = vm;
+                pk.regular_element = (int64_t)e;
+                pk.regular_local = c;
+                pk.regular_point = (uint32_t)node;
+            }
+        }
+    }
+    for (size_t i = 0; i < npoints; ++i) {
+        double c = (double)std::max<uint32_t>(count[i], 1u);
+        for (int j = 0; j < 6; ++j) {
+            stress[6 * i + j] /= c;
+            strain[6 * i + j] /= c;
+        }
+        if (mises_out) mises_out[i] = mises(stress + 6 * i);
+        if (principal_out) principal(stress + 6 * i, principal_out + 3 * i);
+    }
+}
+
 }  // namespace orc

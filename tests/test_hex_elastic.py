@@ -35,6 +35,53 @@ def test_oracle_hex_stiffness_is_symmetric_and_rigid_motions_have_no_force():
         assert np.abs(f).max() < 1e-12 * scale
 
 
+def test_oracle_rigid_motions_have_no_strain():
+    """hex.rs:485-488: the strain of a rigid motion at a point inside the cell is 0."""
+    c = oracle.orthotropic(200.0, 0.3)
+    for f in [lambda x: [1.0, 0.0, 0.0], lambda x: [-x[1], x[0], 0.0],
+              lambda x: [0.0, -x[2], x[1]], lambda x: [x[2], 0.0, -x[0]]]:
+        e, _ = oracle.hex8_strain_stress(SIZE, c, [0.3, -0.2, 0.7], nodal(f), np.zeros(8),
+                                         alpha=[1e-5] * 3)
+        assert np.abs(e).max() < 1e-12
+
+
+def test_oracle_uniform_strain_gives_the_exact_stress():
+    """hex.rs:491-519: a uniform strain field gives e0 and D e0 at each Gauss point, and a
+    uniform temperature change with no displacement gives -D alpha dT."""
+    c = oracle.orthotropic(200.0, 0.3)
+    normal, shear = oracle.isotropic(200.0, 0.3)
+    alpha = [1e-5, 2e-5, 3e-5]
+    e0 = np.array([1e-3, -2e-3, 0.5e-3, 4e-4, -3e-4, 2e-4])
+    u = nodal(lambda x: [e0[0] * x[0] + e0[5] * x[1], e0[1] * x[1] + e0[3] * x[2],
+                         e0[2] * x[2] + e0[4] * x[0]])
+    want = np.concatenate([normal @ e0[:3], shear * e0[3:]])
+    p = 1.0 / np.sqrt(3.0)
+    for b in mg.HEX_BITS:
+        xi = np.where(np.asarray(b) == 1, p, -p)
+        e, s = oracle.hex8_strain_stress(SIZE, c, xi, u, np.zeros(8), alpha=alpha)
+        assert np.abs(e - e0).max() < 1e-15
+        assert np.abs(s - want).max() < 1e-12
+    _, s = oracle.hex8_strain_stress(SIZE, c, [0.1, 0.2, 0.3], np.zeros(24), np.full(8, 10.0),
+                                     alpha=alpha)
+    assert np.abs(s[:3] + normal @ np.asarray(alpha) * 10.0).max() < 1e-12
+
+
+def test_oracle_box_recovery_of_a_uniform_strain():
+    """elastic.rs:615-660 on graded box cells of 1 material: the mean strain and stress at each
+    point of a uniform strain field are e0 (tensor components) and D e0."""
+    c = mg.hex_cantilever(nx=5, ny=3, nz=4, grade=1.5)
+    e0 = np.array([1e-3, -2e-3, 0.5e-3, 4e-4, -3e-4, 2e-4])
+    x = c.xyz
+    u = np.stack([e0[0] * x[:, 0] + e0[5] * x[:, 1], e0[1] * x[:, 1] + e0[3] * x[:, 2],
+                  e0[2] * x[:, 2] + e0[4] * x[:, 0]], axis=1).ravel()
+    r = oracle.recover(c.xyz, c.nodes, c.coef, u, hex=True)
+    normal, shear = oracle.isotropic(1000.0, 0.3)
+    sig = np.concatenate([normal @ e0[:3], shear * e0[3:]])
+    assert np.abs(r["strain"] - [e0[0], e0[1], e0[2], e0[5] / 2, e0[3] / 2, e0[4] / 2]).max() < 1e-15
+    assert np.abs(r["stress"] - [sig[0], sig[1], sig[2], sig[5], sig[3], sig[4]]).max() < 1e-12
+    assert r["peaks"][0].element >= 0
+
+
 def test_oracle_one_cell_bends_with_the_exact_curvature():
     """hex.rs:521-545: u^T K u equals E I kappa^2 L for the pure bending field (nu = 0)."""
     e, kappa = 1000.0, 1e-3
