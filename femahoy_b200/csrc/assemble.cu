@@ -15,6 +15,7 @@
 #include "assemble.cuh"
 #include "common.cuh"
 #include "elements.cuh"
+#include "hex.cuh"
 
 namespace femgpu {
 
@@ -488,149 +489,22 @@ __global__ void __launch_bounds__(32 * WARPS)
 // cells are sorted into classes by the bits of those 12 numbers, each class's 24 x 24 matrix is
 // made once on the device, and the rows are gathered from the class table.
 
-// The 12 words of each cell: the sides (corner 6 minus corner 0) and the 9 orthotropic constants.
+// The words of each cell: the sides (corner 6 minus corner 0), the 9 orthotropic constants and,
+// with `expansion` (width 15), the 3 expansion coefficients.
 __global__ void k_hex_keys(const double* __restrict__ xyz, const uint32_t* __restrict__ el,
-                           const double* __restrict__ coef, int64_t nel,
-                           double* __restrict__ key) {
+                           const double* __restrict__ coef, const double* __restrict__ expansion,
+                           int width, int64_t nel, double* __restrict__ key) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
          e += (int64_t)gridDim.x * blockDim.x) {
         const uint32_t c0 = el[8 * e], c6 = el[8 * e + 6];
-        double* k = key + 12 * e;
+        double* k = key + width * e;
 #pragma unroll
         for (int d = 0; d < 3; ++d) k[d] = xyz[3 * (int64_t)c6 + d] - xyz[3 * (int64_t)c0 + d];
 #pragma unroll
         for (int d = 0; d < 9; ++d) k[3 + d] = coef[9 * e + d];
-    }
-}
-
-// The local corner bits of the 8 corners in VTK order (hex.rs:34-43); the Gauss points of the
-// 2 x 2 x 2 rule take the same order (hex.rs:212-216).
-__constant__ int kHexCorner[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
-                                     {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
-
-// hex.rs:146-160: the gradients of the 8 corner functions and the 3 mode functions (1 - xi^2
-// along each axis) at the local point xi of a box with the sides `size`.
-__device__ void hex_gradients(const double* size, const double* xi, double g[11][3]) {
-    for (int n = 0; n < 8; ++n) {
-        double s[3], f[3];
+        if (width == 15)
 #pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            s[d] = kHexCorner[n][d] == 1 ? 1.0 : -1.0;
-            f[d] = 0.5 * (1.0 + s[d] * xi[d]);
-        }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) g[n][d] = s[d] / size[d] * f[(d + 1) % 3] * f[(d + 2) % 3];
-    }
-#pragma unroll
-    for (int m = 0; m < 3; ++m)
-#pragma unroll
-        for (int d = 0; d < 3; ++d) g[8 + m][d] = m == d ? -4.0 * xi[d] / size[d] : 0.0;
-}
-
-constexpr int HEX_THREADS = 128;
-
-// One block per class. hex.rs:218-297: the 33 x 33 stiffness of the 11 functions x 3
-// components summed over the Gauss points in their order (jac = the volume / 8), the Cholesky
-// factor of the 9 x 9 block of the modes (hex.rs:355-372), its solves on the 24 corner columns
-// (hex.rs:374-389), and K_uu - K_um X. Each sum and each solve runs in the reference's order, so
-// with separate roundings the matrix equals the reference's bit for bit. Flags: 2 no stable
-// material, 3 a modulus not above 0, 4 a side not above 0, 5 the modes' block not positive.
-__global__ void __launch_bounds__(HEX_THREADS)
-    k_hex_condense(const double* __restrict__ key, int64_t nclass, double* __restrict__ table,
-                   int* __restrict__ bad) {
-    __shared__ double g[8][11][3];
-    __shared__ double k[33][33];
-    __shared__ double l[9][9];
-    __shared__ double x[9][24];
-    __shared__ int ok;
-    const int t = threadIdx.x;
-    for (int64_t cl = blockIdx.x; cl < nclass; cl += gridDim.x) {
-        const double* size = key + 12 * cl;
-        Stiffness D;
-        const int st = orthotropic_stiffness(size + 3, &D);
-        bool sides = true;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) sides = sides && isfinite(size[d]) && size[d] > 0.0;
-        if (t == 0) {
-            ok = st == 0 && sides;
-            if (st) atomicExch(bad, st == 1 ? 3 : 2);
-            else if (!sides) atomicExch(bad, 4);
-        }
-        if (t < 8) {
-            const double p = 1.0 / sqrt(3.0);
-            double xi[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) xi[d] = kHexCorner[t][d] == 1 ? p : -p;
-            double gt[11][3];
-            hex_gradients(size, xi, gt);
-            for (int i = 0; i < 11; ++i)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) g[t][i][d] = gt[i][d];
-        }
-        __syncthreads();
-        if (ok) {
-            const double jac = size[0] * size[1] * size[2] / 8.0;
-            for (int o = t; o < 33 * 33; o += HEX_THREADS) {
-                const int r = o / 33, c = o % 33;
-                const int i = r / 3, a = r % 3, j = c / 3, b = c % 3;
-                double v = 0.0;
-#pragma unroll
-                for (int q = 0; q < 8; ++q) v += jac * elastic_term(g[q][i], g[q][j], a, b, D);
-                k[r][c] = v;
-            }
-        }
-        __syncthreads();
-        if (ok && t == 0) {  // cholesky9
-            for (int j = 0; j < 9; ++j) {
-                double d = k[24 + j][24 + j];
-                for (int c = 0; c < j; ++c) d -= l[j][c] * l[j][c];
-                if (!(d > 0.0)) {
-                    ok = 0;
-                    atomicExch(bad, 5);
-                    break;
-                }
-                d = sqrt(d);
-                l[j][j] = d;
-                for (int i = j + 1; i < 9; ++i) {
-                    double v = k[24 + i][24 + j];
-                    for (int c = 0; c < j; ++c) v -= l[i][c] * l[j][c];
-                    l[i][j] = v / d;
-                }
-            }
-        }
-        __syncthreads();
-        if (ok && t < 24) {  // solve9 on column t of K_mu
-            double b[9];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) b[i] = k[24 + i][t];
-#pragma unroll
-            for (int i = 0; i < 9; ++i) {
-#pragma unroll
-                for (int q = 0; q < i; ++q) b[i] -= l[i][q] * b[q];
-                b[i] /= l[i][i];
-            }
-#pragma unroll
-            for (int i = 8; i >= 0; --i) {
-#pragma unroll
-                for (int q = i + 1; q < 9; ++q) b[i] -= l[q][i] * b[q];
-                b[i] /= l[i][i];
-            }
-#pragma unroll
-            for (int i = 0; i < 9; ++i) x[i][t] = b[i];
-        }
-        __syncthreads();
-        double* out = table + 576 * cl;
-        for (int o = t; o < 576; o += HEX_THREADS) {
-            const int r = o / 24, c = o % 24;
-            double v = 0.0;
-            if (ok) {
-                v = k[r][c];
-#pragma unroll
-                for (int i = 0; i < 9; ++i) v -= k[r][24 + i] * x[i][c];
-            }
-            out[o] = v;
-        }
-        __syncthreads();
+            for (int d = 0; d < 3; ++d) k[12 + d] = expansion ? expansion[3 * e + d] : 0.0;
     }
 }
 
@@ -689,8 +563,17 @@ __global__ void __launch_bounds__(32 * WARPS)
 void hex_elements(const double* d_keys, int64_t n, double* d_table, cudaStream_t s) {
     DevBuf<int> bad(1);
     bad.zero(s);
-    k_hex_condense<<<(unsigned)std::min<int64_t>(n, NUM_SMS * 16), HEX_THREADS, 0, s>>>(
-        d_keys, n, d_table, bad.p);
+    k_hex_element<false><<<(unsigned)std::min<int64_t>(n, NUM_SMS * 16), HEX_THREADS, 0, s>>>(
+        d_keys, 12, n, d_table, bad.p);
+    FG_CHECK_LAUNCH();
+    assembly_flag(fetch(bad.p, s));
+}
+
+void hex_modes(const double* d_keys, int64_t n, double* d_modes, cudaStream_t s) {
+    DevBuf<int> bad(1);
+    bad.zero(s);
+    k_hex_element<true><<<(unsigned)std::min<int64_t>(n, NUM_SMS * 16), HEX_THREADS, 0, s>>>(
+        d_keys, 15, n, d_modes, bad.p);
     FG_CHECK_LAUNCH();
     assembly_flag(fetch(bad.p, s));
 }
@@ -698,36 +581,42 @@ void hex_elements(const double* d_keys, int64_t n, double* d_table, cudaStream_t
 // The classes of the cells: the cells in order, each compared with the last new class first
 // (a grid's neighbours mostly share it), then looked up by its 12 words.
 struct KeyHash {
-    size_t operator()(const std::array<uint64_t, 12>& k) const {
+    size_t operator()(const std::array<uint64_t, 15>& k) const {
         uint64_t h = 1469598103934665603ULL;  // FNV-1a over the words
         for (uint64_t w : k) h = (h ^ w) * 1099511628211ULL;
         return (size_t)h;
     }
 };
 
-static int64_t hex_classes(const double* d_key, int64_t nel, DevBuf<uint32_t>* cls,
-                           DevBuf<double>* keys, cudaStream_t s) {
-    std::vector<double> key((size_t)nel * 12);
-    FG_CUDA(cudaMemcpyAsync(key.data(), d_key, key.size() * sizeof(double),
+int64_t hex_classes(const double* xyz, const uint32_t* el, const double* coef,
+                    const double* expansion, int width, int64_t nel, DevBuf<uint32_t>* cls,
+                    DevBuf<double>* keys, cudaStream_t s) {
+    DevBuf<double> d_key(width * nel);
+    k_hex_keys<<<blocks_for(nel, 256), 256, 0, s>>>(xyz, el, coef, expansion, width, nel,
+                                                    d_key.p);
+    FG_CHECK_LAUNCH();
+    std::vector<double> key((size_t)nel * width);
+    FG_CUDA(cudaMemcpyAsync(key.data(), d_key.p, key.size() * sizeof(double),
                             cudaMemcpyDeviceToHost, s));
     FG_CUDA(cudaStreamSynchronize(s));
-    std::unordered_map<std::array<uint64_t, 12>, uint32_t, KeyHash> index;
+    std::unordered_map<std::array<uint64_t, 15>, uint32_t, KeyHash> index;
     std::vector<uint32_t> of((size_t)nel);
     std::vector<double> uniq;
     int64_t last = -1;
+    const size_t bytes = sizeof(double) * width;
     for (int64_t e = 0; e < nel; ++e) {
-        const double* k = key.data() + 12 * e;
-        if (last >= 0 && std::memcmp(k, key.data() + 12 * last, 96) == 0) {
+        const double* k = key.data() + width * e;
+        if (last >= 0 && std::memcmp(k, key.data() + width * last, bytes) == 0) {
             of[e] = of[last];
             continue;
         }
-        std::array<uint64_t, 12> w;
-        std::memcpy(w.data(), k, 96);
+        std::array<uint64_t, 15> w{};
+        std::memcpy(w.data(), k, bytes);
         auto it = index.find(w);
         if (it == index.end()) {
-            const uint32_t id = (uint32_t)(uniq.size() / 12);
+            const uint32_t id = (uint32_t)(uniq.size() / width);
             it = index.emplace(w, id).first;
-            uniq.insert(uniq.end(), k, k + 12);
+            uniq.insert(uniq.end(), k, k + width);
         }
         of[e] = it->second;
         last = e;
@@ -735,7 +624,7 @@ static int64_t hex_classes(const double* d_key, int64_t nel, DevBuf<uint32_t>* c
     cls->upload(of.data(), of.size(), s);
     keys->upload(uniq.data(), uniq.size(), s);
     FG_CUDA(cudaStreamSynchronize(s));
-    return (int64_t)(uniq.size() / 12);
+    return (int64_t)(uniq.size() / width);
 }
 
 // ------------------------------------------------------------------ colouring
@@ -985,14 +874,13 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
                 d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints, K.ptr.p,
                 K.idx.p, K.val.p, bad.p);
         } else if (kind == FEMGPU_HEX8_ELASTIC) {
-            DevBuf<double> key(12 * nel), keys, table;
+            DevBuf<double> keys, table;
             DevBuf<uint32_t> cls;
-            k_hex_keys<<<blocks_for(nel, 256), 256, 0, s>>>(d_xyz, d_el, d_coef, nel, key.p);
-            FG_CHECK_LAUNCH();
-            const int64_t nclass = hex_classes(key.p, nel, &cls, &keys, s);
+            const int64_t nclass =
+                hex_classes(d_xyz, d_el, d_coef, nullptr, 12, nel, &cls, &keys, s);
             table.alloc(576 * nclass);
-            k_hex_condense<<<(unsigned)std::min<int64_t>(nclass, NUM_SMS * 16), HEX_THREADS, 0,
-                             s>>>(keys.p, nclass, table.p, bad.p);
+            k_hex_element<false><<<(unsigned)std::min<int64_t>(nclass, NUM_SMS * 16), HEX_THREADS,
+                                   0, s>>>(keys.p, 12, nclass, table.p, bad.p);
             FG_CHECK_LAUNCH();
             k_gather_hex_elastic<4><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
                 d_el, cls.p, table.p, out->inc.start.p, out->inc.of_node.p, npoints,

@@ -38,6 +38,16 @@ void csr_mul(const DevCsr& a, const double* d_x, double* d_y, cudaStream_t s);
 // Hex::new (hex.rs:218-297) for `n` box cells given by their 12 numbers each (the 3 sides, the
 // 9 orthotropic constants): 576 values per cell into d_table.
 void hex_elements(const double* d_keys, int64_t n, double* d_table, cudaStream_t s);
+// The same with the 3 expansion coefficients after the constants (15 numbers per cell): the
+// recovery record of each (HEX_MODES values, hex.cuh).
+void hex_modes(const double* d_keys, int64_t n, double* d_modes, cudaStream_t s);
+// The classes of `nel` box cells (8 corners each): the cells whose `width` numbers (the sides,
+// the 9 constants of coef, with width 15 the 3 of expansion, which may be null: 0) are equal
+// bit for bit share a class. `cls` gets each cell's class, `keys` the numbers of each class;
+// returns the class count.
+int64_t hex_classes(const double* d_xyz, const uint32_t* d_el, const double* d_coef,
+                    const double* d_expansion, int width, int64_t nel, DevBuf<uint32_t>* cls,
+                    DevBuf<double>* keys, cudaStream_t s);
 // Throws the error of an assembly's device flag (0: none).
 void assembly_flag(int b);
 

@@ -33,6 +33,7 @@
 #include "assemble.cuh"
 #include "common.cuh"
 #include "elements.cuh"
+#include "hex.cuh"
 
 namespace femgpu {
 
@@ -174,8 +175,9 @@ __global__ void k_recover_cells(const double* __restrict__ xyz, const uint32_t* 
     }
 }
 
-// Setup: the place of point v in each of its cells. A cell that names the point twice is listed
-// twice and takes its places in order, as the reference's loop over the 10 points.
+// Setup: the place of point v in each of its cells (M points each). A cell that names the point
+// twice is listed twice and takes its places in order, as the reference's loop over its points.
+template <int M>
 __global__ void k_visit_places(const uint32_t* __restrict__ t10, const int64_t* __restrict__ start,
                                const uint32_t* __restrict__ of_node, int64_t npoints,
                                uint8_t* __restrict__ place) {
@@ -185,10 +187,10 @@ __global__ void k_visit_places(const uint32_t* __restrict__ t10, const int64_t* 
         int lastc = -1;
         for (int64_t k = start[v]; k < start[v + 1]; ++k) {
             const uint32_t e = of_node[k];
-            const uint32_t* t = t10 + 10 * (int64_t)e;
+            const uint32_t* t = t10 + M * (int64_t)e;
             int c = e == last ? lastc + 1 : 0;
-            while (c < 10 && t[c] != (uint32_t)v) ++c;
-            // c < 10: the incidence was built from these cells.
+            while (c < M && t[c] != (uint32_t)v) ++c;
+            // c < M: the incidence was built from these cells.
             place[k] = (uint8_t)c;
             last = e;
             lastc = c;
@@ -385,10 +387,209 @@ __global__ void __launch_bounds__(128, 4)
     }
 }
 
-// 1 thread per part: the reference's Peak (elastic_tet.rs:405-416) from the 3 maxima. The first
-// regular visit stays the regular peak when its value is NaN, since no value is greater than NaN.
+// ------------------------------------------------------------------ box cells
+// The box grid's loop (elastic.rs:615-660): Hex::strain_stress (hex.rs:311-335) at the 8 corners
+// of each cell. Each distinct cell (sides, material, expansion) has a record of HEX_MODES values
+// (hex.cuh: mode_u, mode_t, D, D alpha, the sides), made once at setup; each cell has its class
+// and its part with the `near` flag (8 bytes). A run first forms the 9 mode amplitudes of each
+// cell (a = mode_t T - mode_u u, hex.rs:316-326), once per cell, then 1 thread per point walks its
+// cells in increasing order as for the tetrahedra.
+
+// Setup: each cell's class and tag. Flag 3: a part past the last.
+__global__ void k_recover_hex_cells(const uint32_t* __restrict__ hexes,
+                                    const uint32_t* __restrict__ cls,
+                                    const uint32_t* __restrict__ part, uint32_t nparts,
+                                    const uint8_t* __restrict__ singular, int64_t nel,
+                                    uint2* __restrict__ rec, int* __restrict__ bad) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const uint32_t pt = part ? part[e] : 0u;
+        if (pt >= nparts) atomicExch(bad, 3);
+        bool near = false;
+        if (singular)
+#pragma unroll
+            for (int k = 0; k < 8; ++k) near = near || singular[hexes[8 * e + k]] != 0;
+        rec[e] = make_uint2(cls[e], (pt & ~NEAR_BIT) | (near ? NEAR_BIT : 0u));
+    }
+}
+
+// The 9 mode amplitudes of each cell (hex.rs:316-326): a_i = sum_c mode_t[i][c] T_c, then minus
+// sum_c mode_u[i][c] u_c, each from 0.0 in the reference's order; 12 values per cell.
+__global__ void k_hex_amplitudes(const uint32_t* __restrict__ hexes, const uint2* __restrict__ rec,
+                                 const double* __restrict__ modes, const double* __restrict__ u4,
+                                 const double* __restrict__ dtemp, int64_t nel,
+                                 double* __restrict__ amp) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const double* m = modes + HEX_MODES * (int64_t)__ldg(&rec[e].x);
+        double u[24], t[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            const uint32_t v = __ldg(hexes + 8 * e + n);
+            double unused;
+            ld32(u4 + 4 * (int64_t)v, u[3 * n], u[3 * n + 1], u[3 * n + 2], unused);
+            t[n] = dtemp ? __ldg(dtemp + v) : 0.0;
+        }
+        double* out = amp + 12 * e;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            double a = 0.0;
+#pragma unroll
+            for (int c = 0; c < 8; ++c) a += __ldg(m + HEX_MODE_T + 8 * i + c) * t[c];
+#pragma unroll
+            for (int c = 0; c < 24; ++c) a -= __ldg(m + HEX_MODE_U + 24 * i + c) * u[c];
+            out[i] = a;
+        }
+        out[9] = out[10] = out[11] = 0.0;
+    }
+}
+
+// Hex::strain_stress of cell e at its corner c (xi = -1 or 1 per axis), then reorder and
+// tensor_strain (elastic.rs:967-975): sig and eps in the order xx, yy, zz, xy, yz, xz.
+__device__ __forceinline__ void hex_strain_stress_at(const double* __restrict__ m,
+                                                     const uint32_t t[8],
+                                                     const double* __restrict__ a, int c,
+                                                     const double* __restrict__ u4,
+                                                     const double* __restrict__ dtemp,
+                                                     double sig[6], double eps[6]) {
+    double size[3], xi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        size[d] = __ldg(m + HEX_SIZE + d);
+        xi[d] = hex_bit(c, d) == 1 ? 1.0 : -1.0;
+    }
+    double g[11][3];
+    hex_gradients(size, xi, g);
+    double e[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < 11; ++i) {
+        double ui[3];
+        if (i < 8) {
+            double unused;
+            ld32(u4 + 4 * (int64_t)t[i], ui[0], ui[1], ui[2], unused);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) ui[k] = __ldg(a + 3 * (i - 8) + k);
+        }
+#pragma unroll
+        for (int q = 0; q < 3; ++q) e[q] += g[i][q] * ui[q];
+        // SHEAR (hex.rs:143): yz, xz, xy
+        e[3] += g[i][1] * ui[2] + g[i][2] * ui[1];
+        e[4] += g[i][0] * ui[2] + g[i][2] * ui[0];
+        e[5] += g[i][0] * ui[1] + g[i][1] * ui[0];
+    }
+    double n[8];
+    hex_shape(xi, n);
+    double dt = -0.0;  // the Rust float sum starts from -0.0
+#pragma unroll
+    for (int k = 0; k < 8; ++k) dt += n[k] * (dtemp ? __ldg(dtemp + t[k]) : 0.0);
+    double s[6];
+#pragma unroll
+    for (int q = 0; q < 3; ++q)  // hex.rs:128-139
+        s[q] = __ldg(m + HEX_NORMAL + 3 * q) * e[0] + __ldg(m + HEX_NORMAL + 3 * q + 1) * e[1] +
+               __ldg(m + HEX_NORMAL + 3 * q + 2) * e[2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s[3 + k] = __ldg(m + HEX_SHEAR + k) * e[3 + k];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) s[q] -= __ldg(m + HEX_THERMAL + q) * dt;
+    sig[0] = s[0];
+    sig[1] = s[1];
+    sig[2] = s[2];
+    sig[3] = s[5];
+    sig[4] = s[3];
+    sig[5] = s[4];
+    eps[0] = e[0];
+    eps[1] = e[1];
+    eps[2] = e[2];
+    eps[3] = 0.5 * e[5];
+    eps[4] = 0.5 * e[3];
+    eps[5] = 0.5 * e[4];
+}
+
+// One thread per point, as k_recover_points, over the 8 corners of the box cells (the visit key
+// of a peak is 8 cell + corner: the reference's loop order).
+template <bool PEAKS, bool SMEM>
+__global__ void __launch_bounds__(128, 4)
+    k_recover_hex_points(const uint2* __restrict__ rec, const double* __restrict__ modes,
+                         const double* __restrict__ amp, const uint32_t* __restrict__ hexes,
+                         const int64_t* __restrict__ start, const uint32_t* __restrict__ of_node,
+                         const uint8_t* __restrict__ place, const double* __restrict__ u4,
+                         const double* __restrict__ dtemp, const uint8_t* __restrict__ singular,
+                         int64_t npoints, int nparts, double* __restrict__ stress,
+                         double* __restrict__ strain, double* __restrict__ mises_out,
+                         double* __restrict__ principal_out, u128* __restrict__ peak) {
+    extern __shared__ u128 peak_s[];
+    u128* fold = SMEM ? peak_s : peak;
+    if (PEAKS && SMEM) {
+        for (int i = threadIdx.x; i < 3 * nparts; i += blockDim.x) peak_s[i] = 0;
+        __syncthreads();
+    }
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < npoints;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        double ss[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double se[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        const int64_t b = start[v], end = start[v + 1];
+        const bool sing_v = PEAKS && singular && singular[v];
+        for (int64_t k = b; k < end; ++k) {
+            const uint32_t e = __ldg(of_node + k);
+            const int c = __ldg(place + k);
+            const uint4* row = reinterpret_cast<const uint4*>(hexes + 8 * (int64_t)e);
+            const uint4 w0 = __ldg(row), w1 = __ldg(row + 1);
+            const uint32_t t[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+            const uint2 r = __ldg(rec + e);
+            double sig[6], eps[6];
+            hex_strain_stress_at(modes + HEX_MODES * (int64_t)r.x, t, amp + 12 * (int64_t)e, c, u4,
+                                 dtemp, sig, eps);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                ss[i] += sig[i];
+                se[i] += eps[i];
+            }
+            if (PEAKS) {
+                const unsigned long long bits =
+                    (unsigned long long)__double_as_longlong(mises6(sig));
+                const unsigned long long key = 8ull * e + c;
+                const int p = (int)(r.y & ~NEAR_BIT);
+                const bool reg = !(r.y & NEAR_BIT) && !sing_v;
+                const bool nan = is_nan_bits(bits);
+                const u128 vk = ((u128)bits << 64) | (u128)(NONE - key);
+                if (!nan) fold_max(fold + 3 * p, vk);
+                if (reg) {
+                    if (!nan) fold_max(fold + 3 * p + 1, vk);
+                    fold_max(fold + 3 * p + 2, ((u128)(NONE - key) << 64) | (u128)bits);
+                }
+            }
+        }
+        const int64_t count = end - b;
+        const double cnt = (double)(count > 1 ? count : 1);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            ss[i] /= cnt;
+            se[i] /= cnt;
+            stress[6 * v + i] = ss[i];
+            strain[6 * v + i] = se[i];
+        }
+        if (mises_out) mises_out[v] = mises6(ss);
+        if (principal_out) {
+            double pr[3];
+            principal3(ss, pr);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) principal_out[3 * v + i] = pr[i];
+        }
+    }
+    if (PEAKS && SMEM) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < 3 * nparts; i += blockDim.x)
+            if (peak_s[i] != 0) fold_max(peak + i, peak_s[i]);
+    }
+}
+
+// 1 thread per part: the reference's Peak (elastic_tet.rs:405-416, elastic.rs:636-650) from the
+// 3 maxima; cells of `nn` points (`el`), the tag of cell e at tag[stride e]. The first regular
+// visit stays the regular peak when its value is NaN, since no value is greater than NaN.
 __global__ void k_peak_final(const u128* __restrict__ peak, int nparts,
-                             const uint32_t* __restrict__ t10, const CellRecord* __restrict__ rec,
+                             const uint32_t* __restrict__ t10, int nn,
+                             const uint32_t* __restrict__ tag, int stride,
                              const uint8_t* __restrict__ singular, femgpu_peak* __restrict__ out) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= nparts) return;
@@ -402,11 +603,11 @@ __global__ void k_peak_final(const u128* __restrict__ peak, int nparts,
     } else {
         const uint64_t key = NONE - (uint64_t)all;
         o.mises = __longlong_as_double((long long)(uint64_t)(all >> 64));
-        o.element = (int64_t)(key / 10);
-        o.local = (int32_t)(key % 10);
+        o.element = (int64_t)(key / nn);
+        o.local = (int32_t)(key % nn);
         o.point = t10[key];
         o.singular =
-            ((rec[key / 10].tag & NEAR_BIT) || (singular && singular[o.point])) ? 1 : 0;
+            ((tag[stride * (key / nn)] & NEAR_BIT) || (singular && singular[o.point])) ? 1 : 0;
     }
     uint64_t rk = NONE;
     double rm = -inf;
@@ -425,8 +626,8 @@ __global__ void k_peak_final(const u128* __restrict__ peak, int nparts,
         o.regular_element = -1;
     } else {
         o.regular_mises = rm;
-        o.regular_element = (int64_t)(rk / 10);
-        o.regular_local = (int32_t)(rk % 10);
+        o.regular_element = (int64_t)(rk / nn);
+        o.regular_local = (int32_t)(rk % nn);
         o.regular_point = t10[rk];
     }
     out[p] = o;
@@ -440,6 +641,10 @@ struct femgpu_recovery {
     int64_t npoints = 0, nel = 0, nmat = 0;
     int nparts = 1;
     bool has_singular = false;
+    // Box cells (femgpu_recovery_new_hex): t10 then holds 8 corners per cell.
+    bool hex = false;
+    DevBuf<uint2> hrec;
+    DevBuf<double> hmodes, amp;
     Incidence inc;
     DevBuf<uint8_t> place;
     DevBuf<uint32_t> t10;
@@ -468,6 +673,10 @@ struct femgpu_recovery {
         k_pad_u<<<blocks_for(npoints, 256), 256, 0, s>>>(u, npoints, u4.p);
         FG_CHECK_LAUNCH();
         const int grid = blocks_for(npoints, 128, NUM_SMS * 64);
+        if (hex) {
+            run_hex(dtemp, stress, strain, mises, principal, peaks, grid);
+            return;
+        }
         if (!want_peaks) {
             k_recover_points<false, false><<<grid, 128, 0, s>>>(
                 rec.p, mats.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p, dtemp, sing,
@@ -485,8 +694,9 @@ struct femgpu_recovery {
         }
         FG_CHECK_LAUNCH();
         if (want_peaks) {
-            k_peak_final<<<(nparts + 127) / 128, 128, 0, s>>>(peak.p, nparts, t10.p, rec.p, sing,
-                                                               dpeaks.p);
+            k_peak_final<<<(nparts + 127) / 128, 128, 0, s>>>(
+                peak.p, nparts, t10.p, 10, reinterpret_cast<const uint32_t*>(rec.p) + 25, 32, sing,
+                dpeaks.p);
             FG_CHECK_LAUNCH();
         }
         FG_CUDA(cudaEventRecord(ev1, s));
@@ -500,6 +710,51 @@ struct femgpu_recovery {
         last_bytes = npoints * (24.0 + 32.0 + 32.0) + nel * (sizeof(CellRecord) + 40.0) +
                      nmat * (double)sizeof(MaterialEntry) + (npoints + 1) * 8.0 +
                      10.0 * nel * 5.0 + (dtemp ? npoints * 8.0 : 0.0) + npoints * 96.0 +
+                     (mises ? npoints * 8.0 : 0.0) + (principal ? npoints * 24.0 : 0.0) +
+                     (want_peaks && has_singular ? npoints * 1.0 : 0.0);
+    }
+
+    void run_hex(const double* dtemp, double* stress, double* strain, double* mises,
+                 double* principal, femgpu_peak* peaks, int grid) {
+        const bool want_peaks = peaks != nullptr;
+        const uint8_t* sing = has_singular ? singular.p : nullptr;
+        k_hex_amplitudes<<<blocks_for(nel, 128, NUM_SMS * 32), 128, 0, s>>>(
+            t10.p, hrec.p, hmodes.p, u4.p, dtemp, nel, amp.p);
+        FG_CHECK_LAUNCH();
+        if (!want_peaks) {
+            k_recover_hex_points<false, false><<<grid, 128, 0, s>>>(
+                hrec.p, hmodes.p, amp.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p, dtemp,
+                sing, npoints, nparts, stress, strain, mises, principal, nullptr);
+        } else {
+            peak.zero(s);
+            if (nparts <= SMEM_PARTS)
+                k_recover_hex_points<true, true><<<grid, 128, 3 * sizeof(u128) * nparts, s>>>(
+                    hrec.p, hmodes.p, amp.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p,
+                    dtemp, sing, npoints, nparts, stress, strain, mises, principal, peak.p);
+            else
+                k_recover_hex_points<true, false><<<grid, 128, 0, s>>>(
+                    hrec.p, hmodes.p, amp.p, t10.p, inc.start.p, inc.of_node.p, place.p, u4.p,
+                    dtemp, sing, npoints, nparts, stress, strain, mises, principal, peak.p);
+        }
+        FG_CHECK_LAUNCH();
+        if (want_peaks) {
+            k_peak_final<<<(nparts + 127) / 128, 128, 0, s>>>(
+                peak.p, nparts, t10.p, 8, reinterpret_cast<const uint32_t*>(hrec.p) + 1, 2, sing,
+                dpeaks.p);
+            FG_CHECK_LAUNCH();
+        }
+        FG_CUDA(cudaEventRecord(ev1, s));
+        if (want_peaks) dpeaks.download(peaks, nparts, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        float ms = 0.f;
+        FG_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        last_ms = ms;
+        // Each array once: u read, written padded and read padded; the cells' corners, records
+        // and amplitudes (written and read); the class records; the incidence with its places;
+        // the outputs.
+        last_bytes = npoints * (24.0 + 32.0 + 32.0) + nel * (32.0 + 8.0 + 2 * 96.0) +
+                     nmat * HEX_MODES * 8.0 + (npoints + 1) * 8.0 + 8.0 * nel * 5.0 +
+                     (dtemp ? npoints * 8.0 : 0.0) + npoints * 96.0 +
                      (mises ? npoints * 8.0 : 0.0) + (principal ? npoints * 24.0 : 0.0) +
                      (want_peaks && has_singular ? npoints * 1.0 : 0.0);
     }
@@ -553,7 +808,7 @@ int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uin
         r->t10.upload(tets10, 10 * nel, s);
         build_incidence(r->t10.p, r->nel, 10, r->npoints, &r->inc, s);
         r->place.alloc(10 * nel);
-        k_visit_places<<<blocks_for(r->npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
+        k_visit_places<10><<<blocks_for(r->npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
             r->t10.p, r->inc.start.p, r->inc.of_node.p, r->npoints, r->place.p);
         FG_CHECK_LAUNCH();
         // The distinct materials (E, nu, alpha) by their bits, numbered in order of first sight.
@@ -606,6 +861,67 @@ int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uin
     });
 }
 
+int femgpu_recovery_new_hex(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                            const double* coef, const double* expansion, const uint32_t* part,
+                            size_t nparts, const uint8_t* singular, femgpu_recovery** out) {
+    return recovery_guarded([&] {
+        need(out != nullptr, "out is null");
+        need(npoints > 0 && nel > 0, "an empty mesh");
+        need(xyz && hexes && coef, "a null mesh array");
+        need(nparts >= 1, "no part");
+        if (nparts > (size_t)MAX_PARTS)
+            throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 2048 parts");
+        if (npoints >= 0xffffffffull || nel >= 0xffffffffull / 8)
+            throw Failure(FEMGPU_ERR_TOO_LARGE, "more points or cells than 32-bit numbers hold");
+        for (size_t k = 0; k < 8 * nel; ++k)
+            need(hexes[k] < npoints, "a cell names a point past the last");
+        auto r = std::make_unique<femgpu_recovery>();
+        FG_CUDA(cudaStreamCreateWithFlags(&r->s, cudaStreamNonBlocking));
+        FG_CUDA(cudaEventCreate(&r->ev0));
+        FG_CUDA(cudaEventCreate(&r->ev1));
+        cudaStream_t s = r->s;
+        r->hex = true;
+        r->npoints = (int64_t)npoints;
+        r->nel = (int64_t)nel;
+        r->nparts = (int)nparts;
+        r->t10.upload(hexes, 8 * nel, s);
+        build_incidence(r->t10.p, r->nel, 8, r->npoints, &r->inc, s);
+        r->place.alloc(8 * nel);
+        k_visit_places<8><<<blocks_for(r->npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
+            r->t10.p, r->inc.start.p, r->inc.of_node.p, r->npoints, r->place.p);
+        FG_CHECK_LAUNCH();
+        // The distinct cells (sides, material, expansion) and their recovery records.
+        DevBuf<double> dxyz, dcoef, dexp, keys;
+        DevBuf<uint32_t> cls, dpart;
+        dxyz.upload(xyz, 3 * npoints, s);
+        dcoef.upload(coef, 9 * nel, s);
+        if (expansion) dexp.upload(expansion, 3 * nel, s);
+        r->nmat = hex_classes(dxyz.p, r->t10.p, dcoef.p, expansion ? dexp.p : nullptr, 15,
+                              r->nel, &cls, &keys, s);
+        r->hmodes.alloc(HEX_MODES * r->nmat);
+        hex_modes(keys.p, r->nmat, r->hmodes.p, s);
+        if (part) dpart.upload(part, nel, s);
+        if (singular) {
+            r->singular.upload(singular, npoints, s);
+            r->has_singular = true;
+        }
+        r->hrec.alloc(nel);
+        r->amp.alloc(12 * nel);
+        r->u4.alloc(4 * npoints);
+        DevBuf<int> bad(1);
+        bad.zero(s);
+        k_recover_hex_cells<<<blocks_for(r->nel, 128, NUM_SMS * 32), 128, 0, s>>>(
+            r->t10.p, cls.p, part ? dpart.p : nullptr, (uint32_t)nparts,
+            singular ? r->singular.p : nullptr, r->nel, r->hrec.p, bad.p);
+        FG_CHECK_LAUNCH();
+        if (fetch(bad.p, s) == 3) throw Failure(FEMGPU_ERR_INVALID, "a cell names a part past the last");
+        r->peak.alloc(3 * nparts);
+        r->dpeaks.alloc(nparts);
+        FG_CUDA(cudaStreamSynchronize(s));
+        *out = r.release();
+    });
+}
+
 int femgpu_recovery_run(femgpu_recovery* r, const double* u, const double* dtemp, double* stress,
                         double* strain, double* mises, double* principal, femgpu_peak* peaks) {
     return recovery_guarded([&] {
@@ -648,6 +964,7 @@ int femgpu_recovery_last_time(const femgpu_recovery* r, double* ms, double* byte
 size_t femgpu_recovery_bytes(const femgpu_recovery* r) {
     if (!r) return 0;
     return r->t10.bytes() + r->rec.bytes() + r->mats.bytes() + r->singular.bytes() +
+           r->hrec.bytes() + r->hmodes.bytes() + r->amp.bytes() +
            r->place.bytes() + r->u4.bytes() + r->peak.bytes() + r->dpeaks.bytes() +
            r->inc.start.bytes() +
            r->inc.of_node.bytes() + r->du.bytes() + r->ddt.bytes() + r->dstress.bytes() +

@@ -38,18 +38,22 @@ class Peak:
 
 
 class Recovery:
+    """``hex=True``: the box grid's loop (crates/fem/src/elastic.rs:615-660) over box cells,
+    ``tets10`` then holding the 8 corners of each cell (VTK order) and ``coef`` the 9
+    orthotropic constants of each cell; the peaks' ``local`` is the corner."""
+
     def __init__(self, xyz, tets10, coef, *, expansion=None, part=None, nparts=1,
-                 singular=None):
+                 singular=None, hex=False):
         xyz = L.arr(xyz, np.float64).reshape(-1, 3)
-        t10 = L.arr(tets10, np.uint32).reshape(-1, 10)
-        coef = L.arr(coef, np.float64).reshape(-1, 2)
+        t10 = L.arr(tets10, np.uint32).reshape(-1, 8 if hex else 10)
+        coef = L.arr(coef, np.float64).reshape(-1, 9 if hex else 2)
         exp = None if expansion is None else L.arr(expansion, np.float64).reshape(-1, 3)
         part = None if part is None else L.arr(part, np.uint32)
         sing = None if singular is None else L.arr(singular, np.uint8)
         h = C.c_void_p()
-        L.check(L.lib().femgpu_recovery_new(len(xyz), L.ptr(xyz), len(t10), L.ptr(t10),
-                                            L.ptr(coef), L.ptr(exp), L.ptr(part), nparts,
-                                            L.ptr(sing), C.byref(h)))
+        new = L.lib().femgpu_recovery_new_hex if hex else L.lib().femgpu_recovery_new
+        L.check(new(len(xyz), L.ptr(xyz), len(t10), L.ptr(t10), L.ptr(coef), L.ptr(exp),
+                    L.ptr(part), nparts, L.ptr(sing), C.byref(h)))
         self._h = h.value
         self._free = L.lib().femgpu_recovery_free
         self.npoints = len(xyz)

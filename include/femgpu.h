@@ -516,6 +516,16 @@ typedef struct femgpu_peak {
 int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uint32_t* tets10,
                         const double* coef, const double* expansion, const uint32_t* part,
                         size_t nparts, const uint8_t* singular, femgpu_recovery** out);
+/* The box grid's loop (elastic.rs:615-660 and 709-710): the strain and the stress at the 8
+ * corners of each box cell (Hex::strain_stress, hex.rs:311-335, with the cell's incompatible
+ * modes recovered from its corners), their mean at each point and the peaks of each part. The 8
+ * corners of each cell in VTK order, the sides corner 6 minus corner 0; `coef` holds the 9
+ * orthotropic constants per cell (as FEMGPU_HEX8_ELASTIC), `expansion` alpha_x, alpha_y, alpha_z
+ * per cell (NULL: none; D alpha as hex.rs:222-223); `part` and `singular` as above. The peaks'
+ * `local` is the corner (0-7). femgpu_recovery_run then serves both kinds of cells. */
+int femgpu_recovery_new_hex(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                            const double* coef, const double* expansion, const uint32_t* part,
+                            size_t nparts, const uint8_t* singular, femgpu_recovery** out);
 /* One recovery from the full displacement `u` (3 per point; the solution at the free unknowns
  * and the prescribed values elsewhere, elastic_tet.rs:349-351) and the temperature change of
  * each point (NULL: none; only corners are read). Outputs may be NULL to skip them: stress and

@@ -321,3 +321,77 @@ def test_gpu_box_cantilever_solves_with_cells(precision):
     xd, _ = oracle.direct_solve(Ko.submatrix(c.free), c.xyz[c.free // 3],
                                 Ko.reduced_rhs(c.load, c.values, c.free))
     assert np.linalg.norm(x - xd) <= 1e-8 * np.linalg.norm(xd)
+
+
+def hex_recovery_case(seed=4, nparts=3):
+    """A graded cantilever of 2 materials with a random displacement, a random temperature
+    change, expansion per cell, parts and a few singular points."""
+    c = mg.hex_cantilever(nx=7, ny=3, nz=4, grade=1.4, seed=seed)
+    rng = np.random.default_rng(seed)
+    n, nel = c.mesh.n, len(c.nodes)
+    return {"xyz": c.xyz, "hexes": c.nodes, "coef": c.coef,
+            "expansion": rng.uniform(1e-6, 3e-5, size=(nel, 3)),
+            "part": rng.integers(0, nparts, size=nel).astype(np.uint32), "nparts": nparts,
+            "singular": (rng.random(n) < 0.05).astype(np.uint8),
+            "u": rng.standard_normal(3 * n) * 1e-3, "dtemp": rng.standard_normal(n) * 10.0}
+
+
+def test_oracle_box_recovery_peaks_follow_the_loop():
+    """elastic.rs:636-650: the peak of each part is the first strict maximum over the visits in
+    loop order (cell, then corner), and the regular peak the same over the visits that touch no
+    singular point; checked against a numpy walk of the oracle's own per-visit values."""
+    c = hex_recovery_case()
+    r = oracle.recover(c["xyz"], c["hexes"], c["coef"], c["u"], expansion=c["expansion"],
+                       dtemp=c["dtemp"], part=c["part"], nparts=c["nparts"],
+                       singular=c["singular"], hex=True)
+    best = [(-np.inf, -1, -1)] * c["nparts"]
+    reg = [(-np.inf, -1, -1)] * c["nparts"]
+    seen = [False] * c["nparts"]
+    for e, nodes in enumerate(c["hexes"]):
+        size = c["xyz"][nodes[6]] - c["xyz"][nodes[0]]
+        ue = c["u"].reshape(-1, 3)[nodes].ravel()
+        near = bool(c["singular"][nodes].any())
+        p = c["part"][e]
+        for k, b in enumerate(mg.HEX_BITS):
+            xi = np.where(np.asarray(b) == 1, 1.0, -1.0)
+            _, s = oracle.hex8_strain_stress(size, c["coef"][e], xi, ue, c["dtemp"][nodes],
+                                             alpha=c["expansion"][e])
+            s = [s[0], s[1], s[2], s[5], s[3], s[4]]
+            vm = np.sqrt(0.5 * ((s[0] - s[1]) ** 2 + (s[1] - s[2]) ** 2 + (s[2] - s[0]) ** 2)
+                         + 3.0 * (s[3] ** 2 + s[4] ** 2 + s[5] ** 2))
+            if vm > best[p][0]:
+                best[p] = (vm, e, k)
+            if not (near or c["singular"][nodes[k]]) and (not seen[p] or vm > reg[p][0]):
+                seen[p] = True
+                reg[p] = (vm, e, k)
+    for p, pk in enumerate(r["peaks"]):
+        assert (pk.element, pk.local) == best[p][1:] and abs(pk.mises - best[p][0]) <= 1e-9 * best[p][0]
+        assert (pk.regular_element, pk.regular_local) == reg[p][1:]
+
+
+@pytest.mark.gpu
+def test_gpu_box_recovery_is_bit_identical_to_the_oracle():
+    """elastic.rs:615-660 on the device against the oracle: stress, strain and von Mises bit for
+    bit, the principal stresses to 1e-12 of the largest stress (acos, cos), the peaks equal."""
+    from femahoy_b200.recover import Recovery
+    c = hex_recovery_case()
+    ref = oracle.recover(c["xyz"], c["hexes"], c["coef"], c["u"], expansion=c["expansion"],
+                         dtemp=c["dtemp"], part=c["part"], nparts=c["nparts"],
+                         singular=c["singular"], hex=True)
+    rec = Recovery(c["xyz"], c["hexes"], c["coef"], expansion=c["expansion"], part=c["part"],
+                   nparts=c["nparts"], singular=c["singular"], hex=True)
+    got = rec.run(c["u"], c["dtemp"])
+    for key in ("stress", "strain", "mises"):
+        assert np.array_equal(np.asarray(got[key]).view(np.uint64), ref[key].view(np.uint64)), key
+    scale = np.abs(ref["stress"]).max()
+    assert np.abs(got["principal"] - ref["principal"]).max() <= 1e-12 * scale
+    for g, o in zip(got["peaks"], ref["peaks"]):
+        assert (g.element, g.local, g.point, int(g.singular), g.regular_element, g.regular_local,
+                g.regular_point) == (o.element, o.local, o.point, int(o.singular),
+                                     o.regular_element, o.regular_local, o.regular_point)
+        assert np.array_equal(np.array([g.mises, g.regular_mises]).view(np.uint64),
+                              np.array([o.mises, o.regular_mises]).view(np.uint64))
+    # Without the optional arrays: 1 part, no expansion, no temperature.
+    ref = oracle.recover(c["xyz"], c["hexes"], c["coef"], c["u"], hex=True)
+    got = Recovery(c["xyz"], c["hexes"], c["coef"], hex=True).run(c["u"])
+    assert np.array_equal(got["stress"].view(np.uint64), ref["stress"].view(np.uint64))
