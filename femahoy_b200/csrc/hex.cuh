@@ -49,9 +49,10 @@ __device__ __forceinline__ void hex_shape(const double* xi, double n[8]) {
 constexpr int HEX_THREADS = 128;
 
 // The recovery record of a class (HEX_MODES doubles, 32-byte aligned): mode_u (9 x 24), mode_t
-// (9 x 8), D (normal 3 x 3, then G_yz, G_xz, G_xy), D alpha, the sides.
+// (9 x 8), D (normal 3 x 3, then G_yz, G_xz, G_xy), D alpha, the sides, and the gradients of the
+// 11 functions at each of the 8 corners (hex.rs:146-160 at xi = -1 or 1: 33 per corner).
 constexpr int HEX_MODE_U = 0, HEX_MODE_T = 216, HEX_NORMAL = 288, HEX_SHEAR = 297,
-              HEX_THERMAL = 300, HEX_SIZE = 303, HEX_MODES = 320;
+              HEX_THERMAL = 300, HEX_SIZE = 303, HEX_GRAD = 320, HEX_MODES = 584;
 
 // One block per class of `key` (`width` words each: 3 sides, 9 orthotropic constants, with
 // MODES 3 expansion coefficients). hex.rs:218-297: the 33 x 33 stiffness of the 11 functions x 3
@@ -181,7 +182,16 @@ __global__ void __launch_bounds__(HEX_THREADS)
             }
         } else {
             double* out = out_all + HEX_MODES * cl;
-            for (int o = t; o < HEX_MODES; o += HEX_THREADS) {
+            if (t < 8) {  // the gradients at corner t
+                double xi[3], gc[11][3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) xi[d] = hex_bit(t, d) == 1 ? 1.0 : -1.0;
+                hex_gradients(size, xi, gc);
+                for (int i = 0; i < 11; ++i)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) out[HEX_GRAD + 33 * t + 3 * i + d] = gc[i][d];
+            }
+            for (int o = t; o < HEX_GRAD; o += HEX_THREADS) {
                 double v = 0.0;
                 if (o < HEX_MODE_T)
                     v = ok ? x[o / 24][o % 24] : 0.0;

@@ -452,17 +452,14 @@ __device__ __forceinline__ void hex_strain_stress_at(const double* __restrict__ 
                                                      const double* __restrict__ u4,
                                                      const double* __restrict__ dtemp,
                                                      double sig[6], double eps[6]) {
-    double size[3], xi[3];
+    double xi[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        size[d] = __ldg(m + HEX_SIZE + d);
-        xi[d] = hex_bit(c, d) == 1 ? 1.0 : -1.0;
-    }
-    double g[11][3];
-    hex_gradients(size, xi, g);
+    for (int d = 0; d < 3; ++d) xi[d] = hex_bit(c, d) == 1 ? 1.0 : -1.0;
+    const double* gc = m + HEX_GRAD + 33 * c;  // hex_gradients at this corner, made at setup
     double e[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int i = 0; i < 11; ++i) {
+        const double g[3] = {__ldg(gc + 3 * i), __ldg(gc + 3 * i + 1), __ldg(gc + 3 * i + 2)};
         double ui[3];
         if (i < 8) {
             double unused;
@@ -472,11 +469,11 @@ __device__ __forceinline__ void hex_strain_stress_at(const double* __restrict__ 
             for (int k = 0; k < 3; ++k) ui[k] = __ldg(a + 3 * (i - 8) + k);
         }
 #pragma unroll
-        for (int q = 0; q < 3; ++q) e[q] += g[i][q] * ui[q];
+        for (int q = 0; q < 3; ++q) e[q] += g[q] * ui[q];
         // SHEAR (hex.rs:143): yz, xz, xy
-        e[3] += g[i][1] * ui[2] + g[i][2] * ui[1];
-        e[4] += g[i][0] * ui[2] + g[i][2] * ui[0];
-        e[5] += g[i][0] * ui[1] + g[i][1] * ui[0];
+        e[3] += g[1] * ui[2] + g[2] * ui[1];
+        e[4] += g[0] * ui[2] + g[2] * ui[0];
+        e[5] += g[0] * ui[1] + g[1] * ui[0];
     }
     double n[8];
     hex_shape(xi, n);
