@@ -200,6 +200,8 @@ SIGNATURES = {
     "femgpu_recovery_new_hex": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
                                       C.c_void_p, C.POINTER(C.c_void_p)]),
+    "femgpu_hex_loads": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_recovery_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_recovery_run_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -49,10 +49,12 @@ __device__ __forceinline__ void hex_shape(const double* xi, double n[8]) {
 constexpr int HEX_THREADS = 128;
 
 // The recovery record of a class (HEX_MODES doubles, 32-byte aligned): mode_u (9 x 24), mode_t
-// (9 x 8), D (normal 3 x 3, then G_yz, G_xz, G_xy), D alpha, the sides, and the gradients of the
-// 11 functions at each of the 8 corners (hex.rs:146-160 at xi = -1 or 1: 33 per corner).
+// (9 x 8), D (normal 3 x 3, then G_yz, G_xz, G_xy), D alpha, the sides, the gradients of the 11
+// functions at each of the 8 corners (hex.rs:146-160 at xi = -1 or 1: 33 per corner), and the
+// condensed load of a unit temperature change at each corner (hex.rs:283-289, 24 x 8).
 constexpr int HEX_MODE_U = 0, HEX_MODE_T = 216, HEX_NORMAL = 288, HEX_SHEAR = 297,
-              HEX_THERMAL = 300, HEX_SIZE = 303, HEX_GRAD = 320, HEX_MODES = 584;
+              HEX_THERMAL = 300, HEX_SIZE = 303, HEX_GRAD = 320, HEX_LOAD = 584,
+              HEX_MODES = 776;
 
 // One block per class of `key` (`width` words each: 3 sides, 9 orthotropic constants, with
 // MODES 3 expansion coefficients). hex.rs:218-297: the 33 x 33 stiffness of the 11 functions x 3
@@ -182,6 +184,16 @@ __global__ void __launch_bounds__(HEX_THREADS)
             }
         } else {
             double* out = out_all + HEX_MODES * cl;
+            for (int o = t; o < 192; o += HEX_THREADS) {  // lc = l - K_um mode_t
+                const int r = o / 8, c = o % 8;
+                double v = 0.0;
+                if (ok) {
+                    v = lt[MODES ? r : 0][c];
+#pragma unroll
+                    for (int i = 0; i < 9; ++i) v -= k[r][24 + i] * x[i][24 + c];
+                }
+                out[HEX_LOAD + o] = v;
+            }
             if (t < 8) {  // the gradients at corner t
                 double xi[3], gc[11][3];
 #pragma unroll

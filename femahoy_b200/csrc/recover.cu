@@ -581,6 +581,41 @@ __global__ void __launch_bounds__(128, 4)
     }
 }
 
+// The thermal and volume forces of the box cells (elastic.rs:386-405), 1 thread per point: over
+// its cells in increasing order, f = sum_c load[3 a + d][c] T_c from 0.0 (a = the point's corner),
+// plus accel_d times the volume / 8, added to force[3 v + d] from 0.0: the reference's order.
+__global__ void k_hex_loads(const uint32_t* __restrict__ hexes, const uint32_t* __restrict__ cls,
+                            const double* __restrict__ modes, const int64_t* __restrict__ start,
+                            const uint32_t* __restrict__ of_node, const uint8_t* __restrict__ place,
+                            const double* __restrict__ accel, const double* __restrict__ dtemp,
+                            int64_t npoints, double* __restrict__ force) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < npoints;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        double fv[3] = {0.0, 0.0, 0.0};
+        for (int64_t k = start[v]; k < start[v + 1]; ++k) {
+            const uint32_t e = __ldg(of_node + k);
+            const int a = __ldg(place + k);
+            const double* m = modes + HEX_MODES * (int64_t)__ldg(cls + e);
+            double t[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                t[c] = dtemp ? __ldg(dtemp + __ldg(hexes + 8 * (int64_t)e + c)) : 0.0;
+            const double volume =
+                __ldg(m + HEX_SIZE) * __ldg(m + HEX_SIZE + 1) * __ldg(m + HEX_SIZE + 2);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                double f = 0.0;
+#pragma unroll
+                for (int c = 0; c < 8; ++c) f += __ldg(m + HEX_LOAD + 8 * (3 * a + d) + c) * t[c];
+                f += (accel ? __ldg(accel + 3 * (int64_t)e + d) : 0.0) * volume / 8.0;
+                fv[d] += f;
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) force[3 * v + d] = fv[d];
+    }
+}
+
 // 1 thread per part: the reference's Peak (elastic_tet.rs:405-416, elastic.rs:636-650) from the
 // 3 maxima; cells of `nn` points (`el`), the tag of cell e at tag[stride e]. The first regular
 // visit stays the regular peak when its value is NaN, since no value is greater than NaN.
@@ -916,6 +951,45 @@ int femgpu_recovery_new_hex(size_t npoints, const double* xyz, size_t nel, const
         r->dpeaks.alloc(nparts);
         FG_CUDA(cudaStreamSynchronize(s));
         *out = r.release();
+    });
+}
+
+int femgpu_hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                     const double* coef, const double* expansion, const double* accel,
+                     const double* dtemp, double* force) {
+    return recovery_guarded([&] {
+        need(npoints > 0 && nel > 0, "an empty mesh");
+        need(xyz && hexes && coef && force, "a null mesh array");
+        if (npoints >= 0xffffffffull || nel >= 0xffffffffull / 8)
+            throw Failure(FEMGPU_ERR_TOO_LARGE, "more points or cells than 32-bit numbers hold");
+        for (size_t k = 0; k < 8 * nel; ++k)
+            need(hexes[k] < npoints, "a cell names a point past the last");
+        cudaStream_t s = cudaStreamPerThread;
+        DevBuf<uint32_t> dh, cls;
+        DevBuf<double> dxyz, dcoef, dexp, dacc, dt, keys, modes, df(3 * npoints);
+        DevBuf<uint8_t> place;
+        Incidence inc;
+        dh.upload(hexes, 8 * nel, s);
+        dxyz.upload(xyz, 3 * npoints, s);
+        dcoef.upload(coef, 9 * nel, s);
+        if (expansion) dexp.upload(expansion, 3 * nel, s);
+        if (accel) dacc.upload(accel, 3 * nel, s);
+        if (dtemp) dt.upload(dtemp, npoints, s);
+        build_incidence(dh.p, (int64_t)nel, 8, (int64_t)npoints, &inc, s);
+        place.alloc(8 * nel);
+        k_visit_places<8><<<blocks_for((int64_t)npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
+            dh.p, inc.start.p, inc.of_node.p, (int64_t)npoints, place.p);
+        FG_CHECK_LAUNCH();
+        const int64_t nclass = hex_classes(dxyz.p, dh.p, dcoef.p, expansion ? dexp.p : nullptr,
+                                           15, (int64_t)nel, &cls, &keys, s);
+        modes.alloc(HEX_MODES * nclass);
+        hex_modes(keys.p, nclass, modes.p, s);
+        k_hex_loads<<<blocks_for((int64_t)npoints, 128, NUM_SMS * 32), 128, 0, s>>>(
+            dh.p, cls.p, modes.p, inc.start.p, inc.of_node.p, place.p,
+            accel ? dacc.p : nullptr, dtemp ? dt.p : nullptr, (int64_t)npoints, df.p);
+        FG_CHECK_LAUNCH();
+        df.download(force, 3 * npoints, s);
+        FG_CUDA(cudaStreamSynchronize(s));
     });
 }
 

@@ -37,6 +37,23 @@ class Peak:
                    p.regular_element, p.regular_local, p.regular_point)
 
 
+def hex_loads(xyz, hexes, coef, *, expansion=None, accel=None, dtemp=None):
+    """The forces of the box cells' loop (crates/fem/src/elastic.rs:386-405) on the device: the
+    load of the corner temperature changes ``dtemp`` (1 per point) through each cell's expansion
+    (3 per cell), plus ``accel`` (3 per cell: density times gravity plus the body force) times
+    the volume / 8, summed over the cells in order. Returns 3 values per point."""
+    xyz = L.arr(xyz, np.float64).reshape(-1, 3)
+    hexes = L.arr(hexes, np.uint32).reshape(-1, 8)
+    coef = L.arr(coef, np.float64).reshape(-1, 9)
+    opt = lambda a, k: None if a is None else L.arr(a, np.float64).reshape(-1, k)
+    exp, acc = opt(expansion, 3), opt(accel, 3)
+    dt = None if dtemp is None else L.arr(dtemp, np.float64)
+    force = np.empty(3 * len(xyz))
+    L.check(L.lib().femgpu_hex_loads(len(xyz), L.ptr(xyz), len(hexes), L.ptr(hexes), L.ptr(coef),
+                                     L.ptr(exp), L.ptr(acc), L.ptr(dt), L.ptr(force)))
+    return force
+
+
 class Recovery:
     """``hex=True``: the box grid's loop (crates/fem/src/elastic.rs:615-660) over box cells,
     ``tets10`` then holding the 8 corners of each cell (VTK order) and ``coef`` the 9

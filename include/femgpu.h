@@ -516,6 +516,16 @@ typedef struct femgpu_peak {
 int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uint32_t* tets10,
                         const double* coef, const double* expansion, const uint32_t* part,
                         size_t nparts, const uint8_t* singular, femgpu_recovery** out);
+/* The forces of the box cells' loop (elastic.rs:386-405): for each cell in increasing order and
+ * each of its 24 unknowns, the load of its corner temperature changes (Hex::load, hex.rs:283-289:
+ * D alpha through the 8 corners, the modes condensed) plus `accel` (3 per cell: the density
+ * times gravity plus the body force per unit volume, as the reference sums them) times the
+ * volume / 8, summed into `force` (3 per point, written whole) in the reference's order. `coef`
+ * and `expansion` as femgpu_recovery_new_hex; `accel` and `dtemp` (1 per point) may be null: 0.
+ * The reference's `gross` force scale is not formed. */
+int femgpu_hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                     const double* coef, const double* expansion, const double* accel,
+                     const double* dtemp, double* force);
 /* The box grid's loop (elastic.rs:615-660 and 709-710): the strain and the stress at the 8
  * corners of each box cell (Hex::strain_stress, hex.rs:311-335, with the cell's incompatible
  * modes recovered from its corners), their mean at each point and the peaks of each part. The 8

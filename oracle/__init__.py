@@ -50,6 +50,7 @@ def _load():
         "orc_hex8_element": (I, [P, P, P, P, P, P, P, P, S]),
         "orc_hex8_strain_stress": (I, [P, P, P, P, P, P, P, P, P, S]),
         "orc_recover_hex": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
+        "orc_hex_loads": (I, [S, P, S, P, P, P, P, P, P, P, S]),
         "orc_assemble": (I, [P, I, P, P, S, P, P, S]),
         "orc_quadratic": (S, [P, S, P, S, P, P]),
         "orc_colour": (I, [S, P, S, I, P]),
@@ -290,6 +291,23 @@ def hex8_element(size, c, alpha=(0.0, 0.0, 0.0)):
                              512):
         raise OracleError(err.value.decode())
     return k.reshape(24, 24), load.reshape(24, 8), mu.reshape(9, 24), mt.reshape(9, 8)
+
+
+def hex_loads(xyz, hexes, coef, *, expansion=None, accel=None, dtemp=None):
+    """elastic.rs:386-405: the thermal forces (load T) and the volume forces (accel, the
+    density times gravity plus the body force per unit volume, per cell) of the box cells, summed
+    over the cells in order: 3 values per point."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    hexes = np.ascontiguousarray(hexes, dtype=np.uint32)
+    coef = np.ascontiguousarray(coef, dtype=np.float64)
+    opt = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+    force = np.empty(3 * len(xyz))
+    err = C.create_string_buffer(512)
+    if _lib.orc_hex_loads(len(xyz), _p(xyz), len(hexes), _p(hexes), _p(coef),
+                          _p(opt(expansion)), _p(opt(accel)), _p(opt(dtemp)), _p(force), err,
+                          512):
+        raise OracleError(err.value.decode())
+    return force
 
 
 def hex8_strain_stress(size, c, xi, u, t, alpha=(0.0, 0.0, 0.0)):

@@ -534,6 +534,18 @@ int orc_recover_hex(size_t npoints, const double* xyz, size_t nel, const uint32_
         return -1;
     }
 }
+// elastic.rs:386-405 (see hex_loads).
+int orc_hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+                  const double* coef, const double* expansion, const double* accel,
+                  const double* dtemp, double* force, char* err, size_t len) {
+    try {
+        hex_loads(npoints, xyz, nel, hexes, coef, expansion, accel, dtemp, force);
+        return 0;
+    } catch (const std::exception& x) {
+        put_error(err, len, x.what());
+        return -1;
+    }
+}
 // hex.rs:218-335 for 1 box cell: its load (24 x 8) and mode matrices (9 x 24, 9 x 8), and the
 // strain and stress at xi for the corner values u and t.
 int orc_hex8_element(const double* size, const double* c, const double* alpha, double* k,

@@ -466,5 +466,35 @@ void hex8_strain_stress(const HexElement& h, const double xi[3], const double u[
     for (int a = 0; a < 3; ++a) s[a] -= h.thermal[a] * dt;
 }
 
+// elastic.rs:386-405 (the force part): over the cells in increasing order, each unknown of each
+// cell gets f = sum_c load[r][c] T_c (from 0.0), plus (its acceleration term, density g_d +
+// body_d, given per cell as `accel`) times the volume / 8. `force` (3 per point) is zeroed first.
+void hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+               const double* coef, const double* expansion, const double* accel,
+               const double* dtemp, double* force) {
+    for (size_t i = 0; i < 3 * npoints; ++i) force[i] = 0.0;
+    HexElement h;
+    for (size_t e = 0; e < nel; ++e) {
+        const uint32_t* nodes = hexes + 8 * e;
+        double size[3], alpha[3] = {0.0, 0.0, 0.0};
+        for (int d = 0; d < 3; ++d) {
+            size[d] = xyz[3 * (size_t)nodes[6] + d] - xyz[3 * (size_t)nodes[0] + d];
+            if (expansion) alpha[d] = expansion[3 * e + d];
+        }
+        const double* c9 = coef + 9 * e;
+        hex8_element(size, orthotropic_stiffness(c9, c9 + 3, c9 + 6), alpha, &h);
+        double t[8];
+        for (int c = 0; c < 8; ++c) t[c] = dtemp ? dtemp[nodes[c]] : 0.0;
+        const double volume = size[0] * size[1] * size[2];
+        for (int r = 0; r < 24; ++r) {
+            double f = 0.0;
+            for (int c = 0; c < 8; ++c) f += h.load[r * 8 + c] * t[c];
+            const int d = r % 3;
+            f += (accel ? accel[3 * e + d] : 0.0) * volume / 8.0;
+            force[3 * (size_t)nodes[r / 3] + d] += f;
+        }
+    }
+}
+
 }  // namespace orc
 

@@ -116,6 +116,10 @@ struct HexElement {
     double k[576], load[192], mode_u[216], mode_t[72];
 };
 void hex8_element(const double size[3], const Stiffness& d, const double alpha[3], HexElement* h);
+// elastic.rs:386-405: the thermal and volume forces of the box cells (3 per point).
+void hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
+               const double* coef, const double* expansion, const double* accel,
+               const double* dtemp, double* force);
 // hex.rs:311-335
 void hex8_strain_stress(const HexElement& h, const double xi[3], const double u[24],
                         const double t[8], double e[6], double s[6]);

@@ -395,3 +395,53 @@ def test_gpu_box_recovery_is_bit_identical_to_the_oracle():
     ref = oracle.recover(c["xyz"], c["hexes"], c["coef"], c["u"], hex=True)
     got = Recovery(c["xyz"], c["hexes"], c["coef"], hex=True).run(c["u"])
     assert np.array_equal(got["stress"].view(np.uint64), ref["stress"].view(np.uint64))
+
+
+def test_oracle_thermal_load_of_a_cell_is_its_free_expansion():
+    """hex.rs:222-297: the load of a uniform temperature change dT equals K times the free
+    thermal expansion (alpha_d dT x_d along each axis), which has no stress; with an
+    orthotropic material and an expansion per axis."""
+    c = oracle.orthotropic([200.0, 120.0, 90.0], [0.25, 0.3, 0.35], [70.0, 60.0, 50.0])
+    alpha = np.array([1e-5, 2e-5, 3e-5])
+    k, load, _, _ = oracle.hex8_element(SIZE, c, alpha)
+    dt = 7.0
+    u = nodal(lambda x: list(alpha * dt * np.asarray(x)))
+    f = load @ np.full(8, dt)
+    assert np.abs(k @ u - f).max() <= 1e-12 * np.abs(f).max()
+
+
+def test_oracle_box_loads_sum_the_cells():
+    """elastic.rs:386-405 over graded cells: with no temperature the forces are the volume
+    terms (an eighth of its cell's at each corner), summing to accel times the volume; with a
+    uniform temperature on a free body of 1 material they equal K times the free expansion."""
+    c = mg.hex_cantilever(nx=4, ny=2, nz=3, grade=1.4)
+    nel = len(c.nodes)
+    accel = np.tile([0.0, -2.0, -9.81], (nel, 1))
+    f = oracle.hex_loads(c.xyz, c.nodes, c.coef, accel=accel)
+    vol = np.prod(c.xyz[c.nodes[:, 6]] - c.xyz[c.nodes[:, 0]], axis=1).sum()
+    assert np.allclose(f.reshape(-1, 3).sum(axis=0), [0.0, -2.0 * vol, -9.81 * vol], rtol=1e-13)
+    alpha = np.tile([1e-5, 1e-5, 1e-5], (nel, 1))
+    dt = np.full(c.mesh.n, 5.0)
+    f = oracle.hex_loads(c.xyz, c.nodes, c.coef, expansion=alpha, dtemp=dt)
+    k = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
+    k.assemble(6, c.xyz, c.nodes, c.coef)
+    u = (1e-5 * 5.0 * c.xyz).ravel()
+    assert np.abs(dense(k) @ u - f).max() <= 1e-12 * np.abs(f).max()
+
+
+@pytest.mark.gpu
+def test_gpu_box_loads_are_bit_identical():
+    """elastic.rs:386-405 on the device against the oracle: graded cells, 2 materials, an
+    expansion per cell, a random temperature change and volume forces."""
+    from femahoy_b200.recover import hex_loads
+    c = hex_recovery_case(seed=6)
+    nel = len(c["hexes"])
+    accel = np.random.default_rng(2).standard_normal((nel, 3))
+    ref = oracle.hex_loads(c["xyz"], c["hexes"], c["coef"], expansion=c["expansion"],
+                           accel=accel, dtemp=c["dtemp"])
+    got = hex_loads(c["xyz"], c["hexes"], c["coef"], expansion=c["expansion"], accel=accel,
+                    dtemp=c["dtemp"])
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+    ref = oracle.hex_loads(c["xyz"], c["hexes"], c["coef"], accel=accel)
+    got = hex_loads(c["xyz"], c["hexes"], c["coef"], accel=accel)
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
