@@ -7,20 +7,20 @@ The Python names mirror the reference crate: ``Csr`` (sparse.rs), ``Solver``, ``
 (pmultigrid.rs), ``Quadratic`` (tet10.rs) and ``reduced_rhs`` (heat.rs); ``Recovery`` and
 ``Peak`` are the post-solve loop of elastic_tet.rs:367-427.
 """
-from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
+from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, HEX8_MASS, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
                    P2_ELASTIC_ORTHO, P2_MASS, FemError, LIB_PATH, lib)
 from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT_LIMIT,
                     Cells, Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
-                    coarse_matrix, hex_elements, prolongation, reduced_rhs)
+                    coarse_matrix, hex_elements, hex_mass, prolongation, reduced_rhs)
 from .recover import Peak, Recovery
 from .sparse import Csr, Rect, colour
 
 __all__ = [
-    "COLOUR", "FP64", "GATHER", "HEX8_ELASTIC", "HEX8_HEAT", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "P2_ELASTIC_ORTHO", "P2_MASS",
+    "COLOUR", "FP64", "GATHER", "HEX8_ELASTIC", "HEX8_HEAT", "HEX8_MASS", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "P2_ELASTIC_ORTHO", "P2_MASS",
     "FemError",
     "LIB_PATH", "lib", "PCG_MAX_ITER", "PCG_TOL", "STEADY_DIRECT_LIMIT",
     "TRANSIENT_DIRECT_LIMIT", "Cells", "Crossover", "Level", "Method", "Options", "Quadratic",
-    "Solver", "coarse_matrix", "hex_elements",
+    "Solver", "coarse_matrix", "hex_elements", "hex_mass",
     "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
     "Recovery",
 ]

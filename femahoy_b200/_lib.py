@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(HERE, "libfemgpu.so")
 OK, CANCELLED, NOT_CONVERGED, NOT_SPD, NEEDS_GRID, INVALID, CUDA, TOO_LARGE, PATTERN, MATERIAL, \
     TIMEOUT = range(11)
 
-P1_HEAT, P1_ELASTIC, P2_ELASTIC, P2_MASS, P2_ELASTIC_ORTHO, HEX8_HEAT, HEX8_ELASTIC = range(7)
+P1_HEAT, P1_ELASTIC, P2_ELASTIC, P2_MASS, P2_ELASTIC_ORTHO, HEX8_HEAT, HEX8_ELASTIC, HEX8_MASS = \
+    range(8)
 GATHER, COLOUR = 0, 1
 FP64, MIXED = 0, 1
 
@@ -52,7 +53,7 @@ class Crossover_t(C.Structure):
 
 class Cells_t(C.Structure):
     _fields_ = [("count", C.c_size_t), ("origin", C.c_void_p), ("cls", C.c_void_p),
-                ("matrices", C.c_void_p), ("nclass", C.c_size_t)]
+                ("matrices", C.c_void_p), ("nclass", C.c_size_t), ("mass", C.c_void_p)]
 
 
 class Options_t(C.Structure):
@@ -132,6 +133,7 @@ SIGNATURES = {
                                           C.POINTER(Crossover_t), C.POINTER(Options_t),
                                           C.POINTER(Cells_t), C.POINTER(C.c_void_p)]),
     "femgpu_hex_elements": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p]),
+    "femgpu_hex_mass": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_coarse_matrix": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.POINTER(Cells_t),
                                        C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
                                        C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -182,6 +184,10 @@ SIGNATURES = {
     "femgpu_modes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_double,
                                C.POINTER(Unknowns_t), C.c_int, C.POINTER(Crossover_t),
                                C.POINTER(Options_t), C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.POINTER(ModesStats_t)]),
+    "femgpu_modes_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_double,
+                               C.POINTER(Unknowns_t), C.c_int, C.POINTER(Crossover_t),
+                               C.POINTER(Options_t), C.POINTER(Cells_t), C.c_void_p, C.c_void_p, C.c_void_p,
                                C.POINTER(ModesStats_t)]),
     "femgpu_dense_generalized": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
                                            C.c_void_p]),

@@ -508,12 +508,26 @@ __global__ void k_hex_keys(const double* __restrict__ xyz, const uint32_t* __res
     }
 }
 
+// hex.rs:337-353: entry (3 a + c, 3 j + b) of the consistent mass of a box cell with the sides
+// s and the density rho: rho times the product of the 1D masses s_d / 3 (a and j at the same end
+// of axis d) or s_d / 6, for c = b; 0 else.
+__device__ __forceinline__ double hex_mass_entry(const double* s, double rho, int a, int j, int c,
+                                                 int b) {
+    if (c != b) return 0.0;
+    double v = 1.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) v *= hex_bit(a, d) == hex_bit(j, d) ? s[d] / 3.0 : s[d] / 6.0;
+    return rho * v;
+}
+
 // One warp per node v, for its 3 rows 3v + c, as k_gather_elastic: the rows 3 a + c of the
-// class matrix of each cell of v (a = v's corner), in increasing cell order.
-template <int WARPS>
+// class matrix of each cell of v (a = v's corner), in increasing cell order. MASS: the box
+// cell's consistent mass instead (coef = the density per cell, the sides from xyz).
+template <int WARPS, bool MASS = false>
 __global__ void __launch_bounds__(32 * WARPS)
     k_gather_hex_elastic(const uint32_t* __restrict__ el, const uint32_t* __restrict__ cls,
-                         const double* __restrict__ table, const int64_t* __restrict__ start,
+                         const double* __restrict__ table, const double* __restrict__ xyz,
+                         const double* __restrict__ coef, const int64_t* __restrict__ start,
                          const uint32_t* __restrict__ of_node, int64_t nnodes,
                          const int64_t* __restrict__ nptr, const uint32_t* __restrict__ nidx,
                          const int64_t* __restrict__ ptr, double* __restrict__ val,
@@ -545,10 +559,23 @@ __global__ void __launch_bounds__(32 * WARPS)
             int an = 0;
             while (an < 8 && nodes[an] != (uint32_t)v) ++an;
             __syncwarp();
-            const double* m = table + 576 * (int64_t)cls[e] + 72 * an;  // rows 3 an .. 3 an + 2
-            for (int o = lane; o < 72; o += 32) {
-                const int c = o / 24, col = o % 24;
-                buf[c * rowlen + 3 * spos[w][col / 3] + col % 3] += m[o];
+            if (MASS) {
+                double sd[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    sd[d] = xyz[3 * (int64_t)nodes[6] + d] - xyz[3 * (int64_t)nodes[0] + d];
+                const double rho = coef[e];
+                for (int o = lane; o < 72; o += 32) {
+                    const int c = o / 24, col = o % 24;
+                    buf[c * rowlen + 3 * spos[w][col / 3] + col % 3] +=
+                        hex_mass_entry(sd, rho, an, col / 3, c, col % 3);
+                }
+            } else {
+                const double* m = table + 576 * (int64_t)cls[e] + 72 * an;  // rows 3 an .. +2
+                for (int o = lane; o < 72; o += 32) {
+                    const int c = o / 24, col = o % 24;
+                    buf[c * rowlen + 3 * spos[w][col / 3] + col % 3] += m[o];
+                }
             }
             __syncwarp();
         }
@@ -838,7 +865,7 @@ __global__ void k_colour_fill(const uint32_t* __restrict__ colour, int64_t nel,
 // ------------------------------------------------------------------ assemble
 void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t nel,
               const uint32_t* d_el, const double* d_coef, Assembled* out, cudaStream_t s) {
-    if (kind < 0 || kind > 6) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
+    if (kind < 0 || kind > 7) throw Failure(FEMGPU_ERR_INVALID, "unknown element kind");
     if (mode < 0 || mode > 1) throw Failure(FEMGPU_ERR_INVALID, "unknown assembly mode");
     if (kind >= FEMGPU_P2_MASS && mode != FEMGPU_ASSEMBLE_GATHER)
         throw Failure(FEMGPU_ERR_INVALID,
@@ -883,10 +910,15 @@ void assemble(int kind, int mode, int64_t npoints, const double* d_xyz, int64_t 
                                    0, s>>>(keys.p, 12, nclass, table.p, bad.p);
             FG_CHECK_LAUNCH();
             k_gather_hex_elastic<4><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
-                d_el, cls.p, table.p, out->inc.start.p, out->inc.of_node.p, npoints,
-                out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
+                d_el, cls.p, table.p, nullptr, nullptr, out->inc.start.p, out->inc.of_node.p,
+                npoints, out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
             FG_CHECK_LAUNCH();
             FG_CUDA(cudaStreamSynchronize(s));
+        } else if (kind == FEMGPU_HEX8_MASS) {
+            k_gather_hex_elastic<4, true><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
+                d_el, nullptr, nullptr, d_xyz, d_coef, out->inc.start.p, out->inc.of_node.p,
+                npoints, out->node.ptr.p, out->node.idx.p, K.ptr.p, K.val.p, bad.p);
+            FG_CHECK_LAUNCH();
         } else if (kind == FEMGPU_P1_ELASTIC) {
             k_gather_elastic<4, 4><<<blocks_for(npoints, 4, NUM_SMS * 64), 128, 0, s>>>(
                 d_xyz, d_el, d_coef, out->inc.start.p, out->inc.of_node.p, npoints,

@@ -71,7 +71,7 @@ static int assemble_impl(int kind, int mode, size_t npoints, const double* xyz, 
         int nn = kind >= FEMGPU_HEX8_HEAT ? 8 : (kind >= FEMGPU_P2_ELASTIC ? 10 : 4);
         int nc = (kind == FEMGPU_P1_HEAT || kind == FEMGPU_HEX8_HEAT)
                      ? 3
-                     : (kind == FEMGPU_P2_MASS
+                     : (kind == FEMGPU_P2_MASS || kind == FEMGPU_HEX8_MASS
                             ? 1
                             : (kind == FEMGPU_P2_ELASTIC_ORTHO || kind == FEMGPU_HEX8_ELASTIC ? 9
                                                                                              : 2));
@@ -313,6 +313,27 @@ int femgpu_solver_new_cells(const femgpu_csr* a, const femgpu_unknowns* u, int m
                             const femgpu_crossover* crossover, const femgpu_options* options,
                             const femgpu_cells* cells, femgpu_solver** out) {
     return solver_new_impl(a, u, method, crossover, options, cells, out);
+}
+
+int femgpu_hex_mass(size_t count, const double* sizes, const double* density, double* out) {
+    return guarded([&] {
+        require(count > 0 && sizes && density && out, "null or empty cells");
+        for (size_t e = 0; e < count; ++e) {
+            const double* s = sizes + 3 * e;
+            double* m = out + 576 * e;
+            std::fill(m, m + 576, 0.0);
+            for (int i = 0; i < 8; ++i)
+                for (int j = 0; j < 8; ++j) {
+                    double v = 1.0;  // the product of the 1D masses, from 1.0
+                    for (int d = 0; d < 3; ++d) {
+                        const int bi = d == 0 ? ((i + 1) >> 1) & 1 : (d == 1 ? (i >> 1) & 1 : i >> 2);
+                        const int bj = d == 0 ? ((j + 1) >> 1) & 1 : (d == 1 ? (j >> 1) & 1 : j >> 2);
+                        v *= bi == bj ? s[d] / 3.0 : s[d] / 6.0;
+                    }
+                    for (int a = 0; a < 3; ++a) m[(3 * i + a) * 24 + 3 * j + a] = density[e] * v;
+                }
+        }
+    });
 }
 
 int femgpu_hex_elements(size_t count, const double* keys, double* matrices) {

@@ -174,10 +174,34 @@ int femgpu_dense_generalized(const double* k, const double* m, size_t n, double*
     });
 }
 
+static int modes_impl(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
+                      const femgpu_unknowns* unknowns, int method,
+                      const femgpu_crossover* crossover, const femgpu_options* options,
+                      const femgpu_cells* cells, const volatile int* cancel, double* values,
+                      double* vectors, femgpu_modes_stats* stats);
+
 int femgpu_modes(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
                  const femgpu_unknowns* unknowns, int method, const femgpu_crossover* crossover,
                  const femgpu_options* options, const volatile int* cancel, double* values,
                  double* vectors, femgpu_modes_stats* stats) {
+    return modes_impl(k, m, count, shift, unknowns, method, crossover, options, nullptr, cancel,
+                      values, vectors, stats);
+}
+
+int femgpu_modes_cells(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
+                       const femgpu_unknowns* unknowns, int method,
+                       const femgpu_crossover* crossover, const femgpu_options* options,
+                       const femgpu_cells* cells, const volatile int* cancel, double* values,
+                       double* vectors, femgpu_modes_stats* stats) {
+    return modes_impl(k, m, count, shift, unknowns, method, crossover, options, cells, cancel,
+                      values, vectors, stats);
+}
+
+static int modes_impl(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
+                      const femgpu_unknowns* unknowns, int method,
+                      const femgpu_crossover* crossover, const femgpu_options* options,
+                      const femgpu_cells* cells, const volatile int* cancel, double* values,
+                      double* vectors, femgpu_modes_stats* stats) {
     return modes_guarded([&] {
         need(k && m && unknowns && values, "null argument");
         const int64_t n = k->m.n;
@@ -229,7 +253,21 @@ int femgpu_modes(const femgpu_csr* k, const femgpu_csr* m, size_t count, double 
         femgpu_crossover c{0, 16384, 0.0, 0, 0};
         if (crossover) c = *crossover;
         femgpu_solver* solver = nullptr;
-        int rc = femgpu_solver_new(&a, unknowns, method, &c, options, &solver);
+        // modes.rs:394-404: each cell's matrix of K - shift M (v -= shift * w), for the coarse
+        // matrices from the cells.
+        std::vector<double> shifted;
+        femgpu_cells sc{};
+        if (cells && cells->count) {
+            need(cells->matrices && cells->mass && cells->nclass > 0,
+                 "the cells of a modes solve need their stiffness and mass matrices");
+            shifted.resize(576 * cells->nclass);
+            for (size_t i = 0; i < shifted.size(); ++i)
+                shifted[i] = cells->matrices[i] - shift * cells->mass[i];
+            sc = *cells;
+            sc.matrices = shifted.data();
+        }
+        int rc = femgpu_solver_new_cells(&a, unknowns, method, &c, options,
+                                         sc.count ? &sc : nullptr, &solver);
         if (rc != FEMGPU_OK) {
             char buf[1024];
             femgpu_last_error(buf, sizeof buf);

@@ -24,10 +24,11 @@ class ModesStats:
 
 def modes(k, m, count, unknowns, method=None, crossover: Crossover | None = None, *,
           shift=None, precision=L.FP64, options: Options | None = None, vectors=True,
-          cancel=None):
+          cancel=None, cells=None):
     """The ``count`` lowest eigenpairs of the free submatrices ``k`` and ``m`` (Csr, the same
     pattern): (values, vectors (count, n) or None, ModesStats). ``shift`` None is
-    modes.rs:186-191's default."""
+    modes.rs:186-191's default. ``cells`` (a Cells with its ``mass``): the box grid's modes
+    (modes.rs:355-420), the solver's coarse matrices from the cells of K - shift M."""
     n = k.n
     keep = []
     u = unknowns_c(unknowns, keep)
@@ -39,10 +40,11 @@ def modes(k, m, count, unknowns, method=None, crossover: Crossover | None = None
     st = L.ModesStats_t()
     mth = -1 if method is None else int(method)
     flag = C.byref(cancel) if isinstance(cancel, C.c_int) else None
-    L.check(L.lib().femgpu_modes(k.handle, m.handle, count,
-                                 float("nan") if shift is None else float(shift), C.byref(u),
-                                 mth, C.byref(cr), C.byref(oc), flag, L.ptr(values),
-                                 L.ptr(vecs), C.byref(st)))
+    cc = C.byref(cells._c(keep)) if cells is not None else None
+    L.check(L.lib().femgpu_modes_cells(k.handle, m.handle, count,
+                                       float("nan") if shift is None else float(shift),
+                                       C.byref(u), mth, C.byref(cr), C.byref(oc), cc, flag,
+                                       L.ptr(values), L.ptr(vecs), C.byref(st)))
     return values, vecs, ModesStats(st.iterations, st.solves, st.pcg_iterations, st.shift,
                                     st.seconds)
 

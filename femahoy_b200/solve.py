@@ -165,13 +165,26 @@ class Cells:
     origin: np.ndarray
     cls: np.ndarray
     matrices: np.ndarray
+    mass: np.ndarray | None = None  # the classes' consistent masses, for the modes
 
     def _c(self, keep):
         o = L.arr(self.origin, np.uint32).reshape(-1, 3)
         c = L.arr(self.cls, np.uint32).ravel()
         m = L.arr(self.matrices, np.float64).reshape(-1, 576)
-        keep += [o, c, m]
-        return L.Cells_t(len(o), o.ctypes.data, c.ctypes.data, m.ctypes.data, len(m))
+        w = None if self.mass is None else L.arr(self.mass, np.float64).reshape(-1, 576)
+        keep += [o, c, m, w]
+        return L.Cells_t(len(o), o.ctypes.data, c.ctypes.data, m.ctypes.data, len(m),
+                         None if w is None else w.ctypes.data)
+
+
+def hex_mass(sizes, density):
+    """hex::mass (hex.rs:337-353) of each box cell: ``sizes`` (K, 3), ``density`` (K,). Returns
+    (K, 24, 24)."""
+    s = L.arr(sizes, np.float64).reshape(-1, 3)
+    d = L.arr(density, np.float64).ravel()
+    out = np.empty((len(s), 24, 24))
+    L.check(L.lib().femgpu_hex_mass(len(s), s.ctypes.data, d.ctypes.data, out.ctypes.data))
+    return out
 
 
 def hex_elements(keys):

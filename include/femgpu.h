@@ -52,12 +52,15 @@ enum {
                              (heat.rs:1246-1273) as heat.rs:820-826 assembles it; coef = the 3
                              conductivities; the sides are corner 6 minus corner 0; gather mode
                              only */
-    FEMGPU_HEX8_ELASTIC = 6 /* box cell of the grid, 8 corners in VTK order: the 24 x 24
+    FEMGPU_HEX8_ELASTIC = 6, /* box cell of the grid, 8 corners in VTK order: the 24 x 24
                                stiffness of the 8-node hex with its 9 incompatible modes condensed
                                (Hex::new, hex.rs:218-297), as elastic.rs:386-391 assembles it;
                                coef = the 9 orthotropic constants of FEMGPU_P2_ELASTIC_ORTHO; the
                                sides are corner 6 minus corner 0 (above 0); unknown 3 node +
                                component; gather mode only */
+    FEMGPU_HEX8_MASS = 7 /* box cell of the grid: the consistent mass of its 8 corners
+                            (hex::mass, hex.rs:337-353), coef = the density per cell, as
+                            modes.rs:363-370 assembles it; gather mode only */
 };
 
 /* Assembly modes. */
@@ -254,6 +257,9 @@ typedef struct femgpu_cells {
     const uint32_t* cls;
     const double* matrices;
     size_t nclass;
+    /* femgpu_modes_cells only: the consistent mass of each class (576 values each, the same
+     * classes; hex::mass, hex.rs:337-353), for the cells of K - shift M (modes.rs:394-401). */
+    const double* mass;
 } femgpu_cells;
 
 /* Solver::new (solve.rs:92-183) with `cells` = None. The solver keeps a copy of `a` on the
@@ -272,6 +278,9 @@ int femgpu_solver_new_cells(const femgpu_csr* a, const femgpu_unknowns* unknowns
  * the condensed 24 x 24 stiffness of each (576 values, row-major), bit-identical with the
  * reference's. */
 int femgpu_hex_elements(size_t count, const double* keys, double* matrices);
+/* hex::mass (hex.rs:337-353) of `count` box cells on the host: `sizes` 3 per cell, `density` 1
+ * per cell; `out` gets 576 values per cell, bit-identical with the reference's. */
+int femgpu_hex_mass(size_t count, const double* sizes, const double* density, double* out);
 /* The matrix of multigrid level `level` (>= 1) that the solver of (a, unknowns, cells) forms
  * (cells may be null: the Galerkin products), with the coarse unknowns in the reference's
  * numbering of multigrid.rs:329-452; `level` coarsenings regardless of the size limits. Two
@@ -475,6 +484,13 @@ int femgpu_modes(const femgpu_csr* k, const femgpu_csr* m, size_t count, double 
 /* eigen.rs:183-269 on the host: K q = lambda M q for dense symmetric row-major n x n matrices,
  * M positive definite, n <= 4096; the eigenvalues ascending and the vectors as the columns of
  * q with Q^T M Q = I (the cyclic Jacobi method of eigen.rs:274-331 inside). No device use. */
+/* modes.rs:355-420 for the box grid: femgpu_modes with `cells` (their `mass` set), whose
+ * solver of K - shift M takes its coarse matrices from the cells' K_e - shift M_e. */
+int femgpu_modes_cells(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
+                       const femgpu_unknowns* unknowns, int method,
+                       const femgpu_crossover* crossover, const femgpu_options* options,
+                       const femgpu_cells* cells, const volatile int* cancel, double* values,
+                       double* vectors, femgpu_modes_stats* stats);
 int femgpu_dense_generalized(const double* k, const double* m, size_t n, double* values,
                              double* q);
 

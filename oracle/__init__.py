@@ -51,6 +51,7 @@ def _load():
         "orc_hex8_strain_stress": (I, [P, P, P, P, P, P, P, P, P, S]),
         "orc_recover_hex": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
         "orc_hex_loads": (I, [S, P, S, P, P, P, P, P, P, P, S]),
+        "orc_hex8_mass": (None, [P, D, P]),
         "orc_assemble": (I, [P, I, P, P, S, P, P, S]),
         "orc_quadratic": (S, [P, S, P, S, P, P]),
         "orc_colour": (I, [S, P, S, I, P]),
@@ -291,6 +292,14 @@ def hex8_element(size, c, alpha=(0.0, 0.0, 0.0)):
                              512):
         raise OracleError(err.value.decode())
     return k.reshape(24, 24), load.reshape(24, 8), mu.reshape(9, 24), mt.reshape(9, 8)
+
+
+def hex8_mass(size, density):
+    """hex.rs:337-353: the 24 x 24 consistent mass of a box cell."""
+    size = np.ascontiguousarray(size, dtype=np.float64)
+    m = np.empty(576)
+    _lib.orc_hex8_mass(_p(size), float(density), _p(m))
+    return m.reshape(24, 24)
 
 
 def hex_loads(xyz, hexes, coef, *, expansion=None, accel=None, dtemp=None):

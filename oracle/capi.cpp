@@ -196,6 +196,20 @@ int orc_assemble(void* h, int kind, const double* xyz, const uint32_t* nodes, si
             }
             return 0;
         }
+        if (kind == 7) {  // modes.rs:363-370: box cells, hex::mass per cell
+            vector<double> me(576);
+            uint32_t dofs[24];
+            for (size_t e = 0; e < nel; ++e) {
+                const uint32_t* t = nodes + 8 * e;
+                double s[3];
+                for (int d = 0; d < 3; ++d)
+                    s[d] = xyz[3 * (size_t)t[6] + d] - xyz[3 * (size_t)t[0] + d];
+                hex8_mass(s, coef[e], me.data());
+                for (int k = 0; k < 24; ++k) dofs[k] = 3 * t[k / 3] + (uint32_t)(k % 3);
+                a->add_element(dofs, 24, me.data());
+            }
+            return 0;
+        }
         if (kind == 6) {  // elastic.rs:386-391: box cells, Hex::new per cell
             vector<double> kc(576);
             uint32_t dofs[24];
@@ -534,6 +548,8 @@ int orc_recover_hex(size_t npoints, const double* xyz, size_t nel, const uint32_
         return -1;
     }
 }
+// hex.rs:337-353
+void orc_hex8_mass(const double* size, double density, double* m) { hex8_mass(size, density, m); }
 // elastic.rs:386-405 (see hex_loads).
 int orc_hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
                   const double* coef, const double* expansion, const double* accel,

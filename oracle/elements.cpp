@@ -426,6 +426,21 @@ void hex8_element(const double size[3], const Stiffness& d, const double alpha[3
     }
 }
 
+// hex.rs:337-353: the consistent mass of the 24 corner unknowns, rho times the product of the
+// 1D masses (a / 3 at the same end, a / 6 across).
+void hex8_mass(const double size[3], double density, double m[576]) {
+    static const int BITS[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+    for (int k = 0; k < 576; ++k) m[k] = 0.0;
+    for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+            double v = 1.0;
+            for (int d = 0; d < 3; ++d)
+                v *= BITS[i][d] == BITS[j][d] ? size[d] / 3.0 : size[d] / 6.0;
+            for (int a = 0; a < 3; ++a) m[(3 * i + a) * 24 + 3 * j + a] = density * v;
+        }
+}
+
 void hex8_stiffness(const double size[3], const Stiffness& d, double kc[576]) {
     const double zero[3] = {0.0, 0.0, 0.0};
     HexElement h;

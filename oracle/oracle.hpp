@@ -116,6 +116,8 @@ struct HexElement {
     double k[576], load[192], mode_u[216], mode_t[72];
 };
 void hex8_element(const double size[3], const Stiffness& d, const double alpha[3], HexElement* h);
+// hex.rs:337-353
+void hex8_mass(const double size[3], double density, double m[576]);
 // elastic.rs:386-405: the thermal and volume forces of the box cells (3 per point).
 void hex_loads(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
                const double* coef, const double* expansion, const double* accel,

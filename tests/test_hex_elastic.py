@@ -445,3 +445,71 @@ def test_gpu_box_loads_are_bit_identical():
     ref = oracle.hex_loads(c["xyz"], c["hexes"], c["coef"], accel=accel)
     got = hex_loads(c["xyz"], c["hexes"], c["coef"], accel=accel)
     assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))
+
+
+def test_oracle_box_mass_is_the_integral_of_the_corner_functions():
+    """hex.rs:408-431: each entry is the 2-point Gauss integral of rho N_i N_j (exact for the
+    trilinear functions), 0 between components, and the entries sum to 3 times the mass."""
+    m = oracle.hex8_mass(SIZE, 7.0)
+    jac = np.prod(SIZE) / 8.0
+    p = 1.0 / np.sqrt(3.0)
+
+    def shape(xi):
+        return np.array([np.prod([0.5 * (1 + xi[d]) if b[d] else 0.5 * (1 - xi[d])
+                                  for d in range(3)]) for b in mg.HEX_BITS])
+    gauss = [np.where(np.asarray(b) == 1, p, -p) for b in mg.HEX_BITS]
+    for i in range(8):
+        for j in range(8):
+            exact = sum(7.0 * shape(x)[i] * shape(x)[j] * jac for x in gauss)
+            assert abs(m[3 * i, 3 * j] - exact) < 1e-14
+            assert m[3 * i, 3 * j + 1] == 0.0
+    assert abs(m.sum() - 3.0 * 7.0 * 8.0 * jac) < 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_box_mass_is_bit_identical():
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=6, ny=2, nz=3, grade=1.3, seed=5)
+    rho = np.random.default_rng(1).uniform(1.0, 8.0, len(c.nodes))
+    M = fg.Csr.assemble(fg.HEX8_MASS, c.xyz, c.nodes, rho)
+    Mo = oracle.pattern(3 * c.n_points, oracle.dof_elements(c.nodes))
+    Mo.assemble(7, c.xyz, c.nodes, rho)
+    for a, b in zip(M.arrays(), Mo.arrays()):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
+    sizes = c.xyz[c.nodes[:4, 6]] - c.xyz[c.nodes[:4, 0]]
+    got = fg.hex_mass(sizes, rho[:4])
+    for e in range(4):
+        assert np.array_equal(got[e].view(np.uint64), oracle.hex8_mass(sizes[e], rho[e]).view(np.uint64))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_box_modes_match_the_oracle(precision):
+    """modes.rs:355-420: the 6 lowest modes of a clamped box-cell cantilever by the device's
+    subspace iteration, its PCG preconditioned by the V-cycle whose coarse matrices come from the
+    cells of K - shift M, against the oracle's subspace iteration (its direct solver):
+    eigenvalues to 1e-8."""
+    import femahoy_b200 as fg
+    from femahoy_b200.modes import modes
+    c = mg.hex_cantilever(nx=40, ny=4, nz=4, length=8.0, width=0.8, depth=0.8, grade=1.1, seed=2)
+    rho = np.where(c.coef[:, 1] == c.coef[:, 0], 7.8e-9, 2.7e-9)  # isotropic: steel
+    Kf = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef).submatrix(c.free)
+    Mf = fg.Csr.assemble(fg.HEX8_MASS, c.xyz, c.nodes, rho).submatrix(c.free)
+    origin, cls, keys = mg.hex_classes(c)
+    first = np.array([np.nonzero(cls == k)[0][0] for k in range(len(keys))])
+    cells = fg.Cells(origin, cls, fg.hex_elements(keys), fg.hex_mass(keys[:, :3], rho[first]))
+    planes, pts, comp = mg.grid_unknowns(c)
+    u = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+    opts = fg.Options(precision=precision, coarsest=300)
+    values, vecs, st = modes(Kf, Mf, 6, u, fg.Method.Multigrid, options=opts, cells=cells)
+    ko = oracle.Csr.from_arrays(Kf.n, *Kf.arrays())
+    mo = oracle.Csr.from_arrays(Mf.n, *Mf.arrays())
+    ptr, idx, val = ko.arrays()
+    a = oracle.Csr.from_arrays(ko.n, ptr, idx, val - st.shift * mo.arrays()[2])
+
+    def solve(b, x0):
+        x, _ = oracle.direct_solve(a, c.xyz[c.free // 3], b)
+        return x
+
+    ov, _, _ = oracle.subspace(ko, mo, st.shift, 6, solve)
+    assert np.abs(values - ov).max() <= 1e-8 * ov.max()
