@@ -245,14 +245,18 @@ def hex_classes(prob):
             keys[first])
 
 
-def lumped_capacity(mesh, capacity=1.0):
-    """crates/fem/src/heat.rs:417-423: each corner of a tetrahedron takes capacity V/4, summed
-    in tetrahedron order."""
-    vol = tet_volumes(mesh.points, mesh.tets)
+def lumped_capacity(mesh, capacity=1.0, cells=None):
+    """crates/fem/src/heat.rs:413-423: each corner of a cell takes capacity V / per (4 corners
+    of a tetrahedron, or 8 of a box cell given as ``cells``), summed over the cells in order and
+    then their corners, as the reference's loop."""
+    if cells is None:
+        cells, vol = mesh.tets, tet_volumes(mesh.points, mesh.tets)
+    else:
+        p = mesh.points
+        vol = np.prod(p[cells[:, 6]] - p[cells[:, 0]], axis=1)
+    per = cells.shape[1]
     out = np.zeros(mesh.n)
-    share = capacity * vol / 4.0
-    for c in range(4):
-        np.add.at(out, mesh.tets[:, c], share)
+    np.add.at(out, cells.ravel(), np.repeat(capacity * vol / per, per))
     return out
 
 

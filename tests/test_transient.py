@@ -78,10 +78,10 @@ def test_oracle_transient_right_side_matches_its_definition():
 # ------------------------------------------------------------------ the device loop
 
 
-def gpu_run(h, cap, dt, steps, every, method, precision):
+def gpu_run(h, cap, dt, steps, every, method, precision, kind=None):
     import femahoy_b200 as fg
     from femahoy_b200.transient import Transient
-    K = fg.Csr.assemble(fg.P1_HEAT, h.xyz, h.nodes, h.coef)
+    K = fg.Csr.assemble(fg.P1_HEAT if kind is None else kind, h.xyz, h.nodes, h.coef)
     planes, pts, comp = mg.grid_unknowns(h)
     u = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
     m = fg.Method.Direct if method == "direct" else fg.Method.Multigrid
@@ -137,3 +137,24 @@ def test_gpu_transient_cancelled():
     with pytest.raises(fg.FemError) as e:
         Transient(K, cap, 0.0, h.free, fg.Unknowns.Grid(fg.Level(planes, pts, comp)))
     assert "time step" in str(e.value)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gpu_transient_on_box_cells_matches_the_oracle(precision):
+    """The box grid's transient heat (heat.rs:413-423 with 8 corners per cell, 686-733): the
+    device loop on hex8 conduction cells against the oracle's, multigrid, to 1e-8."""
+    import femahoy_b200 as fg
+    h = mg.heat_cube_hex(14, seed=3)
+    k = oracle.pattern(h.n_points, h.nodes)
+    k.assemble(5, h.xyz, h.nodes, h.coef)
+    cap = mg.lumped_capacity(h.mesh, capacity=3.0, cells=h.nodes)
+    dt, steps, every = 0.02, 8, 4
+    _, (frames, energies, _, _) = gpu_run(h, cap, dt, steps, every, "multigrid", precision,
+                                          kind=fg.HEX8_HEAT)
+    of, oe, _ = oracle.transient(k, cap, dt, h.free, h.load, h.values, steps,
+                                 oracle_solver(h, "multigrid"), output_every=every)
+    for g, o in zip(frames, of):
+        assert np.abs(g - o).max() <= 1e-8 * np.abs(o).max()
+    for g, o in zip(energies, oe):
+        assert abs(g.stored - o[0]) <= 1e-8 * o[2]
