@@ -148,6 +148,8 @@ SIGNATURES = {
                                       C.POINTER(Stats_t)]),
     "femgpu_solver_solve_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.POINTER(Stats_t)]),
+    "femgpu_solver_solve_zero": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.POINTER(Stats_t)]),
     "femgpu_solver_precondition_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_solver_free": (None, [C.c_void_p]),
     "femgpu_solver_stream": (C.c_void_p, [C.c_void_p]),

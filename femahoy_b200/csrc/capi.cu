@@ -486,6 +486,14 @@ int femgpu_solver_solve(femgpu_solver* s, const double* b, double* x, const vola
     });
 }
 
+int femgpu_solver_solve_zero(femgpu_solver* s, const double* b, double* x,
+                             const volatile int* cancel, femgpu_stats* stats) {
+    return guarded([&] {
+        require(s && b && x, "null argument");
+        s->impl.solve_host_zero(b, x, cancel, stats);
+    });
+}
+
 int femgpu_solver_solve_device(femgpu_solver* s, const double* b, double* x,
                                const volatile int* cancel, femgpu_stats* stats) {
     return guarded([&] {

@@ -2145,6 +2145,21 @@ void SolverImpl::solve_host(const double* h_b, double* h_x, const volatile int* 
     FG_CUDA(cudaStreamSynchronize(s_));
 }
 
+void SolverImpl::solve_host_zero(const double* h_b, double* h_x, const volatile int* cancel,
+                                 femgpu_stats* st) {
+    FG_CUDA(cudaMemcpyAsync(b_.p, h_b, n_ * 8, cudaMemcpyHostToDevice, s_));
+    FG_CUDA(cudaMemsetAsync(x_.p, 0, n_ * 8, s_));
+    try {
+        solve(b_.p, x_.p, cancel, st);
+    } catch (const Failure&) {
+        cudaMemcpyAsync(h_x, x_.p, n_ * 8, cudaMemcpyDeviceToHost, s_);
+        cudaStreamSynchronize(s_);
+        throw;
+    }
+    FG_CUDA(cudaMemcpyAsync(h_x, x_.p, n_ * 8, cudaMemcpyDeviceToHost, s_));
+    FG_CUDA(cudaStreamSynchronize(s_));
+}
+
 void SolverImpl::precondition(const double* d_r, double* d_z) {
     FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
     if (direct_) {

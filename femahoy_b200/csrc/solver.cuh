@@ -226,6 +226,9 @@ class SolverImpl {
     // solve.rs:199-250 on device vectors
     void solve(const double* d_b, double* d_x, const volatile int* cancel, femgpu_stats* st);
     void solve_host(const double* h_b, double* h_x, const volatile int* cancel, femgpu_stats* st);
+    // The same from x = 0: x is written only (no host-to-device copy of a start value).
+    void solve_host_zero(const double* h_b, double* h_x, const volatile int* cancel,
+                         femgpu_stats* st);
     void precondition(const double* d_r, double* d_z);
     int method() const { return direct_ ? FEMGPU_METHOD_DIRECT : FEMGPU_METHOD_MULTIGRID; }
     std::vector<int64_t> level_sizes() const;

@@ -305,6 +305,20 @@ class Solver:
         L.check(L.lib().femgpu_solver_solve(self._h, L.ptr(b), L.ptr(x), flag, C.byref(st)))
         return Stats(st.iterations, st.residual, st.true_residual, st.seconds, st.launches)
 
+    def solve_zero(self, b, x=None, cancelled=None) -> Stats:
+        """``solve`` from x = 0 (the start value of the reference's steady callers): ``x`` only
+        gets the solution, so its start value is not copied to the device."""
+        b = L.arr(b, np.float64)
+        if x is None:
+            x = np.empty(self.n)
+        if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+            raise TypeError("x must be a contiguous float64 numpy array (it gets the solution)")
+        flag = C.byref(cancelled) if isinstance(cancelled, C.c_int) else None
+        st = L.Stats_t()
+        L.check(L.lib().femgpu_solver_solve_zero(self._h, L.ptr(b), L.ptr(x), flag,
+                                                 C.byref(st)))
+        return Stats(st.iterations, st.residual, st.true_residual, st.seconds, st.launches)
+
     def solve_device(self, b_ptr: int, x_ptr: int, cancel=None) -> Stats:
         """The same on device vectors (raw CUDA pointers, e.g. torch ``data_ptr()``)."""
         st = L.Stats_t()

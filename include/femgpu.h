@@ -314,6 +314,11 @@ int femgpu_solver_solve(femgpu_solver* s, const double* b, double* x, const vola
                         femgpu_stats* stats);
 int femgpu_solver_solve_device(femgpu_solver* s, const double* b, double* x,
                                const volatile int* cancel, femgpu_stats* stats);
+/* femgpu_solver_solve from the start value x = 0, as every steady caller of the reference
+ * passes it (heat.rs:672, elastic.rs:561, elastic_tet.rs:329, dc.rs:270): `x` is only written,
+ * so its start value is not copied to the device. */
+int femgpu_solver_solve_zero(femgpu_solver* s, const double* b, double* x,
+                             const volatile int* cancel, femgpu_stats* stats);
 /* z = M^-1 r: 1 application of the preconditioner (a V-cycle), device vectors. */
 int femgpu_solver_precondition_device(femgpu_solver* s, const double* r, double* z);
 void femgpu_solver_free(femgpu_solver* s);

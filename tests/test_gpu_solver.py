@@ -313,3 +313,18 @@ def test_block_operators_match_sell_for_elasticity(precision):
         st = s.solve(rhs, x)
         assert st.true_residual <= 1.2e-10
         assert _rel(x, xd) <= 1e-6
+
+
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_solve_from_zero_equals_solve_with_a_zero_start(precision):
+    """femgpu_solver_solve_zero (x written only) gives the bits of femgpu_solver_solve from a
+    zero start value, whatever the output array held before."""
+    h = mg.heat_cube(20, seed=7)
+    A, rhs, _ = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision).with_tol(1e-10)
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    y = np.full(A.n, np.nan)
+    sz = s.solve_zero(rhs, y)
+    assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
+    assert (st.iterations, st.residual) == (sz.iterations, sz.residual)
