@@ -11,7 +11,8 @@ from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, HEX8_MASS, MIX
                    P2_ELASTIC_ORTHO, P2_MASS, FemError, LIB_PATH, lib)
 from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT_LIMIT,
                     Cells, Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
-                    coarse_matrix, hex_elements, hex_mass, prolongation, reduced_rhs)
+                    coarse_matrix, hex_elements, hex_mass, prolongation, reduced_rhs,
+                    symbolic_counts)
 from .recover import Peak, Recovery
 from .sparse import Csr, Rect, colour
 
@@ -20,7 +21,7 @@ __all__ = [
     "FemError",
     "LIB_PATH", "lib", "PCG_MAX_ITER", "PCG_TOL", "STEADY_DIRECT_LIMIT",
     "TRANSIENT_DIRECT_LIMIT", "Cells", "Crossover", "Level", "Method", "Options", "Quadratic",
-    "Solver", "coarse_matrix", "hex_elements", "hex_mass",
+    "Solver", "coarse_matrix", "hex_elements", "hex_mass", "symbolic_counts",
     "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
     "Recovery",
 ]

@@ -133,6 +133,8 @@ SIGNATURES = {
                                           C.POINTER(Crossover_t), C.POINTER(Options_t),
                                           C.POINTER(Cells_t), C.POINTER(C.c_void_p)]),
     "femgpu_hex_elements": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p]),
+    "femgpu_symbolic_counts": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t),
+                                         C.POINTER(C.c_uint64), C.POINTER(C.c_double)]),
     "femgpu_hex_mass": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_coarse_matrix": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.POINTER(Cells_t),
                                        C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),

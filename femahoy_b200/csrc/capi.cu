@@ -348,6 +348,25 @@ int femgpu_hex_elements(size_t count, const double* keys, double* matrices) {
     });
 }
 
+int femgpu_symbolic_counts(const femgpu_csr* a, const femgpu_unknowns* u, uint64_t* entries,
+                           double* flops) {
+    return guarded([&] {
+        require(a && u && entries && flops, "null argument");
+        require(u->kind != FEMGPU_UNKNOWNS_QUADRATIC || u->xyz, "quadratic needs coordinates");
+        HostCsr m = download_csr(a->m, util_stream());
+        std::vector<double> xyz((size_t)3 * m.n);
+        if (u->kind == FEMGPU_UNKNOWNS_GRID) {
+            HostLevel lv = host_level(u, m.n);
+            for (int64_t k = 0; k < m.n; ++k)
+                for (int d = 0; d < 3; ++d) xyz[3 * k + d] = lv.planes[d][lv.points[k][d]];
+        } else {
+            require(u->xyz != nullptr, "points need coordinates");
+            std::copy(u->xyz, u->xyz + 3 * m.n, xyz.begin());
+        }
+        factor_counts(m, nested_dissection(m, xyz.data()), entries, flops);
+    });
+}
+
 int femgpu_coarse_matrix(const femgpu_csr* a, const femgpu_unknowns* u,
                          const femgpu_cells* cells, int level, size_t* n, size_t* nnz,
                          int64_t* ptr, uint32_t* idx, double* val) {

@@ -63,6 +63,19 @@ struct HostCells {
 HostCsr by_cells(const HostLevel& fine, const HostCells& cells, const HostLevel& coarse,
                  HostCells* next, int threads);
 
+// order.rs:19-198: the nested dissection order of the symmetric pattern `a` from the coordinates
+// of each node (3 per node): item k is the old index of the new node k. Coordinate bisection at
+// the best of 5 quantile cuts per axis, the separator from the smaller side, sets of at most 64
+// nodes not split.
+std::vector<int64_t> nested_dissection(const HostCsr& a, const double* xyz);
+
+// symbolic.rs:41-183: the entries (with the diagonal) and the floating point operations of the
+// Cholesky factor of P A P^T for the order `order`, from the elimination tree, its postorder,
+// the column counts and the fundamental supernodes; what the reference's Crossover::Flops reads
+// (solve.rs:108-118, 160-172).
+void factor_counts(const HostCsr& a, const std::vector<int64_t>& order, uint64_t* entries,
+                   double* flops);
+
 // pmultigrid.rs:104-151
 void prolongation(const double* points, int64_t npoints, int64_t corners, const uint32_t* edges,
                   int64_t nedges, const int64_t* free, int64_t nfree, HostRect* p,

@@ -1490,6 +1490,9 @@ std::string SolverImpl::describe() const {
                   direct_ ? "direct" : "multigrid",
                   opt_.precision == FEMGPU_MIXED ? "mixed" : "fp64", (long long)n_);
     out += buf;
+    if (crossover_note_)
+        out += "the crossover chose the sparse direct factor; above the dense solver's 16384 "
+               "unknowns, multigrid runs instead\n";
     if (direct_) return out;
     out += "outer fp64: " + describe_op(op64_) + "\n";
     auto levels = [&](const auto& H, const char* t) {
@@ -1560,12 +1563,13 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
     q_.alloc(n_);
     b_.alloc(n_);
     t_.alloc(n_);
-    if (c.rule != 0 && method < 0)
-        throw Failure(FEMGPU_ERR_INVALID,
-                      "Crossover::Flops needs the symbolic analysis of a sparse factor, which this "
-                      "library does not form: force a method");
     // solve.rs:99-183: the choice of the method.
     bool direct;
+    HostCsr h;
+    {
+        PhaseTimer t{this, "matrix to host", s_};
+        h = download_csr(a_, s_);
+    }
     if (u.kind == FEMGPU_UNKNOWNS_POINTS) {
         if (method == FEMGPU_METHOD_MULTIGRID)
             throw Failure(FEMGPU_ERR_NEEDS_GRID,
@@ -1575,15 +1579,30 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         direct = true;
     } else if (method == FEMGPU_METHOD_MULTIGRID) {
         direct = false;
-    } else {
+    } else if (c.rule == 0) {
         direct = (size_t)a.n <= c.unknowns;
+    } else {
+        // Crossover::Flops (solve.rs:108-118, 160-172): the sparse factor's entries and flops
+        // in the nested dissection order of the unknowns' points.
+        PhaseTimer t{this, "symbolic analysis for the crossover (host)", s_};
+        std::vector<double> xyz((size_t)3 * a.n);
+        for (int64_t k = 0; k < a.n; ++k)
+            for (int d = 0; d < 3; ++d)
+                xyz[3 * k + d] = u.kind == FEMGPU_UNKNOWNS_GRID
+                                     ? u.planes[d][u.points[3 * k + d]]
+                                     : u.xyz[3 * k + d];
+        uint64_t entries = 0;
+        double flops = 0.0;
+        factor_counts(h, nested_dissection(h, xyz.data()), &entries, &flops);
+        direct = entries <= c.entries && (c.flat || flops <= c.flops * (double)a.n);
+        // The direct solver here is a dense factor of at most 16,384 unknowns; a larger system
+        // that the rule gives to the sparse factor runs multigrid instead.
+        if (direct && a.n > 16384) {
+            direct = false;
+            crossover_note_ = true;
+        }
     }
     direct_ = direct;
-    HostCsr h;
-    {
-        PhaseTimer t{this, "matrix to host", s_};
-        h = download_csr(a_, s_);
-    }
     if (direct) {
         dense_direct(h);
         sizes_ = {n_};

@@ -247,6 +247,7 @@ class SolverImpl {
     void phase(const std::string& name, double seconds);
 
    private:
+    bool crossover_note_ = false;  // the Flops rule chose a direct solve too large for it
     void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
                          const HostCells* cells);
     template <class T>

@@ -196,6 +196,16 @@ def hex_elements(keys):
     return out
 
 
+def symbolic_counts(a: Csr, unknowns: Unknowns):
+    """(entries, flops) of the sparse Cholesky factor of ``a`` in the nested dissection order of
+    the unknowns' points (order.rs, symbolic.rs): what Crossover.Flops compares."""
+    keep = []
+    u = unknowns_c(unknowns, keep)
+    e, f = C.c_uint64(), C.c_double()
+    L.check(L.lib().femgpu_symbolic_counts(a.handle, C.byref(u), C.byref(e), C.byref(f)))
+    return e.value, f.value
+
+
 def coarse_matrix(a: Csr, unknowns: Unknowns, level: int, cells: Cells | None = None):
     """The matrix (ptr, idx, val) of multigrid level ``level`` as the solver forms it (the
     Galerkin products, or with ``cells`` the cell-condensed matrices), its unknowns numbered as

@@ -194,7 +194,9 @@ typedef struct femgpu_unknowns {
     const uint8_t* coarse_comp;
 } femgpu_unknowns;
 
-/* solve.rs:28-39 `Crossover`: rule 0 = Unknowns(unknowns); 1 = Flops{flops, entries, flat}. */
+/* solve.rs:28-39 `Crossover`: rule 0 = Unknowns(unknowns); 1 = Flops{flops, entries, flat} (the
+ * sparse factor's figures of femgpu_symbolic_counts; a direct choice above 16,384 unknowns runs
+ * multigrid, the direct solver here being dense). */
 typedef struct femgpu_crossover {
     int rule;
     size_t unknowns;
@@ -281,6 +283,13 @@ int femgpu_hex_elements(size_t count, const double* keys, double* matrices);
 /* hex::mass (hex.rs:337-353) of `count` box cells on the host: `sizes` 3 per cell, `density` 1
  * per cell; `out` gets 576 values per cell, bit-identical with the reference's. */
 int femgpu_hex_mass(size_t count, const double* sizes, const double* density, double* out);
+/* The entries (with the diagonal) and the floating point operations of the sparse Cholesky
+ * factor of `a` in the nested dissection order of the unknowns' points (order.rs:19-198,
+ * symbolic.rs:41-183): the figures Crossover::Flops compares (solve.rs:108-118, 160-172), which
+ * femgpu_solver_new applies. A direct choice above the dense direct solver's 16,384 unknowns runs
+ * multigrid. No reference counterpart as an entry point: for checking the crossover. */
+int femgpu_symbolic_counts(const femgpu_csr* a, const femgpu_unknowns* unknowns,
+                           uint64_t* entries, double* flops);
 /* The matrix of multigrid level `level` (>= 1) that the solver of (a, unknowns, cells) forms
  * (cells may be null: the Galerkin products), with the coarse unknowns in the reference's
  * numbering of multigrid.rs:329-452; `level` coarsenings regardless of the size limits. Two

@@ -52,6 +52,7 @@ def _load():
         "orc_recover_hex": (I, [S, P, S, P, P, P, P, P, P, S, P, P, P, P, P, P, P, S]),
         "orc_hex_loads": (I, [S, P, S, P, P, P, P, P, P, P, S]),
         "orc_hex8_mass": (None, [P, D, P]),
+        "orc_symbolic_counts": (None, [P, P, P, P]),
         "orc_assemble": (I, [P, I, P, P, S, P, P, S]),
         "orc_quadratic": (S, [P, S, P, S, P, P]),
         "orc_colour": (I, [S, P, S, I, P]),
@@ -292,6 +293,15 @@ def hex8_element(size, c, alpha=(0.0, 0.0, 0.0)):
                              512):
         raise OracleError(err.value.decode())
     return k.reshape(24, 24), load.reshape(24, 8), mu.reshape(9, 24), mt.reshape(9, 8)
+
+
+def symbolic_counts(a: Csr, xyz):
+    """symbolic.rs:162-182 (entries, flops) of the factor of ``a`` in the nested dissection
+    order of ``xyz`` (order.rs:19-198)."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+    e, f = C.c_uint64(), C.c_double()
+    _lib.orc_symbolic_counts(a.h, _p(xyz), C.byref(e), C.byref(f))
+    return e.value, f.value
 
 
 def hex8_mass(size, density):

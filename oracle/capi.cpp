@@ -548,6 +548,12 @@ int orc_recover_hex(size_t npoints, const double* xyz, size_t nel, const uint32_
         return -1;
     }
 }
+// symbolic.rs:162-182 of the analysis of `a` in the nested dissection order of `xyz` (order.rs).
+void orc_symbolic_counts(void* a, const double* xyz, uint64_t* entries, double* flops) {
+    Symbolic sym = analyse(*C(a), nested_dissection(*C(a), make_points(xyz, C(a)->n)));
+    *entries = sym.entries();
+    *flops = sym.flops();
+}
 // hex.rs:337-353
 void orc_hex8_mass(const double* size, double density, double* m) { hex8_mass(size, density, m); }
 // elastic.rs:386-405 (see hex_loads).

@@ -328,3 +328,48 @@ def test_solve_from_zero_equals_solve_with_a_zero_start(precision):
     sz = s.solve_zero(rhs, y)
     assert np.array_equal(x.view(np.uint64), y.view(np.uint64))
     assert (st.iterations, st.residual) == (sz.iterations, sz.residual)
+
+
+def _symbolic_cases():
+    h = mg.heat_cube(10, seed=4)
+    c = mg.hex_cantilever(nx=24, ny=3, nz=4, grade=1.2, seed=1)
+    return [("heat", h, 0), ("box cells", c, 6)]
+
+
+@pytest.mark.parametrize("case", [0, 1])
+def test_symbolic_counts_equal_the_oracle(case):
+    """order.rs + symbolic.rs restated in the library: the factor's entries and flops in the
+    nested dissection order equal the oracle's (flops bit for bit)."""
+    name, prob, kind = _symbolic_cases()[case]
+    K = fg.Csr.assemble(kind, prob.xyz, prob.nodes, prob.coef)
+    A = K.submatrix(prob.free)
+    e, f = fg.symbolic_counts(A, _grid(prob))
+    nodes = prob.nodes if kind == 0 else oracle.dof_elements(prob.nodes)
+    Ko = oracle.pattern(prob.n_unknowns, nodes)
+    Ko.assemble(kind, prob.xyz, prob.nodes, prob.coef)
+    planes, pts, comp = mg.grid_unknowns(prob)
+    xyz = np.stack([planes[d][pts[:, d]] for d in range(3)], axis=1)
+    eo, fo = oracle.symbolic_counts(Ko.submatrix(prob.free), xyz)
+    assert e == eo and np.float64(f).view(np.uint64) == np.float64(fo).view(np.uint64), (name, e, eo)
+
+
+def test_flops_crossover_chooses_as_the_reference():
+    """solve.rs:160-172 with the box-grid elastic rule Flops{1.5e5, 2.5e8, flat} (elastic.rs:537):
+    the library's method equals the oracle's for a small beam (direct, 1,480 flops per unknown),
+    a thick one (multigrid, 1.8e5) and the same thick one called flat (direct)."""
+    cases = [(mg.hex_cantilever(nx=6, ny=2, nz=2), False),
+             (mg.hex_cantilever(nx=16, ny=14, nz=14), False),
+             (mg.hex_cantilever(nx=16, ny=14, nz=14), True)]
+    seen = set()
+    for c, flat in cases:
+        K = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef)
+        A = K.submatrix(c.free)
+        s = fg.Solver(A, _grid(c), None, fg.Crossover.Flops(1.5e5, 250_000_000, flat))
+        Ko = oracle.pattern(3 * c.n_points, oracle.dof_elements(c.nodes))
+        Ko.assemble(6, c.xyz, c.nodes, c.coef)
+        planes, pts, comp = mg.grid_unknowns(c)
+        so = oracle.Solver(Ko.submatrix(c.free), "grid", planes=planes, points=pts, comp=comp,
+                           crossover=("flops", 1.5e5, 250_000_000, flat))
+        assert s.method().name.lower() == so.method(), (A.n, flat)
+        seen.add(so.method())
+    assert seen == {"direct", "multigrid"}
