@@ -513,3 +513,27 @@ def test_gpu_box_modes_match_the_oracle(precision):
 
     ov, _, _ = oracle.subspace(ko, mo, st.shift, 6, solve)
     assert np.abs(values - ov).max() <= 1e-8 * ov.max()
+
+
+@pytest.mark.gpu
+def test_gpu_box_cell_errors():
+    """The box-cell kinds assemble by rows only; a cell with a side not above 0 is refused; the
+    cells of a solver must lie inside the planes; coarsening past the grid is refused."""
+    import femahoy_b200 as fg
+    c = mg.hex_cantilever(nx=4, ny=2, nz=2)
+    for kind, coef in ((fg.HEX8_ELASTIC, c.coef), (fg.HEX8_MASS, np.ones(len(c.nodes)))):
+        with pytest.raises(fg.FemError, match="assemble by rows"):
+            fg.Csr.assemble(kind, c.xyz, c.nodes, coef, mode=fg.COLOUR)
+    flipped = c.nodes[:, [6, 7, 4, 5, 2, 3, 0, 1]]  # corner 6 below corner 0
+    with pytest.raises(fg.FemError, match="side not above 0"):
+        fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, flipped, c.coef)
+    K = fg.Csr.assemble(fg.HEX8_ELASTIC, c.xyz, c.nodes, c.coef)
+    A = K.submatrix(c.free)
+    planes, pts, comp = mg.grid_unknowns(c)
+    u = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+    cells, _ = cells_of(c, fg)
+    bad = fg.Cells(cells.origin + np.array([10, 0, 0], np.uint32), cells.cls, cells.matrices)
+    with pytest.raises(fg.FemError, match="past the planes"):
+        fg.Solver(A, u, fg.Method.Multigrid, cells=bad)
+    with pytest.raises(fg.FemError, match="does not coarsen"):
+        fg.coarse_matrix(A, u, 5, cells)
