@@ -369,12 +369,8 @@ def test_oracle_box_recovery_peaks_follow_the_loop():
         assert (pk.regular_element, pk.regular_local) == reg[p][1:]
 
 
-@pytest.mark.gpu
-def test_gpu_box_recovery_is_bit_identical_to_the_oracle():
-    """elastic.rs:615-660 on the device against the oracle: stress, strain and von Mises bit for
-    bit, the principal stresses to 1e-12 of the largest stress (acos, cos), the peaks equal."""
+def box_recovery_parity(c):
     from femahoy_b200.recover import Recovery
-    c = hex_recovery_case()
     ref = oracle.recover(c["xyz"], c["hexes"], c["coef"], c["u"], expansion=c["expansion"],
                          dtemp=c["dtemp"], part=c["part"], nparts=c["nparts"],
                          singular=c["singular"], hex=True)
@@ -383,8 +379,33 @@ def test_gpu_box_recovery_is_bit_identical_to_the_oracle():
     got = rec.run(c["u"], c["dtemp"])
     for key in ("stress", "strain", "mises"):
         assert np.array_equal(np.asarray(got[key]).view(np.uint64), ref[key].view(np.uint64)), key
-    scale = np.abs(ref["stress"]).max()
-    assert np.abs(got["principal"] - ref["principal"]).max() <= 1e-12 * scale
+    scale = np.nanmax(np.abs(ref["stress"]))
+    assert np.allclose(got["principal"], ref["principal"], rtol=0, atol=1e-12 * scale,
+                       equal_nan=True)
+    return ref, got
+
+
+@pytest.mark.gpu
+def test_gpu_box_recovery_ties_and_nan():
+    """All displacements 0 (every strain 0, ties: the first visit wins), then a NaN displacement
+    at a corner: the strains of its cells are NaN at every corner, as the reference's sums over
+    the 11 functions make them (a zero gradient times NaN is NaN)."""
+    c = hex_recovery_case(seed=9)
+    c["u"] = np.zeros_like(c["u"])
+    c["dtemp"] = np.zeros_like(c["dtemp"])
+    box_recovery_parity(c)
+    c["u"][3 * int(c["hexes"][5, 2]) + 1] = np.nan
+    ref, _ = box_recovery_parity(c)
+    assert np.isnan(ref["strain"][c["hexes"][5, 0]]).any()
+
+
+@pytest.mark.gpu
+def test_gpu_box_recovery_is_bit_identical_to_the_oracle():
+    """elastic.rs:615-660 on the device against the oracle: stress, strain and von Mises bit for
+    bit, the principal stresses to 1e-12 of the largest stress (acos, cos), the peaks equal."""
+    from femahoy_b200.recover import Recovery
+    c = hex_recovery_case()
+    ref, got = box_recovery_parity(c)
     for g, o in zip(got["peaks"], ref["peaks"]):
         assert (g.element, g.local, g.point, int(g.singular), g.regular_element, g.regular_local,
                 g.regular_point) == (o.element, o.local, o.point, int(o.singular),
