@@ -69,7 +69,8 @@ def args():
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
                    choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover",
-                            "transient", "modes", "hexheat", "hexbeam", "hexrecover"],
+                            "transient", "modes", "hexheat", "hexbeam", "hexrecover",
+                            "hexmodes"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
@@ -79,7 +80,8 @@ def args():
                         "modes: 10 lowest modes of a 100x10x10 P2 beam; hexheat: the 128^3 "
                         "heat cube on box cells; hexbeam: a cantilever of 256x32x32 box cells "
                         "with incompatible modes (2 materials); hexrecover: the stress "
-                        "recovery of that cantilever")
+                        "recovery of that cantilever; hexmodes: 10 modes of a 128x16x16 "
+                        "box-cell cantilever")
     p.add_argument("--by-cells", action="store_true",
                    help="hexbeam: the coarse matrices from the cells, as the reference forms "
                         "them (default: Galerkin products, fewer iterations here)")
@@ -1101,26 +1103,45 @@ def run_modes(opt, rank, world, local):
     from femahoy_b200.modes import modes
     torch.cuda.set_device(local)
     dist, barrier, max_over_ranks = _plumbing(world)
-    box = mg.box(100, 10, 10, (200.0, 20.0, 20.0))
-    q = fg.Quadratic.new(box.points, box.tets)
-    prob = mg.beam_p2(q.edges, q.tets, mesh=box, seed=SEED)
-    density = np.full(len(q.tets), 2.7e-9)
-    free = prob.free
+    hexes = opt.workload == "hexmodes"
+    cells = None
     t0 = time.perf_counter()
-    Kf = fg.Csr.assemble(fg.P2_ELASTIC, prob.xyz, prob.nodes, prob.coef).submatrix(free)
-    Mf = fg.Csr.assemble(fg.P2_MASS, prob.xyz, prob.nodes, density).submatrix(free)
-    P, coarse = fg.prolongation(prob.xyz, box.n, q.edges, free)
-    u = fg.Unknowns.Quadratic(prob.xyz[free // 3], P, coarse)
+    if hexes:
+        # modes.rs:355-420: a box-cell cantilever of steel, the coarse matrices from the cells
+        # of K - shift M.
+        prob = mg.hex_cantilever(nx=128, ny=16, nz=16, length=8.0, width=1.0, depth=1.0,
+                                 e=210e3, nu=0.3, load=0.0)
+        free = prob.free
+        density = np.full(len(prob.nodes), 7.85e-9)
+        Kf = fg.Csr.assemble(fg.HEX8_ELASTIC, prob.xyz, prob.nodes, prob.coef).submatrix(free)
+        Mf = fg.Csr.assemble(fg.HEX8_MASS, prob.xyz, prob.nodes, density).submatrix(free)
+        origin, cls, keys = mg.hex_classes(prob)
+        cells = fg.Cells(origin, cls, fg.hex_elements(keys),
+                         fg.hex_mass(keys[:, :3], np.full(len(keys), 7.85e-9)))
+        planes, pts, comp = mg.grid_unknowns(prob)
+        u = fg.Unknowns.Grid(fg.Level(planes, pts, comp))
+    else:
+        box = mg.box(100, 10, 10, (200.0, 20.0, 20.0))
+        q = fg.Quadratic.new(box.points, box.tets)
+        prob = mg.beam_p2(q.edges, q.tets, mesh=box, seed=SEED)
+        density = np.full(len(q.tets), 2.7e-9)
+        free = prob.free
+        Kf = fg.Csr.assemble(fg.P2_ELASTIC, prob.xyz, prob.nodes, prob.coef).submatrix(free)
+        Mf = fg.Csr.assemble(fg.P2_MASS, prob.xyz, prob.nodes, density).submatrix(free)
+        P, coarse = fg.prolongation(prob.xyz, box.n, q.edges, free)
+        u = fg.Unknowns.Quadratic(prob.xyz[free // 3], P, coarse)
     assemble_s = time.perf_counter() - t0
     opts = fg.Options(precision=fg.MIXED)
     for _ in range(max(1, opt.warmup)):
-        values, _, st = modes(Kf, Mf, 10, u, fg.Method.Multigrid, options=opts, vectors=False)
+        values, _, st = modes(Kf, Mf, 10, u, fg.Method.Multigrid, options=opts, vectors=False,
+                              cells=cells)
     barrier()
     clocks = Clocks(torch.cuda.current_device())
     clocks.start()
     t0 = time.perf_counter()
     for _ in range(opt.steps):
-        values, _, st = modes(Kf, Mf, 10, u, fg.Method.Multigrid, options=opts, vectors=False)
+        values, _, st = modes(Kf, Mf, 10, u, fg.Method.Multigrid, options=opts, vectors=False,
+                              cells=cells)
     torch.cuda.synchronize()
     wall = max_over_ranks(time.perf_counter() - t0)
     clk = clocks.stop()
@@ -1132,16 +1153,22 @@ def run_modes(opt, rank, world, local):
         Mo = oracle.Csr.from_arrays(Mf.n, *Mf.arrays())
         ptr, idx, val = Ko.arrays()
         Ao = oracle.Csr.from_arrays(Ko.n, ptr, idx, val - st.shift * Mo.arrays()[2])
-        Po = oracle.Rect.from_arrays(P.rows, P.cols, P.ptr, P.idx, P.val)
-        so = oracle.Solver(Ao, "quadratic", xyz=prob.xyz[free // 3], p=Po, coarse=coarse,
-                           method="multigrid")
+        if hexes:
+            oc = (cells.origin, cells.cls, cells.matrices - st.shift * cells.mass)
+            so = oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp,
+                               method="multigrid", cells=oc)
+        else:
+            Po = oracle.Rect.from_arrays(P.rows, P.cols, P.ptr, P.idx, P.val)
+            so = oracle.Solver(Ao, "quadratic", xyz=prob.xyz[free // 3], p=Po, coarse=coarse,
+                               method="multigrid")
         y = Mo.mul(np.random.default_rng(1).standard_normal(Ko.n))
         t1 = time.perf_counter()
         _, its, _ = so.solve(y, tol=1e-10)
         one = time.perf_counter() - t1
         cpu = {"value": 1.0 / (one * st.solves), "unit": "analyses/s", "cores": 1,
                "kind": "port",
-               "sample": f"1 solve of K - shift M by the oracle (the reference's p-multigrid PCG, "
+               "sample": f"1 solve of K - shift M by the oracle (the reference's "
+                         f"{'cell-based multigrid' if hexes else 'p-multigrid'} PCG, "
                          f"{its} iterations, {one:.1f} s) times the device analysis's "
                          f"{st.solves} solves"}
     line = {
@@ -1149,8 +1176,11 @@ def run_modes(opt, rank, world, local):
         "steps": opt.steps, "warmup": opt.warmup, "ms_per_step": 1e3 * wall / opt.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
-        "config": {"workload": "10 lowest modes of the 100x10x10 P2 beam (60,000 10-node tets, "
-                               f"{Kf.n} free unknowns), clamped at x = 0",
+        "config": {"workload": (f"10 lowest modes of the 128x16x16 box-cell cantilever of steel "
+                                f"({Kf.n} free unknowns), clamped at x = 0, coarse matrices "
+                                f"from the cells of K - shift M" if hexes else
+                                "10 lowest modes of the 100x10x10 P2 beam (60,000 10-node "
+                                f"tets, {Kf.n} free unknowns), clamped at x = 0"),
                    "free_dofs": Kf.n, "subspace_vectors": 20,
                    "flush": "inputs larger than L2", "parallelism": f"replicas x{world}"},
         "eigenvalues": [float(v) for v in values],
@@ -1159,7 +1189,9 @@ def run_modes(opt, rank, world, local):
         "assembly_s": assemble_s,
         "roofline": {"bound": "hbm", "achieved": None, "peak": measured_peak()[0],
                      "unit": "GB/s", "frac": None,
-                     "note": "the solves are the p-multigrid PCG of the p2beam line"},
+                     "note": ("the solves are the cell-based multigrid PCG of K - shift M"
+                              if hexes else
+                              "the solves are the p-multigrid PCG of the p2beam line")},
         "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "analyses/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 80},
@@ -1324,7 +1356,7 @@ def main():
         run_recover(opt, rank, world, local)
     elif opt.workload == "transient":
         run_transient(opt, rank, world, local)
-    elif opt.workload == "modes":
+    elif opt.workload in ("modes", "hexmodes"):
         run_modes(opt, rank, world, local)
     elif opt.workload == "batch":
         run_batch(opt, rank, world, local)
