@@ -7,7 +7,6 @@
 #include <algorithm>
 #include <array>
 #include <cstring>
-#include <unordered_map>
 #include <vector>
 
 #include <cub/cub.cuh>
@@ -605,53 +604,81 @@ void hex_modes(const double* d_keys, int64_t n, double* d_modes, cudaStream_t s)
     assembly_flag(fetch(bad.p, s));
 }
 
-// The classes of the cells: the cells in order, each compared with the last new class first
-// (a grid's neighbours mostly share it), then looked up by its 12 words.
-struct KeyHash {
-    size_t operator()(const std::array<uint64_t, 15>& k) const {
-        uint64_t h = 1469598103934665603ULL;  // FNV-1a over the words
-        for (uint64_t w : k) h = (h ^ w) * 1099511628211ULL;
-        return (size_t)h;
+// The classes of the cells, on the device: the cells sorted by a 64-bit hash of their words
+// (FNV-1a), a class starting wherever the hash or any word differs from the previous sorted
+// cell's (a collision that interleaves 2 keys makes extra classes of equal matrices, never a
+// wrong one), numbered by a scan of the starts.
+__global__ void k_key_hash(const double* __restrict__ key, int width, int64_t nel,
+                           uint64_t* __restrict__ hash, uint32_t* __restrict__ pos) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nel;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t h = 1469598103934665603ULL;
+        for (int w = 0; w < width; ++w)
+            h = (h ^ (uint64_t)__double_as_longlong(key[width * e + w])) * 1099511628211ULL;
+        hash[e] = h;
+        pos[e] = (uint32_t)e;
     }
-};
+}
+
+__global__ void k_key_heads(const uint64_t* __restrict__ hash, const uint32_t* __restrict__ pos,
+                            const double* __restrict__ key, int width, int64_t n,
+                            uint32_t* __restrict__ head) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        bool starts = t == 0 || hash[t] != hash[t - 1];
+        if (!starts) {
+            const double* a = key + width * (int64_t)pos[t];
+            const double* b = key + width * (int64_t)pos[t - 1];
+            for (int w = 0; w < width && !starts; ++w)
+                starts = __double_as_longlong(a[w]) != __double_as_longlong(b[w]);
+        }
+        head[t] = starts ? 1u : 0u;
+    }
+}
+
+__global__ void k_key_classes(const uint32_t* __restrict__ head, const int64_t* __restrict__ run,
+                              const uint32_t* __restrict__ pos, const double* __restrict__ key,
+                              int width, int64_t n, uint32_t* __restrict__ cls,
+                              double* __restrict__ keys) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = run[t + 1] - 1;  // the inclusive count of starts
+        cls[pos[t]] = (uint32_t)c;
+        if (head[t])
+            for (int w = 0; w < width; ++w) keys[width * c + w] = key[width * (int64_t)pos[t] + w];
+    }
+}
 
 int64_t hex_classes(const double* xyz, const uint32_t* el, const double* coef,
                     const double* expansion, int width, int64_t nel, DevBuf<uint32_t>* cls,
                     DevBuf<double>* keys, cudaStream_t s) {
+    if (nel >= 0x7fffffffLL) throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 2^31 box cells");
     DevBuf<double> d_key(width * nel);
     k_hex_keys<<<blocks_for(nel, 256), 256, 0, s>>>(xyz, el, coef, expansion, width, nel,
                                                     d_key.p);
+    DevBuf<uint64_t> hash(nel), hash2(nel);
+    DevBuf<uint32_t> pos(nel), pos2(nel), head(nel);
+    k_key_hash<<<blocks_for(nel, 256), 256, 0, s>>>(d_key.p, width, nel, hash.p, pos.p);
     FG_CHECK_LAUNCH();
-    std::vector<double> key((size_t)nel * width);
-    FG_CUDA(cudaMemcpyAsync(key.data(), d_key.p, key.size() * sizeof(double),
-                            cudaMemcpyDeviceToHost, s));
+    size_t tmp = 0;
+    FG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp, hash.p, hash2.p, pos.p, pos2.p,
+                                            (int)nel, 0, 64, s));
+    DevBuf<uint8_t> t(tmp);
+    FG_CUDA(cub::DeviceRadixSort::SortPairs(t.p, tmp, hash.p, hash2.p, pos.p, pos2.p, (int)nel,
+                                            0, 64, s));
+    k_key_heads<<<blocks_for(nel, 256), 256, 0, s>>>(hash2.p, pos2.p, d_key.p, width, nel,
+                                                     head.p);
+    FG_CHECK_LAUNCH();
+    DevBuf<int64_t> run(nel + 1);
+    exclusive_scan32(head.p, run.p, nel, s);
+    const int64_t nclass = fetch(run.p + nel, s);
+    cls->alloc(nel);
+    keys->alloc(width * nclass);
+    k_key_classes<<<blocks_for(nel, 256), 256, 0, s>>>(head.p, run.p, pos2.p, d_key.p, width, nel,
+                                                       cls->p, keys->p);
+    FG_CHECK_LAUNCH();
     FG_CUDA(cudaStreamSynchronize(s));
-    std::unordered_map<std::array<uint64_t, 15>, uint32_t, KeyHash> index;
-    std::vector<uint32_t> of((size_t)nel);
-    std::vector<double> uniq;
-    int64_t last = -1;
-    const size_t bytes = sizeof(double) * width;
-    for (int64_t e = 0; e < nel; ++e) {
-        const double* k = key.data() + width * e;
-        if (last >= 0 && std::memcmp(k, key.data() + width * last, bytes) == 0) {
-            of[e] = of[last];
-            continue;
-        }
-        std::array<uint64_t, 15> w{};
-        std::memcpy(w.data(), k, bytes);
-        auto it = index.find(w);
-        if (it == index.end()) {
-            const uint32_t id = (uint32_t)(uniq.size() / width);
-            it = index.emplace(w, id).first;
-            uniq.insert(uniq.end(), k, k + width);
-        }
-        of[e] = it->second;
-        last = e;
-    }
-    cls->upload(of.data(), of.size(), s);
-    keys->upload(uniq.data(), uniq.size(), s);
-    FG_CUDA(cudaStreamSynchronize(s));
-    return (int64_t)(uniq.size() / width);
+    return nclass;
 }
 
 // ------------------------------------------------------------------ colouring
