@@ -423,8 +423,10 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             o.pdl = options->launch == 0 ? 1 : 0;
             o.values = options->values;
             o.tiles = options->tiles;
+            o.axes = options->axes ? options->axes : 7;
         }
         require(o.tiles >= 0 && o.tiles <= 2, "tiles is 0 (autotuned), 1 (off) or 2 (on)");
+        require(o.axes >= 1 && o.axes <= 7, "axes is a mask of the axes x (1), y (2), z (4)");
         require(o.values >= 0 && o.values <= 2, "values is 0 (default), 1 (FP32) or 2 (FP16)");
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,
@@ -449,6 +451,8 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             throw Failure(FEMGPU_ERR_INVALID, "unknown unknowns kind");
         }
         HostCells hc = host_cells(cells, u);
+        require(hc.empty() || o.axes == 7,
+                "the coarse matrices from the cells need every axis coarsened (axes 0 or 7)");
         auto* s = new femgpu_solver;
         try {
             s->impl.create(a->m, *u, method, c, o, hc.empty() ? nullptr : &hc);

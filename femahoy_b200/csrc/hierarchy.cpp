@@ -15,7 +15,8 @@ int host_threads() {
     return h ? (int)std::min(h, 64u) : 1;
 }
 
-bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* pout, HostLevel* cout) {
+bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* pout, HostLevel* cout,
+             int axes) {
     struct W {
         uint32_t c;
         double w;
@@ -27,7 +28,7 @@ bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* pout, HostLevel*
         const auto& p = fine.planes[d];
         size_t n = p.size();
         std::vector<size_t> keep;
-        if (n <= 2) {
+        if (n <= 2 || !(axes >> d & 1)) {
             for (size_t i = 0; i < n; ++i) keep.push_back(i);
         } else {
             // Every other plane, and the last (multigrid.rs:341-346).

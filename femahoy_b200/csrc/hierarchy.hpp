@@ -30,8 +30,10 @@ struct HostLevel {
     std::vector<uint8_t> comp;
 };
 
-// multigrid.rs:329-452: false when no axis has more than 2 planes.
-bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* p, HostLevel* coarse);
+// multigrid.rs:329-452: false when no axis has more than 2 planes. `axes` (bits x, y, z): the
+// axes that are halved; the others keep all their planes (7: the reference's rule).
+bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* p, HostLevel* coarse,
+             int axes = 7);
 
 // Renumbers the coarse unknowns of `coarse` in grid order (z, then y, then x, then the
 // component) and the columns of `p` with them. The Galerkin matrix of the renumbered P is the

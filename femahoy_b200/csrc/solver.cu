@@ -1889,7 +1889,7 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
         HostLevel coarse;
         {
             PhaseTimer t{this, "coarsening (host)", s_};
-            if (!coarsen(level, a, &p, &coarse)) break;
+            if (!coarsen(level, a, &p, &coarse, opt_.axes)) break;
             if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
             if (opt_.format == 0) renumber_grid_order(&p, &coarse);
         }

@@ -212,6 +212,7 @@ struct Options {
     int pdl = 1;   // programmatic dependent launch between the iteration's kernels
     int values = 0;  // mixed form's stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
     int tiles = 0;   // finest FP32 stencil steps by bulk-copied tiles: 0 tuned, 1 off, 2 on
+    int axes = 7;    // the axes that the coarsening halves (bits x, y, z)
 };
 
 class SolverImpl {

@@ -245,6 +245,49 @@ def hex_classes(prob):
             keys[first])
 
 
+def extruded(npoints=300, layers=8, height=1.0, seed=0):
+    """A footprint mesh extruded in layers, as the reference's prism meshes are (prism.rs): an
+    unstructured triangulation (scipy Delaunay of jittered points in the unit square) extruded
+    into ``layers`` wedges, each split into 3 tetrahedra by the lowest-index rule (shared quad
+    faces split alike). Returns (xyz, tets): the corner points lie on z planes but not on x or
+    y planes."""
+    from scipy.spatial import Delaunay
+    rng = np.random.default_rng(seed)
+    m = int(np.ceil(np.sqrt(npoints)))
+    g = (np.stack(np.meshgrid(np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 2)
+         + 0.5) / m
+    inner = (g > 0.6 / m).all(axis=1) & (g < 1 - 0.6 / m).all(axis=1)
+    g[inner] += rng.uniform(-0.3 / m, 0.3 / m, size=(inner.sum(), 2))
+    tri = Delaunay(g).simplices
+    n2 = len(g)
+    z = height * np.arange(layers + 1) / layers
+    xyz = np.column_stack([np.tile(g, (layers + 1, 1)), np.repeat(z, n2)])
+    tets = []
+    for k in range(layers):
+        for t in tri:
+            a, b, c = sorted(int(v) for v in t)
+            lo = [a + k * n2, b + k * n2, c + k * n2]
+            hi = [v + n2 for v in lo]
+            tets += [[lo[0], lo[1], lo[2], hi[2]], [lo[0], lo[1], hi[1], hi[2]],
+                     [lo[0], hi[0], hi[1], hi[2]]]
+    tets = np.asarray(tets, dtype=np.uint32)
+    # Positive orientation (the assembly takes |volume| from the gradients either way).
+    p = xyz[tets]
+    neg = np.linalg.det(p[:, 1:] - p[:, :1]) < 0
+    tets[neg, 1], tets[neg, 2] = tets[neg, 2].copy(), tets[neg, 1].copy()
+    return xyz, tets
+
+
+def level_of(xyz, free, comps=3):
+    """The grid level of the free unknowns of points that need not fill a grid: the distinct
+    coordinates of each axis are the planes."""
+    planes = [np.unique(xyz[:, d]) for d in range(3)]
+    node = free // comps
+    pts = np.stack([np.searchsorted(planes[d], xyz[node, d]) for d in range(3)],
+                   axis=1).astype(np.uint32)
+    return planes, pts, (free % comps).astype(np.uint8)
+
+
 def lumped_capacity(mesh, capacity=1.0, cells=None):
     """crates/fem/src/heat.rs:413-423: each corner of a cell takes capacity V / per (4 corners
     of a tetrahedron, or 8 of a box cell given as ``cells``), summed over the cells in order and

@@ -114,11 +114,12 @@ class Options:
     launch: int = 0  # 0: programmatic dependent launch in the PCG loop; 1: plain launches
     values: int = 0  # mixed stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
     tiles: int = 0   # finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on
+    axes: int = 0    # the axes the coarsening halves (bits x 1, y 2, z 4; 0: all)
 
     def _c(self):
         return L.Options_t(self.precision, self.degree, self.lower, self.sell_c, 0, self.coarsest,
                            self.max_levels, self.graph, self.format, self.tail, self.launch,
-                           self.values, self.tiles)
+                           self.values, self.tiles, self.axes)
 
 
 def unknowns_c(unknowns: "Unknowns", keep: list) -> L.Unknowns_t:

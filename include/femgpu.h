@@ -236,6 +236,10 @@ typedef struct femgpu_options {
                              chooses by timing whether its smoothing steps and residuals stream
                              each tile's own arrays into shared memory by bulk copies or read
                              them directly; 1 = directly; 2 = bulk copies (the same bits) */
+    int axes;             /* the axes that the grid coarsening halves (bit 0 x, 1 y, 2 z; 0 = all,
+                             the reference's rule): 4 coarsens only z, for meshes extruded in
+                             layers from an unstructured footprint, whose points are on z planes
+                             but not on x or y planes (prism.rs) */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end

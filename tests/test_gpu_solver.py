@@ -373,3 +373,63 @@ def test_flops_crossover_chooses_as_the_reference():
         assert s.method().name.lower() == so.method(), (A.n, flat)
         seen.add(so.method())
     assert seen == {"direct", "multigrid"}
+
+
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_extruded_mesh_with_z_coarsening(precision):
+    """A footprint mesh extruded in layers (the shape of the reference's prism meshes): its points
+    lie on z planes but not on x or y planes. With only z coarsened (axes = 4) the V-cycle halves
+    the layers down to the dense coarse solve; the PCG solution equals the oracle's direct one."""
+    xyz, tets = mg.extruded(npoints=300, layers=8, seed=3)
+    n = len(xyz)
+    coef = np.tile([1000.0, 0.3], (len(tets), 1))
+    fixed = np.repeat(xyz[:, 2] == 0.0, 3)
+    free = np.nonzero(~fixed)[0].astype(np.int64)
+    load = np.zeros(3 * n)
+    load[3 * np.nonzero(xyz[:, 2] == 1.0)[0] + 0] = 1e-3
+    K = fg.Csr.assemble(fg.P1_ELASTIC, xyz, tets, coef)
+    A = K.submatrix(free)
+    rhs = fg.reduced_rhs(K, load, np.zeros(3 * n), free)
+    planes, pts, comp = mg.level_of(xyz, free)
+    s = fg.Solver(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), fg.Method.Multigrid,
+                  precision=precision,
+                  options=fg.Options(precision=precision, axes=4, coarsest=2000)).with_tol(1e-10)
+    assert len(s.levels()) >= 2 and s.levels()[-1] < s.levels()[0]
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    assert st.true_residual <= 1.2e-10
+    Ko = oracle.pattern(3 * n, oracle.dof_elements(tets))
+    Ko.assemble(1, xyz, tets, coef)
+    xd, _ = oracle.direct_solve(Ko.submatrix(free), xyz[free // 3],
+                                Ko.reduced_rhs(load, np.zeros(3 * n), free))
+    assert _rel(x, xd) <= 1e-8
+
+
+def test_extruded_p2_mesh_with_z_coarsening():
+    """P2 elasticity on the extruded footprint (the reference's prism meshes carry P2 tets,
+    elastic_tet.rs): p-multigrid to the P1 corners, then z-only geometric levels; the solution
+    equals the oracle's direct one."""
+    xyz, tets = mg.extruded(npoints=100, layers=6, seed=5)
+    q = fg.Quadratic.new(xyz, tets)
+    n = len(q.points)
+    coef = np.tile([1000.0, 0.3], (len(q.tets), 1))
+    fixed = np.repeat(q.points[:, 2] == 0.0, 3)
+    free = np.nonzero(~fixed)[0].astype(np.int64)
+    load = np.zeros(3 * n)
+    load[3 * np.nonzero(q.points[:, 2] == 1.0)[0] + 1] = 1e-3
+    K = fg.Csr.assemble(fg.P2_ELASTIC, q.points, q.tets, coef)
+    A = K.submatrix(free)
+    rhs = fg.reduced_rhs(K, load, np.zeros(3 * n), free)
+    P, coarse = fg.prolongation(q.points, len(xyz), q.edges, free)
+    u = fg.Unknowns.Quadratic(q.points[free // 3], P, coarse)
+    s = fg.Solver(A, u, fg.Method.Multigrid,
+                  options=fg.Options(axes=4, coarsest=1000)).with_tol(1e-10)
+    assert len(s.levels()) >= 3
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    assert st.true_residual <= 1.2e-10
+    Ko = oracle.pattern(3 * n, oracle.dof_elements(q.tets))
+    Ko.assemble(2, q.points, q.tets, coef)
+    xd, _ = oracle.direct_solve(Ko.submatrix(free), q.points[free // 3],
+                                Ko.reduced_rhs(load, np.zeros(3 * n), free))
+    assert _rel(x, xd) <= 1e-8
