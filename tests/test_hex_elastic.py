@@ -558,3 +558,23 @@ def test_gpu_box_cell_errors():
         fg.Solver(A, u, fg.Method.Multigrid, cells=bad)
     with pytest.raises(fg.FemError, match="does not coarsen"):
         fg.coarse_matrix(A, u, 5, cells)
+
+
+def test_extruded_mesh_is_conforming_with_points_on_z_planes():
+    """meshgen.extruded: positive volumes summing to the footprint's area times the height,
+    every triangular face shared by at most 2 tetrahedra (the wedges' quad faces split alike),
+    and the corner points on the layers' z planes but not on x planes."""
+    xyz, tets = mg.extruded(npoints=80, layers=3, height=2.0, seed=1)
+    p = xyz[tets]
+    vol = np.linalg.det(p[:, 1:] - p[:, :1]) / 6.0
+    assert vol.min() > 0.0
+    foot = np.unique(xyz[:, :2], axis=0)
+    lo, hi = foot.min(axis=0), foot.max(axis=0)
+    assert abs(vol.sum() - np.prod(hi - lo) * 2.0) < 1e-12
+    faces = np.sort(np.concatenate([tets[:, [0, 1, 2]], tets[:, [0, 1, 3]], tets[:, [0, 2, 3]],
+                                    tets[:, [1, 2, 3]]]), axis=1)
+    _, count = np.unique(faces, axis=0, return_counts=True)
+    assert count.max() == 2
+    planes, pts, comp = mg.level_of(xyz, np.arange(3 * len(xyz)))
+    assert len(planes[2]) == 4 and len(planes[0]) > 10
+    assert np.allclose(planes[2][pts[:, 2]], xyz[np.arange(3 * len(xyz)) // 3, 2])
