@@ -205,8 +205,7 @@ def build_system(opt):
     else:
         prob = build_problem(opt.cells)
         kind, tol = fg.P1_HEAT, TOL
-        text = (f"P1 heat, {opt.cells}^3 Kuhn box (6 tets/hex), lognormal k seed {SEED}, 1 RHS "
-                f"to 1e-8, mixed precision PCG-MG")
+        text = heat_text(opt.cells)
     t0 = time.perf_counter()
     K = fg.Csr.assemble(kind, prob.xyz, prob.nodes, prob.coef)
     assemble_s = time.perf_counter() - t0
@@ -240,7 +239,8 @@ def build_system(opt):
             return oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp,
                                  method="multigrid", cells=oc)
     facts = {"text": text, "tol": tol, "assemble_s": assemble_s, "reduce_s": reduce_s,
-             "oracle_solver": oracle_solver, "cells": cells if opt.workload != "p2beam" else None}
+             "oracle_solver": oracle_solver, "cells": cells if opt.workload != "p2beam" else None,
+             "direct_xyz": prob.xyz[prob.free // prob.comps]}
     return A, rhs, unknowns, facts
 
 
@@ -264,11 +264,15 @@ def profiled_traffic():
 
 
 # ------------------------------------------------------------------ CPU baseline (oracle)
-def oracle_solve_rate(A, rhs, make_solver, tol):
+def oracle_solve_rate(A, rhs, make_solver, tol, direct_xyz=None):
     """The oracle's PCG with the reference's multigrid (FP64) on the same system, on 1 thread
     (the reference's) and then on all host cores (its matrix products and dot products split
-    across threads; the smoothers stay sequential, as the reference's are): (DOF-solves/s,
-    iterations, solve seconds, setup seconds, residual, all-cores DOF-solves/s, cores)."""
+    across threads; the smoothers stay sequential, as the reference's are). Returns a dict:
+    rate, iterations, solve / setup seconds, residual, all-cores rate and cores, and the
+    solutions the device's are checked against: `x_tol` (the oracle's PCG-MG at the same
+    tolerance), `x_tight` (its PCG-MG continued from x_tol to 1e-12 on all cores) and, for
+    systems of at most 40,000 unknowns with `direct_xyz`, `x_direct` (its multifrontal
+    Cholesky, cholesky.rs:44-167)."""
     import oracle
     ptr, idx, val = A.arrays()
     Ao = oracle.Csr.from_arrays(A.n, ptr, idx, val)
@@ -277,7 +281,7 @@ def oracle_solve_rate(A, rhs, make_solver, tol):
     setup = time.perf_counter() - t0
     oracle.set_threads(1)
     t0 = time.perf_counter()
-    _, it, res = so.solve(rhs, tol=tol)
+    x_tol, it, res = so.solve(rhs, tol=tol)
     solve = time.perf_counter() - t0
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
@@ -285,16 +289,50 @@ def oracle_solve_rate(A, rhs, make_solver, tol):
         t0 = time.perf_counter()
         so.solve(rhs, tol=tol)
         solve_all = time.perf_counter() - t0
+        x_tight, _, res_tight = so.solve(rhs, x=x_tol, tol=min(tol, 1e-12))
     finally:
         oracle.set_threads(1)
-    return A.n / solve, it, solve, setup, res, A.n / solve_all, cores
+    out = {"rate": A.n / solve, "iterations": it, "solve_s": solve, "setup_s": setup,
+           "residual": res, "rate_all": A.n / solve_all, "cores": cores, "x_tol": x_tol,
+           "x_tight": x_tight, "residual_tight": res_tight, "x_direct": None}
+    if direct_xyz is not None and A.n <= 40000:
+        out["x_direct"], _ = oracle.direct_solve(Ao, direct_xyz, rhs)
+    return out
+
+
+def error_vs_oracle(x, ref):
+    """|x - x_oracle|_2 / |x_oracle|_2 against each oracle solution of `oracle_solve_rate`."""
+    def rel(y):
+        return float(np.linalg.norm(x - y) / np.linalg.norm(y))
+    out = {"vs_oracle_pcg_mg_same_tol": rel(ref["x_tol"]),
+           "vs_oracle_pcg_mg_1e-12": rel(ref["x_tight"])}
+    if ref.get("x_direct") is not None:
+        out["vs_oracle_direct"] = rel(ref["x_direct"])
+    return out
+
+
+def heat_text(cells):
+    return (f"P1 heat, {cells}^3 Kuhn box (6 tets/hex), lognormal k seed {SEED}, 1 RHS "
+            f"to 1e-8")
+
+
+def workload_config(text, n_free, nnz, tol, world):
+    """The `config` of a single-solver line, the same in both arms: the workload, its size and
+    tolerance, whether its operator alone exceeds the 126 MB L2 (FP32 values and int32
+    columns), and the replicas."""
+    big = nnz * 8 > (126 << 20)
+    return {"workload": text, "free_dofs": int(n_free), "tol": tol,
+            "flush": ("inputs larger than L2" if big else
+                      "none: the whole problem fits L2; launch- and latency-bound"),
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(opt, rank, world):
     """The reference arm: the oracle restatement of the reference's CPU path (assembly, the
     Galerkin hierarchy with line Gauss-Seidel, PCG) on the host, rank 0 only, with every host
     thread it can use (the matrix and dot products; the smoothers stay sequential, as the
-    reference's are)."""
+    reference's are). Each step, warm-up and timed alike, is 1 full solve of the system to the
+    tolerance from x = 0."""
     if rank != 0:
         return
     import oracle
@@ -307,61 +345,36 @@ def run_reference(opt, rank, world):
     k.assemble(0, h.xyz, h.nodes, h.coef)
     a = k.submatrix(h.free)
     rhs = k.reduced_rhs(h.load, h.values, h.free)
+    nnz = len(a.arrays()[1])
+    del k
     assemble_s = time.perf_counter() - t0
     planes, pts, comp = mg.grid_unknowns(h)
     t0 = time.perf_counter()
     so = oracle.Solver(a, "grid", planes=planes, points=pts, comp=comp, method="multigrid")
     setup_s = time.perf_counter() - t0
-    # A step is 1 full solve when it fits the budget, else a bounded run of PCG iterations. A
-    # bounded run holds the solve's fixed work (first residual, first cycle) once, so it is
-    # scaled to a full solve by the ratio of a full solve to the same bounded run, both timed
-    # in the warm-up.
-    t0 = time.perf_counter()
-    _, iters, res = so.solve(rhs, tol=TOL)
-    full = time.perf_counter() - t0
-    per_it = full / max(iters, 1)
-    budget = 150.0 / max(1, opt.steps + opt.warmup)
-    sample_its = iters if full <= budget else max(1, int(budget / per_it))
-
-    def bounded():
-        t = time.perf_counter()
-        try:
-            so.solve(rhs, tol=TOL, max_iter=sample_its)
-        except oracle.OracleError:
-            pass
-        return time.perf_counter() - t
-
-    scale = full / bounded() if sample_its < iters else 1.0
-    times = []
-    for step in range(max(0, opt.warmup - 1) + opt.steps):
-        if sample_its >= iters:
-            t0 = time.perf_counter()
-            so.solve(rhs, tol=TOL)
-            dt = time.perf_counter() - t0
-        else:
-            dt = bounded() * scale
-        if step >= max(0, opt.warmup - 1):
-            times.append(dt)
+    for _ in range(opt.warmup):
+        so.solve(rhs, tol=TOL)
+    times, iters, res = [], 0, None
+    for _ in range(opt.steps):
+        t0 = time.perf_counter()
+        _, iters, res = so.solve(rhs, tol=TOL)
+        times.append(time.perf_counter() - t0)
     value = a.n * len(times) / sum(times)
-    sample = (f"full solves of the {opt.cells}^3 system ({iters} PCG iterations)"
-              if sample_its >= iters else
-              f"{sample_its} of the {iters} PCG iterations of the {opt.cells}^3 solve per step, "
-              f"scaled to 1 solve by the ratio of a full solve to the same bounded run timed "
-              f"in the warm-up ({full:.2f} s / {full / scale:.2f} s)")
+    sample = (f"1 full solve of the {opt.cells}^3 system per step ({iters} PCG iterations, "
+              f"{np.mean(times):.2f} s), matrix and dot products on {cores} host threads")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
         "steps": len(times), "warmup": opt.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"P1 heat, {opt.cells}^3 Kuhn box, lognormal k (seed {SEED}), "
-                               f"1 RHS to 1e-8", "free_dofs": a.n, "tol": TOL,
-                   "precision": "fp64 (reference algorithm: PCG + line Gauss-Seidel MG)"},
+        "config": workload_config(heat_text(opt.cells), a.n, nnz, TOL, world),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_detail": {"iterations": iters, "residual": res, "assembly_s": assemble_s,
-                             "setup_s": setup_s, "full_solve_s": full,
-                             "host_cores": os.cpu_count(),
+                             "setup_s": setup_s, "host_cores": os.cpu_count(),
+                             "precision": "fp64 (the reference's algorithm: PCG + line "
+                                          "Gauss-Seidel multigrid)",
                              "note": "the reference itself is single-threaded (no threads in "
                                      "fh-fem); this arm runs its algorithm with the matrix and "
                                      "dot products on all host threads"},
@@ -399,6 +412,7 @@ def run_ours(opt, rank, world, local):
     tol = facts["tol"]
     assemble_s, reduce_s = facts["assemble_s"], facts["reduce_s"]
     n_free = A.n
+    nnz = A.shape[1]
 
     def make(precision):
         t = time.perf_counter()
@@ -499,6 +513,8 @@ def run_ours(opt, rank, world, local):
     e1.synchronize()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = replica_value(world, n_free, opt.steps, e2e_ms)
+    x_mixed = x.cpu().numpy()
+    x_e2e = hx.numpy().copy()
     mixed_bytes = mixed.device_bytes()
     levels = mixed.levels()
     del mixed
@@ -506,23 +522,34 @@ def run_ours(opt, rank, world, local):
     # The plain FP64 form on the same workload.
     plain, setup_fp64 = make(fg.FP64)
     ms64, lat64, its64, _, res64, _ = timed(plain, opt.steps, opt.warmup)
+    x_fp64 = x.cpu().numpy()
     ms64 = max_over_ranks(ms64)
     value64 = replica_value(world, n_free, opt.steps, ms64)
     del plain
 
     cpu = None
+    errors = None
     if rank == 0 and world == 1 and not opt.no_cpu_baseline:
         try:
-            rate, cit, csolve, csetup, cres, rate_all, cores = oracle_solve_rate(
-                A, rhs, facts["oracle_solver"], tol)
-            cpu = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+            ref = oracle_solve_rate(A, rhs, facts["oracle_solver"], tol, facts["direct_xyz"])
+            cpu = {"value": ref["rate"], "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"1 full solve of the same system by the oracle (reference "
                              f"algorithm: FP64 PCG + the reference's multigrid smoothers), "
-                             f"{cit} iterations, {csolve:.2f} s (setup {csetup:.1f} s "
-                             f"excluded)",
-                   "all_cores": {"value": rate_all, "cores": cores,
+                             f"{ref['iterations']} iterations, {ref['solve_s']:.2f} s (setup "
+                             f"{ref['setup_s']:.1f} s excluded)",
+                   "all_cores": {"value": ref["rate_all"], "cores": ref["cores"],
                                  "sample": "the same solve with the matrix and dot products "
                                            "on all host cores (smoothers sequential)"}}
+            # The device solutions of the timed runs (the last step's) against the oracle's.
+            errors = {"mixed": error_vs_oracle(x_mixed, ref),
+                      "fp64": error_vs_oracle(x_fp64, ref),
+                      "e2e": error_vs_oracle(x_e2e, ref),
+                      "oracle_residual": {"same_tol": ref["residual"],
+                                          "tight": ref["residual_tight"]},
+                      "definition": "|x - x_oracle|_2 / |x_oracle|_2; the oracle's PCG-MG "
+                                    "(the reference's algorithm) at the same tolerance, the "
+                                    "same continued to 1e-12, and (<= 40,000 unknowns) its "
+                                    "multifrontal Cholesky"}
         except Exception as e:  # the baseline is reported, never the product
             cpu = {"value": None, "unit": UNIT, "cores": 1, "kind": "port",
                    "sample": f"failed: {e}"}
@@ -533,13 +560,8 @@ def run_ours(opt, rank, world, local):
         "warmup": opt.warmup, "ms_per_step": ms_max / opt.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer",
         "data": "synthetic",
-        "config": {
-            "workload": facts["text"],
-            "free_dofs": n_free, "tol": tol, "levels": levels,
-            "flush": ("inputs larger than L2" if mixed_bytes > (256 << 20) else
-                      "none: the whole problem fits L2; launch- and latency-bound"),
-            "parallelism": f"replicas x{world}",
-        },
+        "config": workload_config(facts["text"], n_free, nnz, tol, world),
+        "levels": levels,
         "latency_ms": {"p50": float(np.percentile(lat_ms, 50)),
                        "p99": float(np.percentile(lat_ms, 99))},
         "iterations": {"mixed": int(np.median(its)), "fp64": int(np.median(its64))},
@@ -562,6 +584,7 @@ def run_ours(opt, rank, world, local):
                      {"bound": "latency", "achieved": None, "peak": peak, "unit": "GB/s",
                       "frac": None, "note": "no smoothing level: launch- and latency-bound"}),
         "cpu_baseline": cpu,
+        "error_vs_oracle": errors,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * n_free,
                 "d2h_bytes_per_step": 8 * n_free},
         "gpu_launches": launches,

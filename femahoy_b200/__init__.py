@@ -13,7 +13,7 @@ from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT
                     Cells, Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
                     coarse_matrix, hex_elements, hex_mass, prolongation, reduced_rhs,
                     symbolic_counts)
-from .recover import Peak, Recovery
+from .recover import Peak, Reactions, Recovery, reactions
 from .sparse import Csr, Rect, colour
 
 __all__ = [
@@ -23,5 +23,5 @@ __all__ = [
     "TRANSIENT_DIRECT_LIMIT", "Cells", "Crossover", "Level", "Method", "Options", "Quadratic",
     "Solver", "coarse_matrix", "hex_elements", "hex_mass", "symbolic_counts",
     "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
-    "Recovery",
+    "Recovery", "Reactions", "reactions",
 ]

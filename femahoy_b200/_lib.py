@@ -138,8 +138,10 @@ SIGNATURES = {
     "femgpu_hex_mass": (C.c_int, [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_coarse_matrix": (C.c_int, [C.c_void_p, C.POINTER(Unknowns_t), C.POINTER(Cells_t),
                                        C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
-                                       C.c_void_p, C.c_void_p, C.c_void_p]),
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
     "femgpu_solver_set_max_iter": (C.c_int, [C.c_void_p, C.c_size_t]),
+    "femgpu_solver_set_wait_limit": (C.c_int, [C.c_void_p, C.c_uint32]),
     "femgpu_solver_set_tol": (C.c_int, [C.c_void_p, C.c_double]),
     "femgpu_solver_method": (C.c_int, [C.c_void_p]),
     "femgpu_solver_levels": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
@@ -212,6 +214,9 @@ SIGNATURES = {
                                       C.c_void_p, C.POINTER(C.c_void_p)]),
     "femgpu_hex_loads": (C.c_int, [C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_reactions": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_size_t, C.c_void_p, C.c_double, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_recovery_run": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "femgpu_recovery_run_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -36,6 +36,8 @@ UNITS = [
     ("recover.cu", ["-fmad=false"]),
     ("transient.cu", ["-fmad=false"]),
     ("modes.cu", ["-fmad=false"]),
+    ("reactions.cu", ["-fmad=false"]),
+    ("coarsen.cu", []),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("dense_eigen.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"])]

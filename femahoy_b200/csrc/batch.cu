@@ -27,8 +27,10 @@
 
 #include "common.cuh"
 #include "hierarchy.hpp"
+#include "coarsen.cuh"
 #include "block3.cuh"
 #include "solver.cuh"
+#include "rust_format.hpp"
 
 namespace femgpu {
 
@@ -822,7 +824,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     const size_t max_levels = (size_t)(o.max_levels > 0 ? o.max_levels : 30);
     std::vector<std::string> errors(B_);
     std::vector<int> codes(B_, FEMGPU_OK);
-    auto build = [&](int b) {
+    auto build = [&](int b, cudaStream_t st) {
         try {
             const femgpu_unknowns& uu = *u[b];
             const int64_t n = fine[b].n;
@@ -834,20 +836,27 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
                 for (int d = 0; d < 3; ++d) lv.points[k][d] = uu.points[3 * k + d];
             lv.comp.assign(uu.comp, uu.comp + n);
             H[b].mats.push_back(std::move(fine[b]));
+            // The member's coarsening and Galerkin products on the device (coarsen.cu), the
+            // coarse unknowns in grid order (z, y, x, component): the 3 unknowns of a node are
+            // consecutive, which the 3x3-block operators need.
+            DevGrid grid;
+            grid_upload(lv, &grid, st);
+            const DevCsr* cur = a[b];
+            DevCsr held;
             for (;;) {
                 const HostCsr& m = H[b].mats.back();
                 if ((size_t)m.n <= coarsest || H[b].ps.size() >= max_levels) break;
-                HostRect p;
-                HostLevel coarse;
-                if (!coarsen(lv, m, &p, &coarse)) break;
-                if (coarse.points.size() * 10 > (size_t)m.n * 9) break;
-                // Grid order (z, y, x, component): the 3 unknowns of a node are consecutive,
-                // which the 3x3-block operators need.
-                if (o.format == 0) renumber_grid_order(&p, &coarse);
-                HostCsr ac = galerkin(p, m, 1);
-                H[b].mats.push_back(std::move(ac));
-                H[b].ps.push_back(std::move(p));
-                lv = std::move(coarse);
+                DevRect p;
+                DevGrid coarse;
+                if (!coarsen_grid(grid, *cur, 7, &p, &coarse, st)) break;
+                if ((size_t)coarse.n * 10 > (size_t)m.n * 9) break;
+                DevCsr next;
+                galerkin_product(p, *cur, &next, st);
+                H[b].mats.push_back(download_csr(next, st));
+                H[b].ps.push_back(rect_download(p, st));
+                held = std::move(next);
+                cur = &held;
+                grid = std::move(coarse);
             }
             if (H[b].mats.back().n > 4096)
                 throw Failure(FEMGPU_ERR_TOO_LARGE,
@@ -863,9 +872,21 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     };
     const int threads = std::max(1, std::min(host_threads(), B_));
     std::vector<std::thread> pool;
+    int device = 0;
+    FG_CUDA(cudaGetDevice(&device));
     for (int t = 0; t < threads; ++t)
         pool.emplace_back([&, t] {
-            for (int b = t; b < B_; b += threads) build(b);
+            cudaStream_t st = nullptr;
+            if (cudaSetDevice(device) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+                for (int b = t; b < B_; b += threads) {
+                    codes[b] = FEMGPU_ERR_CUDA;
+                    errors[b] = "cudaStreamCreate failed";
+                }
+                return;
+            }
+            for (int b = t; b < B_; b += threads) build(b, st);
+            cudaStreamDestroy(st);
         });
     for (auto& th : pool) th.join();
     for (int b = 0; b < B_; ++b)
@@ -1387,8 +1408,8 @@ void BatchImpl::collect(femgpu_batch_stats* st) {
         else
             std::snprintf(buf, sizeof buf,
                           "system %d, right side %d: conjugate gradients did not converge: the "
-                          "residual is %.2e after %zu iterations",
-                          s / R_, s % R_, res[s], it[s]);
+                          "residual is %s after %zu iterations",
+                          s / R_, s % R_, rust_exp(res[s], 2).c_str(), it[s]);
         throw Failure(FEMGPU_ERR_NOT_CONVERGED, buf);
     }
 }

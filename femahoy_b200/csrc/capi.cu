@@ -7,6 +7,7 @@
 #include "common.cuh"
 #include "hierarchy.hpp"
 #include "solver.cuh"
+#include "coarsen.cuh"
 
 namespace femgpu {
 
@@ -369,32 +370,52 @@ int femgpu_symbolic_counts(const femgpu_csr* a, const femgpu_unknowns* u, uint64
 
 int femgpu_coarse_matrix(const femgpu_csr* a, const femgpu_unknowns* u,
                          const femgpu_cells* cells, int level, size_t* n, size_t* nnz,
-                         int64_t* ptr, uint32_t* idx, double* val) {
+                         int64_t* ptr, uint32_t* idx, double* val, uint32_t* points,
+                         uint8_t* comp) {
     return guarded([&] {
         require(a && u && n && nnz, "null argument");
         require(u->kind == FEMGPU_UNKNOWNS_GRID, "coarse matrices need grid unknowns");
         require(level >= 1, "level 1 is the first coarse level");
-        HostCsr m = download_csr(a->m, util_stream());
-        HostLevel lv = host_level(u, m.n);
+        cudaStream_t s = util_stream();
+        HostLevel lv = host_level(u, a->m.n);
         HostCells stored, first = host_cells(cells, u);
         const int threads = host_threads();
+        DevGrid grid;
+        grid_upload(lv, &grid, s);
+        DevCsr held;
+        const DevCsr* cur = &a->m;
         for (int l = 1; l <= level; ++l) {
-            HostRect p;
-            HostLevel coarse;
-            require(coarsen(lv, m, &p, &coarse), "the grid does not coarsen that far");
+            DevRect p;
+            DevGrid coarse;
+            require(coarsen_grid(grid, *cur, 7, &p, &coarse, s),
+                    "the grid does not coarsen that far");
+            DevCsr next;
             if (!first.empty()) {
                 HostCells nxt;
-                m = by_cells(lv, stored.empty() ? first : stored, coarse, &nxt, threads);
+                HostCsr m = by_cells(grid_download(grid, s), stored.empty() ? first : stored,
+                                     grid_download(coarse, s), &nxt, threads);
                 stored = std::move(nxt);
+                upload_csr(m, &next, s);
             } else {
-                m = galerkin(p, m, threads);
+                galerkin_product(p, *cur, &next, s);
             }
-            lv = std::move(coarse);
+            held = std::move(next);
+            cur = &held;
+            grid = std::move(coarse);
         }
-        *n = (size_t)m.n;
-        *nnz = (size_t)m.nnz();
+        *n = (size_t)held.n;
+        *nnz = (size_t)held.nnz;
+        if (points || comp) {
+            HostLevel h = grid_download(grid, s);
+            for (int64_t k = 0; k < grid.n; ++k) {
+                if (points)
+                    for (int d = 0; d < 3; ++d) points[3 * k + d] = h.points[k][d];
+                if (comp) comp[k] = h.comp[k];
+            }
+        }
         if (!ptr) return;
         require(idx && val, "null output arrays");
+        HostCsr m = download_csr(held, s);
         std::copy(m.ptr.begin(), m.ptr.end(), ptr);
         std::copy(m.idx.begin(), m.idx.end(), idx);
         std::copy(m.val.begin(), m.val.end(), val);
@@ -461,6 +482,13 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             throw;
         }
         *out = s;
+    });
+}
+
+int femgpu_solver_set_wait_limit(femgpu_solver* s, uint32_t polls) {
+    return guarded([&] {
+        require(s != nullptr, "null solver");
+        s->impl.set_wait_limit(polls);
     });
 }
 

@@ -1,5 +1,7 @@
-// Host setup of the multigrid hierarchy (see hierarchy.hpp). Compiled with
-// -ffp-contract=off so that the coarse matrices are formed with the reference's roundings.
+// Host setup steps of the multigrid hierarchy (see hierarchy.hpp): the coarse matrices from the
+// cells, the crossover's counts, the P2 -> P1 prolongation and the grid level of points.
+// Compiled with -ffp-contract=off so that the cells' coarse matrices are formed with the
+// reference's roundings.
 #include "hierarchy.hpp"
 
 #include <algorithm>
@@ -13,220 +15,6 @@ namespace femgpu {
 int host_threads() {
     unsigned h = std::thread::hardware_concurrency();
     return h ? (int)std::min(h, 64u) : 1;
-}
-
-bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* pout, HostLevel* cout,
-             int axes) {
-    struct W {
-        uint32_t c;
-        double w;
-    };
-    std::array<std::vector<std::array<W, 2>>, 3> map;
-    std::array<std::vector<double>, 3> planes;
-    bool any = false;
-    for (int d = 0; d < 3; ++d) {
-        const auto& p = fine.planes[d];
-        size_t n = p.size();
-        std::vector<size_t> keep;
-        if (n <= 2 || !(axes >> d & 1)) {
-            for (size_t i = 0; i < n; ++i) keep.push_back(i);
-        } else {
-            // Every other plane, and the last (multigrid.rs:341-346).
-            any = true;
-            for (size_t i = 0; i < n; i += 2) keep.push_back(i);
-            if (keep.back() != n - 1) keep.push_back(n - 1);
-        }
-        for (size_t i : keep) planes[d].push_back(p[i]);
-        map[d].resize(n);
-        size_t c = 0;
-        for (size_t i = 0; i < n; ++i) {
-            while (keep[c] < i) ++c;
-            if (keep[c] == i) {
-                map[d][i] = {W{(uint32_t)c, 1.0}, W{(uint32_t)c, 0.0}};
-            } else {
-                size_t lo = keep[c - 1], hi = keep[c];
-                double w = (p[i] - p[lo]) / (p[hi] - p[lo]);
-                map[d][i] = {W{(uint32_t)(c - 1), 1.0 - w}, W{(uint32_t)c, w}};
-            }
-        }
-    }
-    if (!any) return false;
-    size_t dims[3] = {planes[0].size(), planes[1].size(), planes[2].size()};
-    size_t comps = 1;
-    for (uint8_t c : fine.comp) comps = std::max(comps, (size_t)c + 1);
-    std::vector<uint32_t> number(comps * dims[0] * dims[1] * dims[2], UINT32_MAX);
-    HostLevel coarse;
-    coarse.planes = planes;
-    HostRect p;
-    p.rows = (int64_t)fine.points.size();
-    p.ptr.reserve(fine.points.size() + 1);
-    p.ptr.push_back(0);
-    std::vector<std::pair<uint32_t, double>> pairs;
-    for (size_t row = 0; row < fine.points.size(); ++row) {
-        size_t start = p.idx.size();
-        const auto& f = fine.points[row];
-        uint8_t c = fine.comp[row];
-        std::array<std::array<W, 2>, 3> weights;
-        for (int d = 0; d < 3; ++d) {
-            auto w = map[d][f[d]];
-            // A scalar takes the operator weights of its row's couplings to the 2 coarse planes
-            // (multigrid.rs:386-401); a displacement keeps the linear weights.
-            if (w[0].c != w[1].c && comps == 1) {
-                double lo = 0.0, hi = 0.0;
-                for (int64_t k = a.ptr[row]; k < a.ptr[row + 1]; ++k) {
-                    const auto& g = fine.points[a.idx[k]];
-                    if (g[d] + 1 == f[d])
-                        lo -= a.val[k];
-                    else if (g[d] == f[d] + 1)
-                        hi -= a.val[k];
-                }
-                if (lo > 0.0 && hi > 0.0) {
-                    w[0].w = lo / (lo + hi);
-                    w[1].w = hi / (lo + hi);
-                }
-            }
-            weights[d] = w;
-        }
-        for (const W& x : weights[0])
-            for (const W& y : weights[1])
-                for (const W& z : weights[2]) {
-                    double w = x.w * y.w * z.w;
-                    if (w == 0.0) continue;
-                    size_t key = c + comps * (x.c + dims[0] * (y.c + dims[1] * (size_t)z.c));
-                    uint32_t& slot = number[key];
-                    if (slot == UINT32_MAX) {
-                        slot = (uint32_t)coarse.points.size();
-                        coarse.points.push_back({x.c, y.c, z.c});
-                        coarse.comp.push_back(c);
-                    }
-                    p.idx.push_back(slot);
-                    p.val.push_back(w);
-                }
-        pairs.clear();
-        for (size_t k = start; k < p.idx.size(); ++k) pairs.push_back({p.idx[k], p.val[k]});
-        std::sort(pairs.begin(), pairs.end(),
-                  [](const auto& s, const auto& t) { return s.first < t.first; });
-        for (size_t k = 0; k < pairs.size(); ++k) {
-            p.idx[start + k] = pairs[k].first;
-            p.val[start + k] = pairs[k].second;
-        }
-        p.ptr.push_back((int64_t)p.idx.size());
-    }
-    p.cols = (int64_t)coarse.points.size();
-    *pout = std::move(p);
-    *cout = std::move(coarse);
-    return true;
-}
-
-void renumber_grid_order(HostRect* p, HostLevel* lv) {
-    size_t n = lv->points.size();
-    std::vector<uint32_t> order(n);
-    for (size_t k = 0; k < n; ++k) order[k] = (uint32_t)k;
-    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        const auto &pa = lv->points[a], &pb = lv->points[b];
-        return std::make_tuple(pa[2], pa[1], pa[0], lv->comp[a]) <
-               std::make_tuple(pb[2], pb[1], pb[0], lv->comp[b]);
-    });
-    std::vector<uint32_t> fresh(n);
-    for (size_t q = 0; q < n; ++q) fresh[order[q]] = (uint32_t)q;
-    std::vector<std::array<uint32_t, 3>> pts(n);
-    std::vector<uint8_t> comp(n);
-    for (size_t q = 0; q < n; ++q) {
-        pts[q] = lv->points[order[q]];
-        comp[q] = lv->comp[order[q]];
-    }
-    lv->points = std::move(pts);
-    lv->comp = std::move(comp);
-    std::vector<std::pair<uint32_t, double>> row;
-    for (int64_t i = 0; i < p->rows; ++i) {
-        row.clear();
-        for (int64_t k = p->ptr[i]; k < p->ptr[i + 1]; ++k) row.push_back({fresh[p->idx[k]], p->val[k]});
-        std::sort(row.begin(), row.end(),
-                  [](const auto& s, const auto& t) { return s.first < t.first; });
-        for (size_t k = 0; k < row.size(); ++k) {
-            p->idx[p->ptr[i] + k] = row[k].first;
-            p->val[p->ptr[i] + k] = row[k].second;
-        }
-    }
-}
-
-HostCsr galerkin(const HostRect& P, const HostCsr& a, int threads) {
-    int64_t nc = P.cols;
-    // The transpose of P, row by row, by a counting sort (fine rows in increasing order).
-    std::vector<int64_t> tptr(nc + 1, 0);
-    for (uint32_t j : P.idx) tptr[j + 1] += 1;
-    for (int64_t j = 0; j < nc; ++j) tptr[j + 1] += tptr[j];
-    std::vector<uint32_t> tidx(P.idx.size());
-    std::vector<double> tval(P.idx.size());
-    {
-        std::vector<int64_t> next(tptr.begin(), tptr.end() - 1);
-        for (int64_t i = 0; i < P.rows; ++i)
-            for (int64_t k = P.ptr[i]; k < P.ptr[i + 1]; ++k) {
-                uint32_t j = P.idx[k];
-                tidx[next[j]] = (uint32_t)i;
-                tval[next[j]] = P.val[k];
-                next[j] += 1;
-            }
-    }
-    threads = std::max(1, std::min<int>(threads, (int)std::max<int64_t>(1, nc / 256)));
-    struct Part {
-        std::vector<int64_t> len;
-        std::vector<uint32_t> idx;
-        std::vector<double> val;
-    };
-    std::vector<Part> parts(threads);
-    auto work = [&](int t) {
-        int64_t c0 = nc * t / threads, c1 = nc * (t + 1) / threads;
-        Part& out = parts[t];
-        std::vector<double> acc(nc, 0.0);
-        std::vector<int64_t> mark(nc, -1);
-        std::vector<uint32_t> row;
-        for (int64_t c = c0; c < c1; ++c) {
-            row.clear();
-            // Row c of P^T A P = sum over P(i, c) of row i of A P (Gustavson, dense accumulator).
-            for (int64_t t2 = tptr[c]; t2 < tptr[c + 1]; ++t2) {
-                int64_t i = tidx[t2];
-                double pic = tval[t2];
-                for (int64_t ka = a.ptr[i]; ka < a.ptr[i + 1]; ++ka) {
-                    int64_t l = a.idx[ka];
-                    double aval = a.val[ka] * pic;
-                    for (int64_t kp = P.ptr[l]; kp < P.ptr[l + 1]; ++kp) {
-                        uint32_t d = P.idx[kp];
-                        if (mark[d] != c) {
-                            mark[d] = c;
-                            acc[d] = 0.0;
-                            row.push_back(d);
-                        }
-                        acc[d] += aval * P.val[kp];
-                    }
-                }
-            }
-            std::sort(row.begin(), row.end());
-            for (uint32_t d : row) {
-                out.idx.push_back(d);
-                out.val.push_back(acc[d]);
-            }
-            out.len.push_back((int64_t)row.size());
-        }
-    };
-    std::vector<std::thread> pool;
-    for (int t = 1; t < threads; ++t) pool.emplace_back(work, t);
-    work(0);
-    for (auto& th : pool) th.join();
-    HostCsr out;
-    out.n = nc;
-    out.ptr.reserve(nc + 1);
-    out.ptr.push_back(0);
-    size_t total = 0;
-    for (auto& pt : parts) total += pt.idx.size();
-    out.idx.reserve(total);
-    out.val.reserve(total);
-    for (auto& pt : parts) {
-        for (int64_t l : pt.len) out.ptr.push_back(out.ptr.back() + l);
-        out.idx.insert(out.idx.end(), pt.idx.begin(), pt.idx.end());
-        out.val.insert(out.val.end(), pt.val.begin(), pt.val.end());
-    }
-    return out;
 }
 
 // ------------------------------------------------------------------ cells (multigrid.rs:458)

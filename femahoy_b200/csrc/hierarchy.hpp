@@ -1,6 +1,7 @@
-// Host setup of the multigrid hierarchy: plane coarsening with its prolongation
-// (multigrid.rs:329-452), the Galerkin product P^T A P (sparse.rs:233-292) on all host threads,
-// the P2 -> P1 prolongation (pmultigrid.rs:104-151), and the grid level of a set of points.
+// Host setup steps of the multigrid hierarchy: the coarse matrices of a box grid from its cells
+// (multigrid.rs:458-681), the figures of Crossover::Flops, the P2 -> P1 prolongation
+// (pmultigrid.rs:104-151) and the grid level of a set of points. The plane coarsening and the
+// Galerkin products run on the device (coarsen.cuh).
 #pragma once
 #include <array>
 #include <cstdint>
@@ -29,21 +30,6 @@ struct HostLevel {
     std::vector<std::array<uint32_t, 3>> points;
     std::vector<uint8_t> comp;
 };
-
-// multigrid.rs:329-452: false when no axis has more than 2 planes. `axes` (bits x, y, z): the
-// axes that are halved; the others keep all their planes (7: the reference's rule).
-bool coarsen(const HostLevel& fine, const HostCsr& a, HostRect* p, HostLevel* coarse,
-             int axes = 7);
-
-// Renumbers the coarse unknowns of `coarse` in grid order (z, then y, then x, then the
-// component) and the columns of `p` with them. The Galerkin matrix of the renumbered P is the
-// same matrix with its rows and columns permuted; in grid order the entries of a box level sit
-// at constant offsets, which the stencil format needs.
-void renumber_grid_order(HostRect* p, HostLevel* coarse);
-
-// sparse.rs:233-292, each coarse row exactly as the reference forms it; rows shared among
-// `threads` host threads.
-HostCsr galerkin(const HostRect& p, const HostCsr& a, int threads);
 
 // multigrid.rs:62-68 `Cells`: the cells of a box-grid displacement level, each by its lowest
 // grid point and the class of its 24 x 24 matrix (row-major, unknown 3 n + c for corner n in

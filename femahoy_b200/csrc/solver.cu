@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cstring>
 #include <mutex>
+#include <optional>
 #include <thread>
 #include <type_traits>
 
@@ -25,6 +26,8 @@
 
 #include "assemble.cuh"
 #include "solver.cuh"
+#include "coarsen.cuh"
+#include "rust_format.hpp"
 
 namespace femgpu {
 
@@ -45,6 +48,9 @@ struct PhaseTimer {
     const char* name;
     cudaStream_t s;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    PhaseTimer(SolverImpl* sv, const char* nm, cudaStream_t st) : solver(sv), name(nm), s(st) {}
+    PhaseTimer(const PhaseTimer&) = delete;
+    PhaseTimer& operator=(const PhaseTimer&) = delete;
     ~PhaseTimer() {
         cudaStreamSynchronize(s);
         solver->phase(name, std::chrono::duration<double>(std::chrono::steady_clock::now() - t0)
@@ -453,9 +459,9 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, unsigned parity) {
         : "memory");
     return ok != 0;
 }
-// Waits for phase `parity` of `bar`, at most BULK_SPIN polls: false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-    for (unsigned k = 0; k < BULK_SPIN; ++k)
+// Waits for phase `parity` of `bar`, at most `limit` polls: false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned limit) {
+    for (unsigned k = 0; k < limit; ++k)
         if (mbar_try(bar, parity)) return true;
     return false;
 }
@@ -465,7 +471,7 @@ __global__ void __launch_bounds__(BULK_TH, 2)
     k_stencil_tiles(StencilView<float> v, const float* __restrict__ b,
                     const float* __restrict__ xin, const float* __restrict__ dinv, float c1,
                     float c2, float* __restrict__ d, float* __restrict__ out,
-                    const int* __restrict__ done, int* __restrict__ timeout) {
+                    const int* __restrict__ done, int* __restrict__ timeout, unsigned spin) {
     constexpr int NA = K + (STEP ? 3 : 1);  // coefficients, b (, D^-1, d)
     constexpr unsigned TILE_BYTES = STENCIL_TILE * sizeof(float);
     extern __shared__ __align__(128) float tiles[];  // [2][NA][STENCIL_TILE]
@@ -514,7 +520,7 @@ __global__ void __launch_bounds__(BULK_TH, 2)
         const int i = r0 + threadIdx.x;
         const bool full = t < nfull;
         if (full) {
-            const bool ok = mbar_wait(&bar[s], (j >> 1) & 1);
+            const bool ok = mbar_wait(&bar[s], (j >> 1) & 1, spin);
             if (__syncthreads_or(!ok)) {
                 if (threadIdx.x == 0) atomicExch(timeout, 1);
                 break;
@@ -555,11 +561,11 @@ __global__ void __launch_bounds__(BULK_TH, 2)
         }
         __syncthreads();
     }
-    // After a timeout: wait, again bounded, for the copies still in flight into this block's
-    // shared memory before the block exits.
+    // After a timeout: wait, again bounded (by the full limit, whatever `spin` was), for the
+    // copies still in flight into this block's shared memory before the block exits.
     if (threadIdx.x == 0)
         for (int s = 0; s < 2; ++s)
-            if (pending[s]) mbar_wait(&bar[s], parity[s]);
+            if (pending[s]) mbar_wait(&bar[s], parity[s], BULK_SPIN);
 }
 
 // bc = P^T r as a gather over the rows of R = P^T (multigrid.rs:166, sparse.rs:223-230).
@@ -962,7 +968,7 @@ __global__ void k_pcg_p(int64_t n, const TZ* __restrict__ z, double* __restrict_
 __global__ void k_loop_control(cudaGraphConditionalHandle h, const Scalars* sc,
                                const volatile int* cancel) {
     double rr = sc->rr;
-    bool go = !sc->done && sc->iters < sc->max_iter && rr == rr && !*cancel;
+    bool go = !sc->done && sc->iters < sc->max_iter && rr == rr && !*cancel && !sc->bulk_timeout;
     cudaGraphSetConditional(h, go ? 1u : 0u);
 }
 
@@ -1185,8 +1191,8 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
         char buf[320];
         std::snprintf(buf, sizeof buf,
                       "the matrix is not positive definite: the pivot of column %lld is 0 or less "
-                      "to the precision of the arithmetic (its diagonal is %e)",
-                      (long long)(st - 1), diag[st - 1]);
+                      "to the precision of the arithmetic (its diagonal is %s)",
+                      (long long)(st - 1), rust_exp_shortest(diag[st - 1]).c_str());
         throw Failure(FEMGPU_ERR_NOT_SPD, buf);
     }
     DevBuf<double> Lr(n * n), Y(n * n);
@@ -1344,7 +1350,7 @@ static void tune_tiles(Operator<float>* op, int mode, cudaStream_t s) {
     const StencilView<float> v = op->sview();
     auto probe = [&]() {
         k_stencil_tiles<8, false><<<tile_grid(n), BULK_TH, tile_smem<false>(), s>>>(
-            v, b.p, x.p, nullptr, 0.f, 0.f, nullptr, r.p, done.p, timeout.p);
+            v, b.p, x.p, nullptr, 0.f, 0.f, nullptr, r.p, done.p, timeout.p, BULK_SPIN);
     };
     cudaEvent_t e0, e1;
     FG_CUDA(cudaEventCreate(&e0));
@@ -1554,7 +1560,10 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
     FG_CUDA(cudaMemcpyAsync(a_.idx.p, a.idx.p, a_.idx.bytes(), cudaMemcpyDeviceToDevice, s_));
     FG_CUDA(cudaMemcpyAsync(a_.val.p, a.val.p, a_.val.bytes(), cudaMemcpyDeviceToDevice, s_));
     int C = o.sell_c ? o.sell_c : 32;
-    make_sell<double>(a_, C, &A64_, s_);
+    {
+        PhaseTimer t{this, "outer SELL", s_};
+        make_sell<double>(a_, C, &A64_, s_);
+    }
     // The block partials of the reductions: 1 block per 256 rows of the largest operator.
     partial_.alloc(2 * (size_t)row_blocks(std::max<int64_t>(a.n, A64_.nslices * A64_.C) + 64));
     x_.alloc(n_);
@@ -1785,17 +1794,21 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         lv.nnz = mats[l].nnz();
         DevCsr d;
         {
-            PhaseTimer t{this, "level operators and autotuner", s_};
+            PhaseTimer t{this, "level operators", s_};
             upload_csr(mats[l], &d, s_);
             make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
             if constexpr (std::is_same<T, float>::value)
                 if (lv.A.stencil && (opt_.values == 2 || (opt_.values == 0 && kHalfDefault)))
                     make_half(&lv.A, s_);
+        }
+        {
+            PhaseTimer t{this, "autotuner", s_};
             tune_operator(&lv.A, s_);
             if constexpr (std::is_same<T, float>::value)
                 if (l == 0) tune_tiles(&lv.A, opt_.tiles, s_);
         }
-        PhaseTimer t_lam{this, "diagonals and lambda_max", s_};
+        std::optional<PhaseTimer> t_lam;
+        t_lam.emplace(this, "diagonals and lambda_max", s_);
         // The diagonal and lambda_max(D^-1 A) in FP64.
         DevBuf<double> dg(lv.n);
         DevBuf<int> bad(1);
@@ -1818,6 +1831,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         int deg = opt_.degree > 0 ? opt_.degree : 2;
         double lower = opt_.lower > 0 ? opt_.lower : 0.3;
         chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2);
+        t_lam.reset();
         PhaseTimer t_tr{this, "transfers", s_};
         // Transfers to the next level.
         const HostRect& P = ps[l];
@@ -1868,44 +1882,59 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
 void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
                                  const HostCells* cells) {
     // multigrid.rs:84-139: coarsen until a level has at most `coarsest` unknowns, 30 levels, or
-    // a coarsening keeps more than 90 % of the unknowns. The coarse matrices are the Galerkin
-    // products, or with cells the cell-condensed matrices (each level's cells from the last).
+    // a coarsening keeps more than 90 % of the unknowns. The coarsening and the Galerkin
+    // products run on the device (coarsen.cu), the coarse unknowns numbered in grid order; with
+    // cells the coarse matrices are the cell-condensed ones (each level's cells from the last).
     std::vector<HostCsr> mats;
     std::vector<HostRect> ps;
     int threads = host_threads();
     mats.push_back(std::move(a0));
+    const DevCsr* cur = &a_;  // the device matrix of the last level
+    DevCsr held;
     if (pfirst) {
         // pmultigrid.rs:47: the P1 level is the Galerkin product with the P2 -> P1 prolongation.
-        mats.push_back(galerkin(*pfirst, mats[0], threads));
+        PhaseTimer t{this, "Galerkin products (device)", s_};
+        DevRect P;
+        rect_upload(*pfirst, &P, s_);
+        galerkin_product(P, a_, &held, s_);
+        cur = &held;
+        mats.push_back(download_csr(held, s_));
         ps.push_back(*pfirst);
     }
     size_t coarsest = (size_t)(opt_.coarsest > 0 ? opt_.coarsest : DEVICE_COARSEST);
     size_t max_levels = (size_t)(opt_.max_levels > 0 ? opt_.max_levels : 30);
     HostCells stored;  // the cells of the last coarse level
+    DevGrid grid;
+    grid_upload(level, &grid, s_);
     for (;;) {
         const HostCsr& a = mats.back();
         if ((size_t)a.n <= coarsest || ps.size() >= max_levels) break;
-        HostRect p;
-        HostLevel coarse;
+        DevRect p;
+        DevGrid coarse;
         {
-            PhaseTimer t{this, "coarsening (host)", s_};
-            if (!coarsen(level, a, &p, &coarse, opt_.axes)) break;
-            if (coarse.points.size() * 10 > (size_t)a.n * 9) break;
-            if (opt_.format == 0) renumber_grid_order(&p, &coarse);
+            PhaseTimer t{this, "coarsening (device)", s_};
+            if (!coarsen_grid(grid, *cur, opt_.axes, &p, &coarse, s_)) break;
+            if ((size_t)coarse.n * 10 > (size_t)a.n * 9) break;
         }
+        DevCsr next;
         HostCsr ac;
         if (cells && !cells->empty()) {
             PhaseTimer t_c{this, "coarse matrices from the cells (host)", s_};
             HostCells nxt;
-            ac = by_cells(level, stored.empty() ? *cells : stored, coarse, &nxt, threads);
+            ac = by_cells(grid_download(grid, s_), stored.empty() ? *cells : stored,
+                          grid_download(coarse, s_), &nxt, threads);
             stored = std::move(nxt);
+            upload_csr(ac, &next, s_);
         } else {
-            PhaseTimer t_g{this, "Galerkin products (host)", s_};
-            ac = galerkin(p, a, threads);
+            PhaseTimer t_g{this, "Galerkin products (device)", s_};
+            galerkin_product(p, *cur, &next, s_);
+            ac = download_csr(next, s_);
         }
+        held = std::move(next);
+        cur = &held;
         mats.push_back(std::move(ac));
-        ps.push_back(std::move(p));
-        level = std::move(coarse);
+        ps.push_back(rect_download(p, s_));
+        grid = std::move(coarse);
     }
     if ((size_t)mats.back().n > 16384)
         throw Failure(FEMGPU_ERR_TOO_LARGE,
@@ -1928,7 +1957,7 @@ void SolverImpl::enqueue_step(MgLevel<T>& L, const T* b, const T* xin, T c1, T c
         if (L.A.bulk) {
             launch_smem(pdl_, k_stencil_tiles<8, true>, tile_grid(L.n), BULK_TH,
                         tile_smem<true>(), s_, L.A.sview(), b, xin, (const float*)L.dinv.p, c1,
-                        c2, L.d.p, xout, done, &sc_.p->bulk_timeout);
+                        c2, L.d.p, xout, done, &sc_.p->bulk_timeout, wait_limit);
             return;
         }
     }
@@ -1945,7 +1974,7 @@ void SolverImpl::enqueue_residual(MgLevel<T>& L, const T* b, const T* x) {
         if (L.A.bulk) {
             launch_smem(pdl_, k_stencil_tiles<8, false>, tile_grid(L.n), BULK_TH,
                         tile_smem<false>(), s_, L.A.sview(), b, x, (const float*)nullptr, 0.f,
-                        0.f, (float*)nullptr, L.r.p, done, &sc_.p->bulk_timeout);
+                        0.f, (float*)nullptr, L.r.p, done, &sc_.p->bulk_timeout, wait_limit);
             return;
         }
     }
@@ -2122,6 +2151,14 @@ void SolverImpl::build_loop_graph() {
             }
         }
     }
+}
+
+void SolverImpl::set_wait_limit(unsigned polls) {
+    wait_limit = polls;
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    exec_ = nullptr;
+    graph_ = nullptr;
 }
 
 void SolverImpl::run_device_loop(const volatile int* cancel) {
@@ -2315,9 +2352,9 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         if (it == max_iter) {
             char buf[200];
             std::snprintf(buf, sizeof buf,
-                          "conjugate gradients did not converge: the residual is %.2e after %zu "
+                          "conjugate gradients did not converge: the residual is %s after %zu "
                           "iterations",
-                          residual, max_iter);
+                          rust_exp(residual, 2).c_str(), max_iter);
             status = FEMGPU_ERR_NOT_CONVERGED;
             message = buf;
             break;
@@ -2337,6 +2374,7 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
             ++it;
         }
         residual = std::sqrt(h_sc_->rr) / norm_b;
+        if (h_sc_->bulk_timeout) break;  // reported below, before any other outcome
         if (!(residual == residual)) {
             status = FEMGPU_ERR_NOT_CONVERGED;
             message = "conjugate gradients broke down: the residual is not a number";
@@ -2353,8 +2391,10 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
     out.seconds = ms * 1e-3;
     out.launches = launches_;
     if (st) *st = out;
-    if (status == FEMGPU_OK && !H32_.levels.empty() && H32_.levels[0].A.bulk) {
-        // The Scalars were read back after the last kernel of the solve.
+    if (!H32_.levels.empty() && H32_.levels[0].A.bulk) {
+        // The Scalars were read back after the last kernel of the solve. A wait that ran out
+        // leaves the iteration's vectors unfinished, so it is the outcome whatever else the
+        // loop saw after it.
         if (h_sc_->bulk_timeout) {
             status = FEMGPU_ERR_TIMEOUT;
             message = "a bulk copy of a stencil tile did not complete within its wait limit";
@@ -2434,7 +2474,7 @@ void SolverImpl::kernel_time(int which, int reps, double* ms, double* bytes) {
             if (L.A.bulk)
                 k_stencil_tiles<8, true><<<tile_grid(L.n), BULK_TH, tile_smem<true>(), s_>>>(
                     L.A.sview(), L.b.p, L.xa.p, L.dinv.p, 0.5f, 0.5f, L.d.p, L.xb.p,
-                    done_zero_.p, &sc_.p->bulk_timeout);
+                    done_zero_.p, &sc_.p->bulk_timeout, wait_limit);
             else
                 with_op(L.A, [&](auto op) {
                     k_cheb_step<float><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5f,

@@ -243,6 +243,11 @@ class SolverImpl {
     void kernel_time(int which, int reps, double* ms, double* bytes);
     size_t max_iter = 500;  // PCG_MAX_ITER, solve.rs:43
     double tol = 1e-10;     // PCG_TOL, solve.rs:42
+    // The polls of each bulk-copy wait of the stencil tile kernels before they report a
+    // timeout (FEMGPU_ERR_TIMEOUT); the default is far above any copy's latency.
+    unsigned wait_limit = 1u << 22;
+    // Sets wait_limit; the captured PCG loop holds the old value, so it is captured again.
+    void set_wait_limit(unsigned polls);
     cudaStream_t stream() const { return s_; }
     // Adds `seconds` to the setup phase `name`.
     void phase(const std::string& name, double seconds);

@@ -37,6 +37,40 @@ class Peak:
                    p.regular_element, p.regular_local, p.regular_point)
 
 
+@dataclass
+class Reactions:
+    """The result of ``reactions``: the force of each load (the reference's ``Reaction::force``
+    for a fixed face set, its ``point_force`` for a point support), the applied forces plus the
+    reactions per component, the gross magnitude of the forces and the imbalance."""
+    load_force: np.ndarray
+    total: np.ndarray
+    gross: float
+    imbalance: float
+
+
+def reactions(k, u, force, fixed, owner, nloads, applied, gross=0.0) -> Reactions:
+    """elastic::reactions (crates/fem/src/elastic.rs:772-839) on the device: r = K u - f at the
+    fixed unknowns, summed per owner load, per component and in magnitude, in the reference's
+    order. ``k`` the full stiffness (Csr), ``u`` and ``force`` full vectors, ``fixed`` a mask,
+    ``owner`` the load that fixed each unknown, ``applied`` the 3 applied sums, ``gross`` the
+    gross magnitude before the reactions."""
+    n = k.n
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    f = np.ascontiguousarray(force, dtype=np.float64)
+    fx = np.ascontiguousarray(fixed, dtype=np.uint8)
+    ow = np.ascontiguousarray(owner, dtype=np.uint32)
+    ap = np.ascontiguousarray(applied, dtype=np.float64)
+    if not (len(u) == len(f) == len(fx) == len(ow) == n) or ap.shape != (3,):
+        raise ValueError("u, force, fixed and owner need 1 value per unknown, applied 3")
+    lf = np.zeros((max(nloads, 1), 3))
+    tot = np.zeros(3)
+    g, imb = C.c_double(), C.c_double()
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    L.check(L.lib().femgpu_reactions(k._h, p(u), p(f), p(fx), p(ow), nloads, p(ap), gross,
+                                     p(lf), p(tot), C.byref(g), C.byref(imb)))
+    return Reactions(lf[:nloads].copy(), tot, g.value, imb.value)
+
+
 def hex_loads(xyz, hexes, coef, *, expansion=None, accel=None, dtemp=None):
     """The forces of the box cells' loop (crates/fem/src/elastic.rs:386-405) on the device: the
     load of the corner temperature changes ``dtemp`` (1 per point) through each cell's expansion

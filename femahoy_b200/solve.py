@@ -209,21 +209,24 @@ def symbolic_counts(a: Csr, unknowns: Unknowns):
 
 def coarse_matrix(a: Csr, unknowns: Unknowns, level: int, cells: Cells | None = None):
     """The matrix (ptr, idx, val) of multigrid level ``level`` as the solver forms it (the
-    Galerkin products, or with ``cells`` the cell-condensed matrices), its unknowns numbered as
-    multigrid.rs:329-452 numbers them."""
+    Galerkin products, or with ``cells`` the cell-condensed matrices), and the grid point (3
+    plane indices) and component of each of its unknowns, which are numbered in grid order (z,
+    y, x, component): (ptr, idx, val, points, comp)."""
     keep = []
     u = unknowns_c(unknowns, keep)
     cc = C.byref(cells._c(keep)) if cells is not None else None
     n, nnz = C.c_size_t(), C.c_size_t()
     L.check(L.lib().femgpu_coarse_matrix(a.handle, C.byref(u), cc, level, C.byref(n),
-                                         C.byref(nnz), None, None, None))
+                                         C.byref(nnz), None, None, None, None, None))
     ptr = np.empty(n.value + 1, np.int64)
     idx = np.empty(nnz.value, np.uint32)
     val = np.empty(nnz.value, np.float64)
+    pts = np.empty((n.value, 3), np.uint32)
+    comp = np.empty(n.value, np.uint8)
     L.check(L.lib().femgpu_coarse_matrix(a.handle, C.byref(u), cc, level, C.byref(n),
                                          C.byref(nnz), ptr.ctypes.data, idx.ctypes.data,
-                                         val.ctypes.data))
-    return ptr, idx, val
+                                         val.ctypes.data, pts.ctypes.data, comp.ctypes.data))
+    return ptr, idx, val, pts, comp
 
 
 class Solver:

@@ -150,12 +150,14 @@ void femgpu_csr_free(femgpu_csr* a);
  * entries (16 MiB held on every GPU that loads the library until the process exits). A larger n
  * fails with FEMGPU_ERR_TOO_LARGE. The result is the allocating entry point's, bit for bit.
  *
- * `stream` is a cudaStream_t (null: the default stream). The call checks the free list on the
- * device and waits for that check, then queues the right side on `stream` and returns;
- * synchronize the stream before reading `out`. The first call on each device looks up the
- * scratch's device address; make that first call before any stream capture. All calls share the
- * scratch, which keeps the last call's contents (each call clears what it uses); calls whose
- * work overlaps on the GPU race on it, so order them on one stream or one host thread. */
+ * `stream` is a cudaStream_t (null: the default stream). The call queues its work on `stream`,
+ * then synchronizes `stream` to read its argument checks (free rows in 0..n, increasing, each
+ * once; the column indices of the free rows in 0..n; else FEMGPU_ERR_INVALID), so `out` is
+ * written when it returns, and it cannot be made while `stream` is being captured. The first
+ * call on each device also looks up the scratch's device address. All calls share the scratch,
+ * which keeps the last call's contents (each call clears what it uses); calls whose work
+ * overlaps on the GPU race on it, so order them on one stream, or synchronize the previous
+ * call's stream before calling on another. */
 int femgpu_reduced_rhs_noalloc(size_t n, const int64_t* ptr, const uint32_t* idx,
                                const double* val, const double* load, const double* t,
                                const int64_t* free, size_t nfree, double* out, void* stream);
@@ -295,13 +297,23 @@ int femgpu_hex_mass(size_t count, const double* sizes, const double* density, do
 int femgpu_symbolic_counts(const femgpu_csr* a, const femgpu_unknowns* unknowns,
                            uint64_t* entries, double* flops);
 /* The matrix of multigrid level `level` (>= 1) that the solver of (a, unknowns, cells) forms
- * (cells may be null: the Galerkin products), with the coarse unknowns in the reference's
- * numbering of multigrid.rs:329-452; `level` coarsenings regardless of the size limits. Two
- * calls: with null arrays it writes n and nnz; then the CSR arrays. No reference counterpart:
- * for checking the hierarchy against the reference. */
+ * (cells may be null: the Galerkin products), `level` coarsenings regardless of the size limits.
+ * The coarse unknowns are numbered in grid order (z, then y, then x, then the component); the
+ * reference numbers the same unknowns in the order it first meets them (multigrid.rs:329-452).
+ * `points` (3 plane indices per unknown) and `comp` (may be null) give each coarse unknown's
+ * grid point and component. Two calls: with null arrays it writes n and nnz; then the CSR
+ * arrays. No reference counterpart: for checking the hierarchy against the reference. */
 int femgpu_coarse_matrix(const femgpu_csr* a, const femgpu_unknowns* unknowns,
                          const femgpu_cells* cells, int level, size_t* n, size_t* nnz,
-                         int64_t* ptr, uint32_t* idx, double* val);
+                         int64_t* ptr, uint32_t* idx, double* val, uint32_t* points,
+                         uint8_t* comp);
+/* The polls of each bounded wait of the device (the mbarrier waits for the bulk copies of the
+ * stencil tile kernels, femgpu_options.tiles) before the solve gives up with
+ * FEMGPU_ERR_TIMEOUT; FEMGPU_WAIT_LIMIT_DEFAULT by default. A wait that runs out ends the solve
+ * with the solver still usable. No reference counterpart: the failure-detection knob of this
+ * library's device waits (0 makes every such wait run out at once, for testing that path). */
+#define FEMGPU_WAIT_LIMIT_DEFAULT 4194304u
+int femgpu_solver_set_wait_limit(femgpu_solver* s, uint32_t polls);
 /* Solver::with_max_iter (solve.rs:187-189). */
 int femgpu_solver_set_max_iter(femgpu_solver* s, size_t max_iter);
 /* The relative residual of each PCG solve; PCG_TOL = 1e-10 (solve.rs:42) by default. */
@@ -587,6 +599,25 @@ int femgpu_recovery_last_time(const femgpu_recovery* r, double* ms, double* byte
 size_t femgpu_recovery_bytes(const femgpu_recovery* r);
 void* femgpu_recovery_stream(const femgpu_recovery* r);
 void femgpu_recovery_free(femgpu_recovery* r);
+
+/* ---------------------------------------------------------------- reactions */
+
+/* elastic::reactions (elastic.rs:772-839), as elastic.rs:585 and elastic_tet.rs:352 call it
+ * after the solve: r = K u - f at each fixed unknown i, in increasing i, summed into
+ * `load_force` (3 per load: the components of the reactions of load owner[i]; for a fixed face
+ * set that is the reference's Reaction::force, for a point support its point_force, whose
+ * warning is |component| > 1e-6 `gross_out`), into `total` (applied + the reactions, per
+ * component) and into `gross_out` (`gross` + |r|); `imbalance` = max |total| / gross_out, 0 when
+ * gross_out is 0 (the reference warns above IMBALANCE = 1e-6, elastic.rs:278). `k` is the full
+ * stiffness (3 unknowns per point, femgpu_assemble); `u` the full displacement and `force` the
+ * full force (3 per point); `fixed` 1 byte per unknown (nonzero: fixed); `owner` the load that
+ * fixed each unknown (values >= nloads are skipped, as the reference's `None`); `applied` the 3
+ * sums of the applied forces. Every sum is in the reference's order: bit-identical. Host
+ * pointers. */
+int femgpu_reactions(const femgpu_csr* k, const double* u, const double* force,
+                     const uint8_t* fixed, const uint32_t* owner, size_t nloads,
+                     const double* applied, double gross, double* load_force, double* total,
+                     double* gross_out, double* imbalance);
 
 #ifdef __cplusplus
 }

@@ -7,7 +7,7 @@ smoke check and the CPU-baseline leg of ``bench.py`` use it, as the checker; the
 (``femahoy_b200`` / ``libfemgpu.so``) never imports it.
 
 Parity is pinned by the reference's own unit-test known answers (sparse.rs:299-325,
-cholesky.rs:527-560, order.rs:336-348, tet10.rs:302-338) ported in ``tests/test_oracle.py``.
+cholesky.rs:260-293, order.rs:186-197, tet10.rs:302-338) ported in ``tests/test_oracle.py``.
 """
 from __future__ import annotations
 
@@ -43,6 +43,7 @@ def _load():
         "orc_set_threads": (None, [C.c_int]),
         "orc_submatrix": (P, [P, P, S]),
         "orc_reduced_rhs": (None, [P, P, P, P, S, P]),
+        "orc_reactions": (None, [P, P, P, P, P, S, P, D, P, P, P, P]),
         "orc_tet_gradients": (None, [P, P, P]),
         "orc_isotropic": (I, [D, D, P, P, P, S]),
         "orc_element_matrix": (I, [I, P, P, P]),
@@ -195,6 +196,21 @@ class Csr:
         if _lib.orc_assemble(self.h, kind, _p(xyz), _p(nodes), nodes.shape[0], _p(coef), err,
                              512):
             raise OracleError(err.value.decode())
+
+
+def reactions(k: Csr, u, force, fixed, owner, nloads, applied, gross=0.0):
+    """elastic.rs:772-839: (load_force (nloads, 3), total (3,), gross, imbalance)."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    f = np.ascontiguousarray(force, dtype=np.float64)
+    fx = np.ascontiguousarray(fixed, dtype=np.uint8)
+    ow = np.ascontiguousarray(owner, dtype=np.uint32)
+    ap = np.ascontiguousarray(applied, dtype=np.float64)
+    lf = np.zeros((max(nloads, 1), 3))
+    tot = np.zeros(3)
+    g, imb = C.c_double(), C.c_double()
+    _lib.orc_reactions(k.h, _p(u), _p(f), _p(fx), _p(ow), nloads, _p(ap), gross, _p(lf),
+                       _p(tot), C.byref(g), C.byref(imb))
+    return lf[:nloads], tot, g.value, imb.value
 
 
 def set_threads(n):

@@ -97,6 +97,13 @@ void orc_reduced_rhs(void* h, const double* load, const double* t, const int64_t
     std::memcpy(out, r.data(), nfree * 8);
 }
 
+void orc_reactions(void* h, const double* u, const double* force, const uint8_t* fixed,
+                   const uint32_t* owner, size_t nloads, const double* applied, double gross,
+                   double* load_force, double* total, double* gross_out, double* imbalance) {
+    reactions(*C(h), u, force, fixed, owner, nloads, applied, gross, load_force, total,
+              gross_out, imbalance);
+}
+
 // ---------------------------------------------------------------- elements
 void orc_tet_gradients(const double* p12, double* g12, double* volume) {
     Vec3 p[4], g[4];

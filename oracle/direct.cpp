@@ -428,8 +428,8 @@ Cholesky factor(const Symbolic& sym, const Csr& a) {
             char buf[320];
             std::snprintf(buf, sizeof buf,
                           "the matrix is not positive definite: the pivot of column %zu is 0 or "
-                          "less to the precision of the arithmetic (its diagonal is %e)",
-                          column, diag[(size_t)bad]);
+                          "less to the precision of the arithmetic (its diagonal is %s)",
+                          column, rust_lower_exp(diag[(size_t)bad], -1).c_str());
             throw Error(buf);
         }
         std::copy(front.begin(), front.begin() + k * m, out.values.begin() + out.offset[s]);

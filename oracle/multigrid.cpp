@@ -4,12 +4,32 @@
 // crates/fem/src/solve.rs:87-250 (the solver dispatch).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <thread>
 #include <tuple>
 
 #include "oracle.hpp"
 
 namespace orc {
+
+std::string rust_lower_exp(double v, int digits) {
+    if (v != v) return "NaN";
+    if (v == HUGE_VAL) return "inf";
+    if (v == -HUGE_VAL) return "-inf";
+    char text[48];
+    int p = digits >= 0 ? digits : 0;
+    for (;; ++p) {
+        std::snprintf(text, sizeof text, "%.*e", p, v);
+        if (digits >= 0 || p >= 16 || std::strtod(text, nullptr) == v) break;
+    }
+    // Split "d.ddde+XX" into the mantissa and the exponent's value.
+    char* e = std::strchr(text, 'e');
+    long ex = std::strtol(e + 1, nullptr, 10);
+    *e = '\0';
+    return std::string(text) + "e" + std::to_string(ex);
+}
 
 static const size_t COARSEST = 3000;  // multigrid.rs:50
 
@@ -518,9 +538,9 @@ Convergence pcg(const Csr& a, const double* b, double* x,
         if (it == max_iter) {
             char buf[200];
             std::snprintf(buf, sizeof buf,
-                          "conjugate gradients did not converge: the residual is %.2e after %zu "
+                          "conjugate gradients did not converge: the residual is %s after %zu "
                           "iterations",
-                          residual, max_iter);
+                          rust_lower_exp(residual, 2).c_str(), max_iter);
             throw Error(buf);
         }
         if (cancelled()) throw Error("cancelled");

@@ -30,6 +30,11 @@ struct Error : std::runtime_error {
     explicit Error(const std::string& s) : std::runtime_error(s) {}
 };
 
+// Rust's LowerExp text of v, as the reference's format! strings write it: digits >= 0 is
+// "{:.digits$e}" (multigrid.rs:730-732 uses 2), digits < 0 is "{:e}", the shortest digits that
+// read back to v (cholesky.rs:92-97). The exponent is a bare integer (1.23e-5, 2.5e0).
+std::string rust_lower_exp(double v, int digits);
+
 // ---------------------------------------------------------------- sparse.rs
 // sparse.rs:12-17: square CSR with both triangles, sorted columns per row.
 // Host threads of the parallel parts of the restatement: the matrix product and the PCG dot
@@ -325,5 +330,11 @@ struct Solver {
     Method method() const { return inner == Direct ? Method::Direct : Method::Multigrid; }
     Stats solve(const double* b, double* x, const std::function<bool()>& cancelled) const;
 };
+
+// elastic.rs:772-839 (reactions.cpp): r = K u - f at the fixed unknowns summed per owner
+// load (3 per load), per component into total (from `applied`) and into the gross magnitude.
+void reactions(const Csr& k, const double* u, const double* force, const uint8_t* fixed,
+               const uint32_t* owner, size_t nloads, const double applied[3], double gross,
+               double* load_force, double total[3], double* gross_out, double* imbalance);
 
 }  // namespace orc

@@ -1,6 +1,7 @@
 """The device solver against the oracle's FP64 direct solve (the reference's multifrontal
 Cholesky) and against the reference's PCG semantics and error texts."""
 import ctypes
+import re
 
 import numpy as np
 import pytest
@@ -129,8 +130,17 @@ def test_not_converged_and_cancelled_texts():
     s = fg.Solver(A, _grid(h), fg.Method.Multigrid,
                   options=fg.Options(coarsest=3000)).with_max_iter(1)
     assert len(s.levels()) >= 2
-    with pytest.raises(fg.FemError, match="^conjugate gradients did not converge: the residual is"):
+    # Rust's "{residual:.2e}": 2 digits after the point, the exponent a bare integer (1.23e-5).
+    with pytest.raises(fg.FemError) as e:
         s.solve(rhs, np.zeros(A.n))
+    assert re.fullmatch(r"conjugate gradients did not converge: the residual is "
+                        r"[1-9]\.[0-9]{2}e-?[1-9][0-9]* after 1 iterations", str(e.value)), str(e.value)
+    # From x = 0 the first residual is |b| / |b| = 1: the whole text is known.
+    s.with_max_iter(0)
+    with pytest.raises(fg.FemError) as e:
+        s.solve(rhs, np.zeros(A.n))
+    assert str(e.value) == ("conjugate gradients did not converge: the residual is 1.00e0 after "
+                            "0 iterations")
     s.with_max_iter(500)
     flag = ctypes.c_int(1)
     with pytest.raises(fg.FemError) as e:
@@ -149,13 +159,23 @@ def test_zero_right_side_gives_zero():
 
 
 def test_singular_matrix_is_not_positive_definite():
-    """cholesky.rs:547-560 on the direct path of the device."""
+    """cholesky.rs:281-293 on the direct path of the device."""
     h = mg.heat_cube(4)
     K = fg.Csr.assemble(fg.P1_HEAT, h.xyz, h.nodes, h.coef)  # no fixed points: singular
     planes = h.mesh.planes
     u = fg.Unknowns.Grid(fg.Level(planes, h.mesh.ijk, np.zeros(h.n_points, np.uint8)))
     with pytest.raises(fg.FemError, match="not positive definite"):
         fg.Solver(K, u, fg.Method.Direct)
+
+
+def test_pivot_text_is_the_references():
+    """cholesky.rs:92-97 writes the diagonal with Rust's "{:e}": the shortest digits that read
+    back, the exponent a bare integer."""
+    A = fg.Csr.from_arrays(1, np.array([0, 1]), np.array([0], np.uint32), np.array([-2.5e-3]))
+    with pytest.raises(fg.FemError) as e:
+        fg.Solver(A, fg.Unknowns.Points(np.zeros((1, 3))), fg.Method.Direct)
+    assert str(e.value) == ("the matrix is not positive definite: the pivot of column 0 is 0 or "
+                            "less to the precision of the arithmetic (its diagonal is -2.5e-3)")
 
 
 def test_solver_reuse_across_right_sides():
@@ -433,3 +453,49 @@ def test_extruded_p2_mesh_with_z_coarsening():
     xd, _ = oracle.direct_solve(Ko.submatrix(free), q.points[free // 3],
                                 Ko.reduced_rhs(load, np.zeros(3 * n), free))
     assert _rel(x, xd) <= 1e-8
+
+
+def test_bounded_wait_runs_out_and_the_solver_stays_usable():
+    """The stencil tile kernels wait on mbarriers for their bulk copies, each wait bounded. With
+    a limit of 0 polls every such wait runs out at once: the solve must end with
+    FEMGPU_ERR_TIMEOUT and its text instead of hanging, and the same handle must solve normally
+    once the default limit is back."""
+    h = mg.heat_cube(64)
+    A, rhs, _ = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=fg.MIXED,
+                  options=fg.Options(precision=fg.MIXED, tiles=2)).with_tol(1e-8)
+    assert "bulk" in s.describe(), s.describe()
+    x = np.zeros(A.n)
+    s.solve(rhs, x)
+    lib = fg.lib()
+    assert lib.femgpu_solver_set_wait_limit(s.handle, 0) == 0
+    with pytest.raises(fg.FemError) as e:
+        s.solve(rhs, np.zeros(A.n))
+    assert e.value.code == 10
+    assert str(e.value) == ("a bulk copy of a stencil tile did not complete within its wait "
+                            "limit")
+    assert lib.femgpu_solver_set_wait_limit(s.handle, 4194304) == 0
+    y = np.zeros(A.n)
+    st = s.solve(rhs, y)
+    assert st.true_residual <= 1e-8
+    assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("level", [1, 2])
+def test_heat_coarse_levels_against_the_oracle(level):
+    """The device's plane coarsening with the operator weights of a scalar (multigrid.rs:386-401)
+    and its Galerkin products P^T A P, on the lognormal heat cube: the coarse unknowns are the
+    oracle's (renumbered in grid order) and the coarse matrices agree to rounding."""
+    from test_hex_elastic import _to_grid_order
+    h = mg.heat_cube(40)
+    A, _, Ao = _system(h)
+    planes, pts, comp = mg.grid_unknowns(h)
+    ptr, idx, val, gp, gc = fg.coarse_matrix(A, _grid(h), level)
+    so = oracle.Solver(Ao, "grid", planes=planes, points=pts, comp=comp, method="multigrid",
+                       crossover=("unknowns", 0))
+    want, wp, wc = _to_grid_order(so, planes, pts, comp, level)
+    assert np.array_equal(gp, wp) and np.array_equal(gc, wc)
+    assert np.array_equal(ptr, want.indptr) and np.array_equal(idx, want.indices)
+    rows = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+    scale = np.maximum.reduceat(np.abs(want.data), ptr[:-1])[rows]
+    assert np.all(np.abs(val - want.data) <= 1e-12 * scale)

@@ -268,11 +268,43 @@ def test_gpu_hex_elements_are_bit_identical():
         fg.hex_elements(bad)
 
 
+def _kept_planes(p):
+    """multigrid.rs:341-346: every other plane and the last (axes of more than 2 planes)."""
+    p = np.asarray(p)
+    if len(p) <= 2:
+        return p
+    k = list(range(0, len(p), 2))
+    if k[-1] != len(p) - 1:
+        k.append(len(p) - 1)
+    return p[k]
+
+
+def _to_grid_order(so, planes, pts, comp, level):
+    """The oracle's matrix of `level` (its unknowns in first-sight order, multigrid.rs:329-452)
+    renumbered in grid order (z, y, x, component), and the grid points in that order."""
+    import scipy.sparse as sp
+    pl, p_, c_ = [np.asarray(x) for x in planes], pts, comp
+    for l in range(level):
+        _, p_, c_ = oracle.coarsen(so.level_matrix(l), pl, p_, c_)
+        pl = [_kept_planes(x) for x in pl]
+    comps = int(c_.max()) + 1
+    key = c_.astype(np.int64) + comps * (p_[:, 0].astype(np.int64) + len(pl[0]) * (
+        p_[:, 1].astype(np.int64) + len(pl[1]) * p_[:, 2].astype(np.int64)))
+    o = np.argsort(key, kind="stable")
+    ptr, idx, val = so.level_matrix(level).arrays()
+    m = sp.csr_matrix((val, idx, ptr), shape=(len(ptr) - 1,) * 2)[o][:, o].tocsr()
+    m.sort_indices()
+    return m, p_[o], c_[o]
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("level", [1, 2])
-def test_gpu_coarse_matrices_from_cells_are_bit_identical(level):
-    """multigrid.rs:458-608: the library's coarse matrices (host threads) equal the oracle's bit
-    for bit on a graded cantilever of 2 materials; level 2 is formed from level 1's cells."""
+def test_gpu_coarse_matrices_against_the_oracle(level):
+    """multigrid.rs:329-681 on a graded cantilever of 2 materials: the device's coarsening (grid
+    order) reaches the oracle's coarse unknowns; the coarse matrices from the cells (host
+    threads, level 2 formed from level 1's cells) equal the oracle's bit for bit, and the
+    device's Galerkin products P^T A P (coarsen.cu, summed in its own order) equal the oracle's
+    to rounding."""
     import femahoy_b200 as fg
     c = mg.hex_cantilever(nx=64, ny=8, nz=12, length=8.0, width=1.0, depth=1.5, load=-1.0,
                           grade=1.3, seed=9)
@@ -280,20 +312,27 @@ def test_gpu_coarse_matrices_from_cells_are_bit_identical(level):
     A = K.submatrix(c.free)
     planes, pts, comp = mg.grid_unknowns(c)
     cells, _ = cells_of(c, fg)
-    got = fg.coarse_matrix(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), level, cells)
+    ptr, idx, val, gp, gc = fg.coarse_matrix(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)),
+                                             level, cells)
     Ko = oracle.pattern(3 * c.mesh.n, oracle.dof_elements(c.nodes))
     Ko.assemble(6, c.xyz, c.nodes, c.coef)
     so = oracle.Solver(Ko.submatrix(c.free), "grid", planes=planes, points=pts, comp=comp,
                        method="multigrid", cells=class_table(c))
-    want = so.level_matrix(level).arrays()
-    for a, b in zip(got, want):
-        assert np.array_equal(np.asarray(a), np.asarray(b))
+    want, wp, wc = _to_grid_order(so, planes, pts, comp, level)
+    assert np.array_equal(gp, wp) and np.array_equal(gc, wc)
+    assert np.array_equal(ptr, want.indptr) and np.array_equal(idx, want.indices)
+    assert np.array_equal(val.view(np.uint64), want.data.view(np.uint64))
     # The Galerkin form through the same entry, against the oracle's P^T A P.
-    gal = fg.coarse_matrix(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), 1)
+    ptr, idx, val, gp, gc = fg.coarse_matrix(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)),
+                                             level)
     sg = oracle.Solver(Ko.submatrix(c.free), "grid", planes=planes, points=pts, comp=comp,
                        method="multigrid")
-    for a, b in zip(gal, sg.level_matrix(1).arrays()):
-        assert np.array_equal(np.asarray(a), np.asarray(b))
+    want, wp, wc = _to_grid_order(sg, planes, pts, comp, level)
+    assert np.array_equal(gp, wp) and np.array_equal(gc, wc)
+    assert np.array_equal(ptr, want.indptr) and np.array_equal(idx, want.indices)
+    rows = np.repeat(np.arange(len(ptr) - 1), np.diff(ptr))
+    scale = np.maximum.reduceat(np.abs(want.data), ptr[:-1])[rows]
+    assert np.all(np.abs(val - want.data) <= 1e-12 * scale)
 
 
 @pytest.mark.gpu

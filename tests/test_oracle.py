@@ -1,5 +1,7 @@
 """The oracle against the reference's own known answers (its unit tests), and the analytic
 identities its integration tests check. CPU only."""
+import re
+
 import numpy as np
 import pytest
 
@@ -8,7 +10,7 @@ from femahoy_b200 import meshgen as mg
 
 
 def laplacian(n):
-    """cholesky.rs:500-525: the shifted 5-point Laplacian of an n x n grid."""
+    """cholesky.rs:234-258: the shifted 5-point Laplacian of an n x n grid."""
     ids = lambda i, j: i + n * j
     elements = []
     for j in range(n):
@@ -51,7 +53,7 @@ def test_galerkin_of_1d_laplacian():
 
 
 def test_factor_solves_grid_laplacian():
-    """cholesky.rs:527-545"""
+    """cholesky.rs:260-279"""
     a, xyz = laplacian(40)
     x = np.sin(np.arange(a.n) * 0.37)
     b = a.mul(x)
@@ -61,7 +63,7 @@ def test_factor_solves_grid_laplacian():
 
 
 def test_singular_matrix_is_an_error():
-    """cholesky.rs:547-560"""
+    """cholesky.rs:281-293"""
     a, xyz = laplacian(10)
     ptr, idx, val = a.arrays()
     for i in range(a.n):
@@ -74,7 +76,7 @@ def test_singular_matrix_is_an_error():
 
 
 def test_order_is_permutation_with_middle_last():
-    """order.rs:336-348"""
+    """order.rs:186-197"""
     n = 200
     el = np.array([[i, i + 1] for i in range(n - 1)])
     a = oracle.pattern(n, el)
@@ -180,8 +182,11 @@ def test_pcg_reports_non_convergence_and_cancel():
     rhs = k.reduced_rhs(h.load, h.values, h.free)
     planes, pts, comp = mg.grid_unknowns(h)
     s = oracle.Solver(a, "grid", planes=planes, points=pts, comp=comp, method="multigrid")
-    with pytest.raises(oracle.OracleError, match="did not converge"):
+    with pytest.raises(oracle.OracleError) as e:
         s.solve(rhs, max_iter=1)
+    assert re.fullmatch(r"conjugate gradients did not converge: the residual is "
+                        r"[1-9]\.[0-9]{2}e-?[1-9][0-9]* after 1 iterations", str(e.value))
+
     with pytest.raises(oracle.OracleError, match="^cancelled$"):
         s.solve(rhs, cancel=True)
 
@@ -216,3 +221,13 @@ def test_orthotropic_with_equal_constants_is_the_isotropic_element():
     iso = oracle.element_matrix(2, p, np.array([e, nu]))
     ortho = oracle.element_matrix(4, p, np.array([e, e, e, nu, nu, nu, g, g, g]))
     assert np.array_equal(iso, ortho)
+
+
+def test_pivot_text_is_the_references():
+    """cholesky.rs:92-97: the diagonal in Rust's "{:e}" form (shortest digits, bare exponent)."""
+    a = oracle.Csr.from_arrays(1, np.array([0, 1]), np.array([0], np.uint32),
+                               np.array([-2.5e-3]))
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.direct_solve(a, np.zeros((1, 3)), np.ones(1))
+    assert str(e.value) == ("the matrix is not positive definite: the pivot of column 0 is 0 or "
+                            "less to the precision of the arithmetic (its diagonal is -2.5e-3)")

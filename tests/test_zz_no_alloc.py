@@ -32,9 +32,10 @@ def _problems():
     return [(K1, heat.load, heat.values, heat.free), (K2, beam.load, t2, beam.free)]
 
 
-def _noalloc(torch, K, load, t, free):
-    """The caller's device buffers, 1 call of the entry point, and the result."""
-    ptr, idx, val = K.arrays()
+def _noalloc(torch, K, load, t, free, arrays=None, nfree=None, check=True):
+    """The caller's device buffers, 1 call of the entry point, and the result (with
+    check=False: the status code and the message)."""
+    ptr, idx, val = K.arrays() if arrays is None else arrays
     dev = "cuda"
     d_ptr = torch.from_numpy(ptr).to(dev)
     d_idx = torch.from_numpy(idx.view(np.int32)).to(dev)
@@ -48,8 +49,13 @@ def _noalloc(torch, K, load, t, free):
     rc = fg.lib().femgpu_reduced_rhs_noalloc(
         K.n, ctypes.c_void_p(d_ptr.data_ptr()), ctypes.c_void_p(d_idx.data_ptr()),
         ctypes.c_void_p(d_val.data_ptr()), ctypes.c_void_p(d_load.data_ptr()),
-        ctypes.c_void_p(d_t.data_ptr()), ctypes.c_void_p(d_free.data_ptr()), len(free),
+        ctypes.c_void_p(d_t.data_ptr()), ctypes.c_void_p(d_free.data_ptr()),
+        len(free) if nfree is None else nfree,
         ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+    if not check:
+        buf = ctypes.create_string_buffer(256)
+        fg.lib().femgpu_last_error(buf, 256)
+        return rc, buf.value.decode()
     _lib.check(rc)
     stream.synchronize()
     return d_out.cpu().numpy()
@@ -75,3 +81,33 @@ def test_noalloc_refuses_a_matrix_past_its_scratch():
     buf = ctypes.create_string_buffer(256)
     fg.lib().femgpu_last_error(buf, 256)
     assert b"4194304" in buf.value
+
+
+def test_noalloc_rejects_bad_free_rows_and_columns_then_still_works():
+    """The argument checks run on the device before the result is trusted; every bad case is
+    FEMGPU_ERR_INVALID with its own text, and a valid call afterwards is still bit-exact (the
+    scratch is cleared per call)."""
+    torch = pytest.importorskip("torch")
+    K, load, t, free = _problems()[0]
+    n = K.n
+    cases = [
+        (np.concatenate([free[:-1], [n + 5]]), None, "a free row is out of range"),
+        (np.concatenate([free[:3], free[2:]]), None, "the free rows hold a row twice"),
+        (free[::-1].copy(), None, "the free rows are not increasing"),
+    ]
+    for bad_free, arrays, text in cases:
+        rc, msg = _noalloc(torch, K, load, t, bad_free, arrays=arrays, check=False)
+        assert rc == 5 and msg == text, (rc, msg)
+    # A column index past n in a free row.
+    ptr, idx, val = K.arrays()
+    idx = idx.copy()
+    idx[ptr[free[0]]] = n + 7
+    rc, msg = _noalloc(torch, K, load, t, free, arrays=(ptr, idx, val), check=False)
+    assert rc == 5 and msg == "a column index of a free row is out of range", (rc, msg)
+    # More free rows than rows, and a count whose size_t wraps to a negative int64.
+    for nfree in (n + 1, 2**64 - 1):
+        rc, msg = _noalloc(torch, K, load, t, free, nfree=nfree, check=False)
+        assert rc == 5 and msg == "more free rows than rows", (rc, msg)
+    expected = fg.reduced_rhs(K, load, t, free)
+    got = _noalloc(torch, K, load, t, free)
+    assert np.array_equal(got.view(np.uint64), expected.view(np.uint64))
