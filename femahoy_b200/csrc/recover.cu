@@ -34,6 +34,7 @@
 #include "common.cuh"
 #include "elements.cuh"
 #include "hex.cuh"
+#include "rust_format.hpp"
 
 namespace femgpu {
 
@@ -212,19 +213,19 @@ __global__ void k_pad_u(const double* __restrict__ u, int64_t npoints, double* _
 // Tet10::strain_stress (tet10.rs:142-169) of cell e (record rp, points t) at its point c,
 // followed by reorder and tensor_strain (elastic.rs:967-975): sig and eps in the order xx, yy,
 // zz, xy, yz, xz.
+__device__ __forceinline__ void strain_stress_l(const CellRecord* __restrict__ rp,
+                                                const MaterialEntry* __restrict__ mats,
+                                                const uint32_t t[10], const double l[4],
+                                                const double* __restrict__ u4,
+                                                const double* __restrict__ dtemp,
+                                                double sig[6], double eps[6], uint32_t* tag);
+
 __device__ __forceinline__ void strain_stress_at(const CellRecord* __restrict__ rp,
                                                  const MaterialEntry* __restrict__ mats,
                                                  const uint32_t t[10], int c,
                                                  const double* __restrict__ u4,
                                                  const double* __restrict__ dtemp,
                                                  double sig[6], double eps[6], uint32_t* tag) {
-    const double* rd = reinterpret_cast<const double*>(rp);
-    double g[12];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) ld32(rd + 4 * k, g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
-    const uint2 mt = __ldg(reinterpret_cast<const uint2*>(rd + 12));
-    const uint32_t mat = mt.x;
-    *tag = mt.y;
     // node_coordinates (tet10.rs:216-228)
     double l[4];
     if (c < 4) {
@@ -235,6 +236,24 @@ __device__ __forceinline__ void strain_stress_at(const CellRecord* __restrict__ 
 #pragma unroll
         for (int k = 0; k < 4; ++k) l[k] = (k == i || k == j) ? 0.5 : 0.0;
     }
+    strain_stress_l(rp, mats, t, l, u4, dtemp, sig, eps, tag);
+}
+
+// Tet10::strain_stress (tet10.rs:142-169) of cell e at the volume coordinates l, with reorder
+// and tensor_strain as above.
+__device__ __forceinline__ void strain_stress_l(const CellRecord* __restrict__ rp,
+                                                const MaterialEntry* __restrict__ mats,
+                                                const uint32_t t[10], const double l[4],
+                                                const double* __restrict__ u4,
+                                                const double* __restrict__ dtemp,
+                                                double sig[6], double eps[6], uint32_t* tag) {
+    const double* rd = reinterpret_cast<const double*>(rp);
+    double g[12];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) ld32(rd + 4 * k, g[4 * k], g[4 * k + 1], g[4 * k + 2], g[4 * k + 3]);
+    const uint2 mt = __ldg(reinterpret_cast<const uint2*>(rd + 12));
+    const uint32_t mat = mt.x;
+    *tag = mt.y;
     double e[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int i = 0; i < 10; ++i) {
@@ -669,6 +688,111 @@ __global__ void k_peak_final(const u128* __restrict__ peak, int nparts,
 
 using namespace femgpu;
 
+// ------------------------------------------------------------------ probes
+// elastic_tet.rs:428-467 with cells_at (elastic_tet.rs:538-553): a probe takes the cells whose
+// volume coordinates of its point are all >= -1e-9. k_probe_hits tests every (probe, cell) pair
+// (a few probes against all cells, as the reference's search) and lists the hits; then 1 thread
+// per probe sorts its hits and sums their shares in increasing cell order, the reference's
+// order, so the values are bit-identical (the unit is built with -fmad=false).
+constexpr int MAX_PROBE_HITS = 512;
+
+// The volume coordinates of x in cell e: l[i] = sum_d g[i][d] (x[d] - p0[d]) for i >= 1 (a
+// float sum from -0.0), l[0] = 1 - l[1] - l[2] - l[3].
+__device__ __forceinline__ void probe_coordinates(const CellRecord& r, const double* p0,
+                                                  const double x[3], double l[4]) {
+#pragma unroll
+    for (int i = 1; i < 4; ++i) {
+        double sum = -0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sum += r.g[3 * i + d] * (x[d] - p0[d]);
+        l[i] = sum;
+    }
+    l[0] = 1.0 - l[1] - l[2] - l[3];
+}
+
+__global__ void k_probe_hits(const CellRecord* __restrict__ rec, const double* __restrict__ xyz,
+                             const uint32_t* __restrict__ t10, int64_t nel,
+                             const double* __restrict__ points, int64_t nprobes,
+                             int* __restrict__ count, int64_t* __restrict__ hits) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nel * nprobes;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = k / nel, e = k % nel;
+        const double x[3] = {points[3 * q], points[3 * q + 1], points[3 * q + 2]};
+        const double* p0 = xyz + 3 * (int64_t)t10[10 * e];
+        double l[4];
+        probe_coordinates(rec[e], p0, x, l);
+        if (l[0] >= -1e-9 && l[1] >= -1e-9 && l[2] >= -1e-9 && l[3] >= -1e-9) {
+            const int slot = atomicAdd(count + q, 1);
+            if (slot < MAX_PROBE_HITS) hits[q * MAX_PROBE_HITS + slot] = e;
+        }
+    }
+}
+
+__global__ void k_probe_values(const CellRecord* __restrict__ rec,
+                               const MaterialEntry* __restrict__ mats,
+                               const double* __restrict__ xyz, const uint32_t* __restrict__ t10,
+                               const double* __restrict__ u4, const double* __restrict__ dtemp,
+                               const double* __restrict__ temperature,
+                               const double* __restrict__ points, int64_t nprobes,
+                               const int* __restrict__ count, int64_t* __restrict__ hits,
+                               double* __restrict__ disp, double* __restrict__ stress,
+                               double* __restrict__ mises, double* __restrict__ temp) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nprobes;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        const int m = count[q];
+        if (m < 1 || m > MAX_PROBE_HITS) continue;
+        int64_t* h = hits + q * MAX_PROBE_HITS;
+        for (int a = 1; a < m; ++a) {  // insertion sort: increasing cells
+            const int64_t v = h[a];
+            int b = a;
+            while (b > 0 && h[b - 1] > v) {
+                h[b] = h[b - 1];
+                --b;
+            }
+            h[b] = v;
+        }
+        const double x[3] = {points[3 * q], points[3 * q + 1], points[3 * q + 2]};
+        const double share = 1.0 / (double)m;
+        double dsp[3] = {0.0, 0.0, 0.0}, sg[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, tv = 0.0;
+        for (int k = 0; k < m; ++k) {
+            const int64_t e = h[k];
+            uint32_t t[10];
+#pragma unroll
+            for (int c = 0; c < 10; ++c) t[c] = t10[10 * e + c];
+            double l[4];
+            probe_coordinates(rec[e], xyz + 3 * (int64_t)t[0], x, l);
+            // Tet10 shape functions (tet10.rs:51-60).
+            double w[10];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) w[i] = l[i] * (2.0 * l[i] - 1.0);
+#pragma unroll
+            for (int j = 0; j < 6; ++j) w[4 + j] = 4.0 * l[edge_corner(j, 0)] * l[edge_corner(j, 1)];
+#pragma unroll
+            for (int c = 0; c < 10; ++c) {
+                double ui[3], unused;
+                ld32(u4 + 4 * (int64_t)t[c], ui[0], ui[1], ui[2], unused);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) dsp[a] += share * w[c] * ui[a];
+            }
+            double sig[6], eps[6];
+            uint32_t tag;
+            strain_stress_l(rec + e, mats, t, l, u4, dtemp, sig, eps, &tag);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) sg[i] += share * sig[i];
+            if (temperature) {
+                double sum = -0.0;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) sum += l[c] * temperature[t[c]];
+                tv += share * sum;
+            }
+        }
+        for (int a = 0; a < 3; ++a) disp[3 * q + a] = dsp[a];
+        for (int i = 0; i < 6; ++i) stress[6 * q + i] = sg[i];
+        mises[q] = mises6(sg);
+        temp[q] = tv;
+    }
+}
+
 struct femgpu_recovery {
     int64_t npoints = 0, nel = 0, nmat = 0;
     int nparts = 1;
@@ -680,6 +804,7 @@ struct femgpu_recovery {
     Incidence inc;
     DevBuf<uint8_t> place;
     DevBuf<uint32_t> t10;
+    DevBuf<double> xyz;  // the points (P2 cells), for the probes
     DevBuf<CellRecord> rec;
     DevBuf<MaterialEntry> mats;
     DevBuf<uint8_t> singular;
@@ -888,6 +1013,7 @@ int femgpu_recovery_new(size_t npoints, const double* xyz, size_t nel, const uin
         if (b == 3) throw Failure(FEMGPU_ERR_INVALID, "a cell names a part past the last");
         r->peak.alloc(3 * nparts);
         r->dpeaks.alloc(nparts);
+        r->xyz = std::move(dxyz);
         FG_CUDA(cudaStreamSynchronize(s));
         *out = r.release();
     });
@@ -1024,6 +1150,57 @@ int femgpu_recovery_run_device(femgpu_recovery* r, const double* u, const double
     });
 }
 
+int femgpu_recovery_probes(femgpu_recovery* r, const double* u, const double* dtemp,
+                           const double* temperature, size_t nprobes, const double* points,
+                           const char* const* names, double* displacement, double* stress,
+                           double* mises, double* temp, int64_t* hits) {
+    return recovery_guarded([&] {
+        need(r && u && points && displacement && stress && mises && temp, "a null argument");
+        need(!r->hex, "the probes take the cells of a P2 model");
+        if (nprobes == 0) return;
+        if (nprobes > (1u << 20)) throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 2^20 probes");
+        cudaStream_t s = r->s;
+        const int64_t n = r->npoints, np = (int64_t)nprobes;
+        r->du.upload(u, 3 * n, s);
+        DevBuf<double> ddt, dtemp_abs, dpts(3 * np), ddisp(3 * np), dstress(6 * np),
+            dmises(np), dtv(np);
+        if (dtemp) ddt.upload(dtemp, n, s);
+        if (temperature) dtemp_abs.upload(temperature, n, s);
+        dpts.upload(points, 3 * np, s);
+        DevBuf<int> count(np);
+        DevBuf<int64_t> dhits(np * MAX_PROBE_HITS);
+        count.zero(s);
+        k_pad_u<<<blocks_for(n, 256), 256, 0, s>>>(r->du.p, n, r->u4.p);
+        k_probe_hits<<<blocks_for(r->nel * np, 256, NUM_SMS * 64), 256, 0, s>>>(
+            r->rec.p, r->xyz.p, r->t10.p, r->nel, dpts.p, np, count.p, dhits.p);
+        k_probe_values<<<blocks_for(np, 64), 64, 0, s>>>(
+            r->rec.p, r->mats.p, r->xyz.p, r->t10.p, r->u4.p, dtemp ? ddt.p : nullptr,
+            temperature ? dtemp_abs.p : nullptr, dpts.p, np, count.p, dhits.p, ddisp.p,
+            dstress.p, dmises.p, dtv.p);
+        FG_CHECK_LAUNCH();
+        std::vector<int> c(np);
+        count.download(c.data(), np, s);
+        ddisp.download(displacement, 3 * np, s);
+        dstress.download(stress, 6 * np, s);
+        dmises.download(mises, np, s);
+        dtv.download(temp, np, s);
+        FG_CUDA(cudaStreamSynchronize(s));
+        for (int64_t q = 0; q < np; ++q) {
+            if (hits) hits[q] = c[q];
+            if (c[q] == 0) {
+                // elastic_tet.rs:433-438
+                const double* x = points + 3 * q;
+                std::string name = names && names[q] ? names[q] : std::to_string(q);
+                throw Failure(FEMGPU_ERR_INVALID, "probe " + name + " at (" + rust_display(x[0]) +
+                                                      ", " + rust_display(x[1]) + ", " +
+                                                      rust_display(x[2]) + ") is in no part");
+            }
+            if (c[q] > MAX_PROBE_HITS)
+                throw Failure(FEMGPU_ERR_TOO_LARGE, "a probe point is in more than 512 cells");
+        }
+    });
+}
+
 int femgpu_recovery_last_time(const femgpu_recovery* r, double* ms, double* bytes) {
     return recovery_guarded([&] {
         need(r != nullptr, "a null handle");
@@ -1037,6 +1214,7 @@ size_t femgpu_recovery_bytes(const femgpu_recovery* r) {
     return r->t10.bytes() + r->rec.bytes() + r->mats.bytes() + r->singular.bytes() +
            r->hrec.bytes() + r->hmodes.bytes() + r->amp.bytes() +
            r->place.bytes() + r->u4.bytes() + r->peak.bytes() + r->dpeaks.bytes() +
+           r->xyz.bytes() +
            r->inc.start.bytes() +
            r->inc.of_node.bytes() + r->du.bytes() + r->ddt.bytes() + r->dstress.bytes() +
            r->dstrain.bytes() + r->dmises.bytes() + r->dprincipal.bytes();

@@ -49,4 +49,39 @@ inline std::string rust_exp_shortest(double v) {
     return rust_exponent_text(buf);
 }
 
+// Rust's "{}" (Display) of v: the shortest digits that read back to v, written out in full
+// positional notation with no exponent (1e-7 is 0.0000001, 1e21 twenty-two digits, 2.0 is 2).
+inline std::string rust_display(double v) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
+    char buf[64];
+    int digits = 0;
+    for (; digits < 17; ++digits) {
+        std::snprintf(buf, sizeof buf, "%.*e", digits, v);
+        if (std::strtod(buf, nullptr) == v) break;
+    }
+    if (digits == 17) std::snprintf(buf, sizeof buf, "%.16e", v);
+    // buf: [-]D[.DDD]e(+|-)XX
+    std::string t(buf);
+    const bool neg = t[0] == '-';
+    if (neg) t.erase(0, 1);
+    const size_t e = t.find('e');
+    const int ex = std::atoi(t.c_str() + e + 1);
+    std::string d;
+    for (size_t k = 0; k < e; ++k)
+        if (t[k] != '.') d += t[k];
+    while (d.size() > 1 && d.back() == '0') d.pop_back();
+    std::string out;
+    if (ex >= 0) {
+        if ((int)d.size() <= ex + 1) {
+            out = d + std::string(ex + 1 - d.size(), '0');
+        } else {
+            out = d.substr(0, ex + 1) + "." + d.substr(ex + 1);
+        }
+    } else {
+        out = "0." + std::string(-ex - 1, '0') + d;
+    }
+    return (neg ? "-" : "") + out;
+}
+
 }  // namespace femgpu

@@ -138,6 +138,33 @@ class Recovery:
         return {"stress": stress, "strain": strain, "mises": mises, "principal": pr,
                 "peaks": [Peak.of(p) for p in pk] if peaks else None}
 
+    def probes(self, u, points, *, dtemp=None, temperature=None, names=None):
+        """The probes (crates/fem/src/elastic_tet.rs:428-467) at ``points`` (P, 3): a dict of
+        displacement (P, 3), stress (P, 6), mises (P,), temperature (P,) and hits (P,), the
+        cells that share each point. ``temperature`` holds the absolute corner temperatures,
+        ``dtemp`` their change (for the stress); ``names`` the probes' names for the error of a
+        point in no cell."""
+        n = self.npoints
+        u = L.arr(u, np.float64).reshape(-1)
+        if len(u) != 3 * n:
+            raise L.FemError(L.INVALID, "u holds 3 values per point")
+        pts = L.arr(points, np.float64).reshape(-1, 3)
+        m = len(pts)
+        dt = None if dtemp is None else L.arr(dtemp, np.float64)
+        tp = None if temperature is None else L.arr(temperature, np.float64)
+        nm = None
+        if names is not None:
+            enc = [x.encode() for x in names]
+            nm = (C.c_char_p * m)(*enc)
+        disp, stress, mises, temp = np.empty((m, 3)), np.empty((m, 6)), np.empty(m), np.empty(m)
+        hits = np.empty(m, np.int64)
+        L.check(L.lib().femgpu_recovery_probes(
+            self._h, L.ptr(u), L.ptr(dt), L.ptr(tp), m, L.ptr(pts),
+            C.cast(nm, C.c_void_p) if nm is not None else None, L.ptr(disp), L.ptr(stress),
+            L.ptr(mises), L.ptr(temp), L.ptr(hits)))
+        return {"displacement": disp, "stress": stress, "mises": mises, "temperature": temp,
+                "hits": hits}
+
     def run_device(self, u, stress, strain, *, dtemp=None, mises=None, principal=None,
                    peaks=True):
         """Device buffers (torch CUDA float64 tensors, contiguous) in and out; returns the list

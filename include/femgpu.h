@@ -593,6 +593,19 @@ int femgpu_recovery_run(femgpu_recovery* r, const double* u, const double* dtemp
 int femgpu_recovery_run_device(femgpu_recovery* r, const double* u, const double* dtemp,
                                double* stress, double* strain, double* mises, double* principal,
                                femgpu_peak* peaks);
+/* The probes of a P2 model (elastic_tet.rs:428-467): for each point (3 coordinates each), the
+ * cells whose volume coordinates of the point are all >= -1e-9 (cells_at, elastic_tet.rs:538-553),
+ * each taking the share 1 / hits of the displacement (the 10 functions of tet10.rs:51-60), the
+ * stress (Tet10::strain_stress with `dtemp`) and the temperature (the 4 corners of `temperature`,
+ * the absolute corner temperatures; NULL: 0), summed in increasing cell order as the reference;
+ * `mises` of the mean stress. Outputs: displacement 3, stress 6 (xx, yy, zz, xy, yz, xz), mises 1,
+ * temp 1 per probe; `hits` (may be NULL) the cells of each. A probe in no cell fails with the
+ * reference's text "probe NAME at (x, y, z) is in no part" (names may be NULL: the index), the
+ * coordinates as Rust's {} writes them. Bit-identical with the reference. Host pointers. */
+int femgpu_recovery_probes(femgpu_recovery* r, const double* u, const double* dtemp,
+                           const double* temperature, size_t nprobes, const double* points,
+                           const char* const* names, double* displacement, double* stress,
+                           double* mises, double* temp, int64_t* hits);
 /* The device time of the recovery kernels of the last run in ms (CUDA events), and the
  * algorithmic bytes they move: the cell records, the incidence and u once, the outputs once. */
 int femgpu_recovery_last_time(const femgpu_recovery* r, double* ms, double* bytes);

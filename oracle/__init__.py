@@ -44,6 +44,7 @@ def _load():
         "orc_submatrix": (P, [P, P, S]),
         "orc_reduced_rhs": (None, [P, P, P, P, S, P]),
         "orc_reactions": (None, [P, P, P, P, P, S, P, D, P, P, P, P]),
+        "orc_probes": (C.c_long, [P, S, P, P, P, P, P, P, S, P, P, P, P, P, P]),
         "orc_tet_gradients": (None, [P, P, P]),
         "orc_isotropic": (I, [D, D, P, P, P, S]),
         "orc_element_matrix": (I, [I, P, P, P]),
@@ -211,6 +212,22 @@ def reactions(k: Csr, u, force, fixed, owner, nloads, applied, gross=0.0):
     _lib.orc_reactions(k.h, _p(u), _p(f), _p(fx), _p(ow), nloads, _p(ap), gross, _p(lf),
                        _p(tot), C.byref(g), C.byref(imb))
     return lf[:nloads], tot, g.value, imb.value
+
+
+def probes(xyz, tets10, coef, u, points, *, expansion=None, dtemp=None, temperature=None):
+    """elastic_tet.rs:428-467: (displacement (P, 3), stress (P, 6), mises (P,), temperature
+    (P,), hits (P,)); raises OracleError for a probe in no cell."""
+    f = lambda a, t=np.float64: None if a is None else np.ascontiguousarray(a, dtype=t)
+    xyz_, t10, cf, uu, pts = f(xyz), f(tets10, np.uint32), f(coef), f(u), f(points)
+    ex, dt, tp = f(expansion), f(dtemp), f(temperature)
+    n = len(pts)
+    dsp, st, ms, tv = np.zeros((n, 3)), np.zeros((n, 6)), np.zeros(n), np.zeros(n)
+    hits = np.zeros(n, np.int64)
+    bad = _lib.orc_probes(_p(xyz_), len(t10), _p(t10), _p(cf), _p(ex), _p(dt), _p(tp), _p(uu),
+                          n, _p(pts), _p(dsp), _p(st), _p(ms), _p(tv), _p(hits))
+    if bad >= 0:
+        raise OracleError(f"probe {bad} is in no part")
+    return dsp, st, ms, tv, hits
 
 
 def set_threads(n):

@@ -540,6 +540,14 @@ int orc_recover(size_t npoints, const double* xyz, size_t nel, const uint32_t* t
         return -1;
     }
 }
+// elastic_tet.rs:428-467 (see probes_tet10).
+long orc_probes(const double* xyz, size_t nel, const uint32_t* tets10, const double* coef,
+                const double* expansion, const double* dtemp, const double* temperature,
+                const double* u, size_t nprobes, const double* points, double* displacement,
+                double* stress, double* mises_out, double* temp_out, int64_t* hits) {
+    return probes_tet10(xyz, nel, tets10, coef, expansion, dtemp, temperature, u, nprobes,
+                        points, displacement, stress, mises_out, temp_out, hits);
+}
 // elastic.rs:615-660 and 709-710 (see recover_hex8), as orc_recover.
 int orc_recover_hex(size_t npoints, const double* xyz, size_t nel, const uint32_t* hexes,
                     const double* coef, const double* expansion, const double* dtemp,

@@ -337,4 +337,11 @@ void reactions(const Csr& k, const double* u, const double* force, const uint8_t
                const uint32_t* owner, size_t nloads, const double applied[3], double gross,
                double* load_force, double total[3], double* gross_out, double* imbalance);
 
+// elastic_tet.rs:428-467 (recover.cpp): the probes of a P2 model; the first probe in no cell,
+// or -1.
+long probes_tet10(const double* xyz, size_t nel, const uint32_t* tets10, const double* coef,
+                  const double* expansion, const double* dtemp, const double* temperature,
+                  const double* u, size_t nprobes, const double* points, double* displacement,
+                  double* stress, double* mises_out, double* temp_out, int64_t* hits_out);
+
 }  // namespace orc

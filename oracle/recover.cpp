@@ -6,7 +6,9 @@
 // (Stiffness::stress), crates/fem/src/elastic.rs:965-1002 (reorder, tensor_strain, mises,
 // principal), elastic_tet.rs:164-170 (D alpha of a material) and elastic_tet.rs:482-483 (the
 // von Mises stress and the principal stresses of the mean stress at each point).
+#include <array>
 #include <cmath>
+#include <utility>
 #include <limits>
 
 #include "oracle.hpp"
@@ -195,6 +197,85 @@ void recover_tet10(size_t npoints, const double* xyz, size_t nel, const uint32_t
         if (mises_out) mises_out[i] = mises(stress + 6 * i);
         if (principal_out) principal(stress + 6 * i, principal_out + 3 * i);
     }
+}
+
+// tet10.rs:51-60: the 10 quadratic functions at the volume coordinates l.
+void tet10_shape(const double l[4], double n[10]) {
+    for (int i = 0; i < 4; ++i) n[i] = l[i] * (2.0 * l[i] - 1.0);
+    for (int k = 0; k < 6; ++k) n[4 + k] = 4.0 * l[EDGES[k][0]] * l[EDGES[k][1]];
+}
+
+// elastic_tet.rs:428-467 with cells_at (elastic_tet.rs:538-553): for each probe, the cells
+// whose volume coordinates of the point are all >= -1e-9, in increasing order, each with the
+// share 1 / hits of the displacement (the 10 functions), the stress (Tet10::strain_stress) and
+// the temperature (the 4 corners; `temperature` NULL: 0) at the point; then the von Mises
+// stress of the mean stress. Returns the first probe in no cell, or -1.
+long probes_tet10(const double* xyz, size_t nel, const uint32_t* tets10, const double* coef,
+                  const double* expansion, const double* dtemp, const double* temperature,
+                  const double* u, size_t nprobes, const double* points, double* displacement,
+                  double* stress, double* mises_out, double* temp_out, int64_t* hits_out) {
+    for (size_t q = 0; q < nprobes; ++q) {
+        const double* x = points + 3 * q;
+        vector<std::pair<size_t, std::array<double, 4>>> hits;
+        for (size_t e = 0; e < nel; ++e) {
+            const uint32_t* nodes = tets10 + 10 * e;
+            Vec3 p[4], g[4];
+            for (int k = 0; k < 4; ++k)
+                for (int dd = 0; dd < 3; ++dd) p[k][dd] = xyz[3 * (size_t)nodes[k] + dd];
+            double volume;
+            tet_gradients(p, g, &volume);
+            std::array<double, 4> l{};
+            for (int i = 1; i < 4; ++i) {
+                double sum = -0.0;
+                for (int dd = 0; dd < 3; ++dd) sum += g[i][dd] * (x[dd] - p[0][dd]);
+                l[i] = sum;
+            }
+            l[0] = 1.0 - l[1] - l[2] - l[3];
+            bool inside = true;
+            for (int k = 0; k < 4; ++k) inside = inside && l[k] >= -1e-9;
+            if (inside) hits.push_back({e, l});
+        }
+        if (hits_out) hits_out[q] = (int64_t)hits.size();
+        if (hits.empty()) return (long)q;
+        const double share = 1.0 / (double)hits.size();
+        double dsp[3] = {0.0, 0.0, 0.0}, sg[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, tv = 0.0;
+        for (const auto& h : hits) {
+            const size_t e = h.first;
+            const double* l = h.second.data();
+            const uint32_t* nodes = tets10 + 10 * e;
+            double w[10];
+            tet10_shape(l, w);
+            for (int c = 0; c < 10; ++c)
+                for (int a = 0; a < 3; ++a) dsp[a] += share * w[c] * u[3 * (size_t)nodes[c] + a];
+            Vec3 p[4], g[4];
+            for (int k = 0; k < 4; ++k)
+                for (int dd = 0; dd < 3; ++dd) p[k][dd] = xyz[3 * (size_t)nodes[k] + dd];
+            double volume;
+            tet_gradients(p, g, &volume);
+            Stiffness d = isotropic_stiffness(coef[2 * e], coef[2 * e + 1]);
+            double alpha[3] = {0.0, 0.0, 0.0};
+            if (expansion)
+                for (int k = 0; k < 3; ++k) alpha[k] = expansion[3 * e + k];
+            double thermal[3];
+            thermal_stress(d, alpha, thermal);
+            double ue[30], te[4], eng[6], sig0[6], sig[6];
+            for (int r = 0; r < 30; ++r) ue[r] = u[3 * (size_t)nodes[r / 3] + r % 3];
+            for (int c = 0; c < 4; ++c) te[c] = dtemp ? dtemp[nodes[c]] : 0.0;
+            tet10_strain_stress(g, d, thermal, l, ue, te, eng, sig0);
+            reorder_stress(sig0, sig);
+            for (int i = 0; i < 6; ++i) sg[i] += share * sig[i];
+            if (temperature) {
+                double sum = -0.0;
+                for (int c = 0; c < 4; ++c) sum += l[c] * temperature[nodes[c]];
+                tv += share * sum;
+            }
+        }
+        for (int a = 0; a < 3; ++a) displacement[3 * q + a] = dsp[a];
+        for (int i = 0; i < 6; ++i) stress[6 * q + i] = sg[i];
+        mises_out[q] = mises(sg);
+        temp_out[q] = tv;
+    }
+    return -1;
 }
 
 // elastic.rs:615-660 (the box grid): the strain and the stress at the 8 corners of each cell
