@@ -38,8 +38,10 @@ UNITS = [
     ("modes.cu", ["-fmad=false"]),
     ("reactions.cu", ["-fmad=false"]),
     ("coarsen.cu", []),
+    ("sparse_direct.cu", []),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
+             ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),
              ("dense_eigen.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"])]
 
 
@@ -95,7 +97,11 @@ def build(verbose: bool = False, force: bool = False) -> str:
             if verbose and err:
                 print(err)
     if force or jobs or _stale(objs, LIB):
-        run([nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart", "-lpthread"])
+        # Link beside the library and rename it into place, so that the file is never seen
+        # half written.
+        tmp = LIB + ".tmp"
+        run([nvcc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lpthread"])
+        os.replace(tmp, LIB)
     return LIB
 
 

@@ -8,6 +8,7 @@
 #include "hierarchy.hpp"
 #include "solver.cuh"
 #include "coarsen.cuh"
+#include "symbolic.hpp"
 
 namespace femgpu {
 
@@ -364,7 +365,7 @@ int femgpu_symbolic_counts(const femgpu_csr* a, const femgpu_unknowns* u, uint64
             require(u->xyz != nullptr, "points need coordinates");
             std::copy(u->xyz, u->xyz + 3 * m.n, xyz.begin());
         }
-        factor_counts(m, nested_dissection(m, xyz.data()), entries, flops);
+        factor_figures(m, nested_dissection(m, xyz.data()), entries, flops);
     });
 }
 

@@ -440,100 +440,6 @@ std::vector<int64_t> nested_dissection(const HostCsr& a, const double* xyz) {
     return order;
 }
 
-void factor_counts(const HostCsr& a, const std::vector<int64_t>& order, uint64_t* entries,
-                   double* flops) {
-    const int64_t n = a.n;
-    auto inverse = [&](const std::vector<int64_t>& p) {
-        std::vector<int64_t> ip(n);
-        for (int64_t k = 0; k < n; ++k) ip[p[k]] = k;
-        return ip;
-    };
-    const std::vector<int64_t> iorder = inverse(order);
-    // symbolic.rs:195-216: the elimination tree with path compression.
-    std::vector<int64_t> parent0(n, NOPE), ancestor(n, NOPE);
-    for (int64_t k = 0; k < n; ++k) {
-        const int64_t old = order[k];
-        for (int64_t e = a.ptr[old]; e < a.ptr[old + 1]; ++e) {
-            int64_t i = iorder[a.idx[e]];
-            while (i != NOPE && i < k) {
-                const int64_t next = ancestor[i];
-                ancestor[i] = k;
-                if (next == NOPE) parent0[i] = k;
-                i = next;
-            }
-        }
-    }
-    // symbolic.rs:218-246: a postorder, children in increasing order.
-    std::vector<int64_t> head(n, NOPE), next(n, NOPE), post;
-    post.reserve(n);
-    for (int64_t j = n - 1; j >= 0; --j)
-        if (parent0[j] != NOPE) {
-            next[j] = head[parent0[j]];
-            head[parent0[j]] = j;
-        }
-    std::vector<int64_t> stack;
-    for (int64_t root = 0; root < n; ++root) {
-        if (parent0[root] != NOPE) continue;
-        stack.push_back(root);
-        while (!stack.empty()) {
-            const int64_t top = stack.back();
-            const int64_t child = head[top];
-            if (child == NOPE) {
-                stack.pop_back();
-                post.push_back(top);
-            } else {
-                head[top] = next[child];
-                stack.push_back(child);
-            }
-        }
-    }
-    std::vector<int64_t> perm(n);
-    for (int64_t k = 0; k < n; ++k) perm[k] = order[post[k]];
-    const std::vector<int64_t> iperm = inverse(perm), ipost = inverse(post);
-    std::vector<int64_t> parent(n);
-    for (int64_t k = 0; k < n; ++k)
-        parent[k] = parent0[post[k]] == NOPE ? NOPE : ipost[parent0[post[k]]];
-    // symbolic.rs:249-266: the column counts from the row subtrees.
-    std::vector<int64_t> counts(n, 1), mark(n, NOPE);
-    for (int64_t i = 0; i < n; ++i) {
-        mark[i] = i;
-        const int64_t old = perm[i];
-        for (int64_t e = a.ptr[old]; e < a.ptr[old + 1]; ++e) {
-            int64_t j = iperm[a.idx[e]];
-            while (j < i && mark[j] != i) {
-                counts[j] += 1;
-                mark[j] = i;
-                j = parent[j];
-            }
-        }
-    }
-    // symbolic.rs:68-79: fundamental supernodes; a supernode's rows number counts[first]
-    // (symbolic.rs:133). entries and flops as symbolic.rs:162-182.
-    std::vector<int64_t> nchild(n, 0);
-    for (int64_t p : parent)
-        if (p != NOPE) nchild[p] += 1;
-    std::vector<int64_t> start{0};
-    for (int64_t j = 1; j < n; ++j)
-        if (!(parent[j - 1] == j && counts[j - 1] == counts[j] + 1 && nchild[j] == 1))
-            start.push_back(j);
-    start.push_back(n);
-    uint64_t ent = 0;
-    double fl = -0.0;  // the Rust float sums start from -0.0
-    for (size_t s = 0; s + 1 < start.size(); ++s) {
-        const uint64_t k = (uint64_t)(start[s + 1] - start[s]);
-        const uint64_t m = (uint64_t)counts[start[s]];
-        ent += k * m - k * (k - 1) / 2;
-        double f = -0.0;
-        for (uint64_t j = 0; j < k; ++j) {
-            const double r = (double)(m - j);
-            f += r * r;
-        }
-        fl += f;
-    }
-    *entries = ent;
-    *flops = fl;
-}
-
 void prolongation(const double* points, int64_t npoints, int64_t corners, const uint32_t* edges,
                   int64_t nedges, const int64_t* free, int64_t nfree, HostRect* pout,
                   std::vector<double>* xyz) {

@@ -57,13 +57,6 @@ HostCsr by_cells(const HostLevel& fine, const HostCells& cells, const HostLevel&
 // nodes not split.
 std::vector<int64_t> nested_dissection(const HostCsr& a, const double* xyz);
 
-// symbolic.rs:41-183: the entries (with the diagonal) and the floating point operations of the
-// Cholesky factor of P A P^T for the order `order`, from the elimination tree, its postorder,
-// the column counts and the fundamental supernodes; what the reference's Crossover::Flops reads
-// (solve.rs:108-118, 160-172).
-void factor_counts(const HostCsr& a, const std::vector<int64_t>& order, uint64_t* entries,
-                   double* flops);
-
 // pmultigrid.rs:104-151
 void prolongation(const double* points, int64_t npoints, int64_t corners, const uint32_t* edges,
                   int64_t nedges, const int64_t* free, int64_t nfree, HostRect* p,

@@ -27,6 +27,7 @@
 #include "assemble.cuh"
 #include "solver.cuh"
 #include "coarsen.cuh"
+#include "symbolic.hpp"
 #include "rust_format.hpp"
 
 namespace femgpu {
@@ -1468,7 +1469,8 @@ size_t Hierarchy<T>::bytes() const {
 
 size_t SolverImpl::bytes() const {
     return A64_.bytes() + op64_.bytes() + a_.ptr.bytes() + a_.idx.bytes() + a_.val.bytes() + H64_.bytes() +
-           H32_.bytes() + dense_inv_.bytes() + 7 * n_ * sizeof(double) + r32_.bytes();
+           H32_.bytes() + dense_inv_.bytes() + 7 * n_ * sizeof(double) + r32_.bytes() +
+           (sparse_ ? sparse_->bytes() : 0);
 }
 
 std::vector<int64_t> SolverImpl::level_sizes() const { return sizes_; }
@@ -1496,9 +1498,7 @@ std::string SolverImpl::describe() const {
                   direct_ ? "direct" : "multigrid",
                   opt_.precision == FEMGPU_MIXED ? "mixed" : "fp64", (long long)n_);
     out += buf;
-    if (crossover_note_)
-        out += "the crossover chose the sparse direct factor; above the dense solver's 16384 "
-               "unknowns, multigrid runs instead\n";
+    if (sparse_) out += sparse_->describe();
     if (direct_) return out;
     out += "outer fp64: " + describe_op(op64_) + "\n";
     auto levels = [&](const auto& H, const char* t) {
@@ -1543,6 +1543,16 @@ void SolverImpl::phase(const std::string& name, double seconds) {
             return;
         }
     setup_s_.emplace_back(name, seconds);
+}
+
+// The coordinates of each unknown (3 each): its grid point, or the given points.
+static std::vector<double> unknown_xyz(const femgpu_unknowns& u, int64_t n) {
+    std::vector<double> xyz((size_t)3 * n);
+    for (int64_t k = 0; k < n; ++k)
+        for (int d = 0; d < 3; ++d)
+            xyz[3 * k + d] = u.kind == FEMGPU_UNKNOWNS_GRID ? u.planes[d][u.points[3 * k + d]]
+                                                            : u.xyz[3 * k + d];
+    return xyz;
 }
 
 void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
@@ -1594,26 +1604,22 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         // Crossover::Flops (solve.rs:108-118, 160-172): the sparse factor's entries and flops
         // in the nested dissection order of the unknowns' points.
         PhaseTimer t{this, "symbolic analysis for the crossover (host)", s_};
-        std::vector<double> xyz((size_t)3 * a.n);
-        for (int64_t k = 0; k < a.n; ++k)
-            for (int d = 0; d < 3; ++d)
-                xyz[3 * k + d] = u.kind == FEMGPU_UNKNOWNS_GRID
-                                     ? u.planes[d][u.points[3 * k + d]]
-                                     : u.xyz[3 * k + d];
+        std::vector<double> xyz = unknown_xyz(u, a.n);
         uint64_t entries = 0;
         double flops = 0.0;
-        factor_counts(h, nested_dissection(h, xyz.data()), &entries, &flops);
+        factor_figures(h, nested_dissection(h, xyz.data()), &entries, &flops);
         direct = entries <= c.entries && (c.flat || flops <= c.flops * (double)a.n);
-        // The direct solver here is a dense factor of at most 16,384 unknowns; a larger system
-        // that the rule gives to the sparse factor runs multigrid instead.
-        if (direct && a.n > 16384) {
-            direct = false;
-            crossover_note_ = true;
-        }
     }
     direct_ = direct;
     if (direct) {
-        dense_direct(h);
+        // A small system takes the dense inverse; a larger one the sparse multifrontal factor in
+        // the reference's order.
+        if (a.n <= DENSE_DIRECT) {
+            dense_direct(h);
+        } else {
+            PhaseTimer t{this, "sparse factor (analysis on the host, fronts on the device)", s_};
+            sparse_direct(h, unknown_xyz(u, a.n));
+        }
         sizes_ = {n_};
         return;
     }
@@ -1642,6 +1648,11 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         HostLevel lv = level_of_points(u.coarse_xyz, p.cols, u.coarse_comp);
         build_multigrid(std::move(h), std::move(lv), &p, nullptr);
     }
+}
+
+void SolverImpl::sparse_direct(const HostCsr& h, const std::vector<double>& xyz) {
+    sparse_ = std::make_unique<SparseFactor>();
+    sparse_->factor(h, xyz.data(), s_);
 }
 
 void SolverImpl::dense_direct(const HostCsr& h) {
@@ -2218,7 +2229,9 @@ void SolverImpl::solve_host_zero(const double* h_b, double* h_x, const volatile 
 
 void SolverImpl::precondition(const double* d_r, double* d_z) {
     FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
-    if (direct_) {
+    if (direct_ && sparse_) {
+        sparse_->solve(d_r, d_z, s_);
+    } else if (direct_) {
         k_gemv<double, false><<<blocks_for(n_ * 32, TH), TH, 0, s_>>>(n_, n_, dense_inv_.p, d_r, d_z,
                                                                done_zero_.p);
     } else if (opt_.precision == FEMGPU_MIXED) {
@@ -2245,17 +2258,23 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
     femgpu_stats out{};
     launches_ = 0;
     if (direct_) {
-        launches_ = 8;
         // solve.rs:206-218: x = A^-1 b (with 1 step of refinement in FP64), then the true
         // residual.
-        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, b_.p,
-                                                                     x_.p, done_zero_.p);
+        auto apply = [&](const double* rhs, double* sol) {
+            if (sparse_) {
+                sparse_->solve(rhs, sol, s_);
+            } else {
+                k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(
+                    n, n, dense_inv_.p, rhs, sol, done_zero_.p);
+            }
+        };
+        launches_ = 8;
+        apply(b_.p, x_.p);
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
             SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p, nullptr, partial_.p);
         k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                    FinResidual0{sc_.p});
-        k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(n, n, dense_inv_.p, r_.p,
-                                                                     t_.p, done_zero_.p);
+        apply(r_.p, t_.p);
         k_add<<<blocks_for(n, TH), TH, 0, s_>>>(n, t_.p, x_.p);
         FG_CHECK_LAUNCH();
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
@@ -2416,7 +2435,9 @@ __global__ void k_fill(int64_t n, double* __restrict__ v, double value) {
 }
 
 std::string SolverImpl::breakdown() {
-    if (direct_) return "direct method: 1 dense product and 1 refinement step\n";
+    if (direct_)
+        return sparse_ ? "direct method: sparse triangular solves and 1 refinement step\n"
+                       : "direct method: 1 dense product and 1 refinement step\n";
     // Defined inputs: b = 1, x = 0, p = 1; no stopping test (tol < 0), so every kernel runs.
     k_fill<<<blocks_for(n_, TH), TH, 0, s_>>>(n_, b_.p, 1.0);
     k_fill<<<blocks_for(n_, TH), TH, 0, s_>>>(n_, x_.p, 0.0);

@@ -11,6 +11,7 @@
 #include "hierarchy.hpp"
 #include "ops.cuh"
 #include "sell.cuh"
+#include "sparse_direct.cuh"
 
 namespace femgpu {
 
@@ -198,6 +199,9 @@ struct Hierarchy {
 // on the device, and on the 128^3 heat cube the level of 4,913 rows taken whole saves 2 coarser
 // levels' kernels and 1 PCG iteration (9 instead of 10, 3.28 instead of 3.50 ms).
 constexpr int DEVICE_COARSEST = 5000;
+// The direct method's dense inverse takes systems of up to this many unknowns; larger ones the
+// sparse multifrontal factor.
+constexpr int64_t DENSE_DIRECT = 4096;
 
 struct Options {
     int precision = FEMGPU_FP64;
@@ -253,7 +257,6 @@ class SolverImpl {
     void phase(const std::string& name, double seconds);
 
    private:
-    bool crossover_note_ = false;  // the Flops rule chose a direct solve too large for it
     void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
                          const HostCells* cells);
     template <class T>
@@ -270,6 +273,7 @@ class SolverImpl {
     void run_device_loop(const volatile int* cancel);
     void run_init(const double* d_b);
     void dense_direct(const HostCsr& a);
+    void sparse_direct(const HostCsr& a, const std::vector<double>& xyz);
 
     cudaStream_t s_ = nullptr;
     Options opt_;
@@ -281,6 +285,7 @@ class SolverImpl {
     Hierarchy<double> H64_;
     Hierarchy<float> H32_;
     DevBuf<double> dense_inv_;  // the direct method: A^-1
+    std::unique_ptr<SparseFactor> sparse_;  // the direct method above DENSE_DIRECT unknowns
     DevBuf<double> x_, r_, p_, q_, b_, z64_, t_;
     DevBuf<float> r32_;
     const double* zd_ = nullptr;  // where the V-cycle leaves z (FP64 form)

@@ -1,0 +1,528 @@
+// The multifrontal sparse Cholesky factor on the device (sparse_direct.cuh).
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdio>
+
+#include "rust_format.hpp"
+#include "sparse_direct.cuh"
+
+namespace femgpu {
+namespace {
+
+constexpr double PIVOT = 1e-10;     // cholesky.rs:22
+constexpr int SMALL_ROWS = 128;     // fronts factored in shared memory by 1 block
+constexpr int PANEL = 32;           // panel width of a large front
+constexpr int TILE = 64;            // trailing-update tile of a large front
+constexpr int CHUNK = 4096;         // entries of an update matrix per extend-add block
+constexpr int TH = 256;
+
+// The front of supernode s: m x m, column-major.
+struct Fronts {
+    const int64_t* first;
+    const int64_t* rows_ptr;
+    const uint32_t* rows;
+    const int64_t* foff;
+    double* f;
+};
+
+__device__ __forceinline__ int64_t lower_bound(const uint32_t* r, int64_t m, uint32_t v) {
+    int64_t lo = 0, hi = m;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (r[mid] < v)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// The entries of A in the lower part of each front (cholesky.rs:60-72), 1 thread per column,
+// and each column's diagonal of A.
+__global__ void k_assemble_fronts(int64_t n, const int64_t* __restrict__ perm,
+                                  const int64_t* __restrict__ iperm,
+                                  const int64_t* __restrict__ aptr,
+                                  const uint32_t* __restrict__ aidx,
+                                  const double* __restrict__ aval,
+                                  const int32_t* __restrict__ col2sn, Fronts fr,
+                                  double* __restrict__ diag0) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int s = col2sn[j];
+        const int64_t r0 = fr.rows_ptr[s], m = fr.rows_ptr[s + 1] - r0;
+        const uint32_t* R = fr.rows + r0;
+        double* F = fr.f + fr.foff[s] + (j - fr.first[s]) * m;
+        const int64_t old = perm[j];
+        double d = 0.0;
+        for (int64_t e = aptr[old]; e < aptr[old + 1]; ++e) {
+            const int64_t i = iperm[aidx[e]];
+            if (i == j) d = aval[e];
+            if (i >= j) F[lower_bound(R, m, (uint32_t)i)] += aval[e];
+        }
+        diag0[j] = d;
+    }
+}
+
+// Extend-add (cholesky.rs:74-86): chunk (child c, part q) adds the lower triangle of a part of
+// c's update matrix into its parent's front at the parent's rows.
+__global__ void k_extend_add(const int2* __restrict__ chunk, Fronts fr,
+                             const int64_t* __restrict__ parent,
+                             const uint32_t* __restrict__ relind,
+                             const int64_t* __restrict__ relind_off) {
+    const int c = chunk[blockIdx.x].x;
+    const int64_t q = chunk[blockIdx.x].y;
+    const int64_t mc = fr.rows_ptr[c + 1] - fr.rows_ptr[c];
+    const int64_t kc = fr.first[c + 1] - fr.first[c];
+    const int64_t mu = mc - kc;
+    const int64_t p = parent[c];
+    const int64_t mp = fr.rows_ptr[p + 1] - fr.rows_ptr[p];
+    const double* U = fr.f + fr.foff[c] + kc * mc + kc;
+    double* F = fr.f + fr.foff[p];
+    const uint32_t* rel = relind + relind_off[c];
+    const int64_t end = min(mu * mu, (q + 1) * (int64_t)CHUNK);
+    for (int64_t t = q * CHUNK + threadIdx.x; t < end; t += blockDim.x) {
+        const int64_t col = t / mu, row = t % mu;
+        if (row < col) continue;
+        F[rel[row] + (int64_t)rel[col] * mp] += U[row + col * mc];
+    }
+}
+
+// Partial Cholesky of the first k columns of a front in shared memory (cholesky.rs:173-225):
+// each pivot checked against PIVOT times its column's diagonal of A, its column scaled, and the
+// rest of the lower triangle updated (right-looking); 1 block per front of at most SMALL_ROWS.
+__global__ void __launch_bounds__(TH)
+    k_front_small(const int64_t* __restrict__ list, Fronts fr,
+                  const double* __restrict__ diag0, unsigned long long* __restrict__ status) {
+    extern __shared__ double S[];
+    __shared__ int stop;
+    const int64_t s = list[blockIdx.x];
+    const int64_t j0 = fr.first[s];
+    const int m = (int)(fr.rows_ptr[s + 1] - fr.rows_ptr[s]);
+    const int k = (int)(fr.first[s + 1] - j0);
+    double* F = fr.f + fr.foff[s];
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) S[t] = F[t];
+    if (threadIdx.x == 0) stop = 0;
+    __syncthreads();
+    for (int j = 0; j < k; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = S[j + j * m];
+            if (!(d > PIVOT * fabs(diag0[j0 + j]))) {
+                atomicMin(status, (unsigned long long)(j0 + j));
+                stop = 1;
+            } else {
+                S[j + j * m] = sqrt(d);
+            }
+        }
+        __syncthreads();
+        if (stop) break;
+        const double inv = 1.0 / S[j + j * m];
+        for (int r = j + 1 + threadIdx.x; r < m; r += blockDim.x) S[r + j * m] *= inv;
+        __syncthreads();
+        // The lower triangle of the trailing block, column by column.
+        const int w = m - j - 1;
+        for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
+            const int c = j + 1 + t / w, r = j + 1 + t % w;
+            if (r >= c) S[r + c * m] -= S[r + j * m] * S[c + j * m];
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) F[t] = S[t];
+}
+
+// A large front, panel [p0, p0 + kb): the diagonal block factored in shared memory, then the
+// panel's rows below solved against it (L21 = A21 L11^-T), 1 block.
+__global__ void __launch_bounds__(TH)
+    k_front_panel(double* __restrict__ F, int64_t m, int64_t p0, int kb,
+                  const double* __restrict__ diag0, int64_t col0,
+                  unsigned long long* __restrict__ status) {
+    __shared__ double D[PANEL][PANEL + 1];
+    __shared__ int stop;
+    for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
+        const int i = t % PANEL, j = t / PANEL;
+        D[i][j] = (i < kb && j < kb) ? F[(p0 + i) + (p0 + j) * m] : 0.0;
+    }
+    if (threadIdx.x == 0) stop = 0;
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = D[j][j];
+            if (!(d > PIVOT * fabs(diag0[p0 + j]))) {
+                atomicMin(status, (unsigned long long)(col0 + p0 + j));
+                stop = 1;
+            } else {
+                D[j][j] = sqrt(d);
+            }
+        }
+        __syncthreads();
+        if (stop) return;
+        if (threadIdx.x > j && threadIdx.x < kb) D[threadIdx.x][j] /= D[j][j];
+        __syncthreads();
+        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+            const int i = t % kb, c = t / kb;
+            if (c > j && i >= c) D[i][c] -= D[i][j] * D[c][j];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int i = t % kb, j = t / kb;
+        if (i >= j) F[(p0 + i) + (p0 + j) * m] = D[i][j];
+    }
+    for (int64_t r = p0 + kb + threadIdx.x; r < m; r += blockDim.x) {
+        double x[PANEL];
+        for (int j = 0; j < kb; ++j) {
+            double v = F[r + (p0 + j) * m];
+            for (int q = 0; q < j; ++q) v -= x[q] * D[j][q];
+            x[j] = v / D[j][j];
+            F[r + (p0 + j) * m] = x[j];
+        }
+    }
+}
+
+// D = A B + D on the FP64 tensor cores: A 8 x 4 (row), B 4 x 8 (column), D 8 x 8; lane l holds
+// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// The trailing update F[t0:m, t0:m] -= L21 L21^T (lower triangle) with L21 = F[t0:m, p0:p0+kb],
+// kb <= 32: 1 block per 64 x 64 tile on or below the diagonal; warp w computes rows 8w..8w+7 of
+// the tile with 8 x 8 tensor-core products over k in steps of 4.
+__global__ void __launch_bounds__(TH)
+    k_front_update(double* __restrict__ F, int64_t m, int64_t t0, int64_t p0, int kb) {
+    __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
+    const int64_t b = blockIdx.x;
+    int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
+    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+    while (bi * (bi + 1) / 2 > b) --bi;
+    const int64_t bj = b - bi * (bi + 1) / 2;
+    const int64_t r0 = t0 + bi * TILE, c0 = t0 + bj * TILE;
+    for (int t = threadIdx.x; t < TILE * PANEL; t += blockDim.x) {
+        const int r = t % TILE, k = t / TILE;
+        As[r][k] = (r0 + r < m && k < kb) ? F[(r0 + r) + (p0 + k) * m] : 0.0;
+        Bs[r][k] = (c0 + r < m && k < kb) ? F[(c0 + r) + (p0 + k) * m] : 0.0;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    double acc[8][2];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < PANEL; kk += 4) {
+        const double a = As[warp * 8 + g][kk + q];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) dmma(acc[nt][0], acc[nt][1], a, Bs[nt * 8 + g][kk + q]);
+    }
+    const int64_t r = r0 + warp * 8 + g;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int64_t c = c0 + nt * 8 + 2 * q + i;
+            if (r < m && c < m && r >= c) F[r + c * m] -= acc[nt][i];
+        }
+}
+
+__global__ void k_permute_in(int64_t n, const int64_t* __restrict__ perm,
+                             const double* __restrict__ b, double* __restrict__ y) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        y[j] = b[perm[j]];
+}
+
+__global__ void k_permute_out(int64_t n, const int64_t* __restrict__ perm,
+                              const double* __restrict__ y, double* __restrict__ x) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        x[perm[j]] = y[j];
+}
+
+// Forward solve of supernode s (1 block): z = its part of y and its children's updates (added
+// child by child in increasing order), then L11 z1 = z1 and z2 -= L21 z1; z1 goes to y, z2 is
+// the update for the parent.
+__global__ void __launch_bounds__(TH)
+    k_forward(const int64_t* __restrict__ list, Fronts fr, const int64_t* __restrict__ zoff,
+              const int64_t* __restrict__ child_ptr, const int64_t* __restrict__ child,
+              const uint32_t* __restrict__ relind, const int64_t* __restrict__ relind_off,
+              double* __restrict__ work, double* __restrict__ y) {
+    __shared__ double v;
+    const int64_t s = list[blockIdx.x];
+    const int64_t j0 = fr.first[s];
+    const int64_t m = fr.rows_ptr[s + 1] - fr.rows_ptr[s], k = fr.first[s + 1] - j0;
+    const double* F = fr.f + fr.foff[s];
+    double* z = work + zoff[s];
+    for (int64_t t = threadIdx.x; t < m; t += blockDim.x) z[t] = t < k ? y[j0 + t] : 0.0;
+    __syncthreads();
+    for (int64_t ci = child_ptr[s]; ci < child_ptr[s + 1]; ++ci) {
+        const int64_t c = child[ci];
+        const int64_t kc = fr.first[c + 1] - fr.first[c];
+        const int64_t mu = fr.rows_ptr[c + 1] - fr.rows_ptr[c] - kc;
+        const double* zc = work + zoff[c] + kc;
+        const uint32_t* rel = relind + relind_off[c];
+        for (int64_t t = threadIdx.x; t < mu; t += blockDim.x) z[rel[t]] += zc[t];
+        __syncthreads();
+    }
+    for (int64_t j = 0; j < k; ++j) {
+        if (threadIdx.x == 0) {
+            v = z[j] / F[j + j * m];
+            z[j] = v;
+        }
+        __syncthreads();
+        const double vj = v;
+        for (int64_t r = j + 1 + threadIdx.x; r < m; r += blockDim.x) z[r] -= F[r + j * m] * vj;
+        __syncthreads();
+    }
+    for (int64_t t = threadIdx.x; t < k; t += blockDim.x) y[j0 + t] = z[t];
+}
+
+// Backward solve of supernode s (1 block), its ancestors done: t_j = y_j - sum over the rows
+// below of L[r][j] x_r (a warp per column), then L11^T x1 = t.
+__global__ void __launch_bounds__(TH)
+    k_backward(const int64_t* __restrict__ list, Fronts fr, const int64_t* __restrict__ zoff,
+               double* __restrict__ work, double* __restrict__ y) {
+    __shared__ double v;
+    const int64_t s = list[blockIdx.x];
+    const int64_t j0 = fr.first[s];
+    const int64_t r0 = fr.rows_ptr[s];
+    const int64_t m = fr.rows_ptr[s + 1] - r0, k = fr.first[s + 1] - j0;
+    const uint32_t* R = fr.rows + r0;
+    const double* F = fr.f + fr.foff[s];
+    double* z = work + zoff[s];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int64_t j = warp; j < k; j += nw) {
+        double acc = 0.0;
+        for (int64_t r = k + lane; r < m; r += 32) acc += F[r + j * m] * y[R[r]];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) z[j] = y[j0 + j] - acc;
+    }
+    __syncthreads();
+    for (int64_t j = k - 1; j >= 0; --j) {
+        if (threadIdx.x == 0) {
+            v = z[j] / F[j + j * m];
+            z[j] = v;
+        }
+        __syncthreads();
+        const double vj = v;
+        for (int64_t i = threadIdx.x; i < j; i += blockDim.x) z[i] -= F[j + i * m] * vj;
+        __syncthreads();
+    }
+    for (int64_t t = threadIdx.x; t < k; t += blockDim.x) y[j0 + t] = z[t];
+}
+
+}  // namespace
+
+void SparseFactor::factor(const HostCsr& a, const double* xyz, cudaStream_t s) {
+    n_ = a.n;
+    // The reference's fill-reducing order (order.rs) and the analysis in it.
+    Supernodal S = analyse_factor(a, nested_dissection(a, xyz));
+    ns_ = S.ns;
+    entries_ = S.entries;
+    flops_ = S.flops;
+    host_first_ = S.first;
+    m_.resize(ns_);
+    k_.resize(ns_);
+    std::vector<int64_t> foff(ns_), zoff(ns_);
+    size_t fv = 0, zv = 0;
+    for (int64_t t = 0; t < ns_; ++t) {
+        m_[t] = S.rows_ptr[t + 1] - S.rows_ptr[t];
+        k_[t] = S.first[t + 1] - S.first[t];
+        foff[t] = (int64_t)fv;
+        zoff[t] = (int64_t)zv;
+        fv += (size_t)(m_[t] * m_[t]);
+        zv += (size_t)m_[t];
+    }
+    front_values_ = fv;
+    if (fv > ((size_t)96 << 30) / 8)
+        throw Failure(FEMGPU_ERR_TOO_LARGE,
+                      "the frontal matrices of the sparse factor need more than 96 GiB");
+    // Children (increasing), relative indices of each child's update rows in its parent.
+    std::vector<int64_t> cptr(ns_ + 1, 0), clist;
+    for (int64_t t = 0; t < ns_; ++t)
+        if (S.parent[t] >= 0) cptr[S.parent[t] + 1] += 1;
+    for (int64_t t = 0; t < ns_; ++t) cptr[t + 1] += cptr[t];
+    clist.resize(cptr[ns_]);
+    std::vector<int64_t> fill(cptr.begin(), cptr.end() - 1);
+    std::vector<int> rank(ns_, 0);
+    for (int64_t t = 0; t < ns_; ++t)
+        if (S.parent[t] >= 0) {
+            rank[t] = (int)(fill[S.parent[t]] - cptr[S.parent[t]]);
+            clist[fill[S.parent[t]]++] = t;
+        }
+    std::vector<int64_t> roff(ns_, 0);
+    std::vector<uint32_t> rel;
+    for (int64_t c = 0; c < ns_; ++c) {
+        roff[c] = (int64_t)rel.size();
+        const int64_t p = S.parent[c];
+        if (p < 0) continue;
+        const uint32_t* Rp = S.rows.data() + S.rows_ptr[p];
+        for (int64_t t = S.rows_ptr[c] + k_[c]; t < S.rows_ptr[c + 1]; ++t)
+            rel.push_back((uint32_t)(std::lower_bound(Rp, Rp + m_[p], S.rows[t]) - Rp));
+    }
+    // The level schedule.
+    height_ = 0;
+    for (int h : S.height) height_ = std::max<int64_t>(height_, h);
+    small_.assign(height_ + 1, {});
+    large_.assign(height_ + 1, {});
+    std::vector<std::vector<int64_t>> all(height_ + 1);
+    for (int64_t t = 0; t < ns_; ++t) {
+        (m_[t] <= SMALL_ROWS ? small_ : large_)[S.height[t]].push_back(t);
+        all[S.height[t]].push_back(t);
+    }
+    std::vector<int64_t> sl, ll;
+    small_at_.assign(1, 0);
+    level_at_.assign(1, 0);
+    for (int64_t h = 0; h <= height_; ++h) {
+        sl.insert(sl.end(), small_[h].begin(), small_[h].end());
+        small_at_.push_back((int64_t)sl.size());
+        ll.insert(ll.end(), all[h].begin(), all[h].end());
+        level_at_.push_back((int64_t)ll.size());
+    }
+    // Extend-add chunks per (height of the parent, rank of the child).
+    std::vector<int2> ch;
+    chunks_.clear();
+    for (int64_t h = 1; h <= height_; ++h) {
+        int maxrank = -1;
+        for (int64_t p : all[h]) maxrank = std::max<int>(maxrank, (int)(cptr[p + 1] - cptr[p]) - 1);
+        for (int r = 0; r <= maxrank; ++r) {
+            Chunks c{(int)h, r, (int64_t)ch.size(), 0};
+            for (int64_t p : all[h]) {
+                if (cptr[p + 1] - cptr[p] <= r) continue;
+                const int64_t cc = clist[cptr[p] + r];
+                const int64_t mu = m_[cc] - k_[cc];
+                const int64_t parts = (mu * mu + CHUNK - 1) / CHUNK;
+                for (int64_t q = 0; q < parts; ++q) ch.push_back(int2{(int)cc, (int)q});
+            }
+            c.count = (int64_t)ch.size() - c.at;
+            if (c.count) chunks_.push_back(c);
+        }
+    }
+    if (ns_ >= INT_MAX) throw Failure(FEMGPU_ERR_TOO_LARGE, "too many supernodes");
+    // Device arrays.
+    std::vector<int32_t> col2sn(n_);
+    for (int64_t t = 0; t < ns_; ++t)
+        for (int64_t j = S.first[t]; j < S.first[t + 1]; ++j) col2sn[j] = (int32_t)t;
+    perm_.upload(S.perm.data(), n_, s);
+    DevBuf<int64_t> iperm;
+    iperm.upload(S.iperm.data(), n_, s);
+    first_.upload(S.first.data(), ns_ + 1, s);
+    rows_ptr_.upload(S.rows_ptr.data(), ns_ + 1, s);
+    rows_.upload(S.rows.data(), S.rows.size(), s);
+    foff_.upload(foff.data(), ns_, s);
+    zoff_.upload(zoff.data(), ns_, s);
+    child_ptr_.upload(cptr.data(), ns_ + 1, s);
+    child_.upload(clist.data(), std::max<size_t>(1, clist.size()), s);
+    relind_.upload(rel.data(), std::max<size_t>(1, rel.size()), s);
+    relind_off_.upload(roff.data(), ns_, s);
+    small_list_.upload(sl.data(), std::max<size_t>(1, sl.size()), s);
+    level_list_.upload(ll.data(), std::max<size_t>(1, ll.size()), s);
+    chunk_.upload(ch.data(), std::max<size_t>(1, ch.size()), s);
+    DevBuf<int64_t> parent;
+    parent.upload(S.parent.data(), ns_, s);
+    DevBuf<int32_t> dcol2sn;
+    dcol2sn.upload(col2sn.data(), n_, s);
+    fronts_.alloc(fv);
+    FG_CUDA(cudaMemsetAsync(fronts_.p, 0, fv * sizeof(double), s));
+    work_.alloc(std::max<size_t>(1, zv));
+    y_.alloc(n_);
+    DevBuf<int64_t> aptr;
+    DevBuf<uint32_t> aidx;
+    DevBuf<double> aval, diag0(n_);
+    aptr.upload(a.ptr.data(), n_ + 1, s);
+    aidx.upload(a.idx.data(), a.nnz(), s);
+    aval.upload(a.val.data(), a.nnz(), s);
+    DevBuf<unsigned long long> status(1);
+    FG_CUDA(cudaMemsetAsync(status.p, 0xff, sizeof(unsigned long long), s));
+    const Fronts fr{first_.p, rows_ptr_.p, rows_.p, foff_.p, fronts_.p};
+    k_assemble_fronts<<<blocks_for(n_, TH), TH, 0, s>>>(n_, perm_.p, iperm.p, aptr.p, aidx.p,
+                                                       aval.p, dcol2sn.p, fr, diag0.p);
+    FG_CHECK_LAUNCH();
+    const size_t smem = (size_t)SMALL_ROWS * SMALL_ROWS * sizeof(double);
+    FG_CUDA(cudaFuncSetAttribute(k_front_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    size_t ci = 0;
+    for (int64_t h = 0; h <= height_; ++h) {
+        for (; ci < chunks_.size() && chunks_[ci].height == h; ++ci)
+            k_extend_add<<<(unsigned)chunks_[ci].count, TH, 0, s>>>(
+                chunk_.p + chunks_[ci].at, fr, parent.p, relind_.p, relind_off_.p);
+        const int64_t ns_small = small_at_[h + 1] - small_at_[h];
+        if (ns_small > 0) {
+            int mmax = 0;
+            for (int64_t t : small_[h]) mmax = std::max<int>(mmax, (int)m_[t]);
+            k_front_small<<<(unsigned)ns_small, TH, (size_t)mmax * mmax * sizeof(double), s>>>(
+                small_list_.p + small_at_[h], fr, diag0.p, status.p);
+        }
+        for (int64_t t : large_[h]) {
+            const int64_t m = m_[t], k = k_[t];
+            double* F = fronts_.p + foff[t];
+            for (int64_t p0 = 0; p0 < k; p0 += PANEL) {
+                const int kb = (int)std::min<int64_t>(PANEL, k - p0);
+                k_front_panel<<<1, TH, 0, s>>>(F, m, p0, kb, diag0.p + S.first[t], S.first[t],
+                                               status.p);
+                const int64_t t0 = p0 + kb;
+                if (t0 < m) {
+                    const int64_t T = (m - t0 + TILE - 1) / TILE;
+                    k_front_update<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(F, m, t0, p0, kb);
+                }
+            }
+        }
+        FG_CHECK_LAUNCH();
+    }
+    unsigned long long bad = fetch(status.p, s);
+    if (bad != ~0ull) {
+        const int64_t j = (int64_t)bad;
+        const double d = fetch(diag0.p + j, s);
+        char buf[320];
+        std::snprintf(buf, sizeof buf,
+                      "the matrix is not positive definite: the pivot of column %lld is 0 or less "
+                      "to the precision of the arithmetic (its diagonal is %s)",
+                      (long long)S.perm[j], rust_exp_shortest(d).c_str());
+        throw Failure(FEMGPU_ERR_NOT_SPD, buf);
+    }
+    FG_CUDA(cudaStreamSynchronize(s));
+}
+
+void SparseFactor::solve(const double* b, double* x, cudaStream_t s) {
+    const Fronts fr{first_.p, rows_ptr_.p, rows_.p, foff_.p, fronts_.p};
+    k_permute_in<<<blocks_for(n_, TH), TH, 0, s>>>(n_, perm_.p, b, y_.p);
+    for (int64_t h = 0; h <= height_; ++h) {
+        const int64_t cnt = level_at_[h + 1] - level_at_[h];
+        if (cnt)
+            k_forward<<<(unsigned)cnt, TH, 0, s>>>(level_list_.p + level_at_[h], fr, zoff_.p,
+                                                   child_ptr_.p, child_.p, relind_.p,
+                                                   relind_off_.p, work_.p, y_.p);
+    }
+    for (int64_t h = height_; h >= 0; --h) {
+        const int64_t cnt = level_at_[h + 1] - level_at_[h];
+        if (cnt)
+            k_backward<<<(unsigned)cnt, TH, 0, s>>>(level_list_.p + level_at_[h], fr, zoff_.p,
+                                                    work_.p, y_.p);
+    }
+    k_permute_out<<<blocks_for(n_, TH), TH, 0, s>>>(n_, perm_.p, y_.p, x);
+    FG_CHECK_LAUNCH();
+}
+
+size_t SparseFactor::bytes() const {
+    return fronts_.bytes() + work_.bytes() + y_.bytes() + perm_.bytes() + first_.bytes() +
+           rows_ptr_.bytes() + rows_.bytes() + foff_.bytes() + zoff_.bytes() +
+           child_ptr_.bytes() + child_.bytes() + relind_.bytes() + relind_off_.bytes() +
+           small_list_.bytes() + level_list_.bytes() + chunk_.bytes();
+}
+
+std::string SparseFactor::describe() const {
+    char buf[256];
+    int64_t nl = 0, mmax = 0;
+    for (const auto& l : large_) nl += (int64_t)l.size();
+    for (int64_t m : m_) mmax = std::max(mmax, m);
+    std::snprintf(buf, sizeof buf,
+                  "sparse multifrontal factor: %lld supernodes, %lld levels, %lld fronts above %d "
+                  "rows (largest %lld), L entries %llu, flops %.3g, front values %zu\n",
+                  (long long)ns_, (long long)height_ + 1, (long long)nl, SMALL_ROWS,
+                  (long long)mmax, (unsigned long long)entries_, flops_, front_values_);
+    return buf;
+}
+
+}  // namespace femgpu
