@@ -42,6 +42,7 @@ UNITS = [
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),
+             ("order.cpp", ["-O3", "-std=c++17", "-fPIC", "-pthread"]),
              ("dense_eigen.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"])]
 
 

@@ -306,140 +306,6 @@ HostCsr by_cells(const HostLevel& fine, const HostCells& cells, const HostLevel&
     return a;
 }
 
-// ------------------------------------------------------------------ order.rs, symbolic.rs
-namespace {
-
-constexpr int64_t NOPE = -1;
-
-// order.rs:143-184: the size of the separator of the cut at `cut` on `axis` (the smaller side's
-// nodes that couple to the other side) and the size of the smaller side.
-std::pair<int64_t, int64_t> cut_cost(const HostCsr& a, const std::vector<int64_t>& set,
-                                     const double* xyz, std::vector<uint8_t>& side, int axis,
-                                     double cut) {
-    int64_t nleft = 0;
-    for (int64_t v : set) {
-        side[v] = xyz[3 * v + axis] < cut ? 1 : 2;
-        nleft += side[v] == 1;
-    }
-    int64_t sl = 0, sr = 0;
-    for (int64_t v : set) {
-        const uint8_t mine = side[v], other = 3 - mine;
-        bool touches = false;
-        for (int64_t k = a.ptr[v]; k < a.ptr[v + 1] && !touches; ++k)
-            touches = side[a.idx[k]] == other;
-        if (touches) (mine == 1 ? sl : sr) += 1;
-    }
-    for (int64_t v : set) side[v] = 0;
-    return {std::min(sl, sr), std::min(nleft, (int64_t)set.size() - nleft)};
-}
-
-// order.rs:66-141: left, right and separator, or false when all nodes are at 1 point.
-bool split_set(const HostCsr& a, const std::vector<int64_t>& set, const double* xyz,
-               std::vector<uint8_t>& side, std::vector<int64_t>* left,
-               std::vector<int64_t>* right, std::vector<int64_t>* sep) {
-    static const double CUTS[5] = {0.3, 0.4, 0.5, 0.6, 0.7};
-    double lo[3], hi[3];
-    for (int d = 0; d < 3; ++d) {
-        lo[d] = INFINITY;
-        hi[d] = -INFINITY;
-    }
-    for (int64_t v : set)
-        for (int d = 0; d < 3; ++d) {
-            lo[d] = std::fmin(lo[d], xyz[3 * v + d]);
-            hi[d] = std::fmax(hi[d], xyz[3 * v + d]);
-        }
-    bool have = false;
-    double best_cost = 0.0, best_cut = 0.0;
-    int best_axis = 0;
-    std::vector<double> values;
-    for (int axis = 0; axis < 3; ++axis) {
-        if (hi[axis] <= lo[axis]) continue;
-        values.clear();
-        for (int64_t v : set) values.push_back(xyz[3 * v + axis]);
-        std::sort(values.begin(), values.end());
-        for (double q : CUTS) {
-            const size_t at =
-                std::min((size_t)((double)values.size() * q), values.size() - 1);
-            double cut = values[at];
-            if (cut <= lo[axis]) {  // more than q of the nodes on the lowest plane: cut above it
-                auto it = std::find_if(values.begin(), values.end(),
-                                       [&](double x) { return x > lo[axis]; });
-                if (it == values.end()) continue;
-                cut = *it;
-            }
-            const auto sc = cut_cost(a, set, xyz, side, axis, cut);
-            const double cost =
-                (double)sc.first / std::sqrt(2.0 * (double)sc.second / (double)set.size());
-            if (!have || cost < best_cost) {
-                have = true;
-                best_cost = cost;
-                best_cut = cut;
-                best_axis = axis;
-            }
-        }
-    }
-    if (!have) return false;
-    left->clear();
-    right->clear();
-    for (int64_t v : set) (xyz[3 * v + best_axis] < best_cut ? left : right)->push_back(v);
-    for (int64_t v : *left) side[v] = 1;
-    for (int64_t v : *right) side[v] = 2;
-    auto touches = [&](int64_t v, uint8_t other) {
-        for (int64_t k = a.ptr[v]; k < a.ptr[v + 1]; ++k)
-            if (side[a.idx[k]] == other) return true;
-        return false;
-    };
-    std::vector<int64_t> sep_left, sep_right;
-    for (int64_t v : *left)
-        if (touches(v, 2)) sep_left.push_back(v);
-    for (int64_t v : *right)
-        if (touches(v, 1)) sep_right.push_back(v);
-    for (int64_t v : set) side[v] = 0;
-    const bool from_left = sep_left.size() <= sep_right.size();
-    *sep = from_left ? sep_left : sep_right;
-    std::vector<int64_t> in_sep(*sep);
-    std::sort(in_sep.begin(), in_sep.end());
-    std::vector<int64_t>* part = from_left ? left : right;
-    std::vector<int64_t> rest;
-    for (int64_t v : *part)
-        if (!std::binary_search(in_sep.begin(), in_sep.end(), v)) rest.push_back(v);
-    *part = std::move(rest);
-    return true;
-}
-
-}  // namespace
-
-std::vector<int64_t> nested_dissection(const HostCsr& a, const double* xyz) {
-    const int64_t n = a.n;
-    std::vector<int64_t> order;
-    order.reserve(n);
-    std::vector<uint8_t> side(n, 0);
-    struct Work {
-        bool emit;
-        std::vector<int64_t> set;
-    };
-    std::vector<Work> stack;
-    {
-        std::vector<int64_t> all(n);
-        for (int64_t i = 0; i < n; ++i) all[i] = i;
-        stack.push_back({false, std::move(all)});
-    }
-    std::vector<int64_t> left, right, sep;
-    while (!stack.empty()) {
-        Work w = std::move(stack.back());
-        stack.pop_back();
-        if (w.emit || w.set.size() <= 64 || !split_set(a, w.set, xyz, side, &left, &right, &sep)) {
-            order.insert(order.end(), w.set.begin(), w.set.end());
-            continue;
-        }
-        // The stack runs the last push first: left, then right, then the separator.
-        stack.push_back({true, sep});
-        stack.push_back({false, right});
-        stack.push_back({false, left});
-    }
-    return order;
-}
-
 void prolongation(const double* points, int64_t npoints, int64_t corners, const uint32_t* edges,
                   int64_t nedges, const int64_t* free, int64_t nfree, HostRect* pout,
                   std::vector<double>* xyz) {

@@ -51,10 +51,10 @@ struct HostCells {
 HostCsr by_cells(const HostLevel& fine, const HostCells& cells, const HostLevel& coarse,
                  HostCells* next, int threads);
 
-// order.rs:19-198: the nested dissection order of the symmetric pattern `a` from the coordinates
-// of each node (3 per node): item k is the old index of the new node k. Coordinate bisection at
-// the best of 5 quantile cuts per axis, the separator from the smaller side, sets of at most 64
-// nodes not split.
+// order.rs:19-179: the nested dissection order of the symmetric pattern `a` from the coordinates
+// of each node (3 per node): item k is the old index of the new node k (order.cpp: coordinate
+// bisection at the best of 5 quantile cuts per axis, the separator from the side with fewer
+// coupled nodes, sets of at most 64 nodes not split; on all host threads).
 std::vector<int64_t> nested_dissection(const HostCsr& a, const double* xyz);
 
 // pmultigrid.rs:104-151
