@@ -39,11 +39,12 @@ UNITS = [
     ("reactions.cu", ["-fmad=false"]),
     ("coarsen.cu", []),
     ("sparse_direct.cu", []),
+    ("dense_eigen.cu", []),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),
              ("order.cpp", ["-O3", "-std=c++17", "-fPIC", "-pthread"]),
-             ("dense_eigen.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"])]
+]
 
 
 def _nvcc():

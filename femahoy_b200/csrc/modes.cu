@@ -3,8 +3,8 @@
 // calls it. K - shift M is formed once on the device and handed to this library's solver (the
 // dense factor or PCG with multigrid), which stays resident for all the solves. The p subspace
 // vectors, their images under M and under (K - shift M)^-1 M, and the projections all stay on
-// the device; only the p x p projected matrices come back, for the dense Rayleigh-Ritz step on
-// the host (dense_eigen.cpp), and the p x p rotation goes back down.
+// the device; only the p x p projected matrices come back for the convergence test, and go down
+// again to the dense Rayleigh-Ritz step on the device (dense_eigen.cu), whose rotation stays there.
 //
 // Built with -fmad=false: K - shift M and the rotation X = Q^T X_bar keep the reference's
 // separate roundings. The projections are sums over n in a fixed order that is not the
@@ -17,8 +17,12 @@
 
 #include "assemble.cuh"
 #include "common.cuh"
-#include "dense_eigen.hpp"
 #include "solver.cuh"
+
+namespace femgpu {
+void dense_generalized_device(const double* k, const double* m, int n, double* values,
+                              double* q, cudaStream_t s);
+}
 
 namespace femgpu {
 
@@ -167,10 +171,22 @@ extern "C" {
 int femgpu_dense_generalized(const double* k, const double* m, size_t n, double* values,
                              double* q) {
     return modes_guarded([&] {
-        need(k && m && values && q && n > 0 && n <= 4096, "invalid dense eigenproblem");
-        std::string err;
-        if (!dense_generalized(k, m, (int)n, values, q, &err))
-            throw Failure(FEMGPU_ERR_NOT_SPD, err);
+        need(k && m && values && q && n > 0 && n <= 1024, "invalid dense eigenproblem");
+        cudaStream_t s = nullptr;
+        FG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        try {
+            DevBuf<double> dk, dm, dv(n), dq(n * n);
+            dk.upload(k, n * n, s);
+            dm.upload(m, n * n, s);
+            dense_generalized_device(dk.p, dm.p, (int)n, dv.p, dq.p, s);
+            dv.download(values, n, s);
+            dq.download(q, n * n, s);
+            FG_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
     });
 }
 
@@ -307,8 +323,8 @@ static int modes_impl(const femgpu_csr* k, const femgpu_csr* m, size_t count, do
             gram.download(out->data(), (size_t)p * p, s);
             FG_CUDA(cudaStreamSynchronize(s));
         };
-        std::vector<double> mu, kr((size_t)p * p), mr((size_t)p * p), g1, g2, vals(p),
-            qh((size_t)p * p);
+        std::vector<double> mu, kr((size_t)p * p), mr((size_t)p * p), g1, g2, vals(p);
+        DevBuf<double> dkr((size_t)p * p), dmr((size_t)p * p), dvals(p);
         femgpu_modes_stats st{};
         st.shift = shift;
         for (int iteration = 1; iteration <= EIGEN_MAX_ITER; ++iteration) {
@@ -342,11 +358,13 @@ static int modes_impl(const femgpu_csr* k, const femgpu_csr* m, size_t count, do
                 const double ka = kr[i * p + i], mb = mr[i * p + i];
                 converged = std::sqrt(std::max(1.0 - ka * ka / mb, 0.0)) <= EIGEN_TOL;
             }
-            std::string err;
-            if (!dense_generalized(kr.data(), mr.data(), p, vals.data(), qh.data(), &err))
-                throw Failure(FEMGPU_ERR_NOT_SPD, err);
+            // The Rayleigh-Ritz problem on the device (dense_eigen.cu); its vectors stay there.
+            dkr.upload(kr.data(), (size_t)p * p, s);
+            dmr.upload(mr.data(), (size_t)p * p, s);
+            dense_generalized_device(dkr.p, dmr.p, p, dvals.p, q.p, s);
+            dvals.download(vals.data(), p, s);
+            FG_CUDA(cudaStreamSynchronize(s));
             mu = vals;
-            q.upload(qh.data(), (size_t)p * p, s);
             k_rotate<<<blocks_for((int64_t)p * n, MT), MT, 0, s>>>(p, n, q.p, B.p, X.p);
             FG_CHECK_LAUNCH();
             st.iterations = (size_t)iteration;

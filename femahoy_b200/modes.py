@@ -50,7 +50,8 @@ def modes(k, m, count, unknowns, method=None, crossover: Crossover | None = None
 
 
 def dense_generalized(k, m):
-    """eigen.rs:183-269 on the host (no device use): (values ascending, Q) with Q^T M Q = I."""
+    """eigen.rs:183-269 on the device (the parallel Jacobi method after the reference's scaled
+    Cholesky reduction): (values ascending, Q) with Q^T M Q = I."""
     k = L.arr(k, np.float64)
     m = L.arr(m, np.float64)
     n = k.shape[0]

@@ -489,8 +489,8 @@ void femgpu_transient_free(femgpu_transient* t);
  * iteration with Rayleigh-Ritz (eigen.rs:81-177) as modes.rs:180-216 runs it: K - shift M is
  * formed on the device and solved by this library's solver (the dense factor or PCG with
  * multigrid, resident for all the solves); the p = max(2 count, count + 8) subspace vectors and
- * their images stay on the device; the p x p Rayleigh-Ritz problem is solved on the host
- * (femgpu_dense_generalized). */
+ * their images stay on the device, and so does the p x p Rayleigh-Ritz problem
+ * (femgpu_dense_generalized's solver). */
 typedef struct femgpu_modes_stats {
     size_t iterations;      /* subspace iterations */
     size_t solves;          /* solves of (K - shift M) x = M y */
@@ -511,9 +511,6 @@ int femgpu_modes(const femgpu_csr* k, const femgpu_csr* m, size_t count, double 
                  const femgpu_unknowns* unknowns, int method, const femgpu_crossover* crossover,
                  const femgpu_options* options, const volatile int* cancel, double* values,
                  double* vectors, femgpu_modes_stats* stats);
-/* eigen.rs:183-269 on the host: K q = lambda M q for dense symmetric row-major n x n matrices,
- * M positive definite, n <= 4096; the eigenvalues ascending and the vectors as the columns of
- * q with Q^T M Q = I (the cyclic Jacobi method of eigen.rs:274-331 inside). No device use. */
 /* modes.rs:355-420 for the box grid: femgpu_modes with `cells` (their `mass` set), whose
  * solver of K - shift M takes its coarse matrices from the cells' K_e - shift M_e. */
 int femgpu_modes_cells(const femgpu_csr* k, const femgpu_csr* m, size_t count, double shift,
@@ -521,6 +518,11 @@ int femgpu_modes_cells(const femgpu_csr* k, const femgpu_csr* m, size_t count, d
                        const femgpu_crossover* crossover, const femgpu_options* options,
                        const femgpu_cells* cells, const volatile int* cancel, double* values,
                        double* vectors, femgpu_modes_stats* stats);
+/* The step of eigen.rs:183-269 on the device: K q = lambda M q for dense symmetric row-major
+ * n x n host matrices, M positive definite, n <= 1024; the eigenvalues ascending and the vectors
+ * as the columns of q with Q^T M Q = I. The scaled Cholesky reduction of the reference, then the
+ * parallel (round-robin) Jacobi method in place of its cyclic one: the reference's results to
+ * rounding, and its texts for an M that is not positive definite or has dependent columns. */
 int femgpu_dense_generalized(const double* k, const double* m, size_t n, double* values,
                              double* q);
 

@@ -110,17 +110,33 @@ def test_oracle_p2_mass_is_the_exact_integral_of_the_functions():
 # ------------------------------------------------------------------ the library
 
 
-def test_library_dense_generalized_equals_the_oracle_bit_for_bit():
-    """The library's host Rayleigh-Ritz solver is the reference's algorithm in the same order:
-    the same bits as the oracle on eigen.rs:365-402's matrices and on a random pair."""
+@pytest.mark.gpu
+def test_library_dense_generalized_matches_the_oracle():
+    """The library's Rayleigh-Ritz solver (on the device: the reference's scaled Cholesky
+    reduction, then the parallel Jacobi method) against the oracle's cyclic Jacobi (eigen.rs:183-331)
+    on eigen.rs:365-402's matrices, on random pairs up to the largest subspace (p = 128) and on a
+    pair with a repeated eigenvalue: the eigenvalues to 1e-12 of the largest, Q^T M Q = I and
+    K Q = M Q diag(values) to 1e-10, and each vector of a simple eigenvalue equal to the oracle's up
+    to its sign."""
     from femahoy_b200.modes import dense_generalized
     rng = np.random.default_rng(4)
-    a = rng.standard_normal((12, 12))
-    b = rng.standard_normal((12, 12))
-    for k, m in (generalized_case(), (a + a.T, b @ b.T + 12 * np.eye(12))):
+    cases = [generalized_case()]
+    for n in (12, 37, 128):
+        a = rng.standard_normal((n, n))
+        b = rng.standard_normal((n, n))
+        cases.append((a + a.T, b @ b.T + n * np.eye(n)))
+    cases.append((np.diag([1.0, 2.0, 2.0, 3.0, 5.0]), np.eye(5)))
+    for k, m in cases:
         v1, q1 = dense_generalized(k, m)
         v2, q2 = oracle.dense_generalized(k, m)
-        assert np.array_equal(v1, v2) and np.array_equal(q1, q2)
+        scale = np.abs(v2).max()
+        assert np.abs(v1 - v2).max() <= 1e-12 * scale
+        assert np.abs(q1.T @ m @ q1 - np.eye(len(v1))).max() <= 1e-10
+        assert np.abs(k @ q1 - (m @ q1) * v1).max() <= 1e-10 * scale
+        gap = np.minimum(np.abs(np.diff(v2, prepend=-np.inf)), np.abs(np.diff(v2, append=np.inf)))
+        for j in np.nonzero(gap > 1e-6 * scale)[0]:
+            sign = np.sign(q1[:, j] @ m @ q2[:, j])
+            assert np.abs(sign * q1[:, j] - q2[:, j]).max() <= 1e-8 * np.abs(q2[:, j]).max()
 
 
 def p2_model(dims=(8, 2, 2), lengths=(80.0, 10.0, 10.0)):
