@@ -187,6 +187,12 @@ SIGNATURES = {
     "femgpu_batch_bytes": (C.c_size_t, [C.c_void_p]),
     "femgpu_batch_stream": (C.c_void_p, [C.c_void_p]),
     "femgpu_batch_free": (None, [C.c_void_p]),
+    "femgpu_stream_new": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "femgpu_stream_submit": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_uint64)]),
+    "femgpu_stream_wait": (C.c_int, [C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p]),
+    "femgpu_stream_counts": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t),
+                                       C.POINTER(C.c_size_t)]),
+    "femgpu_stream_free": (None, [C.c_void_p]),
     "femgpu_modes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_double,
                                C.POINTER(Unknowns_t), C.c_int, C.POINTER(Crossover_t),
                                C.POINTER(Options_t), C.c_void_p, C.c_void_p, C.c_void_p,

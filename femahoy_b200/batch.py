@@ -144,3 +144,53 @@ def _stats(st):
     return BatchStats(st.max_iterations, st.mean_iterations, st.max_residual,
                       st.max_true_residual, st.seconds, st.launches, st.not_converged,
                       st.restarts)
+
+
+class StreamResult(C.Structure):
+    _fields_ = [("iterations", C.c_size_t), ("residual", C.c_double),
+                ("true_residual", C.c_double), ("status", C.c_int), ("latency_s", C.c_double)]
+
+
+class Stream:
+    """Continuous batching over a Batch (include/femgpu.h ``femgpu_stream_*``): ``submit(system,
+    b)`` queues 1 right side of 1 system and returns a ticket; the device loop admits it into a
+    free slot of its system while the other slots keep iterating; ``wait(ticket)`` returns
+    (x, StreamResult). The batch then serves only this stream."""
+
+    def __init__(self, batch: Batch):
+        h = C.c_void_p()
+        L.check(L.lib().femgpu_stream_new(batch._h, C.byref(h)))
+        self._h = h.value
+        self._batch = batch  # the stream uses the batch's operators
+
+    def rows(self, system):
+        return int(self._batch.offsets[system + 1] - self._batch.offsets[system])
+
+    def submit(self, system, b):
+        b = L.arr(b, np.float64).reshape(-1)
+        if 0 <= system < len(self._batch.offsets) - 1 and len(b) != self.rows(system):
+            raise L.FemError(L.INVALID, "the right side has the system's rows")
+        t = C.c_uint64()
+        L.check(L.lib().femgpu_stream_submit(self._h, system, L.ptr(b), C.byref(t)))
+        return (t.value, system)
+
+    def wait(self, ticket):
+        t, system = ticket
+        x = np.empty(self.rows(system))
+        res = StreamResult()
+        L.check(L.lib().femgpu_stream_wait(self._h, t, L.ptr(x), C.byref(res)))
+        return x, res
+
+    def counts(self):
+        loops, served = C.c_size_t(), C.c_size_t()
+        L.check(L.lib().femgpu_stream_counts(self._h, C.byref(loops), C.byref(served)))
+        return loops.value, served.value
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h:
+            L.lib().femgpu_stream_free(h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

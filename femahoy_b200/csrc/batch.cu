@@ -18,6 +18,11 @@
 // batch's order at the start of a solve and back at the end.
 #include <algorithm>
 #include <atomic>
+#include <memory>
+#include <unordered_map>
+#include <mutex>
+#include <deque>
+#include <condition_variable>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -304,6 +309,12 @@ __global__ void k_bpermute(int64_t n, const int* __restrict__ map, const double*
         out[t] = in[other];
 }
 
+// The phases of a streamed segment (continuous batching, femgpu_stream_*): a free slot; a right
+// side admitted this iteration (x = 0, r = b; the iteration's product and update leave them, the
+// cycle and the dots start the recurrence with p = z); running PCG; its true residual being formed
+// (q = A x, r = b - A x) once the recurrence has stopped; finished, its x waiting to be delivered.
+enum { PH_FREE = 0, PH_FRESH = 1, PH_RUN = 2, PH_VERIFY = 3, PH_DONE = 4 };
+
 // ------------------------------------------------------------------ PCG over segments
 // A block of the PCG kernels takes 1 chunk: rows [row0, row1) of member `sys`. Thread t takes
 // column t % R and rows row0 + t / R, row0 + t / R + BTH / R, ...
@@ -365,17 +376,21 @@ template <int R>
 __global__ void __launch_bounds__(BTH)
     k_bpcg_spmv(SellView<double> A, const Chunk* __restrict__ chunks, const double* __restrict__ p,
                 double* __restrict__ q, const int* __restrict__ done,
-                double* __restrict__ partial) {
+                double* __restrict__ partial, const int* __restrict__ phase,
+                const double* __restrict__ xv) {
     pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
+    const int seg = ch.sys * R + col;
+    // A streamed segment being verified takes q = A x (its true residual follows).
+    const double* __restrict__ v = (phase && phase[seg] == PH_VERIFY) ? xv : p;
     double pq = 0;
-    if (!done[ch.sys * R + col])
+    if (!done[seg])
         for (int row = ch.row0 + threadIdx.x / R; row < ch.row1; row += BTH / R) {
             const int64_t t = (int64_t)row * R + col;
-            double ap = sell_row_cols<double, R>(A, row, col, p);
+            double ap = sell_row_cols<double, R>(A, row, col, v);
             q[t] = ap;
-            pq += p[t] * ap;
+            pq += v[t] * ap;
         }
     chunk_partial<R>(pq, 0.0, partial);
 }
@@ -412,20 +427,23 @@ template <int R>
 __global__ void __launch_bounds__(BTH)
     k_bpcg_spmv3(BSell3View<double> A, const Chunk* __restrict__ chunks,
                  const double* __restrict__ p, double* __restrict__ q,
-                 const int* __restrict__ done, double* __restrict__ partial) {
+                 const int* __restrict__ done, double* __restrict__ partial,
+                 const int* __restrict__ phase, const double* __restrict__ xv) {
     pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
+    const int seg = ch.sys * R + col;
+    const double* __restrict__ v = (phase && phase[seg] == PH_VERIFY) ? xv : p;
     double pq = 0;
-    if (!done[ch.sys * R + col])
+    if (!done[seg])
         for (int br = ch.row0 / 3 + threadIdx.x / R; br < ch.row1 / 3; br += BTH / R) {
             double acc[3];
-            bsell3_rows<double, R>(A, br, col, p, acc);
+            bsell3_rows<double, R>(A, br, col, v, acc);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 const int64_t t = (3 * (int64_t)br + a) * R + col;
                 q[t] = acc[a];
-                pq += p[t] * acc[a];
+                pq += v[t] * acc[a];
             }
         }
     chunk_partial<R>(pq, 0.0, partial);
@@ -437,13 +455,23 @@ __global__ void __launch_bounds__(BTH)
     k_bpcg_update(const Chunk* __restrict__ chunks, double* __restrict__ x,
                   double* __restrict__ r, const double* __restrict__ p,
                   const double* __restrict__ q, float* __restrict__ r32, BatchScalars sc,
-                  double* __restrict__ partial) {
+                  double* __restrict__ partial, const int* __restrict__ phase,
+                  const double* __restrict__ b) {
     pdl_wait();
     const Chunk ch = chunks[blockIdx.x];
     const int col = threadIdx.x % R;
     const int seg = ch.sys * R + col;
     double rr = 0;
-    if (!sc.done[seg]) {
+    if (phase && phase[seg] == PH_VERIFY) {
+        // A streamed segment being verified: r = b - A x (q holds A x), x unchanged.
+        for (int row = ch.row0 + threadIdx.x / R; row < ch.row1; row += BTH / R) {
+            const int64_t t = (int64_t)row * R + col;
+            const double ri = b[t] - q[t];
+            r[t] = ri;
+            if (r32) r32[t] = (float)ri;
+            rr += ri * ri;
+        }
+    } else if (!sc.done[seg]) {
         const double alpha = sc.alpha[seg];
         for (int row = ch.row0 + threadIdx.x / R; row < ch.row1; row += BTH / R) {
             const int64_t t = (int64_t)row * R + col;
@@ -506,7 +534,14 @@ __global__ void k_bzero_empty(const Chunk* __restrict__ chunks, const double* __
 }
 
 enum FinishKind { FIN_START = 0, FIN_PQ = 1, FIN_UPDATE = 2, FIN_DOTS = 3, FIN_TRUTH = 4,
-                  FIN_RESTART = 5 };
+                  FIN_RESTART = 5, FIN_SPQ = 6, FIN_SUPDATE = 7, FIN_SDOTS = 8 };
+
+// The per-segment state of streaming (null in a plain batch solve).
+struct StreamState {
+    int* phase;
+    int* restarts;
+    int* fresh;  // 1: the next dots start the recurrence (beta = 0)
+};
 
 // 1 block per member: the sums of each of its R segments over the member's chunks (a fixed
 // tree), then the segment's scalars. FIN_START: the first residual (stop at once if
@@ -517,7 +552,8 @@ enum FinishKind { FIN_START = 0, FIN_PQ = 1, FIN_UPDATE = 2, FIN_DOTS = 3, FIN_T
 template <int R>
 __global__ void __launch_bounds__(BTH)
     k_bfinish(int kind, const int* __restrict__ cstart, const double* __restrict__ partial,
-              BatchScalars sc, double tol, int max_iter, int flexible, int init) {
+              BatchScalars sc, double tol, int max_iter, int flexible, int init,
+              StreamState ss, double true_tol) {
     pdl_wait();
     __shared__ double sa[BTH], sb[BTH];
     const int sys = blockIdx.x;
@@ -541,6 +577,76 @@ __global__ void __launch_bounds__(BTH)
     a = sa[threadIdx.x];
     b = sb[threadIdx.x];
     const int s = sys * R + col;
+    if (kind >= FIN_SPQ) {
+        // Streaming: each segment by its phase.
+        const int ph = ss.phase[s];
+        if (kind == FIN_SPQ) {
+            if (ph == PH_RUN) {
+                sc.pq[s] = a;
+                sc.alpha[s] = sc.rz[s] / a;
+            } else if (ph == PH_FRESH) {
+                sc.alpha[s] = 0.0;  // x and r stay 0 and b
+            }
+        } else if (kind == FIN_SUPDATE) {
+            if (ph == PH_FRESH) {
+                // r = b: the start of multigrid.rs:704-723 from x = 0.
+                sc.bb[s] = a;
+                sc.rr[s] = a;
+                sc.iters[s] = 0;
+                sc.status[s] = 0;
+                sc.truth[s] = 0.0;
+                ss.restarts[s] = 0;
+                if (a == 0.0) {
+                    ss.phase[s] = PH_DONE;  // b = 0 gives x = 0
+                    sc.done[s] = 1;
+                } else if (max_iter <= 0) {
+                    sc.status[s] = 1;
+                    ss.phase[s] = PH_VERIFY;
+                } else {
+                    ss.phase[s] = PH_RUN;
+                    ss.fresh[s] = 1;
+                }
+            } else if (ph == PH_RUN) {
+                sc.rr[s] = a;
+                sc.iters[s] += 1;
+                if (!(a == a)) {
+                    sc.status[s] = 2;
+                    ss.phase[s] = PH_DONE;
+                    sc.done[s] = 1;
+                } else if (sqrt(a) / sqrt(sc.bb[s]) <= tol) {
+                    ss.phase[s] = PH_VERIFY;
+                } else if (sc.iters[s] >= max_iter) {
+                    sc.status[s] = 1;
+                    ss.phase[s] = PH_VERIFY;
+                }
+            } else if (ph == PH_VERIFY) {
+                // The true residual; a mixed form's recurrence that drifted above tol runs
+                // again from x, at most 3 times (as the plain batch's FIN_RESTART).
+                sc.truth[s] = sqrt(a) / sqrt(sc.bb[s]);
+                if (flexible && sc.status[s] == 0 && sc.truth[s] > true_tol &&
+                    ss.restarts[s] < 3 && sc.iters[s] < max_iter) {
+                    ss.restarts[s] += 1;
+                    sc.rr[s] = a;
+                    ss.phase[s] = PH_RUN;
+                    ss.fresh[s] = 1;
+                } else {
+                    ss.phase[s] = PH_DONE;
+                    sc.done[s] = 1;
+                }
+            }
+        } else if (ph == PH_RUN) {  // FIN_SDOTS
+            if (ss.fresh[s]) {
+                sc.beta[s] = 0;
+                ss.fresh[s] = 0;
+            } else if (flexible) {
+                sc.beta[s] = -sc.alpha[s] * b / sc.rz[s];
+            } else {
+                sc.beta[s] = a / sc.rz[s];
+            }
+            sc.rz[s] = a;
+        }
+        return;
+    }
     switch (kind) {
         case FIN_START:
             sc.bb[s] = a;
@@ -614,6 +720,127 @@ __global__ void k_bloop_control(cudaGraphConditionalHandle h, const int* __restr
     }
 }
 
+// ------------------------------------------------------------------ continuous batching
+// The host side of a streamed segment lives in pinned, mapped host memory: the host writes a
+// request's right side into the segment's staging slot and then a new generation number into
+// req[s]; the device copies it in at the start of an iteration, and when the segment is done it
+// writes x into the segment's output slot, its figures into stat[s], and the generation into
+// served[s] (after a system-wide fence), which the host polls.
+struct StreamStat {
+    double residual, truth;
+    int iterations, status;
+};
+
+struct StreamHost {
+    const volatile unsigned long long* req;  // generation of the request in each slot
+    volatile unsigned long long* served;     // generation served
+    const double* in;                        // staging: member k, slot c at boff[k] R + c m_k
+    double* out;
+    StreamStat* stat;
+    const volatile int* stop;
+};
+
+// 1 thread per segment: a free slot with a new generation takes its request (phase FRESH).
+__global__ void k_sadmit(int nseg, StreamHost h, unsigned long long* __restrict__ seen,
+                         int* __restrict__ phase, int* __restrict__ done,
+                         int* __restrict__ admit) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+        int a = 0;
+        if (phase[s] == PH_FREE) {
+            const unsigned long long g = h.req[s];
+            if (g != seen[s]) {
+                seen[s] = g;
+                phase[s] = PH_FRESH;
+                done[s] = 0;
+                a = 1;
+            }
+        }
+        admit[s] = a;
+    }
+}
+
+// The admitted segments' vectors: b and r from the staging slot, x = p = q = 0.
+template <int R>
+__global__ void __launch_bounds__(BTH)
+    k_sadmit_copy(const Chunk* __restrict__ chunks, const int64_t* __restrict__ boff,
+                  const int* __restrict__ admit, StreamHost h, double* __restrict__ b,
+                  double* __restrict__ r, float* __restrict__ r32, double* __restrict__ x,
+                  double* __restrict__ p, double* __restrict__ q) {
+    const Chunk ch = chunks[blockIdx.x];
+    const int col = threadIdx.x % R;
+    if (!admit[ch.sys * R + col]) return;
+    __threadfence_system();
+    const int64_t b0 = boff[ch.sys], m = boff[ch.sys + 1] - b0;
+    const double* in = h.in + b0 * R + col * m;
+    for (int row = ch.row0 + threadIdx.x / R; row < ch.row1; row += BTH / R) {
+        const int64_t t = (int64_t)row * R + col;
+        const double v = in[row - b0];
+        b[t] = v;
+        r[t] = v;
+        if (r32) r32[t] = (float)v;
+        x[t] = 0.0;
+        p[t] = 0.0;
+        q[t] = 0.0;
+    }
+}
+
+// The finished segments' x to their output slots.
+template <int R>
+__global__ void __launch_bounds__(BTH)
+    k_sdeliver_copy(const Chunk* __restrict__ chunks, const int64_t* __restrict__ boff,
+                    const int* __restrict__ phase, StreamHost h, const double* __restrict__ x) {
+    const Chunk ch = chunks[blockIdx.x];
+    const int col = threadIdx.x % R;
+    if (phase[ch.sys * R + col] != PH_DONE) return;
+    const int64_t b0 = boff[ch.sys], m = boff[ch.sys + 1] - b0;
+    double* out = h.out + b0 * R + col * m;
+    for (int row = ch.row0 + threadIdx.x / R; row < ch.row1; row += BTH / R)
+        out[row - b0] = x[(int64_t)row * R + col];
+    __threadfence_system();
+}
+
+// Then their figures and generations, and the slots are free again.
+__global__ void k_sdeliver(int nseg, StreamHost h, const unsigned long long* __restrict__ seen,
+                           int* __restrict__ phase, BatchScalars sc) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nseg; s += gridDim.x * blockDim.x) {
+        if (phase[s] != PH_DONE) continue;
+        StreamStat st;
+        st.residual = sc.bb[s] > 0.0 ? sqrt(sc.rr[s]) / sqrt(sc.bb[s]) : 0.0;
+        st.truth = sc.bb[s] > 0.0 ? sc.truth[s] : 0.0;
+        st.iterations = sc.iters[s];
+        st.status = sc.status[s];
+        h.stat[s] = st;
+        __threadfence_system();
+        h.served[s] = seen[s];
+        phase[s] = PH_FREE;
+    }
+}
+
+// Continue while a segment is busy or a request waits for a free slot, unless stopped.
+__global__ void k_sloop_control(cudaGraphConditionalHandle hc, int nseg, StreamHost h,
+                                const unsigned long long* __restrict__ seen,
+                                const int* __restrict__ phase, int* __restrict__ loops,
+                                unsigned long long* __restrict__ served_iterations) {
+    __shared__ int busy;
+    if (threadIdx.x == 0) busy = 0;
+    __syncthreads();
+    int mine = 0;
+    for (int s = threadIdx.x; s < nseg; s += blockDim.x)
+        if (phase[s] != PH_FREE || h.req[s] != seen[s]) mine = 1;
+    if (mine) atomicOr(&busy, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *loops += 1;
+        cudaGraphSetConditional(hc, (busy && !*h.stop) ? 1u : 0u);
+    }
+    // The segments that this iteration served (running or being verified): the packing.
+    int active = 0;
+    for (int s = threadIdx.x; s < nseg; s += blockDim.x)
+        active += phase[s] == PH_RUN || phase[s] == PH_VERIFY;
+    for (int o = 16; o; o >>= 1) active += __shfl_xor_sync(0xffffffffu, active, o);
+    if ((threadIdx.x & 31) == 0 && active) atomicAdd(served_iterations, (unsigned long long)active);
+}
+
 // ------------------------------------------------------------------ the batch
 struct SystemHierarchy {
     std::vector<HostCsr> mats;
@@ -667,7 +894,48 @@ class BatchImpl {
     void kernel_time(int reps, double* ms, double* bytes);
     double tol = 1e-10;  // PCG_TOL, solve.rs:42
 
+    // Continuous batching (femgpu_stream_*). stream_open allocates the mapped queue and captures
+    // the streamed loop; stream_launch starts it on the batch's stream (it runs until no slot is
+    // busy and no request waits); stream_idle tells whether that launch has ended.
+    void stream_open();
+    void stream_launch();
+    bool stream_idle();
+    void stream_stop();
+    int slots() const { return R_; }
+    int members() const { return B_; }
+    int64_t member_rows(int member) const { return offsets_[member + 1] - offsets_[member]; }
+    // The segment of (caller's member, slot) and the offset of its staging slot.
+    int segment(int member, int slot) const { return position_[member] * R_ + slot; }
+    int64_t slot_offset(int member, int slot) const {
+        return boff_[position_[member]] * R_ + slot * member_rows(member);
+    }
+    volatile unsigned long long* h_req() { return h_req_; }
+    volatile unsigned long long* h_served() { return h_served_; }
+    double* h_in() { return h_in_; }
+    double* h_out() { return h_out_; }
+    const StreamStat* h_stat() { return h_stat_; }
+    size_t stream_loops();
+    size_t stream_served_iterations();
+    bool streaming() const;
+
    private:
+    template <int R>
+    void build_stream_graph();
+    DevBuf<int> phase_, restarts_seg_, fresh_, admit_;
+    DevBuf<unsigned long long> seen_, served_its_;
+    DevBuf<int64_t> boffd_;
+    std::vector<int64_t> boff_;   // the batch order's row offsets
+    std::vector<int> position_;   // caller's member -> batch position
+    unsigned long long *h_req_ = nullptr, *h_served_ = nullptr;
+    double *h_in_ = nullptr, *h_out_ = nullptr;
+    StreamStat* h_stat_ = nullptr;
+    int* h_stop_ = nullptr;
+    StreamHost dh_{};  // the device's view of the mapped arrays
+    cudaGraph_t sgraph_ = nullptr;
+    cudaGraphExec_t sexec_ = nullptr;
+    cudaGraphConditionalHandle scond_ = 0;
+    cudaEvent_t sev_ = nullptr;
+    bool slaunched_ = false;
     template <class T>
     void build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchLevel<T>>* levels);
     template <class T, int R>
@@ -675,9 +943,9 @@ class BatchImpl {
     template <int R>
     void finish(int kind, int init);
     template <int R>
-    void precondition_and_dots(int init);
+    void precondition_and_dots(int init, bool stream);
     template <int R>
-    void iteration();
+    void iteration(bool stream);
     template <int R>
     void run(const volatile int* cancel);
     template <int R>
@@ -791,9 +1059,16 @@ BatchImpl::BatchImpl() {
 }
 
 BatchImpl::~BatchImpl() {
+    if (h_stop_) *(volatile int*)h_stop_ = 1;
     if (s_) cudaStreamSynchronize(s_);
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
+    if (sexec_) cudaGraphExecDestroy(sexec_);
+    if (sgraph_) cudaGraphDestroy(sgraph_);
+    if (sev_) cudaEventDestroy(sev_);
+    for (void* h : {(void*)h_req_, (void*)h_served_, (void*)h_in_, (void*)h_out_, (void*)h_stat_,
+                    (void*)h_stop_})
+        if (h) cudaFreeHost(h);
     if (h_cancel_) cudaFreeHost(h_cancel_);
     if (ev0_) cudaEventDestroy(ev0_);
     if (ev1_) cudaEventDestroy(ev1_);
@@ -912,6 +1187,9 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
         for (int64_t i = 0; i < m; ++i) map[boff[k] + i] = (int)(offsets_[order_[k]] + i);
     }
     map_.upload(map.data(), map.size(), s_);
+    boff_ = boff;
+    position_.assign(B_, 0);
+    for (int k = 0; k < B_; ++k) position_[order_[k]] = k;
     // The exact finest operator (FP64) of the PCG loop and the true residual.
     {
         std::vector<const HostCsr*> parts;
@@ -1141,26 +1419,26 @@ void BatchImpl::finish(int kind, int init) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     const double target = (mixed && kind != FIN_RESTART) ? 0.98 * tol : tol;
     launch(true, k_bfinish<R>, B_, BTH, s_, kind, cstart_.p, partial_.p, scalars(), target,
-           max_iter_, (int)mixed, init);
+           max_iter_, (int)mixed, init, StreamState{phase_.p, restarts_seg_.p, fresh_.p}, tol);
     FG_CHECK_LAUNCH();
     launches_ += 1;
 }
 
 // z = M^-1 r, the sums r.z (and z.q), beta, p.
 template <int R>
-void BatchImpl::precondition_and_dots(int init) {
+void BatchImpl::precondition_and_dots(int init, bool stream) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     if (mixed) {
         const float* z = vcycle<float, R>(L32_, 0, r32_.p);
         launch(true, k_bpcg_dots<R, float>, nchunks_, BTH, s_, chunks(), r_.p, z, q_.p, 1, init,
                done_.p, partial_.p);
-        finish<R>(FIN_DOTS, init);
+        finish<R>(stream ? FIN_SDOTS : FIN_DOTS, init);
         launch(true, k_bpcg_p<R, float>, nchunks_, BTH, s_, chunks(), z, p_.p, scalars(), init);
     } else {
         const double* z = vcycle<double, R>(L64_, 0, r_.p);
         launch(true, k_bpcg_dots<R, double>, nchunks_, BTH, s_, chunks(), r_.p, z, q_.p, 0, init,
                done_.p, partial_.p);
-        finish<R>(FIN_DOTS, init);
+        finish<R>(stream ? FIN_SDOTS : FIN_DOTS, init);
         launch(true, k_bpcg_p<R, double>, nchunks_, BTH, s_, chunks(), z, p_.p, scalars(), init);
     }
     FG_CHECK_LAUNCH();
@@ -1169,21 +1447,24 @@ void BatchImpl::precondition_and_dots(int init) {
 
 // 1 PCG iteration of every running segment (multigrid.rs:739-750).
 template <int R>
-void BatchImpl::iteration() {
+void BatchImpl::iteration(bool stream) {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
+    const int* ph = stream ? phase_.p : nullptr;
+    const double* xv = x_.p;
+    const double* bv = b_.p;
     if (fine3_)
         launch(true, k_bpcg_spmv3<R>, nchunks_, BTH, s_, fine3(), chunks(), p_.p, q_.p, done_.p,
-               partial_.p);
+               partial_.p, ph, xv);
     else
         launch(true, k_bpcg_spmv<R>, nchunks_, BTH, s_, A64_.view(), chunks(), p_.p, q_.p,
-               done_.p, partial_.p);
-    finish<R>(FIN_PQ, 0);
+               done_.p, partial_.p, ph, xv);
+    finish<R>(stream ? FIN_SPQ : FIN_PQ, 0);
     launch(true, k_bpcg_update<R>, nchunks_, BTH, s_, chunks(), x_.p, r_.p, p_.p, q_.p,
-           mixed ? r32_.p : nullptr, scalars(), partial_.p);
-    finish<R>(FIN_UPDATE, 0);
+           mixed ? r32_.p : nullptr, scalars(), partial_.p, ph, bv);
+    finish<R>(stream ? FIN_SUPDATE : FIN_UPDATE, 0);
     FG_CHECK_LAUNCH();
     launches_ += 2;
-    precondition_and_dots<R>(0);
+    precondition_and_dots<R>(0, stream);
 }
 
 bool BatchImpl::any_running() {
@@ -1246,7 +1527,7 @@ void BatchImpl::run(const volatile int* cancel) {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         FG_CUDA(cudaStreamBeginCaptureToGraph(s_, body, nullptr, nullptr, 0,
                                               cudaStreamCaptureModeThreadLocal));
-        iteration<R>();
+        iteration<R>(false);
         k_bloop_control<<<1, BTH, 0, s_>>>(cond_, done_.p, B_ * R, d_cancel_, loops_.p);
         FG_CUDA(cudaStreamEndCapture(s_, &body));
         FG_CUDA(cudaGraphInstantiate(&exec_, graph_, 0));
@@ -1263,7 +1544,7 @@ void BatchImpl::run(const volatile int* cancel) {
     k_bzero_empty<R><<<nchunks_, BTH, 0, s_>>>(chunks(), bb_.p, x_.p);
     FG_CHECK_LAUNCH();
     launches_ += 2;
-    precondition_and_dots<R>(1);
+    precondition_and_dots<R>(1, false);
     for (;;) {
         if (any_running()) launch_loop(cancel);
         if (cancel && *cancel) return;
@@ -1276,9 +1557,117 @@ void BatchImpl::run(const volatile int* cancel) {
         finish<R>(FIN_RESTART, 0);
         if (!any_running()) break;
         ++restarts_;
-        precondition_and_dots<R>(1);
+        precondition_and_dots<R>(1, false);
     }
 }
+
+// ------------------------------------------------------------------ continuous batching
+template <int R>
+void BatchImpl::build_stream_graph() {
+    const bool mixed = opt_.precision == FEMGPU_MIXED;
+    const int S = B_ * R;
+    const size_t before = launches_;
+    FG_CUDA(cudaGraphCreate(&sgraph_, 0));
+    FG_CUDA(cudaGraphConditionalHandleCreate(&scond_, sgraph_, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = scond_;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    FG_CUDA(cudaGraphAddNode(&node, sgraph_, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    FG_CUDA(cudaStreamBeginCaptureToGraph(s_, body, nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal));
+    k_sadmit<<<(S + BTH - 1) / BTH, BTH, 0, s_>>>(S, dh_, seen_.p, phase_.p, done_.p, admit_.p);
+    k_sadmit_copy<R><<<nchunks_, BTH, 0, s_>>>(chunks(), boffd_.p, admit_.p, dh_, b_.p, r_.p,
+                                               mixed ? r32_.p : nullptr, x_.p, p_.p, q_.p);
+    iteration<R>(true);
+    k_sdeliver_copy<R><<<nchunks_, BTH, 0, s_>>>(chunks(), boffd_.p, phase_.p, dh_, x_.p);
+    k_sdeliver<<<(S + BTH - 1) / BTH, BTH, 0, s_>>>(S, dh_, seen_.p, phase_.p, scalars());
+    k_sloop_control<<<1, BTH, 0, s_>>>(scond_, S, dh_, seen_.p, phase_.p, loops_.p,
+                                       served_its_.p);
+    FG_CUDA(cudaStreamEndCapture(s_, &body));
+    FG_CUDA(cudaGraphInstantiate(&sexec_, sgraph_, 0));
+    launches_ = before;
+}
+
+void BatchImpl::stream_open() {
+    if (sexec_) return;
+    const size_t S = (size_t)B_ * R_, vals = (size_t)n_ * R_;
+    phase_.alloc(S);
+    restarts_seg_.alloc(S);
+    fresh_.alloc(S);
+    admit_.alloc(S);
+    seen_.alloc(S);
+    served_its_.alloc(1);
+    served_its_.zero(s_);
+    phase_.zero(s_);
+    restarts_seg_.zero(s_);
+    fresh_.zero(s_);
+    admit_.zero(s_);
+    seen_.zero(s_);
+    boffd_.upload(boff_.data(), boff_.size(), s_);
+    // Every slot starts free and finished (done), its vectors 0.
+    std::vector<int> ones(S, 1);
+    done_.upload(ones.data(), S, s_);
+    for (auto* v : {&x_, &r_, &p_, &q_, &b_}) v->zero(s_);
+    if (r32_.p) r32_.zero(s_);
+    FG_CUDA(cudaHostAlloc(&h_req_, S * sizeof(unsigned long long), cudaHostAllocMapped));
+    FG_CUDA(cudaHostAlloc(&h_served_, S * sizeof(unsigned long long), cudaHostAllocMapped));
+    FG_CUDA(cudaHostAlloc(&h_in_, vals * sizeof(double), cudaHostAllocMapped));
+    FG_CUDA(cudaHostAlloc(&h_out_, vals * sizeof(double), cudaHostAllocMapped));
+    FG_CUDA(cudaHostAlloc(&h_stat_, S * sizeof(StreamStat), cudaHostAllocMapped));
+    FG_CUDA(cudaHostAlloc(&h_stop_, sizeof(int), cudaHostAllocMapped));
+    std::memset(h_req_, 0, S * sizeof(unsigned long long));
+    std::memset(h_served_, 0, S * sizeof(unsigned long long));
+    std::memset(h_stat_, 0, S * sizeof(StreamStat));
+    *h_stop_ = 0;
+    unsigned long long *dreq, *dserved;
+    double *din, *dout;
+    StreamStat* dstat;
+    int* dstop;
+    FG_CUDA(cudaHostGetDevicePointer(&dreq, h_req_, 0));
+    FG_CUDA(cudaHostGetDevicePointer(&dserved, h_served_, 0));
+    FG_CUDA(cudaHostGetDevicePointer(&din, h_in_, 0));
+    FG_CUDA(cudaHostGetDevicePointer(&dout, h_out_, 0));
+    FG_CUDA(cudaHostGetDevicePointer(&dstat, h_stat_, 0));
+    FG_CUDA(cudaHostGetDevicePointer(&dstop, h_stop_, 0));
+    dh_ = StreamHost{dreq, dserved, din, dout, dstat, dstop};
+    FG_CUDA(cudaEventCreateWithFlags(&sev_, cudaEventDisableTiming));
+    if (R_ == 16)
+        build_stream_graph<16>();
+    else if (R_ == 4)
+        build_stream_graph<4>();
+    else
+        build_stream_graph<1>();
+    FG_CUDA(cudaStreamSynchronize(s_));
+}
+
+void BatchImpl::stream_launch() {
+    FG_CUDA(cudaGraphLaunch(sexec_, s_));
+    FG_CUDA(cudaEventRecord(sev_, s_));
+    slaunched_ = true;
+}
+
+bool BatchImpl::stream_idle() {
+    if (!slaunched_) return true;
+    const cudaError_t e = cudaEventQuery(sev_);
+    if (e == cudaErrorNotReady) return false;
+    FG_CUDA(e);
+    slaunched_ = false;
+    return true;
+}
+
+void BatchImpl::stream_stop() {
+    if (h_stop_) *(volatile int*)h_stop_ = 1;
+    FG_CUDA(cudaStreamSynchronize(s_));
+    slaunched_ = false;
+}
+
+size_t BatchImpl::stream_loops() { return (size_t)fetch(loops_.p, s_); }
+size_t BatchImpl::stream_served_iterations() { return (size_t)fetch(served_its_.p, s_); }
+bool BatchImpl::streaming() const { return sexec_ != nullptr; }
 
 void BatchImpl::permute(const double* in, double* out, int scatter) {
     const int64_t e = n_ * R_;
@@ -1305,6 +1694,8 @@ void BatchImpl::solve_loaded(const volatile int* cancel, femgpu_batch_stats* st)
 
 void BatchImpl::solve_device(const double* d_b, double* d_x, const volatile int* cancel,
                              femgpu_batch_stats* st) {
+    if (streaming())
+        throw Failure(FEMGPU_ERR_INVALID, "the batch serves a stream: solve through the stream");
     if (exec_ && (max_iter_ != graph_max_iter_ || tol != graph_tol_)) {
         cudaGraphExecDestroy(exec_);
         cudaGraphDestroy(graph_);
@@ -1326,6 +1717,8 @@ void BatchImpl::solve_device(const double* d_b, double* d_x, const volatile int*
 // Host vectors go through the batch's own staging vector, so a solve allocates nothing.
 void BatchImpl::solve_host(const double* h_b, double* h_x, const volatile int* cancel,
                            femgpu_batch_stats* st) {
+    if (streaming())
+        throw Failure(FEMGPU_ERR_INVALID, "the batch serves a stream: solve through the stream");
     const size_t bytes = (size_t)n_ * R_ * sizeof(double);
     if (exec_ && (max_iter_ != graph_max_iter_ || tol != graph_tol_)) {
         cudaGraphExecDestroy(exec_);
@@ -1487,6 +1880,92 @@ struct femgpu_batch {
     femgpu::BatchImpl impl;
 };
 
+// The host side of continuous batching: requests wait in a queue per system until one of its
+// slots is free, then go into the mapped staging slot and the device loop admits them at its
+// next iteration. 1 worker thread publishes requests, starts the device loop when a slot is busy
+// and it is not running, and collects the finished slots.
+struct femgpu_stream {
+    femgpu_batch* batch = nullptr;
+    int device = 0;
+    std::mutex m;
+    std::condition_variable cv;
+    struct Ticket {
+        int member = 0;
+        std::vector<double> rhs, x;
+        femgpu::StreamStat stat{};
+        std::chrono::steady_clock::time_point t0, t1;
+        bool done = false;
+    };
+    std::unordered_map<uint64_t, Ticket> tickets;
+    uint64_t next = 1;
+    std::vector<std::deque<uint64_t>> queue;  // per system
+    std::vector<uint64_t> slot_ticket;        // per segment, 0 when free
+    std::vector<unsigned long long> gen;      // per segment, the last generation published
+    std::thread worker;
+    bool quit = false;
+    std::string failure;
+
+    void run() {
+        using namespace femgpu;
+        BatchImpl& b = batch->impl;
+        cudaSetDevice(device);
+        const int R = b.slots(), B = b.members();
+        std::unique_lock<std::mutex> lk(m);
+        for (;;) {
+            bool progress = false, busy = false;
+            for (int k = 0; k < B; ++k)
+                for (int c = 0; c < R; ++c) {
+                    const int sg = b.segment(k, c);
+                    const uint64_t t = slot_ticket[sg];
+                    if (!t) continue;
+                    if (b.h_served()[sg] != gen[sg]) {
+                        busy = true;
+                        continue;
+                    }
+                    // Finished: its x and figures from the mapped output slot.
+                    std::atomic_thread_fence(std::memory_order_acquire);
+                    Ticket& tk = tickets[t];
+                    const double* out = b.h_out() + b.slot_offset(k, c);
+                    tk.x.assign(out, out + b.member_rows(k));
+                    tk.stat = b.h_stat()[sg];
+                    tk.t1 = std::chrono::steady_clock::now();
+                    tk.done = true;
+                    slot_ticket[sg] = 0;
+                    progress = true;
+                }
+            for (int k = 0; k < B; ++k)
+                for (int c = 0; c < R && !queue[k].empty(); ++c) {
+                    const int sg = b.segment(k, c);
+                    if (slot_ticket[sg]) continue;
+                    const uint64_t t = queue[k].front();
+                    queue[k].pop_front();
+                    Ticket& tk = tickets[t];
+                    std::memcpy(b.h_in() + b.slot_offset(k, c), tk.rhs.data(),
+                                tk.rhs.size() * sizeof(double));
+                    std::atomic_thread_fence(std::memory_order_release);
+                    gen[sg] += 1;
+                    b.h_req()[sg] = gen[sg];
+                    slot_ticket[sg] = t;
+                    busy = true;
+                    progress = true;
+                }
+            if (progress) cv.notify_all();
+            try {
+                if (busy && b.stream_idle()) b.stream_launch();
+            } catch (const std::exception& e) {
+                failure = e.what();
+                cv.notify_all();
+                return;
+            }
+            if (quit && !busy) return;
+            if (busy)
+                cv.wait_for(lk, std::chrono::microseconds(20));
+            else
+                cv.wait(lk);
+        }
+    }
+};
+
 using namespace femgpu;
 
 template <class F>
@@ -1614,5 +2093,107 @@ void* femgpu_batch_stream(const femgpu_batch* b) {
 }
 
 void femgpu_batch_free(femgpu_batch* b) { delete b; }
+
+int femgpu_stream_new(femgpu_batch* b, femgpu_stream** out) {
+    return batch_guarded([&] {
+        if (!b || !out) throw Failure(FEMGPU_ERR_INVALID, "null argument");
+        if (b->impl.streaming()) throw Failure(FEMGPU_ERR_INVALID, "the batch serves a stream already");
+        b->impl.stream_open();
+        auto st = std::make_unique<femgpu_stream>();
+        st->batch = b;
+        FG_CUDA(cudaGetDevice(&st->device));
+        const int S = b->impl.members() * b->impl.slots();
+        st->queue.resize(b->impl.members());
+        st->slot_ticket.assign(S, 0);
+        st->gen.assign(S, 0);
+        femgpu_stream* raw = st.get();
+        st->worker = std::thread([raw] { raw->run(); });
+        *out = st.release();
+    });
+}
+
+int femgpu_stream_submit(femgpu_stream* s, int system, const double* rhs, uint64_t* ticket) {
+    return batch_guarded([&] {
+        if (!s || !rhs || !ticket) throw Failure(FEMGPU_ERR_INVALID, "null argument");
+        BatchImpl& b = s->batch->impl;
+        if (system < 0 || system >= b.members())
+            throw Failure(FEMGPU_ERR_INVALID, "no such system in the batch");
+        std::lock_guard<std::mutex> lk(s->m);
+        if (!s->failure.empty()) throw Failure(FEMGPU_ERR_CUDA, s->failure);
+        const uint64_t t = s->next++;
+        femgpu_stream::Ticket& tk = s->tickets[t];
+        tk.member = system;
+        tk.rhs.assign(rhs, rhs + b.member_rows(system));
+        tk.t0 = std::chrono::steady_clock::now();
+        s->queue[system].push_back(t);
+        *ticket = t;
+        s->cv.notify_all();
+    });
+}
+
+int femgpu_stream_wait(femgpu_stream* s, uint64_t ticket, double* x,
+                       femgpu_stream_result* result) {
+    return batch_guarded([&] {
+        if (!s || !x) throw Failure(FEMGPU_ERR_INVALID, "null argument");
+        std::unique_lock<std::mutex> lk(s->m);
+        auto it = s->tickets.find(ticket);
+        if (it == s->tickets.end()) throw Failure(FEMGPU_ERR_INVALID, "no such ticket");
+        s->cv.wait(lk, [&] { return it->second.done || !s->failure.empty(); });
+        if (!it->second.done) throw Failure(FEMGPU_ERR_CUDA, s->failure);
+        femgpu_stream::Ticket tk = std::move(it->second);
+        s->tickets.erase(it);
+        lk.unlock();
+        std::memcpy(x, tk.x.data(), tk.x.size() * sizeof(double));
+        if (result) {
+            result->iterations = (size_t)tk.stat.iterations;
+            result->residual = tk.stat.residual;
+            result->true_residual = tk.stat.truth;
+            result->status = tk.stat.status;
+            result->latency_s = std::chrono::duration<double>(tk.t1 - tk.t0).count();
+        }
+        if (tk.stat.status == 2)
+            throw Failure(FEMGPU_ERR_NOT_CONVERGED,
+                          "conjugate gradients broke down: the residual is not a number");
+        if (tk.stat.status == 1) {
+            char buf[200];
+            std::snprintf(buf, sizeof buf,
+                          "conjugate gradients did not converge: the residual is %s after %d "
+                          "iterations",
+                          rust_exp(tk.stat.residual, 2).c_str(), tk.stat.iterations);
+            throw Failure(FEMGPU_ERR_NOT_CONVERGED, buf);
+        }
+    });
+}
+
+int femgpu_stream_counts(femgpu_stream* s, size_t* loops, size_t* served_iterations) {
+    return batch_guarded([&] {
+        if (!s) throw Failure(FEMGPU_ERR_INVALID, "null stream");
+        std::lock_guard<std::mutex> lk(s->m);
+        if (loops) *loops = s->batch->impl.stream_loops();
+        if (served_iterations) *served_iterations = s->batch->impl.stream_served_iterations();
+    });
+}
+
+void femgpu_stream_free(femgpu_stream* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        s->quit = true;
+        s->cv.notify_all();
+    }
+    // Requests still running end with the loop: the device stops at its next iteration.
+    try {
+        s->batch->impl.stream_stop();
+    } catch (...) {
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        for (auto& t : s->slot_ticket) t = 0;
+        s->failure = s->failure.empty() ? "the stream was freed" : s->failure;
+        s->cv.notify_all();
+    }
+    if (s->worker.joinable()) s->worker.join();
+    delete s;
+}
 
 }  // extern "C"

@@ -441,6 +441,37 @@ size_t femgpu_batch_bytes(const femgpu_batch* b);
 void* femgpu_batch_stream(const femgpu_batch* b);
 void femgpu_batch_free(femgpu_batch* b);
 
+/* Continuous batching over a batch's systems. No reference counterpart: the reference's
+ * callers solve 1 model at a time; serving many requests for resident meshes is this library's.
+ * femgpu_stream_new turns a batch into a server of single right sides: each system has `nrhs`
+ * slots; a request (1 right side of 1 system, x from 0) waits until a slot of its system is
+ * free and is then admitted by the running device loop at its next PCG iteration, while the
+ * other slots' solves go on; a finished slot's solution (after its true residual, and restarts
+ * from x for the mixed form as in femgpu_batch_solve) is written back and the slot takes the
+ * next request at once. The loop is the batch's CUDA-graph-captured PCG with the multigrid
+ * V-cycle, 1 launch that runs while any slot is busy; its right sides come in and its solutions
+ * go out through pinned, mapped host memory. Every request's result is the same bit for bit
+ * whatever else is in the loop (each slot's arithmetic reads only its own data), and equals
+ * femgpu_batch_solve's for the same right side from x = 0. While a stream is open, the batch's
+ * own solves refuse; a batch serves 1 stream in its life. rhs and x hold the system's rows in
+ * its own order (femgpu_batch_systems). */
+typedef struct femgpu_stream femgpu_stream;
+typedef struct femgpu_stream_result {
+    size_t iterations;
+    double residual;       /* |r| / |b| of the recurrence */
+    double true_residual;  /* |b - A x| / |b| in FP64 */
+    int status;            /* 0 converged, 1 iteration limit, 2 broke down */
+    double latency_s;      /* from submission to the solution's arrival on the host */
+} femgpu_stream_result;
+int femgpu_stream_new(femgpu_batch* b, femgpu_stream** out);
+int femgpu_stream_submit(femgpu_stream* s, int system, const double* rhs, uint64_t* ticket);
+/* Waits for a request: x gets its solution; the reference's texts for the iteration limit. */
+int femgpu_stream_wait(femgpu_stream* s, uint64_t ticket, double* x, femgpu_stream_result* result);
+/* The device loop's iterations so far, and the slots they served summed over them (their ratio
+ * is the mean number of requests packed into 1 iteration). */
+int femgpu_stream_counts(femgpu_stream* s, size_t* loops, size_t* served_iterations);
+void femgpu_stream_free(femgpu_stream* s);
+
 /* ---------------------------------------------------------------- transient heat */
 
 /* The backward-Euler loop of a transient heat model with lumped capacity (heat.rs:686-733): 1
