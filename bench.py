@@ -68,13 +68,16 @@ def args():
                    help="print each solver's levels and the device time of each kernel of 1 "
                         "PCG iteration (kernels launched one by one), then exit")
     p.add_argument("--workload", default="heat",
-                   choices=["heat", "cantilever", "p2beam", "batch", "serve", "recover",
-                            "transient", "modes", "hexheat", "hexbeam", "hexrecover",
-                            "hexmodes"],
+                   choices=["heat", "cantilever", "p2beam", "batch", "serve", "stream",
+                            "recover", "transient", "modes", "hexheat", "hexbeam",
+                            "hexrecover", "hexmodes"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
                         "serve: a Poisson stream of solve requests through the server; "
+                        "stream: a Poisson stream of single load cases of the 256 batched "
+                        "cantilevers, admitted into the running device loop (continuous "
+                        "batching); "
                         "recover: the stress recovery of the solved 200x20x20 P2 beam; "
                         "transient: backward-Euler steps of the 128^3 heat cube; "
                         "modes: 10 lowest modes of a 100x10x10 P2 beam; hexheat: the 128^3 "
@@ -788,6 +791,104 @@ def run_batch(opt, rank, world, local):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ continuous batching
+STREAM_RATES = (500, 2000, 8000, 32000)
+STREAM_REQUESTS = 3000
+
+
+def run_stream(opt, rank, world, local):
+    """Continuous batching: the 256 cantilevers of the batched workload stay resident in 1 batch
+    with 16 slots each; a seeded Poisson stream of single load cases (a random member and load
+    case each) at each rate of STREAM_RATES is submitted to femgpu_stream_*, whose device loop
+    admits each request into a free slot of its member while the others iterate. Reported per
+    rate: p50 / p99 latency (submission to the solution on the host), throughput in DOF-solves/s
+    over the replay, and the packing (requests served per loop iteration). Each solution is
+    checked bit for bit against the batch's own solve of the same load case."""
+    import threading
+
+    import torch
+
+    import femahoy_b200 as fg
+    from femahoy_b200.batch import Batch, Stream
+
+    torch.cuda.set_device(local)
+    dist, barrier, max_over_ranks = _plumbing(world)
+    members = batch_members(opt.systems, SEED + rank)
+    mats, unknowns, rhs = batch_systems(members)
+    opts = fg.Options(precision=fg.MIXED)
+    ref_batch = Batch(mats, unknowns, BATCH_RHS, precision=fg.MIXED, options=opts).with_tol(TOL)
+    ref, _ = ref_batch.solve(rhs)
+    del ref_batch
+    batch = Batch(mats, unknowns, BATCH_RHS, precision=fg.MIXED, options=opts).with_tol(TOL)
+    stream = Stream(batch)
+    rng = np.random.default_rng(SEED + 7)
+    # Warm-up: 1 request per member.
+    for t in [stream.submit(k, rhs[k][:, 0]) for k in range(len(members))]:
+        stream.wait(t)
+    rates = []
+    identical = total = 0
+    for rate in STREAM_RATES:
+        n = STREAM_REQUESTS
+        gaps = rng.exponential(1.0 / rate, n)
+        picks = [(int(rng.integers(len(members))), int(rng.integers(BATCH_RHS))) for _ in range(n)]
+        tickets = [None] * n
+        loops0, served0 = stream.counts()
+
+        def submitter():
+            t0 = time.perf_counter()
+            due = 0.0
+            for i, (k, r) in enumerate(picks):
+                due += gaps[i]
+                while time.perf_counter() - t0 < due:
+                    pass
+                tickets[i] = stream.submit(k, rhs[k][:, r])
+
+        barrier()
+        t_start = time.perf_counter()
+        th = threading.Thread(target=submitter)
+        th.start()
+        lat, dofs = [], 0
+        for i, (k, r) in enumerate(picks):
+            while tickets[i] is None:
+                time.sleep(0)
+            x, res = stream.wait(tickets[i])
+            lat.append(res.latency_s)
+            dofs += len(x)
+            total += 1
+            identical += int(np.array_equal(x.view(np.uint64), ref[k][:, r].view(np.uint64)))
+        th.join()
+        wall = time.perf_counter() - t_start
+        loops1, served1 = stream.counts()
+        lat_ms = np.array(lat) * 1e3
+        rates.append({"rate_per_s": rate, "requests": n,
+                      "p50_ms": float(np.percentile(lat_ms, 50)),
+                      "p99_ms": float(np.percentile(lat_ms, 99)),
+                      "throughput": world * dofs / max_over_ranks(wall),
+                      "served_per_s": n / wall,
+                      "packing": (served1 - served0) / max(1, loops1 - loops0),
+                      "loop_iterations": loops1 - loops0})
+    stream.close()
+    line = {
+        "metric": "DOF-solves/s of a Poisson request stream under continuous batching; p50/p99 "
+                  "latency",
+        "value": rates[-1]["throughput"], "unit": UNIT, "n_gpus": world,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
+        "config": {"workload": f"{opt.systems} resident P1 elasticity cantilevers (the batched "
+                               f"workload), 16 slots each; Poisson arrivals of single load "
+                               f"cases (seed {SEED}), {STREAM_REQUESTS} requests per rate, to "
+                               f"1e-8, mixed precision", "tol": TOL,
+                   "parallelism": f"replicas x{world}"},
+        "rates": rates,
+        "bit_identical_to_batch_solve": f"{identical}/{total}",
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ------------------------------------------------------------------ the serving workload
 SERVE_BUDGET = 150 << 30
 SERVE_SLOTS = 4
@@ -1385,6 +1486,8 @@ def main():
         run_batch(opt, rank, world, local)
     elif opt.workload == "serve":
         run_serve(opt, rank, world, local)
+    elif opt.workload == "stream":
+        run_stream(opt, rank, world, local)
     else:
         run_ours(opt, rank, world, local)
 
