@@ -40,6 +40,7 @@ UNITS = [
     ("coarsen.cu", []),
     ("sparse_direct.cu", []),
     ("dense_eigen.cu", []),
+    ("dense_factor.cu", []),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),

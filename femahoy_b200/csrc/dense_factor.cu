@@ -1,0 +1,288 @@
+// Dense Cholesky factors and inverses on the FP64 tensor cores (dense_factor.cuh).
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "dense_factor.cuh"
+#include "rust_format.hpp"
+
+namespace femgpu {
+namespace {
+
+constexpr double PIVOT = 1e-10;  // cholesky.rs:22
+constexpr int PANEL = 32;
+constexpr int TILE = 64;
+constexpr int TH = 256;
+
+// Panel [p0, p0 + kb) of the column-major m x m matrix F: the diagonal block factored in shared
+// memory (each pivot tested against PIVOT times its column's diagonal of A), then the panel's
+// rows below solved against it (L21 = A21 L11^-T); 1 block.
+__global__ void __launch_bounds__(TH)
+    k_panel(double* __restrict__ F, int64_t m, int64_t p0, int kb,
+            const double* __restrict__ diag0, int64_t col0,
+            unsigned long long* __restrict__ status) {
+    __shared__ double D[PANEL][PANEL + 1];
+    __shared__ int stop;
+    for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
+        const int i = t % PANEL, j = t / PANEL;
+        D[i][j] = (i < kb && j < kb) ? F[(p0 + i) + (p0 + j) * m] : 0.0;
+    }
+    if (threadIdx.x == 0) stop = 0;
+    __syncthreads();
+    for (int j = 0; j < kb; ++j) {
+        if (threadIdx.x == 0) {
+            const double d = D[j][j];
+            if (!(d > PIVOT * fabs(diag0[p0 + j]))) {
+                atomicMin(status, (unsigned long long)(col0 + p0 + j));
+                stop = 1;
+            } else {
+                D[j][j] = sqrt(d);
+            }
+        }
+        __syncthreads();
+        if (stop) return;
+        if (threadIdx.x > j && threadIdx.x < kb) D[threadIdx.x][j] /= D[j][j];
+        __syncthreads();
+        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+            const int i = t % kb, c = t / kb;
+            if (c > j && i >= c) D[i][c] -= D[i][j] * D[c][j];
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int i = t % kb, j = t / kb;
+        if (i >= j) F[(p0 + i) + (p0 + j) * m] = D[i][j];
+    }
+    for (int64_t r = p0 + kb + threadIdx.x; r < m; r += blockDim.x) {
+        double x[PANEL];
+        for (int j = 0; j < kb; ++j) {
+            double v = F[r + (p0 + j) * m];
+            for (int q = 0; q < j; ++q) v -= x[q] * D[j][q];
+            x[j] = v / D[j][j];
+            F[r + (p0 + j) * m] = x[j];
+        }
+    }
+}
+
+// D = A B + D on the FP64 tensor cores: A 8 x 4 (row), B 4 x 8 (column), D 8 x 8; lane l holds
+// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// The 64 x 64 product of As (64 rows x 32 k) and Bs^T (Bs: 64 columns x 32 k) added into acc:
+// warp w takes rows 8w..8w+7, 8 tiles of 8 columns.
+__device__ __forceinline__ void tile_product(const double (*As)[PANEL + 1],
+                                             const double (*Bs)[PANEL + 1], double acc[8][2]) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < PANEL; kk += 4) {
+        const double a = As[warp * 8 + g][kk + q];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt) dmma(acc[nt][0], acc[nt][1], a, Bs[nt * 8 + g][kk + q]);
+    }
+}
+
+// The trailing update F[t0:m, t0:m] -= L21 L21^T (lower triangle), L21 = F[t0:m, p0:p0+kb],
+// kb <= 32: 1 block per 64 x 64 tile on or below the diagonal.
+__global__ void __launch_bounds__(TH)
+    k_syrk_update(double* __restrict__ F, int64_t m, int64_t t0, int64_t p0, int kb) {
+    __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
+    const int64_t b = blockIdx.x;
+    int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
+    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+    while (bi * (bi + 1) / 2 > b) --bi;
+    const int64_t bj = b - bi * (bi + 1) / 2;
+    const int64_t r0 = t0 + bi * TILE, c0 = t0 + bj * TILE;
+    for (int t = threadIdx.x; t < TILE * PANEL; t += blockDim.x) {
+        const int r = t % TILE, k = t / TILE;
+        As[r][k] = (r0 + r < m && k < kb) ? F[(r0 + r) + (p0 + k) * m] : 0.0;
+        Bs[r][k] = (c0 + r < m && k < kb) ? F[(c0 + r) + (p0 + k) * m] : 0.0;
+    }
+    __syncthreads();
+    double acc[8][2] = {};
+    tile_product(As, Bs, acc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t r = r0 + warp * 8 + (lane >> 2);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int64_t c = c0 + nt * 8 + 2 * (lane & 3) + i;
+            if (r < m && c < m && r >= c) F[r + c * m] -= acc[nt][i];
+        }
+}
+
+// C -= A B for an M x N block C (column-major, ldc), A M x kb (lda), B kb x N (ldb), kb <= 32:
+// 1 block per 64 x 64 tile of C.
+__global__ void __launch_bounds__(TH)
+    k_gemm_sub(double* __restrict__ C, int64_t ldc, const double* __restrict__ A, int64_t lda,
+               const double* __restrict__ B, int64_t ldb, int64_t M, int64_t N, int kb) {
+    __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
+    const int64_t r0 = (int64_t)blockIdx.x * TILE, c0 = (int64_t)blockIdx.y * TILE;
+    for (int t = threadIdx.x; t < TILE * PANEL; t += blockDim.x) {
+        const int r = t % TILE, k = t / TILE;
+        As[r][k] = (r0 + r < M && k < kb) ? A[(r0 + r) + k * lda] : 0.0;
+        const int kk = t % PANEL, c = t / PANEL;
+        Bs[c][kk] = (c0 + c < N && kk < kb) ? B[kk + (c0 + c) * ldb] : 0.0;
+    }
+    __syncthreads();
+    double acc[8][2] = {};
+    tile_product(As, Bs, acc);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t r = r0 + warp * 8 + (lane >> 2);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int64_t c = c0 + nt * 8 + 2 * (lane & 3) + i;
+            if (r < M && c < N) C[r + c * ldc] -= acc[nt][i];
+        }
+}
+
+// Rows [b0, b0 + kb) of W for its columns 0..ncols: W_b = L_bb^-1 W_b (the block's triangle in
+// shared memory), 1 thread per column.
+__global__ void __launch_bounds__(TH)
+    k_trsm_rows(double* __restrict__ W, const double* __restrict__ L, int64_t n, int64_t b0,
+                int kb, int64_t ncols) {
+    __shared__ double D[PANEL][PANEL + 1];
+    for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
+        const int i = t % PANEL, j = t / PANEL;
+        D[i][j] = (i < kb && j < kb && i >= j) ? L[(b0 + i) + (b0 + j) * n] : 0.0;
+    }
+    __syncthreads();
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncols;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        double y[PANEL];
+        for (int i = 0; i < kb; ++i) {
+            double v = W[(b0 + i) + c * n];
+            for (int j = 0; j < i; ++j) v -= D[i][j] * y[j];
+            y[i] = v / D[i][i];
+            W[(b0 + i) + c * n] = y[i];
+        }
+    }
+}
+
+// X = W^T W (W lower triangular, column-major n x n): 1 block per 64 x 64 tile on or below the
+// diagonal, the sum over k from the tile's first row (W[k][i] = 0 for k < i), both halves of X
+// written.
+__global__ void __launch_bounds__(TH)
+    k_gram_lower(const double* __restrict__ W, int64_t n, double* __restrict__ X) {
+    __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
+    const int64_t b = blockIdx.x;
+    int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
+    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
+    while (bi * (bi + 1) / 2 > b) --bi;
+    const int64_t bj = b - bi * (bi + 1) / 2;
+    const int64_t i0 = bi * TILE, j0 = bj * TILE;
+    double acc[8][2] = {};
+    for (int64_t k0 = i0; k0 < n; k0 += PANEL) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < TILE * PANEL; t += blockDim.x) {
+            const int kk = t % PANEL, c = t / PANEL;
+            const bool kin = k0 + kk < n;
+            As[c][kk] = (kin && i0 + c < n) ? W[(k0 + kk) + (i0 + c) * n] : 0.0;
+            Bs[c][kk] = (kin && j0 + c < n) ? W[(k0 + kk) + (j0 + c) * n] : 0.0;
+        }
+        __syncthreads();
+        tile_product(As, Bs, acc);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t i = i0 + warp * 8 + (lane >> 2);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t j = j0 + nt * 8 + 2 * (lane & 3) + h;
+            if (i < n && j < n && i >= j) {
+                X[i + j * n] = acc[nt][h];
+                X[j + i * n] = acc[nt][h];
+            }
+        }
+}
+
+// The dense lower triangle of a host CSR's device copy, and its diagonal.
+__global__ void k_scatter_dense(int64_t n, const int64_t* __restrict__ ptr,
+                                const uint32_t* __restrict__ idx, const double* __restrict__ val,
+                                double* __restrict__ M, double* __restrict__ diag) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int64_t e = ptr[i]; e < ptr[i + 1]; ++e) {
+            const int64_t j = idx[e];
+            if (j == i) d = val[e];
+            if (j >= i) M[j + i * n] = val[e];  // column i, row j (symmetric)
+        }
+        diag[i] = d;
+    }
+}
+
+__global__ void k_identity(int64_t n, double* __restrict__ W) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n * n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        W[t] = (t % n == t / n) ? 1.0 : 0.0;
+}
+
+}  // namespace
+
+void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0, int64_t col0,
+                            unsigned long long* status, cudaStream_t s) {
+    for (int64_t p0 = 0; p0 < k; p0 += PANEL) {
+        const int kb = (int)std::min<int64_t>(PANEL, k - p0);
+        k_panel<<<1, TH, 0, s>>>(F, m, p0, kb, diag0, col0, status);
+        const int64_t t0 = p0 + kb;
+        if (t0 < m) {
+            const int64_t T = (m - t0 + TILE - 1) / TILE;
+            k_syrk_update<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(F, m, t0, p0, kb);
+        }
+    }
+    FG_CHECK_LAUNCH();
+}
+
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
+    const int64_t n = a.n;
+    DevBuf<int64_t> ptr;
+    DevBuf<uint32_t> idx;
+    DevBuf<double> val, diag(n), L(n * n), W(n * n);
+    ptr.upload(a.ptr.data(), n + 1, s);
+    idx.upload(a.idx.data(), a.nnz(), s);
+    val.upload(a.val.data(), a.nnz(), s);
+    L.zero(s);
+    k_scatter_dense<<<blocks_for(n, TH), TH, 0, s>>>(n, ptr.p, idx.p, val.p, L.p, diag.p);
+    DevBuf<unsigned long long> status(1);
+    FG_CUDA(cudaMemsetAsync(status.p, 0xff, sizeof(unsigned long long), s));
+    dense_partial_cholesky(L.p, n, n, diag.p, 0, status.p, s);
+    const unsigned long long bad = fetch(status.p, s);
+    if (bad != ~0ull) {
+        const double d = fetch(diag.p + bad, s);
+        char buf[320];
+        std::snprintf(buf, sizeof buf,
+                      "the matrix is not positive definite: the pivot of column %llu is 0 or less "
+                      "to the precision of the arithmetic (its diagonal is %s)",
+                      bad, rust_exp_shortest(d).c_str());
+        throw Failure(FEMGPU_ERR_NOT_SPD, buf);
+    }
+    // W = L^-1 by block rows of 32: each block's triangle solve, then the rows below updated.
+    k_identity<<<blocks_for(n * n, TH), TH, 0, s>>>(n, W.p);
+    for (int64_t b0 = 0; b0 < n; b0 += PANEL) {
+        const int kb = (int)std::min<int64_t>(PANEL, n - b0);
+        const int64_t ncols = b0 + kb;
+        k_trsm_rows<<<blocks_for(ncols, TH), TH, 0, s>>>(W.p, L.p, n, b0, kb, ncols);
+        const int64_t rows = n - b0 - kb;
+        if (rows > 0) {
+            dim3 grid((unsigned)((rows + TILE - 1) / TILE), (unsigned)((ncols + TILE - 1) / TILE));
+            k_gemm_sub<<<grid, TH, 0, s>>>(W.p + b0 + kb, n, L.p + (b0 + kb) + b0 * n, n,
+                                           W.p + b0, n, rows, ncols, kb);
+        }
+    }
+    inv->alloc(n * n);
+    const int64_t T = (n + TILE - 1) / TILE;
+    k_gram_lower<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(W.p, n, inv->p);
+    FG_CHECK_LAUNCH();
+    FG_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace femgpu

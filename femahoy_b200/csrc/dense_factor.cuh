@@ -1,0 +1,30 @@
+// Dense Cholesky factors and inverses on the device, in FP64 on the tensor cores.
+//
+// The panels of a factor are 32 columns: the diagonal block is factored in shared memory by 1
+// block, which then solves the panel's rows below it; the trailing matrix takes the rank-32
+// update in 64 x 64 tiles of mma.sync m8n8k4 f64 products. The inverse of an SPD matrix is
+// W^T W with W = L^-1, formed by a blocked forward substitution (32 rows at a time, each block's
+// triangle in shared memory, the rest of the rows updated by the same tiled products) and a
+// tiled product W^T W. Pivots at or below 1e-10 of their column's diagonal of A fail
+// (cholesky.rs:22, 173-181): the smallest such column is recorded in `status`.
+#pragma once
+#include <cstdint>
+
+#include "common.cuh"
+#include "hierarchy.hpp"
+
+namespace femgpu {
+
+// Partial Cholesky of the first k columns of the column-major m x m matrix F (lower triangle):
+// columns 0..k get L, the lower triangle of the trailing block the Schur complement. diag0[j]
+// is column j's diagonal of A for the pivot test; a failing column j records col0 + j into
+// *status (an atomic minimum; the caller sets it to ~0 first).
+void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0, int64_t col0,
+                            unsigned long long* status, cudaStream_t s);
+
+// The inverse of the SPD matrix `a` (host CSR, n small) on the device, FP64, n x n (symmetric,
+// so row- and column-major alike). Fails with the reference's text when a pivot is not
+// positive (the column in the natural order).
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s);
+
+}  // namespace femgpu

@@ -1038,174 +1038,9 @@ __global__ void k_diagonal(int64_t n, const int64_t* __restrict__ ptr,
     }
 }
 
-// ------------------------------------------------------------------ dense Cholesky + inverse
-// Column-major n x n; the lower triangle. Blocked right-looking: a 32 x 32 diagonal block in
-// shared memory, the panel below it by rows, then the trailing lower triangle by 32 x 32 tiles.
-__global__ void k_potrf_diag(double* __restrict__ M, int64_t n, int64_t k0, int kb,
-                             const double* __restrict__ diag0, int64_t* __restrict__ status) {
-    __shared__ double A[32][33];
-    __shared__ int stop;
-    int tx = threadIdx.x, ty = threadIdx.y;
-    if (tx < kb && ty < kb) A[tx][ty] = M[(k0 + tx) + (k0 + ty) * n];
-    if (tx == 0 && ty == 0) stop = 0;
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        if (tx == 0 && ty == 0) {
-            double d = A[j][j];
-            if (!(d > PIVOT * fabs(diag0[k0 + j]))) {
-                if (*status == 0) *status = k0 + j + 1;
-                stop = 1;
-            } else {
-                A[j][j] = sqrt(d);
-            }
-        }
-        __syncthreads();
-        if (stop) return;
-        if (ty == 0 && tx > j && tx < kb) A[tx][j] /= A[j][j];
-        __syncthreads();
-        if (ty > j && tx >= ty && tx < kb) A[tx][ty] -= A[tx][j] * A[ty][j];
-        __syncthreads();
-    }
-    if (tx < kb && ty < kb && tx >= ty) M[(k0 + tx) + (k0 + ty) * n] = A[tx][ty];
-}
-
-__global__ void k_trsm_panel(double* __restrict__ M, int64_t n, int64_t k0, int kb,
-                             const int64_t* __restrict__ status) {
-    __shared__ double L[32][33];
-    if (*status) return;
-    for (int t = threadIdx.x; t < 32 * 32; t += blockDim.x) {
-        int i = t % 32, j = t / 32;
-        L[i][j] = (i < kb && j < kb) ? M[(k0 + i) + (k0 + j) * n] : 0.0;
-    }
-    __syncthreads();
-    int64_t i = k0 + kb + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    double l[32];
-    for (int j = 0; j < kb; ++j) {
-        double s = M[i + (k0 + j) * n];
-        for (int p = 0; p < j; ++p) s -= l[p] * L[j][p];
-        l[j] = s / L[j][j];
-        M[i + (k0 + j) * n] = l[j];
-    }
-}
-
-__global__ void k_syrk(double* __restrict__ M, int64_t n, int64_t k0, int kb,
-                       const int64_t* __restrict__ status) {
-    __shared__ double SA[32][33], SB[32][33];
-    if (*status) return;
-    int64_t t0 = k0 + kb;
-    int64_t b = blockIdx.x;
-    int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
-    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
-    while (bi * (bi + 1) / 2 > b) --bi;
-    int64_t bj = b - bi * (bi + 1) / 2;
-    int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 32
-    int64_t ri = t0 + bi * 32 + tx, rj = t0 + bj * 32 + tx;
-    if (ty < kb) {
-        SA[tx][ty] = ri < n ? M[ri + (k0 + ty) * n] : 0.0;
-        SB[tx][ty] = rj < n ? M[rj + (k0 + ty) * n] : 0.0;
-    } else {
-        SA[tx][ty] = 0.0;
-        SB[tx][ty] = 0.0;
-    }
-    __syncthreads();
-    int64_t r = t0 + bi * 32 + tx, c = t0 + bj * 32 + ty;
-    if (r < n && c < n && r >= c) {
-        double acc = 0;
-        for (int p = 0; p < kb; ++p) acc += SA[tx][p] * SB[ty][p];
-        M[r + c * n] -= acc;
-    }
-}
-
-__global__ void k_transpose_lower(const double* __restrict__ L, int64_t n, double* __restrict__ R) {
-    GRID_STRIDE(t, n * n) {
-        int64_t i = t % n, j = t / n;
-        R[i * n + j] = i >= j ? L[i + j * n] : 0.0;
-    }
-}
-
-// Column c of L^-1 (as Y, column-major) by forward substitution: 1 warp per column.
-__global__ void k_inv_forward(const double* __restrict__ Lr, int64_t n, double* __restrict__ Y) {
-    int lane = threadIdx.x & 31;
-    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (c >= n) return;
-    double* y = Y + c * n;
-    for (int64_t k = lane; k < c; k += 32) y[k] = 0.0;
-    for (int64_t i = c; i < n; ++i) {
-        const double* row = Lr + i * n;
-        double s = 0;
-        for (int64_t k = c + lane; k < i; k += 32) s += row[k] * y[k];
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        double v = ((i == c ? 1.0 : 0.0) - s) / row[i];
-        if (lane == 0) y[i] = v;
-        __syncwarp();
-    }
-}
-
-// Column c of L^-T Y: backward substitution with L column-major.
-__global__ void k_inv_backward(const double* __restrict__ L, int64_t n, const double* __restrict__ Y,
-                               double* __restrict__ X) {
-    int lane = threadIdx.x & 31;
-    int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (c >= n) return;
-    double* x = X + c * n;
-    const double* y = Y + c * n;
-    for (int64_t i = n - 1; i >= 0; --i) {
-        const double* col = L + i * n;
-        double s = 0;
-        for (int64_t k = i + 1 + lane; k < n; k += 32) s += col[k] * x[k];
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        double v = (y[i] - s) / col[i];
-        if (lane == 0) x[i] = v;
-        __syncwarp();
-    }
-}
-
-// The inverse of the SPD matrix `a` (host CSR, n small) on the device, FP64, row-major (it is
-// symmetric). Fails with the reference's text when a pivot is not positive.
-void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
-    int64_t n = a.n;
-    std::vector<double> h((size_t)n * n, 0.0), diag(n, 0.0);
-    for (int64_t i = 0; i < n; ++i)
-        for (int64_t k = a.ptr[i]; k < a.ptr[i + 1]; ++k) {
-            h[i + (int64_t)a.idx[k] * n] = a.val[k];
-            if ((int64_t)a.idx[k] == i) diag[i] = a.val[k];
-        }
-    DevBuf<double> M(n * n), d0(n);
-    M.upload(h.data(), n * n, s);
-    d0.upload(diag.data(), n, s);
-    DevBuf<int64_t> status(1);
-    status.zero(s);
-    for (int64_t k0 = 0; k0 < n; k0 += 32) {
-        int kb = (int)std::min<int64_t>(32, n - k0);
-        k_potrf_diag<<<1, dim3(32, 32), 0, s>>>(M.p, n, k0, kb, d0.p, status.p);
-        int64_t rest = n - k0 - kb;
-        if (rest > 0) {
-            k_trsm_panel<<<(unsigned)((rest + 127) / 128), 128, 0, s>>>(M.p, n, k0, kb, status.p);
-            int64_t T = (rest + 31) / 32;
-            k_syrk<<<(unsigned)(T * (T + 1) / 2), dim3(32, 32), 0, s>>>(M.p, n, k0, kb, status.p);
-        }
-        FG_CHECK_LAUNCH();
-    }
-    int64_t st = fetch(status.p, s);
-    if (st) {
-        char buf[320];
-        std::snprintf(buf, sizeof buf,
-                      "the matrix is not positive definite: the pivot of column %lld is 0 or less "
-                      "to the precision of the arithmetic (its diagonal is %s)",
-                      (long long)(st - 1), rust_exp_shortest(diag[st - 1]).c_str());
-        throw Failure(FEMGPU_ERR_NOT_SPD, buf);
-    }
-    DevBuf<double> Lr(n * n), Y(n * n);
-    k_transpose_lower<<<blocks_for(n * n, TH), TH, 0, s>>>(M.p, n, Lr.p);
-    k_inv_forward<<<(unsigned)((n * 32 + 127) / 128), 128, 0, s>>>(Lr.p, n, Y.p);
-    inv->alloc(n * n);
-    k_inv_backward<<<(unsigned)((n * 32 + 127) / 128), 128, 0, s>>>(M.p, n, Y.p, inv->p);
-    FG_CHECK_LAUNCH();
-    FG_CUDA(cudaStreamSynchronize(s));
-}
-
 // ------------------------------------------------------------------ helpers
+// (The dense Cholesky factor and inverse of the direct method and the coarsest level are in
+// dense_factor.cu.)
 void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s) {
     d->n = h.n;
     d->nnz = h.nnz();

@@ -5,6 +5,7 @@
 #include <cstdio>
 
 #include "rust_format.hpp"
+#include "dense_factor.cuh"
 #include "sparse_direct.cuh"
 
 namespace femgpu {
@@ -12,8 +13,6 @@ namespace {
 
 constexpr double PIVOT = 1e-10;     // cholesky.rs:22
 constexpr int SMALL_ROWS = 128;     // fronts factored in shared memory by 1 block
-constexpr int PANEL = 32;           // panel width of a large front
-constexpr int TILE = 64;            // trailing-update tile of a large front
 constexpr int CHUNK = 4096;         // entries of an update matrix per extend-add block
 constexpr int TH = 256;
 
@@ -129,102 +128,6 @@ __global__ void __launch_bounds__(TH)
     }
     __syncthreads();
     for (int t = threadIdx.x; t < m * m; t += blockDim.x) F[t] = S[t];
-}
-
-// A large front, panel [p0, p0 + kb): the diagonal block factored in shared memory, then the
-// panel's rows below solved against it (L21 = A21 L11^-T), 1 block.
-__global__ void __launch_bounds__(TH)
-    k_front_panel(double* __restrict__ F, int64_t m, int64_t p0, int kb,
-                  const double* __restrict__ diag0, int64_t col0,
-                  unsigned long long* __restrict__ status) {
-    __shared__ double D[PANEL][PANEL + 1];
-    __shared__ int stop;
-    for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
-        const int i = t % PANEL, j = t / PANEL;
-        D[i][j] = (i < kb && j < kb) ? F[(p0 + i) + (p0 + j) * m] : 0.0;
-    }
-    if (threadIdx.x == 0) stop = 0;
-    __syncthreads();
-    for (int j = 0; j < kb; ++j) {
-        if (threadIdx.x == 0) {
-            const double d = D[j][j];
-            if (!(d > PIVOT * fabs(diag0[p0 + j]))) {
-                atomicMin(status, (unsigned long long)(col0 + p0 + j));
-                stop = 1;
-            } else {
-                D[j][j] = sqrt(d);
-            }
-        }
-        __syncthreads();
-        if (stop) return;
-        if (threadIdx.x > j && threadIdx.x < kb) D[threadIdx.x][j] /= D[j][j];
-        __syncthreads();
-        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-            const int i = t % kb, c = t / kb;
-            if (c > j && i >= c) D[i][c] -= D[i][j] * D[c][j];
-        }
-        __syncthreads();
-    }
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int i = t % kb, j = t / kb;
-        if (i >= j) F[(p0 + i) + (p0 + j) * m] = D[i][j];
-    }
-    for (int64_t r = p0 + kb + threadIdx.x; r < m; r += blockDim.x) {
-        double x[PANEL];
-        for (int j = 0; j < kb; ++j) {
-            double v = F[r + (p0 + j) * m];
-            for (int q = 0; q < j; ++q) v -= x[q] * D[j][q];
-            x[j] = v / D[j][j];
-            F[r + (p0 + j) * m] = x[j];
-        }
-    }
-}
-
-// D = A B + D on the FP64 tensor cores: A 8 x 4 (row), B 4 x 8 (column), D 8 x 8; lane l holds
-// A[l / 4][l % 4], B[l % 4][l / 4] and D[l / 4][2 (l % 4) + {0, 1}].
-__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
-
-// The trailing update F[t0:m, t0:m] -= L21 L21^T (lower triangle) with L21 = F[t0:m, p0:p0+kb],
-// kb <= 32: 1 block per 64 x 64 tile on or below the diagonal; warp w computes rows 8w..8w+7 of
-// the tile with 8 x 8 tensor-core products over k in steps of 4.
-__global__ void __launch_bounds__(TH)
-    k_front_update(double* __restrict__ F, int64_t m, int64_t t0, int64_t p0, int kb) {
-    __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
-    const int64_t b = blockIdx.x;
-    int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
-    while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
-    while (bi * (bi + 1) / 2 > b) --bi;
-    const int64_t bj = b - bi * (bi + 1) / 2;
-    const int64_t r0 = t0 + bi * TILE, c0 = t0 + bj * TILE;
-    for (int t = threadIdx.x; t < TILE * PANEL; t += blockDim.x) {
-        const int r = t % TILE, k = t / TILE;
-        As[r][k] = (r0 + r < m && k < kb) ? F[(r0 + r) + (p0 + k) * m] : 0.0;
-        Bs[r][k] = (c0 + r < m && k < kb) ? F[(c0 + r) + (p0 + k) * m] : 0.0;
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, q = lane & 3;
-    double acc[8][2];
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = 0.0;
-#pragma unroll
-    for (int kk = 0; kk < PANEL; kk += 4) {
-        const double a = As[warp * 8 + g][kk + q];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) dmma(acc[nt][0], acc[nt][1], a, Bs[nt * 8 + g][kk + q]);
-    }
-    const int64_t r = r0 + warp * 8 + g;
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int64_t c = c0 + nt * 8 + 2 * q + i;
-            if (r < m && c < m && r >= c) F[r + c * m] -= acc[nt][i];
-        }
 }
 
 __global__ void k_permute_in(int64_t n, const int64_t* __restrict__ perm,
@@ -455,20 +358,9 @@ void SparseFactor::factor(const HostCsr& a, const double* xyz, cudaStream_t s) {
             k_front_small<<<(unsigned)ns_small, TH, (size_t)mmax * mmax * sizeof(double), s>>>(
                 small_list_.p + small_at_[h], fr, diag0.p, status.p);
         }
-        for (int64_t t : large_[h]) {
-            const int64_t m = m_[t], k = k_[t];
-            double* F = fronts_.p + foff[t];
-            for (int64_t p0 = 0; p0 < k; p0 += PANEL) {
-                const int kb = (int)std::min<int64_t>(PANEL, k - p0);
-                k_front_panel<<<1, TH, 0, s>>>(F, m, p0, kb, diag0.p + S.first[t], S.first[t],
-                                               status.p);
-                const int64_t t0 = p0 + kb;
-                if (t0 < m) {
-                    const int64_t T = (m - t0 + TILE - 1) / TILE;
-                    k_front_update<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(F, m, t0, p0, kb);
-                }
-            }
-        }
+        for (int64_t t : large_[h])
+            dense_partial_cholesky(fronts_.p + foff[t], m_[t], k_[t], diag0.p + S.first[t],
+                                   S.first[t], status.p, s);
         FG_CHECK_LAUNCH();
     }
     unsigned long long bad = fetch(status.p, s);
