@@ -17,6 +17,8 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <array>
+#include <map>
 #include <mutex>
 #include <optional>
 #include <thread>
@@ -1107,43 +1109,125 @@ static void make_half(Operator<float>* op, cudaStream_t s) {
 // The autotuner's choice for a stencil operator: times y = b - A x with the runtime-K and the
 // compile-time-K kernels (5 launches each after 2 warm-up launches, CUDA events) and keeps the
 // faster. The choice depends on the level's size and on how the L2 serves its offsets.
+// ------------------------------------------------------------------ the autotuner
+// The autotuner's choices per size class, kept for the process: the first operator (or solver)
+// of a class is timed, and later ones of the same class take its choice without timing, so the
+// solvers of one class also choose alike. A class is (what is tuned, the element size, the
+// operator's kind, log2 of its rows, its entries per row).
+namespace {
+std::mutex g_tune_mutex;
+std::map<std::array<int64_t, 5>, int> g_tune;
+
+int64_t log2_of(int64_t n) {
+    int64_t b = 0;
+    while ((int64_t)1 << (b + 1) <= n) ++b;
+    return b;
+}
+
+bool tune_lookup(const std::array<int64_t, 5>& key, int* value) {
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    *value = it->second;
+    return true;
+}
+
+void tune_store(const std::array<int64_t, 5>& key, int value) {
+    std::lock_guard<std::mutex> g(g_tune_mutex);
+    g_tune[key] = value;
+}
+}  // namespace
+
+// The best mean device time (ms) of `launch` over `rounds` rounds of 5, after `warm` launches
+// (the clocks may still be rising after host work).
+template <class F>
+static double time_best(F&& launch, int warm, int rounds, cudaStream_t s) {
+    cudaEvent_t e0, e1;
+    FG_CUDA(cudaEventCreate(&e0));
+    FG_CUDA(cudaEventCreate(&e1));
+    for (int w = 0; w < warm; ++w) launch();
+    FG_CHECK_LAUNCH();
+    double best = 1e30;
+    for (int round = 0; round < rounds; ++round) {
+        FG_CUDA(cudaEventRecord(e0, s));
+        for (int k = 0; k < 5; ++k) launch();
+        FG_CUDA(cudaEventRecord(e1, s));
+        FG_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        best = std::min(best, (double)ms / 5);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+// A stencil level: the runtime-K or the compile-time-K product kernel (the same bits), by timing
+// the residual.
 template <class T>
 static void tune_operator(Operator<T>* op, cudaStream_t s) {
     if (!op->stencil || (op->K != 8 && op->K != 14)) return;
+    const std::array<int64_t, 5> key{0, (int64_t)sizeof(T), op->K, log2_of(op->n), op->half};
+    int v = 0;
+    if (tune_lookup(key, &v)) {
+        op->unrolled = v != 0;
+        return;
+    }
     int64_t n = op->n;
     DevBuf<T> x(n), b(n), r(n);
     x.zero(s);
     b.zero(s);
     DevBuf<int> done(1);
     done.zero(s);
-    cudaEvent_t e0, e1;
-    FG_CUDA(cudaEventCreate(&e0));
-    FG_CUDA(cudaEventCreate(&e1));
     int gs = row_blocks(n);
-    auto launch = [&](int variant) {
-        op->unrolled = variant == 1;
-        with_op(*op, [&](auto o) { k_residual<T><<<gs, TH, 0, s>>>(o, b.p, x.p, r.p, done.p); });
-    };
-    // The GPU may still be raising its clocks after host work: run ~30 launches first, then
-    // alternate the 2 variants over 4 rounds and keep each one's best round.
-    for (int w = 0; w < 30; ++w) launch(w & 1);
-    FG_CHECK_LAUNCH();
-    double best[2] = {1e30, 1e30};
-    for (int round = 0; round < 4; ++round)
-        for (int variant = 0; variant < 2; ++variant) {
-            FG_CUDA(cudaEventRecord(e0, s));
-            for (int k = 0; k < 5; ++k) launch(variant);
-            FG_CUDA(cudaEventRecord(e1, s));
-            FG_CUDA(cudaEventSynchronize(e1));
-            float ms = 0;
-            FG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            best[variant] = std::min(best[variant], (double)ms / 5);
-        }
-    op->probe_ms[0] = best[0];
-    op->probe_ms[1] = best[1];
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for (int variant = 0; variant < 2; ++variant)
+        op->probe_ms[variant] = time_best(
+            [&] {
+                op->unrolled = variant == 1;
+                with_op(*op, [&](auto o) {
+                    k_residual<T><<<gs, TH, 0, s>>>(o, b.p, x.p, r.p, done.p);
+                });
+            },
+            variant == 0 ? 20 : 5, 3, s);
     op->unrolled = op->probe_ms[1] < op->probe_ms[0];
+    tune_store(key, op->unrolled ? 1 : 0);
+}
+
+// A SELL level: the rows per slice (C = 16, 32 or 64; a warp reads 1 slice of 32 rows, 2 of 16,
+// or half of one of 64), by timing the residual of each form.
+template <class T>
+static void tune_sell(const DevCsr& d, Operator<T>* op, cudaStream_t s) {
+    if (op->stencil || op->block3) return;
+    const int64_t per_row = op->n ? (op->nnz + op->n / 2) / op->n : 0;
+    const std::array<int64_t, 5> key{1, (int64_t)sizeof(T), 0, log2_of(op->n), per_row};
+    int C = 0;
+    if (tune_lookup(key, &C)) {
+        if (C != op->sell.C) make_sell<T>(d, C, &op->sell, s);
+        return;
+    }
+    int64_t n = op->n;
+    DevBuf<T> x(n), b(n), r(n);
+    x.zero(s);
+    b.zero(s);
+    DevBuf<int> done(1);
+    done.zero(s);
+    double best = 1e30;
+    int bestC = op->sell.C;
+    for (int c : {16, 32, 64}) {
+        Sell<T> trial;
+        make_sell<T>(d, c, &trial, s);
+        const SellOp<T> o{trial.view()};
+        const int gs = row_blocks(trial.nslices * trial.C);
+        const double ms = time_best(
+            [&] { k_residual<T><<<gs, TH, 0, s>>>(o, b.p, x.p, r.p, done.p); }, 5, 3, s);
+        if (ms < best) {
+            best = ms;
+            bestC = c;
+        }
+    }
+    if (bestC != op->sell.C) make_sell<T>(d, bestC, &op->sell, s);
+    FG_CUDA(cudaStreamSynchronize(s));
+    tune_store(key, bestC);
 }
 
 // The launch of the tile kernels: persistent blocks, 2 per SM, 2 stages of NA tiles each.
@@ -1462,6 +1546,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         PhaseTimer t{this, "outer operator and autotuner", s_};
         make_operator<double>(h, a_, C, opt_.format == 0, &op64_, s_);
         tune_operator(&op64_, s_);
+        if (!opt_.sell_c) tune_sell(a_, &op64_, s_);
     }
     if (u.kind == FEMGPU_UNKNOWNS_GRID) {
         HostLevel lv;
@@ -1483,6 +1568,72 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         HostLevel lv = level_of_points(u.coarse_xyz, p.cols, u.coarse_comp);
         build_multigrid(std::move(h), std::move(lv), &p, nullptr);
     }
+    if (opt_.degree == 0) {
+        PhaseTimer t{this, "autotuner (smoother degree)", s_};
+        tune_degree();
+    }
+}
+
+void SolverImpl::apply_degree(int degree) {
+    const double lower = opt_.lower > 0 ? opt_.lower : 0.3;
+    for (auto& L : H32_.levels) chebyshev(L.lambda, degree, lower, &L.c1, &L.c2);
+    for (auto& L : H64_.levels) chebyshev(L.lambda, degree, lower, &L.c1, &L.c2);
+    // The captured loop holds the coefficients as kernel arguments.
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    exec_ = nullptr;
+    graph_ = nullptr;
+}
+
+// Each candidate degree solves a fixed right side (k_seed) from x = 0 to 1e-4 twice; the second
+// solve's device time per decade of residual reduction decides. Degree 2 is tried first and
+// keeps a tie.
+void SolverImpl::tune_degree() {
+    const bool mixed = opt_.precision == FEMGPU_MIXED;
+    const size_t nlevels = mixed ? H32_.levels.size() : H64_.levels.size();
+    if (nlevels == 0 || opt_.tail > 0) return;  // the fused tail holds its coefficients
+    int64_t kind = -2;  // SELL
+    if (mixed ? H32_.levels[0].A.stencil : H64_.levels[0].A.stencil)
+        kind = mixed ? H32_.levels[0].A.K : H64_.levels[0].A.K;
+    else if (mixed ? H32_.levels[0].A.block3 : H64_.levels[0].A.block3)
+        kind = -1;
+    const std::array<int64_t, 5> key{2, mixed ? 4 : 8, kind, log2_of(n_), (int64_t)nlevels};
+    int degree = 2;
+    if (tune_lookup(key, &degree)) {
+        if (degree != 2) apply_degree(degree);
+        return;
+    }
+    DevBuf<double> rhs(n_);
+    k_seed<<<blocks_for(n_, TH), TH, 0, s_>>>(n_, rhs.p);
+    FG_CHECK_LAUNCH();
+    const double tol0 = tol;
+    const size_t max0 = max_iter;
+    tol = 1e-4;
+    max_iter = 200;
+    double best = 1e30;
+    for (int cand : {2, 1, 3}) {
+        apply_degree(cand);
+        double cost = 1e30;
+        for (int rep = 0; rep < 2; ++rep) {
+            FG_CUDA(cudaMemsetAsync(x_.p, 0, n_ * sizeof(double), s_));
+            femgpu_stats st{};
+            try {
+                solve(rhs.p, x_.p, nullptr, &st);
+            } catch (const Failure&) {
+                st.residual = 1.0;
+            }
+            if (rep == 1 && st.residual > 0.0 && st.residual < 1.0)
+                cost = st.seconds / -std::log10(st.residual);
+        }
+        if (cost < best) {
+            best = cost;
+            degree = cand;
+        }
+    }
+    tol = tol0;
+    max_iter = max0;
+    apply_degree(degree);
+    tune_store(key, degree);
 }
 
 void SolverImpl::sparse_direct(const HostCsr& h, const std::vector<double>& xyz) {
@@ -1650,6 +1801,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         {
             PhaseTimer t{this, "autotuner", s_};
             tune_operator(&lv.A, s_);
+            if (!opt_.sell_c) tune_sell(d, &lv.A, s_);
             if constexpr (std::is_same<T, float>::value)
                 if (l == 0) tune_tiles(&lv.A, opt_.tiles, s_);
         }

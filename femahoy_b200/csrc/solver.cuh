@@ -273,6 +273,9 @@ class SolverImpl {
     void run_device_loop(const volatile int* cancel);
     void run_init(const double* d_b);
     void dense_direct(const HostCsr& a);
+    // The Chebyshev degree of every level (1, 2 or 3) by timed trial solves, per size class.
+    void tune_degree();
+    void apply_degree(int degree);
     void sparse_direct(const HostCsr& a, const std::vector<double>& xyz);
 
     cudaStream_t s_ = nullptr;

@@ -210,9 +210,15 @@ typedef struct femgpu_crossover {
 /* Options of this library (no reference counterpart; zeros pick the defaults). */
 typedef struct femgpu_options {
     int precision;        /* FEMGPU_FP64 or FEMGPU_MIXED */
-    int degree;           /* Chebyshev degree of each pre- and post-smoothing; 0 = autotuned */
+    int degree;           /* Chebyshev degree of each pre- and post-smoothing; 0 = autotuned:
+                             1, 2 or 3 by timed trial solves (device time per decade of residual
+                             reduction), once per size class (the finest level's kind and
+                             log2 rows, the level count, the precision) and kept for the process;
+                             a batch takes 2 */
     double lower;         /* Chebyshev interval lower end as a fraction of lambda_max; 0 = default */
-    int sell_c;           /* SELL chunk height (rows per slice): 0 = autotuned */
+    int sell_c;           /* SELL chunk height (rows per slice; a warp reads 32 rows): 0 =
+                             autotuned, 16, 32 or 64 by timing each level's product, once per
+                             size class (log2 rows, entries per row, element size) */
     int sell_sigma;       /* SELL sorting window in rows: 0 = autotuned */
     int coarsest;         /* the largest level that the dense coarse solve takes; 0 = 5000 (the
                              reference's COARSEST is 3000, multigrid.rs:94; the dense inverse
