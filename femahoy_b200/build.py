@@ -41,6 +41,7 @@ UNITS = [
     ("sparse_direct.cu", []),
     ("dense_eigen.cu", []),
     ("dense_factor.cu", []),
+    ("offsets.cu", []),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),

@@ -17,6 +17,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <deque>
 #include <array>
 #include <map>
 #include <mutex>
@@ -29,6 +30,7 @@
 #include "assemble.cuh"
 #include "solver.cuh"
 #include "coarsen.cuh"
+#include "offsets.cuh"
 #include "symbolic.hpp"
 #include "rust_format.hpp"
 
@@ -124,82 +126,51 @@ template void make_sell<double>(const DevCsr&, int, Sell<double>*, cudaStream_t)
 template void make_sell<float>(const DevCsr&, int, Sell<float>*, cudaStream_t);
 
 // The stencil of a symmetric matrix whose entries sit at a few constant offsets col - row:
-// coef[k n + i] = a(i, i + o_k) for the offsets o_k >= 0. Refused (false) when there are more
-// than MAXK such offsets, or when the slots would hold more than 1.5 times the upper entries.
+// coef[k ld + i] = a(i, i + o_k) for the offsets o_k >= 0, found and filled on the device
+// (offsets.cuh). Refused (false) when there are more than MAXK such offsets, or when the slots
+// would hold more than 1.5 times the upper entries.
 template <class T>
-static bool make_stencil(const HostCsr& h, Operator<T>* out, cudaStream_t s) {
-    int64_t n = h.n;
-    std::vector<int64_t> offs;
-    offs.reserve(64);
-    int64_t upper = 0;
-    for (int64_t i = 0; i < n; ++i)
-        for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) {
-            int64_t o = (int64_t)h.idx[k] - i;
-            if (o < 0) continue;
-            ++upper;
-            if (std::find(offs.begin(), offs.end(), o) == offs.end()) {
-                offs.push_back(o);
-                if ((int)offs.size() > MAXK) return false;
-            }
-        }
-    std::sort(offs.begin(), offs.end());
+static bool make_stencil(const DevCsr& d, Operator<T>* out, cudaStream_t s) {
+    const int64_t n = d.n;
+    OffsetScan sc;
+    if (!scan_offsets(d.ptr.p, d.idx.p, n, true, MAXK, nullptr, &sc, s)) return false;
+    const std::vector<int64_t>& offs = sc.offs;
     if (offs.empty() || offs[0] != 0) return false;
     // 32-bit row arithmetic in the kernels: n + the largest offset must fit.
     if (n + offs.back() >= (int64_t)0x7fffffff) return false;
     // A symmetric pattern has as many entries below the diagonal as above it.
-    int64_t diag = 0;
-    for (int64_t i = 0; i < n; ++i)
-        for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) diag += (int64_t)h.idx[k] == i;
-    if (h.nnz() - upper != upper - diag) return false;
-    int K = (int)offs.size();
-    if ((double)K * n > 1.5 * (double)upper) return false;
+    if (d.nnz - sc.upper != sc.upper - sc.diag) return false;
+    const int K = (int)offs.size();
+    if ((double)K * n > 1.5 * (double)sc.upper) return false;
     const int64_t ld = stencil_ld(n);
     if (ld + offs.back() >= (int64_t)0x7fffffff) return false;
-    std::vector<T> coef((size_t)K * ld, (T)0);
-    for (int64_t i = 0; i < n; ++i)
-        for (int64_t k = h.ptr[i]; k < h.ptr[i + 1]; ++k) {
-            int64_t o = (int64_t)h.idx[k] - i;
-            if (o < 0) continue;
-            int slot = (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
-            coef[(size_t)slot * ld + i] = (T)h.val[k];
-        }
+    out->coef.alloc((size_t)K * ld);
+    fill_offsets<T>(d.ptr.p, d.idx.p, d.val.p, n, true, nullptr, offs, ld, out->coef.p, s);
     out->stencil = true;
     out->n = n;
-    out->nnz = h.nnz();
+    out->nnz = d.nnz;
     out->K = K;
     out->ld = ld;
-    out->off = offs;
-    out->coef.upload(coef.data(), coef.size(), s);
-    FG_CUDA(cudaStreamSynchronize(s));
+    out->off.assign(offs.begin(), offs.end());
     return true;
 }
 
 template <class T>
-void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operator<T>* out,
-                   cudaStream_t s) {
-    if (allow && make_stencil<T>(h, out, s)) return;
+void make_operator(const DevCsr& d, int C, bool allow, Operator<T>* out, cudaStream_t s) {
+    if (allow && make_stencil<T>(d, out, s)) return;
     out->stencil = false;
     out->n = d.n;
     out->nnz = d.nnz;
     // Elasticity levels (node-major unknowns, grid order): the 3x3-block form, 40 bytes per 9
     // FP32 entries instead of 72.
-    std::vector<int64_t> bp;
-    std::vector<uint32_t> bc;
-    std::vector<T> bv;
-    if (allow && make_bsell3<T>(h, &bp, &bc, &bv)) {
+    if (allow && make_bsell3_device<T>(d, &out->b3ptr, &out->b3col, &out->b3val, s)) {
         out->block3 = true;
-        out->b3ptr.upload(bp.data(), bp.size(), s);
-        out->b3col.upload(bc.data(), bc.size(), s);
-        out->b3val.upload(bv.data(), bv.size(), s);
-        FG_CUDA(cudaStreamSynchronize(s));
         return;
     }
     make_sell<T>(d, C, &out->sell, s);
 }
-template void make_operator<double>(const HostCsr&, const DevCsr&, int, bool, Operator<double>*,
-                                    cudaStream_t);
-template void make_operator<float>(const HostCsr&, const DevCsr&, int, bool, Operator<float>*,
-                                   cudaStream_t);
+template void make_operator<double>(const DevCsr&, int, bool, Operator<double>*, cudaStream_t);
+template void make_operator<float>(const DevCsr&, int, bool, Operator<float>*, cudaStream_t);
 
 // Calls f with the kernel-side view of the operator.
 // The stencils of the box-grid hierarchies have K = 8 (the finest P1 level: the 15-point Kuhn
@@ -1503,11 +1474,17 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
     t_.alloc(n_);
     // solve.rs:99-183: the choice of the method.
     bool direct;
+    // The host copy of the matrix, for the host steps of the direct methods only.
     HostCsr h;
-    {
-        PhaseTimer t{this, "matrix to host", s_};
-        h = download_csr(a_, s_);
-    }
+    bool have_h = false;
+    auto host = [&]() -> const HostCsr& {
+        if (!have_h) {
+            PhaseTimer t{this, "matrix to host", s_};
+            h = download_csr(a_, s_);
+            have_h = true;
+        }
+        return h;
+    };
     if (u.kind == FEMGPU_UNKNOWNS_POINTS) {
         if (method == FEMGPU_METHOD_MULTIGRID)
             throw Failure(FEMGPU_ERR_NEEDS_GRID,
@@ -1526,7 +1503,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         std::vector<double> xyz = unknown_xyz(u, a.n);
         uint64_t entries = 0;
         double flops = 0.0;
-        factor_figures(h, nested_dissection(h, xyz.data()), &entries, &flops);
+        factor_figures(host(), nested_dissection(host(), xyz.data()), &entries, &flops);
         direct = entries <= c.entries && (c.flat || flops <= c.flops * (double)a.n);
     }
     direct_ = direct;
@@ -1534,17 +1511,18 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         // A small system takes the dense inverse; a larger one the sparse multifrontal factor in
         // the reference's order.
         if (a.n <= DENSE_DIRECT) {
-            dense_direct(h);
+            dense_direct(host());
         } else {
+            const HostCsr& hh = host();
             PhaseTimer t{this, "sparse factor (analysis on the host, fronts on the device)", s_};
-            sparse_direct(h, unknown_xyz(u, a.n));
+            sparse_direct(hh, unknown_xyz(u, a.n));
         }
         sizes_ = {n_};
         return;
     }
     {
         PhaseTimer t{this, "outer operator and autotuner", s_};
-        make_operator<double>(h, a_, C, opt_.format == 0, &op64_, s_);
+        make_operator<double>(a_, C, opt_.format == 0, &op64_, s_);
         tune_operator(&op64_, s_);
         if (!opt_.sell_c) tune_sell(a_, &op64_, s_);
     }
@@ -1555,7 +1533,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         for (int64_t k = 0; k < n_; ++k)
             for (int d = 0; d < 3; ++d) lv.points[k][d] = u.points[3 * k + d];
         lv.comp.assign(u.comp, u.comp + n_);
-        build_multigrid(std::move(h), std::move(lv), nullptr, cells);
+        build_multigrid(std::move(lv), nullptr, cells);
     } else {
         // p-multigrid (pmultigrid.rs:46-98): the first coarse level is P^T A P on the corners,
         // then geometric levels on the grid of the corner points.
@@ -1566,7 +1544,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
         p.idx.assign(u.p_idx, u.p_idx + p.ptr[n_]);
         p.val.assign(u.p_val, u.p_val + p.ptr[n_]);
         HostLevel lv = level_of_points(u.coarse_xyz, p.cols, u.coarse_comp);
-        build_multigrid(std::move(h), std::move(lv), &p, nullptr);
+        build_multigrid(std::move(lv), &p, nullptr);
     }
     if (opt_.degree == 0) {
         PhaseTimer t{this, "autotuner (smoother degree)", s_};
@@ -1652,57 +1630,24 @@ void SolverImpl::dense_direct(const HostCsr& h) {
 
 // The offset form of a transfer when its entries sit at no more than 32 distinct offsets from
 // each row's first (smallest) column, which they do for the plane coarsening of a box grid in
-// grid order; else `out->ok` stays false and the transfer stays CSR.
+// grid order; else `out->ok` stays false and the transfer stays CSR. Found and filled on the
+// device (offsets.cuh).
 template <class T>
-static void make_offset(const HostRect& M, OffsetTransfer<T>* out, cudaStream_t s) {
+static void make_offset(const DevRect& M, OffsetTransfer<T>* out, cudaStream_t s) {
     out->ok = false;
-    if (M.rows >= 0x7fffffff || M.cols >= 0x7fffffff) return;
-    std::vector<int> base(M.rows, 0);
-    // The rows' bases and each thread's set of offsets (giving up past MAXK), then their union.
-    std::mutex m;
-    std::vector<int64_t> offs;
-    std::atomic<bool> fits{true};
-    parallel_ranges(M.rows, [&](int64_t lo, int64_t hi) {
-        std::vector<int64_t> mine;
-        for (int64_t i = lo; i < hi && fits.load(std::memory_order_relaxed); ++i) {
-            if (M.ptr[i] == M.ptr[i + 1]) continue;
-            uint32_t b = M.idx[M.ptr[i]];
-            for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) b = std::min(b, M.idx[k]);
-            base[i] = (int)b;
-            for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
-                const int64_t o = (int64_t)M.idx[k] - b;
-                if (std::find(mine.begin(), mine.end(), o) == mine.end()) {
-                    if (mine.size() == MAXK) {
-                        fits.store(false);
-                        return;
-                    }
-                    mine.push_back(o);
-                }
-            }
-        }
-        std::lock_guard<std::mutex> g(m);
-        for (int64_t o : mine)
-            if (std::find(offs.begin(), offs.end(), o) == offs.end()) offs.push_back(o);
-    });
-    if (!fits.load() || offs.size() > (size_t)MAXK) return;
-    std::sort(offs.begin(), offs.end());
-    const int K = (int)offs.size();
-    std::vector<T> w((size_t)K * M.rows, (T)0);
-    parallel_ranges(M.rows, [&](int64_t lo, int64_t hi) {
-        for (int64_t i = lo; i < hi; ++i)
-            for (int64_t k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
-                const int64_t o = (int64_t)M.idx[k] - base[i];
-                const int slot =
-                    (int)(std::lower_bound(offs.begin(), offs.end(), o) - offs.begin());
-                w[(size_t)slot * M.rows + i] = (T)M.val[k];
-            }
-    });
+    if (M.rows >= 0x7fffffff || M.cols >= 0x7fffffff || M.nnz == 0) return;
+    out->base.alloc(M.rows);
+    OffsetScan sc;
+    if (!scan_offsets(M.ptr.p, M.idx.p, M.rows, false, MAXK, out->base.p, &sc, s)) {
+        out->base.release();
+        return;
+    }
+    out->w.alloc(sc.offs.size() * (size_t)M.rows);
+    fill_offsets<T>(M.ptr.p, M.idx.p, M.val.p, M.rows, false, out->base.p, sc.offs, M.rows,
+                    out->w.p, s);
     out->rows = M.rows;
     out->cols = M.cols;
-    out->off.assign(offs.begin(), offs.end());
-    out->base.upload(base.data(), base.size(), s);
-    out->w.upload(w.data(), w.size(), s);
-    FG_CUDA(cudaStreamSynchronize(s));
+    out->off.assign(sc.offs.begin(), sc.offs.end());
     out->ok = true;
 }
 
@@ -1780,20 +1725,19 @@ static void build_tail(Hierarchy<T>* H, int tail, cudaStream_t s) {
 }
 
 template <class T>
-void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps,
+void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vector<DevRect>& ps,
                               Hierarchy<T>* H) {
     size_t L = mats.size();
     H->levels.resize(L - 1);
     int C = opt_.sell_c ? opt_.sell_c : 32;
     for (size_t l = 0; l + 1 < L; ++l) {
         MgLevel<T>& lv = H->levels[l];
-        lv.n = mats[l].n;
-        lv.nnz = mats[l].nnz();
-        DevCsr d;
+        const DevCsr& d = *mats[l];
+        lv.n = d.n;
+        lv.nnz = d.nnz;
         {
             PhaseTimer t{this, "level operators", s_};
-            upload_csr(mats[l], &d, s_);
-            make_operator<T>(mats[l], d, C, opt_.format == 0, &lv.A, s_);
+            make_operator<T>(d, C, opt_.format == 0, &lv.A, s_);
             if constexpr (std::is_same<T, float>::value)
                 if (lv.A.stencil && (opt_.values == 2 || (opt_.values == 0 && kHalfDefault)))
                     make_half(&lv.A, s_);
@@ -1822,34 +1766,35 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
         // its own (FP32 in the mixed form, the products accumulated in FP64).
         lv.lambda = l == 0 ? lambda_max(op64_, dg.p, s_, partial_)
                            : lambda_max(lv.A, dg.p, s_, partial_);
-        std::vector<double> hd = dg.to_host(s_);
-        std::vector<double> inv(lv.n);
-        for (int64_t i = 0; i < lv.n; ++i) inv[i] = 1.0 / hd[i];
-        upload_values<T>(inv, &lv.dinv, s_);
+        lv.dinv.alloc(lv.n);
+        reciprocal<T>(lv.n, dg.p, lv.dinv.p, s_);
         int deg = opt_.degree > 0 ? opt_.degree : 2;
         double lower = opt_.lower > 0 ? opt_.lower : 0.3;
         chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2);
         t_lam.reset();
         PhaseTimer t_tr{this, "transfers", s_};
-        // Transfers to the next level.
-        const HostRect& P = ps[l];
-        if ((int64_t)P.idx.size() >= 0x7fffffff || P.rows >= 0x7fffffff)
+        // Transfers to the next level: P and R = P^T (each row's columns increasing).
+        DevRect& P = ps[l];
+        if (P.nnz >= 0x7fffffff || P.rows >= 0x7fffffff)
             throw Failure(FEMGPU_ERR_TOO_LARGE, "a prolongation with 2^31 entries or more");
-        HostRect R = transpose(P);
+        DevRect R;
+        transpose_rect(P, &R, s_);
         lv.nc = P.cols;
         if (opt_.format == 0) {
             make_offset<T>(P, &lv.Po, s_);
             make_offset<T>(R, &lv.Ro, s_);
         }
         if (!lv.Po.ok) {
-            lv.pptr.upload(P.ptr.data(), P.rows + 1, s_);
-            lv.pidx.upload(P.idx.data(), P.idx.size(), s_);
-            upload_values<T>(P.val, &lv.pval, s_);
+            lv.pptr = std::move(P.ptr);
+            lv.pidx = std::move(P.idx);
+            lv.pval.alloc(P.nnz);
+            convert_values<T>(P.nnz, P.val.p, lv.pval.p, s_);
         }
         if (!lv.Ro.ok) {
-            lv.rptr.upload(R.ptr.data(), R.rows + 1, s_);
-            lv.ridx.upload(R.idx.data(), R.idx.size(), s_);
-            upload_values<T>(R.val, &lv.rval, s_);
+            lv.rptr = std::move(R.ptr);
+            lv.ridx = std::move(R.idx);
+            lv.rval.alloc(R.nnz);
+            convert_values<T>(R.nnz, R.val.p, lv.rval.p, s_);
         }
         lv.b.alloc(lv.n);
         lv.xa.alloc(lv.n);
@@ -1860,7 +1805,7 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
     }
     // The coarsest level: its inverse from a dense Cholesky factor on the device.
     PhaseTimer t_dense{this, "coarsest dense inverse", s_};
-    const HostCsr& last = mats.back();
+    const HostCsr last = download_csr(*mats.back(), s_);
     H->ncoarse = last.n;
     DevBuf<double> inv64;
     dense_inverse(last, &inv64, s_);
@@ -1877,27 +1822,26 @@ void SolverImpl::build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>&
     build_tail(H, opt_.tail, s_);
 }
 
-void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
+void SolverImpl::build_multigrid(HostLevel level, const HostRect* pfirst,
                                  const HostCells* cells) {
     // multigrid.rs:84-139: coarsen until a level has at most `coarsest` unknowns, 30 levels, or
-    // a coarsening keeps more than 90 % of the unknowns. The coarsening and the Galerkin
-    // products run on the device (coarsen.cu), the coarse unknowns numbered in grid order; with
-    // cells the coarse matrices are the cell-condensed ones (each level's cells from the last).
-    std::vector<HostCsr> mats;
-    std::vector<HostRect> ps;
+    // a coarsening keeps more than 90 % of the unknowns. The coarsening, the Galerkin products
+    // and the operators of the levels are built on the device (coarsen.cu, offsets.cu), the
+    // coarse unknowns numbered in grid order; with cells the coarse matrices are the
+    // cell-condensed ones (each level's cells from the last, on the host).
+    std::deque<DevCsr> held;  // the coarse matrices
+    std::vector<const DevCsr*> mats{&a_};
+    std::vector<DevRect> ps;
     int threads = host_threads();
-    mats.push_back(std::move(a0));
-    const DevCsr* cur = &a_;  // the device matrix of the last level
-    DevCsr held;
     if (pfirst) {
         // pmultigrid.rs:47: the P1 level is the Galerkin product with the P2 -> P1 prolongation.
         PhaseTimer t{this, "Galerkin products (device)", s_};
         DevRect P;
         rect_upload(*pfirst, &P, s_);
-        galerkin_product(P, a_, &held, s_);
-        cur = &held;
-        mats.push_back(download_csr(held, s_));
-        ps.push_back(*pfirst);
+        held.emplace_back();
+        galerkin_product(P, a_, &held.back(), s_);
+        mats.push_back(&held.back());
+        ps.push_back(std::move(P));
     }
     size_t coarsest = (size_t)(opt_.coarsest > 0 ? opt_.coarsest : DEVICE_COARSEST);
     size_t max_levels = (size_t)(opt_.max_levels > 0 ? opt_.max_levels : 30);
@@ -1905,40 +1849,36 @@ void SolverImpl::build_multigrid(HostCsr a0, HostLevel level, const HostRect* pf
     DevGrid grid;
     grid_upload(level, &grid, s_);
     for (;;) {
-        const HostCsr& a = mats.back();
+        const DevCsr& a = *mats.back();
         if ((size_t)a.n <= coarsest || ps.size() >= max_levels) break;
         DevRect p;
         DevGrid coarse;
         {
             PhaseTimer t{this, "coarsening (device)", s_};
-            if (!coarsen_grid(grid, *cur, opt_.axes, &p, &coarse, s_)) break;
+            if (!coarsen_grid(grid, a, opt_.axes, &p, &coarse, s_)) break;
             if ((size_t)coarse.n * 10 > (size_t)a.n * 9) break;
         }
-        DevCsr next;
-        HostCsr ac;
+        held.emplace_back();
         if (cells && !cells->empty()) {
             PhaseTimer t_c{this, "coarse matrices from the cells (host)", s_};
             HostCells nxt;
-            ac = by_cells(grid_download(grid, s_), stored.empty() ? *cells : stored,
-                          grid_download(coarse, s_), &nxt, threads);
+            HostCsr ac = by_cells(grid_download(grid, s_), stored.empty() ? *cells : stored,
+                                  grid_download(coarse, s_), &nxt, threads);
             stored = std::move(nxt);
-            upload_csr(ac, &next, s_);
+            upload_csr(ac, &held.back(), s_);
         } else {
             PhaseTimer t_g{this, "Galerkin products (device)", s_};
-            galerkin_product(p, *cur, &next, s_);
-            ac = download_csr(next, s_);
+            galerkin_product(p, a, &held.back(), s_);
         }
-        held = std::move(next);
-        cur = &held;
-        mats.push_back(std::move(ac));
-        ps.push_back(rect_download(p, s_));
+        mats.push_back(&held.back());
+        ps.push_back(std::move(p));
         grid = std::move(coarse);
     }
-    if ((size_t)mats.back().n > 16384)
+    if ((size_t)mats.back()->n > 16384)
         throw Failure(FEMGPU_ERR_TOO_LARGE,
                       "the coarsest level has more than 16384 unknowns: the grid does not coarsen");
     sizes_.clear();
-    for (const auto& m : mats) sizes_.push_back(m.n);
+    for (const DevCsr* m : mats) sizes_.push_back(m->n);
     if (opt_.precision == FEMGPU_MIXED) {
         build_levels<float>(mats, ps, &H32_);
         r32_.alloc(n_);

@@ -8,6 +8,7 @@
 
 #include "common.cuh"
 #include "block3.cuh"
+#include "coarsen.cuh"
 #include "hierarchy.hpp"
 #include "ops.cuh"
 #include "sell.cuh"
@@ -89,11 +90,11 @@ struct Operator {
     }
 };
 
-// The operator of the host matrix `h` (also on the device as `d`): a stencil if `allow` and
-// the offsets fit, else SELL-C.
+// The operator of the device matrix `d`, built on the device: a stencil if `allow` and the
+// offsets fit, else (if `allow`) the 3x3-block form where the pattern is node triples, else
+// SELL-C.
 template <class T>
-void make_operator(const HostCsr& h, const DevCsr& d, int C, bool allow, Operator<T>* out,
-                   cudaStream_t s);
+void make_operator(const DevCsr& d, int C, bool allow, Operator<T>* out, cudaStream_t s);
 
 // Setup helpers shared by the solvers (solver.cu).
 void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s);
@@ -257,10 +258,10 @@ class SolverImpl {
     void phase(const std::string& name, double seconds);
 
    private:
-    void build_multigrid(HostCsr a0, HostLevel level, const HostRect* pfirst,
-                         const HostCells* cells);
+    void build_multigrid(HostLevel level, const HostRect* pfirst, const HostCells* cells);
     template <class T>
-    void build_levels(std::vector<HostCsr>& mats, std::vector<HostRect>& ps, Hierarchy<T>* H);
+    void build_levels(const std::vector<const DevCsr*>& mats, std::vector<DevRect>& ps,
+                      Hierarchy<T>* H);
     template <class T>
     const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b);
     template <class T>
