@@ -303,6 +303,20 @@ def oracle_solve_rate(A, rhs, make_solver, tol, direct_xyz=None):
     return out
 
 
+def setup_phases(solver):
+    """The solver's own setup timers (seconds per phase, host clock until the phase's device work
+    finished), from the "setup seconds:" line of its description."""
+    for line in solver.describe().splitlines():
+        if line.startswith("setup seconds:"):
+            out = {}
+            for part in line[len("setup seconds:"):].split(";"):
+                name, _, sec = part.strip().rpartition(" ")
+                if name:
+                    out[name] = float(sec)
+            return out
+    return {}
+
+
 def error_vs_oracle(x, ref):
     """|x - x_oracle|_2 / |x_oracle|_2 against each oracle solution of `oracle_solve_rate`."""
     def rel(y):
@@ -520,12 +534,14 @@ def run_ours(opt, rank, world, local):
     x_e2e = hx.numpy().copy()
     mixed_bytes = mixed.device_bytes()
     levels = mixed.levels()
+    phases_mixed = setup_phases(mixed)
     del mixed
 
     # The plain FP64 form on the same workload.
     plain, setup_fp64 = make(fg.FP64)
     ms64, lat64, its64, _, res64, _ = timed(plain, opt.steps, opt.warmup)
     x_fp64 = x.cpu().numpy()
+    phases_fp64 = setup_phases(plain)
     ms64 = max_over_ranks(ms64)
     value64 = replica_value(world, n_free, opt.steps, ms64)
     del plain
@@ -574,7 +590,8 @@ def run_ours(opt, rank, world, local):
                  "p99_ms": float(np.percentile(np.array(lat64) * 1e3, 99))},
         "mixed_over_fp64": value / value64,
         "setup_s": {"assembly": assemble_s, "submatrix_and_rhs": reduce_s,
-                    "solver_mixed": setup_mixed, "solver_fp64": setup_fp64},
+                    "solver_mixed": setup_mixed, "solver_fp64": setup_fp64,
+                    "phases_mixed": phases_mixed, "phases_fp64": phases_fp64},
         "including_setup": world * n_free / (assemble_s + reduce_s + setup_mixed
                                              + ms_max / opt.steps / 1e3),
         "device_bytes": mixed_bytes,

@@ -225,6 +225,15 @@ __device__ __forceinline__ void cheb_first_row(int i, const T* __restrict__ b,
     x[i] = v;
 }
 
+// The Chebyshev update of 1 row from its product ax: d' = c2 d + c1 D^-1 (b - ax), with 1
+// explicit fused multiply-add, so that every kernel that smooths (1 row or 2 per thread, tiles,
+// the fused coarse levels) gives the same bits whatever the compiler contracts.
+template <class T>
+__device__ __forceinline__ T cheb_update(T bi, T ax, T di, T dprev, T c1, T c2) {
+    const T r = bi - ax;
+    return fmadd(c1 * di, r, c2 * dprev);
+}
+
 // A Chebyshev step: r = b - A x_in, d = c2 d + c1 D^-1 r, x_out = x_in + d.
 template <class T, class Op>
 __device__ __forceinline__ void cheb_step_row(const Op& A, int g, const T* __restrict__ b,
@@ -233,8 +242,7 @@ __device__ __forceinline__ void cheb_step_row(const Op& A, int g, const T* __res
                                               T* __restrict__ d, T* __restrict__ xout) {
     T ax = A.template apply<T>(g, xin);
     if (!A.valid(g)) return;
-    T r = b[g] - ax;
-    T dd = c2 * d[g] + c1 * dinv[g] * r;
+    const T dd = cheb_update(b[g], ax, dinv[g], d[g], c1, c2);
     d[g] = dd;
     xout[g] = xin[g] + dd;
 }
@@ -324,34 +332,41 @@ __device__ __forceinline__ double dot_add(double2 m, double2 x, double s) {
     return s;
 }
 
-// The same row with M at leading dimension dense_ld(n) and b padded to it with zeros: 16-byte
-// loads of M and b, 4 per lane in flight (2 KB per warp), against the 128 bytes of 4 scalar
-// loads: the coarsest product of the box grids (4,913 rows, 96 MB in FP32) is bound by the
-// bytes a warp keeps in flight. 4 partial sums over 16-byte chunks, then the butterfly.
+
+// Row i of x = M b with M at leading dimension ld = dense_ld(n) and b padded to it with zeros,
+// by all TH threads of a block: thread t takes the 16-byte chunks t, t + TH, ... of the row (4 in
+// flight per thread, so a row of the 4,913-row coarsest level of the box grids is read in 1 or
+// 2 round trips), 4 partial sums, a butterfly over each warp, then the warps' sums in order.
+// Every thread of the block must call it; thread 0 returns the sum. `red` holds TH / 32 values.
 template <class T>
-__device__ __forceinline__ T gemv_warp_row_padded(const T* __restrict__ M,
-                                                  const T* __restrict__ b, int64_t ld, int64_t i,
-                                                  int lane) {
+__device__ __forceinline__ T gemv_block_row(const T* __restrict__ M, const T* __restrict__ b,
+                                            int64_t ld, int64_t i, T* red) {
     typedef typename Vec16<T>::type VT;
     const VT* row = reinterpret_cast<const VT*>(M + i * ld);
     const VT* bv = reinterpret_cast<const VT*>(b);
-    const int64_t nc = ld / (int64_t)(sizeof(VT) / sizeof(T));
+    const int nc = (int)(ld / (int64_t)(sizeof(VT) / sizeof(T)));
     T s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    int64_t c = lane;
-    for (; c + 96 < nc; c += 128) {
-        const VT m0 = __ldg(row + c), m1 = __ldg(row + c + 32), m2 = __ldg(row + c + 64),
-                 m3 = __ldg(row + c + 96);
-        const VT x0 = __ldg(bv + c), x1 = __ldg(bv + c + 32), x2 = __ldg(bv + c + 64),
-                 x3 = __ldg(bv + c + 96);
+    int c = threadIdx.x;
+    for (; c + 3 * TH < nc; c += 4 * TH) {
+        const VT m0 = __ldg(row + c), m1 = __ldg(row + c + TH), m2 = __ldg(row + c + 2 * TH),
+                 m3 = __ldg(row + c + 3 * TH);
+        const VT x0 = __ldg(bv + c), x1 = __ldg(bv + c + TH), x2 = __ldg(bv + c + 2 * TH),
+                 x3 = __ldg(bv + c + 3 * TH);
         s0 = dot_add(m0, x0, s0);
         s1 = dot_add(m1, x1, s1);
         s2 = dot_add(m2, x2, s2);
         s3 = dot_add(m3, x3, s3);
     }
-    for (; c < nc; c += 32) s0 = dot_add(__ldg(row + c), __ldg(bv + c), s0);
+    for (; c < nc; c += TH) s0 = dot_add(__ldg(row + c), __ldg(bv + c), s0);
     T s = (s0 + s1) + (s2 + s3);
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    T t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < TH / 32; ++w) t += red[w];
+    __syncthreads();  // `red` is free for the next row
+    return t;
 }
 
 template <class T>
@@ -386,6 +401,106 @@ __global__ void __launch_bounds__(TH)
     const int g = row_of_thread();
     if (g >= A.threads()) return;
     residual_row(A, g, b, x, r);
+}
+
+// ------------------------------------------------------------------ 2 rows per thread
+// The compile-time-K stencil with 2 adjacent rows (i0 even, i0 + 1) per thread: the arrays read
+// once per row from DRAM (each row's own coefficients, x, b, D^-1 and d) come as 8- or 16-byte
+// pairs, so a thread keeps twice the streamed bytes in flight per load; the neighbours (x at
+// i +- o, the coefficients of the rows above, mostly cache hits) as predicated single loads, so
+// that no branch stands between the loads and all of them issue before the first product. Each
+// row's sum is StencilOpK's: the same fused multiply-adds in the same order, so the bits are
+// those of the 1-row kernels.
+template <class T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+    typedef float2 type;
+};
+template <>
+struct Vec2<double> {
+    typedef double2 type;
+};
+template <class T>
+__device__ __forceinline__ typename Vec2<T>::type ld2(const T* p) {
+    return __ldg(reinterpret_cast<const typename Vec2<T>::type*>(p));
+}
+template <class T>
+__device__ __forceinline__ void st2(T* p, T a, T b) {
+    typename Vec2<T>::type v;
+    v.x = a;
+    v.y = b;
+    *reinterpret_cast<typename Vec2<T>::type*>(p) = v;
+}
+
+// Rows i0 (even) and i0 + 1 < n of A x (TA: the accumulation type).
+template <class T, int K, class TA, class TX>
+__device__ __forceinline__ void stencil_pair(const StencilView<T>& v, int i0,
+                                             const TX* __restrict__ x, TA& a0, TA& a1) {
+    const int n = v.n;
+    const T* __restrict__ c = v.coef;
+    const auto cc = ld2(c + i0);
+    const auto xx = ld2(x + i0);
+    a0 = (TA)cc.x * (TA)xx.x;
+    a1 = (TA)cc.y * (TA)xx.y;
+#pragma unroll
+    for (int k = 1; k < K; ++k) {
+        const int o = v.off[k];
+        const T* __restrict__ ck = c + (size_t)k * v.ld;
+        const auto cu = ld2(ck + i0);  // in bounds: i0 + 1 < n <= ld
+        const int j0 = i0 + o, m0 = i0 - o;
+        const bool u0 = j0 < n, u1 = j0 + 1 < n, l0 = m0 >= 0, l1 = m0 + 1 >= 0;
+        const TX xu0 = u0 ? __ldg(x + j0) : (TX)0, xu1 = u1 ? __ldg(x + j0 + 1) : (TX)0;
+        const T cl0 = l0 ? __ldg(ck + m0) : (T)0, cl1 = l1 ? __ldg(ck + m0 + 1) : (T)0;
+        const TX xl0 = l0 ? __ldg(x + m0) : (TX)0, xl1 = l1 ? __ldg(x + m0 + 1) : (TX)0;
+        a0 = fmadd(u0 ? (TA)cu.x : (TA)0, (TA)xu0, a0);
+        a0 = fmadd((TA)cl0, (TA)xl0, a0);
+        a1 = fmadd(u1 ? (TA)cu.y : (TA)0, (TA)xu1, a1);
+        a1 = fmadd((TA)cl1, (TA)xl1, a1);
+    }
+}
+
+// Threads of the 2-row kernels: ceil(n / 2).
+inline int64_t pair_threads(int64_t n) { return (n + 1) / 2; }
+
+template <class T, int K>
+__global__ void __launch_bounds__(TH)
+    k_cheb_step_pair(StencilView<T> v, const T* __restrict__ b, const T* __restrict__ xin,
+                     const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d,
+                     T* __restrict__ xout, const int* __restrict__ done) {
+    pdl_wait();
+    if (*done) return;
+    const int i0 = 2 * row_of_thread();
+    if (i0 >= v.n) return;
+    if (i0 + 1 == v.n) {  // the last row of an odd n
+        cheb_step_row(StencilOpK<T, K>{v}, i0, b, xin, dinv, c1, c2, d, xout);
+        return;
+    }
+    T a0, a1;
+    stencil_pair<T, K, T, T>(v, i0, xin, a0, a1);
+    const auto bb = ld2(b + i0), di = ld2(dinv + i0), dp = ld2(d + i0), xi = ld2(xin + i0);
+    const T d0 = cheb_update(bb.x, a0, di.x, dp.x, c1, c2);
+    const T d1 = cheb_update(bb.y, a1, di.y, dp.y, c1, c2);
+    st2(d + i0, d0, d1);
+    st2(xout + i0, xi.x + d0, xi.y + d1);
+}
+
+template <class T, int K>
+__global__ void __launch_bounds__(TH)
+    k_residual_pair(StencilView<T> v, const T* __restrict__ b, const T* __restrict__ x,
+                    T* __restrict__ r, const int* __restrict__ done) {
+    pdl_wait();
+    if (*done) return;
+    const int i0 = 2 * row_of_thread();
+    if (i0 >= v.n) return;
+    if (i0 + 1 == v.n) {
+        residual_row(StencilOpK<T, K>{v}, i0, b, x, r);
+        return;
+    }
+    T a0, a1;
+    stencil_pair<T, K, T, T>(v, i0, x, a0, a1);
+    const auto bb = ld2(b + i0);
+    st2(r + i0, bb.x - a0, bb.y - a1);
 }
 
 // ------------------------------------------------------------------ stencil tiles by bulk copy
@@ -524,9 +639,7 @@ __global__ void __launch_bounds__(BULK_TH, 2)
             if (STEP) {
                 const float di = full ? own[(K + 1) * STENCIL_TILE + li] : dinv[i];
                 const float dd0 = full ? own[(K + 2) * STENCIL_TILE + li] : d[i];
-                // cheb_step_row
-                float r = bi - acc;
-                float dd = c2 * dd0 + c1 * di * r;
+                const float dd = cheb_update(bi, acc, di, dd0, c1, c2);  // cheb_step_row
                 d[i] = dd;
                 out[i] = xin[i] + dd;
             } else {
@@ -601,7 +714,21 @@ static void launch_transfer(const OffsetTransfer<T>& M, const T* in, T* out, int
 // row. PADDED: ld = dense_ld(n) and b padded to it (the coarsest level of a hierarchy, whose
 // right side is the hierarchy's own padded vector); else scalar loads (the direct method, and a
 // hierarchy of no smoothed level, whose right side is the caller's vector).
-template <class T, bool PADDED>
+// The coarsest product x = M b (padded M and b): 1 block per row at a time.
+template <class T>
+__global__ void __launch_bounds__(TH)
+    k_gemv_rows(int64_t n, int64_t ld, const T* __restrict__ M, const T* __restrict__ b,
+                T* __restrict__ x, const int* __restrict__ done) {
+    pdl_wait();
+    if (*done) return;
+    __shared__ T red[TH / 32];
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const T s = gemv_block_row(M, b, ld, i, red);
+        if (threadIdx.x == 0) x[i] = s;
+    }
+}
+
+template <class T>
 __global__ void k_gemv(int64_t n, int64_t ld, const T* __restrict__ M, const T* __restrict__ b,
                        T* __restrict__ x, const int* __restrict__ done) {
     pdl_wait();
@@ -610,7 +737,7 @@ __global__ void k_gemv(int64_t n, int64_t ld, const T* __restrict__ M, const T* 
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = w; i < n; i += nw) {
-        T s = PADDED ? gemv_warp_row_padded(M, b, ld, i, lane) : gemv_warp_row(M, b, n, ld, i, lane);
+        T s = gemv_warp_row(M, b, n, ld, i, lane);
         if (lane == 0) x[i] = s;
     }
 }
@@ -688,11 +815,11 @@ __global__ void __launch_bounds__(TH)
         grid.sync();
     }
     {
-        const int lane = threadIdx.x & 31;
+        __shared__ T red[TH / 32];
         const T* bc = sL[nl - 1].bc;
-        for (int64_t i = tid >> 5; i < nco; i += nth >> 5) {
-            const T s = gemv_warp_row_padded(inv, bc, dense_ld(nco), i, lane);
-            if (lane == 0) cx[i] = s;
+        for (int64_t i = blockIdx.x; i < nco; i += gridDim.x) {
+            const T s = gemv_block_row(inv, bc, dense_ld(nco), i, red);
+            if (threadIdx.x == 0) cx[i] = s;
         }
         grid.sync();
     }
@@ -853,6 +980,53 @@ __global__ void __launch_bounds__(TH)
         }
     }
     block_partial(pq, 0.0, partial);
+}
+
+// The same with 2 rows per thread (stencil_pair): the block of TH threads covers 2 TH rows and
+// writes the partials of 2 blocks of the 1-row kernel, each summed in that kernel's order (the
+// rows of a warp by the butterfly, then the warps in order), so the result is the same bits.
+template <int K>
+__global__ void __launch_bounds__(TH)
+    k_pcg_spmv_pq_pair(StencilView<double> v, const double* __restrict__ p,
+                       double* __restrict__ q, double* __restrict__ partial,
+                       const Scalars* __restrict__ sc) {
+    pdl_wait();
+    if (sc->done) return;
+    __shared__ double prod[2 * TH];
+    __shared__ double sw[2][TH / 32];
+    const int i0 = 2 * row_of_thread();
+    double pq0 = 0, pq1 = 0;
+    if (i0 + 1 < v.n) {
+        double a0, a1;
+        stencil_pair<double, K, double, double>(v, i0, p, a0, a1);
+        const double2 pp = ld2(p + i0);
+        st2(q + i0, a0, a1);
+        pq0 = pp.x * a0;
+        pq1 = pp.y * a1;
+    } else if (i0 < v.n) {
+        const double a0 = StencilOpK<double, K>{v}.template apply<double>(i0, p);
+        q[i0] = a0;
+        pq0 = p[i0] * a0;
+    }
+    prod[2 * threadIdx.x] = pq0;
+    prod[2 * threadIdx.x + 1] = pq1;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int half = 0; half < 2; ++half) {
+        double a = prod[half * TH + threadIdx.x];
+        for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+        if (lane == 0) sw[half][w] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        const int64_t blk = 2 * (int64_t)blockIdx.x + threadIdx.x;
+        if (blk * TH < v.n) {
+            double t = 0;
+            for (int k = 0; k < TH / 32; ++k) t += sw[threadIdx.x][k];
+            partial[2 * blk] = t;
+            partial[2 * blk + 1] = 0.0;
+        }
+    }
 }
 
 struct FinUpdate {
@@ -1142,6 +1316,7 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
     int v = 0;
     if (tune_lookup(key, &v)) {
         op->unrolled = v != 0;
+        op->pair = v == 2;
         return;
     }
     int64_t n = op->n;
@@ -1151,6 +1326,7 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
     DevBuf<int> done(1);
     done.zero(s);
     int gs = row_blocks(n);
+    op->pair = false;
     for (int variant = 0; variant < 2; ++variant)
         op->probe_ms[variant] = time_best(
             [&] {
@@ -1160,8 +1336,24 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
                 });
             },
             variant == 0 ? 20 : 5, 3, s);
-    op->unrolled = op->probe_ms[1] < op->probe_ms[0];
-    tune_store(key, op->unrolled ? 1 : 0);
+    // The 2-row kernels (FP16 coefficients have none).
+    op->probe_ms[3] = 1e30;
+    if (!op->half) {
+        const StencilView<T> sv = op->sview();
+        const int gp = row_blocks(pair_threads(n));
+        op->probe_ms[3] = time_best(
+            [&] {
+                if (op->K == 8)
+                    k_residual_pair<T, 8><<<gp, TH, 0, s>>>(sv, b.p, x.p, r.p, done.p);
+                else
+                    k_residual_pair<T, 14><<<gp, TH, 0, s>>>(sv, b.p, x.p, r.p, done.p);
+            },
+            5, 3, s);
+    }
+    const double best = std::min({op->probe_ms[0], op->probe_ms[1], op->probe_ms[3]});
+    op->pair = op->probe_ms[3] == best;
+    op->unrolled = op->pair || op->probe_ms[1] == best;
+    tune_store(key, op->pair ? 2 : op->unrolled ? 1 : 0);
 }
 
 // A SELL level: the rows per slice (C = 16, 32 or 64; a warp reads 1 slice of 32 rows, 2 of 16,
@@ -1262,7 +1454,8 @@ static void tune_tiles(Operator<float>* op, int mode, cudaStream_t s) {
     cudaEventDestroy(e1);
     op->probe_ms[2] = best;
     if (fetch(timeout.p, s)) return;
-    const double direct = op->unrolled ? op->probe_ms[1] : op->probe_ms[0];
+    const double direct =
+        op->pair ? op->probe_ms[3] : op->unrolled ? op->probe_ms[1] : op->probe_ms[0];
     op->bulk = mode == 2 || best < direct;
 }
 
@@ -1373,9 +1566,11 @@ static std::string describe_op(const Operator<T>& op) {
     } else if (!op.stencil) {
         std::snprintf(buf, sizeof buf, "sell C=%d nnz=%lld", op.sell.C, (long long)op.nnz);
     } else {
-        std::snprintf(buf, sizeof buf, "stencil K=%d %s%s (probe %.1f / %.1f us)%s nnz=%lld",
-                      op.K, op.half ? "fp16 " : "", op.unrolled ? "unrolled" : "loop",
-                      op.probe_ms[0] * 1e3, op.probe_ms[1] * 1e3,
+        std::snprintf(buf, sizeof buf,
+                      "stencil K=%d %s%s (probe %.1f / %.1f / %.1f us)%s nnz=%lld", op.K,
+                      op.half ? "fp16 " : "",
+                      op.pair ? "unrolled, 2 rows per thread" : op.unrolled ? "unrolled" : "loop",
+                      op.probe_ms[0] * 1e3, op.probe_ms[1] * 1e3, op.probe_ms[3] * 1e3,
                       op.bulk ? ", steps from bulk-copied tiles" : "", (long long)op.nnz);
     }
     return buf;
@@ -1899,6 +2094,16 @@ void SolverImpl::enqueue_step(MgLevel<T>& L, const T* b, const T* xin, T c1, T c
             return;
         }
     }
+    if (L.A.pair) {
+        const int gp = row_blocks(pair_threads(L.n));
+        if (L.A.K == 8)
+            launch(pdl_, k_cheb_step_pair<T, 8>, gp, TH, s_, L.A.sview(), b, xin,
+                   (const T*)L.dinv.p, c1, c2, L.d.p, xout, done);
+        else
+            launch(pdl_, k_cheb_step_pair<T, 14>, gp, TH, s_, L.A.sview(), b, xin,
+                   (const T*)L.dinv.p, c1, c2, L.d.p, xout, done);
+        return;
+    }
     with_op(L.A, [&](auto op) {
         launch(pdl_, k_cheb_step<T, decltype(op)>, row_blocks(L.A.threads()), TH, s_, op, b,
                xin, L.dinv.p, c1, c2, L.d.p, xout, done);
@@ -1916,6 +2121,14 @@ void SolverImpl::enqueue_residual(MgLevel<T>& L, const T* b, const T* x) {
             return;
         }
     }
+    if (L.A.pair) {
+        const int gp = row_blocks(pair_threads(L.n));
+        if (L.A.K == 8)
+            launch(pdl_, k_residual_pair<T, 8>, gp, TH, s_, L.A.sview(), b, x, L.r.p, done);
+        else
+            launch(pdl_, k_residual_pair<T, 14>, gp, TH, s_, L.A.sview(), b, x, L.r.p, done);
+        return;
+    }
     with_op(L.A, [&](auto op) {
         launch(pdl_, k_residual<T, decltype(op)>, row_blocks(L.A.threads()), TH, s_, op, b, x,
                L.r.p, done);
@@ -1928,10 +2141,10 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     if (l == H.levels.size()) {
         int64_t n = H.ncoarse;
         if (b == H.cb.p)
-            launch(pdl_, k_gemv<T, true>, blocks_for(n * 32, TH), TH, s_, n, dense_ld(n),
-                   H.inv.p, b, H.cx.p, done);
+            launch(pdl_, k_gemv_rows<T>, (int)std::min<int64_t>(n, NUM_SMS * 8), TH, s_, n,
+                   dense_ld(n), H.inv.p, b, H.cx.p, done);
         else
-            launch(pdl_, k_gemv<T, false>, blocks_for(n * 32, TH), TH, s_, n, dense_ld(n),
+            launch(pdl_, k_gemv<T>, blocks_for(n * 32, TH), TH, s_, n, dense_ld(n),
                    H.inv.p, b, H.cx.p, done);
         FG_CHECK_LAUNCH();
         mark("coarsest dense solve n=" + std::to_string(n));
@@ -2000,15 +2213,32 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     return xa;
 }
 
+// q = A p with the partials of p.q (FP64).
+void SolverImpl::enqueue_spmv_pq() {
+    Scalars* sc = sc_.p;
+    if (op64_.pair) {
+        const int gp = row_blocks(pair_threads(n_));
+        if (op64_.K == 8)
+            launch(pdl_, k_pcg_spmv_pq_pair<8>, gp, TH, s_, op64_.sview(), p_.p, q_.p,
+                   partial_.p, sc);
+        else
+            launch(pdl_, k_pcg_spmv_pq_pair<14>, gp, TH, s_, op64_.sview(), p_.p, q_.p,
+                   partial_.p, sc);
+    } else {
+        with_op(op64_, [&](auto op) {
+            launch(pdl_, k_pcg_spmv_pq<decltype(op)>, row_blocks(op64_.threads()), TH, s_, op,
+                   p_.p, q_.p, partial_.p, sc);
+        });
+    }
+}
+
 void SolverImpl::enqueue_iteration() {
     int64_t n = n_;
     launches_ += 7;
     Scalars* sc = sc_.p;
     bool mixed = opt_.precision == FEMGPU_MIXED;
     const int nbq = row_blocks(op64_.threads()), nbn = row_blocks(n);
-    with_op(op64_, [&](auto op) {
-        launch(pdl_, k_pcg_spmv_pq<decltype(op)>, nbq, TH, s_, op, p_.p, q_.p, partial_.p, sc);
-    });
+    enqueue_spmv_pq();
     mark("pcg q = A p, p.q partials (fp64)");
     launch(pdl_, k_finish<FinPq>, 1, TH, s_, partial_.p, nbq, FinPq{sc});
     mark("pcg alpha");
@@ -2159,7 +2389,7 @@ void SolverImpl::precondition(const double* d_r, double* d_z) {
     if (direct_ && sparse_) {
         sparse_->solve(d_r, d_z, s_);
     } else if (direct_) {
-        k_gemv<double, false><<<blocks_for(n_ * 32, TH), TH, 0, s_>>>(n_, n_, dense_inv_.p, d_r, d_z,
+        k_gemv<double><<<blocks_for(n_ * 32, TH), TH, 0, s_>>>(n_, n_, dense_inv_.p, d_r, d_z,
                                                                done_zero_.p);
     } else if (opt_.precision == FEMGPU_MIXED) {
         k_convert<double, float><<<blocks_for(n_, TH), TH, 0, s_>>>(n_, d_r, r32_.p);
@@ -2191,7 +2421,7 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
             if (sparse_) {
                 sparse_->solve(rhs, sol, s_);
             } else {
-                k_gemv<double, false><<<blocks_for(n * 32, TH), TH, 0, s_>>>(
+                k_gemv<double><<<blocks_for(n * 32, TH), TH, 0, s_>>>(
                     n, n, dense_inv_.p, rhs, sol, done_zero_.p);
             }
         };
@@ -2410,31 +2640,16 @@ void SolverImpl::kernel_time(int which, int reps, double* ms, double* bytes) {
     if (reps < 1) reps = 1;
     bool mixed = opt_.precision == FEMGPU_MIXED;
     FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
+    // The kernels the solve launches (the same dispatch), with done = 0.
     auto launch = [&]() {
         if (which == 1) {
-            with_op(op64_, [&](auto op) {
-                k_pcg_spmv_pq<<<row_blocks(op64_.threads()), TH, 0, s_>>>(op, p_.p, q_.p,
-                                                                          partial_.p, sc_.p);
-            });
+            enqueue_spmv_pq();
         } else if (mixed) {
             MgLevel<float>& L = H32_.levels.at(0);
-            int gs = row_blocks(L.A.threads());
-            if (L.A.bulk)
-                k_stencil_tiles<8, true><<<tile_grid(L.n), BULK_TH, tile_smem<true>(), s_>>>(
-                    L.A.sview(), L.b.p, L.xa.p, L.dinv.p, 0.5f, 0.5f, L.d.p, L.xb.p,
-                    done_zero_.p, &sc_.p->bulk_timeout, wait_limit);
-            else
-                with_op(L.A, [&](auto op) {
-                    k_cheb_step<float><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5f,
-                                                          0.5f, L.d.p, L.xb.p, done_zero_.p);
-                });
+            enqueue_step(L, L.b.p, L.xa.p, 0.5f, 0.5f, L.xb.p);
         } else {
             MgLevel<double>& L = H64_.levels.at(0);
-            int gs = row_blocks(L.A.threads());
-            with_op(L.A, [&](auto op) {
-                k_cheb_step<double><<<gs, TH, 0, s_>>>(op, L.b.p, L.xa.p, L.dinv.p, 0.5, 0.5,
-                                                       L.d.p, L.xb.p, done_zero_.p);
-            });
+            enqueue_step(L, L.b.p, L.xa.p, 0.5, 0.5, L.xb.p);
         }
     };
     if (which == 0 && (mixed ? H32_.levels.empty() : H64_.levels.empty()))

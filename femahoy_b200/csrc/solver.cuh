@@ -40,7 +40,9 @@ struct Operator {
     bool unrolled = false;  // the compile-time-K kernel (K = 8 or 14), chosen by timing
     bool half = false;      // the stencil's products read its FP16 copy (hcoef, hscale)
     bool bulk = false;      // its smoothing steps and residuals stream tiles by bulk copies
-    double probe_ms[3] = {0, 0, 0};  // the timed product: runtime K, compile-time K, tiles
+    bool pair = false;      // the compile-time-K kernels with 2 rows per thread, chosen by timing
+    // The timed product: runtime K, compile-time K, tiles, 2 rows per thread.
+    double probe_ms[4] = {0, 0, 0, 0};
     int64_t n = 0, nnz = 0;
     Sell<T> sell;
     int K = 0;
@@ -269,6 +271,7 @@ class SolverImpl {
     template <class T>
     void enqueue_residual(MgLevel<T>& L, const T* b, const T* x);
     void enqueue_iteration();
+    void enqueue_spmv_pq();
     void build_loop_graph();
     // Runs PCG iterations on the device until convergence, max_iter, a NaN or a cancel.
     void run_device_loop(const volatile int* cancel);
