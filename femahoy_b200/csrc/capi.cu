@@ -446,13 +446,18 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             o.values = options->values;
             o.tiles = options->tiles;
             o.axes = options->axes ? options->axes : 7;
+            o.stencil = options->stencil;
         }
+        require(o.stencil >= 0 && o.stencil <= 4,
+                "stencil is 0 (autotuned), 1 (runtime K), 2 (compile-time K), 3 (2 rows per "
+                "thread) or 4 (marching planes)");
         require(o.tiles >= 0 && o.tiles <= 2, "tiles is 0 (autotuned), 1 (off) or 2 (on)");
         require(o.axes >= 1 && o.axes <= 7, "axes is a mask of the axes x (1), y (2), z (4)");
         require(o.values >= 0 && o.values <= 2, "values is 0 (default), 1 (FP32) or 2 (FP16)");
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
-        require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32,
-                "the SELL chunk height must be 8, 16 or 32");
+        require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32 ||
+                    o.sell_c == 64,
+                "the SELL chunk height must be 8, 16, 32 or 64");
         require(o.degree >= 0 && o.degree <= 16, "the Chebyshev degree must be 1 to 16");
         require(o.format == 0 || o.format == 1, "the format is 0 (stencil where possible) or 1");
         int64_t n = a->m.n;

@@ -43,6 +43,18 @@ struct StencilView {
     const T* __restrict__ coef;
 };
 
+// The plane frame of a box level's stencil for the marching kernels (solver.cu
+// k_stencil_march): rows z P + j, T rows of a plane per block, `chunk` planes per block.
+struct MarchGeom {
+    int P;       // the plane stride: the first offset after the largest gap of the offsets
+    int s1;      // off[0, s1) are in-plane, off[s1, K) cross-plane (P + delta, delta in [0, H])
+    int H;       // the halo: the largest in-plane offset and cross-plane delta
+    int planes;  // ceil(n / P)
+    int chunk;   // planes per block
+    int tiles;   // blocks per plane: ceil(P / T)
+    int T;       // rows of a plane per block = threads per block
+};
+
 template <class T>
 struct SellOp {
     SellView<T> v;

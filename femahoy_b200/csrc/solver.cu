@@ -655,6 +655,234 @@ __global__ void __launch_bounds__(BULK_TH, 2)
             if (pending[s]) mbar_wait(&bar[s], parity[s], BULK_SPIN);
 }
 
+// ------------------------------------------------------------------ stencil planes, marching
+// The stencil product of a box level with every gather from shared memory. The sorted offsets
+// of a box grid in grid order fall into 2 groups around their largest gap: in-plane offsets
+// (at most about 1 row of a plane, nx + 1) and cross-plane ones P + delta, where P is the first
+// offset after the gap and 0 <= delta <= H. A block takes T consecutive rows j0 + t (t < T,
+// j0 + t < P) of each plane of the frame of stride P (rows z P + j) and marches z over a chunk
+// of planes. Shared memory holds the windows [j0 - H, j0 + T + H) of x of the planes z - 1, z,
+// z + 1 and [j0 - H, j0 + T) of the K coefficient arrays of the planes z - 1 and z, each loaded
+// as a plain range of rows: a window's rows past the plane's end are the next plane's, which is
+// what the product reads there, and rows outside [0, n) load as 0. Row i = z P + j0 + t reads
+// the upper terms' c_k[i] from plane z's window and x[i + o] from plane z's (in-plane o) or
+// z + 1's (cross-plane) x window, the lower terms' c_k[i - o] and x[i - o] from plane z's or
+// z - 1's windows. The next plane's windows and rows (b, D^-1, d) are loaded into registers
+// while this plane computes. Each row's sum is StencilOpK's: the same fused multiply-adds in the
+// same order, and a window's 0 at a missing neighbour is the 0 of StencilOpK's predicates (the
+// coefficient of a missing neighbour is 0 too), so the bits are those of the 1-row kernels.
+// Exact for any level whose in-plane offsets and cross-plane distances are at most H; the host
+// builds the geometry (march_geometry) only when 2 H <= T.
+// Threads per block at most: 1024 for the FP32 K = 8 kernels (52-62 registers), 512 for the
+// others (their next-plane registers take up to 128 without spilling).
+template <class T, int K>
+constexpr int MARCH_TMAX = sizeof(T) == 4 && K == 8 ? 1024 : 512;
+
+template <class T, int K>
+__host__ __device__ inline size_t march_smem(int Tn, int H) {
+    return ((size_t)3 * (Tn + 2 * H) + (size_t)2 * K * (Tn + H)) * sizeof(T);
+}
+
+template <class T, int K, bool STEP>
+__global__ void __launch_bounds__(MARCH_TMAX<T, K>)
+    k_stencil_march(StencilView<T> v, MarchGeom g, const T* __restrict__ b,
+                    const T* __restrict__ xin, const T* __restrict__ dinv, T c1, T c2,
+                    T* __restrict__ d, T* __restrict__ out, const int* __restrict__ done) {
+    pdl_wait();
+    if (*done) return;
+    extern __shared__ __align__(16) unsigned char march_raw[];
+    T* const X = reinterpret_cast<T*>(march_raw);
+    const int Tn = blockDim.x, H = g.H, t = threadIdx.x;
+    const int WX = Tn + 2 * H, WC = Tn + H;
+    T* const C = X + 3 * WX;
+    const int j0 = (blockIdx.x % g.tiles) * Tn;
+    const int z0 = (blockIdx.x / g.tiles) * g.chunk;
+    const int z1 = min(z0 + g.chunk, g.planes);
+    const int64_t n = v.n, P = g.P;
+    const bool own = j0 + t < P;
+    // Window loads: element t and t + Tn of the window that starts at row q P + j0 - H.
+    auto load_x = [&](int q, T r[2]) {
+        const int64_t base = (int64_t)q * P + j0 - H;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int idx = t + e * Tn;
+            const int64_t gi = base + idx;
+            r[e] = (idx < WX && gi >= 0 && gi < n) ? __ldg(xin + gi) : (T)0;
+        }
+    };
+    auto store_x = [&](int q, const T r[2]) {
+        T* dst = X + ((q + 3) % 3) * WX;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int idx = t + e * Tn;
+            if (idx < WX) dst[idx] = r[e];
+        }
+    };
+    auto load_c = [&](int q, T r[K][2]) {
+        const int64_t base = (int64_t)q * P + j0 - H;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int idx = t + e * Tn;
+                const int64_t gi = base + idx;
+                r[k][e] = (idx < WC && gi >= 0 && gi < n)
+                              ? __ldg(v.coef + (size_t)k * v.ld + gi)
+                              : (T)0;
+            }
+    };
+    auto store_c = [&](int q, const T r[K][2]) {
+        T* dst = C + ((q + 2) % 2) * K * WC;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int idx = t + e * Tn;
+                if (idx < WC) dst[k * WC + idx] = r[k][e];
+            }
+    };
+    auto load_rows = [&](int q, T& bo, T& dio, T& dpo) {
+        const int64_t i = (int64_t)q * P + j0 + t;
+        const bool ok = own && i < n;
+        bo = ok ? __ldg(b + i) : (T)0;
+        dio = STEP && ok ? __ldg(dinv + i) : (T)0;
+        dpo = STEP && ok ? d[i] : (T)0;
+    };
+    {
+        T r[2];
+        load_x(z0 - 1, r);
+        store_x(z0 - 1, r);
+        load_x(z0, r);
+        store_x(z0, r);
+        load_x(z0 + 1, r);
+        store_x(z0 + 1, r);
+        T c[K][2];
+        load_c(z0 - 1, c);
+        store_c(z0 - 1, c);
+        load_c(z0, c);
+        store_c(z0, c);
+    }
+    T bo, dio, dpo;
+    load_rows(z0, bo, dio, dpo);
+    __syncthreads();
+    for (int z = z0; z < z1; ++z) {
+        const bool more = z + 1 < z1;
+        T px[2], pc[K][2], nb = 0, ndi = 0, ndp = 0;
+        if (more) {
+            load_x(z + 2, px);
+            load_c(z + 1, pc);
+            load_rows(z + 1, nb, ndi, ndp);
+        }
+        const int64_t i = (int64_t)z * P + j0 + t;
+        if (own && i < n) {
+            const T* X0 = X + (z % 3) * WX + H + t;
+            const T* Xm = X + ((z + 2) % 3) * WX + H + t;
+            const T* Xp = X + ((z + 1) % 3) * WX + H + t;
+            const T* C0 = C + (z % 2) * K * WC + H + t;
+            const T* Cm = C + ((z + 1) % 2) * K * WC + H + t;
+            T acc = C0[0] * X0[0];
+#pragma unroll
+            for (int k = 1; k < K; ++k) {
+                const int o = v.off[k];
+                const T cu = C0[k * WC];
+                T xu, cl, xl;
+                if (k < g.s1) {
+                    xu = X0[o];
+                    cl = C0[k * WC - o];
+                    xl = X0[-o];
+                } else {
+                    const int dl = o - g.P;
+                    xu = Xp[dl];
+                    cl = Cm[k * WC - dl];
+                    xl = Xm[-dl];
+                }
+                acc = fmadd(cu, xu, acc);
+                acc = fmadd(cl, xl, acc);
+            }
+            if (STEP) {
+                const T dd = cheb_update(bo, acc, dio, dpo, c1, c2);
+                d[i] = dd;
+                out[i] = X0[0] + dd;
+            } else {
+                out[i] = bo - acc;
+            }
+        }
+        __syncthreads();
+        if (more) {
+            store_x(z + 2, px);
+            store_c(z + 1, pc);
+            bo = nb;
+            dio = ndi;
+            dpo = ndp;
+        }
+        __syncthreads();
+    }
+}
+
+// The plane frame of a stencil level for k_stencil_march, or false (not a K = 8 or 14 stencil,
+// halo too wide, or shared memory too small). The threads per block: the plane's rows split
+// evenly into blocks of at most 1024 (K = 8) or 512 (K = 14) rows; the chunk of planes per block
+// such that all blocks are resident at once.
+template <class T, int K>
+static bool march_frame(const Operator<T>& op, MarchGeom* g) {
+    const std::vector<int64_t>& o = op.off;  // sorted, o[0] = 0
+    int gap = 0;
+    for (int k = 1; k + 1 < K; ++k)
+        if (o[k + 1] - o[k] > o[gap + 1] - o[gap]) gap = k;
+    const int s1 = gap + 1;
+    const int64_t P = o[s1];
+    const int64_t H = std::max(o[s1 - 1], o[K - 1] - P);
+    const int64_t tmax = MARCH_TMAX<T, K>;
+    const int64_t tiles = (P + tmax - 1) / tmax;
+    const int64_t Tn = ((P + tiles - 1) / tiles + 31) / 32 * 32;
+    if (P >= 0x7fffffff || 2 * H > Tn || Tn > tmax) return false;
+    const size_t smem = march_smem<T, K>((int)Tn, (int)H);
+    if (smem > 227 * 1024) return false;
+    FG_CUDA(cudaFuncSetAttribute(k_stencil_march<T, K, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FG_CUDA(cudaFuncSetAttribute(k_stencil_march<T, K, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, dev = 0, sms = 0;
+    FG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stencil_march<T, K, true>,
+                                                          (int)Tn, smem));
+    FG_CUDA(cudaGetDevice(&dev));
+    FG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return false;
+    const int64_t planes = (op.n + P - 1) / P;
+    const int64_t chunks = std::max<int64_t>(1, std::min<int64_t>(planes, (int64_t)per_sm * sms / tiles));
+    g->P = (int)P;
+    g->s1 = s1;
+    g->H = (int)H;
+    g->planes = (int)planes;
+    g->chunk = (int)((planes + chunks - 1) / chunks);
+    g->tiles = (int)tiles;
+    g->T = (int)Tn;
+    return true;
+}
+
+template <class T>
+static bool march_geometry(const Operator<T>& op, MarchGeom* g) {
+    if (!op.stencil || op.half) return false;
+    if (op.K == 8) return march_frame<T, 8>(op, g);
+    if (op.K == 14) return march_frame<T, 14>(op, g);
+    return false;
+}
+
+// A Chebyshev step (STEP) or a residual by the marching kernel.
+template <class T, bool STEP>
+static void launch_march(bool pdl, const Operator<T>& op, cudaStream_t s, const T* b,
+                         const T* xin, const T* dinv, T c1, T c2, T* d, T* out,
+                         const int* done) {
+    const MarchGeom& g = op.mg;
+    const int grid = g.tiles * ((g.planes + g.chunk - 1) / g.chunk);
+    if (op.K == 8)
+        launch_smem(pdl, k_stencil_march<T, 8, STEP>, grid, g.T, march_smem<T, 8>(g.T, g.H), s,
+                    op.sview(), g, b, xin, dinv, c1, c2, d, out, done);
+    else
+        launch_smem(pdl, k_stencil_march<T, 14, STEP>, grid, g.T, march_smem<T, 14>(g.T, g.H),
+                    s, op.sview(), g, b, xin, dinv, c1, c2, d, out, done);
+}
+
 // bc = P^T r as a gather over the rows of R = P^T (multigrid.rs:166, sparse.rs:223-230).
 template <class T>
 __global__ void k_restrict(int64_t nc, const int64_t* __restrict__ ptr,
@@ -891,16 +1119,23 @@ __device__ __forceinline__ void block_partial(double a, double b, double* __rest
     }
 }
 
+// The threads of a finishing block: 1024, so that the ~8,000 partial pairs of the finest level
+// are read about 8 per thread with all loads in flight (1 L2 round trip instead of 32).
+constexpr int FIN_TH = 1024;
+
 template <class Fin>
-__global__ void __launch_bounds__(TH) k_finish(const double* __restrict__ partial, int nblocks,
-                                                Fin fin) {
+__global__ void __launch_bounds__(FIN_TH) k_finish(const double* __restrict__ partial,
+                                                    int nblocks, Fin fin) {
     pdl_wait();
     if (fin.skip()) return;
-    __shared__ double sa[TH / 32], sb[TH / 32];
+    __shared__ double sa[FIN_TH / 32], sb[FIN_TH / 32];
+    const double2* pp = reinterpret_cast<const double2*>(partial);
     double a = 0, b = 0;
-    for (int k = threadIdx.x; k < nblocks; k += TH) {
-        a += partial[2 * k];
-        b += partial[2 * k + 1];
+#pragma unroll 8
+    for (int k = threadIdx.x; k < nblocks; k += FIN_TH) {
+        const double2 v = pp[k];
+        a += v.x;
+        b += v.y;
     }
     for (int o = 16; o; o >>= 1) {
         a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -912,13 +1147,14 @@ __global__ void __launch_bounds__(TH) k_finish(const double* __restrict__ partia
         sb[w] = b;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double ta = 0, tb = 0;
-        for (int k = 0; k < TH / 32; ++k) {
-            ta += sa[k];
-            tb += sb[k];
+    if (w == 0) {
+        // The warps' sums by a second butterfly (a fixed order: the same bits every time).
+        double ta = lane < FIN_TH / 32 ? sa[lane] : 0.0, tb = lane < FIN_TH / 32 ? sb[lane] : 0.0;
+        for (int o = 16; o; o >>= 1) {
+            ta += __shfl_xor_sync(0xffffffffu, ta, o);
+            tb += __shfl_xor_sync(0xffffffffu, tb, o);
         }
-        fin(ta, tb);
+        if (lane == 0) fin(ta, tb);
     }
 }
 
@@ -1310,13 +1546,21 @@ static double time_best(F&& launch, int warm, int rounds, cudaStream_t s) {
 // A stencil level: the runtime-K or the compile-time-K product kernel (the same bits), by timing
 // the residual.
 template <class T>
-static void tune_operator(Operator<T>* op, cudaStream_t s) {
+static void tune_operator(Operator<T>* op, int force, cudaStream_t s) {
     if (!op->stencil || (op->K != 8 && op->K != 14)) return;
+    if (force > 0) {
+        // The kernel asked for, or the next lower one that the level can take.
+        op->march = force >= 4 && march_geometry(*op, &op->mg);
+        op->pair = !op->march && force >= 3 && !op->half;
+        op->unrolled = force >= 2;
+        return;
+    }
     const std::array<int64_t, 5> key{0, (int64_t)sizeof(T), op->K, log2_of(op->n), op->half};
     int v = 0;
     if (tune_lookup(key, &v)) {
         op->unrolled = v != 0;
         op->pair = v == 2;
+        op->march = v == 3 && march_geometry(*op, &op->mg);
         return;
     }
     int64_t n = op->n;
@@ -1350,10 +1594,23 @@ static void tune_operator(Operator<T>* op, cudaStream_t s) {
             },
             5, 3, s);
     }
-    const double best = std::min({op->probe_ms[0], op->probe_ms[1], op->probe_ms[3]});
-    op->pair = op->probe_ms[3] == best;
-    op->unrolled = op->pair || op->probe_ms[1] == best;
-    tune_store(key, op->pair ? 2 : op->unrolled ? 1 : 0);
+    // The plane-marching kernels.
+    op->probe_ms[4] = 1e30;
+    op->march = false;
+    if (march_geometry(*op, &op->mg)) {
+        op->probe_ms[4] = time_best(
+            [&] {
+                launch_march<T, false>(false, *op, s, b.p, x.p, nullptr, (T)0, (T)0, nullptr,
+                                       r.p, done.p);
+            },
+            5, 3, s);
+    }
+    const double best =
+        std::min({op->probe_ms[0], op->probe_ms[1], op->probe_ms[3], op->probe_ms[4]});
+    op->march = op->probe_ms[4] == best;
+    op->pair = !op->march && op->probe_ms[3] == best;
+    op->unrolled = op->march || op->pair || op->probe_ms[1] == best;
+    tune_store(key, op->march ? 3 : op->pair ? 2 : op->unrolled ? 1 : 0);
 }
 
 // A SELL level: the rows per slice (C = 16, 32 or 64; a warp reads 1 slice of 32 rows, 2 of 16,
@@ -1454,8 +1711,10 @@ static void tune_tiles(Operator<float>* op, int mode, cudaStream_t s) {
     cudaEventDestroy(e1);
     op->probe_ms[2] = best;
     if (fetch(timeout.p, s)) return;
-    const double direct =
-        op->pair ? op->probe_ms[3] : op->unrolled ? op->probe_ms[1] : op->probe_ms[0];
+    const double direct = op->march  ? op->probe_ms[4]
+                          : op->pair   ? op->probe_ms[3]
+                          : op->unrolled ? op->probe_ms[1]
+                                         : op->probe_ms[0];
     op->bulk = mode == 2 || best < direct;
 }
 
@@ -1473,9 +1732,9 @@ double lambda_max(const Operator<T>& A, const double* dg, cudaStream_t s,
         with_op(A, [&](auto op) {
             k_power_step<<<nb, TH, 0, s>>>(op, v.p, dg, w.p, partial.p);
         });
-        k_finish<<<1, TH, 0, s>>>(partial.p, nb, FinTwo{out.p});
+        k_finish<<<1, FIN_TH, 0, s>>>(partial.p, nb, FinTwo{out.p});
         k_norm2<<<nv, TH, 0, s>>>(n, w.p, partial.p);
-        k_finish<<<1, TH, 0, s>>>(partial.p, nv, FinTwo{out.p + 2});
+        k_finish<<<1, FIN_TH, 0, s>>>(partial.p, nv, FinTwo{out.p + 2});
         k_scale_into<<<blocks_for(n, TH), TH, 0, s>>>(n, w.p, out.p + 2, v.p);
         FG_CHECK_LAUNCH();
         if (it >= 12) {
@@ -1567,10 +1826,14 @@ static std::string describe_op(const Operator<T>& op) {
         std::snprintf(buf, sizeof buf, "sell C=%d nnz=%lld", op.sell.C, (long long)op.nnz);
     } else {
         std::snprintf(buf, sizeof buf,
-                      "stencil K=%d %s%s (probe %.1f / %.1f / %.1f us)%s nnz=%lld", op.K,
+                      "stencil K=%d %s%s (probe %.1f / %.1f / %.1f / %.1f us)%s nnz=%lld", op.K,
                       op.half ? "fp16 " : "",
-                      op.pair ? "unrolled, 2 rows per thread" : op.unrolled ? "unrolled" : "loop",
+                      op.march  ? "marching planes"
+                      : op.pair ? "unrolled, 2 rows per thread"
+                      : op.unrolled ? "unrolled"
+                                    : "loop",
                       op.probe_ms[0] * 1e3, op.probe_ms[1] * 1e3, op.probe_ms[3] * 1e3,
+                      op.probe_ms[4] < 1e29 ? op.probe_ms[4] * 1e3 : 0.0,
                       op.bulk ? ", steps from bulk-copied tiles" : "", (long long)op.nnz);
     }
     return buf;
@@ -1718,7 +1981,7 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
     {
         PhaseTimer t{this, "outer operator and autotuner", s_};
         make_operator<double>(a_, C, opt_.format == 0, &op64_, s_);
-        tune_operator(&op64_, s_);
+        tune_operator(&op64_, opt_.stencil, s_);
         if (!opt_.sell_c) tune_sell(a_, &op64_, s_);
     }
     if (u.kind == FEMGPU_UNKNOWNS_GRID) {
@@ -1939,7 +2202,7 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         }
         {
             PhaseTimer t{this, "autotuner", s_};
-            tune_operator(&lv.A, s_);
+            tune_operator(&lv.A, opt_.stencil, s_);
             if (!opt_.sell_c) tune_sell(d, &lv.A, s_);
             if constexpr (std::is_same<T, float>::value)
                 if (l == 0) tune_tiles(&lv.A, opt_.tiles, s_);
@@ -2094,6 +2357,11 @@ void SolverImpl::enqueue_step(MgLevel<T>& L, const T* b, const T* xin, T c1, T c
             return;
         }
     }
+    if (L.A.march) {
+        launch_march<T, true>(pdl_, L.A, s_, b, xin, (const T*)L.dinv.p, c1, c2, L.d.p, xout,
+                              done);
+        return;
+    }
     if (L.A.pair) {
         const int gp = row_blocks(pair_threads(L.n));
         if (L.A.K == 8)
@@ -2120,6 +2388,11 @@ void SolverImpl::enqueue_residual(MgLevel<T>& L, const T* b, const T* x) {
                         0.f, (float*)nullptr, L.r.p, done, &sc_.p->bulk_timeout, wait_limit);
             return;
         }
+    }
+    if (L.A.march) {
+        launch_march<T, false>(pdl_, L.A, s_, b, x, (const T*)nullptr, (T)0, (T)0, (T*)nullptr,
+                               L.r.p, done);
+        return;
     }
     if (L.A.pair) {
         const int gp = row_blocks(pair_threads(L.n));
@@ -2240,19 +2513,19 @@ void SolverImpl::enqueue_iteration() {
     const int nbq = row_blocks(op64_.threads()), nbn = row_blocks(n);
     enqueue_spmv_pq();
     mark("pcg q = A p, p.q partials (fp64)");
-    launch(pdl_, k_finish<FinPq>, 1, TH, s_, partial_.p, nbq, FinPq{sc});
+    launch(pdl_, k_finish<FinPq>, 1, FIN_TH, s_, partial_.p, nbq, FinPq{sc});
     mark("pcg alpha");
     launch(pdl_, k_pcg_update, nbn, TH, s_, n, x_.p, r_.p, p_.p, q_.p, mixed ? r32_.p : nullptr,
                                      partial_.p, sc);
     mark("pcg x, r update, r.r partials");
-    launch(pdl_, k_finish<FinUpdate>, 1, TH, s_, partial_.p, nbn, FinUpdate{sc, tol});
+    launch(pdl_, k_finish<FinUpdate>, 1, FIN_TH, s_, partial_.p, nbn, FinUpdate{sc, tol});
     FG_CHECK_LAUNCH();
     mark("pcg stopping test");
     if (mixed) {
         zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
         launch(pdl_, k_pcg_dots<float>, nbn, TH, s_, n, r_.p, zf_, q_.p, 1, 0, partial_.p, sc);
         mark("pcg r.z, z.q partials");
-        launch(pdl_, k_finish<FinDots>, 1, TH, s_, partial_.p, nbn, FinDots{sc, 1, 0});
+        launch(pdl_, k_finish<FinDots>, 1, FIN_TH, s_, partial_.p, nbn, FinDots{sc, 1, 0});
         mark("pcg beta");
         launch(pdl_, k_pcg_p<float>, nbn, TH, s_, n, zf_, p_.p, sc, 0);
         mark("pcg p = z + beta p");
@@ -2260,7 +2533,7 @@ void SolverImpl::enqueue_iteration() {
         zd_ = enqueue_vcycle<double>(H64_, 0, r_.p);
         launch(pdl_, k_pcg_dots<double>, nbn, TH, s_, n, r_.p, zd_, q_.p, 0, 0, partial_.p, sc);
         mark("pcg r.z partials");
-        launch(pdl_, k_finish<FinDots>, 1, TH, s_, partial_.p, nbn, FinDots{sc, 0, 0});
+        launch(pdl_, k_finish<FinDots>, 1, FIN_TH, s_, partial_.p, nbn, FinDots{sc, 0, 0});
         mark("pcg beta");
         launch(pdl_, k_pcg_p<double>, nbn, TH, s_, n, zd_, p_.p, sc, 0);
         mark("pcg p = z + beta p");
@@ -2429,14 +2702,14 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         apply(b_.p, x_.p);
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
             SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p, nullptr, partial_.p);
-        k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
+        k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                    FinResidual0{sc_.p});
         apply(r_.p, t_.p);
         k_add<<<blocks_for(n, TH), TH, 0, s_>>>(n, t_.p, x_.p);
         FG_CHECK_LAUNCH();
         k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
             SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p, nullptr, partial_.p);
-        k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
+        k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                    FinResidual0{sc_.p});
         FG_CHECK_LAUNCH();
         FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
@@ -2460,7 +2733,7 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         k_pcg_residual<<<row_blocks(op64_.threads()), TH, 0, s_>>>(
             op, b_.p, x_.p, r_.p, mixed ? r32_.p : nullptr, partial_.p);
     });
-    k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(op64_.threads()), FinResidual0{sc_.p});
+    k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(op64_.threads()), FinResidual0{sc_.p});
     FG_CHECK_LAUNCH();
     launches_ += 5;  // this residual and its sum, r.z and its sum, and p = z  // this residual, and r.z and p = z after the first cycle
     FG_CUDA(cudaMemcpyAsync(h_sc_, sc_.p, sizeof(Scalars), cudaMemcpyDeviceToHost, s_));
@@ -2477,13 +2750,13 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
         zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
         k_pcg_dots<float><<<row_blocks(n), TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 1, partial_.p,
                                                         sc_.p);
-        k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(n), FinDots{sc_.p, 1, 1});
+        k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(n), FinDots{sc_.p, 1, 1});
         k_pcg_p<float><<<row_blocks(n), TH, 0, s_>>>(n, zf_, p_.p, sc_.p, 1);
     } else {
         zd_ = enqueue_vcycle<double>(H64_, 0, r_.p);
         k_pcg_dots<double><<<row_blocks(n), TH, 0, s_>>>(n, r_.p, zd_, q_.p, 0, 1, partial_.p,
                                                          sc_.p);
-        k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(n), FinDots{sc_.p, 0, 1});
+        k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(n), FinDots{sc_.p, 0, 1});
         k_pcg_p<double><<<row_blocks(n), TH, 0, s_>>>(n, zd_, p_.p, sc_.p, 1);
     }
     FG_CHECK_LAUNCH();
@@ -2500,7 +2773,7 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
             // from it, and then the solve restarts from x (iterative refinement).
             k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
                 SellOp<double>{A64_.view()}, b_.p, x_.p, t_.p, nullptr, partial_.p);
-            k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
+            k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                        FinResidual0{sc_.p});
             FG_CHECK_LAUNCH();
             launches_ += 2;
@@ -2513,12 +2786,12 @@ void SolverImpl::solve(const double* d_b, double* d_x, const volatile int* cance
             FG_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), s_));
             k_pcg_residual<<<row_blocks(A64_.nslices * A64_.C), TH, 0, s_>>>(
                 SellOp<double>{A64_.view()}, b_.p, x_.p, r_.p, r32_.p, partial_.p);
-            k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
+            k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(A64_.nslices * A64_.C),
                                        FinResidual0{sc_.p});
             zf_ = enqueue_vcycle<float>(H32_, 0, r32_.p);
             k_pcg_dots<float><<<row_blocks(n), TH, 0, s_>>>(n, r_.p, zf_, q_.p, 1, 1, partial_.p,
                                                             sc_.p);
-            k_finish<<<1, TH, 0, s_>>>(partial_.p, row_blocks(n), FinDots{sc_.p, 1, 1});
+            k_finish<<<1, FIN_TH, 0, s_>>>(partial_.p, row_blocks(n), FinDots{sc_.p, 1, 1});
             k_pcg_p<float><<<row_blocks(n), TH, 0, s_>>>(n, zf_, p_.p, sc_.p, 1);
             FG_CHECK_LAUNCH();
             launches_ += 5;

@@ -41,8 +41,10 @@ struct Operator {
     bool half = false;      // the stencil's products read its FP16 copy (hcoef, hscale)
     bool bulk = false;      // its smoothing steps and residuals stream tiles by bulk copies
     bool pair = false;      // the compile-time-K kernels with 2 rows per thread, chosen by timing
-    // The timed product: runtime K, compile-time K, tiles, 2 rows per thread.
-    double probe_ms[4] = {0, 0, 0, 0};
+    bool march = false;     // the plane-marching kernels (gathers from shared memory), by timing
+    MarchGeom mg{};
+    // The timed product: runtime K, compile-time K, tiles, 2 rows per thread, marching planes.
+    double probe_ms[5] = {0, 0, 0, 0, 0};
     int64_t n = 0, nnz = 0;
     Sell<T> sell;
     int K = 0;
@@ -220,6 +222,7 @@ struct Options {
     int values = 0;  // mixed form's stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
     int tiles = 0;   // finest FP32 stencil steps by bulk-copied tiles: 0 tuned, 1 off, 2 on
     int axes = 7;    // the axes that the coarsening halves (bits x, y, z)
+    int stencil = 0; // stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
 };
 
 class SolverImpl {

@@ -115,11 +115,12 @@ class Options:
     values: int = 0  # mixed stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
     tiles: int = 0   # finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on
     axes: int = 0    # the axes the coarsening halves (bits x 1, y 2, z 4; 0: all)
+    stencil: int = 0  # stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
 
     def _c(self):
         return L.Options_t(self.precision, self.degree, self.lower, self.sell_c, 0, self.coarsest,
                            self.max_levels, self.graph, self.format, self.tail, self.launch,
-                           self.values, self.tiles, self.axes)
+                           self.values, self.tiles, self.axes, self.stencil)
 
 
 def unknowns_c(unknowns: "Unknowns", keep: list) -> L.Unknowns_t:

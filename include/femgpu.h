@@ -218,7 +218,8 @@ typedef struct femgpu_options {
     double lower;         /* Chebyshev interval lower end as a fraction of lambda_max; 0 = default */
     int sell_c;           /* SELL chunk height (rows per slice; a warp reads 32 rows): 0 =
                              autotuned, 16, 32 or 64 by timing each level's product, once per
-                             size class (log2 rows, entries per row, element size) */
+                             size class (log2 rows, entries per row, element size); or 8, 16,
+                             32, 64 */
     int sell_sigma;       /* SELL sorting window in rows: 0 = autotuned */
     int coarsest;         /* the largest level that the dense coarse solve takes; 0 = 5000 (the
                              reference's COARSEST is 3000, multigrid.rs:94; the dense inverse
@@ -248,6 +249,12 @@ typedef struct femgpu_options {
                              the reference's rule): 4 coarsens only z, for meshes extruded in
                              layers from an unstructured footprint, whose points are on z planes
                              but not on x or y planes (prism.rs) */
+    int stencil;          /* the product kernel of the stencil levels (K = 8 or 14): 0 = the
+                             autotuner's choice by timing, once per size class; 1 = K read at run
+                             time, 2 = K known at compile time, 3 = 2 adjacent rows per thread,
+                             4 = marching planes (every gather from shared memory). A kernel that
+                             a level cannot take falls back to the next lower one. All give the
+                             same bits. */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end

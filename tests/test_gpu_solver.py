@@ -295,6 +295,31 @@ def test_tile_kernels_give_the_same_bits(precision):
     assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
 
 
+@pytest.mark.parametrize("precision", [fg.MIXED, fg.FP64])
+def test_stencil_kernels_give_the_same_bits(precision):
+    """Every stencil product kernel (K at run time, K at compile time, 2 rows per thread,
+    marching planes with all gathers from shared memory) sums each row in the same order, so the
+    solves are the same bits whichever the autotuner picks (the 56^3 cube: levels of 180,000,
+    24,000 and 3,400 rows, K = 8 and 14)."""
+    h = mg.heat_cube(56, seed=5)
+    A, rhs, _ = _system(h)
+    xs, its = [], []
+    for kernel, text in ((1, "loop"), (2, "unrolled"), (3, "2 rows per thread"),
+                         (4, "marching planes")):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision,
+                      options=fg.Options(precision=precision, stencil=kernel, tiles=1,
+                                         degree=2)).with_tol(1e-10)
+        assert text in s.describe()
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1e-10
+        xs.append(x)
+        its.append(st.iterations)
+    assert len(set(its)) == 1
+    for x in xs[1:]:
+        assert np.array_equal(xs[0].view(np.uint64), x.view(np.uint64))
+
+
 def test_fp16_stencil_coefficients_solve_to_the_same_tolerance():
     """The mixed form with the stencil levels' coefficients in FP16 (scaled by each level's
     largest): the V-cycle changes by about 2^-11 relative, and flexible CG still reaches the
