@@ -53,15 +53,47 @@ __global__ void __launch_bounds__(TH)
         const int i = t % kb, j = t / kb;
         if (i >= j) F[(p0 + i) + (p0 + j) * m] = D[i][j];
     }
-    for (int64_t r = p0 + kb + threadIdx.x; r < m; r += blockDim.x) {
-        double x[PANEL];
-        for (int j = 0; j < kb; ++j) {
-            double v = F[r + (p0 + j) * m];
-            for (int q = 0; q < j; ++q) v -= x[q] * D[j][q];
-            x[j] = v / D[j][j];
-            F[r + (p0 + j) * m] = x[j];
-        }
+}
+
+// The 32 x 32 lower triangle of the factored diagonal block of panel p0 (kb columns) in shared
+// memory, padded with the identity past kb, so that the unrolled solves below need no branch.
+__device__ __forceinline__ void load_panel_triangle(const double* __restrict__ F, int64_t m,
+                                                    int64_t p0, int kb,
+                                                    double (*D)[PANEL + 1]) {
+    for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
+        const int i = t % PANEL, j = t / PANEL;
+        double v = 0.0;
+        if (i < kb && j < kb && i >= j)
+            v = F[(p0 + i) + (p0 + j) * m];
+        else if (i == j)
+            v = 1.0;
+        D[i][j] = v;
     }
+}
+
+// The panel's rows below its diagonal block: L21 = A21 L11^-T, 1 thread per row, the row's 32
+// values in registers (all loads in flight at once), the sums in column order.
+constexpr int ROWS_TH = 128;
+__global__ void __launch_bounds__(ROWS_TH)
+    k_panel_rows(double* __restrict__ F, int64_t m, int64_t p0, int kb) {
+    __shared__ double D[PANEL][PANEL + 1];
+    load_panel_triangle(F, m, p0, kb, D);
+    __syncthreads();
+    const int64_t r = p0 + kb + blockIdx.x * (int64_t)ROWS_TH + threadIdx.x;
+    if (r >= m) return;
+    double x[PANEL];
+#pragma unroll
+    for (int j = 0; j < PANEL; ++j) x[j] = j < kb ? F[r + (p0 + j) * m] : 0.0;
+#pragma unroll
+    for (int j = 0; j < PANEL; ++j) {
+        double v = x[j];
+#pragma unroll
+        for (int q = 0; q < j; ++q) v -= x[q] * D[j][q];
+        x[j] = v / D[j][j];
+    }
+#pragma unroll
+    for (int j = 0; j < PANEL; ++j)
+        if (j < kb) F[r + (p0 + j) * m] = x[j];
 }
 
 // D = A B + D on the FP64 tensor cores: A 8 x 4 (row), B 4 x 8 (column), D 8 x 8; lane l holds
@@ -144,26 +176,28 @@ __global__ void __launch_bounds__(TH)
 }
 
 // Rows [b0, b0 + kb) of W for its columns 0..ncols: W_b = L_bb^-1 W_b (the block's triangle in
-// shared memory), 1 thread per column.
-__global__ void __launch_bounds__(TH)
+// shared memory), 1 thread per column, the column's 32 values in registers.
+__global__ void __launch_bounds__(ROWS_TH)
     k_trsm_rows(double* __restrict__ W, const double* __restrict__ L, int64_t n, int64_t b0,
                 int kb, int64_t ncols) {
     __shared__ double D[PANEL][PANEL + 1];
-    for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
-        const int i = t % PANEL, j = t / PANEL;
-        D[i][j] = (i < kb && j < kb && i >= j) ? L[(b0 + i) + (b0 + j) * n] : 0.0;
-    }
+    load_panel_triangle(L, n, b0, kb, D);
     __syncthreads();
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < ncols;
-         c += (int64_t)gridDim.x * blockDim.x) {
-        double y[PANEL];
-        for (int i = 0; i < kb; ++i) {
-            double v = W[(b0 + i) + c * n];
-            for (int j = 0; j < i; ++j) v -= D[i][j] * y[j];
-            y[i] = v / D[i][i];
-            W[(b0 + i) + c * n] = y[i];
-        }
+    const int64_t c = blockIdx.x * (int64_t)ROWS_TH + threadIdx.x;
+    if (c >= ncols) return;
+    double y[PANEL];
+#pragma unroll
+    for (int i = 0; i < PANEL; ++i) y[i] = i < kb ? W[(b0 + i) + c * n] : 0.0;
+#pragma unroll
+    for (int i = 0; i < PANEL; ++i) {
+        double v = y[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) v -= D[i][j] * y[j];
+        y[i] = v / D[i][i];
     }
+#pragma unroll
+    for (int i = 0; i < PANEL; ++i)
+        if (i < kb) W[(b0 + i) + c * n] = y[i];
 }
 
 // X = W^T W (W lower triangular, column-major n x n): 1 block per 64 x 64 tile on or below the
@@ -234,6 +268,9 @@ void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0
         const int kb = (int)std::min<int64_t>(PANEL, k - p0);
         k_panel<<<1, TH, 0, s>>>(F, m, p0, kb, diag0, col0, status);
         const int64_t t0 = p0 + kb;
+        if (t0 < m)
+            k_panel_rows<<<(unsigned)((m - t0 + ROWS_TH - 1) / ROWS_TH), ROWS_TH, 0, s>>>(F, m, p0,
+                                                                                      kb);
         if (t0 < m) {
             const int64_t T = (m - t0 + TILE - 1) / TILE;
             k_syrk_update<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(F, m, t0, p0, kb);
@@ -270,7 +307,8 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
     for (int64_t b0 = 0; b0 < n; b0 += PANEL) {
         const int kb = (int)std::min<int64_t>(PANEL, n - b0);
         const int64_t ncols = b0 + kb;
-        k_trsm_rows<<<blocks_for(ncols, TH), TH, 0, s>>>(W.p, L.p, n, b0, kb, ncols);
+        k_trsm_rows<<<(unsigned)((ncols + ROWS_TH - 1) / ROWS_TH), ROWS_TH, 0, s>>>(W.p, L.p, n, b0,
+                                                                                    kb, ncols);
         const int64_t rows = n - b0 - kb;
         if (rows > 0) {
             dim3 grid((unsigned)((rows + TILE - 1) / TILE), (unsigned)((ncols + TILE - 1) / TILE));
