@@ -58,6 +58,11 @@ def args():
                    help="Chebyshev interval's lower end as a fraction of lambda_max (0: 0.3)")
     p.add_argument("--coarsest", type=int, default=0,
                    help="the largest level the dense coarse solve takes (0: 3000, the reference's)")
+    p.add_argument("--stencil", type=int, default=0,
+                   help="stencil product kernel: 0 tuned, 1 runtime K, 2 compile-time K, "
+                        "3 2 rows per thread, 4 marching planes")
+    p.add_argument("--l2", type=int, default=0,
+                   help="1: the coarsest inverse persisting in L2")
     p.add_argument("--tiles", type=int, default=0,
                    help="finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on")
     p.add_argument("--values", type=int, default=0,
@@ -438,6 +443,7 @@ def run_ours(opt, rank, world, local):
                                          graph=opt.graph, tail=opt.tail,
                                          degree=opt.degree, launch=opt.launch,
                                          values=opt.values, tiles=opt.tiles,
+                                         stencil=opt.stencil, l2=opt.l2,
                                          coarsest=opt.coarsest,
                                          lower=opt.lower)).with_tol(tol)
         return s, time.perf_counter() - t
@@ -565,6 +571,11 @@ def run_ours(opt, rank, world, local):
                       "e2e": error_vs_oracle(x_e2e, ref),
                       "oracle_residual": {"same_tol": ref["residual"],
                                           "tight": ref["residual_tight"]},
+                      # How far the reference's own solution at the same tolerance is from
+                      # the converged one: the scale of any two solutions' distance at 1e-8.
+                      "oracle_same_tol_vs_1e-12": float(
+                          np.linalg.norm(ref["x_tol"] - ref["x_tight"])
+                          / np.linalg.norm(ref["x_tight"])),
                       "definition": "|x - x_oracle|_2 / |x_oracle|_2; the oracle's PCG-MG "
                                     "(the reference's algorithm) at the same tolerance, the "
                                     "same continued to 1e-12, and (<= 40,000 unknowns) its "

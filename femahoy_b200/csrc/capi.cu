@@ -447,7 +447,10 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             o.tiles = options->tiles;
             o.axes = options->axes ? options->axes : 7;
             o.stencil = options->stencil;
+            o.l2 = options->l2;
         }
+        require(o.l2 == 0 || o.l2 == 1, "l2 is 0 (plain loads) or 1 (the coarsest inverse "
+                                        "persisting in L2)");
         require(o.stencil >= 0 && o.stencil <= 4,
                 "stencil is 0 (autotuned), 1 (runtime K), 2 (compile-time K), 3 (2 rows per "
                 "thread) or 4 (marching planes)");

@@ -1,4 +1,5 @@
 // Dense Cholesky factors and inverses on the FP64 tensor cores (dense_factor.cuh).
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -279,11 +280,22 @@ void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0
     FG_CHECK_LAUNCH();
 }
 
-void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
+                   std::vector<std::pair<const char*, double>>* stages) {
     const int64_t n = a.n;
+    auto t0 = std::chrono::steady_clock::now();
+    auto stage = [&](const char* name) {
+        if (!stages) return;
+        FG_CUDA(cudaStreamSynchronize(s));
+        const auto t1 = std::chrono::steady_clock::now();
+        stages->emplace_back(name, std::chrono::duration<double>(t1 - t0).count());
+        t0 = t1;
+    };
     DevBuf<int64_t> ptr;
     DevBuf<uint32_t> idx;
     DevBuf<double> val, diag(n), L(n * n), W(n * n);
+    inv->alloc(n * n);
+    stage("buffers");
     ptr.upload(a.ptr.data(), n + 1, s);
     idx.upload(a.idx.data(), a.nnz(), s);
     val.upload(a.val.data(), a.nnz(), s);
@@ -292,6 +304,7 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
     DevBuf<unsigned long long> status(1);
     FG_CUDA(cudaMemsetAsync(status.p, 0xff, sizeof(unsigned long long), s));
     dense_partial_cholesky(L.p, n, n, diag.p, 0, status.p, s);
+    stage("factor");
     const unsigned long long bad = fetch(status.p, s);
     if (bad != ~0ull) {
         const double d = fetch(diag.p + bad, s);
@@ -316,11 +329,12 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s) {
                                            W.p + b0, n, rows, ncols, kb);
         }
     }
-    inv->alloc(n * n);
+    stage("L^-1");
     const int64_t T = (n + TILE - 1) / TILE;
     k_gram_lower<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(W.p, n, inv->p);
     FG_CHECK_LAUNCH();
     FG_CUDA(cudaStreamSynchronize(s));
+    stage("W^T W");
 }
 
 }  // namespace femgpu

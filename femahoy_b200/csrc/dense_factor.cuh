@@ -9,6 +9,8 @@
 // (cholesky.rs:22, 173-181): the smallest such column is recorded in `status`.
 #pragma once
 #include <cstdint>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "hierarchy.hpp"
@@ -24,7 +26,9 @@ void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0
 
 // The inverse of the SPD matrix `a` (host CSR, n small) on the device, FP64, n x n (symmetric,
 // so row- and column-major alike). Fails with the reference's text when a pivot is not
-// positive (the column in the natural order).
-void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s);
+// positive (the column in the natural order). With `stages`, the host seconds of its stages
+// (buffers, factor, L^-1, W^T W), each until its device work finished.
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
+                   std::vector<std::pair<const char*, double>>* stages = nullptr);
 
 }  // namespace femgpu

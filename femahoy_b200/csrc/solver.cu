@@ -942,6 +942,31 @@ static void launch_transfer(const OffsetTransfer<T>& M, const T* in, T* out, int
 // row. PADDED: ld = dense_ld(n) and b padded to it (the coarsest level of a hierarchy, whose
 // right side is the hierarchy's own padded vector); else scalar loads (the direct method, and a
 // hierarchy of no smoothed level, whose right side is the caller's vector).
+// A launch with programmatic dependent launch (pdl) and, if `win`, an L2 access policy window.
+template <class... KArgs, class... Args>
+static void launch_window(bool pdl, const cudaAccessPolicyWindow* win, void (*kernel)(KArgs...),
+                          int grid, int block, cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.stream = s;
+    cudaLaunchAttribute attrs[2]{};
+    unsigned na = 0;
+    if (pdl) {
+        attrs[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attrs[na].val.programmaticStreamSerializationAllowed = 1;
+        ++na;
+    }
+    if (win) {
+        attrs[na].id = cudaLaunchAttributeAccessPolicyWindow;
+        attrs[na].val.accessPolicyWindow = *win;
+        ++na;
+    }
+    cfg.attrs = na ? attrs : nullptr;
+    cfg.numAttrs = na;
+    FG_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
+
 // The coarsest product x = M b (padded M and b): 1 block per row at a time.
 template <class T>
 __global__ void __launch_bounds__(TH)
@@ -1787,6 +1812,7 @@ SolverImpl::SolverImpl() {
 }
 
 SolverImpl::~SolverImpl() {
+    if (l2_window_) cudaCtxResetPersistingL2Cache();
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
     if (h_sc_) cudaFreeHost(h_sc_);
@@ -2262,11 +2288,13 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         FG_CUDA(cudaStreamSynchronize(s_));
     }
     // The coarsest level: its inverse from a dense Cholesky factor on the device.
-    PhaseTimer t_dense{this, "coarsest dense inverse", s_};
+    std::optional<PhaseTimer> t_dense;
+    t_dense.emplace(this, "coarsest dense inverse", s_);
     const HostCsr last = download_csr(*mats.back(), s_);
     H->ncoarse = last.n;
     DevBuf<double> inv64;
-    dense_inverse(last, &inv64, s_);
+    std::vector<std::pair<const char*, double>> stages;
+    dense_inverse(last, &inv64, s_, &stages);
     // Rows at leading dimension dense_ld(n), the padding 0; the right side padded with zeros.
     const int64_t ld = dense_ld(last.n);
     H->inv.alloc(last.n * ld);
@@ -2277,7 +2305,30 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
     H->cb.zero(s_);
     FG_CUDA(cudaStreamSynchronize(s_));
     H->cx.alloc(last.n);
+    t_dense.reset();
+    for (const auto& st : stages) phase(std::string("coarsest: ") + st.first, st.second);
     build_tail(H, opt_.tail, s_);
+    if (opt_.l2 == 1) {
+        // The inverse is read once per V-cycle (96 MB in FP32 for the 4,913-row level of the
+        // 128^3 box) and evicted by the finer levels' streams in between; a persisting window
+        // keeps it in L2 across cycles.
+        int dev = 0, maxp = 0, maxw = 0;
+        FG_CUDA(cudaGetDevice(&dev));
+        FG_CUDA(cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev));
+        FG_CUDA(cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+        if (maxp > 0 && maxw > 0) {
+            const size_t want = std::min<size_t>(H->inv.bytes(), (size_t)maxp);
+            size_t cur = 0;
+            FG_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+            if (cur < want) FG_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+            l2win_.base_ptr = H->inv.p;
+            l2win_.num_bytes = std::min<size_t>(H->inv.bytes(), (size_t)maxw);
+            l2win_.hitRatio = (float)std::min(1.0, (double)want / (double)l2win_.num_bytes);
+            l2win_.hitProp = cudaAccessPropertyPersisting;
+            l2win_.missProp = cudaAccessPropertyStreaming;
+            l2_window_ = true;
+        }
+    }
 }
 
 void SolverImpl::build_multigrid(HostLevel level, const HostRect* pfirst,
@@ -2414,8 +2465,9 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     if (l == H.levels.size()) {
         int64_t n = H.ncoarse;
         if (b == H.cb.p)
-            launch(pdl_, k_gemv_rows<T>, (int)std::min<int64_t>(n, NUM_SMS * 8), TH, s_, n,
-                   dense_ld(n), H.inv.p, b, H.cx.p, done);
+            launch_window(pdl_, l2_window_ ? &l2win_ : nullptr, k_gemv_rows<T>,
+                          (int)std::min<int64_t>(n, NUM_SMS * 8), TH, s_, n, dense_ld(n),
+                          H.inv.p, b, H.cx.p, done);
         else
             launch(pdl_, k_gemv<T>, blocks_for(n * 32, TH), TH, s_, n, dense_ld(n),
                    H.inv.p, b, H.cx.p, done);

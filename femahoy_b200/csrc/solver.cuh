@@ -9,6 +9,7 @@
 #include "common.cuh"
 #include "block3.cuh"
 #include "coarsen.cuh"
+#include "dense_factor.cuh"
 #include "hierarchy.hpp"
 #include "ops.cuh"
 #include "sell.cuh"
@@ -101,7 +102,6 @@ template <class T>
 void make_operator(const DevCsr& d, int C, bool allow, Operator<T>* out, cudaStream_t s);
 
 // Setup helpers shared by the solvers (solver.cu).
-void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s);
 void upload_csr(const HostCsr& h, DevCsr* d, cudaStream_t s);
 HostCsr download_csr(const DevCsr& d, cudaStream_t s);
 HostRect transpose(const HostRect& p);
@@ -223,6 +223,7 @@ struct Options {
     int tiles = 0;   // finest FP32 stencil steps by bulk-copied tiles: 0 tuned, 1 off, 2 on
     int axes = 7;    // the axes that the coarsening halves (bits x, y, z)
     int stencil = 0; // stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
+    int l2 = 0;      // 1: the coarsest inverse persisting in L2
 };
 
 class SolverImpl {
@@ -288,6 +289,9 @@ class SolverImpl {
     cudaStream_t s_ = nullptr;
     Options opt_;
     bool direct_ = false;
+    // The persisting L2 window of the coarsest inverse's product (option l2), if any.
+    bool l2_window_ = false;
+    cudaAccessPolicyWindow l2win_{};
     int64_t n_ = 0;
     Sell<double> A64_;          // the matrix exactly (the true residual, the direct method)
     Operator<double> op64_;     // the FP64 operator of PCG

@@ -255,6 +255,10 @@ typedef struct femgpu_options {
                              4 = marching planes (every gather from shared memory). A kernel that
                              a level cannot take falls back to the next lower one. All give the
                              same bits. */
+    int l2;               /* 1 = keep the coarsest level's dense inverse resident in L2 (a
+                             persisting access window on its product; the process's persisting
+                             L2 limit is raised to the inverse's size, at most the device's
+                             maximum); 0 (default) = plain loads */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end
