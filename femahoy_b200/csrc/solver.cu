@@ -1827,7 +1827,8 @@ SolverImpl::~SolverImpl() {
 
 template <class T>
 size_t Hierarchy<T>::bytes() const {
-    size_t b = inv.bytes() + cb.bytes() + cx.bytes();
+    size_t b = inv.bytes() + cb.bytes() + cx.bytes() + cb64.bytes() + cx64.bytes() +
+               (sparse ? sparse->bytes() : 0);
     for (const auto& l : levels)
         b += l.A.bytes() + l.dinv.bytes() + l.pptr.bytes() + l.rptr.bytes() + l.pidx.bytes() +
              l.ridx.bytes() + l.pval.bytes() + l.rval.bytes() + l.Po.bytes() + l.Ro.bytes() +
@@ -1888,7 +1889,12 @@ std::string SolverImpl::describe() const {
                                   : "CSR");
             out += buf;
         }
-        std::snprintf(buf, sizeof buf, "coarsest n=%lld dense inverse\n", (long long)H.ncoarse);
+        if (H.sparse)
+            std::snprintf(buf, sizeof buf, "coarsest n=%lld %s", (long long)H.ncoarse,
+                          H.sparse->describe().c_str());
+        else
+            std::snprintf(buf, sizeof buf, "coarsest n=%lld dense inverse\n",
+                          (long long)H.ncoarse);
         out += buf;
         if (H.tail_from >= 0 && tail_on_) {
             std::snprintf(buf, sizeof buf,
@@ -2104,11 +2110,6 @@ void SolverImpl::sparse_direct(const HostCsr& h, const std::vector<double>& xyz)
 }
 
 void SolverImpl::dense_direct(const HostCsr& h) {
-    const int64_t LIMIT = 16384;
-    if (h.n > LIMIT)
-        throw Failure(FEMGPU_ERR_TOO_LARGE,
-                      "the direct solver of this library is a dense Cholesky factor on the device "
-                      "and holds at most 16384 unknowns: use multigrid");
     dense_inverse(h, &dense_inv_, s_);
 }
 
@@ -2144,7 +2145,7 @@ static void make_offset(const DevRect& M, OffsetTransfer<T>* out, cudaStream_t s
 template <class T>
 static void build_tail(Hierarchy<T>* H, int tail, cudaStream_t s) {
     H->tail_from = -1;
-    if (tail <= 0 || H->levels.empty()) return;
+    if (tail <= 0 || H->levels.empty() || H->sparse) return;
     const int64_t limit = tail;
     size_t from = 0;
     while (from < H->levels.size() && H->levels[from].n > limit) ++from;
@@ -2210,7 +2211,7 @@ static void build_tail(Hierarchy<T>* H, int tail, cudaStream_t s) {
 
 template <class T>
 void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vector<DevRect>& ps,
-                              Hierarchy<T>* H) {
+                              const HostLevel& coarsest, Hierarchy<T>* H) {
     size_t L = mats.size();
     H->levels.resize(L - 1);
     int C = opt_.sell_c ? opt_.sell_c : 32;
@@ -2286,6 +2287,28 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         lv.d.alloc(lv.n);
         lv.r.alloc(lv.n);
         FG_CUDA(cudaStreamSynchronize(s_));
+    }
+    if (mats.back()->n > DENSE_COARSEST_MAX) {
+        // The coarsest level's sparse factor, in the nested dissection order of its points'
+        // coordinates (multigrid.rs:124-131).
+        PhaseTimer t_sparse{this, "coarsest sparse factor", s_};
+        const HostCsr last = download_csr(*mats.back(), s_);
+        std::vector<double> xyz(3 * (size_t)last.n);
+        for (int64_t k = 0; k < last.n; ++k)
+            for (int d = 0; d < 3; ++d)
+                xyz[3 * k + d] = coarsest.planes[d][coarsest.points[k][d]];
+        H->ncoarse = last.n;
+        H->sparse = std::make_unique<SparseFactor>();
+        H->sparse->factor(last, xyz.data(), s_);
+        H->cb.alloc(last.n);
+        H->cb.zero(s_);
+        H->cx.alloc(last.n);
+        if (!std::is_same<T, double>::value) {
+            H->cb64.alloc(last.n);
+            H->cx64.alloc(last.n);
+        }
+        FG_CUDA(cudaStreamSynchronize(s_));
+        return;
     }
     // The coarsest level: its inverse from a dense Cholesky factor on the device.
     std::optional<PhaseTimer> t_dense;
@@ -2383,16 +2406,16 @@ void SolverImpl::build_multigrid(HostLevel level, const HostRect* pfirst,
         ps.push_back(std::move(p));
         grid = std::move(coarse);
     }
-    if ((size_t)mats.back()->n > 16384)
-        throw Failure(FEMGPU_ERR_TOO_LARGE,
-                      "the coarsest level has more than 16384 unknowns: the grid does not coarsen");
+    // The coarsest level's points, for the order of a sparse coarsest factor.
+    HostLevel last;
+    if (mats.back()->n > DENSE_COARSEST_MAX) last = grid_download(grid, s_);
     sizes_.clear();
     for (const DevCsr* m : mats) sizes_.push_back(m->n);
     if (opt_.precision == FEMGPU_MIXED) {
-        build_levels<float>(mats, ps, &H32_);
+        build_levels<float>(mats, ps, last, &H32_);
         r32_.alloc(n_);
     } else {
-        build_levels<double>(mats, ps, &H64_);
+        build_levels<double>(mats, ps, last, &H64_);
     }
 }
 
@@ -2462,6 +2485,23 @@ void SolverImpl::enqueue_residual(MgLevel<T>& L, const T* b, const T* x) {
 template <class T>
 const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     const int* done = &sc_.p->done;
+    if (l == H.levels.size() && H.sparse) {
+        // The sparse coarsest factor's 2 triangular solves in FP64 (the right side and the
+        // solution converted in the mixed form).
+        const int64_t n = H.ncoarse;
+        if constexpr (std::is_same<T, double>::value) {
+            H.sparse->solve(b, H.cx.p, s_);
+        } else {
+            k_convert<T, double><<<blocks_for(n, TH), TH, 0, s_>>>(n, b, H.cb64.p);
+            H.sparse->solve(H.cb64.p, H.cx64.p, s_);
+            k_convert<double, T><<<blocks_for(n, TH), TH, 0, s_>>>(n, H.cx64.p, H.cx.p);
+            launches_ += 2;
+        }
+        FG_CHECK_LAUNCH();
+        mark("coarsest sparse solve n=" + std::to_string(n));
+        launches_ += H.sparse->solve_launches();
+        return H.cx.p;
+    }
     if (l == H.levels.size()) {
         int64_t n = H.ncoarse;
         if (b == H.cb.p)

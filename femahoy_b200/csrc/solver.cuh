@@ -191,6 +191,11 @@ struct Hierarchy {
     int64_t ncoarse = 0;
     DevBuf<T> inv;  // the inverse of the coarsest matrix, n x n (symmetric)
     DevBuf<T> cb, cx;
+    // A coarsest level above DENSE_COARSEST_MAX unknowns (a grid that stops coarsening, e.g. the
+    // layers of an extruded footprint): its sparse multifrontal factor, as the reference's
+    // coarsest solve (multigrid.rs:130-131), applied in FP64.
+    std::unique_ptr<SparseFactor> sparse;
+    DevBuf<double> cb64, cx64;
     // The levels from `tail_from` down, and the coarsest solve, run as 1 cooperative kernel
     // (-1: none) of `tail_grid` blocks.
     int tail_from = -1, tail_grid = 0;
@@ -207,6 +212,9 @@ constexpr int DEVICE_COARSEST = 5000;
 // The direct method's dense inverse takes systems of up to this many unknowns; larger ones the
 // sparse multifrontal factor.
 constexpr int64_t DENSE_DIRECT = 4096;
+// The largest coarsest level that takes the dense inverse; a larger one (a grid that does not
+// coarsen further) takes the sparse factor.
+constexpr int64_t DENSE_COARSEST_MAX = 16384;
 
 struct Options {
     int precision = FEMGPU_FP64;
@@ -267,7 +275,7 @@ class SolverImpl {
     void build_multigrid(HostLevel level, const HostRect* pfirst, const HostCells* cells);
     template <class T>
     void build_levels(const std::vector<const DevCsr*>& mats, std::vector<DevRect>& ps,
-                      Hierarchy<T>* H);
+                      const HostLevel& coarsest, Hierarchy<T>* H);
     template <class T>
     const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b);
     template <class T>

@@ -397,6 +397,13 @@ void SparseFactor::solve(const double* b, double* x, cudaStream_t s) {
     FG_CHECK_LAUNCH();
 }
 
+size_t SparseFactor::solve_launches() const {
+    size_t c = 2;
+    for (int64_t h = 0; h <= height_; ++h)
+        if (level_at_[h + 1] > level_at_[h]) c += 2;
+    return c;
+}
+
 size_t SparseFactor::bytes() const {
     return fronts_.bytes() + work_.bytes() + y_.bytes() + perm_.bytes() + first_.bytes() +
            rows_ptr_.bytes() + rows_.bytes() + foff_.bytes() + zoff_.bytes() +

@@ -38,6 +38,8 @@ class SparseFactor {
     // x = A^-1 b, device arrays of n values (x may not alias b).
     void solve(const double* b, double* x, cudaStream_t s);
     int64_t n() const { return n_; }
+    // The kernels that 1 solve launches.
+    size_t solve_launches() const;
     size_t bytes() const;
     std::string describe() const;
     uint64_t entries() const { return entries_; }

@@ -227,7 +227,7 @@ int femgpu_transient_new(const femgpu_csr* k, const double* capacity, double dt,
         FG_CUDA(cudaStreamSynchronize(s));
         // heat.rs:697-703: Crossover::Unknowns(TRANSIENT_DIRECT_LIMIT), 40,000 in the reference;
         // the direct solver of this library holds at most 16,384 unknowns.
-        femgpu_crossover c{0, 16384, 0.0, 0, 0};
+        femgpu_crossover c{0, 40000, 0.0, 0, 0};  // TRANSIENT_DIRECT_LIMIT, solve.rs:24
         if (crossover) c = *crossover;
         int rc = femgpu_solver_new(&sub, unknowns, method, &c, options, &tr->solver);
         if (rc != FEMGPU_OK) {

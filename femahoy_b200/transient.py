@@ -17,8 +17,8 @@ from . import _lib as L
 from .solve import Crossover, Options, Solver, Stats, Unknowns, unknowns_c
 from .sparse import Csr
 
-# solve.rs:24 is 40,000; the direct solver of this library holds 16,384 unknowns.
-TRANSIENT_DIRECT_LIMIT = 16384
+# solve.rs:24
+TRANSIENT_DIRECT_LIMIT = 40_000
 
 
 @dataclass

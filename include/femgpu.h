@@ -197,8 +197,8 @@ typedef struct femgpu_unknowns {
 } femgpu_unknowns;
 
 /* solve.rs:28-39 `Crossover`: rule 0 = Unknowns(unknowns); 1 = Flops{flops, entries, flat} (the
- * sparse factor's figures of femgpu_symbolic_counts; a direct choice above 16,384 unknowns runs
- * multigrid, the direct solver here being dense). */
+ * sparse factor's figures of femgpu_symbolic_counts). A direct choice is solved directly: by a
+ * dense inverse up to 4,096 unknowns, by the sparse multifrontal factor above. */
 typedef struct femgpu_crossover {
     int rule;
     size_t unknowns;
@@ -309,8 +309,8 @@ int femgpu_hex_mass(size_t count, const double* sizes, const double* density, do
 /* The entries (with the diagonal) and the floating point operations of the sparse Cholesky
  * factor of `a` in the nested dissection order of the unknowns' points (order.rs:19-198,
  * symbolic.rs:41-183): the figures Crossover::Flops compares (solve.rs:108-118, 160-172), which
- * femgpu_solver_new applies. A direct choice above the dense direct solver's 16,384 unknowns runs
- * multigrid. No reference counterpart as an entry point: for checking the crossover. */
+ * femgpu_solver_new applies. No reference counterpart as an entry point: for checking the
+ * crossover. */
 int femgpu_symbolic_counts(const femgpu_csr* a, const femgpu_unknowns* unknowns,
                            uint64_t* entries, double* flops);
 /* The matrix of multigrid level `level` (>= 1) that the solver of (a, unknowns, cells) forms
@@ -510,8 +510,8 @@ typedef struct femgpu_energy {
 /* heat.rs:688-703: `k` the full conductivity matrix (femgpu_assemble, P1 heat), `capacity` the
  * lumped capacity of each point, `dt` the step, `free` the free points (increasing) and
  * `unknowns` their grid level, as for femgpu_solver_new (whose method, crossover and options
- * these are). A NULL crossover is Unknowns(16384): the reference's TRANSIENT_DIRECT_LIMIT is
- * 40,000 (solve.rs:24), and the direct solver of this library holds 16,384 unknowns. */
+ * these are). A NULL crossover is Unknowns(40000), the reference's TRANSIENT_DIRECT_LIMIT
+ * (solve.rs:24). */
 int femgpu_transient_new(const femgpu_csr* k, const double* capacity, double dt,
                          const int64_t* free, size_t nfree, const femgpu_unknowns* unknowns,
                          int method, const femgpu_crossover* crossover,
@@ -550,7 +550,8 @@ typedef struct femgpu_modes_stats {
 /* eigen.rs:81-177. `k` and `m` are the free-unknown submatrices of the stiffness and the mass
  * (the same pattern, as modes.rs:183-185 forms them; femgpu_assemble with FEMGPU_P2_ELASTIC and
  * FEMGPU_P2_MASS, then femgpu_csr_submatrix); `shift` NaN takes modes.rs:186-191's
- * -1e-8 mean(K_ii / M_ii). `unknowns`, `method`, `crossover` (NULL: Unknowns(16384)) and
+ * -1e-8 mean(K_ii / M_ii). `unknowns`, `method`, `crossover` (NULL: Unknowns(16384); the
+ * reference's modes pass Flops{infinity, 2.5e8, flat}, modes.rs:101-107) and
  * `options` are those of femgpu_solver_new for K - shift M. `values` gets `count` eigenvalues
  * ascending, `vectors` (NULL skips them) count x n M-orthonormal vectors. At most 64 modes; the
  * reference's texts for too many modes, non-convergence in 120 iterations and "cancelled"

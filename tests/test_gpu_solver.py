@@ -450,6 +450,37 @@ def test_extruded_mesh_with_z_coarsening(precision):
     assert _rel(x, xd) <= 1e-8
 
 
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_extruded_mesh_with_a_sparse_coarsest_level(precision):
+    """A footprint too large for the dense coarse solve: the z-only coarsening stops at 2 planes
+    of 3,025 points (18,150 unknowns, above the dense inverse's 16,384), and that level takes the
+    sparse multifrontal factor, as the reference's coarsest level always does
+    (multigrid.rs:124-131). The PCG solution equals the oracle's direct one."""
+    xyz, tets = mg.extruded(npoints=3025, layers=4, seed=7)
+    n = len(xyz)
+    coef = np.tile([1000.0, 0.3], (len(tets), 1))
+    fixed = np.repeat(xyz[:, 2] == 0.0, 3)
+    free = np.nonzero(~fixed)[0].astype(np.int64)
+    load = np.zeros(3 * n)
+    load[3 * np.nonzero(xyz[:, 2] == 1.0)[0] + 2] = -1e-3
+    K = fg.Csr.assemble(fg.P1_ELASTIC, xyz, tets, coef)
+    A = K.submatrix(free)
+    rhs = fg.reduced_rhs(K, load, np.zeros(3 * n), free)
+    planes, pts, comp = mg.level_of(xyz, free)
+    s = fg.Solver(A, fg.Unknowns.Grid(fg.Level(planes, pts, comp)), fg.Method.Multigrid,
+                  precision=precision,
+                  options=fg.Options(precision=precision, axes=4, coarsest=2000)).with_tol(1e-10)
+    assert s.levels()[-1] == 18150 and "sparse multifrontal factor" in s.describe()
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    assert st.true_residual <= 1.2e-10
+    Ko = oracle.pattern(3 * n, oracle.dof_elements(tets))
+    Ko.assemble(1, xyz, tets, coef)
+    xd, _ = oracle.direct_solve(Ko.submatrix(free), xyz[free // 3],
+                                Ko.reduced_rhs(load, np.zeros(3 * n), free))
+    assert _rel(x, xd) <= 1e-8
+
+
 def test_extruded_p2_mesh_with_z_coarsening():
     """P2 elasticity on the extruded footprint (the reference's prism meshes carry P2 tets,
     elastic_tet.rs): p-multigrid to the P1 corners, then z-only geometric levels; the solution
