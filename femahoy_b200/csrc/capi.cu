@@ -456,7 +456,9 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
                 "thread) or 4 (marching planes)");
         require(o.tiles >= 0 && o.tiles <= 2, "tiles is 0 (autotuned), 1 (off) or 2 (on)");
         require(o.axes >= 1 && o.axes <= 7, "axes is a mask of the axes x (1), y (2), z (4)");
-        require(o.values >= 0 && o.values <= 2, "values is 0 (default), 1 (FP32) or 2 (FP16)");
+        require(o.values >= 0 && o.values <= 3,
+                "values is 0 (default), 1 (FP32), 2 (FP16 stencil coefficients) or 3 (an FP16 "
+                "coarsest inverse)");
         require(o.precision == FEMGPU_FP64 || o.precision == FEMGPU_MIXED, "unknown precision");
         require(o.sell_c == 0 || o.sell_c == 8 || o.sell_c == 16 || o.sell_c == 32 ||
                     o.sell_c == 64,

@@ -190,6 +190,9 @@ struct Hierarchy {
     std::vector<MgLevel<T>> levels;  // all but the coarsest
     int64_t ncoarse = 0;
     DevBuf<T> inv;  // the inverse of the coarsest matrix, n x n (symmetric)
+    // The mixed form's FP16 copy of the inverse (values 3), divided by its largest entry.
+    DevBuf<__half> hinv;
+    float hscale = 1.0f;
     DevBuf<T> cb, cx;
     // A coarsest level above DENSE_COARSEST_MAX unknowns (a grid that stops coarsening, e.g. the
     // layers of an extruded footprint): its sparse multifrontal factor, as the reference's

@@ -112,7 +112,7 @@ class Options:
     format: int = 0  # 0: stencil where the level allows it, else SELL-C; 1: SELL-C only
     tail: int = 0    # > 0: levels of at most this many rows run as 1 fused kernel (0: none)
     launch: int = 0  # 0: programmatic dependent launch in the PCG loop; 1: plain launches
-    values: int = 0  # mixed stencil levels: 0 default, 1 FP32, 2 FP16 coefficients
+    values: int = 0  # mixed form: 0 default, 1 FP32, 2 FP16 stencils, 3 FP16 coarsest inverse
     tiles: int = 0   # finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on
     axes: int = 0    # the axes the coarsening halves (bits x 1, y 2, z 4; 0: all)
     stencil: int = 0  # stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march

@@ -240,7 +240,9 @@ typedef struct femgpu_options {
     int values;           /* the mixed form's stencil levels: 0 = the default, 1 = FP32
                              coefficients, 2 = FP16 coefficients scaled by the level's largest
                              (the products read about 0.6 of the bytes; the V-cycle changes by
-                             about 2^-11 relative) */
+                             about 2^-11 relative); 3 = FP32 coefficients and the coarsest
+                             level's dense inverse in FP16 scaled by its largest entry (its
+                             product reads half the bytes, sums in FP32) */
     int tiles;            /* the mixed form's finest stencil level (K = 8): 0 = the autotuner
                              chooses by timing whether its smoothing steps and residuals stream
                              each tile's own arrays into shared memory by bulk copies or read
@@ -369,9 +371,12 @@ void femgpu_solver_free(femgpu_solver* s);
  * can order its own work and CUDA events with it. No reference counterpart. */
 void* femgpu_solver_stream(const femgpu_solver* s);
 /* Times `reps` back-to-back launches of 1 kernel of the solve on the solver's stream with CUDA
- * events: which = 0 the finest Chebyshev smoothing step, 1 the FP64 operator product of PCG
- * (fused with p.q). Writes the mean device time of a launch (ms) and the algorithmic bytes of 1
- * launch (values, indices and vectors, each read or written once). No reference counterpart. */
+ * events and the solve's launch attributes: which = 0 the finest Chebyshev smoothing step (on a
+ * stencil level alternately on the level and on a second copy of its operator and vectors, so
+ * that each launch finds its data evicted from L2, as in a solve), 1 the FP64 operator product
+ * of PCG (fused with p.q). Writes the mean device time of a launch (ms) and the algorithmic
+ * bytes of 1 launch (values, indices and vectors, each read or written once). No reference
+ * counterpart. */
 int femgpu_solver_kernel_time(femgpu_solver* s, int which, int reps, double* ms, double* bytes);
 
 /* ---------------------------------------------------------------- serving */

@@ -342,6 +342,31 @@ def test_fp16_stencil_coefficients_solve_to_the_same_tolerance():
     assert "fp16" not in s.describe()
 
 
+def test_fp16_coarsest_inverse_solves_to_the_same_tolerance():
+    """The mixed form with the coarsest level's dense inverse in FP16 (scaled by its largest
+    entry; the product sums in FP32): the coarse correction changes by about 2^-11 relative, and
+    flexible CG still reaches the tolerance on the true FP64 residual in at most 1 more
+    iteration, near the oracle's direct solution. The FP64 form ignores the option."""
+    h = mg.heat_cube(40, seed=7)
+    A, rhs, Ao = _system(h)
+    its, xs = {}, {}
+    for values in (1, 3):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=fg.MIXED,
+                      options=fg.Options(precision=fg.MIXED, values=values,
+                                         coarsest=3000)).with_tol(1e-10)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1.2e-10
+        its[values] = st.iterations
+        xs[values] = x
+    assert its[3] <= its[1] + 1
+    assert _rel(xs[3], xs[1]) <= 1e-8
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=fg.FP64,
+                  options=fg.Options(precision=fg.FP64, values=3)).with_tol(1e-10)
+    x = np.zeros(A.n)
+    assert s.solve(rhs, x).true_residual <= 1.2e-10
+
+
 @pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
 def test_block_operators_match_sell_for_elasticity(precision):
     """Elasticity levels in 3x3-block form (each node's 3 rows share their block columns) solve
