@@ -2116,10 +2116,15 @@ void SolverImpl::create(const DevCsr& a, const femgpu_unknowns& u, int method,
     }
 }
 
-void SolverImpl::apply_degree(int degree) {
+void SolverImpl::apply_degree(int degree, int coarse) {
     const double lower = opt_.lower > 0 ? opt_.lower : 0.3;
-    for (auto& L : H32_.levels) chebyshev(L.lambda, degree, lower, &L.c1, &L.c2);
-    for (auto& L : H64_.levels) chebyshev(L.lambda, degree, lower, &L.c1, &L.c2);
+    if (coarse <= 0) coarse = degree;
+    for (size_t l = 0; l < H32_.levels.size(); ++l)
+        chebyshev(H32_.levels[l].lambda, l == 0 ? degree : coarse, lower, &H32_.levels[l].c1,
+                  &H32_.levels[l].c2);
+    for (size_t l = 0; l < H64_.levels.size(); ++l)
+        chebyshev(H64_.levels[l].lambda, l == 0 ? degree : coarse, lower, &H64_.levels[l].c1,
+                  &H64_.levels[l].c2);
     // The captured loop holds the coefficients as kernel arguments.
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
@@ -2127,9 +2132,10 @@ void SolverImpl::apply_degree(int degree) {
     graph_ = nullptr;
 }
 
-// Each candidate degree solves a fixed right side (k_seed) from x = 0 to 1e-4 twice; the second
-// solve's device time per decade of residual reduction decides. Degree 2 is tried first and
-// keeps a tie.
+// Each candidate (the finest level's degree, the coarser levels') solves a fixed right side
+// (k_seed) from x = 0 to 1e-4 twice; the second solve's device time per decade of residual
+// reduction decides. (2, 2) is tried first and keeps a tie; (2, 1) smooths the latency-bound
+// coarse levels once before and once after their correction.
 void SolverImpl::tune_degree() {
     const bool mixed = opt_.precision == FEMGPU_MIXED;
     const size_t nlevels = mixed ? H32_.levels.size() : H64_.levels.size();
@@ -2140,9 +2146,9 @@ void SolverImpl::tune_degree() {
     else if (mixed ? H32_.levels[0].A.block3 : H64_.levels[0].A.block3)
         kind = -1;
     const std::array<int64_t, 5> key{2, mixed ? 4 : 8, kind, log2_of(n_), (int64_t)nlevels};
-    int degree = 2;
+    int degree = 22;  // 10 * (the finest level's degree) + the coarser levels'
     if (tune_lookup(key, &degree)) {
-        if (degree != 2) apply_degree(degree);
+        if (degree != 22) apply_degree(degree / 10, degree % 10);
         return;
     }
     DevBuf<double> rhs(n_);
@@ -2153,8 +2159,9 @@ void SolverImpl::tune_degree() {
     tol = 1e-4;
     max_iter = 200;
     double best = 1e30;
-    for (int cand : {2, 1, 3}) {
-        apply_degree(cand);
+    for (int cand : {22, 11, 33, 21}) {
+        if (cand % 10 != cand / 10 && nlevels < 2) continue;
+        apply_degree(cand / 10, cand % 10);
         double cost = 1e30;
         for (int rep = 0; rep < 2; ++rep) {
             FG_CUDA(cudaMemsetAsync(x_.p, 0, n_ * sizeof(double), s_));
@@ -2174,7 +2181,7 @@ void SolverImpl::tune_degree() {
     }
     tol = tol0;
     max_iter = max0;
-    apply_degree(degree);
+    apply_degree(degree / 10, degree % 10);
     tune_store(key, degree);
 }
 

@@ -294,7 +294,8 @@ class SolverImpl {
     void dense_direct(const HostCsr& a);
     // The Chebyshev degree of every level (1, 2 or 3) by timed trial solves, per size class.
     void tune_degree();
-    void apply_degree(int degree);
+    // The Chebyshev degree of the finest level and of the coarser ones (0: the same).
+    void apply_degree(int degree, int coarse = 0);
     void sparse_direct(const HostCsr& a, const std::vector<double>& xyz);
 
     cudaStream_t s_ = nullptr;

@@ -211,7 +211,8 @@ typedef struct femgpu_crossover {
 typedef struct femgpu_options {
     int precision;        /* FEMGPU_FP64 or FEMGPU_MIXED */
     int degree;           /* Chebyshev degree of each pre- and post-smoothing; 0 = autotuned:
-                             1, 2 or 3 by timed trial solves (device time per decade of residual
+                             1, 2 or 3 on every level, or 2 on the finest and 1 on the coarser
+                             ones, by timed trial solves (device time per decade of residual
                              reduction), once per size class (the finest level's kind and
                              log2 rows, the level count, the precision) and kept for the process;
                              a batch takes 2 */

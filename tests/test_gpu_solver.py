@@ -245,7 +245,7 @@ def test_fused_coarse_levels_give_the_same_bits(kind, precision):
     for tail in (65536, 0):
         s = fg.Solver(A, _grid(p), fg.Method.Multigrid, precision=precision,
                       options=fg.Options(precision=precision, tail=tail, coarsest=200,
-                                         format=fmt))
+                                         format=fmt, degree=2))
         s = s.with_tol(1e-10)
         assert ("cooperative kernel" in s.describe()) == (tail > 0)
         x = np.zeros(A.n)
