@@ -182,67 +182,119 @@ __global__ void k_low_words(int64_t n, const uint64_t* __restrict__ keys,
         idx[k] = (uint32_t)(keys[k] & 0xffffffffu);
 }
 
-// Row i of C = A B: the products a_ij b_jk in A's row order, then B's, added into a table of the
-// row's columns kept sorted (binary search, shift to insert). The counting pass stores the
-// number of columns; the filling pass writes them with their sums at ptr[i]. A row with more
-// than CAP columns sets *overflow and is left out.
-template <int CAP, bool FILL>
-__global__ void __launch_bounds__(128)
-    k_spgemm(int64_t rows, const int64_t* __restrict__ aptr, const uint32_t* __restrict__ aidx,
-             const double* __restrict__ aval, const int64_t* __restrict__ bptr,
-             const uint32_t* __restrict__ bidx, const double* __restrict__ bval,
-             uint32_t* __restrict__ count, const int64_t* __restrict__ cptr,
-             uint32_t* __restrict__ cidx, double* __restrict__ cval, int* __restrict__ overflow) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < rows;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t col[CAP];
-        double acc[FILL ? CAP : 1];
-        int m = 0;
+// Row i of C = A B by 1 warp with the row's columns in a hash table in shared memory (SPG_TAB
+// slots, linear probing, a slot claimed by compare-and-swap): for each entry a_ij of A's row in
+// order, the lanes take B's row j, 32 entries at a time, and add a_ij b_jk into column k's
+// slot. B's row has distinct columns, so no 2 lanes meet in a slot within a step, and each
+// entry of C is summed in A's row order, whatever the lanes' timing (a slot's first product is
+// stored, not added to 0): the coarse operators are the same bits every time. The counting
+// pass counts the claimed slots;
+// the filling pass writes the row's columns increasing (each entry's rank among the row's
+// columns) with their sums at ptr[i]. A row of more than SPG_CAP columns sets *overflow.
+constexpr int SPG_TAB = 1024, SPG_CAP = 512, SPG_WARPS = 4;
+constexpr uint32_t SPG_EMPTY = 0xffffffffu;
+
+// Shared memory per warp: the table's keys, and for the filling pass its sums and the row's
+// columns compacted.
+template <bool FILL>
+constexpr size_t spg_smem() {
+    return (size_t)SPG_WARPS *
+           (SPG_TAB * sizeof(uint32_t) + (FILL ? SPG_TAB * sizeof(double) + SPG_CAP * 4 : 0));
+}
+
+template <bool FILL>
+__global__ void __launch_bounds__(32 * SPG_WARPS)
+    k_spgemm_warp(int64_t rows, const int64_t* __restrict__ aptr,
+                  const uint32_t* __restrict__ aidx, const double* __restrict__ aval,
+                  const int64_t* __restrict__ bptr, const uint32_t* __restrict__ bidx,
+                  const double* __restrict__ bval, uint32_t* __restrict__ count,
+                  const int64_t* __restrict__ cptr, uint32_t* __restrict__ cidx,
+                  double* __restrict__ cval, int* __restrict__ overflow) {
+    extern __shared__ __align__(16) unsigned char spg_raw[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* vals = reinterpret_cast<double*>(spg_raw) + (size_t)w * SPG_TAB;  // FILL only
+    uint32_t* keys = reinterpret_cast<uint32_t*>(
+                         spg_raw + (FILL ? (size_t)SPG_WARPS * SPG_TAB * sizeof(double) : 0)) +
+                     (size_t)w * SPG_TAB;
+    uint32_t* ck = reinterpret_cast<uint32_t*>(
+                       spg_raw + (size_t)SPG_WARPS * SPG_TAB * (sizeof(double) + 4)) +
+                   (size_t)w * SPG_CAP;  // FILL only
+    const int64_t nwarps = (int64_t)gridDim.x * SPG_WARPS;
+    for (int64_t i = blockIdx.x * (int64_t)SPG_WARPS + w; i < rows; i += nwarps) {
+        for (int t = lane; t < SPG_TAB; t += 32) keys[t] = SPG_EMPTY;
+        __syncwarp();
+        int claimed = 0;  // slots this lane claimed
         bool full = false;
-        for (int64_t ka = aptr[i]; ka < aptr[i + 1] && !full; ++ka) {
+        for (int64_t ka = aptr[i]; ka < aptr[i + 1]; ++ka) {
             const uint32_t j = aidx[ka];
             const double a = aval[ka];
-            for (int64_t kb = bptr[j]; kb < bptr[j + 1]; ++kb) {
+            const int64_t b0 = bptr[j], b1 = bptr[j + 1];
+            for (int64_t kb = b0 + lane; kb < b1 && !full; kb += 32) {
                 const uint32_t c = bidx[kb];
-                int lo = 0, hi = m;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (col[mid] < c)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
+                uint32_t h = (c * 2654435761u) >> (32 - 10);
+                for (int probes = 0;; ++probes) {
+                    if (probes == SPG_TAB) {
+                        full = true;
+                        break;
+                    }
+                    const uint32_t k = *(volatile uint32_t*)&keys[h];
+                    if (k == c) {
+                        if (FILL) vals[h] += a * bval[kb];
+                        break;
+                    }
+                    if (k == SPG_EMPTY) {
+                        const uint32_t old = atomicCAS(&keys[h], SPG_EMPTY, c);
+                        if (old == SPG_EMPTY) {
+                            if (FILL) vals[h] = a * bval[kb];
+                            ++claimed;
+                            break;
+                        }
+                        if (old == c) {
+                            if (FILL) vals[h] += a * bval[kb];
+                            break;
+                        }
+                    }
+                    h = (h + 1) & (SPG_TAB - 1);
                 }
-                if (lo < m && col[lo] == c) {
-                    if (FILL) acc[lo] += a * bval[kb];
-                    continue;
-                }
-                if (m == CAP) {
-                    full = true;
-                    break;
-                }
-                for (int t = m; t > lo; --t) {
-                    col[t] = col[t - 1];
-                    if (FILL) acc[t] = acc[t - 1];
-                }
-                col[lo] = c;
-                if (FILL) acc[lo] = a * bval[kb];
-                ++m;
             }
+            __syncwarp();
         }
+        int m = claimed;
+        for (int o = 16; o; o >>= 1) m += __shfl_xor_sync(0xffffffffu, m, o);
+        full = __any_sync(0xffffffffu, full) || m > SPG_CAP;
         if (full) {
-            atomicExch(overflow, 1);
-            if (!FILL) count[i] = 0;
+            if (lane == 0) {
+                atomicExch(overflow, 1);
+                if (!FILL) count[i] = 0;
+            }
+            __syncwarp();
             continue;
         }
         if (!FILL) {
-            count[i] = (uint32_t)m;
+            if (lane == 0) count[i] = (uint32_t)m;
         } else {
+            // The row's columns compacted, then each claimed slot's rank among them is its place
+            // in the output (the columns increasing).
+            int base = 0;
+            for (int t0 = 0; t0 < SPG_TAB; t0 += 32) {
+                const uint32_t c = keys[t0 + lane];
+                const bool p = c != SPG_EMPTY;
+                const unsigned bal = __ballot_sync(0xffffffffu, p);
+                if (p) ck[base + __popc(bal & ((1u << lane) - 1u))] = c;
+                base += __popc(bal);
+            }
+            __syncwarp();
             const int64_t at = cptr[i];
-            for (int t = 0; t < m; ++t) {
-                cidx[at + t] = col[t];
-                cval[at + t] = acc[t];
+            for (int t = lane; t < SPG_TAB; t += 32) {
+                const uint32_t c = keys[t];
+                if (c == SPG_EMPTY) continue;
+                int rank = 0;
+                for (int u = 0; u < m; ++u) rank += ck[u] < c;
+                cidx[at + rank] = c;
+                cval[at + rank] = vals[t];
             }
         }
+        __syncwarp();
     }
 }
 
@@ -261,36 +313,23 @@ void spgemm(int64_t rows, const int64_t* aptr, const uint32_t* aidx, const doubl
     DevBuf<uint32_t> count(rows > 0 ? rows : 1);
     DevBuf<int> overflow(1);
     overflow.zero(s);
-    const int blocks = blocks_for(rows, 128, NUM_SMS * 32);
-    // Tables of 96 columns fit the rows of the box grids (27 points, 3 components); a wider
-    // row (unstructured footprints) takes the 512-column form.
-    bool wide = false;
-    k_spgemm<96, false><<<blocks, 128, 0, s>>>(rows, aptr, aidx, aval, bptr, bidx, bval, count.p,
-                                               nullptr, nullptr, nullptr, overflow.p);
+    // 1 warp per row, the row's columns hashed in shared memory.
+    const int blocks = blocks_for(rows, SPG_WARPS, NUM_SMS * 16);
+    FG_CUDA(cudaFuncSetAttribute(k_spgemm_warp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)spg_smem<true>()));
+    k_spgemm_warp<false><<<blocks, 32 * SPG_WARPS, spg_smem<false>(), s>>>(
+        rows, aptr, aidx, aval, bptr, bidx, bval, count.p, nullptr, nullptr, nullptr, overflow.p);
     FG_CHECK_LAUNCH();
-    if (fetch(overflow.p, s)) {
-        wide = true;
-        overflow.zero(s);
-        k_spgemm<512, false><<<blocks, 128, 0, s>>>(rows, aptr, aidx, aval, bptr, bidx, bval,
-                                                    count.p, nullptr, nullptr, nullptr,
-                                                    overflow.p);
-        FG_CHECK_LAUNCH();
-        if (fetch(overflow.p, s))
-            throw Failure(FEMGPU_ERR_TOO_LARGE,
-                          "a row of a coarse operator has more than 512 entries");
-    }
+    if (fetch(overflow.p, s))
+        throw Failure(FEMGPU_ERR_TOO_LARGE, "a row of a coarse operator has more than 512 entries");
     cptr->alloc(rows + 1);
     exclusive_scan32(count.p, cptr->p, rows, s);
     int64_t nnz = fetch(cptr->p + rows, s);
     cidx->alloc(nnz > 0 ? nnz : 1);
     cval->alloc(nnz > 0 ? nnz : 1);
-    if (wide)
-        k_spgemm<512, true><<<blocks, 128, 0, s>>>(rows, aptr, aidx, aval, bptr, bidx, bval,
-                                                   nullptr, cptr->p, cidx->p, cval->p,
-                                                   overflow.p);
-    else
-        k_spgemm<96, true><<<blocks, 128, 0, s>>>(rows, aptr, aidx, aval, bptr, bidx, bval,
-                                                  nullptr, cptr->p, cidx->p, cval->p, overflow.p);
+    k_spgemm_warp<true><<<blocks, 32 * SPG_WARPS, spg_smem<true>(), s>>>(
+        rows, aptr, aidx, aval, bptr, bidx, bval, nullptr, cptr->p, cidx->p, cval->p,
+        overflow.p);
     FG_CHECK_LAUNCH();
     (void)cols;
     *cnnz = nnz;

@@ -7,10 +7,10 @@
 // box level's entries sit at constant offsets), by sorting the keys of the coarse grid points
 // that some fine row interpolates from; the reference numbers them in first-sight order, which
 // is the same level up to that permutation. Each fine row forms its at most 8 tensor-product
-// weights in registers (1 thread per row). The sparse products C = A B run 1 thread per row of C
-// with a sorted table of the row's columns in local memory: a counting pass, a scan, and a pass
-// that writes; every entry of C is summed in a fixed order (A's row order, then B's), so the
-// coarse operators are reproducible bit for bit.
+// weights in registers (1 thread per row). The sparse products C = A B run 1 warp per row of C
+// with a hash table of the row's columns in shared memory: a counting pass, a scan, and a pass
+// that writes the columns increasing; every entry of C is summed in a fixed order (A's row
+// order), so the coarse operators are reproducible bit for bit.
 #pragma once
 #include <array>
 #include <vector>
