@@ -61,6 +61,8 @@ def args():
     p.add_argument("--stencil", type=int, default=0,
                    help="stencil product kernel: 0 tuned, 1 runtime K, 2 compile-time K, "
                         "3 2 rows per thread, 4 marching planes")
+    p.add_argument("--smoother", type=int, default=0,
+                   help="Chebyshev smoother polynomial: 0/1 first kind, 4 fourth kind")
     p.add_argument("--l2", type=int, default=0,
                    help="1: the coarsest inverse persisting in L2")
     p.add_argument("--tiles", type=int, default=0,
@@ -444,6 +446,7 @@ def run_ours(opt, rank, world, local):
                                          degree=opt.degree, launch=opt.launch,
                                          values=opt.values, tiles=opt.tiles,
                                          stencil=opt.stencil, l2=opt.l2,
+                                         smoother=opt.smoother,
                                          coarsest=opt.coarsest,
                                          lower=opt.lower)).with_tol(tol)
         return s, time.perf_counter() - t

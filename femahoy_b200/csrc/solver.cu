@@ -1851,7 +1851,22 @@ template double lambda_max<float>(const Operator<float>&, const double*, cudaStr
                                   DevBuf<double>&);
 
 void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
-               std::vector<double>* c2) {
+               std::vector<double>* c2, int kind) {
+    if (kind == 4) {
+        // The fourth-kind Chebyshev smoother on [0, 1.1] x lambda_max of D^-1 A (J. Lottes,
+        // Optimal polynomial smoothers for multigrid V-cycles, Numer. Linear Algebra Appl. 30
+        // (2023) e2518): d_0 = 4 / (3 l) D^-1 r_0, d_k = (2k - 1) / (2k + 3) d_(k-1)
+        // + (8k + 4) / ((2k + 3) l) D^-1 r_k.
+        const double l = 1.1 * lam;
+        c1->assign(degree, 0.0);
+        c2->assign(degree, 0.0);
+        (*c1)[0] = 4.0 / (3.0 * l);
+        for (int k = 1; k < degree; ++k) {
+            (*c2)[k] = (2.0 * k - 1.0) / (2.0 * k + 3.0);
+            (*c1)[k] = (8.0 * k + 4.0) / ((2.0 * k + 3.0) * l);
+        }
+        return;
+    }
     // Y. Saad, Iterative Methods for Sparse Linear Systems, 2nd ed., SIAM 2003, algorithm 12.1,
     // on the interval [lower, 1.1] x lambda_max of D^-1 A.
     double hi = 1.1 * lam, lo = lower * lam;
@@ -2121,10 +2136,10 @@ void SolverImpl::apply_degree(int degree, int coarse) {
     if (coarse <= 0) coarse = degree;
     for (size_t l = 0; l < H32_.levels.size(); ++l)
         chebyshev(H32_.levels[l].lambda, l == 0 ? degree : coarse, lower, &H32_.levels[l].c1,
-                  &H32_.levels[l].c2);
+                  &H32_.levels[l].c2, opt_.smoother);
     for (size_t l = 0; l < H64_.levels.size(); ++l)
         chebyshev(H64_.levels[l].lambda, l == 0 ? degree : coarse, lower, &H64_.levels[l].c1,
-                  &H64_.levels[l].c2);
+                  &H64_.levels[l].c2, opt_.smoother);
     // The captured loop holds the coefficients as kernel arguments.
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
@@ -2336,7 +2351,7 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         reciprocal<T>(lv.n, dg.p, lv.dinv.p, s_);
         int deg = opt_.degree > 0 ? opt_.degree : 2;
         double lower = opt_.lower > 0 ? opt_.lower : 0.3;
-        chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2);
+        chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2, opt_.smoother);
         t_lam.reset();
         PhaseTimer t_tr{this, "transfers", s_};
         // Transfers to the next level: P and R = P^T (each row's columns increasing).

@@ -108,8 +108,10 @@ HostRect transpose(const HostRect& p);
 template <class T>
 double lambda_max(const Operator<T>& A, const double* dg, cudaStream_t s,
                   DevBuf<double>& partial);
+// kind 1: the first-kind Chebyshev polynomial on [lower, 1.1] lambda; 4: the fourth kind on
+// [0, 1.1] lambda.
 void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
-               std::vector<double>* c2);
+               std::vector<double>* c2, int kind = 1);
 
 // The scalars of a PCG solve, in device memory.
 struct Scalars {
@@ -235,6 +237,7 @@ struct Options {
     int axes = 7;    // the axes that the coarsening halves (bits x, y, z)
     int stencil = 0; // stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
     int l2 = 0;      // 1: the coarsest inverse persisting in L2
+    int smoother = 1;  // the Chebyshev polynomial's kind: 1 first, 4 fourth
 };
 
 class SolverImpl {

@@ -342,6 +342,22 @@ def test_fp16_stencil_coefficients_solve_to_the_same_tolerance():
     assert "fp16" not in s.describe()
 
 
+@pytest.mark.parametrize("precision", [fg.FP64, fg.MIXED])
+def test_fourth_kind_chebyshev_smoother(precision):
+    """The fourth-kind Chebyshev smoother (Lottes 2023; the same kernels, other coefficients)
+    solves the lognormal heat cube to the tolerance, to the oracle's direct solution."""
+    h = mg.heat_cube(24, seed=11)
+    A, rhs, Ao = _system(h)
+    s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision,
+                  options=fg.Options(precision=precision, smoother=4, coarsest=1000,
+                                     degree=2)).with_tol(1e-10)
+    x = np.zeros(A.n)
+    st = s.solve(rhs, x)
+    assert st.true_residual <= 1.2e-10
+    xd, _ = oracle.direct_solve(Ao, h.xyz[h.free], rhs)
+    assert _rel(x, xd) <= 1e-8
+
+
 def test_fp16_coarsest_inverse_solves_to_the_same_tolerance():
     """The mixed form with the coarsest level's dense inverse in FP16 (scaled by its largest
     entry; the product sums in FP32): the coarse correction changes by about 2^-11 relative, and
