@@ -699,7 +699,9 @@ def run_batch(opt, rank, world, local):
 
     def make(precision):
         t = time.perf_counter()
-        bt = Batch(mats, unknowns, BATCH_RHS, precision=precision).with_tol(TOL)
+        bt = Batch(mats, unknowns, BATCH_RHS, precision=precision,
+                   options=fg.Options(precision=precision,
+                                      smoother=opt.smoother)).with_tol(TOL)
         return bt, time.perf_counter() - t
 
     def timed(bt, steps, warmup, clocks=None):

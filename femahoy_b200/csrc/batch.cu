@@ -1301,7 +1301,7 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             DevBuf<double> ddg;
             ddg.upload(dg.data(), A.n, s_);
             L.lambda = lambda_max(op, ddg.p, s_, partial_);
-            chebyshev(L.lambda, deg, lower, &L.c1, &L.c2);
+            chebyshev(L.lambda, deg, lower, &L.c1, &L.c2, opt_.smoother);
             std::vector<T> tv(inv.begin(), inv.end());
             L.dinv.upload(tv.data(), tv.size(), s_);
             HostRect Rt = transpose(P);
@@ -2014,6 +2014,11 @@ int femgpu_batch_new(int count, const femgpu_csr* const* a, const femgpu_unknown
             o.coarsest = options->coarsest;
             o.max_levels = options->max_levels;
         }
+        o.smoother = options && options->smoother ? options->smoother : 1;
+        if (o.smoother != 1 && o.smoother != 4)
+            throw Failure(FEMGPU_ERR_INVALID,
+                          "smoother is 1 (the first-kind Chebyshev polynomial) or 0 or 4 (the "
+                          "fourth kind)");
         auto* bt = new femgpu_batch;
         try {
             bt->impl.create(mats, us, nrhs, o);

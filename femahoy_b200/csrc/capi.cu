@@ -448,10 +448,10 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             o.axes = options->axes ? options->axes : 7;
             o.stencil = options->stencil;
             o.l2 = options->l2;
-            o.smoother = options->smoother ? options->smoother : 1;
+            o.smoother = options->smoother ? options->smoother : 4;
         }
         require(o.smoother == 1 || o.smoother == 4,
-                "smoother is 0 or 1 (the first-kind Chebyshev polynomial) or 4 (the fourth kind)");
+                "smoother is 1 (the first-kind Chebyshev polynomial) or 0 or 4 (the fourth kind)");
         require(o.l2 == 0 || o.l2 == 1, "l2 is 0 (plain loads) or 1 (the coarsest inverse "
                                         "persisting in L2)");
         require(o.stencil >= 0 && o.stencil <= 4,

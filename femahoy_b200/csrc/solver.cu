@@ -2160,7 +2160,8 @@ void SolverImpl::tune_degree() {
         kind = mixed ? H32_.levels[0].A.K : H64_.levels[0].A.K;
     else if (mixed ? H32_.levels[0].A.block3 : H64_.levels[0].A.block3)
         kind = -1;
-    const std::array<int64_t, 5> key{2, mixed ? 4 : 8, kind, log2_of(n_), (int64_t)nlevels};
+    const std::array<int64_t, 5> key{2, (mixed ? 4 : 8) + 100 * opt_.smoother, kind, log2_of(n_),
+                                     (int64_t)nlevels};
     int degree = 22;  // 10 * (the finest level's degree) + the coarser levels'
     if (tune_lookup(key, &degree)) {
         if (degree != 22) apply_degree(degree / 10, degree % 10);

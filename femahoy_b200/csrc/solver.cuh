@@ -237,7 +237,7 @@ struct Options {
     int axes = 7;    // the axes that the coarsening halves (bits x, y, z)
     int stencil = 0; // stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
     int l2 = 0;      // 1: the coarsest inverse persisting in L2
-    int smoother = 1;  // the Chebyshev polynomial's kind: 1 first, 4 fourth
+    int smoother = 4;  // the Chebyshev polynomial's kind: 1 first, 4 fourth
 };
 
 class SolverImpl {

@@ -116,7 +116,7 @@ class Options:
     tiles: int = 0   # finest FP32 stencil steps from bulk-copied tiles: 0 tuned, 1 off, 2 on
     axes: int = 0    # the axes the coarsening halves (bits x 1, y 2, z 4; 0: all)
     stencil: int = 0  # stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
-    smoother: int = 0  # Chebyshev polynomial: 0 or 1 the first kind, 4 the fourth kind
+    smoother: int = 0  # Chebyshev polynomial: 0 the default, 1 the first kind, 4 the fourth
     l2: int = 0      # 1: the coarsest inverse persisting in L2
 
     def _c(self):
