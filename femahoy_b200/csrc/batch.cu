@@ -2014,7 +2014,7 @@ int femgpu_batch_new(int count, const femgpu_csr* const* a, const femgpu_unknown
             o.coarsest = options->coarsest;
             o.max_levels = options->max_levels;
         }
-        o.smoother = options && options->smoother ? options->smoother : 1;
+        o.smoother = options && options->smoother ? options->smoother : 4;
         if (o.smoother != 1 && o.smoother != 4)
             throw Failure(FEMGPU_ERR_INVALID,
                           "smoother is 1 (the first-kind Chebyshev polynomial) or 0 or 4 (the "

@@ -259,8 +259,8 @@ typedef struct femgpu_options {
                              a level cannot take falls back to the next lower one. All give the
                              same bits. */
     int smoother;         /* the Chebyshev smoother's polynomial: 0 or 4 = the fourth kind on
-                             [0, 1.1] lambda_max (Lottes 2023; the default of a solver), 1 = the
-                             first kind on [lower, 1.1] lambda_max (the default of a batch) */
+                             [0, 1.1] lambda_max (Lottes 2023; the default), 1 = the first kind
+                             on [lower, 1.1] lambda_max */
     int l2;               /* 1 = keep the coarsest level's dense inverse resident in L2 (a
                              persisting access window on its product; the process's persisting
                              L2 limit is raised to the inverse's size, at most the device's
