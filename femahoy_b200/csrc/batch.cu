@@ -1332,23 +1332,58 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             }
             L.ntiles = (int)tiles.size();
             L.inv.alloc(ioff[L.ndense]);
-            for (int j = 0; j < L.ndense; ++j) {
-                const int64_t m = off[j + 1] - off[j];
-                DevBuf<double> inv64;
-                dense_inverse(H[S + j].mats[l], &inv64, s_);
-                std::vector<double> h((size_t)(m * m));
-                inv64.download(h.data(), m * m, s_);
-                FG_CUDA(cudaStreamSynchronize(s_));
-                const int64_t mt = ioff[j + 1] - ioff[j];
-                std::vector<T> t((size_t)mt, (T)0);
-                for (int64_t r = 0; r < m; ++r)
-                    for (int64_t c = 0; c < m; ++c)
-                        t[(r / DTH) * DTH * m + c * DTH + r % DTH] =
-                            (T)(0.5 * (h[r * m + c] + h[c * m + r]));
-                FG_CUDA(cudaMemcpyAsync(L.inv.p + ioff[j], t.data(), mt * sizeof(T),
-                                        cudaMemcpyHostToDevice, s_));
-                FG_CUDA(cudaStreamSynchronize(s_));
-            }
+            FG_CUDA(cudaStreamSynchronize(s_));
+            // The members' inverses on the host threads, each with its own stream (each is a
+            // chain of small launches), into their own places of L.inv.
+            std::vector<std::string> errors(L.ndense);
+            std::vector<int> codes(L.ndense, FEMGPU_OK);
+            const int threads = std::max(1, std::min(host_threads(), L.ndense));
+            int device = 0;
+            FG_CUDA(cudaGetDevice(&device));
+            std::vector<std::thread> pool;
+            for (int th = 0; th < threads; ++th)
+                pool.emplace_back([&, th] {
+                    cudaStream_t st = nullptr;
+                    if (cudaSetDevice(device) != cudaSuccess ||
+                        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+                        for (int j = th; j < L.ndense; j += threads) {
+                            codes[j] = FEMGPU_ERR_CUDA;
+                            errors[j] = "cudaStreamCreate failed";
+                        }
+                        return;
+                    }
+                    for (int j = th; j < L.ndense; j += threads) {
+                        try {
+                            const int64_t m = off[j + 1] - off[j];
+                            DevBuf<double> inv64;
+                            dense_inverse(H[S + j].mats[l], &inv64, st);
+                            std::vector<double> h((size_t)(m * m));
+                            inv64.download(h.data(), m * m, st);
+                            FG_CUDA(cudaStreamSynchronize(st));
+                            const int64_t mt = ioff[j + 1] - ioff[j];
+                            std::vector<T> t((size_t)mt, (T)0);
+                            for (int64_t r = 0; r < m; ++r)
+                                for (int64_t c = 0; c < m; ++c)
+                                    t[(r / DTH) * DTH * m + c * DTH + r % DTH] =
+                                        (T)(0.5 * (h[r * m + c] + h[c * m + r]));
+                            FG_CUDA(cudaMemcpyAsync(L.inv.p + ioff[j], t.data(), mt * sizeof(T),
+                                                    cudaMemcpyHostToDevice, st));
+                            FG_CUDA(cudaStreamSynchronize(st));
+                        } catch (const Failure& e) {
+                            codes[j] = e.code;
+                            errors[j] = e.what();
+                        } catch (const std::exception& e) {
+                            codes[j] = FEMGPU_ERR_INVALID;
+                            errors[j] = e.what();
+                        }
+                    }
+                    cudaStreamDestroy(st);
+                });
+            for (auto& th : pool) th.join();
+            for (int j = 0; j < L.ndense; ++j)
+                if (codes[j] != FEMGPU_OK)
+                    throw Failure(codes[j],
+                                  "system " + std::to_string(order_[S + j]) + ": " + errors[j]);
             L.doff.upload(off.data(), off.size(), s_);
             L.dioff.upload(ioff.data(), ioff.size(), s_);
             L.tiles.upload(tiles.data(), tiles.size(), s_);
