@@ -63,6 +63,8 @@ def args():
                         "3 2 rows per thread, 4 marching planes")
     p.add_argument("--smoother", type=int, default=0,
                    help="Chebyshev smoother polynomial: 0/1 first kind, 4 fourth kind")
+    p.add_argument("--cluster", type=int, default=0,
+                   help="small levels: 0 each leg as 1 cluster launch, 1 a launch per step")
     p.add_argument("--l2", type=int, default=0,
                    help="1: the coarsest inverse persisting in L2")
     p.add_argument("--tiles", type=int, default=0,
@@ -446,7 +448,7 @@ def run_ours(opt, rank, world, local):
                                          degree=opt.degree, launch=opt.launch,
                                          values=opt.values, tiles=opt.tiles,
                                          stencil=opt.stencil, l2=opt.l2,
-                                         smoother=opt.smoother,
+                                         smoother=opt.smoother, cluster=opt.cluster,
                                          coarsest=opt.coarsest,
                                          lower=opt.lower)).with_tol(tol)
         return s, time.perf_counter() - t

@@ -66,19 +66,19 @@ struct SellOp {
     }
 };
 
-// Row i of the stencil product with K read at run time.
-template <class T, class TA, class TX>
+// Row i of the stencil product with K read at run time (COH: x through ldx<true>).
+template <class T, class TA, class TX, bool COH = false>
 __device__ __forceinline__ TA stencil_apply(const StencilView<T>& v, int i,
                                             const TX* __restrict__ x) {
     const int n = v.n;
     const T* __restrict__ c = v.coef;
-    TA acc = (TA)__ldg(c + i) * (TA)__ldg(x + i);
+    TA acc = (TA)__ldg(c + i) * (TA)ldx<COH>(x + i);
     for (int k = 1; k < v.K; ++k) {
         const int o = v.off[k];
         const T* __restrict__ ck = c + (size_t)k * v.ld;
         const int j = i + o, m = i - o;
-        if (j < n) acc = fmadd((TA)__ldg(ck + i), (TA)__ldg(x + j), acc);
-        if (m >= 0) acc = fmadd((TA)__ldg(ck + m), (TA)__ldg(x + m), acc);
+        if (j < n) acc = fmadd((TA)__ldg(ck + i), (TA)ldx<COH>(x + j), acc);
+        if (m >= 0) acc = fmadd((TA)__ldg(ck + m), (TA)ldx<COH>(x + m), acc);
     }
     return acc;
 }
@@ -95,24 +95,26 @@ struct StencilOp {
 };
 
 // The same products through a reference to a view held elsewhere (shared memory), so that the
-// view is not copied per thread.
-template <class T>
+// view is not copied per thread; COH: for the fused kernels, whose x they wrote themselves.
+template <class T, bool COH = false>
 struct StencilRefOp {
     const StencilView<T>& v;
+    static constexpr bool coherent = COH;
     __device__ __forceinline__ bool valid(int64_t) const { return true; }
     template <class TA, class TX>
     __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
-        return stencil_apply<T, TA, TX>(v, (int)g, x);
+        return stencil_apply<T, TA, TX, COH>(v, (int)g, x);
     }
 };
 
-template <class T>
+template <class T, bool COH = false>
 struct SellRefOp {
     const SellView<T>& v;
+    static constexpr bool coherent = COH;
     __device__ __forceinline__ bool valid(int64_t g) const { return g < v.n; }
     template <class TA, class TX>
     __device__ __forceinline__ TA apply(int64_t g, const TX* __restrict__ x) const {
-        return sell_row<T, TX, TA>(v, g / v.C, (int)(g % v.C), x);
+        return sell_row<T, TX, TA, COH>(v, g / v.C, (int)(g % v.C), x);
     }
 };
 

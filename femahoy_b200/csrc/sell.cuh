@@ -44,8 +44,19 @@ __device__ __forceinline__ float4 load4(const float* p) {
     return __ldg(reinterpret_cast<const float4*>(p));
 }
 
+// A load of a vector: read-only through the non-coherent path (the kernel never writes it), or
+// COH: a load cached in L2 only (ld.global.cg), for a vector that the same kernel wrote before
+// a grid- or cluster-wide barrier, which such a barrier's memory ordering covers.
+template <bool COH, class T>
+__device__ __forceinline__ T ldx(const T* p) {
+    if constexpr (COH)
+        return __ldcg(p);
+    else
+        return __ldg(p);
+}
+
 // (A x)_row for the thread's row in slice `s`, lane `r` of the slice. Accumulates in TA.
-template <class T, class TX, class TA>
+template <class T, class TX, class TA, bool COH = false>
 __device__ __forceinline__ TA sell_row(const SellView<T>& A, int64_t s, int r,
                                        const TX* __restrict__ x) {
     int64_t b = A.slice_ptr[s], e = A.slice_ptr[s + 1];
@@ -56,10 +67,10 @@ __device__ __forceinline__ TA sell_row(const SellView<T>& A, int64_t s, int r,
     for (int64_t k = 0; k < groups; ++k) {
         auto vv = load4(v);
         uint4 cc = __ldg(reinterpret_cast<const uint4*>(c));
-        acc += (TA)vv.x * (TA)__ldg(x + cc.x);
-        acc += (TA)vv.y * (TA)__ldg(x + cc.y);
-        acc += (TA)vv.z * (TA)__ldg(x + cc.z);
-        acc += (TA)vv.w * (TA)__ldg(x + cc.w);
+        acc += (TA)vv.x * (TA)ldx<COH>(x + cc.x);
+        acc += (TA)vv.y * (TA)ldx<COH>(x + cc.y);
+        acc += (TA)vv.z * (TA)ldx<COH>(x + cc.z);
+        acc += (TA)vv.w * (TA)ldx<COH>(x + cc.w);
         v += 4 * A.C;
         c += 4 * A.C;
     }

@@ -219,14 +219,16 @@ __device__ __forceinline__ int row_of_thread() { return (int)(blockIdx.x * block
 
 // ------------------------------------------------------------------ V-cycle rows
 // The work of 1 row of each V-cycle step, shared by the separate kernels below and by the fused
-// kernel of the coarse levels (k_tail), so that both give the same bits.
+// kernel of the coarse levels (k_tail), so that both give the same bits. COH: the fused kernel's
+// form, whose right sides and iterates it wrote itself before a grid-wide barrier, read through
+// ldx<true> (L2, coherent) instead of the read-only path.
 
 // The first Chebyshev step from x = 0: d = c1 D^-1 b, x = d.
-template <class T>
+template <class T, bool COH = false>
 __device__ __forceinline__ void cheb_first_row(int i, const T* __restrict__ b,
                                                const T* __restrict__ dinv, T c1,
                                                T* __restrict__ d, T* __restrict__ x) {
-    T v = c1 * dinv[i] * b[i];
+    T v = c1 * dinv[i] * (COH ? ldx<true>(b + i) : b[i]);
     d[i] = v;
     x[i] = v;
 }
@@ -241,40 +243,41 @@ __device__ __forceinline__ T cheb_update(T bi, T ax, T di, T dprev, T c1, T c2) 
 }
 
 // A Chebyshev step: r = b - A x_in, d = c2 d + c1 D^-1 r, x_out = x_in + d.
-template <class T, class Op>
+template <class T, class Op, bool COH = false>
 __device__ __forceinline__ void cheb_step_row(const Op& A, int g, const T* __restrict__ b,
                                               const T* __restrict__ xin,
                                               const T* __restrict__ dinv, T c1, T c2,
                                               T* __restrict__ d, T* __restrict__ xout) {
     T ax = A.template apply<T>(g, xin);
     if (!A.valid(g)) return;
-    const T dd = cheb_update(b[g], ax, dinv[g], d[g], c1, c2);
+    const T bg = COH ? ldx<true>(b + g) : b[g];
+    const T dd = cheb_update(bg, ax, dinv[g], d[g], c1, c2);
     d[g] = dd;
-    xout[g] = xin[g] + dd;
+    xout[g] = (COH ? ldx<true>(xin + g) : xin[g]) + dd;
 }
 
-template <class T, class Op>
+template <class T, class Op, bool COH = false>
 __device__ __forceinline__ void residual_row(const Op& A, int g, const T* __restrict__ b,
                                              const T* __restrict__ x, T* __restrict__ r) {
     T ax = A.template apply<T>(g, x);
-    if (A.valid(g)) r[g] = b[g] - ax;
+    if (A.valid(g)) r[g] = (COH ? ldx<true>(b + g) : b[g]) - ax;
 }
 
 // Row i of a CSR transfer times x (multigrid.rs:166-172, sparse.rs:212-230).
-template <class T>
+template <class T, bool COH = false>
 __device__ __forceinline__ T csr_row(int i, const int64_t* __restrict__ ptr,
                                      const uint32_t* __restrict__ idx, const T* __restrict__ val,
                                      const T* __restrict__ x) {
     const int e = (int)ptr[i + 1];
     T s = 0;
-    for (int k = (int)ptr[i]; k < e; ++k) s += val[k] * __ldg(x + idx[k]);
+    for (int k = (int)ptr[i]; k < e; ++k) s += val[k] * ldx<COH>(x + idx[k]);
     return s;
 }
 
 // Row i of a transfer in offset form times x. KC > 0: K known at compile time (8 for P, 27 for
 // R), so that all of a row's weight and x loads are in flight at once; KC = 0 reads K from the
 // view. The terms are fused multiply-adds in increasing offset (= column) order either way.
-template <class T, int KC>
+template <class T, int KC, bool COH = false>
 __device__ __forceinline__ T offset_row(const OffsetView<T>& M, int i, const T* __restrict__ x) {
     const int b = M.base[i];
     const int K = KC > 0 ? KC : M.K;
@@ -284,7 +287,7 @@ __device__ __forceinline__ T offset_row(const OffsetView<T>& M, int i, const T* 
         if (KC == 0 && k >= K) break;
         const int j = b + M.off[k];
         const T w = __ldg(M.w + (size_t)k * M.rows + i);
-        const T v = j < M.cols ? __ldg(x + j) : (T)0;
+        const T v = j < M.cols ? ldx<COH>(x + j) : (T)0;
         s = fmadd(w, v, s);
     }
     return s;
@@ -344,7 +347,7 @@ __device__ __forceinline__ double dot_add(double2 m, double2 x, double s) {
 // flight per thread, so a row of the 4,913-row coarsest level of the box grids is read in 1 or
 // 2 round trips), 4 partial sums, a butterfly over each warp, then the warps' sums in order.
 // Every thread of the block must call it; thread 0 returns the sum. `red` holds TH / 32 values.
-template <class T>
+template <class T, bool COH = false>
 __device__ __forceinline__ T gemv_block_row(const T* __restrict__ M, const T* __restrict__ b,
                                             int64_t ld, int64_t i, T* red) {
     typedef typename Vec16<T>::type VT;
@@ -356,14 +359,14 @@ __device__ __forceinline__ T gemv_block_row(const T* __restrict__ M, const T* __
     for (; c + 3 * TH < nc; c += 4 * TH) {
         const VT m0 = __ldg(row + c), m1 = __ldg(row + c + TH), m2 = __ldg(row + c + 2 * TH),
                  m3 = __ldg(row + c + 3 * TH);
-        const VT x0 = __ldg(bv + c), x1 = __ldg(bv + c + TH), x2 = __ldg(bv + c + 2 * TH),
-                 x3 = __ldg(bv + c + 3 * TH);
+        const VT x0 = ldx<COH>(bv + c), x1 = ldx<COH>(bv + c + TH), x2 = ldx<COH>(bv + c + 2 * TH),
+                 x3 = ldx<COH>(bv + c + 3 * TH);
         s0 = dot_add(m0, x0, s0);
         s1 = dot_add(m1, x1, s1);
         s2 = dot_add(m2, x2, s2);
         s3 = dot_add(m3, x3, s3);
     }
-    for (; c < nc; c += TH) s0 = dot_add(__ldg(row + c), __ldg(bv + c), s0);
+    for (; c < nc; c += TH) s0 = dot_add(__ldg(row + c), ldx<COH>(bv + c), s0);
     T s = (s0 + s1) + (s2 + s3);
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -1083,11 +1086,11 @@ __device__ __forceinline__ void tail_smooth(const TailLevel<T>& L, const T* __re
                                             const T* xin, T* xout, T c1, T c2, int tid,
                                             int nth) {
     if (L.stencil) {
-        const StencilRefOp<T> A{L.sv};
-        for (int i = tid; i < L.n; i += nth) cheb_step_row(A, i, b, xin, L.dinv, c1, c2, L.d, xout);
+        const StencilRefOp<T, true> A{L.sv};
+        for (int i = tid; i < L.n; i += nth) cheb_step_row<T, decltype(A), true>(A, i, b, xin, L.dinv, c1, c2, L.d, xout);
     } else {
-        const SellRefOp<T> A{L.sell};
-        for (int i = tid; i < L.n; i += nth) cheb_step_row(A, i, b, xin, L.dinv, c1, c2, L.d, xout);
+        const SellRefOp<T, true> A{L.sell};
+        for (int i = tid; i < L.n; i += nth) cheb_step_row<T, decltype(A), true>(A, i, b, xin, L.dinv, c1, c2, L.d, xout);
     }
 }
 
@@ -1119,7 +1122,7 @@ __global__ void __launch_bounds__(TH)
         const T* b = l == 0 ? b0 : L.b;
         T* xa = L.xa;
         T* xb = L.xb;
-        for (int i = tid; i < L.n; i += nth) cheb_first_row(i, b, L.dinv, L.c1[0], L.d, xa);
+        for (int i = tid; i < L.n; i += nth) cheb_first_row<T, true>(i, b, L.dinv, L.c1[0], L.d, xa);
         grid.sync();
         for (int k = 1; k < L.deg; ++k) {
             tail_smooth(L, b, xa, xb, L.c1[k], L.c2[k], tid, nth);
@@ -1129,23 +1132,23 @@ __global__ void __launch_bounds__(TH)
             xb = t;
         }
         if (L.stencil) {
-            const StencilRefOp<T> A{L.sv};
-            for (int i = tid; i < L.n; i += nth) residual_row(A, i, b, xa, L.r);
+            const StencilRefOp<T, true> A{L.sv};
+            for (int i = tid; i < L.n; i += nth) residual_row<T, decltype(A), true>(A, i, b, xa, L.r);
         } else {
-            const SellRefOp<T> A{L.sell};
-            for (int i = tid; i < L.n; i += nth) residual_row(A, i, b, xa, L.r);
+            const SellRefOp<T, true> A{L.sell};
+            for (int i = tid; i < L.n; i += nth) residual_row<T, decltype(A), true>(A, i, b, xa, L.r);
         }
         grid.sync();
         for (int j = tid; j < L.nc; j += nth)
-            L.bc[j] = L.r_offset ? offset_row<T, 0>(L.Ro, j, L.r)
-                                 : csr_row(j, L.rptr, L.ridx, L.rval, L.r);
+            L.bc[j] = L.r_offset ? offset_row<T, 0, true>(L.Ro, j, L.r)
+                                 : csr_row<T, true>(j, L.rptr, L.ridx, L.rval, L.r);
         grid.sync();
     }
     {
         __shared__ T red[TH / 32];
         const T* bc = sL[nl - 1].bc;
         for (int64_t i = blockIdx.x; i < nco; i += gridDim.x) {
-            const T s = gemv_block_row(inv, bc, dense_ld(nco), i, red);
+            const T s = gemv_block_row<T, true>(inv, bc, dense_ld(nco), i, red);
             if (threadIdx.x == 0) cx[i] = s;
         }
         grid.sync();
@@ -1158,8 +1161,8 @@ __global__ void __launch_bounds__(TH)
         T* xa = (L.deg - 1) % 2 ? L.xb : L.xa;
         T* xb = (L.deg - 1) % 2 ? L.xa : L.xb;
         for (int i = tid; i < L.n; i += nth)
-            xa[i] += L.p_offset ? offset_row<T, 0>(L.Po, i, e)
-                                : csr_row(i, L.pptr, L.pidx, L.pval, e);
+            xa[i] += L.p_offset ? offset_row<T, 0, true>(L.Po, i, e)
+                                : csr_row<T, true>(i, L.pptr, L.pidx, L.pval, e);
         grid.sync();
         for (int k = 0; k < L.deg; ++k) {
             tail_smooth(L, b, xa, xb, L.c1[k], L.c2[k], tid, nth);
@@ -1170,6 +1173,130 @@ __global__ void __launch_bounds__(TH)
         }
         e = xa;
     }
+}
+
+// ------------------------------------------------------------------ small levels by cluster
+// A small level's down leg (the first step, the other pre-smoothing steps, the residual and the
+// restriction into the next level's right side) or up leg (the prolongation and correction, the
+// post-smoothing steps) as 1 launch of 1 thread-block cluster of CL_CTAS blocks: the blocks share
+// the level's rows and meet at a cluster barrier (release and acquire at cluster scope) between
+// steps, which costs well under the several microseconds of a kernel boundary. The steps are the
+// separate kernels' row functions, so the bits are the same; the data that the launch writes and
+// reads again go through coherent loads.
+constexpr int CL_TH = 1024;
+
+template <class T, bool UP>
+__global__ void __launch_bounds__(CL_TH)
+    k_level_cluster(TailLevel<T> L, const T* __restrict__ e, const int* __restrict__ done) {
+    pdl_wait();
+    if (*done) return;  // the same value in every block
+    cg::cluster_group cluster = cg::this_cluster();
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nth = gridDim.x * blockDim.x;
+    const T* b = L.b;
+    if (!UP) {
+        T* xa = L.xa;
+        T* xb = L.xb;
+        for (int i = tid; i < L.n; i += nth) cheb_first_row<T, true>(i, b, L.dinv, L.c1[0], L.d, xa);
+        cluster.sync();
+        for (int k = 1; k < L.deg; ++k) {
+            tail_smooth(L, b, xa, xb, L.c1[k], L.c2[k], tid, nth);
+            cluster.sync();
+            T* t = xa;
+            xa = xb;
+            xb = t;
+        }
+        if (L.stencil) {
+            const StencilRefOp<T, true> A{L.sv};
+            for (int i = tid; i < L.n; i += nth) residual_row<T, decltype(A), true>(A, i, b, xa, L.r);
+        } else {
+            const SellRefOp<T, true> A{L.sell};
+            for (int i = tid; i < L.n; i += nth) residual_row<T, decltype(A), true>(A, i, b, xa, L.r);
+        }
+        cluster.sync();
+        for (int j = tid; j < L.nc; j += nth)
+            L.bc[j] = L.r_offset ? offset_row<T, 0, true>(L.Ro, j, L.r)
+                                 : csr_row<T, true>(j, L.rptr, L.ridx, L.rval, L.r);
+    } else {
+        // Where the pre-smoothing left x: after deg - 1 swaps.
+        T* xa = (L.deg - 1) % 2 ? L.xb : L.xa;
+        T* xb = (L.deg - 1) % 2 ? L.xa : L.xb;
+        for (int i = tid; i < L.n; i += nth)
+            xa[i] = ldx<true>(xa + i) + (L.p_offset ? offset_row<T, 0, true>(L.Po, i, e)
+                                                    : csr_row<T, true>(i, L.pptr, L.pidx,
+                                                                       L.pval, e));
+        cluster.sync();
+        for (int k = 0; k < L.deg; ++k) {
+            tail_smooth(L, b, xa, xb, L.c1[k], L.c2[k], tid, nth);
+            if (k + 1 < L.deg) cluster.sync();
+            T* t = xa;
+            xa = xb;
+            xb = t;
+        }
+    }
+}
+
+// The largest level that takes the cluster legs: 65,536 rows over 16 blocks of 1024 threads is
+// 4 rows per thread and step.
+constexpr int64_t CLUSTER_MAX_ROWS = 65536;
+
+// The blocks of 1 cluster that the device schedules for k_level_cluster: 16 (a non-portable
+// size, where a GPC has room) or 8; 0 if neither.
+template <class T>
+static int cluster_ctas() {
+    for (int ctas : {16, 8}) {
+        auto* kd = k_level_cluster<T, false>;
+        auto* ku = k_level_cluster<T, true>;
+        if (ctas > 8) {
+            if (cudaFuncSetAttribute(kd, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                    cudaSuccess ||
+                cudaFuncSetAttribute(ku, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                    cudaSuccess) {
+                cudaGetLastError();
+                continue;
+            }
+        }
+        cudaLaunchConfig_t cfg{};
+        cfg.gridDim = dim3(ctas);
+        cfg.blockDim = dim3(CL_TH);
+        cudaLaunchAttribute attr{};
+        attr.id = cudaLaunchAttributeClusterDimension;
+        attr.val.clusterDim.x = ctas;
+        attr.val.clusterDim.y = 1;
+        attr.val.clusterDim.z = 1;
+        cfg.attrs = &attr;
+        cfg.numAttrs = 1;
+        int nd = 0, nu = 0;
+        if (cudaOccupancyMaxActiveClusters(&nd, kd, &cfg) == cudaSuccess &&
+            cudaOccupancyMaxActiveClusters(&nu, ku, &cfg) == cudaSuccess && nd > 0 && nu > 0)
+            return ctas;
+        cudaGetLastError();
+    }
+    return 0;
+}
+
+// 1 leg of a small level as 1 cluster launch (with programmatic dependent launch if pdl).
+template <class T, bool UP>
+static void launch_cluster(bool pdl, int ctas, const TailLevel<T>& t, const T* e,
+                           const int* done, cudaStream_t s) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(ctas);
+    cfg.blockDim = dim3(CL_TH);
+    cfg.stream = s;
+    cudaLaunchAttribute attrs[2]{};
+    attrs[0].id = cudaLaunchAttributeClusterDimension;
+    attrs[0].val.clusterDim.x = ctas;
+    attrs[0].val.clusterDim.y = 1;
+    attrs[0].val.clusterDim.z = 1;
+    unsigned na = 1;
+    if (pdl) {
+        attrs[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attrs[1].val.programmaticStreamSerializationAllowed = 1;
+        na = 2;
+    }
+    cfg.attrs = attrs;
+    cfg.numAttrs = na;
+    FG_CUDA(cudaLaunchKernelEx(&cfg, k_level_cluster<T, UP>, t, e, done));
 }
 
 // x += t
@@ -1971,12 +2098,15 @@ std::string SolverImpl::describe() const {
             std::snprintf(buf, sizeof buf, "level %zu %s n=%lld lambda=%.4f degree=%zu: ", l, t,
                           (long long)L.n, L.lambda, L.c1.size());
             out += buf + describe_op(L.A);
-            std::snprintf(buf, sizeof buf, "; P %s, R %s\n",
+            std::snprintf(buf, sizeof buf, "; P %s, R %s",
                           L.Po.ok ? ("offsets K=" + std::to_string(L.Po.off.size())).c_str()
                                   : "CSR",
                           L.Ro.ok ? ("offsets K=" + std::to_string(L.Ro.off.size())).c_str()
                                   : "CSR");
             out += buf;
+            if (cluster_on_ && l < H.cluster.size() && H.cluster[l])
+                out += "; legs as clusters of " + std::to_string(cluster_ctas_) + " blocks";
+            out += "\n";
         }
         if (H.sparse)
             std::snprintf(buf, sizeof buf, "coarsest n=%lld %s", (long long)H.ncoarse,
@@ -2233,6 +2363,50 @@ static void make_offset(const DevRect& M, OffsetTransfer<T>* out, cudaStream_t s
     out->ok = true;
 }
 
+// The descriptor of level l for the fused kernels (stencil or SELL operator, at most
+// TAIL_MAXDEG smoothing steps, fewer than 2^31 rows).
+template <class T>
+static TailLevel<T> tail_level(const Hierarchy<T>& H, size_t l) {
+    const MgLevel<T>& L = H.levels[l];
+    TailLevel<T> t{};
+    t.n = (int)L.n;
+    t.nc = (int)L.nc;
+    t.stencil = L.A.stencil ? 1 : 0;
+    t.deg = (int)L.c1.size();
+    if (L.A.stencil)
+        t.sv = L.A.sview();
+    else
+        t.sell = L.A.sell.view();
+    t.p_offset = L.Po.ok ? 1 : 0;
+    t.r_offset = L.Ro.ok ? 1 : 0;
+    if (L.Po.ok) {
+        t.Po = L.Po.view();
+    } else {
+        t.pptr = L.pptr.p;
+        t.pidx = L.pidx.p;
+        t.pval = L.pval.p;
+    }
+    if (L.Ro.ok) {
+        t.Ro = L.Ro.view();
+    } else {
+        t.rptr = L.rptr.p;
+        t.ridx = L.ridx.p;
+        t.rval = L.rval.p;
+    }
+    t.dinv = L.dinv.p;
+    t.b = L.b.p;
+    t.xa = L.xa.p;
+    t.xb = L.xb.p;
+    t.d = L.d.p;
+    t.r = L.r.p;
+    t.bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
+    for (size_t k = 0; k < L.c1.size() && k < (size_t)TAIL_MAXDEG; ++k) {
+        t.c1[k] = (T)L.c1[k];
+        t.c2[k] = (T)L.c2[k];
+    }
+    return t;
+}
+
 // The descriptors of the fused kernel for the levels from the first one of at most `tail` rows
 // down (tail <= 0: none), and its grid: as many blocks as fit on the GPU at once (a cooperative
 // launch needs them all resident), no more than the largest of those levels has rows for.
@@ -2255,43 +2429,7 @@ static void build_tail(Hierarchy<T>* H, int tail, cudaStream_t s) {
         // The fused kernel reads stencil and SELL levels; a 3x3-block level keeps separate
         // launches.
         if (L.c1.size() > (size_t)TAIL_MAXDEG || L.n >= 0x7fffffff || L.A.block3) return;
-        TailLevel<T> t{};
-        t.n = (int)L.n;
-        t.nc = (int)L.nc;
-        t.stencil = L.A.stencil ? 1 : 0;
-        t.deg = (int)L.c1.size();
-        if (L.A.stencil)
-            t.sv = L.A.sview();
-        else
-            t.sell = L.A.sell.view();
-        t.p_offset = L.Po.ok ? 1 : 0;
-        t.r_offset = L.Ro.ok ? 1 : 0;
-        if (L.Po.ok) {
-            t.Po = L.Po.view();
-        } else {
-            t.pptr = L.pptr.p;
-            t.pidx = L.pidx.p;
-            t.pval = L.pval.p;
-        }
-        if (L.Ro.ok) {
-            t.Ro = L.Ro.view();
-        } else {
-            t.rptr = L.rptr.p;
-            t.ridx = L.ridx.p;
-            t.rval = L.rval.p;
-        }
-        t.dinv = L.dinv.p;
-        t.b = L.b.p;
-        t.xa = L.xa.p;
-        t.xb = L.xb.p;
-        t.d = L.d.p;
-        t.r = L.r.p;
-        t.bc = l + 1 == H->levels.size() ? H->cb.p : H->levels[l + 1].b.p;
-        for (size_t k = 0; k < L.c1.size(); ++k) {
-            t.c1[k] = (T)L.c1[k];
-            t.c2[k] = (T)L.c2[k];
-        }
-        d.push_back(t);
+        d.push_back(tail_level(*H, l));
         rows = std::max(rows, L.n);
     }
     int per_sm = 0, dev = 0, sms = 0;
@@ -2442,6 +2580,17 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
     t_dense.reset();
     for (const auto& st : stages) phase(std::string("coarsest: ") + st.first, st.second);
     build_tail(H, opt_.tail, s_);
+    // The small levels whose legs run as cluster launches: a stencil or SELL operator, at most
+    // CLUSTER_MAX_ROWS rows, and not the first level (its right side is the caller's).
+    H->cluster.assign(H->levels.size(), 0);
+    if (opt_.cluster == 0) {
+        if (cluster_ctas_ == 0) cluster_ctas_ = cluster_ctas<T>();
+        for (size_t l = 1; l < H->levels.size() && cluster_ctas_ > 0; ++l) {
+            const MgLevel<T>& L = H->levels[l];
+            H->cluster[l] = L.n <= CLUSTER_MAX_ROWS && !L.A.block3 &&
+                            L.c1.size() <= (size_t)TAIL_MAXDEG;
+        }
+    }
     if (opt_.l2 == 1 && H->inv.p) {
         // The inverse is read once per V-cycle (96 MB in FP32 for the 4,913-row level of the
         // 128^3 box) and evicted by the finer levels' streams in between; a persisting window
@@ -2657,6 +2806,23 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
         for (size_t k = 1; k < 2 * L.c1.size(); ++k) std::swap(xa, xb);
         return xa;
     }
+    if (cluster_on_ && l < H.cluster.size() && H.cluster[l]) {
+        // The level's 2 legs, each 1 cluster launch, around the coarser levels.
+        MgLevel<T>& L = H.levels[l];
+        TailLevel<T> t = tail_level(H, l);
+        t.b = b;
+        launch_cluster<T, false>(pdl_, cluster_ctas_, t, (const T*)nullptr, done, s_);
+        mark("L" + std::to_string(l) + " smoothing, residual and restriction (1 cluster)");
+        const T* ec = enqueue_vcycle(H, l + 1, t.bc);
+        launch_cluster<T, true>(pdl_, cluster_ctas_, t, ec, done, s_);
+        mark("L" + std::to_string(l) + " prolongation and smoothing (1 cluster)");
+        launches_ += 2;
+        // Where the legs leave x: the separate steps' swaps.
+        T* xa = L.xa.p;
+        T* xb = L.xb.p;
+        for (size_t k = 1; k < 2 * L.c1.size(); ++k) std::swap(xa, xb);
+        return xa;
+    }
     MgLevel<T>& L = H.levels[l];
     int64_t n = L.n;
     const int gb = row_blocks(n);
@@ -2794,9 +2960,15 @@ void SolverImpl::build_loop_graph() {
             exec_ = nullptr;
             graph_ = nullptr;
             launches_ = before;
-            // Give up the fused coarse levels first, then the programmatic launches.
+            // Give up the fused coarse levels first, then the cluster legs, then the
+            // programmatic launches.
+            const bool clustered =
+                std::count(H32_.cluster.begin(), H32_.cluster.end(), 1) +
+                    std::count(H64_.cluster.begin(), H64_.cluster.end(), 1) > 0;
             if (tail_on_ && H32_.tail_from + H64_.tail_from > -2) {
                 tail_on_ = false;
+            } else if (cluster_on_ && clustered) {
+                cluster_on_ = false;
             } else if (pdl_) {
                 pdl_ = false;
             } else {

@@ -204,6 +204,7 @@ struct Hierarchy {
     // The levels from `tail_from` down, and the coarsest solve, run as 1 cooperative kernel
     // (-1: none) of `tail_grid` blocks.
     int tail_from = -1, tail_grid = 0;
+    std::vector<char> cluster;  // per level: its legs run as cluster launches
     DevBuf<TailLevel<T>> tail;
     size_t bytes() const;
 };
@@ -238,6 +239,7 @@ struct Options {
     int stencil = 0; // stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
     int l2 = 0;      // 1: the coarsest inverse persisting in L2
     int smoother = 4;  // the Chebyshev polynomial's kind: 1 first, 4 fourth
+    int cluster = 0;   // 0: small levels' legs as 1 cluster launch each; 1: a launch per step
 };
 
 class SolverImpl {
@@ -335,6 +337,8 @@ class SolverImpl {
     std::vector<std::pair<std::string, cudaEvent_t>>* trace_ = nullptr;
     void mark(const std::string& label);
     bool tail_on_ = true;      // the fused coarse levels (off if a graph would not take them)
+    bool cluster_on_ = true;   // the small levels by cluster (off if a graph would not take them)
+    int cluster_ctas_ = 0;     // blocks of 1 cluster (16 or 8; 0: none can be scheduled)
     bool pdl_ = true;          // programmatic dependent launch of the iteration's kernels
     // Seconds of each phase of the setup, in the order first met (reported by describe()).
     std::vector<std::pair<std::string, double>> setup_s_;

@@ -358,6 +358,28 @@ def test_fourth_kind_chebyshev_smoother(precision):
     assert _rel(x, xd) <= 1e-8
 
 
+@pytest.mark.parametrize("precision", [fg.MIXED, fg.FP64])
+def test_cluster_legs_give_the_same_bits(precision):
+    """The small levels' legs as thread-block cluster launches (cluster barriers between the
+    steps, coherent loads of what the launch wrote) compute what the separate launches compute,
+    bit for bit (the 56^3 cube: levels of 24,000 and 3,400 rows take the cluster legs)."""
+    h = mg.heat_cube(56, seed=5)
+    A, rhs, _ = _system(h)
+    xs, its = [], []
+    for cluster in (1, 0):
+        s = fg.Solver(A, _grid(h), fg.Method.Multigrid, precision=precision,
+                      options=fg.Options(precision=precision, cluster=cluster,
+                                         degree=2)).with_tol(1e-10)
+        assert ("legs as clusters" in s.describe()) == (cluster == 0)
+        x = np.zeros(A.n)
+        st = s.solve(rhs, x)
+        assert st.true_residual <= 1.2e-10
+        xs.append(x)
+        its.append(st.iterations)
+    assert its[0] == its[1]
+    assert np.array_equal(xs[0].view(np.uint64), xs[1].view(np.uint64))
+
+
 def test_fp16_coarsest_inverse_solves_to_the_same_tolerance():
     """The mixed form with the coarsest level's dense inverse in FP16 (scaled by its largest
     entry; the product sums in FP32): the coarse correction changes by about 2^-11 relative, and
