@@ -64,7 +64,7 @@ def args():
     p.add_argument("--smoother", type=int, default=0,
                    help="Chebyshev smoother polynomial: 0/1 first kind, 4 fourth kind")
     p.add_argument("--cluster", type=int, default=0,
-                   help="small levels: 0 each leg as 1 cluster launch, 1 a launch per step")
+                   help="small levels: 1 each leg as 1 cluster launch, 0 a launch per step")
     p.add_argument("--l2", type=int, default=0,
                    help="1: the coarsest inverse persisting in L2")
     p.add_argument("--tiles", type=int, default=0,

@@ -451,7 +451,7 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             o.smoother = options->smoother ? options->smoother : 4;
             o.cluster = options->cluster;
         }
-        require(o.cluster == 0 || o.cluster == 1, "cluster is 0 (on) or 1 (off)");
+        require(o.cluster == 0 || o.cluster == 1, "cluster is 0 (off) or 1 (on)");
         require(o.smoother == 1 || o.smoother == 4,
                 "smoother is 1 (the first-kind Chebyshev polynomial) or 0 or 4 (the fourth kind)");
         require(o.l2 == 0 || o.l2 == 1, "l2 is 0 (plain loads) or 1 (the coarsest inverse "

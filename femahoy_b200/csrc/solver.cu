@@ -2583,7 +2583,7 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
     // The small levels whose legs run as cluster launches: a stencil or SELL operator, at most
     // CLUSTER_MAX_ROWS rows, and not the first level (its right side is the caller's).
     H->cluster.assign(H->levels.size(), 0);
-    if (opt_.cluster == 0) {
+    if (opt_.cluster == 1) {
         if (cluster_ctas_ == 0) cluster_ctas_ = cluster_ctas<T>();
         for (size_t l = 1; l < H->levels.size() && cluster_ctas_ > 0; ++l) {
             const MgLevel<T>& L = H->levels[l];

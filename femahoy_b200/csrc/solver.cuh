@@ -239,7 +239,7 @@ struct Options {
     int stencil = 0; // stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
     int l2 = 0;      // 1: the coarsest inverse persisting in L2
     int smoother = 4;  // the Chebyshev polynomial's kind: 1 first, 4 fourth
-    int cluster = 0;   // 0: small levels' legs as 1 cluster launch each; 1: a launch per step
+    int cluster = 0;   // 1: small levels' legs as 1 cluster launch each; 0: a launch per step
 };
 
 class SolverImpl {

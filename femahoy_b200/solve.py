@@ -117,7 +117,7 @@ class Options:
     axes: int = 0    # the axes the coarsening halves (bits x 1, y 2, z 4; 0: all)
     stencil: int = 0  # stencil kernel: 0 tuned, 1 runtime K, 2 compile-time K, 3 2 rows, 4 march
     smoother: int = 0  # Chebyshev polynomial: 0 the default, 1 the first kind, 4 the fourth
-    cluster: int = 0  # small levels: 0 each leg as 1 cluster launch, 1 a launch per step
+    cluster: int = 0  # small levels: 1 each leg as 1 cluster launch, 0 a launch per step
     l2: int = 0      # 1: the coarsest inverse persisting in L2
 
     def _c(self):

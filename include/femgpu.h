@@ -261,12 +261,13 @@ typedef struct femgpu_options {
     int smoother;         /* the Chebyshev smoother's polynomial: 0 or 4 = the fourth kind on
                              [0, 1.1] lambda_max (Lottes 2023; the default), 1 = the first kind
                              on [lower, 1.1] lambda_max */
-    int cluster;          /* the levels of at most 65,536 rows (stencil or SELL): 0 = each leg of
-                             the cycle there (the pre-smoothing steps, residual and restriction;
-                             the prolongation and the post-smoothing steps) as 1 launch of 1
-                             thread-block cluster with cluster barriers between steps, where the
-                             device schedules clusters of 16 or 8 blocks (default); 1 = a launch
-                             per step (the same bits) */
+    int cluster;          /* the levels of at most 65,536 rows (stencil or SELL) after the first:
+                             1 = each leg of the cycle there (the pre-smoothing steps, residual
+                             and restriction; the prolongation and the post-smoothing steps) as 1
+                             launch of 1 thread-block cluster with cluster barriers between
+                             steps, where the device schedules clusters of 16 or 8 blocks;
+                             0 (default) = a launch per step (the same bits; faster on B200 for
+                             the box grids measured) */
     int l2;               /* 1 = keep the coarsest level's dense inverse resident in L2 (a
                              persisting access window on its product; the process's persisting
                              L2 limit is raised to the inverse's size, at most the device's
