@@ -1637,6 +1637,7 @@ void BatchImpl::stream_open() {
     seen_.alloc(S);
     served_its_.alloc(1);
     served_its_.zero(s_);
+    loops_.zero(s_);  // the stream's loop iterations, counted from its opening
     phase_.zero(s_);
     restarts_seg_.zero(s_);
     fresh_.zero(s_);
