@@ -934,6 +934,25 @@ __global__ void __launch_bounds__(TH)
         out[i] = s;
 }
 
+// The restriction into the next level's right side fused with that level's first smoothing step
+// from x = 0 (cheb_first_row: d = c1 D^-1 b, x = d, on the value just stored): the same bits, 1
+// launch less per level.
+template <class T, int KC>
+__global__ void __launch_bounds__(TH)
+    k_restrict_first(OffsetView<T> M, const T* __restrict__ in, T* __restrict__ out,
+                     const T* __restrict__ dinv, T c1, T* __restrict__ d, T* __restrict__ x,
+                     const int* __restrict__ done) {
+    pdl_wait();
+    if (*done) return;
+    const int i = row_of_thread();
+    if (i >= M.rows) return;
+    const T s = offset_row<T, KC>(M, i, in);
+    out[i] = s;
+    const T v = c1 * dinv[i] * s;
+    d[i] = v;
+    x[i] = v;
+}
+
 template <class T>
 static void launch_transfer(const OffsetTransfer<T>& M, const T* in, T* out, int accumulate,
                             const int* done, cudaStream_t s, bool pdl) {
@@ -2743,7 +2762,7 @@ void SolverImpl::enqueue_residual(MgLevel<T>& L, const T* b, const T* x) {
 }
 
 template <class T>
-const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
+const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b, bool started) {
     const int* done = &sc_.p->done;
     if (l == H.levels.size() && H.sparse) {
         // The sparse coarsest factor's 2 triangular solves in FP64 (the right side and the
@@ -2830,8 +2849,10 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     T* xb = L.xb.p;
     int deg = (int)L.c1.size();
     std::string tag = "L" + std::to_string(l) + " ";
-    launch(pdl_, k_cheb_first<T>, gb, TH, s_, n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
-    mark(tag + "smooth (first, no product)");
+    if (!started) {
+        launch(pdl_, k_cheb_first<T>, gb, TH, s_, n, b, L.dinv.p, (T)L.c1[0], L.d.p, xa, done);
+        mark(tag + "smooth (first, no product)");
+    }
     for (int k = 1; k < deg; ++k) {
         enqueue_step(L, b, xa, (T)L.c1[k], (T)L.c2[k], xb);
         mark(tag + "smooth pre");
@@ -2840,15 +2861,31 @@ const T* SolverImpl::enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b) {
     enqueue_residual(L, b, xa);
     mark(tag + "residual");
     T* bc = l + 1 == H.levels.size() ? H.cb.p : H.levels[l + 1].b.p;
-    if (L.Ro.ok)
+    // The next level's first step rides on the restriction when that level smooths with
+    // separate launches (not the coarsest, the fused tail or the cluster legs).
+    const bool fuse_first = l + 1 < H.levels.size() && L.Ro.ok &&
+                            !((int)(l + 1) == H.tail_from && tail_on_) &&
+                            !(cluster_on_ && l + 1 < H.cluster.size() && H.cluster[l + 1]);
+    if (fuse_first) {
+        MgLevel<T>& N = H.levels[l + 1];
+        const auto v = L.Ro.view();
+        if (v.K == 27)
+            launch(pdl_, k_restrict_first<T, 27>, row_blocks(L.nc), TH, s_, v, (const T*)L.r.p,
+                   bc, (const T*)N.dinv.p, (T)N.c1[0], N.d.p, N.xa.p, done);
+        else
+            launch(pdl_, k_restrict_first<T, 0>, row_blocks(L.nc), TH, s_, v, (const T*)L.r.p,
+                   bc, (const T*)N.dinv.p, (T)N.c1[0], N.d.p, N.xa.p, done);
+    } else if (L.Ro.ok) {
         launch_transfer(L.Ro, (const T*)L.r.p, bc, 0, done, s_, pdl_);
-    else
-        launch(pdl_, k_restrict<T>, row_blocks(L.nc), TH, s_, L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p,
-                                                       bc, done);
+    } else {
+        launch(pdl_, k_restrict<T>, row_blocks(L.nc), TH, s_, L.nc, L.rptr.p, L.ridx.p, L.rval.p,
+               L.r.p, bc, done);
+    }
     FG_CHECK_LAUNCH();
-    mark(tag + "restrict");
-    launches_ += deg + 2;
-    const T* ec = enqueue_vcycle(H, l + 1, bc);
+    mark(tag + (fuse_first ? "restrict + L" + std::to_string(l + 1) + " first smooth"
+                           : std::string("restrict")));
+    launches_ += (started ? deg + 1 : deg + 2);
+    const T* ec = enqueue_vcycle(H, l + 1, bc, fuse_first);
     if (L.Po.ok)
         launch_transfer(L.Po, ec, xa, 1, done, s_, pdl_);
     else

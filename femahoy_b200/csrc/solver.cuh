@@ -285,7 +285,8 @@ class SolverImpl {
     void build_levels(const std::vector<const DevCsr*>& mats, std::vector<DevRect>& ps,
                       const HostLevel& coarsest, Hierarchy<T>* H);
     template <class T>
-    const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b);
+    // `started`: the level's first smoothing step was done by the finer level's restriction.
+    const T* enqueue_vcycle(Hierarchy<T>& H, size_t l, const T* b, bool started = false);
     template <class T>
     void enqueue_step(MgLevel<T>& L, const T* b, const T* xin, T c1, T c2, T* xout);
     template <class T>
