@@ -1710,12 +1710,6 @@ HostRect transpose(const HostRect& p) {
     return r;
 }
 
-template <class T>
-static void upload_values(const std::vector<double>& v, DevBuf<T>* d, cudaStream_t s) {
-    std::vector<T> t(v.begin(), v.end());
-    d->upload(t.data(), t.size(), s);
-    FG_CUDA(cudaStreamSynchronize(s));
-}
 
 // The FP16 copy of a stencil's coefficients (StencilOpH): each divided by the largest
 // magnitude and rounded to nearest. The FP32 coefficients stay for the fused coarse kernel.
