@@ -65,6 +65,8 @@ def args():
                    help="Chebyshev smoother polynomial: 0/1 first kind, 4 fourth kind")
     p.add_argument("--cluster", type=int, default=0,
                    help="small levels: 1 each leg as 1 cluster launch, 0 a launch per step")
+    p.add_argument("--upper", type=float, default=0.0,
+                   help="Chebyshev interval upper end over lambda_max (0: 1.1)")
     p.add_argument("--l2", type=int, default=0,
                    help="1: the coarsest inverse persisting in L2")
     p.add_argument("--tiles", type=int, default=0,
@@ -449,6 +451,7 @@ def run_ours(opt, rank, world, local):
                                          values=opt.values, tiles=opt.tiles,
                                          stencil=opt.stencil, l2=opt.l2,
                                          smoother=opt.smoother, cluster=opt.cluster,
+                                         upper=opt.upper,
                                          coarsest=opt.coarsest,
                                          lower=opt.lower)).with_tol(tol)
         return s, time.perf_counter() - t

@@ -62,7 +62,8 @@ class Options_t(C.Structure):
                 ("max_levels", C.c_int), ("graph", C.c_int), ("format", C.c_int),
                 ("tail", C.c_int), ("launch", C.c_int), ("values", C.c_int),
                 ("tiles", C.c_int), ("axes", C.c_int), ("stencil", C.c_int),
-                ("smoother", C.c_int), ("cluster", C.c_int), ("l2", C.c_int)]
+                ("smoother", C.c_int), ("cluster", C.c_int), ("l2", C.c_int),
+                ("upper", C.c_double)]
 
 
 class BatchStats_t(C.Structure):

@@ -450,8 +450,11 @@ static int solver_new_impl(const femgpu_csr* a, const femgpu_unknowns* u, int me
             o.l2 = options->l2;
             o.smoother = options->smoother ? options->smoother : 4;
             o.cluster = options->cluster;
+            o.upper = options->upper;
         }
         require(o.cluster == 0 || o.cluster == 1, "cluster is 0 (off) or 1 (on)");
+        require(o.upper == 0.0 || (o.upper >= 0.5 && o.upper <= 4.0),
+                "upper is 0 (1.1) or a multiple of lambda_max in [0.5, 4]");
         require(o.smoother == 1 || o.smoother == 4,
                 "smoother is 1 (the first-kind Chebyshev polynomial) or 0 or 4 (the fourth kind)");
         require(o.l2 == 0 || o.l2 == 1, "l2 is 0 (plain loads) or 1 (the coarsest inverse "

@@ -1991,13 +1991,14 @@ template double lambda_max<float>(const Operator<float>&, const double*, cudaStr
                                   DevBuf<double>&);
 
 void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
-               std::vector<double>* c2, int kind) {
+               std::vector<double>* c2, int kind, double upper) {
+    if (!(upper > 0.0)) upper = 1.1;
     if (kind == 4) {
         // The fourth-kind Chebyshev smoother on [0, 1.1] x lambda_max of D^-1 A (J. Lottes,
         // Optimal polynomial smoothers for multigrid V-cycles, Numer. Linear Algebra Appl. 30
         // (2023) e2518): d_0 = 4 / (3 l) D^-1 r_0, d_k = (2k - 1) / (2k + 3) d_(k-1)
         // + (8k + 4) / ((2k + 3) l) D^-1 r_k.
-        const double l = 1.1 * lam;
+        const double l = upper * lam;
         c1->assign(degree, 0.0);
         c2->assign(degree, 0.0);
         (*c1)[0] = 4.0 / (3.0 * l);
@@ -2009,7 +2010,7 @@ void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
     }
     // Y. Saad, Iterative Methods for Sparse Linear Systems, 2nd ed., SIAM 2003, algorithm 12.1,
     // on the interval [lower, 1.1] x lambda_max of D^-1 A.
-    double hi = 1.1 * lam, lo = lower * lam;
+    double hi = upper * lam, lo = lower * lam;
     double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo), sigma = theta / delta;
     c1->assign(degree, 0.0);
     c2->assign(degree, 0.0);
@@ -2279,10 +2280,10 @@ void SolverImpl::apply_degree(int degree, int coarse) {
     if (coarse <= 0) coarse = degree;
     for (size_t l = 0; l < H32_.levels.size(); ++l)
         chebyshev(H32_.levels[l].lambda, l == 0 ? degree : coarse, lower, &H32_.levels[l].c1,
-                  &H32_.levels[l].c2, opt_.smoother);
+                  &H32_.levels[l].c2, opt_.smoother, opt_.upper);
     for (size_t l = 0; l < H64_.levels.size(); ++l)
         chebyshev(H64_.levels[l].lambda, l == 0 ? degree : coarse, lower, &H64_.levels[l].c1,
-                  &H64_.levels[l].c2, opt_.smoother);
+                  &H64_.levels[l].c2, opt_.smoother, opt_.upper);
     // The captured loop holds the coefficients as kernel arguments.
     if (exec_) cudaGraphExecDestroy(exec_);
     if (graph_) cudaGraphDestroy(graph_);
@@ -2503,7 +2504,7 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         reciprocal<T>(lv.n, dg.p, lv.dinv.p, s_);
         int deg = opt_.degree > 0 ? opt_.degree : 2;
         double lower = opt_.lower > 0 ? opt_.lower : 0.3;
-        chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2, opt_.smoother);
+        chebyshev(lv.lambda, deg, lower, &lv.c1, &lv.c2, opt_.smoother, opt_.upper);
         t_lam.reset();
         PhaseTimer t_tr{this, "transfers", s_};
         // Transfers to the next level: P and R = P^T (each row's columns increasing).

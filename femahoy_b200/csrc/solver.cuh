@@ -108,10 +108,10 @@ HostRect transpose(const HostRect& p);
 template <class T>
 double lambda_max(const Operator<T>& A, const double* dg, cudaStream_t s,
                   DevBuf<double>& partial);
-// kind 1: the first-kind Chebyshev polynomial on [lower, 1.1] lambda; 4: the fourth kind on
-// [0, 1.1] lambda.
+// kind 1: the first-kind Chebyshev polynomial on [lower, upper] lambda; 4: the fourth kind on
+// [0, upper] lambda (upper 0: 1.1).
 void chebyshev(double lam, int degree, double lower, std::vector<double>* c1,
-               std::vector<double>* c2, int kind = 1);
+               std::vector<double>* c2, int kind = 1, double upper = 1.1);
 
 // The scalars of a PCG solve, in device memory.
 struct Scalars {
@@ -240,6 +240,7 @@ struct Options {
     int l2 = 0;      // 1: the coarsest inverse persisting in L2
     int smoother = 4;  // the Chebyshev polynomial's kind: 1 first, 4 fourth
     int cluster = 0;   // 1: small levels' legs as 1 cluster launch each; 0: a launch per step
+    double upper = 0;  // the Chebyshev interval's upper end over lambda_max (0: 1.1)
 };
 
 class SolverImpl {

@@ -119,12 +119,13 @@ class Options:
     smoother: int = 0  # Chebyshev polynomial: 0 the default, 1 the first kind, 4 the fourth
     cluster: int = 0  # small levels: 1 each leg as 1 cluster launch, 0 a launch per step
     l2: int = 0      # 1: the coarsest inverse persisting in L2
+    upper: float = 0.0  # Chebyshev interval upper end over lambda_max (0: 1.1)
 
     def _c(self):
         return L.Options_t(self.precision, self.degree, self.lower, self.sell_c, 0, self.coarsest,
                            self.max_levels, self.graph, self.format, self.tail, self.launch,
                            self.values, self.tiles, self.axes, self.stencil, self.smoother,
-                           self.cluster, self.l2)
+                           self.cluster, self.l2, self.upper)
 
 
 def unknowns_c(unknowns: "Unknowns", keep: list) -> L.Unknowns_t:

@@ -272,6 +272,8 @@ typedef struct femgpu_options {
                              persisting access window on its product; the process's persisting
                              L2 limit is raised to the inverse's size, at most the device's
                              maximum); 0 (default) = plain loads */
+    double upper;         /* the Chebyshev interval's upper end as a multiple of the power
+                             method's lambda_max; 0 = 1.1 */
 } femgpu_options;
 
 /* solve.rs:81-86 `Stats`, plus the true residual |b - A x| / |b| computed in FP64 at the end
