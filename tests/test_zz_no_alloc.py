@@ -1,4 +1,4 @@
-"""femgpu_reduced_rhs_noalloc against femgpu_reduced_rhs, through the C ABI.
+"""femgpu_reduced_rhs_noalloc against femgpu_reduced_rhs and the oracle, through the C ABI.
 
 The no-allocation entry point exists for callers that must not call cudaMalloc or cudaFree:
 code that shares the GPU with other work in flight (cudaFree waits for the whole device and
@@ -22,14 +22,22 @@ from femahoy_b200 import meshgen as mg
 pytestmark = pytest.mark.gpu
 
 
-def _problems():
+def _problems(with_oracle=False):
     heat = mg.heat_cube(12)
     K1 = fg.Csr.assemble(fg.P1_HEAT, heat.xyz, heat.nodes, heat.coef)
     beam = mg.cantilever_p1(dims=(10, 2, 2), lengths=(25.0, 5.0, 5.0))
     K2 = fg.Csr.assemble(fg.P1_ELASTIC, beam.xyz, beam.nodes, beam.coef)
     rng = np.random.default_rng(7)
     t2 = np.where(beam.fixed, rng.uniform(-0.1, 0.1, beam.n_unknowns), 0.0)
-    return [(K1, heat.load, heat.values, heat.free), (K2, beam.load, t2, beam.free)]
+    out = [(K1, heat.load, heat.values, heat.free), (K2, beam.load, t2, beam.free)]
+    if not with_oracle:
+        return out
+    import oracle
+    K1o = oracle.pattern(heat.n_points, heat.nodes)
+    K1o.assemble(0, heat.xyz, heat.nodes, heat.coef)
+    K2o = oracle.pattern(3 * beam.n_points, oracle.dof_elements(beam.nodes))
+    K2o.assemble(1, beam.xyz, beam.nodes, beam.coef)
+    return [p + (o,) for p, o in zip(out, (K1o, K2o))]
 
 
 def _noalloc(torch, K, load, t, free, arrays=None, nfree=None, check=True):
@@ -62,13 +70,16 @@ def _noalloc(torch, K, load, t, free, arrays=None, nfree=None, check=True):
 
 
 def test_noalloc_right_side_equals_the_allocating_one_twice_in_a_row():
+    """... and the oracle's reduced_rhs (heat.rs:1219-1244), bit for bit."""
     torch = pytest.importorskip("torch")
-    for K, load, t, free in _problems():
+    for K, load, t, free, Ko in _problems(with_oracle=True):
         expected = fg.reduced_rhs(K, load, t, free)
         got = _noalloc(torch, K, load, t, free)
         # The same sums in the same order: equal bit for bit (the other right-side tests are
         # bit-exact too).
         assert np.array_equal(got.view(np.uint64), expected.view(np.uint64))
+        want = Ko.reduced_rhs(load, t, free)
+        assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
 
 
 def test_noalloc_refuses_a_matrix_past_its_scratch():
