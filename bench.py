@@ -734,6 +734,7 @@ def run_batch(opt, rank, world, local):
         return e0.elapsed_time(e1), stats, clk
 
     mixed, setup_mixed = make(fg.MIXED)
+    batch_phases = setup_phases(mixed)
     rows = mixed.rows
     clocks = Clocks(torch.cuda.current_device())
     ms, stats, clk = timed(mixed, opt.steps, opt.warmup, clocks)
@@ -809,7 +810,7 @@ def run_batch(opt, rank, world, local):
         "fp64": {"value": value64, "unit": UNIT, "ms_per_step": ms64 / opt.steps},
         "mixed_over_fp64": value / value64,
         "setup_s": {"assembly": assemble_s, "batch_mixed": setup_mixed,
-                    "batch_fp64": setup_fp64},
+                    "batch_fp64": setup_fp64, "phases_mixed": batch_phases},
         "device_bytes": nbytes,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,

@@ -178,6 +178,7 @@ SIGNATURES = {
     "femgpu_batch_set_max_iter": (C.c_int, [C.c_void_p, C.c_size_t]),
     "femgpu_batch_systems": (C.c_int, [C.c_void_p, C.c_void_p]),
     "femgpu_batch_levels": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_batch_describe": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "femgpu_batch_solve": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.POINTER(BatchStats_t)]),
     "femgpu_batch_solve_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -74,6 +74,12 @@ class Batch:
         L.check(L.lib().femgpu_batch_set_max_iter(self._h, m))
         return self
 
+    def describe(self):
+        """The setup seconds by phase."""
+        buf = C.create_string_buffer(4096)
+        L.check(L.lib().femgpu_batch_describe(self._h, buf, 4096))
+        return buf.value.decode()
+
     def levels(self):
         k = L.lib().femgpu_batch_levels(self._h, None)
         out = np.zeros(k, dtype=np.uint64)

@@ -887,6 +887,8 @@ class BatchImpl {
     void segments(size_t* iterations, double* truth, double* residual, int* status) const;
     const std::vector<int64_t>& offsets() const { return offsets_; }
     std::vector<int64_t> level_sizes() const { return sizes_; }
+    // "setup seconds: phase s; ..." of the batch's creation.
+    std::string describe() const;
     size_t bytes() const;
     cudaStream_t stream() const { return s_; }
     // The mean device time (ms) of 1 launch of the finest level's Chebyshev step over all
@@ -966,6 +968,21 @@ class BatchImpl {
     int B_ = 0, R_ = 1, nchunks_ = 0, max_iter_ = 500, graph_max_iter_ = -1;
     int64_t n_ = 0;
     std::vector<int64_t> offsets_, sizes_;  // the caller's member order
+    // The creation's phases (host seconds until each phase's device work finished).
+    std::vector<std::pair<std::string, double>> setup_s_;
+    std::chrono::steady_clock::time_point phase_t0_;
+    void phase_end(const char* name) {
+        FG_CUDA(cudaStreamSynchronize(s_));
+        const auto t = std::chrono::steady_clock::now();
+        const double sec = std::chrono::duration<double>(t - phase_t0_).count();
+        phase_t0_ = t;
+        for (auto& ph : setup_s_)
+            if (ph.first == name) {
+                ph.second += sec;
+                return;
+            }
+        setup_s_.emplace_back(name, sec);
+    }
     std::vector<int> order_;                // batch position -> caller's member
     DevBuf<int> map_;                       // batch row -> caller's row
     Sell<double> A64_;  // the block-diagonal finest matrix (batch order), exactly
@@ -1083,6 +1100,8 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     R_ = nrhs;
     B_ = (int)a.size();
     if (B_ < 1) throw Failure(FEMGPU_ERR_INVALID, "an empty batch");
+    setup_s_.clear();
+    phase_t0_ = std::chrono::steady_clock::now();
     // Each member's hierarchy on the host (multigrid.rs:84-139), the members shared among the
     // host threads.
     std::vector<HostCsr> fine(B_);
@@ -1090,6 +1109,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
         if (a[b]->n < 1) throw Failure(FEMGPU_ERR_INVALID, "an empty system");
         fine[b] = download_csr(*a[b], s_);
     }
+    phase_end("matrices to host");
     std::vector<SystemHierarchy> H(B_);
     // 1024 by default: the thin members (plates 1 cell thick) converge slowly under plane
     // coarsening, and a dense deepest level of up to 1024 unknowns per member cuts the most
@@ -1167,6 +1187,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     for (int b = 0; b < B_; ++b)
         if (codes[b] != FEMGPU_OK)
             throw Failure(codes[b], "system " + std::to_string(b) + ": " + errors[b]);
+    phase_end("members' coarsening and Galerkin products (device, host threads)");
     // The caller's row offsets, then the batch order: deepest first (stable).
     offsets_.assign(B_ + 1, 0);
     for (int b = 0; b < B_; ++b) offsets_[b + 1] = offsets_[b] + H[b].mats[0].n;
@@ -1210,6 +1231,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
         }
         FG_CUDA(cudaStreamSynchronize(s_));
     }
+    phase_end("finest operator (host combination, 3x3 blocks)");
     // The chunks of the PCG kernels: rows of 1 member each; up to 4 rows per thread, or 2 block
     // rows (6 rows) per thread with the 3x3-block operator, whose chunks hold whole nodes.
     const int chunk_rows = fine3_ ? 3 * 2 * (BTH / R_) : 4 * BTH / R_;
@@ -1239,6 +1261,17 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     for (auto* v : {&x_, &r_, &p_, &q_, &b_, &stage_}) v->alloc((size_t)n_ * R_);
     if (opt_.precision == FEMGPU_MIXED) r32_.alloc((size_t)n_ * R_);
     FG_CUDA(cudaStreamSynchronize(s_));
+    phase_end("vectors");
+}
+
+std::string BatchImpl::describe() const {
+    std::string out = "setup seconds:";
+    char buf[128];
+    for (const auto& ph : setup_s_) {
+        std::snprintf(buf, sizeof buf, " %s %.3f;", ph.first.c_str(), ph.second);
+        out += buf;
+    }
+    return out + "\n";
 }
 
 template <class T>
@@ -1315,6 +1348,7 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             L.rval.upload(rv.data(), rv.size(), s_);
             L.d.alloc((size_t)L.ns * R_);
             L.r.alloc((size_t)L.ns * R_);
+            phase_end("smoothed levels (host combination, lambda_max, transfers)");
         }
         // The members that end here: a dense inverse each, from a dense Cholesky factor on the
         // device, made exactly symmetric, stored in tiles of DTH rows (k_bdense's layout).
@@ -1387,6 +1421,7 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             L.doff.upload(off.data(), off.size(), s_);
             L.dioff.upload(ioff.data(), ioff.size(), s_);
             L.tiles.upload(tiles.data(), tiles.size(), s_);
+            phase_end("deepest levels' dense inverses (host threads)");
         }
         for (auto* v : {&L.b, &L.xa, &L.xb}) v->alloc((size_t)L.n * R_);
         FG_CUDA(cudaStreamSynchronize(s_));
@@ -2086,6 +2121,13 @@ int femgpu_batch_systems(const femgpu_batch* b, size_t* offsets) {
     if (offsets)
         for (size_t k = 0; k < o.size(); ++k) offsets[k] = (size_t)o[k];
     return (int)o.size() - 1;
+}
+
+int femgpu_batch_describe(const femgpu_batch* b, char* buf, size_t len) {
+    if (!b || !buf || len == 0) return FEMGPU_ERR_INVALID;
+    const std::string d = b->impl.describe();
+    std::snprintf(buf, len, "%s", d.c_str());
+    return FEMGPU_OK;
 }
 
 int femgpu_batch_levels(const femgpu_batch* b, size_t* sizes) {

@@ -455,6 +455,9 @@ int femgpu_batch_set_max_iter(femgpu_batch* b, size_t max_iter); /* default PCG_
 int femgpu_batch_systems(const femgpu_batch* b, size_t* offsets);
 /* The number of levels; `sizes` (may be null) gets the combined unknowns of each. */
 int femgpu_batch_levels(const femgpu_batch* b, size_t* sizes);
+/* The batch's setup seconds by phase ("setup seconds: phase s; ..."), as much as fits in `len`
+ * bytes with the terminating 0. No reference counterpart. */
+int femgpu_batch_describe(const femgpu_batch* b, char* buf, size_t len);
 /* Solves every segment from the start value in x (host arrays of rows * nrhs values). A segment
  * that hits the iteration limit or breaks down makes the call return FEMGPU_ERR_NOT_CONVERGED
  * naming the first such segment, with every x written; femgpu_batch_segments tells which. */
