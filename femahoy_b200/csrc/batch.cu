@@ -841,6 +841,17 @@ __global__ void k_sloop_control(cudaGraphConditionalHandle hc, int nseg, StreamH
     if ((threadIdx.x & 31) == 0 && active) atomicAdd(served_iterations, (unsigned long long)active);
 }
 
+// A member's FP64 inverse h (m x m, row-major) made exactly symmetric and stored in row tiles
+// of DTH rows, each tile by column (k_bdense's layout), in T.
+template <class T>
+__global__ void k_tile_inverse(int64_t m, const double* __restrict__ h, T* __restrict__ t) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < m * m;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / m, c = e % m;
+        t[(r / DTH) * DTH * m + c * DTH + r % DTH] = (T)(0.5 * (h[r * m + c] + h[c * m + r]));
+    }
+}
+
 // ------------------------------------------------------------------ the batch
 struct SystemHierarchy {
     std::vector<HostCsr> mats;
@@ -1366,6 +1377,7 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             }
             L.ntiles = (int)tiles.size();
             L.inv.alloc(ioff[L.ndense]);
+            L.inv.zero(s_);  // the padding rows of each member's last tile
             FG_CUDA(cudaStreamSynchronize(s_));
             // The members' inverses on the host threads, each with its own stream (each is a
             // chain of small launches), into their own places of L.inv.
@@ -1386,22 +1398,18 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
                         }
                         return;
                     }
+                    // The thread's work buffers and inverse, kept across its members (no
+                    // cudaFree, which would wait on every stream of the device, per member).
+                    DenseWork work;
+                    DevBuf<double> inv64;
                     for (int j = th; j < L.ndense; j += threads) {
                         try {
                             const int64_t m = off[j + 1] - off[j];
-                            DevBuf<double> inv64;
-                            dense_inverse(H[S + j].mats[l], &inv64, st);
-                            std::vector<double> h((size_t)(m * m));
-                            inv64.download(h.data(), m * m, st);
-                            FG_CUDA(cudaStreamSynchronize(st));
-                            const int64_t mt = ioff[j + 1] - ioff[j];
-                            std::vector<T> t((size_t)mt, (T)0);
-                            for (int64_t r = 0; r < m; ++r)
-                                for (int64_t c = 0; c < m; ++c)
-                                    t[(r / DTH) * DTH * m + c * DTH + r % DTH] =
-                                        (T)(0.5 * (h[r * m + c] + h[c * m + r]));
-                            FG_CUDA(cudaMemcpyAsync(L.inv.p + ioff[j], t.data(), mt * sizeof(T),
-                                                    cudaMemcpyHostToDevice, st));
+                            if (inv64.count < (size_t)(m * m)) inv64.alloc(m * m);
+                            dense_inverse(H[S + j].mats[l], inv64.p, &work, st);
+                            k_tile_inverse<T><<<blocks_for(m * m, BTH), BTH, 0, st>>>(
+                                m, inv64.p, L.inv.p + ioff[j]);
+                            FG_CUDA(cudaGetLastError());
                             FG_CUDA(cudaStreamSynchronize(st));
                         } catch (const Failure& e) {
                             codes[j] = e.code;

@@ -280,7 +280,7 @@ void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0
     FG_CHECK_LAUNCH();
 }
 
-void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
+void dense_inverse(const HostCsr& a, double* inv, DenseWork* w, cudaStream_t s,
                    std::vector<std::pair<const char*, double>>* stages) {
     const int64_t n = a.n;
     auto t0 = std::chrono::steady_clock::now();
@@ -291,23 +291,29 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
         stages->emplace_back(name, std::chrono::duration<double>(t1 - t0).count());
         t0 = t1;
     };
-    DevBuf<int64_t> ptr;
-    DevBuf<uint32_t> idx;
-    DevBuf<double> val, diag(n), L(n * n), W(n * n);
-    inv->alloc(n * n);
+    // The work buffers grow to the largest system they have served and are kept.
+    auto fit = [&](DevBuf<double>& b, size_t count) {
+        if (b.count < count) b.alloc(count);
+    };
+    fit(w->diag, n);
+    fit(w->L, n * n);
+    fit(w->W, n * n);
+    if (!w->status.p) w->status.alloc(1);
+    double* L = w->L.p;
+    double* W = w->W.p;
     stage("buffers");
-    ptr.upload(a.ptr.data(), n + 1, s);
-    idx.upload(a.idx.data(), a.nnz(), s);
-    val.upload(a.val.data(), a.nnz(), s);
-    L.zero(s);
-    k_scatter_dense<<<blocks_for(n, TH), TH, 0, s>>>(n, ptr.p, idx.p, val.p, L.p, diag.p);
-    DevBuf<unsigned long long> status(1);
-    FG_CUDA(cudaMemsetAsync(status.p, 0xff, sizeof(unsigned long long), s));
-    dense_partial_cholesky(L.p, n, n, diag.p, 0, status.p, s);
+    w->ptr.upload(a.ptr.data(), n + 1, s);
+    w->idx.upload(a.idx.data(), a.nnz(), s);
+    w->val.upload(a.val.data(), a.nnz(), s);
+    FG_CUDA(cudaMemsetAsync(L, 0, (size_t)n * n * sizeof(double), s));
+    k_scatter_dense<<<blocks_for(n, TH), TH, 0, s>>>(n, w->ptr.p, w->idx.p, w->val.p, L,
+                                                     w->diag.p);
+    FG_CUDA(cudaMemsetAsync(w->status.p, 0xff, sizeof(unsigned long long), s));
+    dense_partial_cholesky(L, n, n, w->diag.p, 0, w->status.p, s);
     stage("factor");
-    const unsigned long long bad = fetch(status.p, s);
+    const unsigned long long bad = fetch(w->status.p, s);
     if (bad != ~0ull) {
-        const double d = fetch(diag.p + bad, s);
+        const double d = fetch(w->diag.p + bad, s);
         char buf[320];
         std::snprintf(buf, sizeof buf,
                       "the matrix is not positive definite: the pivot of column %llu is 0 or less "
@@ -316,25 +322,32 @@ void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
         throw Failure(FEMGPU_ERR_NOT_SPD, buf);
     }
     // W = L^-1 by block rows of 32: each block's triangle solve, then the rows below updated.
-    k_identity<<<blocks_for(n * n, TH), TH, 0, s>>>(n, W.p);
+    k_identity<<<blocks_for(n * n, TH), TH, 0, s>>>(n, W);
     for (int64_t b0 = 0; b0 < n; b0 += PANEL) {
         const int kb = (int)std::min<int64_t>(PANEL, n - b0);
         const int64_t ncols = b0 + kb;
-        k_trsm_rows<<<(unsigned)((ncols + ROWS_TH - 1) / ROWS_TH), ROWS_TH, 0, s>>>(W.p, L.p, n, b0,
+        k_trsm_rows<<<(unsigned)((ncols + ROWS_TH - 1) / ROWS_TH), ROWS_TH, 0, s>>>(W, L, n, b0,
                                                                                     kb, ncols);
         const int64_t rows = n - b0 - kb;
         if (rows > 0) {
             dim3 grid((unsigned)((rows + TILE - 1) / TILE), (unsigned)((ncols + TILE - 1) / TILE));
-            k_gemm_sub<<<grid, TH, 0, s>>>(W.p + b0 + kb, n, L.p + (b0 + kb) + b0 * n, n,
-                                           W.p + b0, n, rows, ncols, kb);
+            k_gemm_sub<<<grid, TH, 0, s>>>(W + b0 + kb, n, L + (b0 + kb) + b0 * n, n, W + b0, n,
+                                           rows, ncols, kb);
         }
     }
     stage("L^-1");
     const int64_t T = (n + TILE - 1) / TILE;
-    k_gram_lower<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(W.p, n, inv->p);
+    k_gram_lower<<<(unsigned)(T * (T + 1) / 2), TH, 0, s>>>(W, n, inv);
     FG_CHECK_LAUNCH();
-    FG_CUDA(cudaStreamSynchronize(s));
     stage("W^T W");
+}
+
+void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
+                   std::vector<std::pair<const char*, double>>* stages) {
+    DenseWork w;
+    inv->alloc(a.n * a.n);
+    dense_inverse(a, inv->p, &w, s, stages);
+    FG_CUDA(cudaStreamSynchronize(s));
 }
 
 }  // namespace femgpu

@@ -31,4 +31,17 @@ void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0
 void dense_inverse(const HostCsr& a, DevBuf<double>* inv, cudaStream_t s,
                    std::vector<std::pair<const char*, double>>* stages = nullptr);
 
+// Work buffers of dense_inverse, kept across calls (many small systems on 1 stream allocate and
+// free nothing per system, so no call waits on the whole device in cudaFree).
+struct DenseWork {
+    DevBuf<int64_t> ptr;
+    DevBuf<uint32_t> idx;
+    DevBuf<double> val, diag, L, W;
+    DevBuf<unsigned long long> status;
+};
+// The same into `inv` (n x n, the caller's), with the buffers of `w`; returns with the work
+// queued on `s` (the pivot test has synchronized `s` after the factor).
+void dense_inverse(const HostCsr& a, double* inv, DenseWork* w, cudaStream_t s,
+                   std::vector<std::pair<const char*, double>>* stages = nullptr);
+
 }  // namespace femgpu
