@@ -98,7 +98,48 @@ class Peak_t(C.Structure):
 _lib = None
 
 # Every symbol of include/femgpu.h with its signature.
+class Outline_t(C.Structure):
+    _fields_ = [("circle", C.c_int), ("ncorners", C.c_size_t), ("corners", C.c_void_p),
+                ("centre", C.c_double * 2), ("radius", C.c_double)]
+
+
+class Part_t(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("material", C.c_size_t), ("priority", C.c_int64),
+                ("lo", C.c_double * 3), ("hi", C.c_double * 3), ("has_footprint", C.c_int),
+                ("outline", Outline_t), ("nholes", C.c_size_t), ("holes", C.c_void_p)]
+
+
+class Spacing_t(C.Structure):
+    _fields_ = [("max_cell", C.c_double), ("max_growth", C.c_double), ("min_cells", C.c_size_t)]
+
+
+class TetmeshCounts_t(C.Structure):
+    _fields_ = [(k, C.c_size_t) for k in ("points", "tets", "faces", "face_circles", "circles",
+                                           "triangles", "planes")]
+
+
+CLASSIFY_FN = C.CFUNCTYPE(C.c_uint32, C.POINTER(C.c_double), C.c_void_p)
+
 SIGNATURES = {
+    "femgpu_prism_mesh": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(Spacing_t),
+                                    C.c_size_t, C.c_char_p, C.c_int, C.c_void_p, C.c_size_t,
+                                    C.POINTER(C.c_void_p)]),
+    "femgpu_tetmesh_sizes": (C.c_int, [C.c_void_p, C.POINTER(TetmeshCounts_t)]),
+    "femgpu_tetmesh_copy": (C.c_int, [C.c_void_p] + [C.c_void_p] * 9),
+    "femgpu_tetmesh_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "femgpu_tetmesh_free": (None, [C.c_void_p]),
+    "femgpu_axis_planes": (C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.POINTER(Spacing_t),
+                                     C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                     C.POINTER(C.c_size_t)]),
+    "femgpu_mesh2d": (C.c_int, [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_double,
+                                C.c_double, C.c_int, CLASSIFY_FN, C.c_void_p,
+                                C.POINTER(C.c_void_p)]),
+    "femgpu_mesh2_sizes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t),
+                                     C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "femgpu_mesh2_copy": (C.c_int, [C.c_void_p] + [C.c_void_p] * 7),
+    "femgpu_mesh2_free": (None, [C.c_void_p]),
+    "femgpu_split_prism": (C.c_int, [C.c_void_p, C.c_void_p]),
     "femgpu_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "femgpu_version": (C.c_char_p, []),
     "femgpu_assemble": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_size_t,

@@ -42,10 +42,13 @@ UNITS = [
     ("dense_eigen.cu", []),
     ("dense_factor.cu", []),
     ("offsets.cu", []),
+    ("extrude.cu", ["-fmad=false"]),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),
              ("order.cpp", ["-O3", "-std=c++17", "-fPIC", "-pthread"]),
+             ("mesh2d.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]),
+             ("prism.cpp", ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off"]),
 ]
 
 

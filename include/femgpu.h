@@ -704,6 +704,99 @@ int femgpu_reactions(const femgpu_csr* k, const double* u, const double* force,
                      const double* applied, double gross, double* load_force, double* total,
                      double* gross_out, double* imbalance);
 
+/* ---------------------------------------------------------------- prism meshes */
+
+/* prism.rs:29-37 Outline: a polygon (`ncorners` corners, 2 coordinates each across the axis, in
+ * either direction) or a circle (`centre`, `radius`). */
+typedef struct femgpu_outline {
+    int circle;
+    size_t ncorners;
+    const double* corners;
+    double centre[2];
+    double radius;
+} femgpu_outline;
+
+/* grid.rs:22-35 Part: a box [lo, hi] of material `material`; where parts overlap the higher
+ * `priority` holds the space. With `has_footprint` the part is the prism of the footprint
+ * (prism.rs:40-44: `outline` and `nholes` holes) between lo and hi on the extrusion axis. */
+typedef struct femgpu_part {
+    const char* name;
+    size_t material;
+    int64_t priority;
+    double lo[3], hi[3];
+    int has_footprint;
+    femgpu_outline outline;
+    size_t nholes;
+    const femgpu_outline* holes;
+} femgpu_part;
+
+/* grid.rs:37-46 Spacing. */
+typedef struct femgpu_spacing {
+    double max_cell;
+    double max_growth;
+    size_t min_cells;
+} femgpu_spacing;
+
+typedef struct femgpu_tetmesh femgpu_tetmesh; /* prism.rs:117-132 TetMesh */
+typedef struct femgpu_tetmesh_counts {
+    size_t points, tets, faces, face_circles, circles, triangles, planes;
+} femgpu_tetmesh_counts;
+
+/* prism::mesh_hollow (prism.rs:185-380; prism::mesh, prism.rs:170-181, with no hollow part), as
+ * heat.rs:898, elastic_tet.rs:98 and modes.rs:432 call it: the footprints of all parts meshed in
+ * 1 quality triangle mesh on the host (mesh2d.rs), extruded through the graded planes of `axis`
+ * (grid.rs:418) and cut into 3 tetrahedra per prism on the device. `hollow[k]` nonzero: part k
+ * keeps its space but no tetrahedra (missing items: 0). More than `max_points` points ends with
+ * FEMGPU_ERR_TOO_LARGE and the text `refusal`; the reference's other errors come with their texts
+ * (FEMGPU_ERR_INVALID). The points and tetrahedra stay on the device for femgpu_assemble_device
+ * (femgpu_tetmesh_device) and are copied to the host (femgpu_tetmesh_copy). Host pointers. */
+int femgpu_prism_mesh(const femgpu_part* parts, size_t nparts, int axis,
+                      const femgpu_spacing* spacing, size_t max_points, const char* refusal,
+                      int periodic, const uint8_t* hollow, size_t nhollow, femgpu_tetmesh** out);
+int femgpu_tetmesh_sizes(const femgpu_tetmesh* m, femgpu_tetmesh_counts* sizes);
+/* Any pointer may be null (skipped). points 3 per point; tets 4 per tetrahedron (positive
+ * volume); part 1 per tetrahedron; the boundary faces sorted by (tet, nodes): face_nodes 3 per
+ * face (counterclockwise from outside), face_tet, face_beyond (the hollow part beyond, or
+ * 0xffffffff), face_circle_start (faces + 1 offsets into face_circles: the circles whose outline
+ * holds the face); circles 3 per circle (centre, radius). */
+int femgpu_tetmesh_copy(const femgpu_tetmesh* m, double* points, uint32_t* tets, uint32_t* part,
+                        uint32_t* face_nodes, uint32_t* face_tet, uint32_t* face_beyond,
+                        uint64_t* face_circle_start, uint32_t* face_circles, double* circles);
+/* The device copies of the points, tetrahedra and parts (owned by the mesh). */
+int femgpu_tetmesh_device(const femgpu_tetmesh* m, const double** points, const uint32_t** tets,
+                          const uint32_t** part);
+void femgpu_tetmesh_free(femgpu_tetmesh* m);
+
+/* grid::axis_planes (grid.rs:418-484): the graded planes of axis `axis` for the parts and the
+ * `extra` key planes; `count` is set to their number and up to `cap` are written. Host only (no
+ * device work). */
+int femgpu_axis_planes(const femgpu_part* parts, size_t nparts, int axis,
+                       const femgpu_spacing* spacing, const double* extra, size_t nextra,
+                       double* planes, size_t cap, size_t* count);
+
+/* mesh2d::mesh / periodic_mesh (mesh2d.rs:87-110): the quality triangle mesh of `points` (2
+ * coordinates each) and `segments` (2 point numbers each); `classify(point, ctx)` labels a point
+ * inside a region, or returns 0xffffffff (outside). Host only (no device work). */
+typedef uint32_t (*femgpu_classify_fn)(const double* point, void* ctx);
+typedef struct femgpu_mesh2 femgpu_mesh2; /* mesh2d.rs:72-82 Mesh2 */
+int femgpu_mesh2d(const double* points, size_t npoints, const uint32_t* segments,
+                  size_t nsegments, double max_size, double max_growth, int periodic,
+                  femgpu_classify_fn classify, void* ctx, femgpu_mesh2** out);
+int femgpu_mesh2_sizes(const femgpu_mesh2* m, size_t* points, size_t* triangles,
+                       size_t* segment_edges, size_t* segment_origins);
+/* Any pointer may be null. points 2 per point; triangles 3 per triangle (counterclockwise);
+ * label 1 per triangle; across 3 per triangle (the triangle across the edge opposite each point,
+ * or 0xffffffff); the edges on segments (2 points each, smaller first, in increasing order) with
+ * their input segments: origin_start (edges + 1 offsets) into origins. */
+int femgpu_mesh2_copy(const femgpu_mesh2* m, double* points, uint32_t* triangles, uint32_t* label,
+                      uint32_t* across, uint32_t* edges, uint64_t* origin_start,
+                      uint32_t* origins);
+void femgpu_mesh2_free(femgpu_mesh2* m);
+
+/* prism::split_prism (prism.rs:144-154): the 3 tetrahedra (12 local corners) of a prism whose
+ * corners (bottom 0 1 2, top 3 4 5, 3 above 0) have the global numbers g[6]. */
+int femgpu_split_prism(const uint64_t* g, int32_t* out);
+
 #ifdef __cplusplus
 }
 #endif
