@@ -6,7 +6,7 @@ The Python names mirror the reference crate: ``Csr`` (sparse.rs), ``Solver``, ``
 ``Method``, ``Crossover``, ``Stats`` (solve.rs), ``Level`` (multigrid.rs), ``prolongation``
 (pmultigrid.rs), ``Quadratic`` (tet10.rs) and ``reduced_rhs`` (heat.rs); ``Recovery`` and
 ``Peak`` are the post-solve loop of elastic_tet.rs:367-427; ``prism`` the reference's prism
-meshes (prism.rs, mesh2d.rs).
+meshes (prism.rs, mesh2d.rs) and ``grid`` its box grid (grid.rs Grid::build).
 """
 from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, HEX8_MASS, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
                    P2_ELASTIC_ORTHO, P2_MASS, FemError, LIB_PATH, lib)
@@ -16,7 +16,7 @@ from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT
                     symbolic_counts)
 from .recover import Peak, Reactions, Recovery, reactions
 from .sparse import Csr, Rect, colour
-from . import prism
+from . import grid, prism
 
 __all__ = [
     "COLOUR", "FP64", "GATHER", "HEX8_ELASTIC", "HEX8_HEAT", "HEX8_MASS", "MIXED", "P1_ELASTIC", "P1_HEAT", "P2_ELASTIC", "P2_ELASTIC_ORTHO", "P2_MASS",
@@ -25,5 +25,5 @@ __all__ = [
     "TRANSIENT_DIRECT_LIMIT", "Cells", "Crossover", "Level", "Method", "Options", "Quadratic",
     "Solver", "coarse_matrix", "hex_elements", "hex_mass", "symbolic_counts",
     "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
-    "Recovery", "Reactions", "reactions", "prism",
+    "Recovery", "Reactions", "reactions", "grid", "prism",
 ]

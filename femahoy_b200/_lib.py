@@ -118,6 +118,11 @@ class TetmeshCounts_t(C.Structure):
                                            "triangles", "planes")]
 
 
+class BoxgridCounts_t(C.Structure):
+    _fields_ = [("planes", C.c_size_t * 3), ("grid_cells", C.c_size_t), ("points", C.c_size_t),
+                ("cells", C.c_size_t), ("faces", C.c_size_t)]
+
+
 CLASSIFY_FN = C.CFUNCTYPE(C.c_uint32, C.POINTER(C.c_double), C.c_void_p)
 
 SIGNATURES = {
@@ -140,6 +145,13 @@ SIGNATURES = {
     "femgpu_mesh2_copy": (C.c_int, [C.c_void_p] + [C.c_void_p] * 7),
     "femgpu_mesh2_free": (None, [C.c_void_p]),
     "femgpu_split_prism": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_box_grid": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(Spacing_t), C.c_void_p,
+                                  C.c_void_p, C.c_size_t, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "femgpu_boxgrid_sizes": (C.c_int, [C.c_void_p, C.POINTER(BoxgridCounts_t)]),
+    "femgpu_boxgrid_copy": (C.c_int, [C.c_void_p] + [C.c_void_p] * 9),
+    "femgpu_boxgrid_device": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p),
+                                        C.POINTER(C.c_void_p)]),
+    "femgpu_boxgrid_free": (None, [C.c_void_p]),
     "femgpu_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "femgpu_version": (C.c_char_p, []),
     "femgpu_assemble": (C.c_int, [C.c_int, C.c_int, C.c_size_t, C.c_void_p, C.c_size_t,

@@ -43,6 +43,7 @@ UNITS = [
     ("dense_factor.cu", []),
     ("offsets.cu", []),
     ("extrude.cu", ["-fmad=false"]),
+    ("boxgrid.cu", ["-fmad=false"]),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),

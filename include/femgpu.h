@@ -793,6 +793,32 @@ int femgpu_mesh2_copy(const femgpu_mesh2* m, double* points, uint32_t* triangles
                       uint32_t* origins);
 void femgpu_mesh2_free(femgpu_mesh2* m);
 
+/* grid::Grid::build (grid.rs:116-158, the cells' parts by grid.rs:292-330) and the hex mesh of
+ * its cells (heat.rs:1165-1210 `number`), as heat.rs:755-800 and elastic.rs call them through
+ * build_grid: the graded planes of each axis (with the `nextra[d]` extra key planes `extra[d]`,
+ * for example a plane of symmetry), each cell's part (the highest priority holding its centre;
+ * the footprints of the parts are not read), the mesh points numbered in first use over the cells
+ * of the parts (cell order i + nx (j + ny k), corners in VTK order) and the model's faces (sides
+ * with no cell of a part beyond, grid.rs:234-254). More than `max_points` mesh points ends with
+ * FEMGPU_ERR_TOO_LARGE and the text `refusal`; the reference's other errors come with their texts.
+ * The mesh points and cells stay on the device (femgpu_boxgrid_device). Host pointers. */
+typedef struct femgpu_boxgrid femgpu_boxgrid;
+typedef struct femgpu_boxgrid_counts {
+    size_t planes[3], grid_cells, points, cells, faces;
+} femgpu_boxgrid_counts;
+int femgpu_box_grid(const femgpu_part* parts, size_t nparts, const femgpu_spacing* spacing,
+                    const double* const* extra, const size_t* nextra, size_t max_points,
+                    const char* refusal, femgpu_boxgrid** out);
+int femgpu_boxgrid_sizes(const femgpu_boxgrid* g, femgpu_boxgrid_counts* counts);
+/* Any pointer may be null. planes: 3 arrays; part per grid cell (0xffffffff: void); points 3 per
+ * mesh point and ijk its grid point; cells 8 per mesh cell; cell_of its grid cell; mesh_part its
+ * part; the faces as (grid cell, side in x-, x+, y-, y+, z-, z+ order). */
+int femgpu_boxgrid_copy(const femgpu_boxgrid* g, double* const* planes, uint32_t* part,
+                        double* points, uint32_t* ijk, uint32_t* cells, uint64_t* cell_of,
+                        uint32_t* mesh_part, uint64_t* face_cell, uint8_t* face_side);
+int femgpu_boxgrid_device(const femgpu_boxgrid* g, const double** points, const uint32_t** cells);
+void femgpu_boxgrid_free(femgpu_boxgrid* g);
+
 /* prism::split_prism (prism.rs:144-154): the 3 tetrahedra (12 local corners) of a prism whose
  * corners (bottom 0 1 2, top 3 4 5, 3 above 0) have the global numbers g[6]. */
 int femgpu_split_prism(const uint64_t* g, int32_t* out);
