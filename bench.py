@@ -814,7 +814,7 @@ def run_batch(opt, rank, world, local):
         "device_bytes": nbytes,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,
-                     "kernel": "k_bcheb_step<float,16> (finest level)",
+                     "kernel": "k_bcheb_step3<float,16> (finest level, 3x3 blocks)",
                      "bytes_per_launch": kbytes, "launch_ms": kms, "traffic": None},
         "cpu_baseline": cpu,
         "e2e": {"value": world * rows * BATCH_RHS * opt.steps / (e2e_ms / 1e3), "unit": UNIT,

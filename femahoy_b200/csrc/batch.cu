@@ -42,6 +42,55 @@ namespace femgpu {
 constexpr int BTH = 256;
 constexpr int DTH = 32;   // rows of a dense tile
 
+// ------------------------------------------------------------------ right sides in lanes
+// A thread of the smoother kernels takes W = 16 bytes / sizeof(T) adjacent right sides (all R
+// when fewer), loaded and stored as 16-byte vectors.
+template <class T, int R>
+struct Lanes {
+    static constexpr int W = (int)(16 / sizeof(T)) < R ? (int)(16 / sizeof(T)) : R;
+};
+
+template <class T, int W>
+__device__ __forceinline__ void load_lanes(const T* p, T (&o)[W]) {
+    if constexpr (W * sizeof(T) == 16 && sizeof(T) == 4) {
+        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = q.w;
+    } else if constexpr (W * sizeof(T) == 16 && sizeof(T) == 8) {
+        const double2 q = __ldg(reinterpret_cast<const double2*>(p));
+        o[0] = q.x, o[1] = q.y;
+    } else {
+#pragma unroll
+        for (int e = 0; e < W; ++e) o[e] = __ldg(p + e);
+    }
+}
+
+// Loads and stores of data that the same launch writes (no read-only path).
+template <class T, int W>
+__device__ __forceinline__ void read_lanes(const T* p, T (&o)[W]) {
+    if constexpr (W * sizeof(T) == 16 && sizeof(T) == 4) {
+        const float4 q = *reinterpret_cast<const float4*>(p);
+        o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = q.w;
+    } else if constexpr (W * sizeof(T) == 16 && sizeof(T) == 8) {
+        const double2 q = *reinterpret_cast<const double2*>(p);
+        o[0] = q.x, o[1] = q.y;
+    } else {
+#pragma unroll
+        for (int e = 0; e < W; ++e) o[e] = p[e];
+    }
+}
+
+template <class T, int W>
+__device__ __forceinline__ void write_lanes(T* p, const T (&v)[W]) {
+    if constexpr (W * sizeof(T) == 16 && sizeof(T) == 4) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (W * sizeof(T) == 16 && sizeof(T) == 8) {
+        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    } else {
+#pragma unroll
+        for (int e = 0; e < W; ++e) p[e] = v[e];
+    }
+}
+
 // ------------------------------------------------------------------ operator with R columns
 // (A x)[row][col] for the SELL matrix A and the column `col` of the interleaved x.
 template <class T, int R>
@@ -82,36 +131,127 @@ __global__ void k_bcheb_first(int64_t n, const T* __restrict__ b, const T* __res
     x[t] = v;
 }
 
+// sell_row_cols for the W right sides col .. col + W of a thread, each summed in the same order.
+template <class T, int R>
+__device__ __forceinline__ void sell_row_lanes(const SellView<T>& A, int row, int col,
+                                               const T* __restrict__ x,
+                                               T (&acc)[Lanes<T, R>::W]) {
+    constexpr int W = Lanes<T, R>::W;
+    const int s = row / A.C, r = row % A.C;
+    const int64_t b = A.slice_ptr[s], e = A.slice_ptr[s + 1];
+    const int groups = (int)((e - b) / (4 * A.C));
+    const T* v = A.val + b + 4 * r;
+    const uint32_t* c = A.col + b + 4 * r;
+#pragma unroll
+    for (int q = 0; q < W; ++q) acc[q] = 0;
+    for (int k = 0; k < groups; ++k) {
+        auto vv = load4(v);
+        uint4 cc = __ldg(reinterpret_cast<const uint4*>(c));
+        T x0[W], x1[W], x2[W], x3[W];
+        load_lanes<T, W>(x + (size_t)cc.x * R + col, x0);
+        load_lanes<T, W>(x + (size_t)cc.y * R + col, x1);
+        load_lanes<T, W>(x + (size_t)cc.z * R + col, x2);
+        load_lanes<T, W>(x + (size_t)cc.w * R + col, x3);
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            acc[q] += vv.x * x0[q];
+            acc[q] += vv.y * x1[q];
+            acc[q] += vv.z * x2[q];
+            acc[q] += vv.w * x3[q];
+        }
+        v += 4 * A.C;
+        c += 4 * A.C;
+    }
+}
+
 // d = c2 d + c1 D^-1 (b - A x), x_out = x + d.
 template <class T, int R>
 __global__ void __launch_bounds__(BTH)
     k_bcheb_step(SellView<T> A, const T* __restrict__ b, const T* __restrict__ xin,
                  const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d, T* __restrict__ xout) {
+    constexpr int W = Lanes<T, R>::W, P = R / W;
     pdl_wait();
     const int64_t t = elem_of_thread();
-    if (t >= A.n * R) return;
-    const int row = (int)(t / R), col = (int)(t % R);
-    T r = b[t] - sell_row_cols<T, R>(A, row, col, xin);
-    T dd = c2 * d[t] + c1 * dinv[row] * r;
-    d[t] = dd;
-    xout[t] = xin[t] + dd;
+    if (t >= A.n * P) return;
+    const int row = (int)(t / P), col = (int)(t % P) * W;
+    T acc[W], bb[W], dd[W], xx[W];
+    sell_row_lanes<T, R>(A, row, col, xin, acc);
+    const int64_t i = (int64_t)row * R + col;
+    read_lanes<T, W>(b + i, bb);
+    read_lanes<T, W>(d + i, dd);
+    read_lanes<T, W>(xin + i, xx);
+    const T di = dinv[row];
+#pragma unroll
+    for (int q = 0; q < W; ++q) {
+        const T r = bb[q] - acc[q];
+        dd[q] = c2 * dd[q] + c1 * di * r;
+        xx[q] = xx[q] + dd[q];
+    }
+    write_lanes<T, W>(d + i, dd);
+    write_lanes<T, W>(xout + i, xx);
 }
 
 template <class T, int R>
 __global__ void __launch_bounds__(BTH)
     k_bresidual(SellView<T> A, const T* __restrict__ b, const T* __restrict__ x, T* __restrict__ r) {
+    constexpr int W = Lanes<T, R>::W, P = R / W;
     pdl_wait();
     const int64_t t = elem_of_thread();
-    if (t >= A.n * R) return;
-    r[t] = b[t] - sell_row_cols<T, R>(A, (int)(t / R), (int)(t % R), x);
+    if (t >= A.n * P) return;
+    const int row = (int)(t / P), col = (int)(t % P) * W;
+    T acc[W], bb[W];
+    sell_row_lanes<T, R>(A, row, col, x, acc);
+    const int64_t i = (int64_t)row * R + col;
+    read_lanes<T, W>(b + i, bb);
+#pragma unroll
+    for (int q = 0; q < W; ++q) bb[q] = bb[q] - acc[q];
+    write_lanes<T, W>(r + i, bb);
 }
 
 // ------------------------------------------------------------------ 3x3-block operators
-// (A x)[3 br + a][col] for a = 0, 1, 2 on the 3x3-block form (block3.cuh): the R threads of a
-// block row load each x block (3 rows of R values) once for the 3 rows.
+// (A x)[3 br + a][col .. col + W) for a = 0, 1, 2 on the 3x3-block form (block3.cuh): each of
+// the R / W threads of a block row takes W adjacent right sides, so that a block's column and 9
+// values are loaded once per W right sides and each x block row arrives as 16-byte vectors. Each
+// (row, right side) sum runs over the blocks in order, 3 terms per block, as with 1 right side
+// per thread.
 template <class T, int R>
 __device__ __forceinline__ void bsell3_rows(const BSell3View<T>& A, int br, int col,
-                                            const T* __restrict__ x, T* acc) {
+                                            const T* __restrict__ x,
+                                            T (&acc)[3][Lanes<T, R>::W]) {
+    constexpr int W = Lanes<T, R>::W;
+    const int s = br / B3C, r = br % B3C;
+    const int64_t b = A.slice_ptr[s], e = A.slice_ptr[s + 1];
+    const int w = (int)((e - b) / B3C);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int q = 0; q < W; ++q) acc[a][q] = 0;
+    for (int k = 0; k < w; ++k) {
+        const int64_t blk = b + (int64_t)k * B3C + r;
+        const uint32_t J = __ldg(A.col + blk);
+        const T* v = A.val + blk * 9;
+        T x0[W], x1[W], x2[W];
+        load_lanes<T, W>(x + ((size_t)3 * J) * R + col, x0);
+        load_lanes<T, W>(x + ((size_t)3 * J + 1) * R + col, x1);
+        load_lanes<T, W>(x + ((size_t)3 * J + 2) * R + col, x2);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T v0 = __ldg(v + 3 * a), v1 = __ldg(v + 3 * a + 1), v2 = __ldg(v + 3 * a + 2);
+#pragma unroll
+            for (int q = 0; q < W; ++q) {
+                acc[a][q] += v0 * x0[q];
+                acc[a][q] += v1 * x1[q];
+                acc[a][q] += v2 * x2[q];
+            }
+        }
+    }
+}
+
+// The sums of bsell3_rows for 1 right side `col` (the FP64 outer iteration's kernels, whose
+// dot products are formed per right side).
+template <class T, int R>
+__device__ __forceinline__ void bsell3_rows_col(const BSell3View<T>& A, int br, int col,
+                                                const T* __restrict__ x, T* acc) {
     const int s = br / B3C, r = br % B3C;
     const int64_t b = A.slice_ptr[s], e = A.slice_ptr[s + 1];
     const int w = (int)((e - b) / B3C);
@@ -138,19 +278,29 @@ __global__ void __launch_bounds__(BTH)
     k_bcheb_step3(BSell3View<T> A, const T* __restrict__ b, const T* __restrict__ xin,
                   const T* __restrict__ dinv, T c1, T c2, T* __restrict__ d,
                   T* __restrict__ xout) {
+    constexpr int W = Lanes<T, R>::W, P = R / W;
     pdl_wait();
     const int64_t t = elem_of_thread();
-    if (t >= A.nb * R) return;
-    const int br = (int)(t / R), col = (int)(t % R);
-    T acc[3];
+    if (t >= A.nb * P) return;
+    const int br = (int)(t / P), col = (int)(t % P) * W;
+    T acc[3][W];
     bsell3_rows<T, R>(A, br, col, xin, acc);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int64_t row = 3 * (int64_t)br + a, i = row * R + col;
-        T r = b[i] - acc[a];
-        T dd = c2 * d[i] + c1 * dinv[row] * r;
-        d[i] = dd;
-        xout[i] = xin[i] + dd;
+        T bb[W], dd[W], xx[W];
+        read_lanes<T, W>(b + i, bb);
+        read_lanes<T, W>(d + i, dd);
+        read_lanes<T, W>(xin + i, xx);
+        const T di = dinv[row];
+#pragma unroll
+        for (int q = 0; q < W; ++q) {
+            const T r = bb[q] - acc[a][q];
+            dd[q] = c2 * dd[q] + c1 * di * r;
+            xx[q] = xx[q] + dd[q];
+        }
+        write_lanes<T, W>(d + i, dd);
+        write_lanes<T, W>(xout + i, xx);
     }
 }
 
@@ -158,16 +308,21 @@ template <class T, int R>
 __global__ void __launch_bounds__(BTH)
     k_bresidual3(BSell3View<T> A, const T* __restrict__ b, const T* __restrict__ x,
                  T* __restrict__ r) {
+    constexpr int W = Lanes<T, R>::W, P = R / W;
     pdl_wait();
     const int64_t t = elem_of_thread();
-    if (t >= A.nb * R) return;
-    const int br = (int)(t / R), col = (int)(t % R);
-    T acc[3];
+    if (t >= A.nb * P) return;
+    const int br = (int)(t / P), col = (int)(t % P) * W;
+    T acc[3][W];
     bsell3_rows<T, R>(A, br, col, x, acc);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int64_t i = (3 * (int64_t)br + a) * R + col;
-        r[i] = b[i] - acc[a];
+        T bb[W];
+        read_lanes<T, W>(b + i, bb);
+#pragma unroll
+        for (int q = 0; q < W; ++q) bb[q] = bb[q] - acc[a][q];
+        write_lanes<T, W>(r + i, bb);
     }
 }
 
@@ -409,7 +564,7 @@ __global__ void __launch_bounds__(BTH)
     double bb = 0, rr = 0;
     for (int br = ch.row0 / 3 + threadIdx.x / R; br < ch.row1 / 3; br += BTH / R) {
         double acc[3];
-        bsell3_rows<double, R>(A, br, col, x, acc);
+        bsell3_rows_col<double, R>(A, br, col, x, acc);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int64_t t = (3 * (int64_t)br + a) * R + col;
@@ -438,7 +593,7 @@ __global__ void __launch_bounds__(BTH)
     if (!done[seg])
         for (int br = ch.row0 / 3 + threadIdx.x / R; br < ch.row1 / 3; br += BTH / R) {
             double acc[3];
-            bsell3_rows<double, R>(A, br, col, v, acc);
+            bsell3_rows_col<double, R>(A, br, col, v, acc);
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
                 const int64_t t = (3 * (int64_t)br + a) * R + col;
@@ -1447,13 +1602,14 @@ const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b)
         const int g = (int)((L.ns * R + BTH - 1) / BTH);
         const int deg = (int)L.c1.size();
         launch(true, k_bcheb_first<T, R>, g, BTH, s_, L.ns, b, L.dinv.p, (T)L.c1[0], L.d.p, xa);
-        const int g3 = (int)((L.ns / 3 * R + BTH - 1) / BTH);
+        const int g3 = (int)((L.ns / 3 * (R / Lanes<T, R>::W) + BTH - 1) / BTH);
+        const int gs = (int)((L.ns * (R / Lanes<T, R>::W) + BTH - 1) / BTH);
         auto step = [&](const T* xin, T* xout, int k) {
             if (L.block3)
                 launch(true, k_bcheb_step3<T, R>, g3, BTH, s_, L.view3(), b, xin, L.dinv.p,
                        (T)L.c1[k], (T)L.c2[k], L.d.p, xout);
             else
-                launch(true, k_bcheb_step<T, R>, g, BTH, s_, L.A.view(), b, xin, L.dinv.p,
+                launch(true, k_bcheb_step<T, R>, gs, BTH, s_, L.A.view(), b, xin, L.dinv.p,
                        (T)L.c1[k], (T)L.c2[k], L.d.p, xout);
         };
         for (int k = 1; k < deg; ++k) {
@@ -1463,7 +1619,7 @@ const T* BatchImpl::vcycle(std::vector<BatchLevel<T>>& Ls, size_t l, const T* b)
         if (L.block3)
             launch(true, k_bresidual3<T, R>, g3, BTH, s_, L.view3(), b, xa, L.r.p);
         else
-            launch(true, k_bresidual<T, R>, g, BTH, s_, L.A.view(), b, xa, L.r.p);
+            launch(true, k_bresidual<T, R>, gs, BTH, s_, L.A.view(), b, xa, L.r.p);
         T* bc = Ls[l + 1].b.p;
         const int gc = (int)((L.nc * R + BTH - 1) / BTH);
         launch(true, k_bgather<T, R>, gc, BTH, s_, L.nc, L.rptr.p, L.ridx.p, L.rval.p, L.r.p, bc, 0);
@@ -1894,8 +2050,8 @@ void BatchImpl::kernel_time(int reps, double* ms, double* bytes) {
     auto go = [&](auto& L, auto r) {
         using T = typename std::remove_reference<decltype(*L.dinv.p)>::type;
         constexpr int R = decltype(r)::value;
-        const int g = (int)((L.ns * R + BTH - 1) / BTH);
-        const int g3 = (int)((L.ns / 3 * R + BTH - 1) / BTH);
+        const int g = (int)((L.ns * (R / Lanes<T, R>::W) + BTH - 1) / BTH);
+        const int g3 = (int)((L.ns / 3 * (R / Lanes<T, R>::W) + BTH - 1) / BTH);
         for (int k = 0; k < reps + 5; ++k) {
             if (k == 5) FG_CUDA(cudaEventRecord(ev0_, s_));
             if (L.block3)
