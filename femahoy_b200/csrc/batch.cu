@@ -52,12 +52,18 @@ struct Lanes {
 
 template <class T, int W>
 __device__ __forceinline__ void load_lanes(const T* p, T (&o)[W]) {
-    if constexpr (W * sizeof(T) == 16 && sizeof(T) == 4) {
-        const float4 q = __ldg(reinterpret_cast<const float4*>(p));
-        o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = q.w;
-    } else if constexpr (W * sizeof(T) == 16 && sizeof(T) == 8) {
-        const double2 q = __ldg(reinterpret_cast<const double2*>(p));
-        o[0] = q.x, o[1] = q.y;
+    if constexpr ((W * sizeof(T)) % 16 == 0 && sizeof(T) == 4) {
+#pragma unroll
+        for (int h = 0; h < W / 4; ++h) {
+            const float4 q = __ldg(reinterpret_cast<const float4*>(p) + h);
+            o[4 * h] = q.x, o[4 * h + 1] = q.y, o[4 * h + 2] = q.z, o[4 * h + 3] = q.w;
+        }
+    } else if constexpr ((W * sizeof(T)) % 16 == 0 && sizeof(T) == 8) {
+#pragma unroll
+        for (int h = 0; h < W / 2; ++h) {
+            const double2 q = __ldg(reinterpret_cast<const double2*>(p) + h);
+            o[2 * h] = q.x, o[2 * h + 1] = q.y;
+        }
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) o[e] = __ldg(p + e);
@@ -67,12 +73,18 @@ __device__ __forceinline__ void load_lanes(const T* p, T (&o)[W]) {
 // Loads and stores of data that the same launch writes (no read-only path).
 template <class T, int W>
 __device__ __forceinline__ void read_lanes(const T* p, T (&o)[W]) {
-    if constexpr (W * sizeof(T) == 16 && sizeof(T) == 4) {
-        const float4 q = *reinterpret_cast<const float4*>(p);
-        o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = q.w;
-    } else if constexpr (W * sizeof(T) == 16 && sizeof(T) == 8) {
-        const double2 q = *reinterpret_cast<const double2*>(p);
-        o[0] = q.x, o[1] = q.y;
+    if constexpr ((W * sizeof(T)) % 16 == 0 && sizeof(T) == 4) {
+#pragma unroll
+        for (int h = 0; h < W / 4; ++h) {
+            const float4 q = reinterpret_cast<const float4*>(p)[h];
+            o[4 * h] = q.x, o[4 * h + 1] = q.y, o[4 * h + 2] = q.z, o[4 * h + 3] = q.w;
+        }
+    } else if constexpr ((W * sizeof(T)) % 16 == 0 && sizeof(T) == 8) {
+#pragma unroll
+        for (int h = 0; h < W / 2; ++h) {
+            const double2 q = reinterpret_cast<const double2*>(p)[h];
+            o[2 * h] = q.x, o[2 * h + 1] = q.y;
+        }
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) o[e] = p[e];
@@ -81,10 +93,15 @@ __device__ __forceinline__ void read_lanes(const T* p, T (&o)[W]) {
 
 template <class T, int W>
 __device__ __forceinline__ void write_lanes(T* p, const T (&v)[W]) {
-    if constexpr (W * sizeof(T) == 16 && sizeof(T) == 4) {
-        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-    } else if constexpr (W * sizeof(T) == 16 && sizeof(T) == 8) {
-        *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+    if constexpr ((W * sizeof(T)) % 16 == 0 && sizeof(T) == 4) {
+#pragma unroll
+        for (int h = 0; h < W / 4; ++h)
+            reinterpret_cast<float4*>(p)[h] =
+                make_float4(v[4 * h], v[4 * h + 1], v[4 * h + 2], v[4 * h + 3]);
+    } else if constexpr ((W * sizeof(T)) % 16 == 0 && sizeof(T) == 8) {
+#pragma unroll
+        for (int h = 0; h < W / 2; ++h)
+            reinterpret_cast<double2*>(p)[h] = make_double2(v[2 * h], v[2 * h + 1]);
     } else {
 #pragma unroll
         for (int e = 0; e < W; ++e) p[e] = v[e];
