@@ -243,7 +243,35 @@ __device__ __forceinline__ void bsell3_rows(const BSell3View<T>& A, int br, int 
     for (int a = 0; a < 3; ++a)
 #pragma unroll
         for (int q = 0; q < W; ++q) acc[a][q] = 0;
-    for (int k = 0; k < w; ++k) {
+    // 2 blocks per pass: both columns, then both blocks' x rows and values in flight before
+    // the sums, which stay in block order.
+    int k = 0;
+    for (; k + 1 < w; k += 2) {
+        const int64_t blk = b + (int64_t)k * B3C + r;
+        const uint32_t J0 = __ldg(A.col + blk), J1 = __ldg(A.col + blk + B3C);
+        T xv[2][3][W], v[2][9];
+#pragma unroll
+        for (int h = 0; h < 3; ++h) {
+            load_lanes<T, W>(x + ((size_t)3 * J0 + h) * R + col, xv[0][h]);
+            load_lanes<T, W>(x + ((size_t)3 * J1 + h) * R + col, xv[1][h]);
+        }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            v[0][e] = __ldg(A.val + blk * 9 + e);
+            v[1][e] = __ldg(A.val + (blk + B3C) * 9 + e);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int q = 0; q < W; ++q) {
+                    acc[a][q] += v[u][3 * a] * xv[u][0][q];
+                    acc[a][q] += v[u][3 * a + 1] * xv[u][1][q];
+                    acc[a][q] += v[u][3 * a + 2] * xv[u][2][q];
+                }
+    }
+    if (k < w) {
         const int64_t blk = b + (int64_t)k * B3C + r;
         const uint32_t J = __ldg(A.col + blk);
         const T* v = A.val + blk * 9;
