@@ -301,7 +301,31 @@ __device__ __forceinline__ void bsell3_rows_col(const BSell3View<T>& A, int br, 
     const int64_t b = A.slice_ptr[s], e = A.slice_ptr[s + 1];
     const int w = (int)((e - b) / B3C);
     acc[0] = acc[1] = acc[2] = 0;
-    for (int k = 0; k < w; ++k) {
+    int k = 0;
+    for (; k + 1 < w; k += 2) {  // 2 blocks' loads in flight, the sums in block order
+        const int64_t blk = b + (int64_t)k * B3C + r;
+        const uint32_t J0 = __ldg(A.col + blk), J1 = __ldg(A.col + blk + B3C);
+        T xv[2][3], v[2][9];
+#pragma unroll
+        for (int h = 0; h < 3; ++h) {
+            xv[0][h] = __ldg(x + ((size_t)3 * J0 + h) * R + col);
+            xv[1][h] = __ldg(x + ((size_t)3 * J1 + h) * R + col);
+        }
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            v[0][e] = __ldg(A.val + blk * 9 + e);
+            v[1][e] = __ldg(A.val + (blk + B3C) * 9 + e);
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                acc[a] += v[u][3 * a] * xv[u][0];
+                acc[a] += v[u][3 * a + 1] * xv[u][1];
+                acc[a] += v[u][3 * a + 2] * xv[u][2];
+            }
+    }
+    if (k < w) {
         const int64_t blk = b + (int64_t)k * B3C + r;
         const uint32_t J = __ldg(A.col + blk);
         const T* v = A.val + blk * 9;
