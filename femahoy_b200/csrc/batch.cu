@@ -1603,57 +1603,49 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             L.inv.alloc(ioff[L.ndense]);
             L.inv.zero(s_);  // the padding rows of each member's last tile
             FG_CUDA(cudaStreamSynchronize(s_));
-            // The members' inverses on the host threads, each with its own stream (each is a
-            // chain of small launches), into their own places of L.inv.
-            std::vector<std::string> errors(L.ndense);
-            std::vector<int> codes(L.ndense, FEMGPU_OK);
-            const int threads = std::max(1, std::min(host_threads(), L.ndense));
-            int device = 0;
-            FG_CUDA(cudaGetDevice(&device));
-            std::vector<std::thread> pool;
-            for (int th = 0; th < threads; ++th)
-                pool.emplace_back([&, th] {
-                    cudaStream_t st = nullptr;
-                    if (cudaSetDevice(device) != cudaSuccess ||
-                        cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
-                        for (int j = th; j < L.ndense; j += threads) {
-                            codes[j] = FEMGPU_ERR_CUDA;
-                            errors[j] = "cudaStreamCreate failed";
-                        }
-                        return;
-                    }
-                    // The thread's work buffers and inverse, kept across its members (no
-                    // cudaFree, which would wait on every stream of the device, per member).
-                    DenseWork work;
-                    DevBuf<double> inv64;
-                    for (int j = th; j < L.ndense; j += threads) {
-                        try {
-                            const int64_t m = off[j + 1] - off[j];
-                            if (inv64.count < (size_t)(m * m)) inv64.alloc(m * m);
-                            dense_inverse(H[S + j].mats[l], inv64.p, &work, st);
-                            k_tile_inverse<T><<<blocks_for(m * m, BTH), BTH, 0, st>>>(
-                                m, inv64.p, L.inv.p + ioff[j]);
-                            FG_CUDA(cudaGetLastError());
-                            FG_CUDA(cudaStreamSynchronize(st));
-                        } catch (const Failure& e) {
-                            codes[j] = e.code;
-                            errors[j] = e.what();
-                        } catch (const std::exception& e) {
-                            codes[j] = FEMGPU_ERR_INVALID;
-                            errors[j] = e.what();
-                        }
-                    }
-                    cudaStreamDestroy(st);
-                });
-            for (auto& th : pool) th.join();
-            for (int j = 0; j < L.ndense; ++j)
-                if (codes[j] != FEMGPU_OK)
-                    throw Failure(codes[j],
-                                  "system " + std::to_string(order_[S + j]) + ": " + errors[j]);
+            // The members' inverses in groups (their square work buffers within a budget), each
+            // step of a group 1 launch for all its members (dense_inverse_batch), then each
+            // inverse tiled into its place of L.inv.
+            constexpr int64_t kGroupEntries = (int64_t)48 << 20;  // 384 MB per square buffer
+            DenseBatchWork work;
+            DevBuf<double> inv64;
+            for (int j0 = 0; j0 < L.ndense;) {
+                int j1 = j0;
+                int64_t entries = 0;
+                while (j1 < L.ndense) {
+                    const int64_t m = off[j1 + 1] - off[j1];
+                    if (j1 > j0 && entries + m * m > kGroupEntries) break;
+                    entries += m * m;
+                    ++j1;
+                }
+                if (inv64.count < (size_t)entries) inv64.alloc(entries);
+                std::vector<const HostCsr*> mats;
+                std::vector<double*> outs;
+                int64_t at = 0;
+                for (int j = j0; j < j1; ++j) {
+                    const int64_t m = off[j + 1] - off[j];
+                    mats.push_back(&H[S + j].mats[l]);
+                    outs.push_back(inv64.p + at);
+                    at += m * m;
+                }
+                std::string text;
+                const int bad = dense_inverse_batch(mats, outs, &work, s_, &text);
+                if (bad >= 0)
+                    throw Failure(FEMGPU_ERR_NOT_SPD,
+                                  "system " + std::to_string(order_[S + j0 + bad]) + ": " + text);
+                for (int j = j0; j < j1; ++j) {
+                    const int64_t m = off[j + 1] - off[j];
+                    k_tile_inverse<T><<<blocks_for(m * m, BTH), BTH, 0, s_>>>(
+                        m, outs[j - j0], L.inv.p + ioff[j]);
+                }
+                FG_CHECK_LAUNCH();
+                FG_CUDA(cudaStreamSynchronize(s_));
+                j0 = j1;
+            }
             L.doff.upload(off.data(), off.size(), s_);
             L.dioff.upload(ioff.data(), ioff.size(), s_);
             L.tiles.upload(tiles.data(), tiles.size(), s_);
-            phase_end("deepest levels' dense inverses (host threads)");
+            phase_end("deepest levels' dense inverses (device, batched)");
         }
         for (auto* v : {&L.b, &L.xa, &L.xb}) v->alloc((size_t)L.n * R_);
         FG_CUDA(cudaStreamSynchronize(s_));

@@ -18,10 +18,9 @@ constexpr int TH = 256;
 // Panel [p0, p0 + kb) of the column-major m x m matrix F: the diagonal block factored in shared
 // memory (each pivot tested against PIVOT times its column's diagonal of A), then the panel's
 // rows below solved against it (L21 = A21 L11^-T); 1 block.
-__global__ void __launch_bounds__(TH)
-    k_panel(double* __restrict__ F, int64_t m, int64_t p0, int kb,
-            const double* __restrict__ diag0, int64_t col0,
-            unsigned long long* __restrict__ status) {
+__device__ __forceinline__ void panel_body(double* __restrict__ F, int64_t m, int64_t p0, int kb,
+                                           const double* __restrict__ diag0, int64_t col0,
+                                           unsigned long long* __restrict__ status) {
     __shared__ double D[PANEL][PANEL + 1];
     __shared__ int stop;
     for (int t = threadIdx.x; t < PANEL * PANEL; t += blockDim.x) {
@@ -56,6 +55,13 @@ __global__ void __launch_bounds__(TH)
     }
 }
 
+__global__ void __launch_bounds__(TH)
+    k_panel(double* __restrict__ F, int64_t m, int64_t p0, int kb,
+            const double* __restrict__ diag0, int64_t col0,
+            unsigned long long* __restrict__ status) {
+    panel_body(F, m, p0, kb, diag0, col0, status);
+}
+
 // The 32 x 32 lower triangle of the factored diagonal block of panel p0 (kb columns) in shared
 // memory, padded with the identity past kb, so that the unrolled solves below need no branch.
 __device__ __forceinline__ void load_panel_triangle(const double* __restrict__ F, int64_t m,
@@ -75,12 +81,12 @@ __device__ __forceinline__ void load_panel_triangle(const double* __restrict__ F
 // The panel's rows below its diagonal block: L21 = A21 L11^-T, 1 thread per row, the row's 32
 // values in registers (all loads in flight at once), the sums in column order.
 constexpr int ROWS_TH = 128;
-__global__ void __launch_bounds__(ROWS_TH)
-    k_panel_rows(double* __restrict__ F, int64_t m, int64_t p0, int kb) {
+__device__ __forceinline__ void panel_rows_body(double* __restrict__ F, int64_t m, int64_t p0,
+                                                int kb, int64_t tile) {
     __shared__ double D[PANEL][PANEL + 1];
     load_panel_triangle(F, m, p0, kb, D);
     __syncthreads();
-    const int64_t r = p0 + kb + blockIdx.x * (int64_t)ROWS_TH + threadIdx.x;
+    const int64_t r = p0 + kb + tile * (int64_t)ROWS_TH + threadIdx.x;
     if (r >= m) return;
     double x[PANEL];
 #pragma unroll
@@ -95,6 +101,11 @@ __global__ void __launch_bounds__(ROWS_TH)
 #pragma unroll
     for (int j = 0; j < PANEL; ++j)
         if (j < kb) F[r + (p0 + j) * m] = x[j];
+}
+
+__global__ void __launch_bounds__(ROWS_TH)
+    k_panel_rows(double* __restrict__ F, int64_t m, int64_t p0, int kb) {
+    panel_rows_body(F, m, p0, kb, blockIdx.x);
 }
 
 // D = A B + D on the FP64 tensor cores: A 8 x 4 (row), B 4 x 8 (column), D 8 x 8; lane l holds
@@ -121,10 +132,9 @@ __device__ __forceinline__ void tile_product(const double (*As)[PANEL + 1],
 
 // The trailing update F[t0:m, t0:m] -= L21 L21^T (lower triangle), L21 = F[t0:m, p0:p0+kb],
 // kb <= 32: 1 block per 64 x 64 tile on or below the diagonal.
-__global__ void __launch_bounds__(TH)
-    k_syrk_update(double* __restrict__ F, int64_t m, int64_t t0, int64_t p0, int kb) {
+__device__ __forceinline__ void syrk_body(double* __restrict__ F, int64_t m, int64_t t0,
+                                          int64_t p0, int kb, int64_t b) {
     __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
-    const int64_t b = blockIdx.x;
     int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
     while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
     while (bi * (bi + 1) / 2 > b) --bi;
@@ -149,13 +159,20 @@ __global__ void __launch_bounds__(TH)
         }
 }
 
+__global__ void __launch_bounds__(TH)
+    k_syrk_update(double* __restrict__ F, int64_t m, int64_t t0, int64_t p0, int kb) {
+    syrk_body(F, m, t0, p0, kb, blockIdx.x);
+}
+
 // C -= A B for an M x N block C (column-major, ldc), A M x kb (lda), B kb x N (ldb), kb <= 32:
 // 1 block per 64 x 64 tile of C.
-__global__ void __launch_bounds__(TH)
-    k_gemm_sub(double* __restrict__ C, int64_t ldc, const double* __restrict__ A, int64_t lda,
-               const double* __restrict__ B, int64_t ldb, int64_t M, int64_t N, int kb) {
+__device__ __forceinline__ void gemm_sub_body(double* __restrict__ C, int64_t ldc,
+                                              const double* __restrict__ A, int64_t lda,
+                                              const double* __restrict__ B, int64_t ldb,
+                                              int64_t M, int64_t N, int kb, int64_t bx,
+                                              int64_t by) {
     __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
-    const int64_t r0 = (int64_t)blockIdx.x * TILE, c0 = (int64_t)blockIdx.y * TILE;
+    const int64_t r0 = bx * TILE, c0 = by * TILE;
     for (int t = threadIdx.x; t < TILE * PANEL; t += blockDim.x) {
         const int r = t % TILE, k = t / TILE;
         As[r][k] = (r0 + r < M && k < kb) ? A[(r0 + r) + k * lda] : 0.0;
@@ -176,15 +193,21 @@ __global__ void __launch_bounds__(TH)
         }
 }
 
+__global__ void __launch_bounds__(TH)
+    k_gemm_sub(double* __restrict__ C, int64_t ldc, const double* __restrict__ A, int64_t lda,
+               const double* __restrict__ B, int64_t ldb, int64_t M, int64_t N, int kb) {
+    gemm_sub_body(C, ldc, A, lda, B, ldb, M, N, kb, blockIdx.x, blockIdx.y);
+}
+
 // Rows [b0, b0 + kb) of W for its columns 0..ncols: W_b = L_bb^-1 W_b (the block's triangle in
 // shared memory), 1 thread per column, the column's 32 values in registers.
-__global__ void __launch_bounds__(ROWS_TH)
-    k_trsm_rows(double* __restrict__ W, const double* __restrict__ L, int64_t n, int64_t b0,
-                int kb, int64_t ncols) {
+__device__ __forceinline__ void trsm_rows_body(double* __restrict__ W,
+                                               const double* __restrict__ L, int64_t n,
+                                               int64_t b0, int kb, int64_t ncols, int64_t tile) {
     __shared__ double D[PANEL][PANEL + 1];
     load_panel_triangle(L, n, b0, kb, D);
     __syncthreads();
-    const int64_t c = blockIdx.x * (int64_t)ROWS_TH + threadIdx.x;
+    const int64_t c = tile * (int64_t)ROWS_TH + threadIdx.x;
     if (c >= ncols) return;
     double y[PANEL];
 #pragma unroll
@@ -201,13 +224,18 @@ __global__ void __launch_bounds__(ROWS_TH)
         if (i < kb) W[(b0 + i) + c * n] = y[i];
 }
 
+__global__ void __launch_bounds__(ROWS_TH)
+    k_trsm_rows(double* __restrict__ W, const double* __restrict__ L, int64_t n, int64_t b0,
+                int kb, int64_t ncols) {
+    trsm_rows_body(W, L, n, b0, kb, ncols, blockIdx.x);
+}
+
 // X = W^T W (W lower triangular, column-major n x n): 1 block per 64 x 64 tile on or below the
 // diagonal, the sum over k from the tile's first row (W[k][i] = 0 for k < i), both halves of X
 // written.
-__global__ void __launch_bounds__(TH)
-    k_gram_lower(const double* __restrict__ W, int64_t n, double* __restrict__ X) {
+__device__ __forceinline__ void gram_lower_body(const double* __restrict__ W, int64_t n,
+                                                double* __restrict__ X, int64_t b) {
     __shared__ double As[TILE][PANEL + 1], Bs[TILE][PANEL + 1];
-    const int64_t b = blockIdx.x;
     int64_t bi = (int64_t)((sqrt(8.0 * (double)b + 1.0) - 1.0) / 2.0);
     while ((bi + 1) * (bi + 2) / 2 <= b) ++bi;
     while (bi * (bi + 1) / 2 > b) --bi;
@@ -239,6 +267,11 @@ __global__ void __launch_bounds__(TH)
         }
 }
 
+__global__ void __launch_bounds__(TH)
+    k_gram_lower(const double* __restrict__ W, int64_t n, double* __restrict__ X) {
+    gram_lower_body(W, n, X, blockIdx.x);
+}
+
 // The dense lower triangle of a host CSR's device copy, and its diagonal.
 __global__ void k_scatter_dense(int64_t n, const int64_t* __restrict__ ptr,
                                 const uint32_t* __restrict__ idx, const double* __restrict__ val,
@@ -261,7 +294,180 @@ __global__ void k_identity(int64_t n, double* __restrict__ W) {
         W[t] = (t % n == t / n) ? 1.0 : 0.0;
 }
 
+// ---------------------------------------------------------------- many systems at once
+// The same steps for a set of systems: the system is blockIdx.z, and a block past its system's
+// size returns at once, so that each step is 1 launch for all of them.
+
+__global__ void k_scatter_dense_b(const DenseMember* __restrict__ M) {
+    const DenseMember d = M[blockIdx.z];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < d.n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double g = 0.0;
+        for (int64_t e = d.ptr[i]; e < d.ptr[i + 1]; ++e) {
+            const int64_t j = d.idx[e];
+            if (j == i) g = d.val[e];
+            if (j >= i) d.L[j + i * d.n] = d.val[e];
+        }
+        d.diag[i] = g;
+    }
+}
+
+__global__ void __launch_bounds__(TH) k_panel_b(const DenseMember* __restrict__ M, int64_t p0) {
+    const DenseMember d = M[blockIdx.z];
+    if (p0 >= d.n) return;
+    panel_body(d.L, d.n, p0, (int)min((int64_t)PANEL, d.n - p0), d.diag, 0, d.status);
+}
+
+__global__ void __launch_bounds__(ROWS_TH)
+    k_panel_rows_b(const DenseMember* __restrict__ M, int64_t p0) {
+    const DenseMember d = M[blockIdx.z];
+    if (p0 >= d.n) return;
+    const int kb = (int)min((int64_t)PANEL, d.n - p0);
+    if (p0 + kb + (int64_t)blockIdx.x * ROWS_TH >= d.n) return;
+    panel_rows_body(d.L, d.n, p0, kb, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(TH) k_syrk_update_b(const DenseMember* __restrict__ M, int64_t p0) {
+    const DenseMember d = M[blockIdx.z];
+    if (p0 >= d.n) return;
+    const int kb = (int)min((int64_t)PANEL, d.n - p0);
+    const int64_t t0 = p0 + kb;
+    if (t0 >= d.n) return;
+    const int64_t T = (d.n - t0 + TILE - 1) / TILE;
+    if ((int64_t)blockIdx.x >= T * (T + 1) / 2) return;
+    syrk_body(d.L, d.n, t0, p0, kb, blockIdx.x);
+}
+
+__global__ void k_identity_b(const DenseMember* __restrict__ M) {
+    const DenseMember d = M[blockIdx.z];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < d.n * d.n;
+         t += (int64_t)gridDim.x * blockDim.x)
+        d.W[t] = (t % d.n == t / d.n) ? 1.0 : 0.0;
+}
+
+__global__ void __launch_bounds__(ROWS_TH)
+    k_trsm_rows_b(const DenseMember* __restrict__ M, int64_t b0) {
+    const DenseMember d = M[blockIdx.z];
+    if (b0 >= d.n) return;
+    const int kb = (int)min((int64_t)PANEL, d.n - b0);
+    const int64_t ncols = b0 + kb;
+    if ((int64_t)blockIdx.x * ROWS_TH >= ncols) return;
+    trsm_rows_body(d.W, d.L, d.n, b0, kb, ncols, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(TH) k_gemm_sub_b(const DenseMember* __restrict__ M, int64_t b0) {
+    const DenseMember d = M[blockIdx.z];
+    if (b0 >= d.n) return;
+    const int kb = (int)min((int64_t)PANEL, d.n - b0);
+    const int64_t rows = d.n - b0 - kb, ncols = b0 + kb;
+    if ((int64_t)blockIdx.x * TILE >= rows || (int64_t)blockIdx.y * TILE >= ncols) return;
+    const int64_t n = d.n;
+    gemm_sub_body(d.W + b0 + kb, n, d.L + (b0 + kb) + b0 * n, n, d.W + b0, n, rows, ncols, kb,
+                  blockIdx.x, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(TH) k_gram_lower_b(const DenseMember* __restrict__ M) {
+    const DenseMember d = M[blockIdx.z];
+    const int64_t T = (d.n + TILE - 1) / TILE;
+    if ((int64_t)blockIdx.x >= T * (T + 1) / 2) return;
+    gram_lower_body(d.W, d.n, d.inv, blockIdx.x);
+}
+
 }  // namespace
+
+int dense_inverse_batch(const std::vector<const HostCsr*>& a, const std::vector<double*>& inv,
+                        DenseBatchWork* w, cudaStream_t s, std::string* text) {
+    const int count = (int)a.size();
+    if (count == 0) return -1;
+    if (count > 65535) throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 65535 dense systems at once");
+    // The systems' CSR arrays end to end, and their square buffers.
+    std::vector<int64_t> ptr;
+    std::vector<uint32_t> idx;
+    std::vector<double> val;
+    std::vector<int64_t> p_at(count), e_at(count), sq_at(count), n_at(count);
+    int64_t nsq = 0, nrows = 0, nmax = 0;
+    for (int j = 0; j < count; ++j) {
+        const HostCsr& m = *a[j];
+        p_at[j] = (int64_t)ptr.size();
+        e_at[j] = (int64_t)idx.size();
+        ptr.insert(ptr.end(), m.ptr.begin(), m.ptr.begin() + m.n + 1);
+        idx.insert(idx.end(), m.idx.begin(), m.idx.begin() + m.nnz());
+        val.insert(val.end(), m.val.begin(), m.val.begin() + m.nnz());
+        sq_at[j] = nsq;
+        n_at[j] = nrows;
+        nsq += m.n * m.n;
+        nrows += m.n;
+        nmax = std::max<int64_t>(nmax, m.n);
+    }
+    auto fit = [](auto& b, size_t c) {
+        if (b.count < c) b.alloc(c);
+    };
+    fit(w->L, nsq);
+    fit(w->W, nsq);
+    fit(w->diag, nrows);
+    fit(w->status, count);
+    fit(w->members, count);
+    fit(w->ptr, ptr.size());
+    fit(w->idx, std::max<size_t>(idx.size(), 1));
+    fit(w->val, std::max<size_t>(val.size(), 1));
+    w->ptr.upload(ptr.data(), ptr.size(), s);
+    if (!idx.empty()) {
+        w->idx.upload(idx.data(), idx.size(), s);
+        w->val.upload(val.data(), val.size(), s);
+    }
+    std::vector<DenseMember> dm(count);
+    for (int j = 0; j < count; ++j)
+        dm[j] = DenseMember{w->ptr.p + p_at[j], w->idx.p + e_at[j], w->val.p + e_at[j],
+                            w->L.p + sq_at[j],  w->W.p + sq_at[j], inv[j], w->diag.p + n_at[j],
+                            w->status.p + j,    a[j]->n};
+    w->members.upload(dm.data(), count, s);
+    const DenseMember* M = w->members.p;
+    FG_CUDA(cudaMemsetAsync(w->L.p, 0, (size_t)nsq * sizeof(double), s));
+    FG_CUDA(cudaMemsetAsync(w->status.p, 0xff, (size_t)count * sizeof(unsigned long long), s));
+    const unsigned z = (unsigned)count;
+    k_scatter_dense_b<<<dim3((unsigned)blocks_for(nmax, TH), 1, z), TH, 0, s>>>(M);
+    for (int64_t p0 = 0; p0 < nmax; p0 += PANEL) {
+        k_panel_b<<<dim3(1, 1, z), TH, 0, s>>>(M, p0);
+        const int64_t t0 = std::min(nmax, p0 + PANEL);
+        if (t0 < nmax) {
+            k_panel_rows_b<<<dim3((unsigned)((nmax - t0 + ROWS_TH - 1) / ROWS_TH), 1, z), ROWS_TH,
+                             0, s>>>(M, p0);
+            const int64_t T = (nmax - t0 + TILE - 1) / TILE;
+            k_syrk_update_b<<<dim3((unsigned)(T * (T + 1) / 2), 1, z), TH, 0, s>>>(M, p0);
+        }
+    }
+    FG_CHECK_LAUNCH();
+    std::vector<unsigned long long> bad(count);
+    FG_CUDA(cudaMemcpyAsync(bad.data(), w->status.p, count * sizeof(unsigned long long),
+                            cudaMemcpyDeviceToHost, s));
+    FG_CUDA(cudaStreamSynchronize(s));
+    for (int j = 0; j < count; ++j)
+        if (bad[j] != ~0ull) {
+            const double d = fetch(w->diag.p + n_at[j] + (int64_t)bad[j], s);
+            char buf[320];
+            std::snprintf(buf, sizeof buf,
+                          "the matrix is not positive definite: the pivot of column %llu is 0 or "
+                          "less to the precision of the arithmetic (its diagonal is %s)",
+                          bad[j], rust_exp_shortest(d).c_str());
+            *text = buf;
+            return j;
+        }
+    k_identity_b<<<dim3((unsigned)blocks_for(nmax * nmax, TH), 1, z), TH, 0, s>>>(M);
+    for (int64_t b0 = 0; b0 < nmax; b0 += PANEL) {
+        const int64_t ncols = std::min(nmax, b0 + PANEL);
+        k_trsm_rows_b<<<dim3((unsigned)((ncols + ROWS_TH - 1) / ROWS_TH), 1, z), ROWS_TH, 0, s>>>(
+            M, b0);
+        const int64_t rows = nmax - ncols;
+        if (rows > 0)
+            k_gemm_sub_b<<<dim3((unsigned)((rows + TILE - 1) / TILE),
+                                (unsigned)((ncols + TILE - 1) / TILE), z),
+                           TH, 0, s>>>(M, b0);
+    }
+    const int64_t T = (nmax + TILE - 1) / TILE;
+    k_gram_lower_b<<<dim3((unsigned)(T * (T + 1) / 2), 1, z), TH, 0, s>>>(M);
+    FG_CHECK_LAUNCH();
+    return -1;
+}
 
 void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0, int64_t col0,
                             unsigned long long* status, cudaStream_t s) {

@@ -9,6 +9,7 @@
 // (cholesky.rs:22, 173-181): the smallest such column is recorded in `status`.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <utility>
 #include <vector>
 
@@ -43,5 +44,30 @@ struct DenseWork {
 // queued on `s` (the pivot test has synchronized `s` after the factor).
 void dense_inverse(const HostCsr& a, double* inv, DenseWork* w, cudaStream_t s,
                    std::vector<std::pair<const char*, double>>* stages = nullptr);
+
+// One system of dense_inverse_batch on the device: its CSR, its buffers and its size.
+struct DenseMember {
+    const int64_t* ptr;
+    const uint32_t* idx;
+    const double* val;
+    double *L, *W, *inv, *diag;
+    unsigned long long* status;
+    int64_t n;
+};
+
+struct DenseBatchWork {
+    DevBuf<int64_t> ptr;
+    DevBuf<uint32_t> idx;
+    DevBuf<double> val, diag, L, W;
+    DevBuf<unsigned long long> status;
+    DevBuf<DenseMember> members;
+};
+
+// The inverses of the SPD matrices a[j] into inv[j] (device, n_j x n_j each), all systems in
+// each launch (the system on the grid's z): as many launches as for the largest system alone.
+// Returns -1, or the first system whose pivot failed with *text the reference's text for it.
+// Returns with the inverses queued on `s`; the buffers of `w` grow to the largest set served.
+int dense_inverse_batch(const std::vector<const HostCsr*>& a, const std::vector<double*>& inv,
+                        DenseBatchWork* w, cudaStream_t s, std::string* text);
 
 }  // namespace femgpu
