@@ -33,6 +33,7 @@
 #include "common.cuh"
 #include "hierarchy.hpp"
 #include "coarsen.cuh"
+#include "offsets.cuh"
 #include "block3.cuh"
 #include "solver.cuh"
 #include "rust_format.hpp"
@@ -1077,9 +1078,12 @@ __global__ void k_tile_inverse(int64_t m, const double* __restrict__ h, T* __res
 }
 
 // ------------------------------------------------------------------ the batch
+// A member's levels on the device: its matrices (the first the caller's, the coarser ones held
+// in `owned`, whose elements keep their addresses) and its prolongations.
 struct SystemHierarchy {
-    std::vector<HostCsr> mats;
-    std::vector<HostRect> ps;
+    std::deque<DevCsr> owned;
+    std::vector<const DevCsr*> mats;
+    std::vector<DevRect> ps;
 };
 
 // Level l: rows [0, ns) of the members that smooth here and go on to level l + 1, then rows
@@ -1248,55 +1252,108 @@ class BatchImpl {
 
 namespace {
 
-// The block-diagonal matrix of the members' matrices.
-HostCsr combine(const std::vector<const HostCsr*>& parts) {
-    HostCsr out;
-    int64_t n = 0, nnz = 0;
-    for (auto* a : parts) {
-        n += a->n;
-        nnz += a->nnz();
-    }
-    if (n >= 0x7fffffff) throw Failure(FEMGPU_ERR_TOO_LARGE, "a batch of 2^31 unknowns or more");
-    out.n = n;
-    out.ptr.reserve(n + 1);
-    out.idx.reserve(nnz);
-    out.val.reserve(nnz);
-    out.ptr.push_back(0);
-    int64_t off = 0;
-    for (auto* a : parts) {
-        for (int64_t i = 0; i < a->n; ++i) {
-            for (int64_t k = a->ptr[i]; k < a->ptr[i + 1]; ++k) {
-                out.idx.push_back((uint32_t)(a->idx[k] + off));
-                out.val.push_back(a->val[k]);
-            }
-            out.ptr.push_back((int64_t)out.idx.size());
-        }
-        off += a->n;
-    }
-    return out;
+// A part of a block-diagonal combination: its CSR arrays on the device, its size, and where its
+// rows, entries and columns start in the combination.
+struct CombinePart {
+    const int64_t* ptr;
+    const uint32_t* idx;
+    const double* val;
+    int64_t rows, row0, nnz0, col0;
+};
+
+// The combination's row pointers (the part is blockIdx.y) and its entries, each part's columns
+// shifted by the columns before it.
+__global__ void k_combine_ptr(const CombinePart* __restrict__ parts, int64_t* __restrict__ ptr) {
+    const CombinePart c = parts[blockIdx.y];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < c.rows;
+         i += (int64_t)gridDim.x * blockDim.x)
+        ptr[c.row0 + i + 1] = c.nnz0 + c.ptr[i + 1];
 }
 
-// The block-diagonal transfer of the members' transfers.
-HostRect combine_rect(const std::vector<const HostRect*>& parts) {
-    HostRect out;
-    for (auto* p : parts) {
-        out.rows += p->rows;
-        out.cols += p->cols;
+__global__ void k_combine_entries(const CombinePart* __restrict__ parts, uint32_t* __restrict__ idx,
+                                  double* __restrict__ val) {
+    const CombinePart c = parts[blockIdx.y];
+    const int64_t nnz = c.ptr[c.rows];
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < nnz;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        idx[c.nnz0 + e] = (uint32_t)(c.idx[e] + c.col0);
+        val[c.nnz0 + e] = c.val[e];
     }
-    out.ptr.reserve(out.rows + 1);
-    out.ptr.push_back(0);
-    int64_t off = 0;
-    for (auto* p : parts) {
-        for (int64_t i = 0; i < p->rows; ++i) {
-            for (int64_t k = p->ptr[i]; k < p->ptr[i + 1]; ++k) {
-                out.idx.push_back((uint32_t)(p->idx[k] + off));
-                out.val.push_back(p->val[k]);
-            }
-            out.ptr.push_back((int64_t)out.idx.size());
-        }
-        off += p->cols;
+}
+
+// The block-diagonal matrix of `count` parts (rows, columns, nnz each, and their device arrays).
+void combine_parts(const std::vector<CombinePart>& host, int64_t rows, int64_t nnz, int64_t maxr,
+                   int64_t maxnnz, int64_t* out_ptr, uint32_t* out_idx, double* out_val,
+                   cudaStream_t s) {
+    if (host.empty()) return;
+    if (host.size() > 65535) throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 65535 members");
+    DevBuf<CombinePart> d;
+    d.upload(host.data(), host.size(), s);
+    FG_CUDA(cudaMemsetAsync(out_ptr, 0, sizeof(int64_t), s));
+    const unsigned ny = (unsigned)host.size();
+    k_combine_ptr<<<dim3((unsigned)blocks_for(std::max<int64_t>(maxr, 1), BTH, 64), ny), BTH, 0,
+                    s>>>(d.p, out_ptr);
+    k_combine_entries<<<dim3((unsigned)blocks_for(std::max<int64_t>(maxnnz, 1), BTH, 256), ny),
+                        BTH, 0, s>>>(d.p, out_idx, out_val);
+    FG_CHECK_LAUNCH();
+    FG_CUDA(cudaStreamSynchronize(s));  // the part table is freed on return
+    (void)rows;
+    (void)nnz;
+}
+
+// The block-diagonal matrix of the members' matrices, on the device.
+void combine(const std::vector<const DevCsr*>& parts, DevCsr* out, cudaStream_t s) {
+    std::vector<CombinePart> h;
+    int64_t n = 0, nnz = 0, maxr = 0, maxnnz = 0;
+    for (auto* a : parts) {
+        h.push_back({a->ptr.p, a->idx.p, a->val.p, a->n, n, nnz, n});
+        n += a->n;
+        nnz += a->nnz;
+        maxr = std::max(maxr, a->n);
+        maxnnz = std::max(maxnnz, a->nnz);
     }
-    return out;
+    if (n >= 0x7fffffff) throw Failure(FEMGPU_ERR_TOO_LARGE, "a batch of 2^31 unknowns or more");
+    out->n = n;
+    out->nnz = nnz;
+    out->ptr.alloc(n + 1);
+    out->idx.alloc(std::max<int64_t>(nnz, 1));
+    out->val.alloc(std::max<int64_t>(nnz, 1));
+    combine_parts(h, n, nnz, maxr, maxnnz, out->ptr.p, out->idx.p, out->val.p, s);
+}
+
+// The block-diagonal transfer of the members' transfers, on the device.
+void combine_rect(const std::vector<const DevRect*>& parts, DevRect* out, cudaStream_t s) {
+    std::vector<CombinePart> h;
+    int64_t rows = 0, cols = 0, nnz = 0, maxr = 0, maxnnz = 0;
+    for (auto* p : parts) {
+        h.push_back({p->ptr.p, p->idx.p, p->val.p, p->rows, rows, nnz, cols});
+        rows += p->rows;
+        cols += p->cols;
+        nnz += p->nnz;
+        maxr = std::max(maxr, p->rows);
+        maxnnz = std::max(maxnnz, p->nnz);
+    }
+    out->rows = rows;
+    out->cols = cols;
+    out->nnz = nnz;
+    out->ptr.alloc(rows + 1);
+    out->idx.alloc(std::max<int64_t>(nnz, 1));
+    out->val.alloc(std::max<int64_t>(nnz, 1));
+    combine_parts(h, rows, nnz, maxr, maxnnz, out->ptr.p, out->idx.p, out->val.p, s);
+}
+
+// The diagonal of a device CSR; *bad is set when an entry is not above 0.
+__global__ void k_batch_diagonal(int64_t n, const int64_t* __restrict__ ptr,
+                                 const uint32_t* __restrict__ idx, const double* __restrict__ val,
+                                 double* __restrict__ dg, int* __restrict__ bad) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int64_t k = ptr[i]; k < ptr[i + 1]; ++k)
+            if ((int64_t)idx[k] == i) d = val[k];
+        dg[i] = d;
+        if (!(d > 0.0)) *bad = 1;
+    }
 }
 
 }  // namespace
@@ -1337,14 +1394,10 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     if (B_ < 1) throw Failure(FEMGPU_ERR_INVALID, "an empty batch");
     setup_s_.clear();
     phase_t0_ = std::chrono::steady_clock::now();
-    // Each member's hierarchy on the host (multigrid.rs:84-139), the members shared among the
-    // host threads.
-    std::vector<HostCsr> fine(B_);
-    for (int b = 0; b < B_; ++b) {
+    // Each member's hierarchy on the device (multigrid.rs:84-139), the members shared among the
+    // host threads, each with its own stream.
+    for (int b = 0; b < B_; ++b)
         if (a[b]->n < 1) throw Failure(FEMGPU_ERR_INVALID, "an empty system");
-        fine[b] = download_csr(*a[b], s_);
-    }
-    phase_end("matrices to host");
     std::vector<SystemHierarchy> H(B_);
     // 1024 by default: the thin members (plates 1 cell thick) converge slowly under plane
     // coarsening, and a dense deepest level of up to 1024 unknowns per member cuts the most
@@ -1357,7 +1410,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     auto build = [&](int b, cudaStream_t st) {
         try {
             const femgpu_unknowns& uu = *u[b];
-            const int64_t n = fine[b].n;
+            const int64_t n = a[b]->n;
             HostLevel lv;
             for (int d = 0; d < 3; ++d)
                 lv.planes[d].assign(uu.planes[d], uu.planes[d] + uu.nplanes[d]);
@@ -1365,30 +1418,27 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
             for (int64_t k = 0; k < n; ++k)
                 for (int d = 0; d < 3; ++d) lv.points[k][d] = uu.points[3 * k + d];
             lv.comp.assign(uu.comp, uu.comp + n);
-            H[b].mats.push_back(std::move(fine[b]));
+            H[b].mats.push_back(a[b]);
             // The member's coarsening and Galerkin products on the device (coarsen.cu), the
             // coarse unknowns in grid order (z, y, x, component): the 3 unknowns of a node are
             // consecutive, which the 3x3-block operators need.
             DevGrid grid;
             grid_upload(lv, &grid, st);
-            const DevCsr* cur = a[b];
-            DevCsr held;
             for (;;) {
-                const HostCsr& m = H[b].mats.back();
+                const DevCsr& m = *H[b].mats.back();
                 if ((size_t)m.n <= coarsest || H[b].ps.size() >= max_levels) break;
                 DevRect p;
                 DevGrid coarse;
-                if (!coarsen_grid(grid, *cur, 7, &p, &coarse, st)) break;
+                if (!coarsen_grid(grid, m, 7, &p, &coarse, st)) break;
                 if ((size_t)coarse.n * 10 > (size_t)m.n * 9) break;
-                DevCsr next;
-                galerkin_product(p, *cur, &next, st);
-                H[b].mats.push_back(download_csr(next, st));
-                H[b].ps.push_back(rect_download(p, st));
-                held = std::move(next);
-                cur = &held;
+                H[b].owned.emplace_back();
+                galerkin_product(p, m, &H[b].owned.back(), st);
+                H[b].mats.push_back(&H[b].owned.back());
+                H[b].ps.push_back(std::move(p));
                 grid = std::move(coarse);
             }
-            if (H[b].mats.back().n > 4096)
+            FG_CUDA(cudaStreamSynchronize(st));
+            if (H[b].mats.back()->n > 4096)
                 throw Failure(FEMGPU_ERR_TOO_LARGE,
                               "the deepest level has more than 4096 unknowns: the grid does not "
                               "coarsen");
@@ -1425,7 +1475,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     phase_end("members' coarsening and Galerkin products (device, host threads)");
     // The caller's row offsets, then the batch order: deepest first (stable).
     offsets_.assign(B_ + 1, 0);
-    for (int b = 0; b < B_; ++b) offsets_[b + 1] = offsets_[b] + H[b].mats[0].n;
+    for (int b = 0; b < B_; ++b) offsets_[b + 1] = offsets_[b] + H[b].mats[0]->n;
     n_ = offsets_[B_];
     if (n_ * R_ >= 0x7fffffff)
         throw Failure(FEMGPU_ERR_TOO_LARGE, "a batch of 2^31 values or more per vector");
@@ -1438,7 +1488,7 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     std::vector<int> map(n_);
     std::vector<int64_t> boff(B_ + 1, 0);  // the batch order's row offsets
     for (int k = 0; k < B_; ++k) {
-        const int64_t m = Hs[k].mats[0].n;
+        const int64_t m = Hs[k].mats[0]->n;
         boff[k + 1] = boff[k] + m;
         for (int64_t i = 0; i < m; ++i) map[boff[k] + i] = (int)(offsets_[order_[k]] + i);
     }
@@ -1448,25 +1498,17 @@ void BatchImpl::create(const std::vector<const DevCsr*>& a,
     for (int k = 0; k < B_; ++k) position_[order_[k]] = k;
     // The exact finest operator (FP64) of the PCG loop and the true residual.
     {
-        std::vector<const HostCsr*> parts;
-        for (auto& h : Hs) parts.push_back(&h.mats[0]);
-        HostCsr f = combine(parts);
-        std::vector<int64_t> bp;
-        std::vector<uint32_t> bc;
-        std::vector<double> bv;
-        if (opt_.format == 0 && make_bsell3<double>(f, &bp, &bc, &bv)) {
+        std::vector<const DevCsr*> parts;
+        for (auto& h : Hs) parts.push_back(h.mats[0]);
+        DevCsr f;
+        combine(parts, &f, s_);
+        if (opt_.format == 0 && make_bsell3_device<double>(f, &f3ptr_, &f3col_, &f3val_, s_))
             fine3_ = true;
-            f3ptr_.upload(bp.data(), bp.size(), s_);
-            f3col_.upload(bc.data(), bc.size(), s_);
-            f3val_.upload(bv.data(), bv.size(), s_);
-        } else {
-            DevCsr d;
-            upload_csr(f, &d, s_);
-            make_sell<double>(d, 32, &A64_, s_);
-        }
+        else
+            make_sell<double>(f, 32, &A64_, s_);
         FG_CUDA(cudaStreamSynchronize(s_));
     }
-    phase_end("finest operator (host combination, 3x3 blocks)");
+    phase_end("finest operator (device combination, 3x3 blocks)");
     // The chunks of the PCG kernels: rows of 1 member each; up to 4 rows per thread, or 2 block
     // rows (6 rows) per thread with the 3x3-block operator, whose chunks hold whole nodes.
     const int chunk_rows = fine3_ ? 3 * 2 * (BTH / R_) : 4 * BTH / R_;
@@ -1522,68 +1564,58 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
         int K = 0, S = 0;
         while (K < B_ && H[K].mats.size() > l) ++K;
         while (S < K && H[S].mats.size() > l + 1) ++S;
-        for (int k = 0; k < K; ++k) L.n += H[k].mats[l].n;
-        for (int k = 0; k < S; ++k) L.ns += H[k].mats[l].n;
+        for (int k = 0; k < K; ++k) L.n += H[k].mats[l]->n;
+        for (int k = 0; k < S; ++k) L.ns += H[k].mats[l]->n;
         sizes_.push_back(L.n);
         if (S > 0) {
-            std::vector<const HostCsr*> mats;
-            std::vector<const HostRect*> ps;
+            std::vector<const DevCsr*> mats;
+            std::vector<const DevRect*> ps;
             for (int k = 0; k < S; ++k) {
-                mats.push_back(&H[k].mats[l]);
+                mats.push_back(H[k].mats[l]);
                 ps.push_back(&H[k].ps[l]);
             }
-            HostCsr A = combine(mats);
-            HostRect P = combine_rect(ps);
             DevCsr d;
-            upload_csr(A, &d, s_);
-            {
-                std::vector<int64_t> bp;
-                std::vector<uint32_t> bc;
-                std::vector<T> bv;
-                if (opt_.format == 0 && make_bsell3<T>(A, &bp, &bc, &bv)) {
-                    L.block3 = true;
-                    L.b3ptr.upload(bp.data(), bp.size(), s_);
-                    L.b3col.upload(bc.data(), bc.size(), s_);
-                    L.b3val.upload(bv.data(), bv.size(), s_);
-                } else {
-                    make_sell<T>(d, 32, &L.A, s_);
-                }
-            }
+            combine(mats, &d, s_);
+            if (opt_.format == 0 && make_bsell3_device<T>(d, &L.b3ptr, &L.b3col, &L.b3val, s_))
+                L.block3 = true;
+            else
+                make_sell<T>(d, 32, &L.A, s_);
             // The diagonal, and lambda_max of the block-diagonal D^-1 A: the largest of the
             // members'.
-            std::vector<double> dg(A.n, 0.0), inv(A.n);
-            for (int64_t i = 0; i < A.n; ++i)
-                for (int64_t k = A.ptr[i]; k < A.ptr[i + 1]; ++k)
-                    if ((int64_t)A.idx[k] == i) dg[i] = A.val[k];
-            for (int64_t i = 0; i < A.n; ++i) {
-                if (!(dg[i] > 0.0))
-                    throw Failure(FEMGPU_ERR_NOT_SPD,
-                                  "the matrix is not positive definite: it has a diagonal entry "
-                                  "that is not above 0");
-                inv[i] = 1.0 / dg[i];
-            }
+            DevBuf<double> ddg(d.n);
+            DevBuf<int> bad(1);
+            bad.zero(s_);
+            k_batch_diagonal<<<blocks_for(d.n, BTH), BTH, 0, s_>>>(d.n, d.ptr.p, d.idx.p, d.val.p,
+                                                                   ddg.p, bad.p);
+            FG_CHECK_LAUNCH();
+            if (fetch(bad.p, s_))
+                throw Failure(FEMGPU_ERR_NOT_SPD,
+                              "the matrix is not positive definite: it has a diagonal entry "
+                              "that is not above 0");
             Operator<double> op;
-            op.n = A.n;
-            op.nnz = A.nnz();
+            op.n = d.n;
+            op.nnz = d.nnz;
             make_sell<double>(d, 32, &op.sell, s_);
-            DevBuf<double> ddg;
-            ddg.upload(dg.data(), A.n, s_);
             L.lambda = lambda_max(op, ddg.p, s_, partial_);
             chebyshev(L.lambda, deg, lower, &L.c1, &L.c2, opt_.smoother);
-            std::vector<T> tv(inv.begin(), inv.end());
-            L.dinv.upload(tv.data(), tv.size(), s_);
-            HostRect Rt = transpose(P);
+            L.dinv.alloc(d.n);
+            reciprocal<T>(d.n, ddg.p, L.dinv.p, s_);
+            DevRect P, Rt;
+            combine_rect(ps, &P, s_);
+            transpose_rect(P, &Rt, s_);
             L.nc = P.cols;
-            L.pptr.upload(P.ptr.data(), P.rows + 1, s_);
-            L.pidx.upload(P.idx.data(), P.idx.size(), s_);
-            std::vector<T> pv(P.val.begin(), P.val.end()), rv(Rt.val.begin(), Rt.val.end());
-            L.pval.upload(pv.data(), pv.size(), s_);
-            L.rptr.upload(Rt.ptr.data(), Rt.rows + 1, s_);
-            L.ridx.upload(Rt.idx.data(), Rt.idx.size(), s_);
-            L.rval.upload(rv.data(), rv.size(), s_);
+            L.pptr = std::move(P.ptr);
+            L.pidx = std::move(P.idx);
+            L.pval.alloc(std::max<int64_t>(P.nnz, 1));
+            convert_values<T>(P.nnz, P.val.p, L.pval.p, s_);
+            L.rptr = std::move(Rt.ptr);
+            L.ridx = std::move(Rt.idx);
+            L.rval.alloc(std::max<int64_t>(Rt.nnz, 1));
+            convert_values<T>(Rt.nnz, Rt.val.p, L.rval.p, s_);
             L.d.alloc((size_t)L.ns * R_);
             L.r.alloc((size_t)L.ns * R_);
-            phase_end("smoothed levels (host combination, lambda_max, transfers)");
+            FG_CUDA(cudaStreamSynchronize(s_));
+            phase_end("smoothed levels (device combination, lambda_max, transfers)");
         }
         // The members that end here: a dense inverse each, from a dense Cholesky factor on the
         // device, made exactly symmetric, stored in tiles of DTH rows (k_bdense's layout).
@@ -1593,7 +1625,7 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
             std::vector<int2> tiles;
             off[0] = L.ns;
             for (int j = 0; j < L.ndense; ++j) {
-                const int64_t m = H[S + j].mats[l].n;
+                const int64_t m = H[S + j].mats[l]->n;
                 off[j + 1] = off[j] + m;
                 // Row tiles of DTH rows (the last padded with zero rows), each stored by column.
                 ioff[j + 1] = ioff[j] + (m + DTH - 1) / DTH * DTH * m;
@@ -1619,12 +1651,12 @@ void BatchImpl::build_levels(std::vector<SystemHierarchy>& H, std::vector<BatchL
                     ++j1;
                 }
                 if (inv64.count < (size_t)entries) inv64.alloc(entries);
-                std::vector<const HostCsr*> mats;
+                std::vector<const DevCsr*> mats;
                 std::vector<double*> outs;
                 int64_t at = 0;
                 for (int j = j0; j < j1; ++j) {
                     const int64_t m = off[j + 1] - off[j];
-                    mats.push_back(&H[S + j].mats[l]);
+                    mats.push_back(H[S + j].mats[l]);
                     outs.push_back(inv64.p + at);
                     at += m * m;
                 }

@@ -375,29 +375,21 @@ __global__ void __launch_bounds__(TH) k_gram_lower_b(const DenseMember* __restri
 
 }  // namespace
 
-int dense_inverse_batch(const std::vector<const HostCsr*>& a, const std::vector<double*>& inv,
+int dense_inverse_batch(const std::vector<const DevCsr*>& a, const std::vector<double*>& inv,
                         DenseBatchWork* w, cudaStream_t s, std::string* text) {
     const int count = (int)a.size();
     if (count == 0) return -1;
     if (count > 65535) throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 65535 dense systems at once");
-    // The systems' CSR arrays end to end, and their square buffers.
-    std::vector<int64_t> ptr;
-    std::vector<uint32_t> idx;
-    std::vector<double> val;
-    std::vector<int64_t> p_at(count), e_at(count), sq_at(count), n_at(count);
+    // The systems' square buffers end to end.
+    std::vector<int64_t> sq_at(count), n_at(count);
     int64_t nsq = 0, nrows = 0, nmax = 0;
     for (int j = 0; j < count; ++j) {
-        const HostCsr& m = *a[j];
-        p_at[j] = (int64_t)ptr.size();
-        e_at[j] = (int64_t)idx.size();
-        ptr.insert(ptr.end(), m.ptr.begin(), m.ptr.begin() + m.n + 1);
-        idx.insert(idx.end(), m.idx.begin(), m.idx.begin() + m.nnz());
-        val.insert(val.end(), m.val.begin(), m.val.begin() + m.nnz());
+        const int64_t n = a[j]->n;
         sq_at[j] = nsq;
         n_at[j] = nrows;
-        nsq += m.n * m.n;
-        nrows += m.n;
-        nmax = std::max<int64_t>(nmax, m.n);
+        nsq += n * n;
+        nrows += n;
+        nmax = std::max<int64_t>(nmax, n);
     }
     auto fit = [](auto& b, size_t c) {
         if (b.count < c) b.alloc(c);
@@ -407,19 +399,11 @@ int dense_inverse_batch(const std::vector<const HostCsr*>& a, const std::vector<
     fit(w->diag, nrows);
     fit(w->status, count);
     fit(w->members, count);
-    fit(w->ptr, ptr.size());
-    fit(w->idx, std::max<size_t>(idx.size(), 1));
-    fit(w->val, std::max<size_t>(val.size(), 1));
-    w->ptr.upload(ptr.data(), ptr.size(), s);
-    if (!idx.empty()) {
-        w->idx.upload(idx.data(), idx.size(), s);
-        w->val.upload(val.data(), val.size(), s);
-    }
     std::vector<DenseMember> dm(count);
     for (int j = 0; j < count; ++j)
-        dm[j] = DenseMember{w->ptr.p + p_at[j], w->idx.p + e_at[j], w->val.p + e_at[j],
-                            w->L.p + sq_at[j],  w->W.p + sq_at[j], inv[j], w->diag.p + n_at[j],
-                            w->status.p + j,    a[j]->n};
+        dm[j] = DenseMember{a[j]->ptr.p,       a[j]->idx.p,      a[j]->val.p,
+                            w->L.p + sq_at[j], w->W.p + sq_at[j], inv[j],
+                            w->diag.p + n_at[j], w->status.p + j, a[j]->n};
     w->members.upload(dm.data(), count, s);
     const DenseMember* M = w->members.p;
     FG_CUDA(cudaMemsetAsync(w->L.p, 0, (size_t)nsq * sizeof(double), s));

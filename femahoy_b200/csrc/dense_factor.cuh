@@ -56,18 +56,17 @@ struct DenseMember {
 };
 
 struct DenseBatchWork {
-    DevBuf<int64_t> ptr;
-    DevBuf<uint32_t> idx;
-    DevBuf<double> val, diag, L, W;
+    DevBuf<double> diag, L, W;
     DevBuf<unsigned long long> status;
     DevBuf<DenseMember> members;
 };
 
-// The inverses of the SPD matrices a[j] into inv[j] (device, n_j x n_j each), all systems in
-// each launch (the system on the grid's z): as many launches as for the largest system alone.
+// The inverses of the SPD matrices a[j] (device CSR, both triangles) into inv[j] (device,
+// n_j x n_j each), all systems in each launch (the system on the grid's z): as many launches as
+// for the largest system alone.
 // Returns -1, or the first system whose pivot failed with *text the reference's text for it.
 // Returns with the inverses queued on `s`; the buffers of `w` grow to the largest set served.
-int dense_inverse_batch(const std::vector<const HostCsr*>& a, const std::vector<double*>& inv,
+int dense_inverse_batch(const std::vector<const DevCsr*>& a, const std::vector<double*>& inv,
                         DenseBatchWork* w, cudaStream_t s, std::string* text);
 
 }  // namespace femgpu
