@@ -11,9 +11,9 @@ meshes (prism.rs, mesh2d.rs) and ``grid`` its box grid (grid.rs Grid::build).
 from ._lib import (COLOUR, FP64, GATHER, HEX8_ELASTIC, HEX8_HEAT, HEX8_MASS, MIXED, P1_ELASTIC, P1_HEAT, P2_ELASTIC,
                    P2_ELASTIC_ORTHO, P2_MASS, FemError, LIB_PATH, lib)
 from .solve import (PCG_MAX_ITER, PCG_TOL, STEADY_DIRECT_LIMIT, TRANSIENT_DIRECT_LIMIT,
-                    Cells, Crossover, Level, Method, Options, Quadratic, Solver, Stats, Unknowns,
-                    coarse_matrix, hex_elements, hex_mass, prolongation, reduced_rhs,
-                    symbolic_counts)
+                    Cells, Convergence, Crossover, Level, Method, Options, Quadratic, Solver,
+                    Stats, Unknowns, coarse_matrix, hex_elements, hex_mass, pcg, prolongation,
+                    reduced_rhs, symbolic_counts)
 from .recover import Peak, Reactions, Recovery, reactions
 from .sparse import Csr, Rect, colour
 from . import grid, prism
@@ -25,5 +25,5 @@ __all__ = [
     "TRANSIENT_DIRECT_LIMIT", "Cells", "Crossover", "Level", "Method", "Options", "Quadratic",
     "Solver", "coarse_matrix", "hex_elements", "hex_mass", "symbolic_counts",
     "Stats", "Unknowns", "prolongation", "reduced_rhs", "Csr", "Rect", "colour", "Peak",
-    "Recovery", "Reactions", "reactions", "grid", "prism",
+    "Recovery", "Reactions", "reactions", "grid", "prism", "pcg", "Convergence",
 ]

@@ -123,6 +123,15 @@ class BoxgridCounts_t(C.Structure):
                 ("cells", C.c_size_t), ("faces", C.c_size_t)]
 
 
+class Convergence_t(C.Structure):
+    _fields_ = [("iterations", C.c_size_t), ("residual", C.c_double)]
+
+
+PRECONDITION_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_size_t,
+                              C.c_void_p)
+PRECONDITION_DEVICE_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p,
+                                     C.c_void_p)
+
 CLASSIFY_FN = C.CFUNCTYPE(C.c_uint32, C.POINTER(C.c_double), C.c_void_p)
 
 SIGNATURES = {
@@ -145,6 +154,11 @@ SIGNATURES = {
     "femgpu_mesh2_copy": (C.c_int, [C.c_void_p] + [C.c_void_p] * 7),
     "femgpu_mesh2_free": (None, [C.c_void_p]),
     "femgpu_split_prism": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_pcg": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, PRECONDITION_FN, C.c_void_p,
+                             C.c_double, C.c_size_t, C.c_void_p, C.POINTER(Convergence_t)]),
+    "femgpu_pcg_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, PRECONDITION_DEVICE_FN,
+                                    C.c_void_p, C.c_double, C.c_size_t, C.c_void_p, C.c_void_p,
+                                    C.POINTER(Convergence_t)]),
     "femgpu_box_grid": (C.c_int, [C.c_void_p, C.c_size_t, C.POINTER(Spacing_t), C.c_void_p,
                                   C.c_void_p, C.c_size_t, C.c_char_p, C.POINTER(C.c_void_p)]),
     "femgpu_boxgrid_sizes": (C.c_int, [C.c_void_p, C.POINTER(BoxgridCounts_t)]),

@@ -398,3 +398,44 @@ class Quadratic:
         edges = edges[:ne.value].copy()
         mid = 0.5 * (pts[edges[:, 0]] + pts[edges[:, 1]])
         return cls(np.concatenate([pts, mid]), len(pts), edges, t10)
+
+
+@dataclass
+class Convergence:
+    """multigrid.rs:680-686: the iterations and |b - A x| / |b| at the end."""
+    iterations: int
+    residual: float
+
+
+def pcg(a: Csr, b, x, precondition=None, tol=PCG_TOL, max_iter=PCG_MAX_ITER,
+        cancelled=None) -> Convergence:
+    """multigrid::pcg (multigrid.rs:692-753): conjugate gradients from the start value in ``x``
+    (numpy, updated in place, the last iterate also on failure) with the preconditioner
+    ``precondition(r, z)`` (numpy arrays; it writes z = M^-1 r), None for z = r. ``cancelled``
+    is a ctypes int flag read before each step (or a callable read once). Raises FemError with
+    the reference's texts."""
+    b = L.arr(b, np.float64)
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous):
+        raise TypeError("x must be a contiguous float64 numpy array (it gets the solution)")
+    failure = []
+
+    def call(r, z, n, _ctx):
+        try:
+            zr = np.ctypeslib.as_array(z, shape=(n,))
+            precondition(np.ctypeslib.as_array(r, shape=(n,)).copy(), zr)
+        except BaseException as e:  # noqa: BLE001 - reported after the call
+            failure.append(e)
+
+    cb = L.PRECONDITION_FN(call) if precondition is not None else L.PRECONDITION_FN()
+    flag = None
+    if isinstance(cancelled, C.c_int):
+        flag = C.byref(cancelled)
+    elif callable(cancelled) and cancelled():
+        flag = C.byref(C.c_int(1))
+    out = L.Convergence_t()
+    status = L.lib().femgpu_pcg(a.handle, L.ptr(b), L.ptr(x), cb, None, float(tol),
+                                int(max_iter), flag, C.byref(out))
+    if failure:
+        raise failure[0]
+    L.check(status)
+    return Convergence(out.iterations, out.residual)

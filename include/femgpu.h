@@ -378,6 +378,31 @@ int femgpu_solver_solve_zero(femgpu_solver* s, const double* b, double* x,
                              const volatile int* cancel, femgpu_stats* stats);
 /* z = M^-1 r: 1 application of the preconditioner (a V-cycle), device vectors. */
 int femgpu_solver_precondition_device(femgpu_solver* s, const double* r, double* z);
+
+/* multigrid::pcg (multigrid.rs:692-753), the reference's public conjugate gradients with the
+ * caller's preconditioner z = M^-1 r: from the start value x to |b - A x| <= tol |b| (tested
+ * before each step), FEMGPU_ERR_NOT_CONVERGED after max_iter iterations and
+ * FEMGPU_ERR_CANCELLED when *cancel is nonzero, with the reference's texts; x holds the last
+ * iterate either way. `precondition` NULL: z = r. The vectors live on the device; A p is summed
+ * row by row in column order (Csr::mul), the dot products in fixed blocks. femgpu_pcg: host
+ * vectors, a host preconditioner (r and z host arrays of n values). femgpu_pcg_device: device
+ * vectors b and x on `stream` (a cudaStream_t, NULL for the legacy stream), a preconditioner on
+ * device vectors: r is complete when it is called, and z must be complete on `stream` when it
+ * returns (work queued on `stream`, or finished), e.g. femgpu_solver_precondition_device. */
+typedef struct femgpu_convergence {
+    size_t iterations;
+    double residual; /* |b - A x| / |b| at the end (multigrid.rs:680-686) */
+} femgpu_convergence;
+typedef void (*femgpu_precondition_fn)(const double* r, double* z, size_t n, void* ctx);
+typedef void (*femgpu_precondition_device_fn)(const double* r, double* z, size_t n, void* stream,
+                                              void* ctx);
+int femgpu_pcg(const femgpu_csr* a, const double* b, double* x, femgpu_precondition_fn precondition,
+               void* ctx, double tol, size_t max_iter, const volatile int* cancel,
+               femgpu_convergence* out);
+int femgpu_pcg_device(const femgpu_csr* a, const double* b, double* x,
+                      femgpu_precondition_device_fn precondition, void* ctx, double tol,
+                      size_t max_iter, const volatile int* cancel, void* stream,
+                      femgpu_convergence* out);
 void femgpu_solver_free(femgpu_solver* s);
 
 /* The CUDA stream (a cudaStream_t) on which the solver launches all its work, so that a caller

@@ -71,6 +71,7 @@ def _load():
         "orc_prolongation": (P, [P, S, S, P, S, P, S, P, P]),
         "orc_nested_dissection": (None, [P, P, P]),
         "orc_direct_solve": (I, [P, P, P, P, P, S]),
+        "orc_pcg": (I, [P, P, P, C.CFUNCTYPE(None, P, P, S, P), P, D, S, P, P, P, P, S]),
         "orc_solver_new": (P, [P, I, P, S, P, S, P, S, P, P, P, P, P, S, I, I, S, D,
                                C.c_uint64, I, S, P, P, P, S, P, S]),
         "orc_solver_level_matrix": (P, [P, S]),
@@ -525,6 +526,29 @@ def direct_solve(a: Csr, xyz, b):
     if _lib.orc_direct_solve(a.h, _p(xyz), _p(x), C.byref(entries), err, 512):
         raise OracleError(err.value.decode())
     return x, entries.value
+
+
+_PRE = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p)
+
+
+def pcg(a: Csr, b, x, precondition=None, tol=1e-10, max_iter=500, cancel=None):
+    """multigrid.rs:692-753: x (numpy, updated in place) from its start value; precondition(r,
+    z) writes z = M^-1 r into the numpy array z (None: z = r). Returns (iterations, residual)."""
+    b = np.ascontiguousarray(b, dtype=np.float64)
+
+    def call(r, z, n, _ctx):
+        zr = np.ctypeslib.as_array(C.cast(z, C.POINTER(C.c_double)), shape=(n,))
+        rr = np.ctypeslib.as_array(C.cast(r, C.POINTER(C.c_double)), shape=(n,))
+        precondition(rr.copy(), zr)
+
+    cb = _PRE(call) if precondition is not None else _PRE()
+    it, res = C.c_size_t(), C.c_double()
+    err = C.create_string_buffer(512)
+    flag = C.byref(cancel) if cancel is not None else None
+    if _lib.orc_pcg(a.h, _p(b), _p(x), cb, None, tol, max_iter, flag, C.byref(it),
+                    C.byref(res), err, 512):
+        raise OracleError(err.value.decode())
+    return it.value, res.value
 
 
 class Solver:

@@ -492,6 +492,30 @@ int orc_solver_solve(void* s, const double* b, double* x, double tol, size_t max
         return -1;
     }
 }
+// multigrid.rs:692-753 with a caller's preconditioner (a C function; NULL: z = r).
+int orc_pcg(void* a, const double* b, double* x, void (*pre)(const double*, double*, size_t, void*),
+            void* ctx, double tol, size_t max_iter, const volatile int* cancel,
+            size_t* iterations, double* residual, char* err, size_t len) {
+    try {
+        const size_t n = C(a)->n;
+        Convergence c = pcg(
+            *C(a), b, x,
+            [&](const double* r, double* z) {
+                if (pre)
+                    pre(r, z, n, ctx);
+                else
+                    std::copy(r, r + n, z);
+            },
+            tol, max_iter, [cancel] { return cancel && *cancel != 0; });
+        *iterations = c.iterations;
+        *residual = c.residual;
+        return 0;
+    } catch (const std::exception& e) {
+        put_error(err, len, e.what());
+        return -1;
+    }
+}
+
 // z = M^-1 r of the solver's preconditioner (1 V-cycle).
 void orc_solver_precondition(void* s, const double* r, double* z) {
     auto* o = static_cast<OSolver*>(s);
