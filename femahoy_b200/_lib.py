@@ -154,6 +154,13 @@ SIGNATURES = {
     "femgpu_mesh2_copy": (C.c_int, [C.c_void_p] + [C.c_void_p] * 7),
     "femgpu_mesh2_free": (None, [C.c_void_p]),
     "femgpu_split_prism": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_csr_diagonal": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "femgpu_rect_upload": (C.c_int, [C.c_size_t, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.POINTER(C.c_void_p)]),
+    "femgpu_rect_mul": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_rect_mul_transpose": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "femgpu_rect_galerkin": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "femgpu_rect_free": (None, [C.c_void_p]),
     "femgpu_pcg": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, PRECONDITION_FN, C.c_void_p,
                              C.c_double, C.c_size_t, C.c_void_p, C.POINTER(Convergence_t)]),
     "femgpu_pcg_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, PRECONDITION_DEVICE_FN,

@@ -45,6 +45,7 @@ UNITS = [
     ("extrude.cu", ["-fmad=false"]),
     ("boxgrid.cu", ["-fmad=false"]),
     ("pcg.cu", ["-fmad=false"]),
+    ("rect.cu", ["-fmad=false"]),
 ]
 CXX_UNITS = [("hierarchy.cpp", ["-O3", "-std=c++17", "-fPIC", "-ffp-contract=off", "-pthread"]),
              ("symbolic.cpp", ["-O3", "-std=c++17", "-fPIC"]),

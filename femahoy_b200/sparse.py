@@ -113,14 +113,9 @@ class Csr:
         return y
 
     def diagonal(self):
-        """sparse.rs:89-93"""
-        ptr, idx, val = self.arrays()
-        d = np.zeros(len(ptr) - 1)
-        for i in range(len(d)):
-            row = idx[ptr[i]:ptr[i + 1]]
-            k = np.searchsorted(row, i)
-            if k < len(row) and row[k] == i:
-                d[i] = val[ptr[i] + k]
+        """sparse.rs:89-93, on the device."""
+        d = np.empty(self.n)
+        L.check(L.lib().femgpu_csr_diagonal(self._h, L.ptr(d)))
         return d
 
 
@@ -134,20 +129,52 @@ class Rect:
     idx: np.ndarray
     val: np.ndarray
 
+    def _device(self):
+        """The device copy (femgpu_rect), made on first use and kept with the arrays."""
+        h = self.__dict__.get("_handle")
+        if h is None:
+            ptr, idx, val = (L.arr(self.ptr, np.int64), L.arr(self.idx, np.uint32),
+                             L.arr(self.val, np.float64))
+            out = C.c_void_p()
+            L.check(L.lib().femgpu_rect_upload(int(self.rows), int(self.cols), L.ptr(ptr),
+                                               L.ptr(idx), L.ptr(val), C.byref(out)))
+            h = _RectHandle(out.value)
+            self.__dict__["_handle"] = h
+        return h.h
+
     def mul(self, x):
-        """sparse.rs:212-220"""
-        out = np.zeros(self.rows)
-        for i in range(self.rows):
-            s = slice(self.ptr[i], self.ptr[i + 1])
-            out[i] = np.dot(self.val[s], x[self.idx[s]])
-        return out
+        """sparse.rs:212-220: y = P x on the device, each row summed in the reference's order."""
+        x = L.arr(x, np.float64)
+        y = np.empty(self.rows)
+        L.check(L.lib().femgpu_rect_mul(self._device(), L.ptr(x), L.ptr(y)))
+        return y
 
     def mul_transpose(self, x):
-        """sparse.rs:223-230"""
-        y = np.zeros(self.cols)
-        rows = np.repeat(np.arange(self.rows), np.diff(self.ptr))
-        np.add.at(y, self.idx, self.val * x[rows])
+        """sparse.rs:223-230: y = P^T x on the device, each entry summed in the reference's
+        order (increasing row of P)."""
+        x = L.arr(x, np.float64)
+        y = np.empty(self.cols)
+        L.check(L.lib().femgpu_rect_mul_transpose(self._device(), L.ptr(x), L.ptr(y)))
         return y
+
+    def galerkin(self, a: "Csr") -> "Csr":
+        """sparse.rs:233-292: P^T A P on the device (the reference's pattern; its entries to
+        rounding)."""
+        out = C.c_void_p()
+        L.check(L.lib().femgpu_rect_galerkin(self._device(), a.handle, C.byref(out)))
+        return Csr(out.value)
+
+
+class _RectHandle:
+    """Frees a femgpu_rect with its owner."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def __del__(self):
+        h, self.h = self.h, None
+        if h:
+            L.lib().femgpu_rect_free(h)
 
 
 def colour(n, elements):

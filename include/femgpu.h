@@ -123,6 +123,22 @@ int femgpu_csr_download(const femgpu_csr* a, int64_t* ptr, uint32_t* idx, double
 /* A device matrix from host CSR arrays (the Rust `Csr` handed to Solver::new). */
 int femgpu_csr_upload(size_t n, const int64_t* ptr, const uint32_t* idx, const double* val,
                       femgpu_csr** out);
+/* Csr::diagonal (sparse.rs:88-93): the n diagonal entries (0 where a row has none). */
+int femgpu_csr_diagonal(const femgpu_csr* a, double* d);
+
+/* Rect (sparse.rs:196-293), a rectangular CSR matrix such as a prolongation, on the device:
+ * y = P x (mul, sparse.rs:212-220) and y = P^T x (mul_transpose, :223-230), each output summed
+ * in the reference's order (bit-identical), and the Galerkin product P^T A P (galerkin,
+ * :233-292; its entries the reference's to rounding, its pattern the same). `ptr` starts at 0
+ * and does not decrease; every column is below `cols`. */
+typedef struct femgpu_rect femgpu_rect;
+int femgpu_rect_upload(size_t rows, size_t cols, const int64_t* ptr, const uint32_t* idx,
+                       const double* val, femgpu_rect** out);
+int femgpu_rect_mul(femgpu_rect* r, const double* x, double* y);
+int femgpu_rect_mul_transpose(femgpu_rect* r, const double* x, double* y);
+int femgpu_rect_galerkin(const femgpu_rect* r, const femgpu_csr* a, femgpu_csr** out);
+void femgpu_rect_free(femgpu_rect* r);
+
 /* Csr::submatrix (sparse.rs:108-135): rows and columns `keep` (each index once). */
 int femgpu_csr_submatrix(const femgpu_csr* a, const int64_t* keep, size_t nkeep,
                          femgpu_csr** out);
