@@ -122,6 +122,31 @@ def test_boxes_and_priorities_along_x_equal_the_oracle():
     assert set(tm.part.tolist()) == {0, 1, 2}
 
 
+def test_a_periodic_unit_cell_equals_the_oracle_and_its_sides_match():
+    """prism.rs:170's `periodic` (mesh2d.rs:1136-1197): a unit cell with an off-centre round
+    inclusion, extruded along z; the points on x = 0 and x = 1 (and on y = 0, y = 1) pair up."""
+    cell = ("matrix", 0, 0, (0.0, 0.0, 0.0), (1.0, 1.0, 0.5),
+            (("polygon", [(0.0, 0.0), (1.0, 0.0), (1.0, 1.0), (0.0, 1.0)]), []))
+    fibre = ("fibre", 1, 1, (0.0, 0.0, 0.0), (0.0, 0.0, 0.5),
+             (("circle", (0.4, 0.55), 0.2), []))
+    parts = [cell, fibre]
+    sp = P.Spacing(0.2, 1.3, 2)
+    tm = P.mesh([_part(p) for p in parts], 2, sp, 10**9, "", periodic=True)
+    pts, segs, segcirc, circles, classify, covers = O.footprint_inputs(parts, 2, sp.max_cell)
+    m2 = P.periodic_mesh2d(np.array(pts), np.array(segs, dtype=np.uint32),
+                           P.Size(sp.max_cell, sp.max_growth), classify)
+    planes = O.axis_planes([(p[3], p[4]) for p in parts], 2, (0.2, 1.3, 2))
+    ref = O.extrude(parts, 2, planes, [tuple(p) for p in m2.points], m2.triangles.tolist(),
+                    m2.label.tolist(), covers, m2.segments, segcirc, 10**9)
+    _same(tm, (ref, circles, len(m2.triangles), len(planes)))
+    for d in range(2):
+        o = 1 - d
+        lo = sorted((round(q[o], 12), round(q[2], 12)) for q in tm.points if abs(q[d]) < 1e-12)
+        hi = sorted((round(q[o], 12), round(q[2], 12)) for q in tm.points
+                    if abs(q[d] - 1.0) < 1e-12)
+        assert lo == hi and lo
+
+
 def test_prism_mesh_errors_carry_the_reference_texts():
     sp = P.Spacing(0.2, 1.3, 2)
     with pytest.raises(FemError, match="too many tetrahedra for this case") as e:
