@@ -81,7 +81,7 @@ def args():
     p.add_argument("--workload", default="heat",
                    choices=["heat", "cantilever", "p2beam", "batch", "serve", "stream",
                             "recover", "transient", "modes", "hexheat", "hexbeam",
-                            "hexrecover", "hexmodes"],
+                            "hexrecover", "hexmodes", "prism"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
@@ -100,6 +100,8 @@ def args():
                    help="hexbeam: the coarse matrices from the cells, as the reference forms "
                         "them (default: Galerkin products, fewer iterations here)")
     p.add_argument("--systems", type=int, default=256, help="batch: cantilevers in the batch")
+    p.add_argument("--prism-cell", type=float, default=0.04,
+                   help="prism: max_cell of the prism mesh (grid.rs Spacing)")
     p.add_argument("--rates", default="10,50,200,500",
                    help="serve: Poisson arrival rates (requests/s) to replay the stream at")
     p.add_argument("--requests", type=int, default=40, help="serve: requests per rate")
@@ -1509,6 +1511,124 @@ def run_recover(opt, rank, world, local):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ the prism-mesh workload
+PRISM_METRIC = "DOF-solves/s at 1e-8 rel. residual of P2 elasticity on the reference's prism mesh"
+
+
+def run_prism(opt, rank, world, local):
+    """elastic_tet.rs:88-337's path end to end on the reference's own mesh (prism.rs:170): a
+    4 x 2 x 0.25 plate with 3 round holes and a boss of a second material on top, meshed
+    (footprint triangulation on the host, extrusion on the device), Quadratic, P2 assembly,
+    clamped at x = 0 with a downward load at x = 4, p-multigrid to the corners and z-only
+    geometric levels (the points lie on the planes of the axis). The stage seconds are reported;
+    a step is 1 mixed solve from x = 0 to 1e-8; e2e is the same through the host C ABI."""
+    import torch
+    import femahoy_b200 as fg
+    from femahoy_b200 import prism as P
+    torch.cuda.set_device(local)
+    dist, barrier, max_over_ranks = _plumbing(world)
+    lib = fg.lib()
+    stages = {}
+    t = time.perf_counter()
+    hole = lambda c, r: P.Outline.circle(c, r)  # noqa: E731
+    plate = P.Part("plate", 0, 0, (0.0, 0.0, 0.0), (0.0, 0.0, 0.25),
+                   P.Footprint(P.Outline.polygon([(0, 0), (4, 0), (4, 2), (0, 2)]),
+                               [hole((1.0, 1.0), 0.3), hole((2.2, 0.6), 0.2),
+                                hole((3.2, 1.3), 0.25)]))
+    boss = P.Part("boss", 1, 1, (0.0, 0.0, 0.25), (0.0, 0.0, 0.45),
+                  P.Footprint(P.Outline.polygon([(1.8, 1.1), (2.8, 1.1), (2.8, 1.8),
+                                                 (1.8, 1.8)]), []))
+    tm = P.mesh([plate, boss], 2, P.Spacing(opt.prism_cell, 1.3, 2), 250_000,
+                "the mesh has more points than the solver takes")
+    stages["mesh (2D on the host, extrusion on the device)"] = time.perf_counter() - t
+    t = time.perf_counter()
+    q = fg.Quadratic.new(tm.points, tm.tets)
+    stages["quadratic"] = time.perf_counter() - t
+    n = len(q.points)
+    e = np.array([200e9, 70e9])[tm.part]
+    nu = np.array([0.3, 0.33])[tm.part]
+    coef = np.stack([e, nu], axis=1)
+    t = time.perf_counter()
+    K = fg.Csr.assemble(fg.P2_ELASTIC, q.points, q.tets, coef)
+    stages["assembly"] = time.perf_counter() - t
+    fixed = np.repeat(q.points[:, 0] == 0.0, 3)
+    free = np.nonzero(~fixed)[0].astype(np.int64)
+    load = np.zeros(3 * n)
+    at = np.nonzero(q.points[:, 0] == 4.0)[0]
+    load[3 * at + 2] = -1e3 / len(at)
+    t = time.perf_counter()
+    A = K.submatrix(free)
+    rhs = fg.reduced_rhs(K, load, np.zeros(3 * n), free)
+    Pm, coarse = fg.prolongation(q.points, len(tm.points), q.edges, free)
+    stages["submatrix, right side, prolongation"] = time.perf_counter() - t
+    t = time.perf_counter()
+    s = fg.Solver(A, fg.Unknowns.Quadratic(q.points[free // 3], Pm, coarse),
+                  fg.Method.Multigrid,
+                  options=fg.Options(precision=fg.MIXED, axes=4)).with_tol(TOL)
+    stages["solver"] = time.perf_counter() - t
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.zeros_like(b)
+    stream = torch.cuda.ExternalStream(lib.femgpu_solver_stream(s.handle))
+    for _ in range(opt.warmup):
+        with torch.cuda.stream(stream):
+            x.zero_()
+        s.solve_device(b.data_ptr(), x.data_ptr())
+    barrier()
+    stream.synchronize()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    its, res, launches = [], [], 0
+    e0.record(stream)
+    for _ in range(opt.steps):
+        with torch.cuda.stream(stream):
+            x.zero_()
+        st = s.solve_device(b.data_ptr(), x.data_ptr())
+        its.append(st.iterations)
+        res.append(st.true_residual)
+        launches += st.launches + 1
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    barrier()
+    xh = np.zeros(A.n)
+    t0 = time.perf_counter()
+    for _ in range(opt.steps):
+        s.solve_zero(rhs, xh)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    kms, kbytes = ctypes.c_double(), ctypes.c_double()
+    roof = None
+    if lib.femgpu_solver_kernel_time(s.handle, 0, 50, ctypes.byref(kms), ctypes.byref(kbytes)) == 0:
+        peak, kind = measured_peak()
+        ach = kbytes.value / (kms.value / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                "peak_kind": kind, "kernel": "the finest FP32 smoothing step",
+                "bytes_per_launch": kbytes.value, "launch_ms": kms.value, "traffic": None}
+    line = {
+        "metric": PRISM_METRIC, "value": replica_value(world, A.n, opt.steps, ms),
+        "unit": UNIT, "n_gpus": world, "steps": opt.steps, "warmup": opt.warmup,
+        "ms_per_step": ms / opt.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 V-cycle / f64 outer", "data": "synthetic",
+        "config": {"workload": f"P2 elasticity of a plate with 3 holes and a boss, prism mesh "
+                               f"max_cell {opt.prism_cell} ({len(tm.points)} points, "
+                               f"{len(tm.tets)} tetrahedra, {tm.triangles} triangles x "
+                               f"{tm.planes} planes)", "free_dofs": A.n, "tol": TOL,
+                   "levels": s.levels(), "flush": "inputs larger than L2",
+                   "parallelism": f"replicas x{world}"},
+        "iterations": {"max": max(its)}, "true_residual": max(res),
+        "stages_s": stages, "roofline": roof, "cpu_baseline": None,
+        "e2e": {"value": replica_value(world, A.n, opt.steps, e2e_s * 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * A.n, "d2h_bytes_per_step": 8 * A.n},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     opt = args()
     rank, world, local = dist_env()
@@ -1527,6 +1647,8 @@ def main():
         run_serve(opt, rank, world, local)
     elif opt.workload == "stream":
         run_stream(opt, rank, world, local)
+    elif opt.workload == "prism":
+        run_prism(opt, rank, world, local)
     else:
         run_ours(opt, rank, world, local)
 
