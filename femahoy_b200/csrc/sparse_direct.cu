@@ -145,14 +145,13 @@ __global__ void k_permute_out(int64_t n, const int64_t* __restrict__ perm,
 }
 
 // Forward solve of supernode s (1 block): z = its part of y and its children's updates (added
-// child by child in increasing order), then L11 z1 = z1 and z2 -= L21 z1; z1 goes to y, z2 is
-// the update for the parent.
+// child by child in increasing order), then L11 z1 = z1 and z2 -= L21 z1 by blocks of 32 columns;
+// z1 goes to y, z2 is the update for the parent.
 __global__ void __launch_bounds__(TH)
     k_forward(const int64_t* __restrict__ list, Fronts fr, const int64_t* __restrict__ zoff,
               const int64_t* __restrict__ child_ptr, const int64_t* __restrict__ child,
               const uint32_t* __restrict__ relind, const int64_t* __restrict__ relind_off,
               double* __restrict__ work, double* __restrict__ y) {
-    __shared__ double v;
     const int64_t s = list[blockIdx.x];
     const int64_t j0 = fr.first[s];
     const int64_t m = fr.rows_ptr[s + 1] - fr.rows_ptr[s], k = fr.first[s + 1] - j0;
@@ -169,14 +168,40 @@ __global__ void __launch_bounds__(TH)
         for (int64_t t = threadIdx.x; t < mu; t += blockDim.x) z[rel[t]] += zc[t];
         __syncthreads();
     }
-    for (int64_t j = 0; j < k; ++j) {
-        if (threadIdx.x == 0) {
-            v = z[j] / F[j + j * m];
-            z[j] = v;
+    // The columns in blocks of 32: warp 0 solves the block's triangle with shuffles (lane i
+    // holds row jb + i), then every thread takes rows below the block and subtracts the block's
+    // 32 columns times the solved values: 2 barriers per 32 columns instead of 2 per column.
+    __shared__ double zb[32];
+    for (int64_t jb = 0; jb < k; jb += 32) {
+        const int kb = (int)min((int64_t)32, k - jb);
+        if (threadIdx.x < 32) {
+            // Lane l holds row jb + l of the block's triangle in registers (all loads issued
+            // before the serial steps, which then only shuffle).
+            const int l = threadIdx.x;
+            double row[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                row[j] = (j < kb && l < kb && j <= l) ? F[(jb + l) + (jb + j) * m] : 0.0;
+            double x = l < kb ? z[jb + l] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                if (j < kb) {
+                    if (l == j) x = x / row[j];
+                    const double xj = __shfl_sync(0xffffffffu, x, j);
+                    if (l > j) x -= row[j] * xj;
+                }
+            }
+            if (l < kb) {
+                z[jb + l] = x;
+                zb[l] = x;
+            }
         }
         __syncthreads();
-        const double vj = v;
-        for (int64_t r = j + 1 + threadIdx.x; r < m; r += blockDim.x) z[r] -= F[r + j * m] * vj;
+        for (int64_t r = jb + kb + threadIdx.x; r < m; r += blockDim.x) {
+            double acc = 0.0;
+            for (int j = 0; j < kb; ++j) acc += F[r + (jb + j) * m] * zb[j];
+            z[r] -= acc;
+        }
         __syncthreads();
     }
     for (int64_t t = threadIdx.x; t < k; t += blockDim.x) y[j0 + t] = z[t];
@@ -187,7 +212,6 @@ __global__ void __launch_bounds__(TH)
 __global__ void __launch_bounds__(TH)
     k_backward(const int64_t* __restrict__ list, Fronts fr, const int64_t* __restrict__ zoff,
                double* __restrict__ work, double* __restrict__ y) {
-    __shared__ double v;
     const int64_t s = list[blockIdx.x];
     const int64_t j0 = fr.first[s];
     const int64_t r0 = fr.rows_ptr[s];
@@ -203,14 +227,40 @@ __global__ void __launch_bounds__(TH)
         if (lane == 0) z[j] = y[j0 + j] - acc;
     }
     __syncthreads();
-    for (int64_t j = k - 1; j >= 0; --j) {
-        if (threadIdx.x == 0) {
-            v = z[j] / F[j + j * m];
-            z[j] = v;
+    // L11^T x1 = t in blocks of 32 from the last: warp 0 solves the block's triangle with
+    // shuffles, then every row above the block subtracts the block's solved values times its
+    // row of L (the 32 entries contiguous in the column-major front).
+    __shared__ double zb[32];
+    for (int64_t je = k; je > 0; je -= 32) {
+        const int64_t jb = je >= 32 ? je - 32 : 0;
+        const int kb = (int)(je - jb);
+        if (threadIdx.x < 32) {
+            // Lane l holds column jb + l of the block's triangle (contiguous in the front).
+            const int l = threadIdx.x;
+            double col[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                col[j] = (j < kb && l < kb && j >= l) ? F[(jb + j) + (jb + l) * m] : 0.0;
+            double x = l < kb ? z[jb + l] : 0.0;
+#pragma unroll
+            for (int j = 31; j >= 0; --j) {
+                if (j < kb) {
+                    if (l == j) x = x / col[j];
+                    const double xj = __shfl_sync(0xffffffffu, x, j);
+                    if (l < j) x -= col[j] * xj;
+                }
+            }
+            if (l < kb) {
+                z[jb + l] = x;
+                zb[l] = x;
+            }
         }
         __syncthreads();
-        const double vj = v;
-        for (int64_t i = threadIdx.x; i < j; i += blockDim.x) z[i] -= F[j + i * m] * vj;
+        for (int64_t i = threadIdx.x; i < jb; i += blockDim.x) {
+            double acc = 0.0;
+            for (int j = 0; j < kb; ++j) acc += F[(jb + j) + i * m] * zb[j];
+            z[i] -= acc;
+        }
         __syncthreads();
     }
     for (int64_t t = threadIdx.x; t < k; t += blockDim.x) y[j0 + t] = z[t];
