@@ -220,11 +220,24 @@ __global__ void __launch_bounds__(TH)
     const double* F = fr.f + fr.foff[s];
     double* z = work + zoff[s];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (int64_t j = warp; j < k; j += nw) {
-        double acc = 0.0;
-        for (int64_t r = k + lane; r < m; r += 32) acc += F[r + j * m] * y[R[r]];
-        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-        if (lane == 0) z[j] = y[j0 + j] - acc;
+    // The solved values of the rows below (y at R[r], r >= k) gathered into shared memory a
+    // chunk at a time, so that each warp's column sums read the front coalesced and x from
+    // shared memory, with no dependent global loads.
+    constexpr int XG = 1024;
+    __shared__ double xg[XG];
+    for (int64_t t = threadIdx.x; t < k; t += blockDim.x) z[t] = y[j0 + t];
+    for (int64_t r0 = k; r0 < m; r0 += XG) {
+        const int cnt = (int)min((int64_t)XG, m - r0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) xg[t] = y[R[r0 + t]];
+        __syncthreads();
+        for (int64_t j = warp; j < k; j += nw) {
+            const double* col = F + r0 + j * m;
+            double acc = 0.0;
+            for (int t = lane; t < cnt; t += 32) acc += col[t] * xg[t];
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) z[j] -= acc;
+        }
     }
     __syncthreads();
     // L11^T x1 = t in blocks of 32 from the last: warp 0 solves the block's triangle with
