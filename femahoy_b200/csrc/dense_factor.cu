@@ -453,6 +453,36 @@ int dense_inverse_batch(const std::vector<const DevCsr*>& a, const std::vector<d
     return -1;
 }
 
+void triangular_inverse_batch(const std::vector<int64_t>& n, const std::vector<double*>& L,
+                              const std::vector<double*>& W, DenseBatchWork* w, cudaStream_t s) {
+    const int count = (int)n.size();
+    if (count == 0) return;
+    if (count > 65535) throw Failure(FEMGPU_ERR_TOO_LARGE, "more than 65535 triangles at once");
+    int64_t nmax = 0;
+    std::vector<DenseMember> dm(count);
+    for (int j = 0; j < count; ++j) {
+        dm[j] = DenseMember{nullptr, nullptr, nullptr, L[j], W[j], nullptr, nullptr, nullptr, n[j]};
+        nmax = std::max(nmax, n[j]);
+    }
+    if (w->members.count < (size_t)count) w->members.alloc(count);
+    w->members.upload(dm.data(), count, s);
+    const DenseMember* M = w->members.p;
+    const unsigned z = (unsigned)count;
+    k_identity_b<<<dim3((unsigned)blocks_for(nmax * nmax, TH), 1, z), TH, 0, s>>>(M);
+    for (int64_t b0 = 0; b0 < nmax; b0 += PANEL) {
+        const int64_t ncols = std::min(nmax, b0 + PANEL);
+        k_trsm_rows_b<<<dim3((unsigned)((ncols + ROWS_TH - 1) / ROWS_TH), 1, z), ROWS_TH, 0, s>>>(
+            M, b0);
+        const int64_t rows = nmax - ncols;
+        if (rows > 0)
+            k_gemm_sub_b<<<dim3((unsigned)((rows + TILE - 1) / TILE),
+                                (unsigned)((ncols + TILE - 1) / TILE), z),
+                           TH, 0, s>>>(M, b0);
+    }
+    FG_CHECK_LAUNCH();
+    FG_CUDA(cudaStreamSynchronize(s));  // the member table is the caller's until here
+}
+
 void dense_partial_cholesky(double* F, int64_t m, int64_t k, const double* diag0, int64_t col0,
                             unsigned long long* status, cudaStream_t s) {
     for (int64_t p0 = 0; p0 < k; p0 += PANEL) {

@@ -69,4 +69,9 @@ struct DenseBatchWork {
 int dense_inverse_batch(const std::vector<const DevCsr*>& a, const std::vector<double*>& inv,
                         DenseBatchWork* w, cudaStream_t s, std::string* text);
 
+// W[j] = L[j]^-1 for the lower triangular n_j x n_j matrices L[j] (device, column-major, zeros
+// above the diagonal), each step 1 launch for all; returns with the work finished.
+void triangular_inverse_batch(const std::vector<int64_t>& n, const std::vector<double*>& L,
+                              const std::vector<double*>& W, DenseBatchWork* w, cudaStream_t s);
+
 }  // namespace femgpu

@@ -2549,6 +2549,9 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         H->ncoarse = last.n;
         H->sparse = std::make_unique<SparseFactor>();
         H->sparse->factor(last, xyz.data(), s_);
+        // Inside the V-cycle the large supernodes' triangles are applied by products with their
+        // inverses (parallel) rather than by substitution column by column.
+        H->sparse->invert_blocks(64, s_);
         H->cb.alloc(last.n);
         H->cb.zero(s_);
         H->cx.alloc(last.n);

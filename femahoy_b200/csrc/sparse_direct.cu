@@ -144,6 +144,72 @@ __global__ void k_permute_out(int64_t n, const int64_t* __restrict__ perm,
         x[perm[j]] = y[j];
 }
 
+// The product forms of a supernode's triangular solves, when the inverse W = L11^-1 of its
+// diagonal block is kept (k x k, column-major): z1 = W z1 and z2 -= L21 z1 in the forward
+// direction, x1 = W^T t in the backward one. The vector is staged in shared memory 1024 values
+// at a time; tmp is the supernode's own range of a scratch vector (its columns j0 .. j0 + k).
+constexpr int ZS = 1024;
+
+__device__ void forward_by_inverse(const double* __restrict__ W, const double* __restrict__ F,
+                                   int64_t m, int64_t k, double* __restrict__ z,
+                                   double* __restrict__ tmp) {
+    __shared__ double zs[ZS];
+    for (int64_t i = threadIdx.x; i < k; i += blockDim.x) tmp[i] = 0.0;
+    for (int64_t c0 = 0; c0 < k; c0 += ZS) {
+        const int cnt = (int)min((int64_t)ZS, k - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) zs[t] = z[c0 + t];
+        __syncthreads();
+        for (int64_t i = c0 + threadIdx.x; i < k; i += blockDim.x) {
+            const int hi = (int)min((int64_t)cnt, i - c0 + 1);  // W lower: j <= i
+            double acc = 0.0;
+            for (int j = 0; j < hi; ++j) acc += W[i + (c0 + j) * k] * zs[j];
+            tmp[i] += acc;
+        }
+    }
+    __syncthreads();
+    for (int64_t i = threadIdx.x; i < k; i += blockDim.x) z[i] = tmp[i];
+    // z2 -= L21 z1, z1 staged again.
+    for (int64_t c0 = 0; c0 < k; c0 += ZS) {
+        const int cnt = (int)min((int64_t)ZS, k - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) zs[t] = z[c0 + t];
+        __syncthreads();
+        for (int64_t r = k + threadIdx.x; r < m; r += blockDim.x) {
+            double acc = 0.0;
+            for (int j = 0; j < cnt; ++j) acc += F[r + (c0 + j) * m] * zs[j];
+            z[r] -= acc;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ void backward_by_inverse(const double* __restrict__ W, int64_t k,
+                                    double* __restrict__ z, double* __restrict__ tmp) {
+    __shared__ double ts[ZS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int64_t j = threadIdx.x; j < k; j += blockDim.x) tmp[j] = 0.0;
+    for (int64_t c0 = 0; c0 < k; c0 += ZS) {
+        const int cnt = (int)min((int64_t)ZS, k - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) ts[t] = z[c0 + t];
+        __syncthreads();
+        // x1[j] += sum over rows i of the chunk with i >= j of W[i][j] t[i] (column j of W is
+        // contiguous): a warp per column.
+        for (int64_t j = warp; j < k && j < c0 + cnt; j += nw) {
+            const int lo = (int)max((int64_t)0, j - c0);
+            const double* col = W + c0 + j * k;
+            double acc = 0.0;
+            for (int t = lo + lane; t < cnt; t += 32) acc += col[t] * ts[t];
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (lane == 0) tmp[j] += acc;
+        }
+    }
+    __syncthreads();
+    for (int64_t j = threadIdx.x; j < k; j += blockDim.x) z[j] = tmp[j];
+    __syncthreads();
+}
+
 // Forward solve of supernode s (1 block): z = its part of y and its children's updates (added
 // child by child in increasing order), then L11 z1 = z1 and z2 -= L21 z1 by blocks of 32 columns;
 // z1 goes to y, z2 is the update for the parent.
@@ -151,7 +217,9 @@ __global__ void __launch_bounds__(TH)
     k_forward(const int64_t* __restrict__ list, Fronts fr, const int64_t* __restrict__ zoff,
               const int64_t* __restrict__ child_ptr, const int64_t* __restrict__ child,
               const uint32_t* __restrict__ relind, const int64_t* __restrict__ relind_off,
-              double* __restrict__ work, double* __restrict__ y) {
+              double* __restrict__ work, double* __restrict__ y,
+              const int64_t* __restrict__ winv_off, const double* __restrict__ winv,
+              double* __restrict__ tmp) {
     const int64_t s = list[blockIdx.x];
     const int64_t j0 = fr.first[s];
     const int64_t m = fr.rows_ptr[s + 1] - fr.rows_ptr[s], k = fr.first[s + 1] - j0;
@@ -167,6 +235,11 @@ __global__ void __launch_bounds__(TH)
         const uint32_t* rel = relind + relind_off[c];
         for (int64_t t = threadIdx.x; t < mu; t += blockDim.x) z[rel[t]] += zc[t];
         __syncthreads();
+    }
+    if (winv_off && winv_off[s] >= 0) {
+        forward_by_inverse(winv + winv_off[s], F, m, k, z, tmp + j0);
+        for (int64_t t = threadIdx.x; t < k; t += blockDim.x) y[j0 + t] = z[t];
+        return;
     }
     // The columns in blocks of 32: warp 0 solves the block's triangle with shuffles (lane i
     // holds row jb + i), then every thread takes rows below the block and subtracts the block's
@@ -211,7 +284,9 @@ __global__ void __launch_bounds__(TH)
 // below of L[r][j] x_r (a warp per column), then L11^T x1 = t.
 __global__ void __launch_bounds__(TH)
     k_backward(const int64_t* __restrict__ list, Fronts fr, const int64_t* __restrict__ zoff,
-               double* __restrict__ work, double* __restrict__ y) {
+               double* __restrict__ work, double* __restrict__ y,
+               const int64_t* __restrict__ winv_off, const double* __restrict__ winv,
+               double* __restrict__ tmp) {
     const int64_t s = list[blockIdx.x];
     const int64_t j0 = fr.first[s];
     const int64_t r0 = fr.rows_ptr[s];
@@ -240,6 +315,11 @@ __global__ void __launch_bounds__(TH)
         }
     }
     __syncthreads();
+    if (winv_off && winv_off[s] >= 0) {
+        backward_by_inverse(winv + winv_off[s], k, z, tmp + j0);
+        for (int64_t t = threadIdx.x; t < k; t += blockDim.x) y[j0 + t] = z[t];
+        return;
+    }
     // L11^T x1 = t in blocks of 32 from the last: warp 0 solves the block's triangle with
     // shuffles, then every row above the block subtracts the block's solved values times its
     // row of L (the 32 entries contiguous in the column-major front).
@@ -378,6 +458,7 @@ void SparseFactor::factor(const HostCsr& a, const double* xyz, cudaStream_t s) {
     rows_ptr_.upload(S.rows_ptr.data(), ns_ + 1, s);
     rows_.upload(S.rows.data(), S.rows.size(), s);
     foff_.upload(foff.data(), ns_, s);
+    host_foff_ = foff;
     zoff_.upload(zoff.data(), ns_, s);
     child_ptr_.upload(cptr.data(), ns_ + 1, s);
     child_.upload(clist.data(), std::max<size_t>(1, clist.size()), s);
@@ -440,6 +521,63 @@ void SparseFactor::factor(const HostCsr& a, const double* xyz, cudaStream_t s) {
     FG_CUDA(cudaStreamSynchronize(s));
 }
 
+namespace {
+
+// The lower triangle of the k x k diagonal block of front F (leading dimension m) into L (leading
+// dimension k), zeros above: 1 member of the copy per blockIdx.y.
+struct BlockCopy {
+    const double* F;
+    double* L;
+    int64_t m, k;
+};
+
+__global__ void k_copy_blocks(const BlockCopy* __restrict__ c) {
+    const BlockCopy b = c[blockIdx.y];
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < b.k * b.k;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t % b.k, j = t / b.k;
+        b.L[t] = i >= j ? b.F[i + j * b.m] : 0.0;
+    }
+}
+
+}  // namespace
+
+void SparseFactor::invert_blocks(int64_t min_cols, cudaStream_t s) {
+    std::vector<int64_t> off(ns_, -1);
+    std::vector<int64_t> members;
+    int64_t total = 0, kmax = 0;
+    for (int64_t t = 0; t < ns_; ++t)
+        if (k_[t] >= min_cols) {
+            off[t] = total;
+            total += k_[t] * k_[t];
+            members.push_back(t);
+            kmax = std::max(kmax, k_[t]);
+        }
+    if (members.empty()) return;
+    if (members.size() > 65535) throw Failure(FEMGPU_ERR_TOO_LARGE, "too many large supernodes");
+    winv_.alloc(total);
+    tmp_.alloc(std::max<int64_t>(n_, 1));
+    DevBuf<double> lc(total);
+    std::vector<BlockCopy> bc;
+    std::vector<int64_t> ns;
+    std::vector<double*> ls, ws;
+    for (int64_t t : members) {
+        bc.push_back({fronts_.p + host_foff_[t], lc.p + off[t], m_[t], k_[t]});
+        ns.push_back(k_[t]);
+        ls.push_back(lc.p + off[t]);
+        ws.push_back(winv_.p + off[t]);
+    }
+    DevBuf<BlockCopy> dbc;
+    dbc.upload(bc.data(), bc.size(), s);
+    k_copy_blocks<<<dim3((unsigned)blocks_for(kmax * kmax, TH, 256), (unsigned)bc.size()), TH, 0,
+                    s>>>(dbc.p);
+    FG_CHECK_LAUNCH();
+    DenseBatchWork w;
+    triangular_inverse_batch(ns, ls, ws, &w, s);
+    winv_off_.upload(off.data(), ns_, s);
+    FG_CUDA(cudaStreamSynchronize(s));
+}
+
 void SparseFactor::solve(const double* b, double* x, cudaStream_t s) {
     const Fronts fr{first_.p, rows_ptr_.p, rows_.p, foff_.p, fronts_.p};
     k_permute_in<<<blocks_for(n_, TH), TH, 0, s>>>(n_, perm_.p, b, y_.p);
@@ -448,13 +586,15 @@ void SparseFactor::solve(const double* b, double* x, cudaStream_t s) {
         if (cnt)
             k_forward<<<(unsigned)cnt, TH, 0, s>>>(level_list_.p + level_at_[h], fr, zoff_.p,
                                                    child_ptr_.p, child_.p, relind_.p,
-                                                   relind_off_.p, work_.p, y_.p);
+                                                   relind_off_.p, work_.p, y_.p, winv_off_.p,
+                                                   winv_.p, tmp_.p);
     }
     for (int64_t h = height_; h >= 0; --h) {
         const int64_t cnt = level_at_[h + 1] - level_at_[h];
         if (cnt)
             k_backward<<<(unsigned)cnt, TH, 0, s>>>(level_list_.p + level_at_[h], fr, zoff_.p,
-                                                    work_.p, y_.p);
+                                                    work_.p, y_.p, winv_off_.p, winv_.p,
+                                                    tmp_.p);
     }
     k_permute_out<<<blocks_for(n_, TH), TH, 0, s>>>(n_, perm_.p, y_.p, x);
     FG_CHECK_LAUNCH();

@@ -37,6 +37,11 @@ class SparseFactor {
     void factor(const HostCsr& a, const double* xyz, cudaStream_t s);
     // x = A^-1 b, device arrays of n values (x may not alias b).
     void solve(const double* b, double* x, cudaStream_t s);
+    // Keeps W = L11^-1 of the diagonal block of each supernode of at least `min_cols` columns,
+    // so that the solves take its triangles by 2 products (fully parallel) instead of column by
+    // column: for a factor used inside an iteration (the V-cycle's coarsest level), where the
+    // products' rounding (W's, not the substitution's) does not matter.
+    void invert_blocks(int64_t min_cols, cudaStream_t s);
     int64_t n() const { return n_; }
     // The kernels that 1 solve launches.
     size_t solve_launches() const;
@@ -54,6 +59,10 @@ class SparseFactor {
     DevBuf<uint32_t> rows_, relind_;
     DevBuf<int64_t> relind_off_;
     DevBuf<double> fronts_, work_, y_;
+    // invert_blocks: the inverses end to end, each supernode's offset into them (-1: none), and
+    // a scratch vector of n values.
+    DevBuf<double> winv_, tmp_;
+    DevBuf<int64_t> winv_off_;
     // The level schedule (host): the supernodes of each height, small and large fronts apart,
     // and the extend-add chunks per (height, child rank).
     std::vector<std::vector<int64_t>> small_, large_;
@@ -66,7 +75,7 @@ class SparseFactor {
     };
     std::vector<Chunks> chunks_;
     DevBuf<int2> chunk_;  // (child, first entry / 4096)
-    std::vector<int64_t> host_first_;
+    std::vector<int64_t> host_first_, host_foff_;
 };
 
 }  // namespace femgpu
