@@ -292,3 +292,34 @@ def test_axis_planes_with_extra_keys_equal_the_oracle():
         got = P.axis_planes(parts, d, sp, extra=[0.7, 1.1])
         assert got.tolist() == O.axis_planes([(p.lo, p.hi) for p in parts], d, (0.2, 1.3, 2),
                                              [0.7, 1.1])
+
+
+# ------------------------------------------------------------------ the box grid's oracle (grid.rs)
+
+def test_box_grid_oracle_passes_the_reference_tests():
+    """oracle/grid.py against grid.rs:548-642: the higher priority holds the overlap, the same
+    priority with other materials is refused, the faces of a box cover its surface."""
+    from oracle import grid as OG
+    sp = (1.0, 1.3, 2)
+    parts = [("a", 0, 0, (0.0,) * 3, (2.0,) * 3), ("b", 1, 1, (1.0,) * 3, (3.0,) * 3)]
+    planes, part = OG.build(parts, sp)
+    nx, ny = len(planes[0]) - 1, len(planes[1]) - 1
+
+    def cell_at(x):
+        i = [int(np.searchsorted(planes[d], x[d]) - 1) for d in range(3)]
+        return i[0] + nx * (i[1] + ny * i[2])
+
+    assert part[cell_at((1.5, 1.5, 1.5))] == 1 and part[cell_at((0.5, 0.5, 0.5))] == 0
+    assert part[cell_at((2.5, 0.5, 0.5))] == OG.VOID
+    with pytest.raises(ValueError, match="same priority"):
+        OG.build([("a", 0, 0, (0.0,) * 3, (2.0,) * 3), ("b", 1, 0, (1.0,) * 3, (3.0,) * 3)], sp)
+    planes, part = OG.build([("a", 0, 0, (0.0,) * 3, (2.0, 3.0, 4.0))], sp)
+    n = [len(p) - 1 for p in planes]
+    area = 0.0
+    for cell, side in OG.faces(planes, part):
+        c = (cell % n[0], (cell // n[0]) % n[1], cell // (n[0] * n[1]))
+        size = [planes[d][c[d] + 1] - planes[d][c[d]] for d in range(3)]
+        area += np.prod([size[d] for d in range(3) if d != side // 2])
+    assert abs(area - 2.0 * (6.0 + 8.0 + 12.0)) < 1e-9
+    points, ijk, cells, cell_of, mpart = OG.number(planes, part)
+    assert len(points) == (n[0] + 1) * (n[1] + 1) * (n[2] + 1) and len(cells) == len(part)
