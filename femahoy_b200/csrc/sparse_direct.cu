@@ -611,7 +611,8 @@ size_t SparseFactor::bytes() const {
     return fronts_.bytes() + work_.bytes() + y_.bytes() + perm_.bytes() + first_.bytes() +
            rows_ptr_.bytes() + rows_.bytes() + foff_.bytes() + zoff_.bytes() +
            child_ptr_.bytes() + child_.bytes() + relind_.bytes() + relind_off_.bytes() +
-           small_list_.bytes() + level_list_.bytes() + chunk_.bytes();
+           small_list_.bytes() + level_list_.bytes() + chunk_.bytes() + winv_.bytes() +
+           tmp_.bytes() + winv_off_.bytes();
 }
 
 std::string SparseFactor::describe() const {
