@@ -1569,6 +1569,16 @@ def run_prism(opt, rank, world, local):
     b = torch.from_numpy(rhs).cuda()
     x = torch.zeros_like(b)
     stream = torch.cuda.ExternalStream(lib.femgpu_solver_stream(s.handle))
+    if opt.breakdown:
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                x.zero_()
+            st = s.solve_device(b.data_ptr(), x.data_ptr())
+        if rank == 0:
+            print(f"== mixed: {st.iterations} iterations, {st.seconds * 1e3:.3f} ms per solve")
+            print(s.describe())
+            print(s.breakdown(), flush=True)
+        return
     for _ in range(opt.warmup):
         with torch.cuda.stream(stream):
             x.zero_()
