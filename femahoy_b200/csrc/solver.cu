@@ -2333,6 +2333,12 @@ void SolverImpl::tune_degree() {
             }
             if (rep == 1 && st.residual > 0.0 && st.residual < 1.0)
                 cost = st.seconds / -std::log10(st.residual);
+            // A trial of 50 ms or more: the first solve's graph capture is a small part of it,
+            // so its time decides and the second is not run.
+            if (rep == 0 && st.seconds >= 0.05 && st.residual > 0.0 && st.residual < 1.0) {
+                cost = st.seconds / -std::log10(st.residual);
+                break;
+            }
         }
         if (cost < best) {
             best = cost;
