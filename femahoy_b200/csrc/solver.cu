@@ -2354,10 +2354,10 @@ void SolverImpl::tune_degree() {
 void SolverImpl::sparse_direct(const HostCsr& h, const std::vector<double>& xyz) {
     sparse_ = std::make_unique<SparseFactor>();
     sparse_->factor(h, xyz.data(), s_);
-    // The triangles of supernodes of 32 columns or more by products with their inverses: the
-    // direct solve of a 36,300-unknown P2 beam 3.7 against 5.9 ms, of a 32^3 heat cube 6.6
+    // The triangles of supernodes of 8 columns or more by products with their inverses: the
+    // direct solve of a 36,300-unknown P2 beam 3.7 against 5.9 ms, of a 32^3 heat cube 6.3
     // against 9.6 ms.
-    sparse_->invert_blocks(32, s_);
+    sparse_->invert_blocks(8, s_);
 }
 
 void SolverImpl::dense_direct(const HostCsr& h) {
@@ -2561,7 +2561,7 @@ void SolverImpl::build_levels(const std::vector<const DevCsr*>& mats, std::vecto
         H->sparse->factor(last, xyz.data(), s_);
         // Inside the V-cycle the large supernodes' triangles are applied by products with their
         // inverses (parallel) rather than by substitution column by column.
-        H->sparse->invert_blocks(32, s_);
+        H->sparse->invert_blocks(8, s_);
         H->cb.alloc(last.n);
         H->cb.zero(s_);
         H->cx.alloc(last.n);
