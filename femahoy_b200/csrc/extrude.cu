@@ -272,9 +272,11 @@ struct TetMesh {
 };
 
 // prism.rs:185-380 mesh_hollow.
+// The host steps first (footprints, planes, the parts of the layers, their errors), then the
+// stream *stream is created for the device steps (the caller destroys it).
 void prism_mesh(const std::vector<Part>& parts, int axis, const Spacing& spacing,
                 size_t max_points, const std::string& refusal, bool periodic,
-                const std::vector<uint8_t>& hollow_in, TetMesh* out, cudaStream_t s) {
+                const std::vector<uint8_t>& hollow_in, TetMesh* out, cudaStream_t* stream) {
     std::vector<uint8_t> hollow(parts.size(), 0);
     for (size_t k = 0; k < parts.size() && k < hollow_in.size(); ++k) hollow[k] = hollow_in[k] != 0;
     if (parts.empty()) throw Failure(FEMGPU_ERR_INVALID, "the model has no part");
@@ -320,6 +322,8 @@ void prism_mesh(const std::vector<Part>& parts, int axis, const Spacing& spacing
     const int64_t nv = (int64_t)m.points.size(), nt = (int64_t)m.triangles.size();
     if ((uint64_t)nv * planes.size() > 0xffffffffull)
         throw Failure(FEMGPU_ERR_TOO_LARGE, "the mesh has too many points: use a larger max_cell");
+    FG_CUDA(cudaStreamCreateWithFlags(stream, cudaStreamNonBlocking));
+    const cudaStream_t s = *stream;
     const int64_t nq = nt * layers, slots = nv * (int64_t)planes.size();
     // The flat mesh and the tables on the device.
     DevBuf<double> d_flat, d_planes;
@@ -526,13 +530,15 @@ int femgpu_prism_mesh(const femgpu_part* parts, size_t nparts, int axis,
         std::vector<uint8_t> hol(hollow, hollow + nhollow);
         const Spacing sp{spacing->max_cell, spacing->max_growth, spacing->min_cells};
         cudaStream_t s = nullptr;
-        FG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         auto* h = new femgpu_tetmesh;
         try {
-            prism_mesh(ps, axis, sp, max_points, refusal ? refusal : "", periodic != 0, hol, &h->m, s);
+            prism_mesh(ps, axis, sp, max_points, refusal ? refusal : "", periodic != 0, hol, &h->m,
+                       &s);
         } catch (...) {
-            cudaStreamSynchronize(s);
-            cudaStreamDestroy(s);
+            if (s) {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
             delete h;
             throw;
         }

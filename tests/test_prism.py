@@ -323,3 +323,35 @@ def test_box_grid_oracle_passes_the_reference_tests():
     assert abs(area - 2.0 * (6.0 + 8.0 + 12.0)) < 1e-9
     points, ijk, cells, cell_of, mpart = OG.number(planes, part)
     assert len(points) == (n[0] + 1) * (n[1] + 1) * (n[2] + 1) and len(cells) == len(part)
+
+
+def test_prism_mesh_refuses_bad_parts_with_the_reference_texts_before_any_device_work():
+    """prism.rs:197-200, 404-481, 224-240: the host steps run first, so these refusals need no
+    GPU; each text is the reference's."""
+    sp = P.Spacing(0.2, 1.3, 2)
+    poly = lambda c: P.Footprint(P.Outline.polygon(c), [])  # noqa: E731
+    sq = [(0, 0), (1, 0), (1, 1), (0, 1)]
+    cases = [
+        ([], sp, "the model has no part"),
+        ([P.Part("a", 0, 0, (0, 0, 0), (1, 1, 1))], P.Spacing(float("inf"), 1.3, 2),
+         "max_cell must be a number above 0"),
+        ([P.Part("c", 0, 0, (0, 0, 1), (1, 1, 1))], sp,
+         "part c: its z range must be 2 finite numbers, the first smaller"),
+        ([P.Part("b", 0, 0, (1, 0, 0), (1, 1, 1))], sp,
+         "part b: each range must have the first number smaller"),
+        ([P.Part("p", 0, 0, (0, 0, 0), (0, 0, 1), poly([(0, 0), (1, 0)]))], sp,
+         "part p: a polygon needs 3 or more corners with finite coordinates"),
+        ([P.Part("q", 0, 0, (0, 0, 0), (0, 0, 1),
+                 P.Footprint(P.Outline.circle((0, 0), 0.0), []))], sp,
+         "part q: a circle needs a finite centre and a radius above 0"),
+        ([P.Part("z", 0, 0, (0, 0, 0), (0, 0, 1), poly([(0, 0), (1, 1), (2, 2)]))], sp,
+         "part z: an outline has no area"),
+        ([P.Part("a", 0, 0, (0, 0, 0), (0, 0, 1), poly(sq)),
+          P.Part("b", 1, 0, (0, 0, 0), (0, 0, 1), poly([(0.5, 0.5), (2, 0.5), (2, 2), (0.5, 2)]))],
+         sp, "parts a and b overlap with the same priority and other materials: give the part "
+             "that must hold the overlap a higher priority"),
+    ]
+    for parts, spacing, text in cases:
+        with pytest.raises(FemError) as e:
+            P.mesh(parts, 2, spacing, 10**9, "")
+        assert str(e.value) == text
