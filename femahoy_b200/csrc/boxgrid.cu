@@ -168,9 +168,11 @@ struct BoxGrid {
     DevBuf<uint32_t> d_cells;
 };
 
+// The host steps first (the checks, the planes), then the stream *stream is created for the
+// device steps (the caller destroys it).
 void box_grid(const std::vector<Part>& parts, const Spacing& spacing,
               const std::vector<double> extra[3], size_t max_points, const std::string& refusal,
-              BoxGrid* out, cudaStream_t s) {
+              BoxGrid* out, cudaStream_t* stream) {
     auto fail = [](const std::string& t) { throw Failure(FEMGPU_ERR_INVALID, t); };
     const char* axis[3] = {"x", "y", "z"};
     if (parts.empty()) fail("the model has no part");
@@ -210,6 +212,8 @@ void box_grid(const std::vector<Part>& parts, const Spacing& spacing,
         pr[k].priority = parts[k].priority;
         pr[k].material = parts[k].material;
     }
+    FG_CUDA(cudaStreamCreateWithFlags(stream, cudaStreamNonBlocking));
+    const cudaStream_t s = *stream;
     DevBuf<PartRange> d_pr;
     d_pr.upload(pr.data(), pr.size(), s);
     DevBuf<uint32_t> part(ncells);
@@ -351,13 +355,14 @@ int femgpu_box_grid(const femgpu_part* parts, size_t nparts, const femgpu_spacin
             }
         const Spacing sp{spacing->max_cell, spacing->max_growth, spacing->min_cells};
         cudaStream_t s = nullptr;
-        FG_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         auto* h = new femgpu_boxgrid;
         try {
-            box_grid(ps, sp, ex, max_points, refusal ? refusal : "", &h->g, s);
+            box_grid(ps, sp, ex, max_points, refusal ? refusal : "", &h->g, &s);
         } catch (...) {
-            cudaStreamSynchronize(s);
-            cudaStreamDestroy(s);
+            if (s) {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
             delete h;
             throw;
         }

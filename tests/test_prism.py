@@ -355,3 +355,22 @@ def test_prism_mesh_refuses_bad_parts_with_the_reference_texts_before_any_device
         with pytest.raises(FemError) as e:
             P.mesh(parts, 2, spacing, 10**9, "")
         assert str(e.value) == text
+
+
+def test_box_grid_refuses_bad_parts_and_spacings_before_any_device_work():
+    """grid.rs:119-143 and 473-481: the checks and the planes run on the host first, so these
+    refusals need no GPU; each text is the reference's."""
+    from femahoy_b200 import grid as G
+    a = P.Part("a", 0, 0, (0.0,) * 3, (1.0,) * 3)
+    cases = [
+        ([], P.Spacing(1.0, 1.3, 2), "the model has no part"),
+        ([a], P.Spacing(0.0, 1.3, 2), "max_cell must be a number above 0"),
+        ([a], P.Spacing(0.5, 1.0, 2), "max_growth must be a number above 1"),
+        ([a], P.Spacing(0.5, 1.3, 0), "min_cells must be 1 or more"),
+        ([P.Part("bad", 0, 0, (0.0, 1.0, 0.0), (1.0, 1.0, 1.0))], P.Spacing(1.0, 1.3, 2),
+         "part bad: its y range must be 2 finite numbers, the first smaller"),
+    ]
+    for parts, sp, text in cases:
+        with pytest.raises(FemError) as e:
+            G.build(parts, sp)
+        assert str(e.value) == text
