@@ -81,7 +81,7 @@ def args():
     p.add_argument("--workload", default="heat",
                    choices=["heat", "cantilever", "p2beam", "batch", "serve", "stream",
                             "recover", "transient", "modes", "hexheat", "hexbeam",
-                            "hexrecover", "hexmodes", "prism"],
+                            "hexrecover", "hexmodes", "prism", "direct"],
                    help="heat: 1 right side of the 128^3 heat cube (the headline line); "
                         "cantilever: the 40x4x4 P1 cantilever at 1e-10; p2beam: the 200x20x20 "
                         "P2 beam; batch: 256 cantilevers x 16 load cases in 1 batched solve; "
@@ -1511,6 +1511,89 @@ def run_recover(opt, rank, world, local):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ the direct workload
+DIRECT_METRIC = "DOF-solves/s of the direct method (sparse multifrontal factor on the device)"
+
+
+def run_direct(opt, rank, world, local):
+    """The direct method of solve.rs:92-250 above 4,096 unknowns (the reference's choice for P2
+    models up to 30,000 unknowns, elastic_tet.rs:52-56): the 50 x 5 x 5 P2 beam (36,300 free
+    unknowns), factored once on the device (cholesky.rs:44-167's multifrontal factor in the
+    order of order.rs); a step is 1 solve of a resident right side (the 2 triangular solves).
+    The solution is checked against the oracle's factor (CPU) and timed beside it."""
+    import torch
+    import femahoy_b200 as fg
+    import oracle
+    from femahoy_b200 import meshgen as mg
+    torch.cuda.set_device(local)
+    dist, barrier, max_over_ranks = _plumbing(world)
+    dims, lengths = (50, 5, 5), (250.0, 25.0, 25.0)
+    m = mg.box(*dims, lengths)
+    q = fg.Quadratic.new(m.points, m.tets)
+    prob = mg.beam_p2(q.edges, q.tets, dims=dims, lengths=lengths, mesh=m, seed=SEED)
+    K = fg.Csr.assemble(fg.P2_ELASTIC, prob.xyz, prob.nodes, prob.coef)
+    A = K.submatrix(prob.free)
+    rhs = fg.reduced_rhs(K, prob.load, prob.values, prob.free)
+    xyz = prob.xyz[prob.free // 3]
+    P, coarse = fg.prolongation(prob.xyz, m.n, q.edges, prob.free)
+    t = time.perf_counter()
+    s = fg.Solver(A, fg.Unknowns.Quadratic(xyz, P, coarse), fg.Method.Direct)
+    setup_s = time.perf_counter() - t
+    b = torch.from_numpy(rhs).cuda()
+    x = torch.zeros_like(b)
+    for _ in range(opt.warmup):
+        s.solve_device(b.data_ptr(), x.data_ptr())
+    barrier()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    secs, res, launches = [], [], 0
+    for _ in range(opt.steps):
+        st = s.solve_device(b.data_ptr(), x.data_ptr())
+        secs.append(st.seconds)
+        res.append(st.true_residual)
+        launches += st.launches
+    clk = clocks.stop()
+    ms = max_over_ranks(1e3 * sum(secs))
+    xh = np.zeros(A.n)
+    t0 = time.perf_counter()
+    for _ in range(opt.steps):
+        s.solve(rhs, xh)
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    cpu = None
+    err = None
+    if rank == 0 and not opt.no_cpu_baseline:
+        Ko = oracle.pattern(prob.n_unknowns, oracle.dof_elements(prob.nodes))
+        Ko.assemble(2, prob.xyz, prob.nodes, prob.coef)
+        t0 = time.perf_counter()
+        xd, _ = oracle.direct_solve(Ko.submatrix(prob.free), xyz, rhs)
+        cpu_s = time.perf_counter() - t0
+        err = float(np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd))
+        cpu = {"value": A.n / cpu_s, "unit": "DOF-solves/s", "cores": 1, "kind": "port",
+               "sample": "1 factor and solve of the same system by the oracle (its whole direct "
+                         "solve, the factor included)"}
+    line = {
+        "metric": DIRECT_METRIC, "value": replica_value(world, A.n, opt.steps, ms),
+        "unit": UNIT, "n_gpus": world, "steps": opt.steps, "warmup": opt.warmup,
+        "ms_per_step": ms / opt.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "the direct method on the 50x5x5 P2 beam (36,300 free unknowns)",
+                   "free_dofs": A.n, "parallelism": f"replicas x{world}",
+                   "flush": "none: each solve reads the factor's L entries (0.11 GB) and its "
+                            "block inverses, about the size of L2"},
+        "setup_s": setup_s, "true_residual": max(res), "error_vs_oracle": err,
+        "describe": s.describe().strip().splitlines()[-1],
+        "cpu_baseline": cpu, "roofline": None,
+        "e2e": {"value": replica_value(world, A.n, opt.steps, e2e_s * 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": 8 * A.n, "d2h_bytes_per_step": 8 * A.n},
+        "gpu_launches": launches, "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ------------------------------------------------------------------ the prism-mesh workload
 PRISM_METRIC = "DOF-solves/s at 1e-8 rel. residual of P2 elasticity on the reference's prism mesh"
 
@@ -1659,6 +1742,8 @@ def main():
         run_stream(opt, rank, world, local)
     elif opt.workload == "prism":
         run_prism(opt, rank, world, local)
+    elif opt.workload == "direct":
+        run_direct(opt, rank, world, local)
     else:
         run_ours(opt, rank, world, local)
 
