@@ -515,9 +515,9 @@ __global__ void __launch_bounds__(TH)
 // ------------------------------------------------------------------ stencil tiles by bulk copy
 // The finest level's Chebyshev steps and residuals with the row-own arrays streamed into shared
 // memory. Each block of 1024 threads takes tiles of STENCIL_TILE rows, 1 row per thread. One
-// thread issues 1D bulk copies (cp.async.bulk into this block's own shared memory) of the tile's K coefficient
-// arrays, b, and for a step D^-1 and d, completing on an mbarrier; the next tile's copies run
-// while this tile computes (2 stages). The rows' x neighbours, and the coefficients of rows
+// thread issues 1D bulk copies (cp.async.bulk into the block's own shared memory) of the tile's
+// K coefficient arrays, b, and for a step D^-1 and d, completing on an mbarrier; the next tile's
+// copies run while this tile computes (2 stages). The rows' x neighbours, and the coefficients of rows
 // above the tile, come from L1/L2 as in StencilOpK. The arithmetic is StencilOpK's and
 // cheb_step_row's / residual_row's in the same order on the same values, so the bits are those
 // of the kernels it replaces. A partial last tile reads global memory directly. Every wait on an
